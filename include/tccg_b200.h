@@ -1,0 +1,183 @@
+/*
+ * tccg_b200 -- C ABI of the B200 tensor-contraction library.
+ *
+ * Computes  C = alpha * contract(A, B) + beta * C  for dense or strided
+ * tensors on one NVIDIA B200 (sm_100a). All pointers are device pointers
+ * owned by the caller; every call is stream-ordered on the given stream
+ * (a cudaStream_t passed as void*; NULL = legacy default stream).
+ *
+ * Every function returns 0 on success or a negative TCCG_ERR_* code and never
+ * aborts the process; tccg_last_error() returns a thread-local message.
+ *
+ * Boundary with the reference (HPAC/tccg), which emits one specialised C++
+ * function per contraction:
+ *
+ *   void gett(float* A, float* B, float* C, const float alpha, const float beta)
+ *       -- tccg/gett.py:342-344 (the name is `gett` for the fastest candidate,
+ *          gett.py:1240-1241; `double` for --floatType=d). Extents and strides
+ *          are compile-time constants there; here they are a tccg_desc bound
+ *          once into a tccg_plan (tccg_plan_create), which plays the role of
+ *          the specialised function, and tccg_plan_run is the call.
+ *   int ttgemmt_<cand>(cublasHandle_t, const T* A, const T* B, T* C, T alpha,
+ *                      T beta, T* work_)
+ *       -- tccg/ttgemmt.py:212-214, 296-300 (returns the workspace size when
+ *          work_ == NULL). Replaced by tccg_plan_create with
+ *          TCCG_METHOD_TTGT plus tccg_plan_workspace / tccg_plan_run.
+ *   int LoG_<...>(cublasHandle_t, const T* A, const T* B, T* C, T alpha, T beta)
+ *       -- tccg/gemm_loop.py:94-97. Replaced by TCCG_METHOD_LOG.
+ *   hptt::create_plan(perm, dim, alpha, A, size, outerSizeA, beta, B,
+ *                     outerSizeB, ...)->execute()
+ *       -- the transposition TCCG's TTGT and GETT packing call
+ *          (tccg/transpose.py:140-141). Replaced by tccg_transpose.
+ *
+ * The emitted per-contraction artifact (python -m tccg_b200 file.tccg) wraps
+ * a plan behind TCCG's exact `gett(A, B, C, alpha, beta)` signature.
+ */
+#ifndef TCCG_B200_H
+#define TCCG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCCG_MAX_MODES 12 /* per index class (M, N or K) after index fusion */
+
+/* error codes */
+#define TCCG_OK 0
+#define TCCG_ERR_INVALID (-1)      /* bad argument or descriptor */
+#define TCCG_ERR_UNSUPPORTED (-2)  /* valid request this build cannot run */
+#define TCCG_ERR_WORKSPACE (-3)    /* workspace missing or too small */
+#define TCCG_ERR_CUDA (-4)         /* a CUDA runtime call failed */
+#define TCCG_ERR_ALIGNMENT (-5)    /* pointer alignment requirement not met */
+#define TCCG_ERR_DEVICE (-6)       /* a kernel reported an error (e.g. a bounded wait ran out) */
+
+/* operand element types */
+#define TCCG_F32 0
+#define TCCG_F64 1
+#define TCCG_BF16 2
+
+/* arithmetic of the contraction */
+#define TCCG_PREC_FP32 0   /* FP32 FFMA on the CUDA cores */
+#define TCCG_PREC_FP64 1   /* FP64 DFMA; k-split partial sums and alpha/beta in FP64 */
+#define TCCG_PREC_BF16 2   /* BF16 products on tcgen05 tensor cores, FP32 accumulation in TMEM */
+#define TCCG_PREC_BF16X3 3 /* split-BF16x3: a*b ~ ah*bh + ah*bl + al*bh on tcgen05, FP32 accumulation */
+
+/* method (TCCG's three code styles, tccg/tccg.py:121-130) */
+#define TCCG_METHOD_GETT 0
+#define TCCG_METHOD_TTGT 1
+#define TCCG_METHOD_LOG 2
+
+/*
+ * A contraction in GETT form (TCCG's classification, tccg/tccg_util.py:212-296,
+ * 597-611): M = indices of C that are in the operand holding C's stride-one
+ * index ("GA"), N = indices of C in the other operand ("GB"), K = contracted
+ * indices. Strides are in elements; the M, N and K modes are listed in the
+ * linearisation order the kernels use (first = fastest). swap_ab != 0 says
+ * that GA is the caller's B: tccg_plan_run then reads its B argument as GA
+ * (the operand swap of tccg/gett.py:70-76), so callers always pass (A, B) in
+ * file order.
+ */
+typedef struct tccg_desc {
+  int32_t nm, nn, nk;
+  int32_t swap_ab;
+  int64_t m_ext[TCCG_MAX_MODES];
+  int64_t n_ext[TCCG_MAX_MODES];
+  int64_t k_ext[TCCG_MAX_MODES];
+  int64_t a_m_stride[TCCG_MAX_MODES]; /* GA stride of each M mode */
+  int64_t a_k_stride[TCCG_MAX_MODES]; /* GA stride of each K mode */
+  int64_t b_n_stride[TCCG_MAX_MODES]; /* GB stride of each N mode */
+  int64_t b_k_stride[TCCG_MAX_MODES]; /* GB stride of each K mode */
+  int64_t c_m_stride[TCCG_MAX_MODES]; /* C stride of each M mode */
+  int64_t c_n_stride[TCCG_MAX_MODES]; /* C stride of each N mode */
+} tccg_desc;
+
+/* Kernel choices the autotuner searches over; zero-initialised = defaults. */
+typedef struct tccg_tuning {
+  int32_t method;      /* TCCG_METHOD_* */
+  int32_t variant;     /* kernel tile variant (0 = default; see tccg_plan_describe) */
+  int32_t ksplit;      /* k-split factor for the SIMT kernels (0/1 = none) */
+  int32_t raster;      /* tile-raster group size of the persistent tcgen05 kernel (0 = default) */
+  int32_t max_ctas;    /* persistent grid size cap (0 = one CTA per SM) */
+  int32_t reserved[3];
+} tccg_tuning;
+
+typedef struct tccg_plan tccg_plan; /* opaque */
+
+/* Library version string and the build's target ("sm_100a"). */
+const char* tccg_version(void);
+
+/* Thread-local message of the last failing call on this thread. */
+const char* tccg_last_error(void);
+
+/*
+ * Bind a contraction to a plan: validates the descriptor, builds the offset
+ * tables (uploaded to the current device) and picks kernels.
+ * dtype: element type of A and B (TCCG_F32, TCCG_BF16 or TCCG_F64); C is
+ * float for TCCG_F32/TCCG_BF16 and double for TCCG_F64. tuning may be NULL.
+ */
+int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t precision,
+                     const tccg_tuning* tuning, tccg_plan** out);
+
+/* Bytes of device workspace tccg_plan_run needs (ws_bytes >= this). */
+int tccg_plan_workspace(const tccg_plan* plan, size_t* bytes);
+
+/*
+ * C = alpha * contract(A, B) + beta * C on `stream`. A and B are in the
+ * caller's (file) order; ws must be 256-byte aligned when ws_bytes > 0.
+ * With beta == 0, C is written without being read (as TCCG's update=0 path).
+ */
+int tccg_plan_run(const tccg_plan* plan, const void* A, const void* B, void* C, double alpha,
+                  double beta, void* ws, size_t ws_bytes, void* stream);
+
+/* Human-readable plan summary (method, kernels, tiles, workspace). */
+int tccg_plan_describe(const tccg_plan* plan, char* buf, size_t len);
+
+/* FLOPs of one run by TCCG's count (tccg/tccg.py:1230-1234): 2MNK (+3MN if beta != 0). */
+double tccg_plan_flops(const tccg_plan* plan, double beta);
+
+int tccg_plan_destroy(tccg_plan* plan);
+
+/*
+ * Device-side status of the plan's kernels since the last call: 0, or the
+ * TCCG_DEVSTAT_* code a kernel recorded (a bounded wait that ran out, ...).
+ * Synchronises the device, reads and clears the word.
+ */
+#define TCCG_DEVSTAT_TIMEOUT_PRODUCER 1
+#define TCCG_DEVSTAT_TIMEOUT_MMA 2
+#define TCCG_DEVSTAT_TIMEOUT_EPILOGUE 3
+int tccg_plan_status(const tccg_plan* plan, int32_t* device_status);
+
+/*
+ * HPTT-style out-of-place transposition (the call TCCG emits at
+ * tccg/transpose.py:140-141):  B[perm(i)] = alpha * A[i] + beta * B[perm(i)],
+ * where dimension j of B is dimension perm[j] of A. size[] are A's extents,
+ * outer_a / outer_b the padded extents (NULL = dense). beta == 0 does not read B.
+ */
+int tccg_transpose(int32_t dtype, int32_t dim, const int32_t* perm, const int64_t* size,
+                   const int64_t* outer_a, const int64_t* outer_b, double alpha, const void* A,
+                   double beta, void* B, void* stream);
+
+/*
+ * Grouped launch: many plans of the same precision run by ONE persistent
+ * kernel launch (plus one packing launch). tccg_group_bind fixes the operand
+ * pointers and workspace (it uploads the work list, synchronously), after
+ * which tccg_group_run only launches kernels and can be captured in a CUDA
+ * graph.
+ */
+typedef struct tccg_group tccg_group; /* opaque */
+int tccg_group_create(const tccg_plan* const* plans, int32_t count, tccg_group** out);
+int tccg_group_workspace(const tccg_group* group, size_t* bytes);
+int tccg_group_bind(tccg_group* group, const void* const* A, const void* const* B,
+                    void* const* C, const double* alpha, const double* beta, void* ws,
+                    size_t ws_bytes);
+int tccg_group_run(const tccg_group* group, void* stream);
+int tccg_group_destroy(tccg_group* group);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCCG_B200_H */

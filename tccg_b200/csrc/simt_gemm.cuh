@@ -1,0 +1,271 @@
+// SIMT GETT kernels: FP32 FFMA and FP64 DFMA on the CUDA cores.
+//
+// Operands come packed MN-major by pack_kernel (Ap[k][Mp], Bp[k][Np], zero
+// padded), so the main loop is a dense 16-byte cp.async pipeline. The
+// epilogue writes C straight into its own (multi-index) layout through the
+// offset tables: element (m, n) of the GETT view is C[c_m_off[m] + c_n_off[n]].
+// That is GETT's defining property (TCCG's micro-kernel stores into C's
+// original layout, tccg/gett.py:192-223) -- there is no C transposition.
+//
+// beta == 0 writes C without reading it (TCCG's update = 0 path,
+// tccg/gett.py:516-525). With a k-split the CTAs of split z write raw partial
+// sums to a workspace and simt_reduce_kernel adds them (in T: FP64 for the
+// double path) and applies alpha/beta, like TCCG's k-split with one private C
+// per k-group and a final sum (tccg/gett.py:755-781).
+#pragma once
+#include "common.cuh"
+
+namespace tccg {
+
+template <typename T>
+struct SimtCfg;
+
+template <>
+struct SimtCfg<float> {
+  static constexpr int BM = 128, BN = 128, BK = 16;
+  static constexpr int WARPS_M = 2, WARPS_N = 4;
+  static constexpr int TMG = 2, TNG = 2;  // 4-wide groups per thread along m / n
+  static constexpr int STAGES = 4;
+  static constexpr int EPN = 64;          // epilogue columns per pass
+  static constexpr int PAD = 4;
+};
+
+template <>
+struct SimtCfg<double> {
+  static constexpr int BM = 128, BN = 64, BK = 8;
+  static constexpr int WARPS_M = 2, WARPS_N = 4;
+  static constexpr int TMG = 2, TNG = 1;
+  static constexpr int STAGES = 4;
+  static constexpr int EPN = 32;
+  static constexpr int PAD = 2;
+};
+
+template <typename T>
+struct SimtArgs {
+  const T* Ap;  // [Kp][Mp]
+  const T* Bp;  // [Kp][Np]
+  int64_t Mp, Np, M, N;
+  int32_t ktiles;          // Kp / BK
+  int32_t ktiles_per_split;
+  T* C;
+  const int64_t* c_m_off;
+  const int64_t* c_n_off;
+  T alpha, beta;
+  T* partial;  // non-null: write raw sums to partial[z][n][Mp]
+};
+
+template <typename T>
+constexpr size_t simt_smem_bytes() {
+  using Cfg = SimtCfg<T>;
+  size_t pipe = (size_t)Cfg::STAGES * Cfg::BK * (Cfg::BM + Cfg::BN) * sizeof(T);
+  size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T);
+  return pipe > epi ? pipe : epi;
+}
+
+template <typename T>
+struct Vec4 {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ Vec4<T> lds4(const T* p) {
+  Vec4<T> r;
+  if constexpr (sizeof(T) == 4) {
+    float4 x = *reinterpret_cast<const float4*>(p);
+    r.v[0] = x.x; r.v[1] = x.y; r.v[2] = x.z; r.v[3] = x.w;
+  } else {
+    double2 x = *reinterpret_cast<const double2*>(p);
+    double2 y = *reinterpret_cast<const double2*>(p + 2);
+    r.v[0] = x.x; r.v[1] = x.y; r.v[2] = y.x; r.v[3] = y.y;
+  }
+  return r;
+}
+
+// One BM x BN tile (bx, by) of split bz; all 256 threads of the CTA take part.
+template <typename T>
+__device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int by, int bz) {
+  using Cfg = SimtCfg<T>;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
+  constexpr int TM = Cfg::TMG * 4, TN = Cfg::TNG * 4;
+  constexpr int VEC = 16 / sizeof(T);                 // elements per 16-byte chunk
+  constexpr int A_CHUNKS = BK * BM / VEC, B_CHUNKS = BK * BN / VEC;
+  constexpr int A_ROW_CHUNKS = BM / VEC, B_ROW_CHUNKS = BN / VEC;
+  static_assert(Cfg::WARPS_M * Cfg::TMG * 32 == BM, "tile M");
+  static_assert(Cfg::WARPS_N * Cfg::TNG * 16 == BN, "tile N");
+
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);              // [STAGES][BK][BM]
+  T* Bs = As + (size_t)STAGES * BK * BM;               // [STAGES][BK][BN]
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
+  const int lm = lane & 7, ln = lane >> 3;
+  const int64_t m0 = (int64_t)bx * BM, n0 = (int64_t)by * BN;
+  const int kt_begin = bz * a.ktiles_per_split;
+  int kt_end = kt_begin + a.ktiles_per_split;
+  if (kt_end > a.ktiles) kt_end = a.ktiles;
+
+  auto load_stage = [&](int stage, int kt) {
+    T* as = As + (size_t)stage * BK * BM;
+    T* bs = Bs + (size_t)stage * BK * BN;
+    const int64_t krow = (int64_t)kt * BK;
+#pragma unroll
+    for (int c = tid; c < A_CHUNKS; c += 256) {
+      const int row = c / A_ROW_CHUNKS, col = (c % A_ROW_CHUNKS) * VEC;
+      cp_async_16(as + row * BM + col, a.Ap + (krow + row) * a.Mp + m0 + col);
+    }
+#pragma unroll
+    for (int c = tid; c < B_CHUNKS; c += 256) {
+      const int row = c / B_ROW_CHUNKS, col = (c % B_ROW_CHUNKS) * VEC;
+      cp_async_16(bs + row * BN + col, a.Bp + (krow + row) * a.Np + n0 + col);
+    }
+  };
+
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (kt_begin + s < kt_end) load_stage(s, kt_begin + s);
+    cp_async_commit();
+  }
+
+  const int a_off = wm * (Cfg::TMG * 32) + lm * 4;
+  const int b_off = wn * (Cfg::TNG * 16) + ln * 4;
+  for (int kt = kt_begin; kt < kt_end; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + STAGES - 1;
+      if (nk < kt_end) load_stage((nk - kt_begin) % STAGES, nk);
+      cp_async_commit();
+    }
+    const int stage = (kt - kt_begin) % STAGES;
+    const T* as = As + (size_t)stage * BK * BM;
+    const T* bs = Bs + (size_t)stage * BK * BN;
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      T av[TM], bv[TN];
+#pragma unroll
+      for (int g = 0; g < Cfg::TMG; ++g) {
+        Vec4<T> x = lds4<T>(as + k * BM + a_off + g * 32);
+        av[g * 4 + 0] = x.v[0]; av[g * 4 + 1] = x.v[1]; av[g * 4 + 2] = x.v[2]; av[g * 4 + 3] = x.v[3];
+      }
+#pragma unroll
+      for (int g = 0; g < Cfg::TNG; ++g) {
+        Vec4<T> x = lds4<T>(bs + k * BN + b_off + g * 16);
+        bv[g * 4 + 0] = x.v[0]; bv[g * 4 + 1] = x.v[1]; bv[g * 4 + 2] = x.v[2]; bv[g * 4 + 3] = x.v[3];
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // thread fragment coordinates (tile-local)
+  auto mloc = [&](int i) { return a_off + (i / 4) * 32 + (i % 4); };
+  auto nloc = [&](int j) { return b_off + (j / 4) * 16 + (j % 4); };
+
+  if (a.partial != nullptr) {
+    T* P = a.partial + (size_t)bz * a.Np * a.Mp;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int64_t n = n0 + nloc(j);
+#pragma unroll
+      for (int i = 0; i < TM; ++i) P[n * a.Mp + m0 + mloc(i)] = acc[i][j];
+    }
+    return;
+  }
+
+  // Epilogue through shared memory so that each warp stores 32 consecutive m
+  // (C's stride-one index is the first M mode) -> coalesced C traffic.
+  constexpr int EPN = Cfg::EPN, LDC = BM + Cfg::PAD;
+  T* Cs = reinterpret_cast<T*>(smem_raw);  // [EPN][LDC]
+  const int m_l = tid % BM;
+  const int64_t m = m0 + m_l;
+  const bool m_ok = m < a.M;
+  const int64_t cmo = m_ok ? a.c_m_off[m] : 0;
+  const T alpha = a.alpha, beta = a.beta;
+  for (int p = 0; p < BN / EPN; ++p) {
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int nl = nloc(j) - p * EPN;
+      if (nl >= 0 && nl < EPN) {
+#pragma unroll
+        for (int i = 0; i < TM; ++i) Cs[nl * LDC + mloc(i)] = acc[i][j];
+      }
+    }
+    __syncthreads();
+    if (m_ok) {
+      constexpr int NSTEP = 256 / BM;
+      for (int nl = tid / BM; nl < EPN; nl += NSTEP) {
+        const int64_t n = n0 + p * EPN + nl;
+        if (n < a.N) {
+          T* dst = a.C + cmo + a.c_n_off[n];
+          T v = alpha * Cs[nl * LDC + m_l];
+          if (beta != T(0)) v = fma(beta, *dst, v);
+          *dst = v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) simt_gett_kernel(const SimtArgs<T> a) {
+  simt_gett_tile<T>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Grouped launch: item i owns CTAs [tile_begin[i], tile_begin[i+1]); the CTA
+// finds its item by binary search and runs the same tile code.
+template <typename T>
+struct SimtGroupItem {
+  SimtArgs<T> args;
+  int64_t tile_begin;
+  int32_t tiles_m, pad;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) simt_gett_group_kernel(const SimtGroupItem<T>* items,
+                                                                  int n_items) {
+  const int64_t t = blockIdx.x;
+  int lo = 0, hi = n_items - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+  }
+  const SimtGroupItem<T>& it = items[lo];
+  const int64_t local = t - it.tile_begin;
+  simt_gett_tile<T>(it.args, (int)(local % it.tiles_m), (int)(local / it.tiles_m), 0);
+}
+
+// C = alpha * sum_z partial[z] + beta * C.
+// grid = (ceil(M/256), min(N, 65535)), block 256; n strides by gridDim.y.
+template <typename T>
+__global__ void __launch_bounds__(256) simt_reduce_kernel(const T* __restrict__ partial,
+                                                          int splits, int64_t Mp, int64_t Np,
+                                                          int64_t M, int64_t N, T* C,
+                                                          const int64_t* c_m_off,
+                                                          const int64_t* c_n_off, T alpha,
+                                                          T beta) {
+  const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (m >= M) return;
+  const int64_t cmo = c_m_off[m];
+  for (int64_t n = blockIdx.y; n < N; n += gridDim.y) {
+    T s = T(0);
+    for (int z = 0; z < splits; ++z) s += partial[(size_t)z * Np * Mp + n * Mp + m];
+    T* dst = C + cmo + c_n_off[n];
+    T v = alpha * s;
+    if (beta != T(0)) v = fma(beta, *dst, v);
+    *dst = v;
+  }
+}
+
+}  // namespace tccg

@@ -1,0 +1,337 @@
+// tcgen05 GETT kernel (sm_100a): BF16 and split-BF16x3 products on the 5th
+// generation tensor cores with FP32 accumulation in tensor memory.
+//
+// Operands arrive packed K-major by pack_kernel: GA as [M][Kc] and GB as
+// [N][Kc] bf16 rows. In BF16 mode a 128-byte row chunk holds 64 consecutive k;
+// in BF16X3 mode it holds [hi(k..k+31) | lo(k..k+31)], so both modes load the
+// same TMA boxes (64 x 128 rows for GA, 64 x 256 rows for GB, 128-byte
+// swizzle) and only the MMA schedule differs:
+//   BF16  : 4 MMAs (k-steps of 16) per stage
+//   BF16X3: per k-step of 16, D += ah*bh, D += ah*bl, D += al*bh
+// (al*bl, ~2^-16 relative, is dropped).
+//
+// Structure: one persistent CTA per SM, 6 warps.
+//   warp 0     TMA producer (one lane): STAGES-deep smem ring, mbarrier full/empty
+//   warp 1     TMEM owner + MMA issuer (one lane): 128x256 UMMA tiles into one of
+//              two 256-column FP32 accumulators (double buffering)
+//   warps 2-5  epilogue: tcgen05.ld of their 32-lane TMEM quadrant, then
+//              C[c_m_off[m] + c_n_off[n]] = alpha*acc (+ beta*C), written straight
+//              into C's own layout (GETT: no transposition of C).
+// Every mbarrier wait is bounded (TCCG_DEVICE_WAIT_NS); a wait that runs out
+// records an error code in *status and the CTA winds down: in-flight TMA loads
+// and MMAs are waited for (bounded) and TMEM is released before returning.
+#pragma once
+#include <cuda.h>
+#include "common.cuh"
+
+namespace tccg {
+
+struct TcCfg {
+  static constexpr int BM = 128, BN = 256;
+  static constexpr int ROW_BYTES = 128;  // one swizzle row per operand row per stage
+  static constexpr int STAGES = 4;
+  static constexpr int A_STAGE = BM * ROW_BYTES;   // 16 KB
+  static constexpr int B_STAGE = BN * ROW_BYTES;   // 32 KB
+  static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+  static constexpr int TMEM_COLS = 2 * BN;         // two FP32 accumulators
+  static constexpr int NUM_THREADS = 192;
+  static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
+};
+
+enum TcMode : int { TC_BF16 = 0, TC_BF16X3 = 1 };
+
+struct TcArgs {
+  int32_t M, N, K;
+  int32_t num_kb;           // 128-byte k-chunks per row: BF16 ceil(K/64), BF16X3 ceil(K/32)
+  int32_t tiles_m, tiles_n;
+  int32_t raster;           // tiles along m per raster group
+  int32_t pad0;
+  float* C;
+  const int64_t* c_m_off;
+  const int64_t* c_n_off;
+  float alpha, beta;
+  int32_t* status;
+};
+
+// Grouped launch: one entry per contraction, in device memory. The tensor maps
+// live here (64-byte aligned) and are read by TMA from global memory.
+struct __align__(64) TcGroupItem {
+  CUtensorMap tmA;
+  CUtensorMap tmB;
+  TcArgs args;
+  int64_t tile_begin;  // first global tile of this item
+};
+
+struct TcGroup {
+  const TcGroupItem* items;
+  int32_t n_items;
+  int32_t total_tiles;
+};
+
+__device__ __forceinline__ void record_error(int32_t* status, int32_t code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+__device__ __forceinline__ void tile_coords(int tile, const TcArgs& a, int& tm, int& tn) {
+  const int group = a.raster * a.tiles_n;
+  const int gid = tile / group;
+  const int first_m = gid * a.raster;
+  int gm = a.tiles_m - first_m;
+  if (gm > a.raster) gm = a.raster;
+  const int r = tile - gid * group;
+  tm = first_m + r % gm;
+  tn = r / gm;
+}
+
+// Resolves a global tile index to (item arguments, tensor maps, tile coords).
+struct TileRef {
+  const TcArgs* a;
+  const CUtensorMap* tA;
+  const CUtensorMap* tB;
+  int tm, tn;
+};
+
+template <bool GROUPED>
+__device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA,
+                                                const CUtensorMap* tmB, const TcArgs* a1,
+                                                const TcGroup& g) {
+  TileRef r;
+  if constexpr (GROUPED) {
+    int lo = 0, hi = g.n_items - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (g.items[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    const TcGroupItem& it = g.items[lo];
+    r.a = &it.args;
+    r.tA = &it.tmA;
+    r.tB = &it.tmB;
+    tile_coords(tile - (int)it.tile_begin, it.args, r.tm, r.tn);
+  } else {
+    r.a = a1;
+    r.tA = tmA;
+    r.tB = tmB;
+    tile_coords(tile, *a1, r.tm, r.tn);
+  }
+  return r;
+}
+
+template <int MODE, bool GROUPED>
+__device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUtensorMap* tmB,
+                                             const TcArgs* a1, const TcGroup& g,
+                                             int32_t* status) {
+  using Cfg = TcCfg;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + (((raw_addr + 1023u) & ~1023u) - raw_addr);
+  uint8_t* sA = smem;                                   // STAGES x 16 KB
+  uint8_t* sB = smem + Cfg::STAGES * Cfg::A_STAGE;      // STAGES x 32 KB
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
+  uint64_t* full = bars;                   // [STAGES]
+  uint64_t* empty = bars + Cfg::STAGES;    // [STAGES]
+  uint64_t* accf = bars + 2 * Cfg::STAGES; // [2] accumulator ready
+  uint64_t* acce = accf + 2;               // [2] accumulator drained
+  uint64_t* drain = acce + 2;              // MMA completion on the abort path
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int num_tiles = GROUPED ? g.total_tiles : a1->tiles_m * a1->tiles_n;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    mbar_init(drain, 1);
+    fence_mbar_init();
+    if (!GROUPED) {
+      tma_prefetch_desc(tmA);
+      tma_prefetch_desc(tmB);
+    }
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    int stage = 0;
+    uint32_t phase = 0;
+    int issued_phase[Cfg::STAGES];
+    for (int s = 0; s < Cfg::STAGES; ++s) issued_phase[s] = -1;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+      const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
+      const int nkb = t.a->num_kb;
+      for (int kb = 0; kb < nkb; ++kb) {
+        if (!mbar_wait(&empty[stage], phase ^ 1)) {
+          record_error(status, 1);
+          ok = false;
+          break;
+        }
+        mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
+        tma_load_2d(sA + stage * Cfg::A_STAGE, t.tA, kb * 64, t.tm * Cfg::BM, &full[stage]);
+        tma_load_2d(sB + stage * Cfg::B_STAGE, t.tB, kb * 64, t.tn * Cfg::BN, &full[stage]);
+        issued_phase[stage] = (int)phase;
+        if (++stage == Cfg::STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+    }
+    if (!ok) {  // let in-flight copies land before the CTA's smem goes away
+      for (int s = 0; s < Cfg::STAGES; ++s)
+        if (issued_phase[s] >= 0) (void)mbar_wait(&full[s], (uint32_t)issued_phase[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t idesc = idesc_bf16_f32(Cfg::BM, Cfg::BN);
+    int stage = 0;
+    uint32_t phase = 0;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true, issued_any = false;
+    for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+      const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
+      const int nkb = t.a->num_kb, K = t.a->K;
+      if (!mbar_wait(&acce[acc], acc_phase ^ 1)) {
+        record_error(status, 2);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d_tmem = tbase + (uint32_t)(acc * Cfg::BN);
+      uint32_t accumulate = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        if (!mbar_wait(&full[stage], phase)) {
+          record_error(status, 2);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t ad = umma_desc_k128(smem_u32(sA + stage * Cfg::A_STAGE));
+        const uint64_t bd = umma_desc_k128(smem_u32(sB + stage * Cfg::B_STAGE));
+        if constexpr (MODE == TC_BF16) {
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            if (kb * 64 + ks * 16 < K) {
+              tc_mma_f16(d_tmem, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);
+              accumulate = 1;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            if (kb * 32 + ks * 16 < K) {
+              // descriptor start address is in 16-byte units: +2 = 32 B (16 bf16),
+              // +4 = 64 B (the lo half of the 128-byte row)
+              tc_mma_f16(d_tmem, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);      // ah*bh
+              tc_mma_f16(d_tmem, ad + 2 * ks, bd + 4 + 2 * ks, idesc, 1);           // ah*bl
+              tc_mma_f16(d_tmem, ad + 4 + 2 * ks, bd + 2 * ks, idesc, 1);           // al*bh
+              accumulate = 1;
+            }
+          }
+        }
+        issued_any = true;
+        tc_commit(&empty[stage]);  // frees the smem stage when these MMAs finish
+        if (++stage == Cfg::STAGES) {
+          stage = 0;
+          phase ^= 1;
+        }
+      }
+      if (!ok) break;
+      tc_commit(&accf[acc]);  // accumulator ready for the epilogue
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+    if (!ok && issued_any) {  // wait for outstanding MMAs before TMEM is released
+      tc_commit(drain);
+      (void)mbar_wait(drain, 0);
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue ----------------
+    const int q = warp & 3;  // TMEM lanes [32q, 32q+32) are accessible to this warp
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+      const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
+      const TcArgs& a = *t.a;
+      const float alpha = a.alpha, beta = a.beta;
+      if (!mbar_wait(&accf[acc], acc_phase)) {
+        record_error(status, 3);
+        break;
+      }
+      tc_fence_after();
+      const int64_t m = (int64_t)t.tm * Cfg::BM + q * 32 + lane;
+      const bool m_ok = m < a.M;
+      const int64_t cmo = m_ok ? a.c_m_off[m] : 0;
+      const int64_t nbase = (int64_t)t.tn * Cfg::BN;
+      const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * Cfg::BN);
+#pragma unroll 1
+      for (int c = 0; c < Cfg::BN; c += 32) {
+        uint32_t r[32];
+        tmem_ld_32x32b_x32(trow + (uint32_t)c, r);
+        tmem_ld_wait();
+        if (c == Cfg::BN - 32) {  // accumulator fully read: hand it back to the MMA warp
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[acc]);
+        }
+        if (m_ok) {
+          const int64_t nlim = a.N - (nbase + c);
+          if (beta != 0.0f) {
+            float old[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              old[j] = (j < nlim) ? a.C[cmo + __ldg(a.c_n_off + nbase + c + j)] : 0.0f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (j < nlim)
+                a.C[cmo + __ldg(a.c_n_off + nbase + c + j)] =
+                    fmaf(beta, old[j], alpha * __uint_as_float(r[j]));
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (j < nlim)
+                a.C[cmo + __ldg(a.c_n_off + nbase + c + j)] = alpha * __uint_as_float(r[j]);
+          }
+        }
+      }
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tbase, Cfg::TMEM_COLS);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TcCfg::NUM_THREADS, 1)
+    gett_tc_kernel(const __grid_constant__ CUtensorMap tmA,
+                   const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
+  TcGroup g{nullptr, 0, 0};
+  gett_tc_body<MODE, false>(&tmA, &tmB, &a, g, a.status);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TcCfg::NUM_THREADS, 1)
+    gett_tc_group_kernel(const TcGroup g, int32_t* status) {
+  gett_tc_body<MODE, true>(nullptr, nullptr, nullptr, g, status);
+}
+
+}  // namespace tccg

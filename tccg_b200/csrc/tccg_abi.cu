@@ -1,0 +1,920 @@
+// C ABI of tccg_b200 (declared in include/tccg_b200.h): plan objects, kernel
+// dispatch, tensor-map encoding, transposition and grouped launches.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tccg_b200.h"
+#include "common.cuh"
+#include "pack.cuh"
+#include "simt_gemm.cuh"
+#include "tc_gemm.cuh"
+#include "transpose.cuh"
+
+using namespace tccg;
+
+// --------------------------------------------------------------------------
+// errors
+// --------------------------------------------------------------------------
+static thread_local char g_err[1024] = "";
+
+static int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (expr);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(TCCG_ERR_CUDA, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                     \
+  } while (0)
+
+extern "C" const char* tccg_last_error(void) { return g_err; }
+extern "C" const char* tccg_version(void) { return "tccg_b200 0.1 (sm_100a)"; }
+
+// --------------------------------------------------------------------------
+// plan
+// --------------------------------------------------------------------------
+struct tccg_plan {
+  tccg_desc d;
+  int32_t dtype = 0, prec = 0;
+  tccg_tuning tune{};
+  int device = 0;
+  int num_sms = 148;
+  int64_t M = 1, N = 1, K = 1;
+  // device offset tables (elements)
+  int64_t* t_a_m = nullptr;
+  int64_t* t_a_k = nullptr;
+  int64_t* t_b_n = nullptr;
+  int64_t* t_b_k = nullptr;
+  int64_t* t_c_m = nullptr;
+  int64_t* t_c_n = nullptr;
+  int64_t* t_id_m = nullptr;  // TTGT: identity tables of the contiguous C' = [M][N]
+  int64_t* t_id_n = nullptr;
+  int32_t* d_status = nullptr;
+  int32_t read_k_fast_a = 0, read_k_fast_b = 0;
+  bool c_is_mn_dense = false;  // C is already the column-major [M-modes][N-modes] matrix
+  // SIMT geometry
+  int64_t Mp = 0, Np = 0, Kp = 0;
+  int32_t ktiles = 0, ksplit = 1, ktiles_per_split = 0;
+  // tcgen05 geometry
+  int64_t Kc = 0;
+  int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0;
+  // workspace layout
+  size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
+  char describe[512] = "";
+};
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+static int64_t cdiv(int64_t x, int64_t a) { return (x + a - 1) / a; }
+
+// offsets[l] = sum_i idx_i(l) * stride_i, l the linear index over the modes
+// (first mode fastest).
+static void build_offsets(int n, const int64_t* ext, const int64_t* stride,
+                          std::vector<int64_t>& out) {
+  int64_t total = 1;
+  for (int i = 0; i < n; ++i) total *= ext[i];
+  out.resize((size_t)total);
+  int64_t idx[TCCG_MAX_MODES] = {0};
+  int64_t off = 0;
+  for (int64_t l = 0; l < total; ++l) {
+    out[(size_t)l] = off;
+    for (int i = 0; i < n; ++i) {
+      idx[i]++;
+      off += stride[i];
+      if (idx[i] < ext[i]) break;
+      off -= idx[i] * stride[i];
+      idx[i] = 0;
+    }
+  }
+}
+
+static int upload(const std::vector<int64_t>& h, int64_t** dptr) {
+  size_t bytes = std::max<size_t>(h.size(), 1) * sizeof(int64_t);
+  CUDA_TRY(cudaMalloc((void**)dptr, bytes));
+  if (!h.empty()) CUDA_TRY(cudaMemcpy(*dptr, h.data(), h.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  return TCCG_OK;
+}
+
+// Fast read direction of an operand: 1 when its first K mode (extent > 1) has
+// a smaller stride than its first row mode, i.e. consecutive k are closer in
+// memory than consecutive m (or n).
+static int32_t pick_read_k_fast(int nr, const int64_t* rext, const int64_t* rstr, int nk,
+                                const int64_t* kext, const int64_t* kstr) {
+  int64_t rs = INT64_MAX, ks = INT64_MAX;
+  for (int i = 0; i < nr; ++i)
+    if (rext[i] > 1) { rs = rstr[i] < 0 ? -rstr[i] : rstr[i]; break; }
+  for (int i = 0; i < nk; ++i)
+    if (kext[i] > 1) { ks = kstr[i] < 0 ? -kstr[i] : kstr[i]; break; }
+  return ks < rs ? 1 : 0;
+}
+
+static void plan_free(tccg_plan* p) {
+  if (!p) return;
+  int64_t* ts[] = {p->t_a_m, p->t_a_k, p->t_b_n, p->t_b_k, p->t_c_m, p->t_c_n, p->t_id_m, p->t_id_n};
+  for (auto t : ts)
+    if (t) cudaFree(t);
+  if (p->d_status) cudaFree(p->d_status);
+  delete p;
+}
+
+static int plan_layout(tccg_plan* p);
+
+extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t precision,
+                                const tccg_tuning* tuning, tccg_plan** out) {
+  if (!desc || !out) return fail(TCCG_ERR_INVALID, "null descriptor or output pointer");
+  *out = nullptr;
+  const tccg_desc& d = *desc;
+  if (d.nm < 1 || d.nn < 1 || d.nk < 1 || d.nm > TCCG_MAX_MODES || d.nn > TCCG_MAX_MODES ||
+      d.nk > TCCG_MAX_MODES)
+    return fail(TCCG_ERR_INVALID, "mode counts (nm=%d nn=%d nk=%d) must be in [1,%d]", d.nm, d.nn,
+                d.nk, TCCG_MAX_MODES);
+  if (dtype != TCCG_F32 && dtype != TCCG_F64 && dtype != TCCG_BF16)
+    return fail(TCCG_ERR_INVALID, "unknown dtype %d", dtype);
+  if (precision < TCCG_PREC_FP32 || precision > TCCG_PREC_BF16X3)
+    return fail(TCCG_ERR_INVALID, "unknown precision %d", precision);
+  if ((dtype == TCCG_F64) != (precision == TCCG_PREC_FP64))
+    return fail(TCCG_ERR_UNSUPPORTED, "FP64 operands need TCCG_PREC_FP64 and vice versa");
+  if (dtype == TCCG_BF16 && precision != TCCG_PREC_BF16)
+    return fail(TCCG_ERR_UNSUPPORTED, "BF16 operands are supported with TCCG_PREC_BF16 only");
+  int64_t M = 1, N = 1, K = 1;
+  for (int i = 0; i < d.nm; ++i) {
+    if (d.m_ext[i] < 1) return fail(TCCG_ERR_INVALID, "M extent %d is %lld", i, (long long)d.m_ext[i]);
+    M *= d.m_ext[i];
+  }
+  for (int i = 0; i < d.nn; ++i) {
+    if (d.n_ext[i] < 1) return fail(TCCG_ERR_INVALID, "N extent %d is %lld", i, (long long)d.n_ext[i]);
+    N *= d.n_ext[i];
+  }
+  for (int i = 0; i < d.nk; ++i) {
+    if (d.k_ext[i] < 1) return fail(TCCG_ERR_INVALID, "K extent %d is %lld", i, (long long)d.k_ext[i]);
+    K *= d.k_ext[i];
+  }
+  if (M > (int64_t)1 << 31 || N > (int64_t)1 << 31 || K > (int64_t)1 << 31)
+    return fail(TCCG_ERR_UNSUPPORTED, "M, N and K must each be <= 2^31");
+
+  tccg_plan* p = new tccg_plan();
+  p->d = d;
+  p->dtype = dtype;
+  p->prec = precision;
+  if (tuning) p->tune = *tuning;
+  p->M = M;
+  p->N = N;
+  p->K = K;
+  if (p->tune.method != TCCG_METHOD_GETT && p->tune.method != TCCG_METHOD_TTGT) {
+    plan_free(p);
+    return fail(TCCG_ERR_UNSUPPORTED, "method %d is not available in this build", p->tune.method);
+  }
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device);
+  if (e != cudaSuccess) {
+    plan_free(p);
+    return fail(TCCG_ERR_CUDA, "no usable CUDA device: %s", cudaGetErrorString(e));
+  }
+  std::vector<int64_t> h;
+  int rc = TCCG_OK;
+  build_offsets(d.nm, d.m_ext, d.a_m_stride, h);
+  if (!rc) rc = upload(h, &p->t_a_m);
+  build_offsets(d.nk, d.k_ext, d.a_k_stride, h);
+  if (!rc) rc = upload(h, &p->t_a_k);
+  build_offsets(d.nn, d.n_ext, d.b_n_stride, h);
+  if (!rc) rc = upload(h, &p->t_b_n);
+  build_offsets(d.nk, d.k_ext, d.b_k_stride, h);
+  if (!rc) rc = upload(h, &p->t_b_k);
+  build_offsets(d.nm, d.m_ext, d.c_m_stride, h);
+  // C is "already [M][N]" when its M modes are dense from stride 1 and the N
+  // modes continue densely after them (TTGT then needs no C transposition).
+  {
+    bool dense = true;
+    int64_t s = 1;
+    for (int i = 0; i < d.nm; ++i) { dense &= d.c_m_stride[i] == s; s *= d.m_ext[i]; }
+    for (int i = 0; i < d.nn; ++i) { dense &= d.c_n_stride[i] == s; s *= d.n_ext[i]; }
+    p->c_is_mn_dense = dense;
+  }
+  if (!rc) rc = upload(h, &p->t_c_m);
+  build_offsets(d.nn, d.n_ext, d.c_n_stride, h);
+  if (!rc) rc = upload(h, &p->t_c_n);
+  if (!rc) {
+    e = cudaMalloc((void**)&p->d_status, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int32_t));
+    if (e != cudaSuccess) rc = fail(TCCG_ERR_CUDA, "status word: %s", cudaGetErrorString(e));
+  }
+  p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
+  p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
+  if (!rc) rc = plan_layout(p);
+  if (rc) {
+    plan_free(p);
+    return rc;
+  }
+  *out = p;
+  return TCCG_OK;
+}
+
+static int plan_layout(tccg_plan* p) {
+  size_t ws = 0;
+  const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
+  if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) {
+    const bool dbl = p->prec == TCCG_PREC_FP64;
+    const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
+    const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+    const int BK = dbl ? SimtCfg<double>::BK : SimtCfg<float>::BK;
+    const size_t es = dbl ? 8 : 4;
+    p->Mp = round_up(p->M, BM);
+    p->Np = round_up(p->N, BN);
+    p->Kp = round_up(p->K, BK);
+    p->ktiles = (int32_t)(p->Kp / BK);
+    int ks = p->tune.ksplit > 1 ? p->tune.ksplit : 1;
+    if (ks > p->ktiles) ks = p->ktiles;
+    p->ktiles_per_split = (int32_t)cdiv(p->ktiles, ks);
+    ks = (int32_t)cdiv(p->ktiles, p->ktiles_per_split);  // no empty splits
+    p->ksplit = ks;
+    p->off_a = 0;
+    ws = align_up((size_t)(p->Kp * p->Mp) * es, 256);
+    p->off_b = ws;
+    ws = align_up(ws + (size_t)(p->Kp * p->Np) * es, 256);
+    if (p->ksplit > 1) {
+      p->off_part = ws;
+      ws = align_up(ws + (size_t)p->ksplit * p->Np * p->Mp * es, 256);
+    }
+    snprintf(p->describe, sizeof(p->describe),
+             "method=%s prec=%s kernel=simt_gett<%s> tile=%dx%dx%d M=%lld N=%lld K=%lld "
+             "ksplit=%d pack=MN(read_k_fast a=%d b=%d)",
+             ttgt ? "TTGT" : "GETT", dbl ? "fp64" : "fp32", dbl ? "f64" : "f32", BM, BN, BK,
+             (long long)p->M, (long long)p->N, (long long)p->K, p->ksplit, p->read_k_fast_a,
+             p->read_k_fast_b);
+  } else {
+    const bool x3 = p->prec == TCCG_PREC_BF16X3;
+    if (x3) {
+      p->Kc = 2 * round_up(p->K, 32);
+      p->num_kb = (int32_t)cdiv(p->K, 32);
+    } else {
+      p->Kc = round_up(p->K, 8);
+      p->num_kb = (int32_t)cdiv(p->K, 64);
+    }
+    p->tiles_m = (int32_t)cdiv(p->M, TcCfg::BM);
+    p->tiles_n = (int32_t)cdiv(p->N, TcCfg::BN);
+    p->raster = p->tune.raster > 0 ? p->tune.raster : 8;
+    const int64_t tiles = (int64_t)p->tiles_m * p->tiles_n;
+    if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
+    int ctas = p->tune.max_ctas > 0 ? std::min(p->tune.max_ctas, p->num_sms) : p->num_sms;
+    p->grid = (int32_t)std::min<int64_t>(tiles, ctas);
+    p->off_a = 0;
+    ws = align_up((size_t)(p->M * p->Kc) * 2, 256);
+    p->off_b = ws;
+    ws = align_up(ws + (size_t)(p->N * p->Kc) * 2, 256);
+    snprintf(p->describe, sizeof(p->describe),
+             "method=%s prec=%s kernel=gett_tc<%s> tile=128x256 stages=%d M=%lld N=%lld K=%lld "
+             "kblocks=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d)",
+             ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", x3 ? "BF16X3" : "BF16",
+             TcCfg::STAGES, (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->grid,
+             p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b);
+  }
+  if (ttgt) {
+    // contiguous C' = [M][N] (column-major) in the workspace, then C' -> C
+    const size_t es = p->prec == TCCG_PREC_FP64 ? 8 : 4;
+    std::vector<int64_t> h((size_t)p->M);
+    for (int64_t i = 0; i < p->M; ++i) h[(size_t)i] = i;
+    int rc = upload(h, &p->t_id_m);
+    if (rc) return rc;
+    h.resize((size_t)p->N);
+    for (int64_t i = 0; i < p->N; ++i) h[(size_t)i] = i * p->M;
+    rc = upload(h, &p->t_id_n);
+    if (rc) return rc;
+    if (!p->c_is_mn_dense) {
+      p->off_cprime = ws;
+      ws = align_up(ws + (size_t)(p->M * p->N) * es, 256);
+    }
+  }
+  p->ws_bytes = ws;
+  return TCCG_OK;
+}
+
+extern "C" int tccg_plan_workspace(const tccg_plan* p, size_t* bytes) {
+  if (!p || !bytes) return fail(TCCG_ERR_INVALID, "null argument");
+  *bytes = p->ws_bytes;
+  return TCCG_OK;
+}
+
+extern "C" int tccg_plan_describe(const tccg_plan* p, char* buf, size_t len) {
+  if (!p || !buf || len == 0) return fail(TCCG_ERR_INVALID, "null argument");
+  snprintf(buf, len, "%s ws=%zu", p->describe, p->ws_bytes);
+  return TCCG_OK;
+}
+
+extern "C" double tccg_plan_flops(const tccg_plan* p, double beta) {
+  if (!p) return 0.0;
+  double f = 2.0 * (double)p->M * (double)p->N * (double)p->K;
+  if (beta != 0.0) f += 3.0 * (double)p->M * (double)p->N;
+  return f;
+}
+
+extern "C" int tccg_plan_destroy(tccg_plan* p) {
+  plan_free(p);
+  return TCCG_OK;
+}
+
+extern "C" int tccg_plan_status(const tccg_plan* p, int32_t* device_status) {
+  if (!p || !device_status) return fail(TCCG_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(device_status, p->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int32_t)));
+  return TCCG_OK;
+}
+
+// --------------------------------------------------------------------------
+// kernel attributes (once per process)
+// --------------------------------------------------------------------------
+static std::once_flag g_attr_once;
+static cudaError_t g_attr_err = cudaSuccess;
+
+static void set_attrs() {
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess && x != cudaSuccess) e = x; };
+  chk(cudaFuncSetAttribute(simt_gett_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)simt_smem_bytes<float>()));
+  chk(cudaFuncSetAttribute(simt_gett_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TcCfg::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TcCfg::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(simt_gett_group_kernel<float>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<float>()));
+  chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg::SMEM_BYTES));
+  g_attr_err = e;
+}
+
+static int ensure_attrs() {
+  std::call_once(g_attr_once, set_attrs);
+  if (g_attr_err != cudaSuccess)
+    return fail(TCCG_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(g_attr_err));
+  return TCCG_OK;
+}
+
+// --------------------------------------------------------------------------
+// tensor maps
+// --------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static std::once_flag g_encode_once;
+
+static int get_encode() {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!g_encode) return fail(TCCG_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  return TCCG_OK;
+}
+
+// 2-D bf16 K-major operand [rows][cols], box {64, box_rows}, 128-byte swizzle.
+static int encode_kmajor(CUtensorMap* tm, const void* base, int64_t rows, int64_t cols,
+                         int box_rows) {
+  int rc = get_encode();
+  if (rc) return rc;
+  if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (cols * 2) % 16 != 0)
+    return fail(TCCG_ERR_ALIGNMENT, "TMA operand not 16-byte aligned");
+  cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t gstride[1] = {(cuuint64_t)(cols * 2)};
+  cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), gdim,
+                        gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(TCCG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return TCCG_OK;
+}
+
+// --------------------------------------------------------------------------
+// launches
+// --------------------------------------------------------------------------
+static int launch_check(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(TCCG_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  return TCCG_OK;
+}
+
+static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* coff, int64_t R,
+                           int64_t Kk, int64_t Rcover, int64_t Kcover, void* dst, int64_t ld,
+                           int32_t kfast) {
+  PackOperand o;
+  o.src = src;
+  o.row_off = roff;
+  o.col_off = coff;
+  o.R = R;
+  o.Kk = Kk;
+  o.Rcover = Rcover;
+  o.Kcover = Kcover;
+  o.dst = dst;
+  o.ld = ld;
+  o.read_k_fast = kfast;
+  o.active = 1;
+  return o;
+}
+
+template <typename Tin, typename Tout, int LAYOUT>
+static int launch_pack(const PackArgs& pa, cudaStream_t s) {
+  int64_t kx = std::max(pa.op[0].Kcover, pa.op[1].Kcover);
+  int64_t ry = std::max(pa.op[0].Rcover, pa.op[1].Rcover);
+  dim3 grid((unsigned)cdiv(kx, 32), (unsigned)cdiv(ry, 32), 2);
+  if (grid.y > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "operand has too many rows (%lld)", (long long)ry);
+  pack_kernel<Tin, Tout, LAYOUT><<<grid, dim3(32, 8), 0, s>>>(pa);
+  return launch_check("pack");
+}
+
+template <typename T>
+static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
+                    const int64_t* c_m, const int64_t* c_n, T alpha, T beta, char* ws,
+                    cudaStream_t s) {
+  using Cfg = SimtCfg<T>;
+  T* Ap = reinterpret_cast<T*>(ws + p->off_a);
+  T* Bp = reinterpret_cast<T*>(ws + p->off_b);
+  PackArgs pa;
+  pa.op[0] = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, Ap, p->Mp, p->read_k_fast_a);
+  pa.op[1] = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, Bp, p->Np, p->read_k_fast_b);
+  int rc = launch_pack<T, T, PACK_MN>(pa, s);
+  if (rc) return rc;
+  SimtArgs<T> a;
+  a.Ap = Ap;
+  a.Bp = Bp;
+  a.Mp = p->Mp;
+  a.Np = p->Np;
+  a.M = p->M;
+  a.N = p->N;
+  a.ktiles = p->ktiles;
+  a.ktiles_per_split = p->ktiles_per_split;
+  a.C = Cout;
+  a.c_m_off = c_m;
+  a.c_n_off = c_n;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(ws + p->off_part) : nullptr;
+  dim3 grid((unsigned)(p->Mp / Cfg::BM), (unsigned)(p->Np / Cfg::BN), (unsigned)p->ksplit);
+  if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
+  simt_gett_kernel<T><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+  rc = launch_check("simt_gett");
+  if (rc) return rc;
+  if (p->ksplit > 1) {
+    dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
+    simt_reduce_kernel<T><<<g2, 256, 0, s>>>(a.partial, p->ksplit, p->Mp, p->Np, p->M, p->N,
+                                             Cout, c_m, c_n, alpha, beta);
+    rc = launch_check("simt_reduce");
+  }
+  return rc;
+}
+
+static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cout,
+                  const int64_t* c_m, const int64_t* c_n, float alpha, float beta, char* ws,
+                  cudaStream_t s) {
+  const bool x3 = p->prec == TCCG_PREC_BF16X3;
+  void* Ap = ws + p->off_a;
+  void* Bp = ws + p->off_b;
+  PackArgs pa;
+  const int64_t kcover = x3 ? round_up(p->K, 32) : p->Kc;
+  pa.op[0] = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap, p->Kc, p->read_k_fast_a);
+  pa.op[1] = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp, p->Kc, p->read_k_fast_b);
+  int rc;
+  if (x3)
+    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s);
+  else if (p->dtype == TCCG_BF16)
+    rc = launch_pack<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16>(pa, s);
+  else
+    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s);
+  if (rc) return rc;
+  CUtensorMap tmA, tmB;
+  rc = encode_kmajor(&tmA, Ap, p->M, p->Kc, TcCfg::BM);
+  if (rc) return rc;
+  rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, TcCfg::BN);
+  if (rc) return rc;
+  TcArgs a;
+  a.M = (int32_t)p->M;
+  a.N = (int32_t)p->N;
+  a.K = (int32_t)p->K;
+  a.num_kb = p->num_kb;
+  a.tiles_m = p->tiles_m;
+  a.tiles_n = p->tiles_n;
+  a.raster = p->raster;
+  a.pad0 = 0;
+  a.C = Cout;
+  a.c_m_off = c_m;
+  a.c_n_off = c_n;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.status = p->d_status;
+  if (x3)
+    gett_tc_kernel<TC_BF16X3><<<p->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tmA, tmB, a);
+  else
+    gett_tc_kernel<TC_BF16><<<p->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tmA, tmB, a);
+  return launch_check("gett_tc");
+}
+
+static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s);
+
+extern "C" int tccg_plan_run(const tccg_plan* p, const void* A, const void* B, void* C,
+                             double alpha, double beta, void* ws, size_t ws_bytes, void* stream) {
+  if (!p) return fail(TCCG_ERR_INVALID, "null plan");
+  if (!A || !B || !C) return fail(TCCG_ERR_INVALID, "null operand pointer");
+  if (ws_bytes < p->ws_bytes || (p->ws_bytes > 0 && !ws))
+    return fail(TCCG_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", p->ws_bytes, ws_bytes);
+  if ((reinterpret_cast<uintptr_t>(ws) & 255u) != 0)
+    return fail(TCCG_ERR_ALIGNMENT, "workspace must be 256-byte aligned");
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != p->device)
+    return fail(TCCG_ERR_INVALID, "plan was created on device %d, current device is %d", p->device, dev);
+  int rc = ensure_attrs();
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const void* GA = p->d.swap_ab ? B : A;
+  const void* GB = p->d.swap_ab ? A : B;
+  char* w = static_cast<char*>(ws);
+  const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
+  // TTGT: the GEMM writes the contiguous [M][N] matrix C' (or C itself when C
+  // already has that layout), then one transposition applies alpha/beta.
+  const bool direct = !ttgt || p->c_is_mn_dense;
+  const int64_t* cm = direct && !ttgt ? p->t_c_m : p->t_id_m;
+  const int64_t* cn = direct && !ttgt ? p->t_c_n : p->t_id_n;
+  void* Cdst = direct ? C : (void*)(w + p->off_cprime);
+  const double ga = direct ? alpha : 1.0, gb = direct ? beta : 0.0;
+  if (p->prec == TCCG_PREC_FP64)
+    rc = run_simt<double>(p, GA, GB, static_cast<double*>(Cdst), cm, cn, ga, gb, w, s);
+  else if (p->prec == TCCG_PREC_FP32)
+    rc = run_simt<float>(p, GA, GB, static_cast<float*>(Cdst), cm, cn, (float)ga, (float)gb, w, s);
+  else
+    rc = run_tc(p, GA, GB, static_cast<float*>(Cdst), cm, cn, (float)ga, (float)gb, w, s);
+  if (rc || direct) return rc;
+  // C'[m + M n] -> C[c_m_stride . m_idx + c_n_stride . n_idx]
+  PermArgs pa{};
+  pa.A = Cdst;
+  pa.B = C;
+  pa.alpha = alpha;
+  pa.beta = beta;
+  int dim = 0;
+  int64_t s_cp = 1;
+  for (int i = 0; i < p->d.nm; ++i, ++dim) {
+    pa.ext[dim] = p->d.m_ext[i];
+    pa.sa[dim] = s_cp;
+    pa.sb[dim] = p->d.c_m_stride[i];
+    s_cp *= p->d.m_ext[i];
+  }
+  for (int i = 0; i < p->d.nn; ++i, ++dim) {
+    pa.ext[dim] = p->d.n_ext[i];
+    pa.sa[dim] = s_cp;
+    pa.sb[dim] = p->d.c_n_stride[i];
+    s_cp *= p->d.n_ext[i];
+  }
+  pa.dim = dim;
+  return permute_launch(p->prec == TCCG_PREC_FP64 ? TCCG_F64 : TCCG_F32, pa, s);
+}
+
+// --------------------------------------------------------------------------
+// transposition
+// --------------------------------------------------------------------------
+// Sorts the output dims so that dim 0 is B's stride-one dim, finds the dim of
+// A's stride one and launches permute_kernel.
+static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s) {
+  PermArgs pa = pa0;
+  if (pa.dim < 1 || pa.dim > PERM_MAX_DIMS) return fail(TCCG_ERR_INVALID, "bad dimension count");
+  // put the output dim with the smallest B stride first
+  int b0 = 0;
+  for (int d = 1; d < pa.dim; ++d)
+    if (pa.sb[d] < pa.sb[b0]) b0 = d;
+  std::swap(pa.ext[0], pa.ext[b0]);
+  std::swap(pa.sa[0], pa.sa[b0]);
+  std::swap(pa.sb[0], pa.sb[b0]);
+  int da = 0;
+  for (int d = 1; d < pa.dim; ++d)
+    if (pa.sa[d] < pa.sa[da]) da = d;
+  if (pa.sa[da] == pa.sa[0]) da = 0;
+  pa.da = da;
+  int64_t rest = 1;
+  for (int d = 1; d < pa.dim; ++d)
+    if (d != da) rest *= pa.ext[d];
+  pa.rest = rest;
+  dim3 grid;
+  if (da == 0) {
+    pa.nt0 = cdiv(pa.ext[0], 256);
+    pa.nta = 1;
+    grid.x = (unsigned)pa.nt0;
+  } else {
+    pa.nt0 = cdiv(pa.ext[0], 32);
+    pa.nta = cdiv(pa.ext[da], 32);
+    if (pa.nt0 * pa.nta > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "transpose too large");
+    grid.x = (unsigned)(pa.nt0 * pa.nta);
+  }
+  grid.y = (unsigned)std::min<int64_t>(rest, 65535);
+  grid.z = (unsigned)std::min<int64_t>(cdiv(rest, grid.y), 1024);
+  if (dtype == TCCG_F64)
+    permute_kernel<double><<<grid, dim3(32, 8), 0, s>>>(pa);
+  else if (dtype == TCCG_F32)
+    permute_kernel<float><<<grid, dim3(32, 8), 0, s>>>(pa);
+  else
+    return fail(TCCG_ERR_UNSUPPORTED, "transpose supports TCCG_F32 and TCCG_F64");
+  return launch_check("permute");
+}
+
+extern "C" int tccg_transpose(int32_t dtype, int32_t dim, const int32_t* perm,
+                              const int64_t* size, const int64_t* outer_a,
+                              const int64_t* outer_b, double alpha, const void* A, double beta,
+                              void* B, void* stream) {
+  if (dim < 1 || dim > PERM_MAX_DIMS || !perm || !size || !A || !B)
+    return fail(TCCG_ERR_INVALID, "bad transpose arguments");
+  bool seen[PERM_MAX_DIMS] = {false};
+  for (int j = 0; j < dim; ++j) {
+    if (perm[j] < 0 || perm[j] >= dim || seen[perm[j]]) return fail(TCCG_ERR_INVALID, "perm is not a permutation");
+    seen[perm[j]] = true;
+    if (size[j] < 1) return fail(TCCG_ERR_INVALID, "size[%d] = %lld", j, (long long)size[j]);
+  }
+  int64_t stA[PERM_MAX_DIMS], stB[PERM_MAX_DIMS];
+  int64_t s = 1;
+  for (int i = 0; i < dim; ++i) {  // A strides (input order)
+    stA[i] = s;
+    const int64_t o = outer_a ? outer_a[i] : size[i];
+    if (o < size[i]) return fail(TCCG_ERR_INVALID, "outer_a[%d] < size", i);
+    s *= o;
+  }
+  s = 1;
+  for (int j = 0; j < dim; ++j) {  // B strides (output order)
+    stB[j] = s;
+    const int64_t o = outer_b ? outer_b[j] : size[perm[j]];
+    if (o < size[perm[j]]) return fail(TCCG_ERR_INVALID, "outer_b[%d] < size", j);
+    s *= o;
+  }
+  PermArgs pa{};
+  pa.A = A;
+  pa.B = B;
+  pa.dim = dim;
+  pa.alpha = alpha;
+  pa.beta = beta;
+  for (int j = 0; j < dim; ++j) {
+    pa.ext[j] = size[perm[j]];
+    pa.sa[j] = stA[perm[j]];
+    pa.sb[j] = stB[j];
+  }
+  return permute_launch(dtype, pa, reinterpret_cast<cudaStream_t>(stream));
+}
+
+// --------------------------------------------------------------------------
+// grouped launches (implemented in grouped.cu)
+// --------------------------------------------------------------------------
+struct tccg_group {
+  std::vector<const tccg_plan*> plans;
+  int32_t prec = 0, dtype = 0;
+  int device = 0, num_sms = 148;
+  std::vector<size_t> ws_off;  // per item: start of its packed operands
+  size_t ws_bytes = 0;
+  void* d_items = nullptr;     // SimtGroupItem<T>[] or TcGroupItem[]
+  PackJob* d_jobs = nullptr;
+  int32_t n_jobs = 0;
+  int64_t pack_ctas = 0, total_tiles = 0;
+  int32_t grid = 0;
+  bool bound = false;
+};
+
+static void group_free(tccg_group* g) {
+  if (!g) return;
+  if (g->d_items) cudaFree(g->d_items);
+  if (g->d_jobs) cudaFree(g->d_jobs);
+  delete g;
+}
+
+extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, tccg_group** out) {
+  if (!plans || count < 1 || !out) return fail(TCCG_ERR_INVALID, "bad group arguments");
+  *out = nullptr;
+  tccg_group* g = new tccg_group();
+  g->prec = plans[0]->prec;
+  g->dtype = plans[0]->dtype;
+  g->device = plans[0]->device;
+  g->num_sms = plans[0]->num_sms;
+  size_t ws = 0;
+  int64_t tiles = 0;
+  for (int i = 0; i < count; ++i) {
+    const tccg_plan* p = plans[i];
+    if (!p) { group_free(g); return fail(TCCG_ERR_INVALID, "plan %d is null", i); }
+    if (p->prec != g->prec || p->dtype != g->dtype || p->device != g->device) {
+      group_free(g);
+      return fail(TCCG_ERR_UNSUPPORTED, "all plans of a group need the same precision, dtype and device");
+    }
+    if (p->tune.method != TCCG_METHOD_GETT || p->ksplit > 1) {
+      group_free(g);
+      return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without k-split (plan %d)", i);
+    }
+    g->plans.push_back(p);
+    g->ws_off.push_back(ws);
+    ws = align_up(ws + p->ws_bytes, 256);
+    if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) {
+      const int BM = p->prec == TCCG_PREC_FP64 ? SimtCfg<double>::BM : SimtCfg<float>::BM;
+      const int BN = p->prec == TCCG_PREC_FP64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+      tiles += (p->Mp / BM) * (p->Np / BN);
+    } else {
+      tiles += (int64_t)p->tiles_m * p->tiles_n;
+    }
+  }
+  if (tiles > INT32_MAX) { group_free(g); return fail(TCCG_ERR_UNSUPPORTED, "too many tiles"); }
+  g->ws_bytes = ws;
+  g->total_tiles = tiles;
+  g->n_jobs = 2 * count;
+  size_t item_bytes = (g->prec == TCCG_PREC_FP64)   ? sizeof(SimtGroupItem<double>)
+                      : (g->prec == TCCG_PREC_FP32) ? sizeof(SimtGroupItem<float>)
+                                                    : sizeof(TcGroupItem);
+  cudaError_t e = cudaMalloc(&g->d_items, item_bytes * count);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_jobs, sizeof(PackJob) * g->n_jobs);
+  if (e != cudaSuccess) {
+    group_free(g);
+    return fail(TCCG_ERR_CUDA, "group tables: %s", cudaGetErrorString(e));
+  }
+  *out = g;
+  return TCCG_OK;
+}
+
+extern "C" int tccg_group_workspace(const tccg_group* g, size_t* bytes) {
+  if (!g || !bytes) return fail(TCCG_ERR_INVALID, "null argument");
+  *bytes = g->ws_bytes;
+  return TCCG_OK;
+}
+
+template <typename T>
+static SimtArgs<T> simt_args_for(const tccg_plan* p, char* w, void* C, double alpha, double beta) {
+  SimtArgs<T> a;
+  a.Ap = reinterpret_cast<T*>(w + p->off_a);
+  a.Bp = reinterpret_cast<T*>(w + p->off_b);
+  a.Mp = p->Mp;
+  a.Np = p->Np;
+  a.M = p->M;
+  a.N = p->N;
+  a.ktiles = p->ktiles;
+  a.ktiles_per_split = p->ktiles;
+  a.C = static_cast<T*>(C);
+  a.c_m_off = p->t_c_m;
+  a.c_n_off = p->t_c_n;
+  a.alpha = (T)alpha;
+  a.beta = (T)beta;
+  a.partial = nullptr;
+  return a;
+}
+
+extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* const* B,
+                               void* const* C, const double* alpha, const double* beta, void* ws,
+                               size_t ws_bytes) {
+  if (!g || !A || !B || !C || !alpha || !beta) return fail(TCCG_ERR_INVALID, "null argument");
+  if (ws_bytes < g->ws_bytes || (g->ws_bytes && !ws))
+    return fail(TCCG_ERR_WORKSPACE, "group workspace of %zu bytes needed, %zu given", g->ws_bytes, ws_bytes);
+  if ((reinterpret_cast<uintptr_t>(ws) & 255u) != 0) return fail(TCCG_ERR_ALIGNMENT, "workspace must be 256-byte aligned");
+  const int n = (int)g->plans.size();
+  std::vector<PackJob> jobs(2 * n);
+  int64_t pack_ctas = 0;
+  const bool simt = g->prec == TCCG_PREC_FP32 || g->prec == TCCG_PREC_FP64;
+  std::vector<SimtGroupItem<float>> sf;
+  std::vector<SimtGroupItem<double>> sd;
+  std::vector<TcGroupItem> tc;
+  int64_t tile = 0;
+  for (int i = 0; i < n; ++i) {
+    const tccg_plan* p = g->plans[i];
+    if (!A[i] || !B[i] || !C[i]) return fail(TCCG_ERR_INVALID, "null operand pointer for item %d", i);
+    char* w = static_cast<char*>(ws) + g->ws_off[i];
+    const void* GA = p->d.swap_ab ? B[i] : A[i];
+    const void* GB = p->d.swap_ab ? A[i] : B[i];
+    PackOperand oa, ob;
+    if (simt) {
+      oa = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, w + p->off_a, p->Mp, p->read_k_fast_a);
+      ob = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, w + p->off_b, p->Np, p->read_k_fast_b);
+    } else {
+      const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
+      oa = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, w + p->off_a, p->Kc, p->read_k_fast_a);
+      ob = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b, p->Kc, p->read_k_fast_b);
+    }
+    PackOperand ops[2] = {oa, ob};
+    for (int j = 0; j < 2; ++j) {
+      PackJob& jb = jobs[2 * i + j];
+      jb.op = ops[j];
+      jb.begin = pack_ctas;
+      jb.ktiles = cdiv(ops[j].Kcover, 32);
+      pack_ctas += jb.ktiles * cdiv(ops[j].Rcover, 32);
+    }
+    if (g->prec == TCCG_PREC_FP32) {
+      SimtGroupItem<float> it;
+      it.args = simt_args_for<float>(p, w, C[i], alpha[i], beta[i]);
+      it.tile_begin = tile;
+      it.tiles_m = (int32_t)(p->Mp / SimtCfg<float>::BM);
+      it.pad = 0;
+      tile += (int64_t)it.tiles_m * (p->Np / SimtCfg<float>::BN);
+      sf.push_back(it);
+    } else if (g->prec == TCCG_PREC_FP64) {
+      SimtGroupItem<double> it;
+      it.args = simt_args_for<double>(p, w, C[i], alpha[i], beta[i]);
+      it.tile_begin = tile;
+      it.tiles_m = (int32_t)(p->Mp / SimtCfg<double>::BM);
+      it.pad = 0;
+      tile += (int64_t)it.tiles_m * (p->Np / SimtCfg<double>::BN);
+      sd.push_back(it);
+    } else {
+      TcGroupItem it;
+      memset(&it, 0, sizeof(it));
+      int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, TcCfg::BM);
+      if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, TcCfg::BN);
+      if (rc) return rc;
+      TcArgs& a = it.args;
+      a.M = (int32_t)p->M;
+      a.N = (int32_t)p->N;
+      a.K = (int32_t)p->K;
+      a.num_kb = p->num_kb;
+      a.tiles_m = p->tiles_m;
+      a.tiles_n = p->tiles_n;
+      a.raster = p->raster;
+      a.pad0 = 0;
+      a.C = static_cast<float*>(C[i]);
+      a.c_m_off = p->t_c_m;
+      a.c_n_off = p->t_c_n;
+      a.alpha = (float)alpha[i];
+      a.beta = (float)beta[i];
+      a.status = p->d_status;
+      it.tile_begin = tile;
+      tile += (int64_t)p->tiles_m * p->tiles_n;
+      tc.push_back(it);
+    }
+  }
+  if (pack_ctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
+  CUDA_TRY(cudaMemcpy(g->d_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
+  if (g->prec == TCCG_PREC_FP32)
+    CUDA_TRY(cudaMemcpy(g->d_items, sf.data(), sizeof(sf[0]) * sf.size(), cudaMemcpyHostToDevice));
+  else if (g->prec == TCCG_PREC_FP64)
+    CUDA_TRY(cudaMemcpy(g->d_items, sd.data(), sizeof(sd[0]) * sd.size(), cudaMemcpyHostToDevice));
+  else
+    CUDA_TRY(cudaMemcpy(g->d_items, tc.data(), sizeof(tc[0]) * tc.size(), cudaMemcpyHostToDevice));
+  g->pack_ctas = pack_ctas;
+  g->grid = simt ? (int32_t)g->total_tiles : (int32_t)std::min<int64_t>(g->total_tiles, g->num_sms);
+  g->bound = true;
+  return TCCG_OK;
+}
+
+extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
+  if (!g) return fail(TCCG_ERR_INVALID, "null group");
+  if (!g->bound) return fail(TCCG_ERR_INVALID, "tccg_group_bind must be called before tccg_group_run");
+  int rc = ensure_attrs();
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const dim3 pgrid((unsigned)g->pack_ctas);
+  const int nj = g->n_jobs;
+  switch (g->prec) {
+    case TCCG_PREC_FP32:
+      pack_group_kernel<float, float, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      if ((rc = launch_check("pack_group"))) return rc;
+      simt_gett_group_kernel<float><<<g->grid, 256, simt_smem_bytes<float>(), s>>>(
+          static_cast<const SimtGroupItem<float>*>(g->d_items), (int)g->plans.size());
+      return launch_check("simt_gett_group");
+    case TCCG_PREC_FP64:
+      pack_group_kernel<double, double, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      if ((rc = launch_check("pack_group"))) return rc;
+      simt_gett_group_kernel<double><<<g->grid, 256, simt_smem_bytes<double>(), s>>>(
+          static_cast<const SimtGroupItem<double>*>(g->d_items), (int)g->plans.size());
+      return launch_check("simt_gett_group");
+    default: {
+      const bool x3 = g->prec == TCCG_PREC_BF16X3;
+      if (x3)
+        pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      else if (g->dtype == TCCG_BF16)
+        pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      else
+        pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      if ((rc = launch_check("pack_group"))) return rc;
+      TcGroup tg;
+      tg.items = static_cast<const TcGroupItem*>(g->d_items);
+      tg.n_items = (int32_t)g->plans.size();
+      tg.total_tiles = (int32_t)g->total_tiles;
+      int32_t* st = g->plans[0]->d_status;
+      if (x3)
+        gett_tc_group_kernel<TC_BF16X3><<<g->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tg, st);
+      else
+        gett_tc_group_kernel<TC_BF16><<<g->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tg, st);
+      return launch_check("gett_tc_group");
+    }
+  }
+}
+
+extern "C" int tccg_group_destroy(tccg_group* g) {
+  group_free(g);
+  return TCCG_OK;
+}
