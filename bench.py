@@ -1,0 +1,467 @@
+#!/usr/bin/env python
+"""Benchmark of the GETT hot path on B200 (one JSON line on stdout).
+
+Workload (the compute-bound 6-index contraction the headline metric is
+quoted on): C[a,b,c,i,j,k] = A[a,m,b,n,c] * B[m,i,n,j,k], a=b=c=i=j=k=32,
+m=n=64 (M = N = 32768, K = 4096), A and B ~ N(0,1) FP32 from a seed, beta=0.
+
+A step is one GETT call: operand packing + the contraction kernel, inputs
+resident in HBM (A, B 512 MiB each, C 4 GiB: larger than the 126 MB L2, so
+no flush is needed between steps). ``value`` is split-BF16x3 TFLOP/s by
+TCCG's flop count (2MNK); plain FP32 GETT on the same inputs is reported
+beside it, and so are the errors of both against the FP64 path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank computes its own C slab of
+a k-sharded problem (weak scaling, no collective); time = max over ranks.
+``--impl reference`` times the reference's CPU implementation of the path
+(the loop nest TCCG emits, compiled from its generator when that build is
+present, else the oracle's C restatement of it) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+def workload(k_extent: int = 32):
+    """The .tccg text of the workload; k_extent < 32 gives the C slab k < k_extent
+    (used for profiler captures of the same kernel on a smaller case)."""
+    return ("C[a,b,c,i,j,k] = A[a,m,b,n,c] * B[m,i,n,j,k]\n"
+            "a = 32\nb = 32\nc = 32\ni = 32\nj = 32\nk = %d\nm = 64\nn = 64\n" % k_extent)
+
+
+def workload_name(k_extent: int = 32) -> str:
+    return ("C[a,b,c,i,j,k] = A[a,m,b,n,c] * B[m,i,n,j,k], a=b=c=i=j=32, k=%d, m=n=64 "
+            "(M=32768, N=%d, K=4096), N(0,1) FP32 inputs, alpha=1, beta=0"
+            % (k_extent, 1024 * k_extent))
+METRIC = "GETT TFLOP/s & %roofline: BF16x3 vs plain FP32 on 1xB200 at rel err <=1e-5"
+FP32_SIMT_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FFMA peak at max clock
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """Samples SM clock, power and clock-event reasons every 20 ms through NVML
+    (falls back to ``nvidia-smi -lms 100``) while the timed region runs."""
+
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown"}
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+
+    def _poll(self):
+        nv = self._nvml
+        h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, mx, pw, rs))
+            except Exception:  # noqa: BLE001
+                pass
+            self._stop.wait(0.02)
+
+    def start(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self._nvml = nv
+            # NVML numbers devices like nvidia-smi; map the torch index through
+            # CUDA_VISIBLE_DEVICES when it is set
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            if vis:
+                ids = [x for x in vis.split(",") if x.strip()]
+                if self.gpu < len(ids) and ids[self.gpu].strip().isdigit():
+                    self.gpu = int(ids[self.gpu])
+            self._thread = threading.Thread(target=self._poll, daemon=True)
+            self._thread.start()
+        except Exception:  # noqa: BLE001
+            self._nvml = None
+        time.sleep(0.05)
+
+    def stop(self):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": "nvml" if self._nvml else "unavailable"}
+        sm = [x[0] for x in self.samples]
+        reasons = sorted({name for x in self.samples for bit, name in self.REASONS.items()
+                          if x[3] & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm),
+                "sm_max_mhz": self.samples[0][1], "power_w_max": max(x[2] for x in self.samples),
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml, 20 ms"}
+
+
+# --------------------------------------------------------------------------
+# helpers
+# --------------------------------------------------------------------------
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def read_traffic(name: str):
+    """DRAM bytes per launch of the named kernel from its committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def cpu_loopnest_sample(con, A_np, B_np, seconds=10.0, threads=0, gpu_C=None):
+    """Time the oracle loop nest (TCCG's referenceVersion restated) on the first
+    S column-major entries of C, S sized for about `seconds`; optionally check
+    the GPU result on those entries against the FP64 oracle."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from oracle import LoopNest, error_metrics, lib  # noqa: E402
+    threads = threads or os.cpu_count() or 1
+    c, a, b = con.C0.labels, con.A0.labels, con.B0.labels
+    sizes = {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices}
+    ln = LoopNest(c, a, b, sizes)
+    Cbuf = np.zeros(ln.size_c, dtype=np.float32)
+    s, t = 8192, 0.0
+    while True:  # grow the calibration sample until it runs for >= 0.5 s
+        t0 = time.perf_counter()
+        ln.run(A_np, B_np, Cbuf, 1.0, 0.0, 0, s, threads)
+        t = max(time.perf_counter() - t0, 1e-6)
+        if t >= 0.5 or s >= ln.size_c:
+            break
+        s = min(ln.size_c, s * 4)
+    S = int(min(ln.size_c, max(s, s * seconds / t)))
+    t0 = time.perf_counter()
+    ln.run(A_np, B_np, Cbuf, 1.0, 0.0, 0, S, threads)
+    t = time.perf_counter() - t0
+    flops = 2.0 * S * ln.size_k
+    out = {"value": flops / t / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+           "sample": "first %d column-major entries of C (%.2e of the %d) through the oracle's C "
+                     "restatement of TCCG's loop-nest reference, %d OpenMP threads, %.1f s"
+                     % (S, S / ln.size_c, ln.size_c, threads, t)}
+    if gpu_C is not None:
+        lins = np.arange(0, S, max(1, S // 4096), dtype=np.int64)
+        ref = ln.sample64(A_np, B_np, None, 1.0, 0.0, lins, threads)
+        m = error_metrics(gpu_C[lins], ref)
+        out["check_vs_fp64_oracle"] = {"entries": int(len(lins)), "normwise": m["normwise"],
+                                       "max_abs_over_max_ref": m["max_abs_over_max_ref"]}
+    return out
+
+
+def reference_impl_sample(con, A_np, B_np, seconds, threads):
+    """The reference's own CPU code for this workload: the loop nest TCCG emits
+    (tccg.py:686-723) for the C slab C[:,:,:,:,0,0], compiled from the
+    generator's output into oracle/_ref/ (built in the build container).
+    Returns None when that build is absent."""
+    import ctypes
+    import numpy as np
+    so = os.path.join(ROOT, "oracle", "_ref", "cfg3_slab_reference.so")
+    if not os.path.exists(so):
+        return None
+    L = ctypes.CDLL(so)
+    L.referenceVersion.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_float, ctypes.c_float]
+    # slab: all of a,b,c,i for j=k=0 -> 2^20 entries of K=4096 each
+    Cs = np.zeros(32 ** 4, dtype=np.float32)
+    t0 = time.perf_counter()
+    L.referenceVersion(A_np.ctypes.data, B_np.ctypes.data, Cs.ctypes.data, 1.0, 0.0)
+    t = time.perf_counter() - t0
+    flops = 2.0 * Cs.size * 4096
+    return {"value": flops / t / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+            "sample": "slab C[:,:,:,:,0,0] (2^20 entries, 1/1024 of C) computed by the loop nest "
+                      "TCCG's generator emits for this contraction, g++ -O3 -fopenmp, %d threads, "
+                      "%.2f s" % (threads, t)}
+
+
+# --------------------------------------------------------------------------
+# arms
+# --------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    """CPU reference arm: rank 0 only."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    from tccg_b200 import parse_text
+    con = parse_text(workload(args.k_extent))
+    threads = os.cpu_count() or 1
+    g = torch.Generator().manual_seed(0)
+    A = torch.randn(con.A0.num_elements(), generator=g).numpy()
+    B = torch.randn(con.B0.num_elements(), generator=g).numpy()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    vals = []
+    info = None
+    per_step = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
+    for it in range(args.warmup + args.steps):
+        r = reference_impl_sample(con, A, B, per_step, threads)
+        if r is None:
+            r = cpu_loopnest_sample(con, A, B, seconds=per_step, threads=threads)
+        if it >= args.warmup:
+            vals.append(r["value"])
+            info = r
+    v = statistics.median(vals)
+    flops_step = con.flop_count()
+    line = {
+        "metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": flops_step / (v * 1e12) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": workload_name(args.k_extent), "precision": "fp32 (CPU loop nest)",
+                   "parallelism": "host cores of rank 0"},
+        "cpu_baseline": {"kind": info["kind"], "cores": info["cores"], "sample": info["sample"],
+                         "value": v, "unit": "TFLOP/s"},
+        "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from tccg_b200 import parse_text
+    from tccg_b200.api import Compiled
+    from tccg_b200.plan import Tuning
+
+    dev = torch.device("cuda", local)
+    con = parse_text(workload(args.k_extent))
+    flops = con.flop_count()
+    peaks, peak_src = measured_peaks()
+    g = torch.Generator(device=dev).manual_seed(1000 + rank)
+    nA, nB, nC = con.A0.num_elements(), con.B0.num_elements(), con.C0.num_elements()
+    A = torch.randn(nA, generator=g, device=dev, dtype=torch.float32)
+    B = torch.randn(nB, generator=g, device=dev, dtype=torch.float32)
+    C = torch.empty(nC, device=dev, dtype=torch.float32)
+
+    x3 = Compiled(con, "bf16x3", Tuning(raster=args.raster, max_ctas=args.max_ctas))
+    ws = x3.workspace(dev)
+
+    # ---- headline: split-BF16x3, device-resident -------------------------
+    for _ in range(args.warmup):
+        x3.plan.run(A, B, C, workspace=ws)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        x3.plan.run(A, B, C, workspace=ws)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_total = e0.elapsed_time(e1)
+    clocks = sampler.stop() if sampler else None
+    ms_step = max_over_ranks(ms_total / args.steps, world)
+    value = world * flops / (ms_step * 1e-3) / 1e12
+    status = x3.plan.status()
+
+    # per-kernel breakdown (same stream, CUDA events around each kernel)
+    kt = [x3.plan.run_timed(A, B, C, workspace=ws) for _ in range(max(2, min(args.steps, 5)))]
+    pack_ms = statistics.mean(k[0] for k in kt)
+    gemm_ms = statistics.mean(k[1] for k in kt)
+    achieved = flops / (gemm_ms * 1e-3) / 1e12
+    bf16_peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+    peak = bf16_peak / 3.0
+    traffic = read_traffic("gett_tc_bf16x3_cfg3.txt")
+
+    # ---- plain FP32 GETT on the same inputs --------------------------------
+    res = {}
+    if not args.skip_fp32:
+        f32 = Compiled(con, "fp32")
+        C32 = torch.empty_like(C)
+        f32.plan.run(A, B, C32, workspace=f32.workspace(dev))
+        torch.cuda.synchronize()
+        n32 = max(1, min(args.steps, 3))
+        e0.record()
+        for _ in range(n32):
+            f32.plan.run(A, B, C32, workspace=f32.workspace(dev))
+        e1.record()
+        torch.cuda.synchronize()
+        ms32 = max_over_ranks(e0.elapsed_time(e1) / n32, world)
+        k32 = f32.plan.run_timed(A, B, C32, workspace=f32.workspace(dev))
+        res["fp32"] = {"value": world * flops / (ms32 * 1e-3) / 1e12, "unit": "TFLOP/s",
+                       "ms_per_step": ms32,
+                       "kernel_frac_of_fp32_simt_peak": flops / (k32[1] * 1e-3) / 1e12 / FP32_SIMT_PEAK_TFLOPS}
+        f32._ws = None
+    else:
+        C32 = None
+
+    # ---- errors against the FP64 path --------------------------------------
+    if not args.skip_errors:
+        f64 = Compiled(con, "fp64")
+        C64 = torch.empty(nC, device=dev, dtype=torch.float64)
+        f64.plan.run(A.double(), B.double(), C64, workspace=f64.workspace(dev))
+        torch.cuda.synchronize()
+        nrm = torch.linalg.vector_norm(C64).item()
+        err = {"reference": "this library's FP64 path (DFMA), itself checked against the FP64 oracle in tests/",
+               "bf16x3_normwise": (torch.linalg.vector_norm(C.double() - C64).item() / nrm)}
+        err["bf16x3_max_abs_over_max_ref"] = ((C.double() - C64).abs().max().item()
+                                              / C64.abs().max().item())
+        if C32 is not None:
+            err["fp32_normwise"] = torch.linalg.vector_norm(C32.double() - C64).item() / nrm
+        res["errors"] = err
+        del C64, f64
+    del C32
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with host buffers -------------
+    if args.skip_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "TFLOP/s",
+                              "ms_per_step": ms_step, "roofline_kernel_ms": gemm_ms,
+                              "pack_ms": pack_ms, "partial": "--skip-e2e"}), flush=True)
+        return 0
+    Ah = A.cpu().pin_memory()
+    Bh = B.cpu().pin_memory()
+    Ch = torch.empty(nC, dtype=torch.float32).pin_memory()
+    for _ in range(min(args.warmup, 2)):
+        h2d, d2h = x3.run_host(Ah, Bh, Ch, device=dev)
+    torch.cuda.synchronize()
+    ne2e = max(1, min(args.steps, 5))
+    barrier(world)
+    e0.record()
+    for _ in range(ne2e):
+        h2d, d2h = x3.run_host(Ah, Bh, Ch, device=dev)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / ne2e, world)
+
+    # ---- CPU baseline (rank 0, single GPU only) ----------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        Cx3 = Ch.numpy()  # last e2e result = the BF16x3 output for these inputs
+        cpu = cpu_loopnest_sample(con, Ah.numpy(), Bh.numpy(), seconds=args.cpu_seconds,
+                                  gpu_C=Cx3)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3", "data": "synthetic",
+            "config": {"workload": workload_name(args.k_extent),
+                       "precision": "split-BF16x3 (bf16 products, f32 accumulate)",
+                       "M": con.sizeM, "N": con.sizeN, "K": con.sizeK, "flop_per_step": flops,
+                       "l2": "inputs larger than L2 (A, B 512 MiB, C 4 GiB); no flush",
+                       "parallelism": "weak: one C slab per GPU, no collective" if world > 1 else "1 GPU",
+                       "plan": x3.describe()},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "gett_tc_kernel<BF16X3>",
+                         "kernel_ms": gemm_ms, "pack_ms": pack_ms,
+                         "peak_note": "%s sustained dense BF16 %.1f TFLOP/s / 3 (three BF16 MMAs per "
+                                      "algorithmic multiply-add); frac = tensor-pipe share of measured "
+                                      "peak; of burst (%.1f/3): %.3f"
+                                      % (peak_src, bf16_peak, peaks.get("bf16_tflops", bf16_peak),
+                                         achieved / (peaks.get("bf16_tflops", bf16_peak) / 3.0))},
+            "e2e": {"value": world * flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": ms_e2e,
+                    "path": "Compiled.run_host: pinned host A, B -> device, tccg_plan_run, C -> pinned host"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+            "device_status": status,
+            "cpu_baseline": cpu,
+        }
+        line.update(res)
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--raster", type=int, default=0)
+    ap.add_argument("--max-ctas", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-fp32", action="store_true")
+    ap.add_argument("--skip-errors", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--k-extent", type=int, default=32,
+                    help="extent of C's last index (32 = the full workload)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, world, rank)
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -132,6 +132,16 @@ int tccg_plan_workspace(const tccg_plan* plan, size_t* bytes);
 int tccg_plan_run(const tccg_plan* plan, const void* A, const void* B, void* C, double alpha,
                   double beta, void* ws, size_t ws_bytes, void* stream);
 
+/*
+ * tccg_plan_run with CUDA-event timing of each kernel it launches, for
+ * benchmarks and the autotuner: kernel_ms[0] = operand packing,
+ * kernel_ms[1] = the GEMM kernel (SIMT or tcgen05), kernel_ms[2] = k-split
+ * reduction or TTGT output transposition (0 if none). Synchronises `stream`.
+ */
+int tccg_plan_run_timed(const tccg_plan* plan, const void* A, const void* B, void* C,
+                        double alpha, double beta, void* ws, size_t ws_bytes, void* stream,
+                        float* kernel_ms);
+
 /* Human-readable plan summary (method, kernels, tiles, workspace). */
 int tccg_plan_describe(const tccg_plan* plan, char* buf, size_t len);
 

@@ -30,7 +30,7 @@ METHODS = {"gett": METHOD_GETT, "ttgt": METHOD_TTGT, "log": METHOD_LOG}
 
 EXPORTED = [
     "tccg_version", "tccg_last_error", "tccg_plan_create", "tccg_plan_workspace",
-    "tccg_plan_run", "tccg_plan_describe", "tccg_plan_flops", "tccg_plan_destroy",
+    "tccg_plan_run", "tccg_plan_run_timed", "tccg_plan_describe", "tccg_plan_flops", "tccg_plan_destroy",
     "tccg_plan_status", "tccg_transpose", "tccg_group_create", "tccg_group_workspace",
     "tccg_group_bind", "tccg_group_run", "tccg_group_destroy",
 ]
@@ -76,6 +76,8 @@ def _declare(L):
                                    ctypes.POINTER(vp)]
     L.tccg_plan_workspace.argtypes = [vp, ctypes.POINTER(sz)]
     L.tccg_plan_run.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, sz, vp]
+    L.tccg_plan_run_timed.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, sz,
+                                      vp, ctypes.POINTER(ctypes.c_float)]
     L.tccg_plan_describe.argtypes = [vp, ctypes.c_char_p, sz]
     L.tccg_plan_flops.argtypes = [vp, ctypes.c_double]
     L.tccg_plan_flops.restype = ctypes.c_double

@@ -411,6 +411,14 @@ static int encode_kmajor(CUtensorMap* tm, const void* base, int64_t rows, int64_
 // --------------------------------------------------------------------------
 // launches
 // --------------------------------------------------------------------------
+// Optional per-kernel timing (tccg_plan_run_timed): events[2*i], events[2*i+1]
+// bracket kernel slot i (0 pack, 1 GEMM, 2 reduce/transpose) on the stream.
+static thread_local cudaEvent_t* g_events = nullptr;
+
+static void mark(int slot, int end, cudaStream_t s) {
+  if (g_events) cudaEventRecord(g_events[2 * slot + end], s);
+}
+
 static int launch_check(const char* what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TCCG_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
@@ -441,7 +449,9 @@ static int launch_pack(const PackArgs& pa, cudaStream_t s) {
   int64_t ry = std::max(pa.op[0].Rcover, pa.op[1].Rcover);
   dim3 grid((unsigned)cdiv(kx, 32), (unsigned)cdiv(ry, 32), 2);
   if (grid.y > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "operand has too many rows (%lld)", (long long)ry);
+  mark(0, 0, s);
   pack_kernel<Tin, Tout, LAYOUT><<<grid, dim3(32, 8), 0, s>>>(pa);
+  mark(0, 1, s);
   return launch_check("pack");
 }
 
@@ -474,13 +484,17 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(ws + p->off_part) : nullptr;
   dim3 grid((unsigned)(p->Mp / Cfg::BM), (unsigned)(p->Np / Cfg::BN), (unsigned)p->ksplit);
   if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
+  mark(1, 0, s);
   simt_gett_kernel<T><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+  mark(1, 1, s);
   rc = launch_check("simt_gett");
   if (rc) return rc;
   if (p->ksplit > 1) {
     dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
+    mark(2, 0, s);
     simt_reduce_kernel<T><<<g2, 256, 0, s>>>(a.partial, p->ksplit, p->Mp, p->Np, p->M, p->N,
                                              Cout, c_m, c_n, alpha, beta);
+    mark(2, 1, s);
     rc = launch_check("simt_reduce");
   }
   return rc;
@@ -524,10 +538,12 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.alpha = alpha;
   a.beta = beta;
   a.status = p->d_status;
+  mark(1, 0, s);
   if (x3)
     gett_tc_kernel<TC_BF16X3><<<p->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tmA, tmB, a);
   else
     gett_tc_kernel<TC_BF16><<<p->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tmA, tmB, a);
+  mark(1, 1, s);
   return launch_check("gett_tc");
 }
 
@@ -590,6 +606,30 @@ extern "C" int tccg_plan_run(const tccg_plan* p, const void* A, const void* B, v
   return permute_launch(p->prec == TCCG_PREC_FP64 ? TCCG_F64 : TCCG_F32, pa, s);
 }
 
+extern "C" int tccg_plan_run_timed(const tccg_plan* p, const void* A, const void* B, void* C,
+                                   double alpha, double beta, void* ws, size_t ws_bytes,
+                                   void* stream, float* kernel_ms) {
+  if (!kernel_ms) return fail(TCCG_ERR_INVALID, "null kernel_ms");
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; ++i) CUDA_TRY(cudaEventCreate(&ev[i]));
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // pre-record every event so that slots without a kernel read as 0 ms
+  for (int i = 0; i < 6; ++i) cudaEventRecord(ev[i], s);
+  g_events = ev;
+  int rc = tccg_plan_run(p, A, B, C, alpha, beta, ws, ws_bytes, stream);
+  g_events = nullptr;
+  cudaError_t e = cudaStreamSynchronize(s);
+  for (int i = 0; i < 3; ++i) {
+    float ms = 0.f;
+    if (!rc && e == cudaSuccess) cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+    kernel_ms[i] = ms;
+  }
+  for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(TCCG_ERR_CUDA, "stream sync: %s", cudaGetErrorString(e));
+  return TCCG_OK;
+}
+
 // --------------------------------------------------------------------------
 // transposition
 // --------------------------------------------------------------------------
@@ -627,12 +667,14 @@ static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s) {
   }
   grid.y = (unsigned)std::min<int64_t>(rest, 65535);
   grid.z = (unsigned)std::min<int64_t>(cdiv(rest, grid.y), 1024);
+  mark(2, 0, s);
   if (dtype == TCCG_F64)
     permute_kernel<double><<<grid, dim3(32, 8), 0, s>>>(pa);
   else if (dtype == TCCG_F32)
     permute_kernel<float><<<grid, dim3(32, 8), 0, s>>>(pa);
   else
     return fail(TCCG_ERR_UNSUPPORTED, "transpose supports TCCG_F32 and TCCG_F64");
+  mark(2, 1, s);
   return launch_check("permute");
 }
 

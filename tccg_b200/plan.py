@@ -217,6 +217,26 @@ class Plan:
         self.run_ptr(A.data_ptr(), B.data_ptr(), C.data_ptr(), alpha, beta, ws_ptr, ws_n,
                      stream.cuda_stream)
 
+    def run_timed(self, A, B, C, alpha: Optional[float] = None, beta: Optional[float] = None,
+                  workspace=None, stream=None) -> Tuple[float, float, float]:
+        """``run`` with CUDA-event timing of each kernel; returns milliseconds of
+        (packing, GEMM kernel, reduction/transposition). Synchronises."""
+        import torch
+        alpha = self.con.alpha if alpha is None else alpha
+        beta = self.con.beta if beta is None else beta
+        if workspace is None and self.workspace_bytes:
+            workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=C.device)
+        ws_ptr = workspace.data_ptr() if workspace is not None else 0
+        ws_n = workspace.numel() if workspace is not None else 0
+        if stream is None:
+            stream = torch.cuda.current_stream(C.device)
+        ms = (ctypes.c_float * 3)()
+        N.check(self._lib.tccg_plan_run_timed(
+            self._h, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(B.data_ptr()),
+            ctypes.c_void_p(C.data_ptr()), float(alpha), float(beta), ctypes.c_void_p(ws_ptr),
+            ctypes.c_size_t(ws_n), ctypes.c_void_p(stream.cuda_stream), ms))
+        return float(ms[0]), float(ms[1]), float(ms[2])
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
