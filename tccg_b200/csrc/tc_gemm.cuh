@@ -7,24 +7,27 @@
 // same TMA boxes (64 x 128 rows for GA, 64 x 256 rows for GB, 128-byte
 // swizzle) and only the MMA schedule differs:
 //   BF16  : 4 MMAs (k-steps of 16) per stage
-//   BF16X3: per k-step of 16, Dhh += ah*bh and Dc += ah*bl, Dc += al*bh
-// (al*bl, ~2^-16 relative, is dropped). The tensor cores add each MMA's
-// result into the FP32 accumulator with truncation, so the small correction
-// products get their own accumulator Dc: they are then truncated relative to
-// their own (2^-8 smaller) magnitude instead of the main sum's, and the main
-// sum Dhh takes one truncating add per k-step instead of three. The epilogue
-// adds Dhh + Dc with an IEEE (round-to-nearest) FP32 add. On N(0,1) data with
-// K = 4096 this brings the normwise error from ~1.5e-5 (one accumulator) to
-// ~5e-6.
+//   BF16X3: per k-step of 16, D += ah*bh, D += ah*bl, D += al*bh
+// (al*bl, ~2^-16 relative, is dropped).
 //
-// Structure: one persistent CTA per SM, 6 warps.
+// Accumulation in chunks of K: the tensor cores add each MMA's result into the
+// FP32 accumulator with truncation, so a long sum in one accumulator drifts
+// (normwise ~1.5e-5 at K = 4096 on N(0,1) data). The MMA warp therefore
+// accumulates each chunk of `chunk_kb` k-blocks (512 k by default in BF16X3
+// mode) into a fresh TMEM accumulator, and the epilogue adds the chunk sums in
+// registers with IEEE round-to-nearest FP32 adds (~5e-6 at K = 4096). The two
+// 256-column accumulators ping-pong between chunks (and tiles), so the MMAs of
+// one chunk overlap the epilogue's read of the previous one. BF16 mode uses
+// one chunk per tile.
+//
+// Structure: one persistent CTA per SM, 10 warps.
 //   warp 0     TMA producer (one lane): STAGES-deep smem ring, mbarrier full/empty
-//   warp 1     TMEM owner + MMA issuer (one lane): 128x256 UMMA tiles. BF16 mode
-//              double-buffers two 256-column FP32 accumulators across tiles;
-//              BF16X3 mode uses the 512 columns for one tile's Dhh and Dc.
-//   warps 2-5  epilogue: tcgen05.ld of their 32-lane TMEM quadrant, then
-//              C[c_m_off[m] + c_n_off[n]] = alpha*acc (+ beta*C), written straight
-//              into C's own layout (GETT: no transposition of C).
+//   warp 1     TMEM owner + MMA issuer (one lane): 128x256 UMMA tiles into one of
+//              two 256-column FP32 accumulators (double buffering)
+//   warps 2-9  epilogue: warp w reads TMEM lane quadrant w%4, columns
+//              [128*h, 128*h+128) with h = (w-2)/4, sums the chunks, then writes
+//              C[c_m_off[m] + c_n_off[n]] = alpha*acc (+ beta*C) straight into
+//              C's own layout (GETT: no transposition of C).
 // Every mbarrier wait is bounded (TCCG_DEVICE_WAIT_NS); a wait that runs out
 // records an error code in *status and the CTA winds down: in-flight TMA loads
 // and MMAs are waited for (bounded) and TMEM is released before returning.
@@ -34,26 +37,33 @@
 
 namespace tccg {
 
-struct TcCfg {
-  static constexpr int BM = 128, BN = 256;
+enum TcMode : int { TC_BF16 = 0, TC_BF16X3 = 1 };
+
+// Tile configuration per mode. BF16X3 uses 128x192 tiles so that each of the 8
+// epilogue warps keeps its 96-column running chunk sum in registers (a 10-warp
+// CTA has at most 168 registers per thread: 3 warps share one SM sub-partition).
+template <int MODE>
+struct TcCfgT {
+  static constexpr int BM = 128;
+  static constexpr int BN = (MODE == TC_BF16X3) ? 192 : 256;
   static constexpr int ROW_BYTES = 128;  // one swizzle row per operand row per stage
-  static constexpr int STAGES = 4;
+  static constexpr int STAGES = (MODE == TC_BF16X3) ? 5 : 4;
   static constexpr int A_STAGE = BM * ROW_BYTES;   // 16 KB
-  static constexpr int B_STAGE = BN * ROW_BYTES;   // 32 KB
+  static constexpr int B_STAGE = BN * ROW_BYTES;   // 24 / 32 KB
   static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-  static constexpr int TMEM_COLS = 2 * BN;         // two FP32 accumulators
-  static constexpr int NUM_THREADS = 192;
+  static constexpr int TMEM_COLS = 512;            // two accumulators of BN columns
+  static constexpr int ACC_STRIDE = 256;           // accumulator b starts at column 256*b
+  static constexpr int NUM_THREADS = 320;
+  static constexpr int EPI_WARPS = 8;
   static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
 };
-
-enum TcMode : int { TC_BF16 = 0, TC_BF16X3 = 1 };
 
 struct TcArgs {
   int32_t M, N, K;
   int32_t num_kb;           // 128-byte k-chunks per row: BF16 ceil(K/64), BF16X3 ceil(K/32)
   int32_t tiles_m, tiles_n;
   int32_t raster;           // tiles along m per raster group
-  int32_t pad0;
+  int32_t chunk_kb;         // k-blocks accumulated per TMEM accumulator (>= 1)
   float* C;
   const int64_t* c_m_off;
   const int64_t* c_n_off;
@@ -128,7 +138,7 @@ template <int MODE, bool GROUPED>
 __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUtensorMap* tmB,
                                              const TcArgs* a1, const TcGroup& g,
                                              int32_t* status) {
-  using Cfg = TcCfg;
+  using Cfg = TcCfgT<MODE>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_addr = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + (((raw_addr + 1023u) & ~1023u) - raw_addr);
@@ -152,7 +162,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 4);
+      mbar_init(&acce[b], Cfg::EPI_WARPS);
     }
     mbar_init(drain, 1);
     fence_mbar_init();
@@ -200,7 +210,6 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
     constexpr uint32_t idesc = idesc_bf16_f32(Cfg::BM, Cfg::BN);
-    constexpr int NBUF = (MODE == TC_BF16X3) ? 1 : 2;
     int stage = 0;
     uint32_t phase = 0;
     int acc = 0;
@@ -208,58 +217,60 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     bool ok = true, issued_any = false;
     for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
-      const int nkb = t.a->num_kb, K = t.a->K;
-      if (!mbar_wait(&acce[acc], acc_phase ^ 1)) {
-        record_error(status, 2);
-        ok = false;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t d_tmem = tbase + (uint32_t)(acc * Cfg::BN);
-      const uint32_t d_corr = tbase + (uint32_t)Cfg::BN;  // BF16X3: correction accumulator
-      uint32_t accumulate = 0;
-      for (int kb = 0; kb < nkb; ++kb) {
-        if (!mbar_wait(&full[stage], phase)) {
+      const int nkb = t.a->num_kb, K = t.a->K, ckb = t.a->chunk_kb;
+      for (int kb0 = 0; kb0 < nkb && ok; kb0 += ckb) {
+        if (!mbar_wait(&acce[acc], acc_phase ^ 1)) {
           record_error(status, 2);
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint64_t ad = umma_desc_k128(smem_u32(sA + stage * Cfg::A_STAGE));
-        const uint64_t bd = umma_desc_k128(smem_u32(sB + stage * Cfg::B_STAGE));
-        if constexpr (MODE == TC_BF16) {
+        const uint32_t d_tmem = tbase + (uint32_t)(acc * Cfg::ACC_STRIDE);
+        uint32_t accumulate = 0;
+        const int kend = (kb0 + ckb < nkb) ? kb0 + ckb : nkb;
+        for (int kb = kb0; kb < kend; ++kb) {
+          if (!mbar_wait(&full[stage], phase)) {
+            record_error(status, 2);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t ad = umma_desc_k128(smem_u32(sA + stage * Cfg::A_STAGE));
+          const uint64_t bd = umma_desc_k128(smem_u32(sB + stage * Cfg::B_STAGE));
+          if constexpr (MODE == TC_BF16) {
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks) {
-            if (kb * 64 + ks * 16 < K) {
-              tc_mma_f16(d_tmem, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);
-              accumulate = 1;
+            for (int ks = 0; ks < 4; ++ks) {
+              if (kb * 64 + ks * 16 < K) {
+                tc_mma_f16(d_tmem, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);
+                accumulate = 1;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+              if (kb * 32 + ks * 16 < K) {
+                // descriptor start address is in 16-byte units: +2 = 32 B (16 bf16),
+                // +4 = 64 B (the lo half of the 128-byte row)
+                tc_mma_f16(d_tmem, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);  // ah*bh
+                tc_mma_f16(d_tmem, ad + 2 * ks, bd + 4 + 2 * ks, idesc, 1);       // ah*bl
+                tc_mma_f16(d_tmem, ad + 4 + 2 * ks, bd + 2 * ks, idesc, 1);       // al*bh
+                accumulate = 1;
+              }
             }
           }
-        } else {
-#pragma unroll
-          for (int ks = 0; ks < 2; ++ks) {
-            if (kb * 32 + ks * 16 < K) {
-              // descriptor start address is in 16-byte units: +2 = 32 B (16 bf16),
-              // +4 = 64 B (the lo half of the 128-byte row)
-              tc_mma_f16(d_tmem, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);      // ah*bh
-              tc_mma_f16(d_corr, ad + 2 * ks, bd + 4 + 2 * ks, idesc, accumulate);  // ah*bl
-              tc_mma_f16(d_corr, ad + 4 + 2 * ks, bd + 2 * ks, idesc, 1);           // al*bh
-              accumulate = 1;
-            }
+          issued_any = true;
+          tc_commit(&empty[stage]);  // frees the smem stage when these MMAs finish
+          if (++stage == Cfg::STAGES) {
+            stage = 0;
+            phase ^= 1;
           }
         }
-        issued_any = true;
-        tc_commit(&empty[stage]);  // frees the smem stage when these MMAs finish
-        if (++stage == Cfg::STAGES) {
-          stage = 0;
-          phase ^= 1;
+        if (!ok) break;
+        tc_commit(&accf[acc]);  // chunk sum ready for the epilogue
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1;
         }
-      }
-      if (!ok) break;
-      tc_commit(&accf[acc]);  // accumulator ready for the epilogue
-      if (++acc == NBUF) {
-        acc = 0;
-        acc_phase ^= 1;
       }
     }
     if (!ok && issued_any) {  // wait for outstanding MMAs before TMEM is released
@@ -268,66 +279,112 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     }
   } else if (warp >= 2) {
     // ---------------- epilogue ----------------
-    const int q = warp & 3;  // TMEM lanes [32q, 32q+32) are accessible to this warp
-    constexpr int NBUF = (MODE == TC_BF16X3) ? 1 : 2;
+    const int q = warp & 3;             // TMEM lanes [32q, 32q+32) are accessible to this warp
+    const int h = (warp - 2) >> 2;      // column half of the tile
+    constexpr int HC = Cfg::BN / 2;     // columns per epilogue warp
     int acc = 0;
     uint32_t acc_phase = 0;
-    for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
       const TcArgs& a = *t.a;
-      const float alpha = a.alpha, beta = a.beta;
-      if (!mbar_wait(&accf[acc], acc_phase)) {
-        record_error(status, 3);
-        break;
-      }
-      tc_fence_after();
       const int64_t m = (int64_t)t.tm * Cfg::BM + q * 32 + lane;
       const bool m_ok = m < a.M;
       const int64_t cmo = m_ok ? a.c_m_off[m] : 0;
-      const int64_t nbase = (int64_t)t.tn * Cfg::BN;
-      const uint32_t trow = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * Cfg::BN);
+      const int64_t n0 = (int64_t)t.tn * Cfg::BN + h * HC;
+      const int64_t nlim = a.N - n0;
+      const float alpha = a.alpha, beta = a.beta;
+      if constexpr (MODE == TC_BF16) {
+        // one accumulator per tile: stream TMEM -> C
+        if (!mbar_wait(&accf[acc], acc_phase)) {
+          record_error(status, 3);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tsrc = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * Cfg::ACC_STRIDE + h * HC);
 #pragma unroll 1
-      for (int c = 0; c < Cfg::BN; c += 32) {
-        uint32_t r[32];
-        tmem_ld_32x32b_x32(trow + (uint32_t)c, r);
-        if constexpr (MODE == TC_BF16X3) {
-          uint32_t rc[32];
-          tmem_ld_32x32b_x32(trow + (uint32_t)(Cfg::BN + c), rc);
+        for (int cc = 0; cc < HC; cc += 32) {
+          uint32_t r[32];
+          tmem_ld_32x32b_x32(tsrc + (uint32_t)cc, r);
           tmem_ld_wait();
+          if (cc == HC - 32) {  // accumulator fully read: hand it back to the MMA warp
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[acc]);
+          }
+          if (m_ok) {
+            if (beta != 0.0f) {
+              float old[32];
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            r[j] = __float_as_uint(__fadd_rn(__uint_as_float(r[j]), __uint_as_float(rc[j])));
-        } else {
-          tmem_ld_wait();
-        }
-        if (c == Cfg::BN - 32) {  // accumulator fully read: hand it back to the MMA warp
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acce[acc]);
-        }
-        if (m_ok) {
-          const int64_t nlim = a.N - (nbase + c);
-          if (beta != 0.0f) {
-            float old[32];
+              for (int j = 0; j < 32; ++j)
+                old[j] = (cc + j < nlim) ? a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] : 0.0f;
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-              old[j] = (j < nlim) ? a.C[cmo + __ldg(a.c_n_off + nbase + c + j)] : 0.0f;
+              for (int j = 0; j < 32; ++j)
+                if (cc + j < nlim)
+                  a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] =
+                      fmaf(beta, old[j], alpha * __uint_as_float(r[j]));
+            } else {
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (j < nlim)
-                a.C[cmo + __ldg(a.c_n_off + nbase + c + j)] =
-                    fmaf(beta, old[j], alpha * __uint_as_float(r[j]));
-          } else {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (j < nlim)
-                a.C[cmo + __ldg(a.c_n_off + nbase + c + j)] = alpha * __uint_as_float(r[j]);
+              for (int j = 0; j < 32; ++j)
+                if (cc + j < nlim)
+                  a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] = alpha * __uint_as_float(r[j]);
+            }
           }
         }
-      }
-      if (++acc == NBUF) {
-        acc = 0;
-        acc_phase ^= 1;
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1;
+        }
+      } else {
+        // chunked accumulation: sum the chunk accumulators in registers (RN adds)
+        const int nchunks = (a.num_kb + a.chunk_kb - 1) / a.chunk_kb;
+        float sum[HC];
+        for (int ch = 0; ch < nchunks; ++ch) {
+          if (!mbar_wait(&accf[acc], acc_phase)) {
+            record_error(status, 3);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t tsrc = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * Cfg::ACC_STRIDE + h * HC);
+#pragma unroll
+          for (int cc = 0; cc < HC; cc += 16) {
+            uint32_t r[16];
+            tmem_ld_32x32b_x16(tsrc + (uint32_t)cc, r);
+            tmem_ld_wait();
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              sum[cc + j] = (ch == 0) ? __uint_as_float(r[j])
+                                      : __fadd_rn(sum[cc + j], __uint_as_float(r[j]));
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[acc]);  // accumulator free for the MMA warp
+          if (++acc == 2) {
+            acc = 0;
+            acc_phase ^= 1;
+          }
+        }
+        if (!ok) break;
+        if (m_ok) {
+          if (beta != 0.0f) {
+#pragma unroll
+            for (int cc = 0; cc < HC; cc += 8) {
+              float old[8];
+#pragma unroll
+              for (int j = 0; j < 8; ++j)
+                old[j] = (cc + j < nlim) ? a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] : 0.0f;
+#pragma unroll
+              for (int j = 0; j < 8; ++j)
+                if (cc + j < nlim)
+                  a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] = fmaf(beta, old[j], alpha * sum[cc + j]);
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < HC; ++j)
+              if (j < nlim) a.C[cmo + __ldg(a.c_n_off + n0 + j)] = alpha * sum[j];
+          }
+        }
       }
     }
   }
@@ -341,7 +398,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(TcCfg::NUM_THREADS, 1)
+__global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
     gett_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                    const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
   TcGroup g{nullptr, 0, 0};
@@ -349,7 +406,7 @@ __global__ void __launch_bounds__(TcCfg::NUM_THREADS, 1)
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(TcCfg::NUM_THREADS, 1)
+__global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
     gett_tc_group_kernel(const TcGroup g, int32_t* status) {
   gett_tc_body<MODE, true>(nullptr, nullptr, nullptr, g, status);
 }

@@ -72,7 +72,7 @@ struct tccg_plan {
   int32_t ktiles = 0, ksplit = 1, ktiles_per_split = 0;
   // tcgen05 geometry
   int64_t Kc = 0;
-  int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0;
+  int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0, chunk_kb = 1, bn = 256;
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
   char describe[512] = "";
@@ -265,8 +265,13 @@ static int plan_layout(tccg_plan* p) {
       p->Kc = round_up(p->K, 8);
       p->num_kb = (int32_t)cdiv(p->K, 64);
     }
-    p->tiles_m = (int32_t)cdiv(p->M, TcCfg::BM);
-    p->tiles_n = (int32_t)cdiv(p->N, TcCfg::BN);
+    // BF16X3 accumulates 512 k per TMEM accumulator (tuning.variant overrides,
+    // in k-blocks of 32); BF16 one chunk per tile
+    p->chunk_kb = x3 ? (p->tune.variant > 0 ? p->tune.variant : 16) : p->num_kb;
+    if (p->chunk_kb < 1) p->chunk_kb = 1;
+    p->bn = x3 ? TcCfgT<TC_BF16X3>::BN : TcCfgT<TC_BF16>::BN;
+    p->tiles_m = (int32_t)cdiv(p->M, 128);
+    p->tiles_n = (int32_t)cdiv(p->N, p->bn);
     p->raster = p->tune.raster > 0 ? p->tune.raster : 8;
     const int64_t tiles = (int64_t)p->tiles_m * p->tiles_n;
     if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
@@ -277,10 +282,10 @@ static int plan_layout(tccg_plan* p) {
     p->off_b = ws;
     ws = align_up(ws + (size_t)(p->N * p->Kc) * 2, 256);
     snprintf(p->describe, sizeof(p->describe),
-             "method=%s prec=%s kernel=gett_tc<%s> tile=128x256 stages=%d M=%lld N=%lld K=%lld "
-             "kblocks=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d)",
-             ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", x3 ? "BF16X3" : "BF16",
-             TcCfg::STAGES, (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->grid,
+             "method=%s prec=%s kernel=gett_tc<%s> tile=128x%d stages=%d M=%lld N=%lld K=%lld "
+             "kblocks=%d chunk=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d)",
+             ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", x3 ? "BF16X3" : "BF16", p->bn,
+             x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES, (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->grid,
              p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b);
   }
   if (ttgt) {
@@ -349,17 +354,18 @@ static void set_attrs() {
   chk(cudaFuncSetAttribute(simt_gett_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)simt_smem_bytes<double>()));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfg::SMEM_BYTES));
+                           (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfg::SMEM_BYTES));
+                           (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<float>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<float>()));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
   chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg::SMEM_BYTES));
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg::SMEM_BYTES));
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
   g_attr_err = e;
 }
 
@@ -519,9 +525,9 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
     rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s);
   if (rc) return rc;
   CUtensorMap tmA, tmB;
-  rc = encode_kmajor(&tmA, Ap, p->M, p->Kc, TcCfg::BM);
+  rc = encode_kmajor(&tmA, Ap, p->M, p->Kc, 128);
   if (rc) return rc;
-  rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, TcCfg::BN);
+  rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, p->bn);
   if (rc) return rc;
   TcArgs a;
   a.M = (int32_t)p->M;
@@ -531,7 +537,7 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.tiles_m = p->tiles_m;
   a.tiles_n = p->tiles_n;
   a.raster = p->raster;
-  a.pad0 = 0;
+  a.chunk_kb = p->chunk_kb;
   a.C = Cout;
   a.c_m_off = c_m;
   a.c_n_off = c_n;
@@ -540,9 +546,11 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.status = p->d_status;
   mark(1, 0, s);
   if (x3)
-    gett_tc_kernel<TC_BF16X3><<<p->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tmA, tmB, a);
+    gett_tc_kernel<TC_BF16X3><<<p->grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
+                                TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tmA, tmB, a);
   else
-    gett_tc_kernel<TC_BF16><<<p->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tmA, tmB, a);
+    gett_tc_kernel<TC_BF16><<<p->grid, TcCfgT<TC_BF16>::NUM_THREADS, TcCfgT<TC_BF16>::SMEM_BYTES,
+                              s>>>(tmA, tmB, a);
   mark(1, 1, s);
   return launch_check("gett_tc");
 }
@@ -875,8 +883,8 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     } else {
       TcGroupItem it;
       memset(&it, 0, sizeof(it));
-      int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, TcCfg::BM);
-      if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, TcCfg::BN);
+      int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, 128);
+      if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, p->bn);
       if (rc) return rc;
       TcArgs& a = it.args;
       a.M = (int32_t)p->M;
@@ -886,7 +894,7 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       a.tiles_m = p->tiles_m;
       a.tiles_n = p->tiles_n;
       a.raster = p->raster;
-      a.pad0 = 0;
+      a.chunk_kb = p->chunk_kb;
       a.C = static_cast<float*>(C[i]);
       a.c_m_off = p->t_c_m;
       a.c_n_off = p->t_c_n;
@@ -948,9 +956,11 @@ extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
       tg.total_tiles = (int32_t)g->total_tiles;
       int32_t* st = g->plans[0]->d_status;
       if (x3)
-        gett_tc_group_kernel<TC_BF16X3><<<g->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tg, st);
+        gett_tc_group_kernel<TC_BF16X3><<<g->grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
+                                          TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tg, st);
       else
-        gett_tc_group_kernel<TC_BF16><<<g->grid, TcCfg::NUM_THREADS, TcCfg::SMEM_BYTES, s>>>(tg, st);
+        gett_tc_group_kernel<TC_BF16><<<g->grid, TcCfgT<TC_BF16>::NUM_THREADS,
+                                        TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, st);
       return launch_check("gett_tc_group");
     }
   }

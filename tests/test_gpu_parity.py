@@ -129,3 +129,21 @@ def test_beta_zero_ignores_nan_in_c(cuda):
     for prec in ("fp32", "bf16x3"):
         out, _ = run_gpu(con, prec, A.astype(np.float32), B.astype(np.float32), Cn)
         assert np.isfinite(out).all(), prec
+
+
+@pytest.mark.parametrize("chunk_kb", [1, 3, 16, 1000])
+def test_bf16x3_k_chunks(cuda, chunk_kb):
+    """Chunked accumulation (TMEM accumulators ping-pong every chunk_kb
+    k-blocks of 32): odd K over many chunks, partial 128x192 tiles."""
+    from tccg_b200.plan import Tuning
+    sizes = dict(m=300, n=500, k=1000)
+    con = make_contraction("mn", "km", "kn", sizes)
+    ln = LoopNest("mn", "km", "kn", sizes)
+    A = seeded_normal(ln.size_a, 21).astype(np.float32)
+    B = seeded_normal(ln.size_b, 22).astype(np.float32)
+    C = np.zeros(ln.size_c, dtype=np.float32)
+    out, p = run_gpu(con, "bf16x3", A, B, C, tuning=Tuning(variant=chunk_kb))
+    assert "chunk=%d" % chunk_kb in p.describe()
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 1.0, 0.0)
+    m = error_metrics(out, ref)
+    assert m["normwise"] <= 1e-5, m
