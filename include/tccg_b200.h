@@ -161,6 +161,26 @@ int tccg_plan_destroy(tccg_plan* plan);
 int tccg_plan_status(const tccg_plan* plan, int32_t* device_status);
 
 /*
+ * Allocation-free split-BF16x3 GETT. This entry point has no counterpart in
+ * the reference. It is for callers that must not allocate device memory --
+ * a process whose HBM a framework's caching allocator has already reserved,
+ * or a latency-critical loop that cannot afford cudaMalloc/cudaFree (which may
+ * synchronise the device) -- and it allocates nothing: no plan, no workspace.
+ * Its scratch (offset tables, packed operands, status word) is a static
+ * 64 MiB device array that every GPU loading the library holds until the
+ * process exits; a contraction needing more is rejected with
+ * TCCG_ERR_WORKSPACE and a message (use tccg_plan_run then). The first call
+ * on each device looks up the array's device address with that device
+ * current; make that first call before any stream capture. All calls share
+ * the array (each clears what must start at zero), so calls whose kernels
+ * overlap on the GPU -- e.g. on two streams -- race; serialise them.
+ * A, B, C: device pointers, float, in the caller's (file) order as for
+ * tccg_plan_run; desc as for tccg_plan_create.
+ */
+int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, const float* B, float* C,
+                             double alpha, double beta, void* stream);
+
+/*
  * HPTT-style out-of-place transposition (the call TCCG emits at
  * tccg/transpose.py:140-141):  B[perm(i)] = alpha * A[i] + beta * B[perm(i)],
  * where dimension j of B is dimension perm[j] of A. size[] are A's extents,

@@ -32,7 +32,7 @@ EXPORTED = [
     "tccg_version", "tccg_last_error", "tccg_plan_create", "tccg_plan_workspace",
     "tccg_plan_run", "tccg_plan_run_timed", "tccg_plan_describe", "tccg_plan_flops", "tccg_plan_destroy",
     "tccg_plan_status", "tccg_transpose", "tccg_group_create", "tccg_group_workspace",
-    "tccg_group_bind", "tccg_group_run", "tccg_group_destroy",
+    "tccg_group_bind", "tccg_group_run", "tccg_group_destroy", "tccg_gett_bf16x3_noalloc",
 ]
 
 
@@ -92,6 +92,8 @@ def _declare(L):
                                   vp, sz]
     L.tccg_group_run.argtypes = [vp, vp]
     L.tccg_group_destroy.argtypes = [vp]
+    L.tccg_gett_bf16x3_noalloc.argtypes = [ctypes.POINTER(Desc), vp, vp, vp, ctypes.c_double,
+                                           ctypes.c_double, vp]
     for name in EXPORTED:
         if name not in ("tccg_version", "tccg_last_error", "tccg_plan_flops"):
             getattr(L, name).restype = ctypes.c_int

@@ -970,3 +970,159 @@ extern "C" int tccg_group_destroy(tccg_group* g) {
   group_free(g);
   return TCCG_OK;
 }
+
+// --------------------------------------------------------------------------
+// allocation-free split-BF16x3 GETT
+// --------------------------------------------------------------------------
+// For callers that must not allocate device memory: a process whose HBM is
+// already reserved up front by a framework's caching allocator (cudaMalloc
+// would fail or fragment its pool), or a latency-critical serving loop that
+// cannot afford cudaMalloc/cudaFree, which may synchronise the device. This
+// entry point runs the same packing and tcgen05 kernels as tccg_plan_run with
+// PREC_BF16X3, but everything it needs besides the caller's A, B and C -- the
+// offset tables, the packed operands and the status word -- lives in the
+// static device array below: TCCG_NOALLOC_SCRATCH_BYTES (64 MiB) on every GPU
+// that loads the library, held until the process exits.
+#define TCCG_NOALLOC_SCRATCH_BYTES (64ull << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[TCCG_NOALLOC_SCRATCH_BYTES];
+
+#define TCCG_NOALLOC_MAX_DEVICES 64
+static void* g_noalloc_ptr[TCCG_NOALLOC_MAX_DEVICES];
+static int g_noalloc_sms[TCCG_NOALLOC_MAX_DEVICES];
+static cudaError_t g_noalloc_err[TCCG_NOALLOC_MAX_DEVICES];
+static std::once_flag g_noalloc_once[TCCG_NOALLOC_MAX_DEVICES];
+
+// The host-side name g_noalloc_scratch is only a stand-in for the device
+// array; its device address comes from cudaGetSymbolAddress, once per device,
+// with that device current (the first call on each device does this).
+static int noalloc_setup(int dev) {
+  std::call_once(g_noalloc_once[dev], [dev] {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&g_noalloc_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    g_noalloc_ptr[dev] = (e == cudaSuccess) ? ptr : nullptr;
+    g_noalloc_err[dev] = e;
+  });
+  if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev])
+    return fail(TCCG_ERR_CUDA, "scratch address of device %d: %s", dev,
+                cudaGetErrorString(g_noalloc_err[dev]));
+  return TCCG_OK;
+}
+
+// The six offset tables of a descriptor, computed on the device (so that no
+// host buffer or host-to-device copy is needed). Table t, entry l:
+// sum_i idx_i(l) * stride_i with the modes of that table, first mode fastest.
+__global__ void __launch_bounds__(256) noalloc_tables_kernel(const tccg_desc d, int64_t* a_m,
+                                                             int64_t* a_k, int64_t* b_n,
+                                                             int64_t* b_k, int64_t* c_m,
+                                                             int64_t* c_n, int64_t M, int64_t N,
+                                                             int64_t K) {
+  const int64_t total = 2 * (M + N + K);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t l = t;
+    int n;
+    const int64_t *ext, *str;
+    int64_t* out;
+    if (l < M) { n = d.nm; ext = d.m_ext; str = d.a_m_stride; out = a_m; }
+    else if ((l -= M) < K) { n = d.nk; ext = d.k_ext; str = d.a_k_stride; out = a_k; }
+    else if ((l -= K) < N) { n = d.nn; ext = d.n_ext; str = d.b_n_stride; out = b_n; }
+    else if ((l -= N) < K) { n = d.nk; ext = d.k_ext; str = d.b_k_stride; out = b_k; }
+    else if ((l -= K) < M) { n = d.nm; ext = d.m_ext; str = d.c_m_stride; out = c_m; }
+    else { l -= M; n = d.nn; ext = d.n_ext; str = d.c_n_stride; out = c_n; }
+    int64_t rem = l, off = 0;
+    for (int i = 0; i < n; ++i) {
+      off += (rem % ext[i]) * str[i];
+      rem /= ext[i];
+    }
+    out[l] = off;
+  }
+}
+
+extern "C" int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, const float* B,
+                                        float* C, double alpha, double beta, void* stream) {
+  if (!desc || !A || !B || !C) return fail(TCCG_ERR_INVALID, "null argument");
+  const tccg_desc& d = *desc;
+  if (d.nm < 1 || d.nn < 1 || d.nk < 1 || d.nm > TCCG_MAX_MODES || d.nn > TCCG_MAX_MODES ||
+      d.nk > TCCG_MAX_MODES)
+    return fail(TCCG_ERR_INVALID, "mode counts (nm=%d nn=%d nk=%d) must be in [1,%d]", d.nm, d.nn,
+                d.nk, TCCG_MAX_MODES);
+  int64_t M = 1, N = 1, K = 1;
+  for (int i = 0; i < d.nm; ++i) { if (d.m_ext[i] < 1) return fail(TCCG_ERR_INVALID, "bad M extent"); M *= d.m_ext[i]; }
+  for (int i = 0; i < d.nn; ++i) { if (d.n_ext[i] < 1) return fail(TCCG_ERR_INVALID, "bad N extent"); N *= d.n_ext[i]; }
+  for (int i = 0; i < d.nk; ++i) { if (d.k_ext[i] < 1) return fail(TCCG_ERR_INVALID, "bad K extent"); K *= d.k_ext[i]; }
+  if (M > (int64_t)1 << 31 || N > (int64_t)1 << 31 || K > (int64_t)1 << 31)
+    return fail(TCCG_ERR_UNSUPPORTED, "M, N and K must each be <= 2^31");
+  // scratch layout: status | a_m | a_k | b_n | b_k | c_m | c_n | A' | B'
+  const int64_t Kc = 2 * round_up(K, 32);
+  size_t off = 256;
+  const size_t o_am = off; off = align_up(off + (size_t)M * 8, 256);
+  const size_t o_ak = off; off = align_up(off + (size_t)K * 8, 256);
+  const size_t o_bn = off; off = align_up(off + (size_t)N * 8, 256);
+  const size_t o_bk = off; off = align_up(off + (size_t)K * 8, 256);
+  const size_t o_cm = off; off = align_up(off + (size_t)M * 8, 256);
+  const size_t o_cn = off; off = align_up(off + (size_t)N * 8, 256);
+  const size_t o_pa = off; off = align_up(off + (size_t)(M * Kc) * 2, 256);
+  const size_t o_pb = off; off = align_up(off + (size_t)(N * Kc) * 2, 256);
+  if (off > TCCG_NOALLOC_SCRATCH_BYTES)
+    return fail(TCCG_ERR_WORKSPACE,
+                "contraction needs %zu bytes of scratch; the allocation-free entry point has a "
+                "fixed %llu-byte static scratch (use tccg_plan_run with a workspace instead)",
+                off, (unsigned long long)TCCG_NOALLOC_SCRATCH_BYTES);
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= TCCG_NOALLOC_MAX_DEVICES) return fail(TCCG_ERR_UNSUPPORTED, "device index %d", dev);
+  int rc = noalloc_setup(dev);
+  if (rc) return rc;
+  rc = ensure_attrs();
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* w = static_cast<char*>(g_noalloc_ptr[dev]);
+  int32_t* status = reinterpret_cast<int32_t*>(w);
+  int64_t* t_am = reinterpret_cast<int64_t*>(w + o_am);
+  int64_t* t_ak = reinterpret_cast<int64_t*>(w + o_ak);
+  int64_t* t_bn = reinterpret_cast<int64_t*>(w + o_bn);
+  int64_t* t_bk = reinterpret_cast<int64_t*>(w + o_bk);
+  int64_t* t_cm = reinterpret_cast<int64_t*>(w + o_cm);
+  int64_t* t_cn = reinterpret_cast<int64_t*>(w + o_cn);
+  // the previous call's status word may be left over: clear it
+  CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int32_t), s));
+  const int64_t ntab = 2 * (M + N + K);
+  noalloc_tables_kernel<<<(unsigned)std::min<int64_t>(cdiv(ntab, 256), 4096), 256, 0, s>>>(
+      d, t_am, t_ak, t_bn, t_bk, t_cm, t_cn, M, N, K);
+  if ((rc = launch_check("noalloc_tables"))) return rc;
+  const void* GA = d.swap_ab ? (const void*)B : (const void*)A;
+  const void* GB = d.swap_ab ? (const void*)A : (const void*)B;
+  PackArgs pa;
+  const int64_t kcover = round_up(K, 32);
+  pa.op[0] = pack_op(GA, t_am, t_ak, M, K, M, kcover, w + o_pa, Kc,
+                     pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride));
+  pa.op[1] = pack_op(GB, t_bn, t_bk, N, K, N, kcover, w + o_pb, Kc,
+                     pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride));
+  if ((rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s))) return rc;
+  using Cfg = TcCfgT<TC_BF16X3>;
+  CUtensorMap tmA, tmB;
+  if ((rc = encode_kmajor(&tmA, w + o_pa, M, Kc, Cfg::BM))) return rc;
+  if ((rc = encode_kmajor(&tmB, w + o_pb, N, Kc, Cfg::BN))) return rc;
+  TcArgs a;
+  a.M = (int32_t)M;
+  a.N = (int32_t)N;
+  a.K = (int32_t)K;
+  a.num_kb = (int32_t)cdiv(K, 32);
+  a.tiles_m = (int32_t)cdiv(M, Cfg::BM);
+  a.tiles_n = (int32_t)cdiv(N, Cfg::BN);
+  a.raster = 8;
+  a.chunk_kb = 16;
+  a.C = C;
+  a.c_m_off = t_cm;
+  a.c_n_off = t_cn;
+  a.alpha = (float)alpha;
+  a.beta = (float)beta;
+  a.status = status;
+  const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
+  if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
+  const int grid = (int)std::min<int64_t>(tiles, g_noalloc_sms[dev]);
+  gett_tc_kernel<TC_BF16X3><<<grid, Cfg::NUM_THREADS, Cfg::SMEM_BYTES, s>>>(tmA, tmB, a);
+  return launch_check("gett_tc (allocation-free)");
+}
