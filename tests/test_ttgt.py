@@ -1,0 +1,85 @@
+"""TTGT (transpose-transpose-GEMM-transpose, tccg/ttgemmt.py, transpose.py)
+and the HPTT-style transposition entry point; FP64 k-split."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from helpers import run_gpu, seeded_normal
+from oracle import LoopNest, error_metrics
+from tccg_b200.plan import Tuning
+from tccg_b200.spec import make_contraction
+
+CASES = [
+    ("abcd", "aeb", "edc", dict(a=40, b=24, c=32, d=20, e=16), 1.0, 1.0),   # C already [M][N]
+    ("acbd", "aeb", "edc", dict(a=40, b=24, c=32, d=20, e=16), 1.5, 0.5),   # C needs a transposition
+    ("abij", "ima", "mjb", dict(a=24, b=24, i=24, j=24, m=24), 1.0, 0.0),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3", "fp64"])
+def test_ttgt_matches_gett(cuda, case, precision):
+    lc, la, lb, sizes, alpha, beta = CASES[case]
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    dt = np.float64 if precision == "fp64" else np.float32
+    A = seeded_normal(ln.size_a, 61).astype(dt)
+    B = seeded_normal(ln.size_b, 62).astype(dt)
+    C = seeded_normal(ln.size_c, 63).astype(dt)
+    gett, _ = run_gpu(con, precision, A, B, C)
+    ttgt, p = run_gpu(con, precision, A, B, C, tuning=Tuning(method="ttgt"))
+    assert "method=TTGT" in p.describe()
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    tol = {"fp32": 1e-6, "bf16x3": 1e-5, "fp64": 1e-13}[precision]
+    assert error_metrics(ttgt, ref)["normwise"] <= tol
+    assert error_metrics(gett, ref)["normwise"] <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ksplit", [2, 5])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_ksplit(cuda, ksplit, precision):
+    sizes = dict(a=50, b=70, k=900)
+    con = make_contraction("ab", "ka", "kb", sizes, 2.0, -1.0)
+    ln = LoopNest("ab", "ka", "kb", sizes)
+    dt = np.float64 if precision == "fp64" else np.float32
+    A, B, C = (seeded_normal(n, s).astype(dt) for n, s in ((ln.size_a, 71), (ln.size_b, 72), (ln.size_c, 73)))
+    out, p = run_gpu(con, precision, A, B, C, tuning=Tuning(ksplit=ksplit))
+    assert "ksplit=%d" % ksplit in p.describe()
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 2.0, -1.0)
+    assert error_metrics(out, ref)["normwise"] <= (1e-13 if precision == "fp64" else 1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_transpose_entry_point(cuda, dtype):
+    """tccg_transpose: B[perm] = alpha * A + beta * B with outer (padded) sizes,
+    HPTT's semantics (dimension j of B is dimension perm[j] of A)."""
+    import torch
+    from tccg_b200 import _native as N
+    tdt = torch.float32 if dtype == "f32" else torch.float64
+    size = [5, 7, 3, 4]
+    outer_a = [6, 7, 4, 4]
+    perm = [2, 0, 3, 1]
+    outer_b = [size[perm[j]] + (1 if j == 1 else 0) for j in range(4)]
+    g = torch.Generator(device="cuda").manual_seed(1)
+    A = torch.randn(int(np.prod(outer_a)), generator=g, device="cuda", dtype=tdt)
+    B = torch.randn(int(np.prod(outer_b)), generator=g, device="cuda", dtype=tdt)
+    B0 = B.clone()
+    i32 = (ctypes.c_int32 * 4)(*perm)
+    i64 = lambda v: (ctypes.c_int64 * 4)(*v)
+    rc = N.lib().tccg_transpose(N.F32 if dtype == "f32" else N.F64, 4, i32, i64(size), i64(outer_a),
+                                i64(outer_b), 2.0, ctypes.c_void_p(A.data_ptr()), 0.5,
+                                ctypes.c_void_p(B.data_ptr()), None)
+    N.check(rc)
+    torch.cuda.synchronize()
+    # reference in numpy: column-major views
+    An = A.cpu().numpy().reshape(outer_a[::-1]).transpose()[:size[0], :size[1], :size[2], :size[3]]
+    Bv = B0.cpu().numpy().reshape(outer_b[::-1]).transpose()
+    want = Bv.copy()
+    sl = tuple(slice(0, size[perm[j]]) for j in range(4))
+    want[sl] = 2.0 * np.transpose(An, perm) + 0.5 * Bv[sl]
+    got = B.cpu().numpy().reshape(outer_b[::-1]).transpose()
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
