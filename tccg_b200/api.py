@@ -34,7 +34,11 @@ class Compiled:
                  dtype: Optional[str] = None):
         self.contraction = con
         self.precision = precision
-        self.plan = Plan(con, precision=precision, tuning=tuning, dtype=dtype)
+        if tuning is not None and tuning.method == "log":
+            from .loops import LoG
+            self.plan = _LoGAdapter(LoG(con, precision))
+        else:
+            self.plan = Plan(con, precision=precision, tuning=tuning, dtype=dtype)
         self._ws = None
 
     @property
@@ -91,6 +95,21 @@ class Compiled:
 
     def flops(self, beta: Optional[float] = None) -> float:
         return self.contraction.flop_count(beta)
+
+
+class _LoGAdapter:
+    """Gives a LoG the Plan interface used by Compiled."""
+
+    def __init__(self, log):
+        self.log = log
+        self.workspace_bytes = 0
+        self.c_dtype = "f64" if log.precision == "fp64" else "f32"
+
+    def run(self, A, B, C, alpha=None, beta=None, workspace=None, stream=None):
+        self.log.run(A, B, C, alpha, beta, stream=stream)
+
+    def describe(self):
+        return self.log.describe()
 
 
 def compile(spec, float_type: str = "s", precision: Optional[str] = None,

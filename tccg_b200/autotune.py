@@ -1,0 +1,193 @@
+"""On-device autotuner with a persistent cache.
+
+TCCG ranks GETT candidates with a performance model (gett.py:590-687), builds
+the best ``--maxImplementations`` of them with make, times them in a
+generated harness and keeps the results in SQLite keyed on the contraction,
+the sizes, the CPU and the types (sql_util.py:206-306; lookup tccg.py:192-221).
+
+Here the candidates are kernel choices of one native plan -- method (GETT or
+TTGT), k-split for the SIMT kernels, tile-raster group and K-chunk length for
+the tcgen05 kernels -- ordered by a simple model (defaults first), timed on
+the device with CUDA events (minimum over repetitions, L2 flushed in between
+like TCCG's trashCache, tccg.py:725-737), and the winner is stored in SQLite
+keyed on (contraction, extents, precision, operand type, beta != 0, GPU name,
+SM count, library version). A cache hit skips the search.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sqlite3
+import time
+from typing import List, Optional, Tuple
+
+from .plan import Plan, Tuning
+from .spec import Contraction
+
+CODE_VERSION = "tccg_b200-0.1"
+
+
+def default_db_path() -> str:
+    if os.environ.get("TCCG_B200_DB"):
+        return os.environ["TCCG_B200_DB"]
+    if os.environ.get("TCCG_ROOT"):
+        return os.path.join(os.environ["TCCG_ROOT"], "tccg_b200.db")
+    return os.path.join(os.path.expanduser("~"), ".cache", "tccg_b200", "tuning.db")
+
+
+def contraction_key(con: Contraction) -> str:
+    """Contraction string with extents, on the original (file) indices."""
+    t = lambda T: "%s[%s]" % (T.label, ",".join("%s:%d" % (i.label, i.size) for i in T.indices))
+    return "%s=%s*%s" % (t(con.C0), t(con.A0), t(con.B0))
+
+
+class TuningDB:
+    """SQLite store of measurements and of the best tuning per key."""
+
+    def __init__(self, path: Optional[str] = None):
+        self.path = path or default_db_path()
+        d = os.path.dirname(self.path)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        self.conn = sqlite3.connect(self.path)
+        c = self.conn.cursor()
+        c.execute("CREATE TABLE IF NOT EXISTS measurements (key TEXT, tuning TEXT, ms REAL, "
+                  "gflops REAL, ts REAL)")
+        c.execute("CREATE TABLE IF NOT EXISTS best (key TEXT PRIMARY KEY, tuning TEXT, ms REAL, "
+                  "gflops REAL, ts REAL)")
+        self.conn.commit()
+
+    def lookup(self, key: str) -> Optional[Tuple[Tuning, float]]:
+        r = self.conn.execute("SELECT tuning, gflops FROM best WHERE key = ?", (key,)).fetchone()
+        if r is None:
+            return None
+        return Tuning(**json.loads(r[0])), float(r[1])
+
+    def record(self, key: str, tuning: Tuning, ms: float, gflops: float) -> None:
+        self.conn.execute("INSERT INTO measurements VALUES (?, ?, ?, ?, ?)",
+                          (key, json.dumps(tuning.__dict__), ms, gflops, time.time()))
+        self.conn.commit()
+
+    def store_best(self, key: str, tuning: Tuning, ms: float, gflops: float) -> None:
+        self.conn.execute("INSERT OR REPLACE INTO best VALUES (?, ?, ?, ?, ?)",
+                          (key, json.dumps(tuning.__dict__), ms, gflops, time.time()))
+        self.conn.commit()
+
+    def measurements(self, key: str):
+        return self.conn.execute("SELECT tuning, ms, gflops FROM measurements WHERE key = ?",
+                                 (key,)).fetchall()
+
+
+def gpu_signature() -> str:
+    import torch
+    p = torch.cuda.get_device_properties(torch.cuda.current_device())
+    return "%s/sm%d%d/%dSM" % (p.name, p.major, p.minor, p.multi_processor_count)
+
+
+def tuning_key(con: Contraction, precision: str, dtype: str, gpu: str) -> str:
+    return "|".join([contraction_key(con), precision, dtype, "beta" if con.beta != 0 else "nobeta",
+                     gpu, CODE_VERSION])
+
+
+def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_sms: int = 148
+               ) -> List[Tuning]:
+    """Candidate tunings, the model's favourite first: the defaults, then
+    variations that matter for this shape."""
+    M, N, K = con.sizeM, con.sizeN, max(1, con.sizeK)
+    out: List[Tuning] = []
+    for method in methods:
+        if precision in ("fp32", "fp64"):
+            bm, bn = (128, 128) if precision == "fp32" else (128, 64)
+            tiles = -(-M // bm) * -(-N // bn)
+            splits = [1]
+            # k-split only pays when there are fewer tiles than SMs can hold
+            # (TCCG: only when M*N is small, gett.py:933)
+            if tiles < 2 * num_sms:
+                for s in (2, 4, 8, 16):
+                    if K >= 64 * s:
+                        splits.append(s)
+            splits.sort(key=lambda s: abs(tiles * s - 2 * num_sms))
+            out += [Tuning(method=method, ksplit=s) for s in splits]
+        else:
+            rasters = [8, 4, 16]
+            chunks = [16, 32, 8] if precision == "bf16x3" else [0]
+            for r in rasters:
+                for c in chunks:
+                    out.append(Tuning(method=method, raster=r, variant=c))
+    return out
+
+
+def _flush_l2(buf):
+    buf.add_(1.0)
+
+
+def measure(plan: Plan, reps: int = 5, inputs=None) -> float:
+    """Minimum device time (ms) of one plan run over ``reps`` repetitions,
+    with a 256 MB buffer written between repetitions to flush L2."""
+    import torch
+    con = plan.con
+    dev = torch.device("cuda", torch.cuda.current_device())
+    tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}
+    if inputs is None:
+        g = torch.Generator(device=dev).manual_seed(0)
+        A = torch.randn(con.A0.num_elements(), generator=g, device=dev).to(tdt[plan.dtype])
+        B = torch.randn(con.B0.num_elements(), generator=g, device=dev).to(tdt[plan.dtype])
+        C = torch.randn(con.C0.num_elements(), generator=g, device=dev).to(tdt[plan.c_dtype])
+    else:
+        A, B, C = inputs
+    ws = torch.empty(max(plan.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+    trash = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    plan.run(A, B, C, workspace=ws)  # warm-up
+    torch.cuda.synchronize()
+    best = float("inf")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(reps):
+        _flush_l2(trash)
+        e0.record()
+        plan.run(A, B, C, workspace=ws)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    if plan.status() != 0:
+        raise RuntimeError("device error while tuning %s" % plan.describe())
+    return best
+
+
+def autotune(con: Contraction, precision: str, max_implementations: int = 16,
+             cache_path: Optional[str] = None, dtype: Optional[str] = None,
+             ignore_cache: bool = False, methods=("gett", "ttgt"), verbose: bool = False,
+             max_workspace_gb: Optional[float] = None) -> Tuning:
+    """Best tuning for ``con``: from the cache, else by timing up to
+    ``max_implementations`` candidates (-1 = all)."""
+    import torch
+    from .plan import operand_dtype
+    dtype = dtype or operand_dtype(precision)
+    db = TuningDB(cache_path)
+    key = tuning_key(con, precision, dtype, gpu_signature())
+    if not ignore_cache:
+        hit = db.lookup(key)
+        if hit is not None:
+            if verbose:
+                print("[tccg_b200] tuning cache hit: %s (%.2f GFLOPS)" % (hit[0].key(), hit[1]))
+            return hit[0]
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    cands = candidates(con, precision, methods, sms)
+    if max_implementations >= 0:
+        cands = cands[:max(1, max_implementations)]
+    best, best_ms = None, float("inf")
+    flops = con.flop_count()
+    for t in cands:
+        p = Plan(con, precision=precision, tuning=t, dtype=dtype)
+        if max_workspace_gb is not None and p.workspace_bytes > max_workspace_gb * 2 ** 30:
+            continue
+        ms = measure(p)
+        gf = flops / (ms * 1e-3) / 1e9
+        db.record(key, t, ms, gf)
+        if verbose:
+            print("[tccg_b200] %-28s %9.3f ms %10.1f GFLOPS  %s" % (t.key(), ms, gf, p.describe()))
+        if ms < best_ms:
+            best, best_ms = t, ms
+    if best is None:
+        raise RuntimeError("no candidate fits the workspace limit")
+    db.store_best(key, best, best_ms, flops / (best_ms * 1e-3) / 1e9)
+    return best

@@ -83,3 +83,29 @@ def test_transpose_entry_point(cuda, dtype):
     want[sl] = 2.0 * np.transpose(An, perm) + 0.5 * Bv[sl]
     got = B.cpu().numpy().reshape(outer_b[::-1]).transpose()
     assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+@pytest.mark.parametrize("case", [
+    ("abij", "ima", "mjb", dict(a=24, b=20, i=6, j=5, m=24), 1.0, 0.0),     # loops over i, j
+    ("pqr", "qs", "spr", dict(p=37, q=29, r=11, s=53), 0.75, -0.5),         # swap, loop over r
+    ("ab", "ak", "kb", dict(a=70, b=50, k=90), 1.0, 0.0),                    # plain GEMM: one item
+])
+def test_loops_over_gemm(cuda, precision, case):
+    """LoG (tccg/gemm_loop.py) as one batched launch matches the oracle."""
+    import torch
+    from tccg_b200.loops import LoG
+    lc, la, lb, sizes, alpha, beta = case
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A = seeded_normal(ln.size_a, 81).astype(np.float32)
+    B = seeded_normal(ln.size_b, 82).astype(np.float32)
+    C = seeded_normal(ln.size_c, 83).astype(np.float32)
+    log = LoG(con, precision)
+    dA, dB, dC = (torch.from_numpy(x).cuda() for x in (A, B, C))
+    log.run(dA, dB, dC)
+    torch.cuda.synchronize()
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    tol = {"fp32": 1e-6, "bf16x3": 1e-5}[precision]
+    assert error_metrics(dC.double().cpu().numpy(), ref)["normwise"] <= tol, log.describe()
