@@ -93,35 +93,167 @@ __device__ __forceinline__ void pack_tile(const PackOperand& o, int64_t kt, int6
       const int64_t k = k0 + i;
       if (k < o.Kcover && r < o.Rcover) dst[k * o.ld + r] = static_cast<Tout>(tile[i][tx]);
     }
-  } else if constexpr (LAYOUT == PACK_K_BF16) {
-    const int64_t k = k0 + tx;
+  } else {
+    // K-major bf16 rows: thread t packs 4 consecutive k of row t/8 and writes
+    // them as one 8-byte store (two for BF16X3: hi and lo). Reads of
+    // tile[kq + j][row] hit 32 distinct banks across the warp.
+    const int t = ty * 32 + tx;
+    const int rl = t >> 3, kq = (t & 7) * 4;
+    const int64_t r = r0 + rl;
+    __nv_bfloat16* base = reinterpret_cast<__nv_bfloat16*>(dst) + r * o.ld;
+    if (r < o.Rcover) {
+      if constexpr (LAYOUT == PACK_K_BF16) {
+        const int64_t k = k0 + kq;
+        if (k + 3 < o.Kcover && (o.ld & 3) == 0) {
+          __nv_bfloat162 p0 = __floats2bfloat162_rn((float)tile[kq][rl], (float)tile[kq + 1][rl]);
+          __nv_bfloat162 p1 = __floats2bfloat162_rn((float)tile[kq + 2][rl], (float)tile[kq + 3][rl]);
+          uint2 u;
+          u.x = *reinterpret_cast<uint32_t*>(&p0);
+          u.y = *reinterpret_cast<uint32_t*>(&p1);
+          *reinterpret_cast<uint2*>(base + k) = u;
+        } else {
 #pragma unroll
-    for (int i = ty; i < 32; i += 8) {
-      const int64_t r = r0 + i;
-      if (r < o.Rcover && k < o.Kcover) dst[r * o.ld + k] = __float2bfloat16_rn((float)tile[tx][i]);
-    }
-  } else {  // PACK_K_BF16X3: each 32-wide k block becomes [hi x32 | lo x32]
+          for (int j = 0; j < 4; ++j)
+            if (k + j < o.Kcover) base[k + j] = __float2bfloat16_rn((float)tile[kq + j][rl]);
+        }
+      } else {  // PACK_K_BF16X3: each 32-wide k block becomes [hi x32 | lo x32]
+        float v[4];
+        __nv_bfloat16 hi[4], lo[4];
 #pragma unroll
-    for (int i = ty; i < 32; i += 8) {
-      const int64_t r = r0 + i;
-      if (r < o.Rcover) {
-        const float v = (float)tile[tx][i];
-        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-        __nv_bfloat16* row = reinterpret_cast<__nv_bfloat16*>(dst) + r * o.ld + (k0 / 32) * 64;
-        row[tx] = hi;
-        row[32 + tx] = lo;
+        for (int j = 0; j < 4; ++j) {
+          v[j] = (float)tile[kq + j][rl];
+          hi[j] = __float2bfloat16_rn(v[j]);
+          lo[j] = __float2bfloat16_rn(v[j] - __bfloat162float(hi[j]));
+        }
+        __nv_bfloat16* row = base + (k0 / 32) * 64;  // 16-byte aligned: ld % 64 == 0
+        uint2 uh, ul;
+        __nv_bfloat162 h0 = __halves2bfloat162(hi[0], hi[1]), h1 = __halves2bfloat162(hi[2], hi[3]);
+        __nv_bfloat162 l0 = __halves2bfloat162(lo[0], lo[1]), l1 = __halves2bfloat162(lo[2], lo[3]);
+        uh.x = *reinterpret_cast<uint32_t*>(&h0);
+        uh.y = *reinterpret_cast<uint32_t*>(&h1);
+        ul.x = *reinterpret_cast<uint32_t*>(&l0);
+        ul.y = *reinterpret_cast<uint32_t*>(&l1);
+        *reinterpret_cast<uint2*>(row + kq) = uh;
+        *reinterpret_cast<uint2*>(row + 32 + kq) = ul;
       }
     }
   }
 }
 
-// grid = (ceil(Kcover/32), ceil(Rcover/32), 2), block = (32, 8)
+// K-major layouts: one CTA packs 32 rows x 128 k. All 16 loads of a thread are
+// issued before the first shared-memory store, so each thread keeps 16
+// global loads in flight (the 32x32 tile left the pass latency-bound).
+constexpr int PACK_KT_WIDE = 128;
+
+template <int LAYOUT>
+__host__ __device__ constexpr int pack_k_tile() {
+  return LAYOUT == PACK_MN ? 32 : PACK_KT_WIDE;
+}
+
+template <typename Tin, int LAYOUT>
+__device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t kt, int64_t rt) {
+  constexpr int KT = PACK_KT_WIDE, SB = KT / 32;
+  const int64_t k0 = kt * KT, r0 = rt * 32;
+  if (k0 >= o.Kcover || r0 >= o.Rcover) return;
+  __shared__ float tile[KT][33];  // [k_local][r_local]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const Tin* src = static_cast<const Tin*>(o.src);
+  float v[SB][4];
+  if (o.read_k_fast) {
+    int64_t roff[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t r = r0 + ty + 8 * i;
+      roff[i] = (r < o.R) ? o.row_off[r] : -1;
+    }
+#pragma unroll
+    for (int sb = 0; sb < SB; ++sb) {
+      const int64_t k = k0 + sb * 32 + tx;
+      const int64_t coff = (k < o.Kk) ? o.col_off[k] : -1;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        v[sb][i] = (roff[i] >= 0 && coff >= 0) ? load_as_acc<Tin>(src + roff[i] + coff) : 0.0f;
+    }
+#pragma unroll
+    for (int sb = 0; sb < SB; ++sb)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) tile[sb * 32 + tx][ty + 8 * i] = v[sb][i];
+  } else {
+    const int64_t r = r0 + tx;
+    const int64_t roff = (r < o.R) ? o.row_off[r] : -1;
+#pragma unroll
+    for (int sb = 0; sb < SB; ++sb)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int64_t k = k0 + sb * 32 + ty + 8 * i;
+        v[sb][i] = (roff >= 0 && k < o.Kk) ? load_as_acc<Tin>(src + roff + o.col_off[k]) : 0.0f;
+      }
+#pragma unroll
+    for (int sb = 0; sb < SB; ++sb)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) tile[sb * 32 + ty + 8 * i][tx] = v[sb][i];
+  }
+  __syncthreads();
+  // write: thread t packs 4 consecutive k of row t/8 per 32-wide k block
+  const int t = ty * 32 + tx;
+  const int rl = t >> 3, kq = (t & 7) * 4;
+  const int64_t r = r0 + rl;
+  if (r >= o.Rcover) return;
+  __nv_bfloat16* base = static_cast<__nv_bfloat16*>(o.dst) + r * o.ld;
+#pragma unroll
+  for (int sb = 0; sb < SB; ++sb) {
+    const int kl = sb * 32 + kq;
+    const int64_t k = k0 + kl;
+    if (k >= o.Kcover) break;
+    if constexpr (LAYOUT == PACK_K_BF16) {
+      if (k + 3 < o.Kcover && (o.ld & 3) == 0) {
+        __nv_bfloat162 p0 = __floats2bfloat162_rn(tile[kl][rl], tile[kl + 1][rl]);
+        __nv_bfloat162 p1 = __floats2bfloat162_rn(tile[kl + 2][rl], tile[kl + 3][rl]);
+        uint2 u;
+        u.x = *reinterpret_cast<uint32_t*>(&p0);
+        u.y = *reinterpret_cast<uint32_t*>(&p1);
+        *reinterpret_cast<uint2*>(base + k) = u;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (k + j < o.Kcover) base[k + j] = __float2bfloat16_rn(tile[kl + j][rl]);
+      }
+    } else {  // PACK_K_BF16X3: each 32-wide k block becomes [hi x32 | lo x32]
+      __nv_bfloat16 hi[4], lo[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float x = tile[kl + j][rl];
+        hi[j] = __float2bfloat16_rn(x);
+        lo[j] = __float2bfloat16_rn(x - __bfloat162float(hi[j]));
+      }
+      __nv_bfloat16* row = base + ((k0 + sb * 32) / 32) * 64;  // 16-byte aligned: ld % 64 == 0
+      __nv_bfloat162 h0 = __halves2bfloat162(hi[0], hi[1]), h1 = __halves2bfloat162(hi[2], hi[3]);
+      __nv_bfloat162 l0 = __halves2bfloat162(lo[0], lo[1]), l1 = __halves2bfloat162(lo[2], lo[3]);
+      uint2 uh, ul;
+      uh.x = *reinterpret_cast<uint32_t*>(&h0);
+      uh.y = *reinterpret_cast<uint32_t*>(&h1);
+      ul.x = *reinterpret_cast<uint32_t*>(&l0);
+      ul.y = *reinterpret_cast<uint32_t*>(&l1);
+      *reinterpret_cast<uint2*>(row + kq) = uh;
+      *reinterpret_cast<uint2*>(row + 32 + kq) = ul;
+    }
+  }
+}
+
+template <typename Tin, typename Tout, int LAYOUT>
+__device__ __forceinline__ void pack_any(const PackOperand& o, int64_t kt, int64_t rt) {
+  if constexpr (LAYOUT == PACK_MN)
+    pack_tile<Tin, Tout, LAYOUT>(o, kt, rt);
+  else
+    pack_tile_kmajor<Tin, LAYOUT>(o, kt, rt);
+}
+
+// grid = (ceil(Kcover/pack_k_tile), ceil(Rcover/32), 2), block = (32, 8)
 template <typename Tin, typename Tout, int LAYOUT>
 __global__ void __launch_bounds__(256) pack_kernel(const PackArgs args) {
   const PackOperand& o = args.op[blockIdx.z];
   if (!o.active) return;
-  pack_tile<Tin, Tout, LAYOUT>(o, blockIdx.x, blockIdx.y);
+  pack_any<Tin, Tout, LAYOUT>(o, blockIdx.x, blockIdx.y);
 }
 
 // Grouped packing: job j (an operand of one contraction) owns the CTAs
@@ -129,7 +261,7 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackArgs args) {
 struct PackJob {
   PackOperand op;
   int64_t begin;   // first CTA of this job
-  int64_t ktiles;  // tiles along k
+  int64_t ktiles;  // tiles along k (pack_k_tile<LAYOUT>() wide)
 };
 
 template <typename Tin, typename Tout, int LAYOUT>
@@ -142,7 +274,7 @@ __global__ void __launch_bounds__(256) pack_group_kernel(const PackJob* jobs, in
   }
   const PackJob& j = jobs[lo];
   const int64_t local = t - j.begin;
-  pack_tile<Tin, Tout, LAYOUT>(j.op, local % j.ktiles, local / j.ktiles);
+  pack_any<Tin, Tout, LAYOUT>(j.op, local % j.ktiles, local / j.ktiles);
 }
 
 }  // namespace tccg

@@ -453,7 +453,7 @@ template <typename Tin, typename Tout, int LAYOUT>
 static int launch_pack(const PackArgs& pa, cudaStream_t s) {
   int64_t kx = std::max(pa.op[0].Kcover, pa.op[1].Kcover);
   int64_t ry = std::max(pa.op[0].Rcover, pa.op[1].Rcover);
-  dim3 grid((unsigned)cdiv(kx, 32), (unsigned)cdiv(ry, 32), 2);
+  dim3 grid((unsigned)cdiv(kx, pack_k_tile<LAYOUT>()), (unsigned)cdiv(ry, 32), 2);
   if (grid.y > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "operand has too many rows (%lld)", (long long)ry);
   mark(0, 0, s);
   pack_kernel<Tin, Tout, LAYOUT><<<grid, dim3(32, 8), 0, s>>>(pa);
@@ -857,11 +857,12 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       ob = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b, p->Kc, p->read_k_fast_b);
     }
     PackOperand ops[2] = {oa, ob};
+    const int kt = simt ? pack_k_tile<PACK_MN>() : pack_k_tile<PACK_K_BF16>();
     for (int j = 0; j < 2; ++j) {
       PackJob& jb = jobs[2 * i + j];
       jb.op = ops[j];
       jb.begin = pack_ctas;
-      jb.ktiles = cdiv(ops[j].Kcover, 32);
+      jb.ktiles = cdiv(ops[j].Kcover, kt);
       pack_ctas += jb.ktiles * cdiv(ops[j].Rcover, 32);
     }
     if (g->prec == TCCG_PREC_FP32) {
