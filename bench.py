@@ -432,6 +432,217 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+# --------------------------------------------------------------------------
+# every configuration (python bench.py --suite): the tables of DESIGN.md
+# --------------------------------------------------------------------------
+SUITE = {
+    "cfg1": "C[a,b,i,j] = A[i,m,a] * B[m,j,b]\na=48\nb=48\ni=48\nj=48\nm=48\n",
+    "cfg2": "C[a,b,c,d] = A[a,e,b] * B[e,d,c] + C[a,b,c,d]\na=96\nb=96\nc=96\nd=96\ne=16\n",
+    "cfg3": workload(32),
+    "cfg4": "C[i0,j0,j1,i1] = A[k0,i0,k1,i1] * B[k1,j1,k0,j0]\ni0=64\ni1=64\nj0=64\nj1=64\nk0=32\nk1=32\n",
+}
+
+
+def _time(fn, warm=3, reps=20, flush=None):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(reps):
+        if flush is not None:
+            flush.add_(1.0)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def _cpu_tccg_gett(name, A, B, C, alpha, beta, flops):
+    """TCCG's generated GETT candidates (oracle/_ref/<name>.so) timed TCCG's
+    way: min of 4 runs after a 2x128 MiB cache trash (tccg.py:975-1057);
+    the best candidate is reported, as TCCG selects it."""
+    import ctypes
+    import numpy as np
+    so = os.path.join(ROOT, "oracle", "_ref", name + ".so")
+    if not os.path.exists(so):
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import aligned_copy
+    L = ctypes.CDLL(so)
+    L.tccg_gett_count.restype = ctypes.c_int
+    L.tccg_gett_threads.restype = ctypes.c_int
+    L.tccg_gett_name.restype = ctypes.c_char_p
+    L.tccg_gett_run.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 3 + [ctypes.c_float] * 2
+    A, B, C0 = aligned_copy(A), aligned_copy(B), aligned_copy(C)
+    trash1 = np.ones(32 * 1024 * 1024, dtype=np.float32)
+    trash2 = np.ones(32 * 1024 * 1024, dtype=np.float32)
+    best = (float("inf"), None)
+    for i in range(L.tccg_gett_count()):
+        for _ in range(4):
+            Cw = aligned_copy(C0)
+            trash1 += 0.999 * trash2
+            t0 = time.perf_counter()
+            L.tccg_gett_run(i, A.ctypes.data, B.ctypes.data, Cw.ctypes.data, alpha, beta)
+            t = time.perf_counter() - t0
+            if t < best[0]:
+                best = (t, L.tccg_gett_name(i).decode())
+    return {"gflops": flops / best[0] / 1e9, "threads": L.tccg_gett_threads(),
+            "candidates": L.tccg_gett_count(), "best": best[1][:60],
+            "note": "TCCG-generated AVX2 GETT with the oracle's HPTT-API stand-in, g++ -O3 -march=x86-64-v3"}
+
+
+def run_suite(args):
+    import numpy as np
+    import torch
+    from tccg_b200 import parse_text
+    from tccg_b200.api import Compiled
+    from tccg_b200.autograd import GettFunction
+    from tccg_b200.grouped import Group
+    from tccg_b200.plan import Tuning
+    from tccg_b200.workloads import batched_workload
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import LoopNest
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    flush = torch.empty(64 * 1024 * 1024, device=dev)
+    peaks, _ = measured_peaks()
+    out = {}
+
+    def gen(n, seed, dist):
+        g = torch.Generator(device=dev).manual_seed(seed)
+        x = torch.randn(n, generator=g, device=dev)
+        return x if dist == "normal" else (torch.rand(n, generator=g, device=dev) * 2 - 1)
+
+    def errs(C, C64):
+        n = torch.linalg.vector_norm(C64).item()
+        return torch.linalg.vector_norm(C.double() - C64).item() / n
+
+    def cpu_loop(con, A, B, C, alpha, beta, secs=3.0):
+        c, a, b = con.C0.labels, con.A0.labels, con.B0.labels
+        sizes = {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices}
+        ln = LoopNest(c, a, b, sizes)
+        Cb = C.copy()
+        s = 8192
+        while True:
+            t0 = time.perf_counter()
+            ln.run(A, B, Cb, alpha, beta, 0, s)
+            t = time.perf_counter() - t0
+            if t > 0.3 or s >= ln.size_c:
+                break
+            s = min(ln.size_c, s * 4)
+        return 2.0 * s * ln.size_k / t / 1e9
+
+    wanted = set(args.suite_configs.split(","))
+    for name in ("cfg1", "cfg2", "cfg3"):
+        if name not in wanted:
+            continue
+        con = parse_text(SUITE[name])
+        dist = "uniform" if name == "cfg1" else "normal"
+        nA, nB, nC = con.A0.num_elements(), con.B0.num_elements(), con.C0.num_elements()
+        A, B, C0 = gen(nA, 1, dist), gen(nB, 2, dist), gen(nC, 3, dist)
+        small = (nA + nB + nC) * 4 < 126e6
+        C64 = C0.double().clone()
+        Compiled(con, "fp64")(A.double(), B.double(), C64)
+        flops = con.flop_count()
+        byts = (nA + nB) * 4 + nC * 4 * (2 if con.beta else 1)
+        res = {"flop": flops, "algorithmic_bytes_fp32": byts}
+        modes = [("fp32", "gett"), ("bf16x3", "gett"), ("bf16", "gett"), ("fp64", "gett")]
+        if name == "cfg2":
+            modes += [("fp32", "ttgt"), ("bf16", "ttgt"), ("bf16x3", "ttgt")]
+        for prec, method in modes:
+            if name == "cfg3" and method == "ttgt":
+                continue
+            dbl = prec == "fp64"
+            c = Compiled(con, prec, Tuning(method=method))
+            Ai, Bi = (A.double(), B.double()) if dbl else (A, B)
+            if prec == "bf16" and name == "cfg2":
+                c = Compiled(con, prec, Tuning(method=method), dtype="bf16")
+                Ai, Bi = A.bfloat16(), B.bfloat16()
+            Cw = C0.double().clone() if dbl else C0.clone()
+            ws = c.workspace(dev)
+            reps = 5 if (name == "cfg3" and prec in ("fp32", "fp64")) else 20
+            ms = _time(lambda: c.plan.run(Ai, Bi, Cw, workspace=ws), 2, reps, flush if small else None)
+            Cw = C0.double().clone() if dbl else C0.clone()
+            c.plan.run(Ai, Bi, Cw, workspace=ws)
+            torch.cuda.synchronize()
+            e = errs(Cw, C64) if not dbl else errs(Cw, C64)
+            key = "%s_%s" % (prec, method)
+            gbps = (byts * (2 if dbl else 1) if prec != "bf16" else byts - (nA + nB) * 2) / (ms * 1e-3) / 1e9
+            res[key] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "gbs": gbps,
+                        "hbm_frac": gbps / peaks["hbm_gbs"], "normwise_vs_fp64": e,
+                        "plan": c.describe()}
+            del Cw, c, ws
+            torch.cuda.empty_cache()
+        # CPU baselines (host cores)
+        An, Bn, Cn = A.cpu().numpy(), B.cpu().numpy(), C0.cpu().numpy()
+        res["cpu_loop_nest_gflops"] = cpu_loop(con, An, Bn, Cn, con.alpha, con.beta)
+        res["cpu_threads"] = os.cpu_count()
+        if name in ("cfg1", "cfg2"):
+            res["cpu_tccg_gett"] = _cpu_tccg_gett("tccg_gett_" + name, An, Bn, Cn, con.alpha,
+                                                  con.beta, flops)
+        out[name] = res
+        print(json.dumps({name: res}), flush=True)
+        del A, B, C0, C64
+        torch.cuda.empty_cache()
+
+    # configuration 4: forward + dA + dB through the autograd Function
+    if "cfg4" not in wanted:
+        return out if "cfg5" not in wanted else _suite_cfg5(out, gen, flush, dev)
+    con = parse_text(SUITE["cfg4"])
+    res = {"flop_each": con.flop_count()}
+    for prec, dt in (("fp32", torch.float32), ("bf16", torch.bfloat16), ("bf16x3", torch.float32)):
+        shA = tuple(i.size for i in reversed(con.A0.indices))
+        shB = tuple(i.size for i in reversed(con.B0.indices))
+        A = gen(con.A0.num_elements(), 4, "normal").reshape(shA).to(dt).requires_grad_()
+        B = gen(con.B0.num_elements(), 5, "normal").reshape(shB).to(dt).requires_grad_()
+        Cout = GettFunction.apply(A, B, con, prec)
+        dC = torch.randn_like(Cout)
+        fwd = _time(lambda: GettFunction.apply(A, B, con, prec), 3, 20, flush)
+        both = _time(lambda: torch.autograd.grad(GettFunction.apply(A, B, con, prec), (A, B), dC),
+                     3, 20, flush)
+        res[prec] = {"fwd_ms": fwd, "fwd_bwd_ms": both,
+                     "fwd_tflops": con.flop_count() / (fwd * 1e-3) / 1e12,
+                     "fwd_bwd_tflops": 3 * con.flop_count() / (both * 1e-3) / 1e12}
+    out["cfg4"] = res
+    print(json.dumps({"cfg4": res}), flush=True)
+    if "cfg5" in wanted:
+        _suite_cfg5(out, gen, flush, dev)
+    return out
+
+
+def _suite_cfg5(out, gen, flush, dev):
+    """Configuration 5: 256 mixed contractions, one grouped launch in a CUDA
+    graph, against one plan run (pack + GETT launch) per contraction."""
+    import torch
+    from tccg_b200.grouped import Group
+    from tccg_b200.workloads import batched_workload
+    items = batched_workload(256, seed=0)
+    tot = sum(c.flop_count() for c in items)
+    res = {"items": 256, "flop": tot}
+    As = [gen(c.A0.num_elements(), 10 + i, "normal") for i, c in enumerate(items)]
+    Bs = [gen(c.B0.num_elements(), 1000 + i, "normal") for i, c in enumerate(items)]
+    Cs = [torch.empty(c.C0.num_elements(), device=dev) for c in items]
+    for prec in ("bf16x3", "fp32"):
+        grp = Group(items, prec)
+        grp.bind(As, Bs, Cs)
+        grp.capture()
+        t_graph = _time(grp.replay, 3, 10, flush)
+        t_items = _time(lambda: grp.run_per_item(), 2, 5, flush)
+        res[prec] = {"graph_ms": t_graph, "graph_tflops": tot / (t_graph * 1e-3) / 1e12,
+                     "per_item_launches_ms": t_items,
+                     "per_item_tflops": tot / (t_items * 1e-3) / 1e12,
+                     "workspace_gib": grp.workspace_bytes / 2 ** 30}
+        del grp
+        torch.cuda.empty_cache()
+    out["cfg5"] = res
+    print(json.dumps({"cfg5": res}), flush=True)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -447,7 +658,13 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--k-extent", type=int, default=32,
                     help="extent of C's last index (32 = the full workload)")
+    ap.add_argument("--suite", action="store_true",
+                    help="measure every configuration (one JSON line each) instead of the headline")
+    ap.add_argument("--suite-configs", default="cfg1,cfg2,cfg3,cfg4,cfg5")
     args = ap.parse_args()
+    if args.suite:
+        run_suite(args)
+        return 0
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":

@@ -184,6 +184,22 @@ class LoopNest:
         return np.asfortranarray(R)
 
 
+def aligned_empty(n: int, dtype=np.float32, align: int = 64) -> np.ndarray:
+    """Uninitialised 1-D array whose data is ``align``-byte aligned (TCCG's
+    generated code uses aligned AVX loads/stores and its harness allocates
+    with posix_memalign(64), tccg.py:910-919)."""
+    itemsize = np.dtype(dtype).itemsize
+    raw = np.empty(n * itemsize + align, dtype=np.uint8)
+    off = (-raw.ctypes.data) % align
+    return raw[off:off + n * itemsize].view(dtype)
+
+
+def aligned_copy(x: np.ndarray, align: int = 64) -> np.ndarray:
+    y = aligned_empty(x.size, x.dtype, align)
+    y[:] = x.ravel()
+    return y
+
+
 def tccg_inputs(n: int, which: str, dtype=np.float32) -> np.ndarray:
     """TCCG's deterministic values for operand ``which`` in {'A','B','C'}
     (tccg.py:957-971)."""

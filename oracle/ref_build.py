@@ -134,7 +134,82 @@ CFG3_SLAB = ("C[a,b,c,i,j,k] = A[a,m,b,n,c] * B[m,i,n,j,k]\n"
 
 def build_all(ref_root: str = DEFAULT_REF) -> List[str]:
     """Everything the GPU box needs from the reference: the timed CPU reference
-    for the benchmark workload."""
+    for the benchmark workload, and TCCG's own generated GETT for the two
+    configurations it can generate (M, N multiples of 24)."""
     if not reference_present(ref_root):
         return []
-    return [build_loop_nest(CFG3_SLAB, "cfg3_slab_reference", flavor="fast", threads=16)]
+    return [build_loop_nest(CFG3_SLAB, "cfg3_slab_reference", flavor="fast", threads=16),
+            build_tccg_gett(CFG1, "tccg_gett_cfg1"),
+            build_tccg_gett(CFG2, "tccg_gett_cfg2")]
+
+
+# ---------------------------------------------------------------------------
+# TCCG's own generated GETT (AVX2) for contractions it can generate
+# ---------------------------------------------------------------------------
+STANDIN = os.path.join(_HERE, "hptt_standin")
+
+CFG1 = "C[a,b,i,j] = A[i,m,a] * B[m,j,b]\na=48\nb=48\ni=48\nj=48\nm=48\n"
+CFG2 = "C[a,b,c,d] = A[a,e,b] * B[e,d,c] + C[a,b,c,d]\na=96\nb=96\nc=96\nd=96\ne=16\n"
+
+
+def build_tccg_gett(tccg_text: str, name: str, threads: int = 16, max_impl: int = 8) -> str:
+    """Run TCCG's GETT generator (Gett.genCode, gett.py:961-1421) for an AVX2
+    target with ``threads`` OpenMP threads, write TCCG's MemoryBroker
+    (tccg.py:739-797), and compile every emitted candidate plus a small C glue
+    into oracle/_ref/<name>.so exporting
+      int tccg_gett_count(void); const char* tccg_gett_name(int);
+      void tccg_gett_run(int i, float* A, float* B, float* C, float alpha, float beta);
+    Flags: g++ -O3 -march=x86-64-v3 (AVX2 + FMA, what the emitted intrinsics
+    need) -fopenmp, with oracle/hptt_standin/hptt.h for HPTT."""
+    import io
+    import shutil
+    from contextlib import redirect_stdout
+    os.makedirs(REF_DIR, exist_ok=True)
+    so = os.path.join(REF_DIR, name + ".so")
+    stamp = so + ".sha1"
+    digest = hashlib.sha1((tccg_text + "%d/%d/v2" % (threads, max_impl) +
+                           open(os.path.join(STANDIN, "hptt.h")).read()).encode()).hexdigest()
+    if os.path.exists(so) and os.path.exists(stamp) and open(stamp).read() == digest:
+        return so
+    mods = _ref()
+    t, _ = reference_front_end(tccg_text, "float", threads)
+    work = tempfile.mkdtemp(prefix="tccg_gett_")
+    cwd = os.getcwd()
+    try:
+        os.chdir(work)
+        arch = mods["arch"].avx2("float")
+        g = mods["gett"].Gett(t.A, t.B, t.C, t.alpha, t.beta, threads, arch, "float", max_impl,
+                              0, 0, 1, 0, 0)
+        with redirect_stdout(io.StringIO()):
+            g.genCode()
+            t.genMemoryBroker()
+        names = [v for key in g.implementations for (v, _) in g.implementations[key]]
+        if not names:
+            raise RuntimeError("TCCG generated no GETT candidate for this contraction")
+        # TCCG's spin barriers need every task of a team on its own thread:
+        # run with exactly the generated thread count (TCCG's harness sets
+        # OMP_NUM_THREADS the same way, tccg.py:285-287)
+        glue = ['#include <omp.h>', '#include "memoryBroker.h"', '#include "gett.hpp"',
+                "MemoryBroker memBroker;",
+                "typedef void (*gett_fn)(float*, float*, float*, const float, const float);",
+                "static gett_fn fns[] = {%s};" % ", ".join(names),
+                "static const char* names[] = {%s};" % ", ".join('"%s"' % n for n in names),
+                'extern "C" int tccg_gett_count(void) { return %d; }' % len(names),
+                'extern "C" const char* tccg_gett_name(int i) { return names[i]; }',
+                'extern "C" int tccg_gett_threads(void) { return %d; }' % threads,
+                'extern "C" void tccg_gett_run(int i, float* A, float* B, float* C, float alpha, '
+                "float beta) { omp_set_num_threads(%d); fns[i](A, B, C, alpha, beta); }" % threads]
+        with open("glue.cpp", "w") as f:
+            f.write("\n".join(glue) + "\n")
+        srcs = sorted(x for x in os.listdir(".") if x.startswith("gett") and x.endswith(".cpp"))
+        cmd = [CXX, "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++14",
+               "-I" + STANDIN, "-I" + work, *srcs, "memoryBroker.cpp", "glue.cpp", "-o", so]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("g++ failed on TCCG's GETT:\n" + r.stderr[-3000:])
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(work, ignore_errors=True)
+    with open(stamp, "w") as f:
+        f.write(digest)
+    return so

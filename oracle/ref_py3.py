@@ -15,7 +15,9 @@ The conversion is mechanical and semantic-preserving for the code paths used:
 * every ``/`` becomes ``_py2div(a, b)``, which floors when both operands are
   integers, exactly like Python 2 (``/=`` likewise);
 * ``d.has_key(k)`` becomes ``k in d``; ``d.keys()[i]`` becomes
-  ``list(d.keys())[i]``.
+  ``list(d.keys())[i]``;
+* ``min``/``max`` keep Python 2's cross-type order (numbers before lists,
+  e.g. ``min(8, strategies)`` is 8, tccg/gett.py:792).
 
 Usage: ``load_reference(ref_root)`` returns a dict of the converted modules.
 """
@@ -40,6 +42,24 @@ def _py2div(a, b):
     if isinstance(a, int) and isinstance(b, int):
         return a // b
     return a / b
+
+def _py2order(x):
+    # Python 2 orders numbers before every other type
+    return (0, x) if isinstance(x, (int, float)) else (1, 0)
+
+def _py2min(*args, **kw):
+    try:
+        return min(*args, **kw)
+    except TypeError:
+        items = args[0] if len(args) == 1 else args
+        return sorted(items, key=_py2order)[0]
+
+def _py2max(*args, **kw):
+    try:
+        return max(*args, **kw)
+    except TypeError:
+        items = args[0] if len(args) == 1 else args
+        return sorted(items, key=_py2order)[-1]
 '''
 
 
@@ -126,6 +146,9 @@ class _Py2Semantics(ast.NodeTransformer):
     def visit_Call(self, node):
         self.generic_visit(node)
         f = node.func
+        if isinstance(f, ast.Name) and f.id in ("min", "max"):
+            node.func = ast.Name("_py2" + f.id, ast.Load())
+            return node
         if isinstance(f, ast.Attribute) and f.attr == "has_key" and len(node.args) == 1:
             return ast.copy_location(
                 ast.Compare(left=node.args[0], ops=[ast.In()], comparators=[f.value]), node)

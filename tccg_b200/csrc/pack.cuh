@@ -248,12 +248,13 @@ __device__ __forceinline__ void pack_any(const PackOperand& o, int64_t kt, int64
     pack_tile_kmajor<Tin, LAYOUT>(o, kt, rt);
 }
 
-// grid = (ceil(Kcover/pack_k_tile), ceil(Rcover/32), 2), block = (32, 8)
+// grid = (ktiles * rtiles, 1, 2) with ktiles = ceil(Kcover / pack_k_tile),
+// block = (32, 8); CTA x covers k tile x % ktiles of row tile x / ktiles.
 template <typename Tin, typename Tout, int LAYOUT>
-__global__ void __launch_bounds__(256) pack_kernel(const PackArgs args) {
+__global__ void __launch_bounds__(256) pack_kernel(const PackArgs args, int64_t ktiles) {
   const PackOperand& o = args.op[blockIdx.z];
   if (!o.active) return;
-  pack_any<Tin, Tout, LAYOUT>(o, blockIdx.x, blockIdx.y);
+  pack_any<Tin, Tout, LAYOUT>(o, (int64_t)blockIdx.x % ktiles, (int64_t)blockIdx.x / ktiles);
 }
 
 // Grouped packing: job j (an operand of one contraction) owns the CTAs

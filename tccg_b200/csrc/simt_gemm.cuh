@@ -26,7 +26,7 @@ struct SimtCfg<float> {
   static constexpr int WARPS_M = 2, WARPS_N = 4;
   static constexpr int TMG = 2, TNG = 2;  // 4-wide groups per thread along m / n
   static constexpr int STAGES = 4;
-  static constexpr int EPN = 64;          // epilogue columns per pass
+  static constexpr int EPN = 128;         // epilogue columns per pass (the whole tile)
   static constexpr int PAD = 4;
 };
 
@@ -36,7 +36,7 @@ struct SimtCfg<double> {
   static constexpr int WARPS_M = 2, WARPS_N = 4;
   static constexpr int TMG = 2, TNG = 1;
   static constexpr int STAGES = 4;
-  static constexpr int EPN = 32;
+  static constexpr int EPN = 64;
   static constexpr int PAD = 2;
 };
 
@@ -183,14 +183,26 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     return;
   }
 
-  // Epilogue through shared memory so that each warp stores 32 consecutive m
-  // (C's stride-one index is the first M mode) -> coalesced C traffic.
+  // Epilogue through shared memory. Each thread owns 4 consecutive m of one
+  // column at a time; where those 4 elements of C are contiguous and 16-byte
+  // aligned (C's stride-one index is the first M mode) they move as one
+  // vector, otherwise element by element. All C loads of a pass are issued
+  // before its stores, so a thread keeps several loads in flight.
   constexpr int EPN = Cfg::EPN, LDC = BM + Cfg::PAD;
+  constexpr int QPC = BM / 4;              // m quads per column
+  constexpr int CPI = 256 / QPC;           // columns per iteration
+  constexpr int ITER = EPN / CPI;
   T* Cs = reinterpret_cast<T*>(smem_raw);  // [EPN][LDC]
-  const int m_l = tid % BM;
-  const int64_t m = m0 + m_l;
-  const bool m_ok = m < a.M;
-  const int64_t cmo = m_ok ? a.c_m_off[m] : 0;
+  const int q = tid % QPC, cl = tid / QPC;
+  const int64_t mq = m0 + 4 * q;
+  int64_t cmo[4];
+  bool mok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    mok[i] = mq + i < a.M;
+    cmo[i] = mok[i] ? a.c_m_off[mq + i] : 0;
+  }
+  const bool vec_m = mok[3] && cmo[1] == cmo[0] + 1 && cmo[2] == cmo[0] + 2 && cmo[3] == cmo[0] + 3;
   const T alpha = a.alpha, beta = a.beta;
   for (int p = 0; p < BN / EPN; ++p) {
 #pragma unroll
@@ -202,15 +214,56 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       }
     }
     __syncthreads();
-    if (m_ok) {
-      constexpr int NSTEP = 256 / BM;
-      for (int nl = tid / BM; nl < EPN; nl += NSTEP) {
-        const int64_t n = n0 + p * EPN + nl;
-        if (n < a.N) {
-          T* dst = a.C + cmo + a.c_n_off[n];
-          T v = alpha * Cs[nl * LDC + m_l];
-          if (beta != T(0)) v = fma(beta, *dst, v);
-          *dst = v;
+    if (mok[0]) {
+      constexpr int CH = sizeof(T) == 8 ? 4 : 8;  // columns whose C loads are in flight together
+#pragma unroll 1
+      for (int it0 = 0; it0 < ITER; it0 += CH) {
+        int64_t coff[CH];
+        bool nok[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int64_t n = n0 + p * EPN + (it0 + u) * CPI + cl;
+          nok[u] = (it0 + u < ITER) && n < a.N;
+          coff[u] = nok[u] ? a.c_n_off[n] : 0;
+        }
+        T old[CH][4];
+        if (beta != T(0)) {
+#pragma unroll
+          for (int u = 0; u < CH; ++u) {
+            if (!nok[u]) continue;
+            const T* d = a.C + cmo[0] + coff[u];
+            if (vec_m && (reinterpret_cast<uintptr_t>(d) % (4 * sizeof(T))) == 0) {
+              const Vec4<T> v = lds4<T>(d);  // 16/32-byte vector load
+              old[u][0] = v.v[0]; old[u][1] = v.v[1]; old[u][2] = v.v[2]; old[u][3] = v.v[3];
+            } else {
+#pragma unroll
+              for (int i = 0; i < 4; ++i) old[u][i] = mok[i] ? a.C[cmo[i] + coff[u]] : T(0);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          if (!nok[u]) continue;
+          const int nl = (it0 + u) * CPI + cl;
+          T v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            v[i] = alpha * Cs[nl * LDC + 4 * q + i];
+            if (beta != T(0)) v[i] = fma(beta, old[u][i], v[i]);
+          }
+          T* d = a.C + cmo[0] + coff[u];
+          if (vec_m && (reinterpret_cast<uintptr_t>(d) % (4 * sizeof(T))) == 0) {
+            if constexpr (sizeof(T) == 4) {
+              *reinterpret_cast<float4*>(d) = make_float4(v[0], v[1], v[2], v[3]);
+            } else {
+              reinterpret_cast<double2*>(d)[0] = make_double2(v[0], v[1]);
+              reinterpret_cast<double2*>(d)[1] = make_double2(v[2], v[3]);
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (mok[i]) a.C[cmo[i] + coff[u]] = v[i];
+          }
         }
       }
     }

@@ -451,12 +451,14 @@ static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* 
 
 template <typename Tin, typename Tout, int LAYOUT>
 static int launch_pack(const PackArgs& pa, cudaStream_t s) {
-  int64_t kx = std::max(pa.op[0].Kcover, pa.op[1].Kcover);
-  int64_t ry = std::max(pa.op[0].Rcover, pa.op[1].Rcover);
-  dim3 grid((unsigned)cdiv(kx, pack_k_tile<LAYOUT>()), (unsigned)cdiv(ry, 32), 2);
-  if (grid.y > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "operand has too many rows (%lld)", (long long)ry);
+  const int64_t kx = std::max(pa.op[0].Kcover, pa.op[1].Kcover);
+  const int64_t ry = std::max(pa.op[0].Rcover, pa.op[1].Rcover);
+  const int64_t ktiles = cdiv(kx, pack_k_tile<LAYOUT>());
+  const int64_t ctas = ktiles * cdiv(ry, 32);
+  if (ctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "operand too large to pack (%lld tiles)", (long long)ctas);
+  dim3 grid((unsigned)ctas, 1, 2);
   mark(0, 0, s);
-  pack_kernel<Tin, Tout, LAYOUT><<<grid, dim3(32, 8), 0, s>>>(pa);
+  pack_kernel<Tin, Tout, LAYOUT><<<grid, dim3(32, 8), 0, s>>>(pa, ktiles);
   mark(0, 1, s);
   return launch_check("pack");
 }
