@@ -294,7 +294,7 @@ def run_ours(args, world, rank, local):
     B = torch.randn(nB, generator=g, device=dev, dtype=torch.float32)
     C = torch.empty(nC, device=dev, dtype=torch.float32)
 
-    x3 = Compiled(con, "bf16x3", Tuning(raster=args.raster, max_ctas=args.max_ctas))
+    x3 = Compiled(con, "bf16x3", Tuning(raster=args.raster, max_ctas=args.max_ctas, pair=args.pair))
     ws = x3.workspace(dev)
 
     # ---- headline: split-BF16x3, device-resident -------------------------
@@ -651,6 +651,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--raster", type=int, default=0)
     ap.add_argument("--max-ctas", type=int, default=0)
+    ap.add_argument("--pair", type=int, default=0,
+                    help="1 = CTA-pair tensor-core kernel (cta_group::2, 256-row tiles)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-errors", action="store_true")

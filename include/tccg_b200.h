@@ -97,11 +97,14 @@ typedef struct tccg_desc {
 /* Kernel choices the autotuner searches over; zero-initialised = defaults. */
 typedef struct tccg_tuning {
   int32_t method;      /* TCCG_METHOD_* */
-  int32_t variant;     /* kernel tile variant (0 = default; see tccg_plan_describe) */
+  int32_t variant;     /* BF16X3: k-blocks (of 32) per TMEM accumulation chunk (0 = 16);
+                          BF16/BF16X3: < 0 selects the CUDA-core kernel (operands rounded
+                          to bf16 for BF16, FP32 FFMA) for bandwidth-bound shapes */
   int32_t ksplit;      /* k-split factor for the SIMT kernels (0/1 = none) */
   int32_t raster;      /* tile-raster group size of the persistent tcgen05 kernel (0 = default) */
   int32_t max_ctas;    /* persistent grid size cap (0 = one CTA per SM) */
-  int32_t reserved[3];
+  int32_t pair;        /* tensor-core precisions: 1 = CTA-pair kernel (cta_group::2, 256-row tiles) */
+  int32_t reserved[2];
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

@@ -61,7 +61,8 @@ class Desc(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("variant", ctypes.c_int32),
                 ("ksplit", ctypes.c_int32), ("raster", ctypes.c_int32),
-                ("max_ctas", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("max_ctas", ctypes.c_int32), ("pair", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
 
 _lib = None

@@ -111,9 +111,11 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
         else:
             rasters = [8, 4, 16]
             chunks = [16, 32, 8] if precision == "bf16x3" else [0]
-            for r in rasters:
-                for c in chunks:
-                    out.append(Tuning(method=method, raster=r, variant=c))
+            tc = [Tuning(method=method, raster=r, variant=c) for r in rasters for c in chunks]
+            # a short K makes the contraction bandwidth-bound: the CUDA-core
+            # kernel (variant < 0) streams C faster than the tensor-core epilogue
+            simt = [Tuning(method=method, variant=-1)]
+            out += (simt + tc) if K <= 128 else (tc + simt)
     return out
 
 

@@ -18,6 +18,7 @@ enum PackLayout : int {
   PACK_MN = 0,        // dst[k * ld + r], rows padded to Rcover, k padded to Kcover (zeros)
   PACK_K_BF16 = 1,    // dst[r * ld + k], bf16, k < Kcover (zeros beyond K)
   PACK_K_BF16X3 = 2,  // dst[r * ld + (k/32)*64 + k%32] = hi, +32 = lo (bf16)
+  PACK_MN_BF16 = 3,   // as PACK_MN, each value rounded to bf16 (BF16 semantics on CUDA cores)
 };
 
 struct PackOperand {
@@ -86,12 +87,17 @@ __device__ __forceinline__ void pack_tile(const PackOperand& o, int64_t kt, int6
   }
   __syncthreads();
   Tout* dst = static_cast<Tout*>(o.dst);
-  if constexpr (LAYOUT == PACK_MN) {
+  if constexpr (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16) {
     const int64_t r = r0 + tx;
 #pragma unroll
     for (int i = ty; i < 32; i += 8) {
       const int64_t k = k0 + i;
-      if (k < o.Kcover && r < o.Rcover) dst[k * o.ld + r] = static_cast<Tout>(tile[i][tx]);
+      if (k < o.Kcover && r < o.Rcover) {
+        if constexpr (LAYOUT == PACK_MN_BF16)
+          dst[k * o.ld + r] = static_cast<Tout>(__bfloat162float(__float2bfloat16_rn((float)tile[i][tx])));
+        else
+          dst[k * o.ld + r] = static_cast<Tout>(tile[i][tx]);
+      }
     }
   } else {
     // K-major bf16 rows: thread t packs 4 consecutive k of row t/8 and writes
@@ -147,7 +153,7 @@ constexpr int PACK_KT_WIDE = 128;
 
 template <int LAYOUT>
 __host__ __device__ constexpr int pack_k_tile() {
-  return LAYOUT == PACK_MN ? 32 : PACK_KT_WIDE;
+  return (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16) ? 32 : PACK_KT_WIDE;
 }
 
 template <typename Tin, int LAYOUT>
@@ -242,7 +248,7 @@ __device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t k
 
 template <typename Tin, typename Tout, int LAYOUT>
 __device__ __forceinline__ void pack_any(const PackOperand& o, int64_t kt, int64_t rt) {
-  if constexpr (LAYOUT == PACK_MN)
+  if constexpr (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16)
     pack_tile<Tin, Tout, LAYOUT>(o, kt, rt);
   else
     pack_tile_kmajor<Tin, LAYOUT>(o, kt, rt);

@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "pack.cuh"
 #include "simt_gemm.cuh"
+#include "tc2_gemm.cuh"
 #include "tc_gemm.cuh"
 #include "transpose.cuh"
 
@@ -78,6 +79,14 @@ struct tccg_plan {
   char describe[512] = "";
 };
 
+// The CUDA-core (SIMT) kernels run FP32 and FP64, and -- when the tuning asks
+// for it with variant < 0 -- the BF16 precisions too (operands rounded to bf16
+// by the pack for TCCG_PREC_BF16, FP32 FFMA accumulation), which is the faster
+// choice for bandwidth-bound contractions with a short K.
+static bool simt_path(const tccg_plan* p) {
+  return p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64 || p->tune.variant < 0;
+}
+
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 static int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 static int64_t cdiv(int64_t x, int64_t a) { return (x + a - 1) / a; }
@@ -133,6 +142,7 @@ static void plan_free(tccg_plan* p) {
 }
 
 static int plan_layout(tccg_plan* p);
+static int pair_clusters(bool x3, int* clusters);
 
 extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t precision,
                                 const tccg_tuning* tuning, tccg_plan** out) {
@@ -227,7 +237,7 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
 static int plan_layout(tccg_plan* p) {
   size_t ws = 0;
   const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
-  if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) {
+  if (simt_path(p)) {
     const bool dbl = p->prec == TCCG_PREC_FP64;
     const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
     const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
@@ -250,12 +260,13 @@ static int plan_layout(tccg_plan* p) {
       p->off_part = ws;
       ws = align_up(ws + (size_t)p->ksplit * p->Np * p->Mp * es, 256);
     }
+    static const char* pn[] = {"fp32", "fp64", "bf16", "bf16x3"};
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=simt_gett<%s> tile=%dx%dx%d M=%lld N=%lld K=%lld "
-             "ksplit=%d pack=MN(read_k_fast a=%d b=%d)",
-             ttgt ? "TTGT" : "GETT", dbl ? "fp64" : "fp32", dbl ? "f64" : "f32", BM, BN, BK,
-             (long long)p->M, (long long)p->N, (long long)p->K, p->ksplit, p->read_k_fast_a,
-             p->read_k_fast_b);
+             "ksplit=%d pack=MN%s(read_k_fast a=%d b=%d)",
+             ttgt ? "TTGT" : "GETT", pn[p->prec], dbl ? "f64" : "f32", BM, BN, BK,
+             (long long)p->M, (long long)p->N, (long long)p->K, p->ksplit,
+             p->prec == TCCG_PREC_BF16 ? " bf16-rounded" : "", p->read_k_fast_a, p->read_k_fast_b);
   } else {
     const bool x3 = p->prec == TCCG_PREC_BF16X3;
     if (x3) {
@@ -269,23 +280,36 @@ static int plan_layout(tccg_plan* p) {
     // in k-blocks of 32); BF16 one chunk per tile
     p->chunk_kb = x3 ? (p->tune.variant > 0 ? p->tune.variant : 16) : p->num_kb;
     if (p->chunk_kb < 1) p->chunk_kb = 1;
-    p->bn = x3 ? TcCfgT<TC_BF16X3>::BN : TcCfgT<TC_BF16>::BN;
-    p->tiles_m = (int32_t)cdiv(p->M, 128);
+    const bool pair = p->tune.pair != 0;
+    if (pair)
+      p->bn = x3 ? Tc2Cfg<TC_BF16X3>::BN : Tc2Cfg<TC_BF16>::BN;
+    else
+      p->bn = x3 ? TcCfgT<TC_BF16X3>::BN : TcCfgT<TC_BF16>::BN;
+    p->tiles_m = (int32_t)cdiv(p->M, pair ? 256 : 128);
     p->tiles_n = (int32_t)cdiv(p->N, p->bn);
     p->raster = p->tune.raster > 0 ? p->tune.raster : 8;
     const int64_t tiles = (int64_t)p->tiles_m * p->tiles_n;
     if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
     int ctas = p->tune.max_ctas > 0 ? std::min(p->tune.max_ctas, p->num_sms) : p->num_sms;
-    p->grid = (int32_t)std::min<int64_t>(tiles, ctas);
+    if (pair) {  // clusters of two CTAs, one pair tile per cluster at a time
+      int resident = 0;
+      int rc = pair_clusters(x3, &resident);
+      if (rc) return rc;
+      const int clusters = std::max(1, std::min(ctas / 2, resident));
+      p->grid = 2 * (int32_t)std::min<int64_t>(tiles, clusters);
+    } else
+      p->grid = (int32_t)std::min<int64_t>(tiles, ctas);
     p->off_a = 0;
     ws = align_up((size_t)(p->M * p->Kc) * 2, 256);
     p->off_b = ws;
     ws = align_up(ws + (size_t)(p->N * p->Kc) * 2, 256);
     snprintf(p->describe, sizeof(p->describe),
-             "method=%s prec=%s kernel=gett_tc<%s> tile=128x%d stages=%d M=%lld N=%lld K=%lld "
+             "method=%s prec=%s kernel=gett_tc%s<%s> tile=%dx%d stages=%d M=%lld N=%lld K=%lld "
              "kblocks=%d chunk=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d)",
-             ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", x3 ? "BF16X3" : "BF16", p->bn,
-             x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES, (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->grid,
+             ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", pair ? "2" : "", x3 ? "BF16X3" : "BF16",
+             pair ? 256 : 128, p->bn,
+             pair ? (x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES)
+                  : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES), (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->grid,
              p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b);
   }
   if (ttgt) {
@@ -361,6 +385,10 @@ static void set_attrs() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<float>()));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Tc2Cfg<TC_BF16>::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Tc2Cfg<TC_BF16X3>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3>,
@@ -373,6 +401,23 @@ static int ensure_attrs() {
   std::call_once(g_attr_once, set_attrs);
   if (g_attr_err != cudaSuccess)
     return fail(TCCG_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(g_attr_err));
+  return TCCG_OK;
+}
+
+// Clusters of the CTA-pair kernel that fit on the device at once (an SM whose
+// partner in the GPC is unavailable cannot host half a cluster).
+static int pair_clusters(bool x3, int* clusters) {
+  int rc = ensure_attrs();
+  if (rc) return rc;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(x3 ? Tc2Cfg<TC_BF16X3>::NUM_THREADS : Tc2Cfg<TC_BF16>::NUM_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = x3 ? Tc2Cfg<TC_BF16X3>::SMEM_BYTES : Tc2Cfg<TC_BF16>::SMEM_BYTES;
+  cudaError_t e = x3 ? cudaOccupancyMaxActiveClusters(clusters, gett_tc2_kernel<TC_BF16X3>, &cfg)
+                     : cudaOccupancyMaxActiveClusters(clusters, gett_tc2_kernel<TC_BF16>, &cfg);
+  if (e != cudaSuccess)
+    return fail(TCCG_ERR_CUDA, "cudaOccupancyMaxActiveClusters: %s", cudaGetErrorString(e));
+  if (*clusters < 1) return fail(TCCG_ERR_UNSUPPORTED, "the CTA-pair kernel does not fit on this device");
   return TCCG_OK;
 }
 
@@ -473,7 +518,17 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   PackArgs pa;
   pa.op[0] = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, Ap, p->Mp, p->read_k_fast_a);
   pa.op[1] = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, Bp, p->Np, p->read_k_fast_b);
-  int rc = launch_pack<T, T, PACK_MN>(pa, s);
+  int rc;
+  if constexpr (sizeof(T) == 8) {
+    rc = launch_pack<T, T, PACK_MN>(pa, s);
+  } else {
+    if (p->dtype == TCCG_BF16)
+      rc = launch_pack<__nv_bfloat16, float, PACK_MN>(pa, s);
+    else if (p->prec == TCCG_PREC_BF16)
+      rc = launch_pack<float, float, PACK_MN_BF16>(pa, s);
+    else
+      rc = launch_pack<float, float, PACK_MN>(pa, s);
+  }
   if (rc) return rc;
   SimtArgs<T> a;
   a.Ap = Ap;
@@ -527,9 +582,10 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
     rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s);
   if (rc) return rc;
   CUtensorMap tmA, tmB;
+  const bool pair = p->tune.pair != 0;
   rc = encode_kmajor(&tmA, Ap, p->M, p->Kc, 128);
   if (rc) return rc;
-  rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, p->bn);
+  rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, pair ? p->bn / 2 : p->bn);
   if (rc) return rc;
   TcArgs a;
   a.M = (int32_t)p->M;
@@ -547,7 +603,13 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.beta = beta;
   a.status = p->d_status;
   mark(1, 0, s);
-  if (x3)
+  if (pair && x3)
+    gett_tc2_kernel<TC_BF16X3><<<p->grid, Tc2Cfg<TC_BF16X3>::NUM_THREADS,
+                                 Tc2Cfg<TC_BF16X3>::SMEM_BYTES, s>>>(tmA, tmB, a);
+  else if (pair)
+    gett_tc2_kernel<TC_BF16><<<p->grid, Tc2Cfg<TC_BF16>::NUM_THREADS, Tc2Cfg<TC_BF16>::SMEM_BYTES,
+                               s>>>(tmA, tmB, a);
+  else if (x3)
     gett_tc_kernel<TC_BF16X3><<<p->grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
                                 TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tmA, tmB, a);
   else
@@ -587,7 +649,7 @@ extern "C" int tccg_plan_run(const tccg_plan* p, const void* A, const void* B, v
   const double ga = direct ? alpha : 1.0, gb = direct ? beta : 0.0;
   if (p->prec == TCCG_PREC_FP64)
     rc = run_simt<double>(p, GA, GB, static_cast<double*>(Cdst), cm, cn, ga, gb, w, s);
-  else if (p->prec == TCCG_PREC_FP32)
+  else if (simt_path(p))
     rc = run_simt<float>(p, GA, GB, static_cast<float*>(Cdst), cm, cn, (float)ga, (float)gb, w, s);
   else
     rc = run_tc(p, GA, GB, static_cast<float*>(Cdst), cm, cn, (float)ga, (float)gb, w, s);
@@ -770,7 +832,8 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "all plans of a group need the same precision, dtype and device");
     }
-    if (p->tune.method != TCCG_METHOD_GETT || p->ksplit > 1) {
+    if (p->tune.method != TCCG_METHOD_GETT || p->ksplit > 1 || p->tune.pair ||
+        (simt_path(p) && p->prec != TCCG_PREC_FP32 && p->prec != TCCG_PREC_FP64)) {
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without k-split (plan %d)", i);
     }

@@ -132,6 +132,7 @@ class Tuning:
     raster: int = 0
     max_ctas: int = 0
     variant: int = 0
+    pair: int = 0
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -140,10 +141,12 @@ class Tuning:
         t.raster = int(self.raster)
         t.max_ctas = int(self.max_ctas)
         t.variant = int(self.variant)
+        t.pair = int(self.pair)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d" % (self.method, self.ksplit, self.raster, self.max_ctas, self.variant)
+        return "%s/k%d/r%d/c%d/v%d/p%d" % (self.method, self.ksplit, self.raster, self.max_ctas,
+                                           self.variant, self.pair)
 
 
 class Plan:

@@ -109,3 +109,27 @@ def test_loops_over_gemm(cuda, precision, case):
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
     tol = {"fp32": 1e-6, "bf16x3": 1e-5}[precision]
     assert error_metrics(dC.double().cpu().numpy(), ref)["normwise"] <= tol, log.describe()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16", "bf16x3"])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_cuda_core_variant_of_bf16_precisions(cuda, precision, dtype):
+    """variant < 0: BF16 precisions on the CUDA-core kernel (bandwidth-bound
+    shapes); BF16 keeps its semantics (operands rounded to bf16)."""
+    import torch
+    if precision == "bf16x3" and dtype == "bf16":
+        pytest.skip("BF16 operands go with the bf16 precision only")
+    lc, la, lb, sizes, alpha, beta = CASES[0]
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A = seeded_normal(ln.size_a, 91).astype(np.float32)
+    B = seeded_normal(ln.size_b, 92).astype(np.float32)
+    C = seeded_normal(ln.size_c, 93).astype(np.float32)
+    out, p = run_gpu(con, precision, A, B, C, tuning=Tuning(variant=-1), dtype=dtype)
+    assert "simt_gett<f32>" in p.describe()
+    if precision == "bf16":
+        A = torch.from_numpy(A).bfloat16().float().numpy()
+        B = torch.from_numpy(B).bfloat16().float().numpy()
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    assert error_metrics(out, ref)["normwise"] <= 1e-6
