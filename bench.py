@@ -550,17 +550,19 @@ def run_suite(args):
         flops = con.flop_count()
         byts = (nA + nB) * 4 + nC * 4 * (2 if con.beta else 1)
         res = {"flop": flops, "algorithmic_bytes_fp32": byts}
-        modes = [("fp32", "gett"), ("bf16x3", "gett"), ("bf16", "gett"), ("fp64", "gett")]
+        modes = [("fp32", "gett", 0), ("bf16x3", "gett", 0), ("bf16", "gett", 0), ("fp64", "gett", 0)]
+        if name in ("cfg1", "cfg2"):
+            # short K: the BF16 precisions on the CUDA-core kernel as well
+            modes += [("bf16x3", "gett", -1), ("bf16", "gett", -1)]
         if name == "cfg2":
-            modes += [("fp32", "ttgt"), ("bf16", "ttgt"), ("bf16x3", "ttgt")]
-        for prec, method in modes:
-            if name == "cfg3" and method == "ttgt":
-                continue
+            modes += [("fp32", "ttgt", 0), ("bf16", "ttgt", 0), ("bf16x3", "ttgt", 0)]
+        for prec, method, variant in modes:
             dbl = prec == "fp64"
-            c = Compiled(con, prec, Tuning(method=method))
+            tune = Tuning(method=method, variant=variant)
+            c = Compiled(con, prec, tune)
             Ai, Bi = (A.double(), B.double()) if dbl else (A, B)
             if prec == "bf16" and name == "cfg2":
-                c = Compiled(con, prec, Tuning(method=method), dtype="bf16")
+                c = Compiled(con, prec, tune, dtype="bf16")
                 Ai, Bi = A.bfloat16(), B.bfloat16()
             Cw = C0.double().clone() if dbl else C0.clone()
             ws = c.workspace(dev)
@@ -570,7 +572,7 @@ def run_suite(args):
             c.plan.run(Ai, Bi, Cw, workspace=ws)
             torch.cuda.synchronize()
             e = errs(Cw, C64) if not dbl else errs(Cw, C64)
-            key = "%s_%s" % (prec, method)
+            key = "%s_%s%s" % (prec, method, "_cuda_core" if variant < 0 else "")
             gbps = (byts * (2 if dbl else 1) if prec != "bf16" else byts - (nA + nB) * 2) / (ms * 1e-3) / 1e9
             res[key] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "gbs": gbps,
                         "hbm_frac": gbps / peaks["hbm_gbs"], "normwise_vs_fp64": e,

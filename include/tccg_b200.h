@@ -100,11 +100,15 @@ typedef struct tccg_tuning {
   int32_t variant;     /* BF16X3: k-blocks (of 32) per TMEM accumulation chunk (0 = 16);
                           BF16/BF16X3: < 0 selects the CUDA-core kernel (operands rounded
                           to bf16 for BF16, FP32 FFMA) for bandwidth-bound shapes */
-  int32_t ksplit;      /* k-split factor for the SIMT kernels (0/1 = none) */
+  int32_t ksplit;      /* k-split factor: 0 = automatic (split K over CTAs when the C tiles
+                          cannot fill the GPU), 1 = none, > 1 = that many slices
+                          (the CTA-pair kernel never splits) */
   int32_t raster;      /* tile-raster group size of the persistent tcgen05 kernel (0 = default) */
   int32_t max_ctas;    /* persistent grid size cap (0 = one CTA per SM) */
   int32_t pair;        /* tensor-core precisions: 1 = CTA-pair kernel (cta_group::2, 256-row tiles) */
-  int32_t reserved[2];
+  int32_t direct;      /* CUDA-core kernels: 0 = automatic (no packing pass when K <= 256 and the
+                          operand loads stay coalesced), 1 = always, -1 = never (GETT only) */
+  int32_t reserved[1];
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

@@ -62,7 +62,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("variant", ctypes.c_int32),
                 ("ksplit", ctypes.c_int32), ("raster", ctypes.c_int32),
                 ("max_ctas", ctypes.c_int32), ("pair", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 2)]
+                ("direct", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1)]
 
 
 _lib = None

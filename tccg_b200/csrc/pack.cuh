@@ -31,6 +31,11 @@ struct PackOperand {
   int64_t ld;             // dst leading dimension in elements
   int32_t read_k_fast;    // 1: consecutive threads read consecutive k
   int32_t active;
+  // K-major layouts only: null, or the destination row of tile row r (then
+  // row_off is indexed by the same visit order). Lets the pass walk the rows
+  // along the operand's unit-stride mode when that is not the first mode of
+  // the destination order; each destination row is written whole either way.
+  const int64_t* row_dst;
 };
 
 struct PackArgs {
@@ -205,7 +210,8 @@ __device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t k
   const int rl = t >> 3, kq = (t & 7) * 4;
   const int64_t r = r0 + rl;
   if (r >= o.Rcover) return;
-  __nv_bfloat16* base = static_cast<__nv_bfloat16*>(o.dst) + r * o.ld;
+  const int64_t rd = o.row_dst ? o.row_dst[r] : r;
+  __nv_bfloat16* base = static_cast<__nv_bfloat16*>(o.dst) + rd * o.ld;
 #pragma unroll
   for (int sb = 0; sb < SB; ++sb) {
     const int kl = sb * 32 + kq;

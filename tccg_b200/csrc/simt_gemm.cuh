@@ -1,7 +1,10 @@
 // SIMT GETT kernels: FP32 FFMA and FP64 DFMA on the CUDA cores.
 //
 // Operands come packed MN-major by pack_kernel (Ap[k][Mp], Bp[k][Np], zero
-// padded), so the main loop is a dense 16-byte cp.async pipeline. The
+// padded), so the main loop is a dense 16-byte cp.async pipeline -- or, for
+// bandwidth-bound contractions (short K), straight from the user's tensors
+// through the offset tables with element-wise cp.async ("direct": one read of
+// each operand instead of read + packed write + packed read). The
 // epilogue writes C straight into its own (multi-index) layout through the
 // offset tables: element (m, n) of the GETT view is C[c_m_off[m] + c_n_off[n]].
 // That is GETT's defining property (TCCG's micro-kernel stores into C's
@@ -52,6 +55,17 @@ struct SimtArgs {
   const int64_t* c_n_off;
   T alpha, beta;
   T* partial;  // non-null: write raw sums to partial[z][n][Mp]
+  // direct != 0: no packing pass; the stage loader gathers A[k][m] =
+  // Asrc[a_m_off[m] + a_k_off[k]] and B[k][n] = Bsrc[b_n_off[n] + b_k_off[k]]
+  // element by element (zeros beyond M, N, K)
+  int32_t direct;
+  int64_t K;
+  const T* Asrc;
+  const T* Bsrc;
+  const int64_t* a_m_off;
+  const int64_t* a_k_off;
+  const int64_t* b_n_off;
+  const int64_t* b_k_off;
 };
 
 template <typename T>
@@ -105,10 +119,55 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   int kt_end = kt_begin + a.ktiles_per_split;
   if (kt_end > a.ktiles) kt_end = a.ktiles;
 
+  // direct loads: thread tid always fills column tid % BM of A's stage and
+  // tid % BN of B's (256 is a multiple of both), rows tid / BM + j * 256 / BM
+  static_assert(256 % BM == 0 && 256 % BN == 0, "direct loader layout");
+  const int dcol_a = tid % BM, drow_a = tid / BM;
+  const int dcol_b = tid % BN, drow_b = tid / BN;
+  constexpr int64_t NONE = INT64_MIN;  // offsets may be negative (negative strides)
+  int64_t dm_off = NONE, dn_off = NONE;
+  if (a.direct) {
+    if (m0 + dcol_a < a.M) dm_off = a.a_m_off[m0 + dcol_a];
+    if (n0 + dcol_b < a.N) dn_off = a.b_n_off[n0 + dcol_b];
+  }
+
   auto load_stage = [&](int stage, int kt) {
     T* as = As + (size_t)stage * BK * BM;
     T* bs = Bs + (size_t)stage * BK * BN;
     const int64_t krow = (int64_t)kt * BK;
+    if (a.direct) {
+      // all k offsets first (independent loads), then the copies: an offset
+      // load between two asynchronous copies would serialise them
+      constexpr int JA = BK * BM / 256, JB = BK * BN / 256;
+      int64_t koa[JA], kob[JB];
+#pragma unroll
+      for (int j = 0; j < JA; ++j) {
+        const int64_t k = krow + drow_a + j * (256 / BM);
+        koa[j] = k < a.K ? __ldg(a.a_k_off + k) : NONE;
+      }
+#pragma unroll
+      for (int j = 0; j < JB; ++j) {
+        const int64_t k = krow + drow_b + j * (256 / BN);
+        kob[j] = k < a.K ? __ldg(a.b_k_off + k) : NONE;
+      }
+#pragma unroll
+      for (int j = 0; j < JA; ++j) {
+        T* dst = as + (drow_a + j * (256 / BM)) * BM + dcol_a;
+        if (dm_off != NONE && koa[j] != NONE)
+          cp_async_elem<sizeof(T)>(dst, a.Asrc + dm_off + koa[j]);
+        else
+          *dst = T(0);
+      }
+#pragma unroll
+      for (int j = 0; j < JB; ++j) {
+        T* dst = bs + (drow_b + j * (256 / BN)) * BN + dcol_b;
+        if (dn_off != NONE && kob[j] != NONE)
+          cp_async_elem<sizeof(T)>(dst, a.Bsrc + dn_off + kob[j]);
+        else
+          *dst = T(0);
+      }
+      return;
+    }
 #pragma unroll
     for (int c = tid; c < A_CHUNKS; c += 256) {
       const int row = c / A_ROW_CHUNKS, col = (c % A_ROW_CHUNKS) * VEC;
@@ -133,7 +192,13 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     cp_async_commit();
   }
 
-  const int a_off = wm * (Cfg::TMG * 32) + lm * 4;
+  // A fragment: per group g of 32 m, a thread owns 4 m. FP32: m = 4 lm + i,
+  // one 16-byte load. FP64: two 16-byte loads at m = 2 lm + {0,1} and
+  // 16 + 2 lm + {0,1}, so the 8 lane groups of each load read 128 contiguous
+  // bytes (4 consecutive doubles per lane would put lanes lm and lm + 4 on
+  // the same banks: a 2-way conflict on every A load).
+  constexpr bool PAIRS = sizeof(T) == 8;
+  const int a_off = wm * (Cfg::TMG * 32) + lm * (PAIRS ? 2 : 4);
   const int b_off = wn * (Cfg::TNG * 16) + ln * 4;
   for (int kt = kt_begin; kt < kt_end; ++kt) {
     cp_async_wait<STAGES - 2>();
@@ -151,7 +216,14 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       T av[TM], bv[TN];
 #pragma unroll
       for (int g = 0; g < Cfg::TMG; ++g) {
-        Vec4<T> x = lds4<T>(as + k * BM + a_off + g * 32);
+        Vec4<T> x;
+        if constexpr (PAIRS) {
+          const double2 lo = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32);
+          const double2 hi = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32 + 16);
+          x.v[0] = lo.x; x.v[1] = lo.y; x.v[2] = hi.x; x.v[3] = hi.y;
+        } else {
+          x = lds4<T>(as + k * BM + a_off + g * 32);
+        }
         av[g * 4 + 0] = x.v[0]; av[g * 4 + 1] = x.v[1]; av[g * 4 + 2] = x.v[2]; av[g * 4 + 3] = x.v[3];
       }
 #pragma unroll
@@ -169,7 +241,9 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   __syncthreads();
 
   // thread fragment coordinates (tile-local)
-  auto mloc = [&](int i) { return a_off + (i / 4) * 32 + (i % 4); };
+  auto mloc = [&](int i) {
+    return PAIRS ? a_off + (i / 4) * 32 + ((i % 4) / 2) * 16 + (i % 2) : a_off + (i / 4) * 32 + (i % 4);
+  };
   auto nloc = [&](int j) { return b_off + (j / 4) * 16 + (j % 4); };
 
   if (a.partial != nullptr) {
@@ -282,7 +356,7 @@ template <typename T>
 struct SimtGroupItem {
   SimtArgs<T> args;
   int64_t tile_begin;
-  int32_t tiles_m, pad;
+  int32_t tiles_m, tiles_n;  // tiles of one k-split slice
 };
 
 template <typename T>
@@ -296,7 +370,9 @@ __global__ void __launch_bounds__(256, 2) simt_gett_group_kernel(const SimtGroup
   }
   const SimtGroupItem<T>& it = items[lo];
   const int64_t local = t - it.tile_begin;
-  simt_gett_tile<T>(it.args, (int)(local % it.tiles_m), (int)(local / it.tiles_m), 0);
+  const int64_t mn = (int64_t)it.tiles_m * it.tiles_n;
+  const int64_t rem = local % mn;
+  simt_gett_tile<T>(it.args, (int)(rem % it.tiles_m), (int)(rem / it.tiles_m), (int)(local / mn));
 }
 
 // C = alpha * sum_z partial[z] + beta * C.
@@ -317,6 +393,48 @@ __global__ void __launch_bounds__(256) simt_reduce_kernel(const T* __restrict__ 
     T* dst = C + cmo + c_n_off[n];
     T v = alpha * s;
     if (beta != T(0)) v = fma(beta, *dst, v);
+    *dst = v;
+  }
+}
+
+// Grouped k-split reduction: job j (one contraction with a k-split) owns the
+// CTAs [begin, begin + mblocks * nblocks); CTA (mb, nb) sums the slices of
+// 256 rows over columns [64 nb, 64 nb + 64) in split order.
+template <typename T>
+struct ReduceJob {
+  const T* partial;
+  int64_t Mp, Np, M, N;
+  T* C;
+  const int64_t* c_m_off;
+  const int64_t* c_n_off;
+  T alpha, beta;
+  int64_t begin;
+  int32_t splits, mblocks;
+};
+
+constexpr int REDUCE_NCOLS = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(256) reduce_group_kernel(const ReduceJob<T>* jobs, int n_jobs) {
+  const int64_t t = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].begin <= t) lo = mid; else hi = mid - 1;
+  }
+  const ReduceJob<T>& j = jobs[lo];
+  const int64_t local = t - j.begin;
+  const int64_t m = (local % j.mblocks) * 256 + threadIdx.x;
+  if (m >= j.M) return;
+  const int64_t n0 = (local / j.mblocks) * REDUCE_NCOLS;
+  const int64_t n1 = n0 + REDUCE_NCOLS < j.N ? n0 + REDUCE_NCOLS : j.N;
+  const int64_t cmo = j.c_m_off[m];
+  for (int64_t n = n0; n < n1; ++n) {
+    T s = T(0);
+    for (int z = 0; z < j.splits; ++z) s += j.partial[(size_t)z * j.Np * j.Mp + n * j.Mp + m];
+    T* dst = j.C + cmo + j.c_n_off[n];
+    T v = j.alpha * s;
+    if (j.beta != T(0)) v = fma(j.beta, *dst, v);
     *dst = v;
   }
 }

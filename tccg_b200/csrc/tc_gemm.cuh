@@ -28,6 +28,9 @@
 //              [128*h, 128*h+128) with h = (w-2)/4, sums the chunks, then writes
 //              C[c_m_off[m] + c_n_off[n]] = alpha*acc (+ beta*C) straight into
 //              C's own layout (GETT: no transposition of C).
+// With a k-split (contractions whose C tiles cannot fill the GPU), tile
+// indices run over (split, tile) and each split's epilogue writes raw sums to
+// a workspace slice; simt_reduce_kernel adds the slices in split order.
 // Every mbarrier wait is bounded (TCCG_DEVICE_WAIT_NS); a wait that runs out
 // records an error code in *status and the CTA winds down: in-flight TMA loads
 // and MMAs are waited for (bounded) and TMEM is released before returning.
@@ -69,6 +72,11 @@ struct TcArgs {
   const int64_t* c_n_off;
   float alpha, beta;
   int32_t* status;
+  // k-split: the tiles of split z cover k-blocks [z*kb_per_split, ...) and
+  // write raw FP32 sums to partial[z][n][M]; a reduction kernel applies
+  // alpha/beta. ksplit == 1 writes C directly.
+  int32_t ksplit, kb_per_split;
+  float* partial;
 };
 
 // Grouped launch: one entry per contraction, in device memory. The tensor maps
@@ -101,13 +109,23 @@ __device__ __forceinline__ void tile_coords(int tile, const TcArgs& a, int& tm, 
   tn = r / gm;
 }
 
-// Resolves a global tile index to (item arguments, tensor maps, tile coords).
+// Resolves a global tile index to (item arguments, tensor maps, tile coords,
+// k-split slice). Splits are the outermost tile dimension.
 struct TileRef {
   const TcArgs* a;
   const CUtensorMap* tA;
   const CUtensorMap* tB;
   int tm, tn;
+  int z, kb_begin, kb_end;
 };
+
+__device__ __forceinline__ void split_coords(int local, const TcArgs& a, TileRef& r) {
+  const int mn = a.tiles_m * a.tiles_n;
+  r.z = local / mn;
+  tile_coords(local - r.z * mn, a, r.tm, r.tn);
+  r.kb_begin = r.z * a.kb_per_split;
+  r.kb_end = r.kb_begin + a.kb_per_split < a.num_kb ? r.kb_begin + a.kb_per_split : a.num_kb;
+}
 
 template <bool GROUPED>
 __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA,
@@ -124,12 +142,12 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
     r.a = &it.args;
     r.tA = &it.tmA;
     r.tB = &it.tmB;
-    tile_coords(tile - (int)it.tile_begin, it.args, r.tm, r.tn);
+    split_coords(tile - (int)it.tile_begin, it.args, r);
   } else {
     r.a = a1;
     r.tA = tmA;
     r.tB = tmB;
-    tile_coords(tile, *a1, r.tm, r.tn);
+    split_coords(tile, *a1, r);
   }
   return r;
 }
@@ -153,7 +171,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int num_tiles = GROUPED ? g.total_tiles : a1->tiles_m * a1->tiles_n;
+  const int num_tiles = GROUPED ? g.total_tiles : a1->tiles_m * a1->tiles_n * a1->ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -186,8 +204,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     bool ok = true;
     for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
-      const int nkb = t.a->num_kb;
-      for (int kb = 0; kb < nkb; ++kb) {
+      for (int kb = t.kb_begin; kb < t.kb_end; ++kb) {
         if (!mbar_wait(&empty[stage], phase ^ 1)) {
           record_error(status, 1);
           ok = false;
@@ -217,8 +234,8 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     bool ok = true, issued_any = false;
     for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
-      const int nkb = t.a->num_kb, K = t.a->K, ckb = t.a->chunk_kb;
-      for (int kb0 = 0; kb0 < nkb && ok; kb0 += ckb) {
+      const int nkb = t.kb_end, K = t.a->K, ckb = t.a->chunk_kb;
+      for (int kb0 = t.kb_begin; kb0 < nkb && ok; kb0 += ckb) {
         if (!mbar_wait(&acce[acc], acc_phase ^ 1)) {
           record_error(status, 2);
           ok = false;
@@ -294,6 +311,8 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       const int64_t n0 = (int64_t)t.tn * Cfg::BN + h * HC;
       const int64_t nlim = a.N - n0;
       const float alpha = a.alpha, beta = a.beta;
+      // k-split slice: raw sums to partial[z][n][M] (coalesced along m)
+      float* part = a.partial ? a.partial + (size_t)t.z * a.N * a.M + m : nullptr;
       if constexpr (MODE == TC_BF16) {
         // one accumulator per tile: stream TMEM -> C
         if (!mbar_wait(&accf[acc], acc_phase)) {
@@ -312,7 +331,11 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce[acc]);
           }
-          if (m_ok) {
+          if (m_ok && part) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (cc + j < nlim) part[(size_t)(n0 + cc + j) * a.M] = __uint_as_float(r[j]);
+          } else if (m_ok) {
             if (beta != 0.0f) {
               float old[32];
 #pragma unroll
@@ -337,7 +360,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
         }
       } else {
         // chunked accumulation: sum the chunk accumulators in registers (RN adds)
-        const int nchunks = (a.num_kb + a.chunk_kb - 1) / a.chunk_kb;
+        const int nchunks = (t.kb_end - t.kb_begin + a.chunk_kb - 1) / a.chunk_kb;
         float sum[HC];
         for (int ch = 0; ch < nchunks; ++ch) {
           if (!mbar_wait(&accf[acc], acc_phase)) {
@@ -366,7 +389,11 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
           }
         }
         if (!ok) break;
-        if (m_ok) {
+        if (m_ok && part) {
+#pragma unroll
+          for (int j = 0; j < HC; ++j)
+            if (j < nlim) part[(size_t)(n0 + j) * a.M] = sum[j];
+        } else if (m_ok) {
           if (beta != 0.0f) {
 #pragma unroll
             for (int cc = 0; cc < HC; cc += 8) {

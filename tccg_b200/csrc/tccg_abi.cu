@@ -65,6 +65,12 @@ struct tccg_plan {
   int64_t* t_c_n = nullptr;
   int64_t* t_id_m = nullptr;  // TTGT: identity tables of the contiguous C' = [M][N]
   int64_t* t_id_n = nullptr;
+  // tensor-core packs: rows visited along the operand's unit-stride mode
+  // (source offsets and destination rows in that order), or null
+  int64_t* t_a_vsrc = nullptr;
+  int64_t* t_a_vdst = nullptr;
+  int64_t* t_b_vsrc = nullptr;
+  int64_t* t_b_vdst = nullptr;
   int32_t* d_status = nullptr;
   int32_t read_k_fast_a = 0, read_k_fast_b = 0;
   bool c_is_mn_dense = false;  // C is already the column-major [M-modes][N-modes] matrix
@@ -74,6 +80,8 @@ struct tccg_plan {
   // tcgen05 geometry
   int64_t Kc = 0;
   int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0, chunk_kb = 1, bn = 256;
+  int32_t kb_per_split = 0;
+  bool direct = false;  // CUDA-core kernel gathers operands without a packing pass
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
   char describe[512] = "";
@@ -87,9 +95,51 @@ static bool simt_path(const tccg_plan* p) {
   return p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64 || p->tune.variant < 0;
 }
 
+// First mode of extent > 1 has unit stride (or no such mode).
+static bool unit_first(int n, const int64_t* ext, const int64_t* str) {
+  for (int i = 0; i < n; ++i)
+    if (ext[i] > 1) return str[i] == 1;
+  return true;
+}
+
+// The CUDA-core kernel reads the operands in place (no packing pass) when the
+// tuning asks for it, or -- automatically -- for a short K (bandwidth-bound:
+// the pack would triple the operand traffic) as long as each operand's
+// gather runs along a unit-stride mode or the operand is small enough to stay
+// cached. Not for TTGT (whose point is the transposition) and not where the
+// pack converts (bf16 operands, BF16 rounding).
+static bool choose_direct(const tccg_plan* p) {
+  if (!simt_path(p) || p->tune.method != TCCG_METHOD_GETT || p->tune.direct < 0) return false;
+  if (p->dtype == TCCG_BF16 || p->prec == TCCG_PREC_BF16) return false;
+  if (p->tune.direct > 0) return true;
+  if (p->K > 256) return false;
+  const int64_t es = p->prec == TCCG_PREC_FP64 ? 8 : 4, small = 4 << 20;
+  const tccg_desc& d = p->d;
+  const bool a_ok = unit_first(d.nm, d.m_ext, d.a_m_stride) || p->M * p->K * es <= small;
+  const bool b_ok = unit_first(d.nn, d.n_ext, d.b_n_stride) || p->N * p->K * es <= small;
+  return a_ok && b_ok;
+}
+
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 static int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 static int64_t cdiv(int64_t x, int64_t a) { return (x + a - 1) / a; }
+
+// K slices for `tiles` C tiles over `kblocks` k-blocks when `slots` CTAs run
+// at once: the requested count, or (requested == 0) as many slices as fill
+// the idle slots, each at least `min_kb` k-blocks long. Returns the k-blocks
+// per slice; *splits gets the slice count (no empty slices).
+static int64_t choose_ksplit(int32_t requested, int64_t tiles, int64_t kblocks, int64_t slots,
+                             int64_t min_kb, int32_t* splits) {
+  int64_t ks = 1;
+  if (requested > 1)
+    ks = requested;
+  else if (requested == 0 && 2 * tiles <= slots)
+    ks = std::min<int64_t>(slots / tiles, kblocks / min_kb);
+  ks = std::max<int64_t>(1, std::min<int64_t>(ks, kblocks));
+  const int64_t per = cdiv(kblocks, ks);
+  *splits = (int32_t)cdiv(kblocks, per);
+  return per;
+}
 
 // offsets[l] = sum_i idx_i(l) * stride_i, l the linear index over the modes
 // (first mode fastest).
@@ -134,7 +184,8 @@ static int32_t pick_read_k_fast(int nr, const int64_t* rext, const int64_t* rstr
 
 static void plan_free(tccg_plan* p) {
   if (!p) return;
-  int64_t* ts[] = {p->t_a_m, p->t_a_k, p->t_b_n, p->t_b_k, p->t_c_m, p->t_c_n, p->t_id_m, p->t_id_n};
+  int64_t* ts[] = {p->t_a_m, p->t_a_k, p->t_b_n, p->t_b_k, p->t_c_m, p->t_c_n, p->t_id_m, p->t_id_n,
+                   p->t_a_vsrc, p->t_a_vdst, p->t_b_vsrc, p->t_b_vdst};
   for (auto t : ts)
     if (t) cudaFree(t);
   if (p->d_status) cudaFree(p->d_status);
@@ -143,6 +194,50 @@ static void plan_free(tccg_plan* p) {
 
 static int plan_layout(tccg_plan* p);
 static int pair_clusters(bool x3, int* clusters);
+
+// For a K-major pack whose rows are read one per lane: if a later row mode
+// has a smaller stride than the first (non-unit) mode, visit the rows with
+// that mode fastest. vsrc[v] = source offset, vdst[v] = destination row of
+// visit index v. Returns false (tables untouched) when no reorder helps.
+static bool build_visit(int n, const int64_t* ext, const int64_t* str, std::vector<int64_t>& vsrc,
+                        std::vector<int64_t>& vdst) {
+  int first = -1, best = -1;
+  for (int i = 0; i < n; ++i) {
+    if (ext[i] <= 1) continue;
+    if (first < 0) first = i;
+    if (best < 0 || std::llabs(str[i]) < std::llabs(str[best])) best = i;
+  }
+  if (first < 0 || best == first || std::llabs(str[best]) >= std::llabs(str[first])) return false;
+  std::vector<int> order{best};
+  for (int i = 0; i < n; ++i)
+    if (i != best) order.push_back(i);
+  std::vector<int64_t> place(n);
+  int64_t total = 1;
+  for (int i = 0; i < n; ++i) {
+    place[i] = total;
+    total *= ext[i];
+  }
+  vsrc.assign((size_t)total, 0);
+  vdst.assign((size_t)total, 0);
+  std::vector<int64_t> idx(n, 0);
+  int64_t so = 0, dr = 0;
+  for (int64_t v = 0; v < total; ++v) {
+    vsrc[(size_t)v] = so;
+    vdst[(size_t)v] = dr;
+    for (int j = 0; j < n; ++j) {  // odometer in visit order
+      const int i = order[j];
+      if (++idx[i] < ext[i]) {
+        so += str[i];
+        dr += place[i];
+        break;
+      }
+      so -= (ext[i] - 1) * str[i];
+      dr -= (ext[i] - 1) * place[i];
+      idx[i] = 0;
+    }
+  }
+  return true;
+}
 
 extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t precision,
                                 const tccg_tuning* tuning, tccg_plan** out) {
@@ -225,6 +320,17 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   }
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
+  if (!rc && !simt_path(p)) {  // tensor-core packs: rows along the unit-stride mode
+    std::vector<int64_t> vs, vd;
+    if (!p->read_k_fast_a && build_visit(d.nm, d.m_ext, d.a_m_stride, vs, vd)) {
+      rc = upload(vs, &p->t_a_vsrc);
+      if (!rc) rc = upload(vd, &p->t_a_vdst);
+    }
+    if (!rc && !p->read_k_fast_b && build_visit(d.nn, d.n_ext, d.b_n_stride, vs, vd)) {
+      rc = upload(vs, &p->t_b_vsrc);
+      if (!rc) rc = upload(vd, &p->t_b_vdst);
+    }
+  }
   if (!rc) rc = plan_layout(p);
   if (rc) {
     plan_free(p);
@@ -247,15 +353,17 @@ static int plan_layout(tccg_plan* p) {
     p->Np = round_up(p->N, BN);
     p->Kp = round_up(p->K, BK);
     p->ktiles = (int32_t)(p->Kp / BK);
-    int ks = p->tune.ksplit > 1 ? p->tune.ksplit : 1;
-    if (ks > p->ktiles) ks = p->ktiles;
-    p->ktiles_per_split = (int32_t)cdiv(p->ktiles, ks);
-    ks = (int32_t)cdiv(p->ktiles, p->ktiles_per_split);  // no empty splits
-    p->ksplit = ks;
+    const int64_t tiles = (p->Mp / BM) * (p->Np / BN);
+    // two CTAs per SM; a slice is at least 8 k-tiles
+    p->ktiles_per_split = (int32_t)choose_ksplit(p->tune.ksplit, tiles, p->ktiles,
+                                                 2 * (int64_t)p->num_sms, 8, &p->ksplit);
+    p->direct = choose_direct(p);
     p->off_a = 0;
-    ws = align_up((size_t)(p->Kp * p->Mp) * es, 256);
-    p->off_b = ws;
-    ws = align_up(ws + (size_t)(p->Kp * p->Np) * es, 256);
+    if (!p->direct) {
+      ws = align_up((size_t)(p->Kp * p->Mp) * es, 256);
+      p->off_b = ws;
+      ws = align_up(ws + (size_t)(p->Kp * p->Np) * es, 256);
+    }
     if (p->ksplit > 1) {
       p->off_part = ws;
       ws = align_up(ws + (size_t)p->ksplit * p->Np * p->Mp * es, 256);
@@ -263,10 +371,11 @@ static int plan_layout(tccg_plan* p) {
     static const char* pn[] = {"fp32", "fp64", "bf16", "bf16x3"};
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=simt_gett<%s> tile=%dx%dx%d M=%lld N=%lld K=%lld "
-             "ksplit=%d pack=MN%s(read_k_fast a=%d b=%d)",
+             "ksplit=%d pack=%s%s(read_k_fast a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", pn[p->prec], dbl ? "f64" : "f32", BM, BN, BK,
              (long long)p->M, (long long)p->N, (long long)p->K, p->ksplit,
-             p->prec == TCCG_PREC_BF16 ? " bf16-rounded" : "", p->read_k_fast_a, p->read_k_fast_b);
+             p->direct ? "none" : "MN", p->prec == TCCG_PREC_BF16 ? " bf16-rounded" : "",
+             p->read_k_fast_a, p->read_k_fast_b);
   } else {
     const bool x3 = p->prec == TCCG_PREC_BF16X3;
     if (x3) {
@@ -288,9 +397,14 @@ static int plan_layout(tccg_plan* p) {
     p->tiles_m = (int32_t)cdiv(p->M, pair ? 256 : 128);
     p->tiles_n = (int32_t)cdiv(p->N, p->bn);
     p->raster = p->tune.raster > 0 ? p->tune.raster : 8;
-    const int64_t tiles = (int64_t)p->tiles_m * p->tiles_n;
-    if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
+    int64_t tiles = (int64_t)p->tiles_m * p->tiles_n;
     int ctas = p->tune.max_ctas > 0 ? std::min(p->tune.max_ctas, p->num_sms) : p->num_sms;
+    // one CTA per SM; a slice is at least one accumulation chunk (BF16X3) or
+    // 512 k (BF16). The CTA-pair kernel does not split.
+    p->kb_per_split = (int32_t)choose_ksplit(pair ? 1 : p->tune.ksplit, tiles, p->num_kb, ctas,
+                                             x3 ? p->chunk_kb : 8, &p->ksplit);
+    tiles *= p->ksplit;
+    if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
     if (pair) {  // clusters of two CTAs, one pair tile per cluster at a time
       int resident = 0;
       int rc = pair_clusters(x3, &resident);
@@ -303,14 +417,20 @@ static int plan_layout(tccg_plan* p) {
     ws = align_up((size_t)(p->M * p->Kc) * 2, 256);
     p->off_b = ws;
     ws = align_up(ws + (size_t)(p->N * p->Kc) * 2, 256);
+    if (p->ksplit > 1) {  // FP32 slices [split][N][M]
+      p->off_part = ws;
+      ws = align_up(ws + (size_t)p->ksplit * p->N * p->M * 4, 256);
+    }
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=gett_tc%s<%s> tile=%dx%d stages=%d M=%lld N=%lld K=%lld "
-             "kblocks=%d chunk=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d)",
+             "kblocks=%d chunk=%d ksplit=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
+             "visit a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", pair ? "2" : "", x3 ? "BF16X3" : "BF16",
              pair ? 256 : 128, p->bn,
              pair ? (x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES)
-                  : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES), (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->grid,
-             p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b);
+                  : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES), (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit, p->grid,
+             p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
+             p->t_a_vsrc ? 1 : 0, p->t_b_vsrc ? 1 : 0);
   }
   if (ttgt) {
     // contiguous C' = [M][N] (column-major) in the workspace, then C' -> C
@@ -491,6 +611,16 @@ static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* 
   o.ld = ld;
   o.read_k_fast = kfast;
   o.active = 1;
+  o.row_dst = nullptr;
+  return o;
+}
+
+// Row visit order of a K-major pack (tables built at plan creation).
+static PackOperand with_visit(PackOperand o, const int64_t* vsrc, const int64_t* vdst) {
+  if (vsrc && vdst) {
+    o.row_off = vsrc;
+    o.row_dst = vdst;
+  }
   return o;
 }
 
@@ -509,6 +639,18 @@ static int launch_pack(const PackArgs& pa, cudaStream_t s) {
 }
 
 template <typename T>
+static void set_direct(SimtArgs<T>& a, const tccg_plan* p, const void* GA, const void* GB) {
+  a.direct = p->direct ? 1 : 0;
+  a.K = p->K;
+  a.Asrc = static_cast<const T*>(GA);
+  a.Bsrc = static_cast<const T*>(GB);
+  a.a_m_off = p->t_a_m;
+  a.a_k_off = p->t_a_k;
+  a.b_n_off = p->t_b_n;
+  a.b_k_off = p->t_b_k;
+}
+
+template <typename T>
 static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
                     const int64_t* c_m, const int64_t* c_n, T alpha, T beta, char* ws,
                     cudaStream_t s) {
@@ -518,8 +660,10 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   PackArgs pa;
   pa.op[0] = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, Ap, p->Mp, p->read_k_fast_a);
   pa.op[1] = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, Bp, p->Np, p->read_k_fast_b);
-  int rc;
-  if constexpr (sizeof(T) == 8) {
+  int rc = TCCG_OK;
+  if (p->direct) {
+    // no packing pass
+  } else if constexpr (sizeof(T) == 8) {
     rc = launch_pack<T, T, PACK_MN>(pa, s);
   } else {
     if (p->dtype == TCCG_BF16)
@@ -545,6 +689,7 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   a.alpha = alpha;
   a.beta = beta;
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(ws + p->off_part) : nullptr;
+  set_direct(a, p, GA, GB);
   dim3 grid((unsigned)(p->Mp / Cfg::BM), (unsigned)(p->Np / Cfg::BN), (unsigned)p->ksplit);
   if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
   mark(1, 0, s);
@@ -571,8 +716,10 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   void* Bp = ws + p->off_b;
   PackArgs pa;
   const int64_t kcover = x3 ? round_up(p->K, 32) : p->Kc;
-  pa.op[0] = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap, p->Kc, p->read_k_fast_a);
-  pa.op[1] = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp, p->Kc, p->read_k_fast_b);
+  pa.op[0] = with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap, p->Kc,
+                                p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst);
+  pa.op[1] = with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp, p->Kc,
+                                p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst);
   int rc;
   if (x3)
     rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s);
@@ -602,6 +749,9 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.alpha = alpha;
   a.beta = beta;
   a.status = p->d_status;
+  a.ksplit = p->ksplit;
+  a.kb_per_split = p->kb_per_split;
+  a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(ws + p->off_part) : nullptr;
   mark(1, 0, s);
   if (pair && x3)
     gett_tc2_kernel<TC_BF16X3><<<p->grid, Tc2Cfg<TC_BF16X3>::NUM_THREADS,
@@ -616,7 +766,14 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
     gett_tc_kernel<TC_BF16><<<p->grid, TcCfgT<TC_BF16>::NUM_THREADS, TcCfgT<TC_BF16>::SMEM_BYTES,
                               s>>>(tmA, tmB, a);
   mark(1, 1, s);
-  return launch_check("gett_tc");
+  rc = launch_check("gett_tc");
+  if (rc || p->ksplit == 1) return rc;
+  dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
+  mark(2, 0, s);
+  simt_reduce_kernel<float><<<g2, 256, 0, s>>>(a.partial, p->ksplit, p->M, p->N, p->M, p->N, Cout,
+                                               c_m, c_n, alpha, beta);
+  mark(2, 1, s);
+  return launch_check("tc_reduce");
 }
 
 static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s);
@@ -805,6 +962,9 @@ struct tccg_group {
   int32_t n_jobs = 0;
   int64_t pack_ctas = 0, total_tiles = 0;
   int32_t grid = 0;
+  void* d_reduce = nullptr;    // ReduceJob<T>[] of the items with a k-split
+  int32_t n_reduce = 0;
+  int64_t reduce_ctas = 0;
   bool bound = false;
 };
 
@@ -812,6 +972,7 @@ static void group_free(tccg_group* g) {
   if (!g) return;
   if (g->d_items) cudaFree(g->d_items);
   if (g->d_jobs) cudaFree(g->d_jobs);
+  if (g->d_reduce) cudaFree(g->d_reduce);
   delete g;
 }
 
@@ -832,10 +993,11 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "all plans of a group need the same precision, dtype and device");
     }
-    if (p->tune.method != TCCG_METHOD_GETT || p->ksplit > 1 || p->tune.pair ||
+    if (p->tune.method != TCCG_METHOD_GETT || p->tune.pair ||
         (simt_path(p) && p->prec != TCCG_PREC_FP32 && p->prec != TCCG_PREC_FP64)) {
       group_free(g);
-      return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without k-split (plan %d)", i);
+      return fail(TCCG_ERR_UNSUPPORTED,
+                  "grouped plans must be GETT on the one-SM kernel of their precision (plan %d)", i);
     }
     g->plans.push_back(p);
     g->ws_off.push_back(ws);
@@ -843,9 +1005,9 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) {
       const int BM = p->prec == TCCG_PREC_FP64 ? SimtCfg<double>::BM : SimtCfg<float>::BM;
       const int BN = p->prec == TCCG_PREC_FP64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
-      tiles += (p->Mp / BM) * (p->Np / BN);
+      tiles += (p->Mp / BM) * (p->Np / BN) * p->ksplit;
     } else {
-      tiles += (int64_t)p->tiles_m * p->tiles_n;
+      tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
   }
   if (tiles > INT32_MAX) { group_free(g); return fail(TCCG_ERR_UNSUPPORTED, "too many tiles"); }
@@ -857,6 +1019,7 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
                                                     : sizeof(TcGroupItem);
   cudaError_t e = cudaMalloc(&g->d_items, item_bytes * count);
   if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_jobs, sizeof(PackJob) * g->n_jobs);
+  if (e == cudaSuccess) e = cudaMalloc(&g->d_reduce, sizeof(ReduceJob<double>) * count);
   if (e != cudaSuccess) {
     group_free(g);
     return fail(TCCG_ERR_CUDA, "group tables: %s", cudaGetErrorString(e));
@@ -872,7 +1035,11 @@ extern "C" int tccg_group_workspace(const tccg_group* g, size_t* bytes) {
 }
 
 template <typename T>
-static SimtArgs<T> simt_args_for(const tccg_plan* p, char* w, void* C, double alpha, double beta) {
+static void set_direct(SimtArgs<T>& a, const tccg_plan* p, const void* GA, const void* GB);
+
+template <typename T>
+static SimtArgs<T> simt_args_for(const tccg_plan* p, char* w, const void* GA, const void* GB,
+                                 void* C, double alpha, double beta) {
   SimtArgs<T> a;
   a.Ap = reinterpret_cast<T*>(w + p->off_a);
   a.Bp = reinterpret_cast<T*>(w + p->off_b);
@@ -881,14 +1048,42 @@ static SimtArgs<T> simt_args_for(const tccg_plan* p, char* w, void* C, double al
   a.M = p->M;
   a.N = p->N;
   a.ktiles = p->ktiles;
-  a.ktiles_per_split = p->ktiles;
+  a.ktiles_per_split = p->ktiles_per_split;
   a.C = static_cast<T*>(C);
   a.c_m_off = p->t_c_m;
   a.c_n_off = p->t_c_n;
   a.alpha = (T)alpha;
   a.beta = (T)beta;
-  a.partial = nullptr;
+  a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(w + p->off_part) : nullptr;
+  set_direct(a, p, GA, GB);
   return a;
+}
+
+// Reduction job of a k-split item: slices [split][Np][Mp] -> C.
+template <typename T>
+static ReduceJob<T> reduce_job_for(const T* partial, int32_t splits, int64_t Mp, int64_t Np,
+                                   const tccg_plan* p, void* C, double alpha, double beta,
+                                   int64_t begin) {
+  ReduceJob<T> j;
+  j.partial = partial;
+  j.Mp = Mp;
+  j.Np = Np;
+  j.M = p->M;
+  j.N = p->N;
+  j.C = static_cast<T*>(C);
+  j.c_m_off = p->t_c_m;
+  j.c_n_off = p->t_c_n;
+  j.alpha = (T)alpha;
+  j.beta = (T)beta;
+  j.begin = begin;
+  j.splits = splits;
+  j.mblocks = (int32_t)cdiv(p->M, 256);
+  return j;
+}
+
+template <typename T>
+static int64_t reduce_ctas(const ReduceJob<T>& j) {
+  return (int64_t)j.mblocks * cdiv(j.N, REDUCE_NCOLS);
 }
 
 extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* const* B,
@@ -905,7 +1100,9 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
   std::vector<SimtGroupItem<float>> sf;
   std::vector<SimtGroupItem<double>> sd;
   std::vector<TcGroupItem> tc;
-  int64_t tile = 0;
+  std::vector<ReduceJob<float>> rf;
+  std::vector<ReduceJob<double>> rd;
+  int64_t tile = 0, rctas = 0;
   for (int i = 0; i < n; ++i) {
     const tccg_plan* p = g->plans[i];
     if (!A[i] || !B[i] || !C[i]) return fail(TCCG_ERR_INVALID, "null operand pointer for item %d", i);
@@ -918,8 +1115,10 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       ob = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, w + p->off_b, p->Np, p->read_k_fast_b);
     } else {
       const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
-      oa = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, w + p->off_a, p->Kc, p->read_k_fast_a);
-      ob = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b, p->Kc, p->read_k_fast_b);
+      oa = with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, w + p->off_a, p->Kc,
+                              p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst);
+      ob = with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b, p->Kc,
+                              p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst);
     }
     PackOperand ops[2] = {oa, ob};
     const int kt = simt ? pack_k_tile<PACK_MN>() : pack_k_tile<PACK_K_BF16>();
@@ -928,24 +1127,35 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       jb.op = ops[j];
       jb.begin = pack_ctas;
       jb.ktiles = cdiv(ops[j].Kcover, kt);
-      pack_ctas += jb.ktiles * cdiv(ops[j].Rcover, 32);
+      if (!p->direct)  // a direct item's jobs own no CTAs
+        pack_ctas += jb.ktiles * cdiv(ops[j].Rcover, 32);
     }
     if (g->prec == TCCG_PREC_FP32) {
       SimtGroupItem<float> it;
-      it.args = simt_args_for<float>(p, w, C[i], alpha[i], beta[i]);
+      it.args = simt_args_for<float>(p, w, GA, GB, C[i], alpha[i], beta[i]);
       it.tile_begin = tile;
       it.tiles_m = (int32_t)(p->Mp / SimtCfg<float>::BM);
-      it.pad = 0;
-      tile += (int64_t)it.tiles_m * (p->Np / SimtCfg<float>::BN);
+      it.tiles_n = (int32_t)(p->Np / SimtCfg<float>::BN);
+      tile += (int64_t)it.tiles_m * it.tiles_n * p->ksplit;
       sf.push_back(it);
+      if (p->ksplit > 1) {
+        rf.push_back(reduce_job_for<float>(it.args.partial, p->ksplit, p->Mp, p->Np, p, C[i],
+                                           alpha[i], beta[i], rctas));
+        rctas += reduce_ctas(rf.back());
+      }
     } else if (g->prec == TCCG_PREC_FP64) {
       SimtGroupItem<double> it;
-      it.args = simt_args_for<double>(p, w, C[i], alpha[i], beta[i]);
+      it.args = simt_args_for<double>(p, w, GA, GB, C[i], alpha[i], beta[i]);
       it.tile_begin = tile;
       it.tiles_m = (int32_t)(p->Mp / SimtCfg<double>::BM);
-      it.pad = 0;
-      tile += (int64_t)it.tiles_m * (p->Np / SimtCfg<double>::BN);
+      it.tiles_n = (int32_t)(p->Np / SimtCfg<double>::BN);
+      tile += (int64_t)it.tiles_m * it.tiles_n * p->ksplit;
       sd.push_back(it);
+      if (p->ksplit > 1) {
+        rd.push_back(reduce_job_for<double>(it.args.partial, p->ksplit, p->Mp, p->Np, p, C[i],
+                                            alpha[i], beta[i], rctas));
+        rctas += reduce_ctas(rd.back());
+      }
     } else {
       TcGroupItem it;
       memset(&it, 0, sizeof(it));
@@ -967,9 +1177,17 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       a.alpha = (float)alpha[i];
       a.beta = (float)beta[i];
       a.status = p->d_status;
+      a.ksplit = p->ksplit;
+      a.kb_per_split = p->kb_per_split;
+      a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
       it.tile_begin = tile;
-      tile += (int64_t)p->tiles_m * p->tiles_n;
+      tile += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
       tc.push_back(it);
+      if (p->ksplit > 1) {
+        rf.push_back(reduce_job_for<float>(a.partial, p->ksplit, p->M, p->N, p, C[i], alpha[i],
+                                           beta[i], rctas));
+        rctas += reduce_ctas(rf.back());
+      }
     }
   }
   if (pack_ctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
@@ -980,10 +1198,26 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     CUDA_TRY(cudaMemcpy(g->d_items, sd.data(), sizeof(sd[0]) * sd.size(), cudaMemcpyHostToDevice));
   else
     CUDA_TRY(cudaMemcpy(g->d_items, tc.data(), sizeof(tc[0]) * tc.size(), cudaMemcpyHostToDevice));
+  if (!rf.empty())
+    CUDA_TRY(cudaMemcpy(g->d_reduce, rf.data(), sizeof(rf[0]) * rf.size(), cudaMemcpyHostToDevice));
+  if (!rd.empty())
+    CUDA_TRY(cudaMemcpy(g->d_reduce, rd.data(), sizeof(rd[0]) * rd.size(), cudaMemcpyHostToDevice));
+  if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
+  g->n_reduce = (int32_t)(rf.size() + rd.size());
+  g->reduce_ctas = rctas;
   g->pack_ctas = pack_ctas;
   g->grid = simt ? (int32_t)g->total_tiles : (int32_t)std::min<int64_t>(g->total_tiles, g->num_sms);
   g->bound = true;
   return TCCG_OK;
+}
+
+// Third launch of a group, only when some item has a k-split.
+template <typename T>
+static int group_reduce(const tccg_group* g, cudaStream_t s) {
+  if (g->n_reduce == 0) return TCCG_OK;
+  reduce_group_kernel<T><<<(unsigned)g->reduce_ctas, 256, 0, s>>>(
+      static_cast<const ReduceJob<T>*>(g->d_reduce), g->n_reduce);
+  return launch_check("reduce_group");
 }
 
 extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
@@ -994,19 +1228,22 @@ extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const dim3 pgrid((unsigned)g->pack_ctas);
   const int nj = g->n_jobs;
+  const bool pack = g->pack_ctas > 0;  // all items direct: no packing launch
   switch (g->prec) {
     case TCCG_PREC_FP32:
-      pack_group_kernel<float, float, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      if (pack) pack_group_kernel<float, float, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
       if ((rc = launch_check("pack_group"))) return rc;
       simt_gett_group_kernel<float><<<g->grid, 256, simt_smem_bytes<float>(), s>>>(
           static_cast<const SimtGroupItem<float>*>(g->d_items), (int)g->plans.size());
-      return launch_check("simt_gett_group");
+      if ((rc = launch_check("simt_gett_group"))) return rc;
+      return group_reduce<float>(g, s);
     case TCCG_PREC_FP64:
-      pack_group_kernel<double, double, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
+      if (pack) pack_group_kernel<double, double, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
       if ((rc = launch_check("pack_group"))) return rc;
       simt_gett_group_kernel<double><<<g->grid, 256, simt_smem_bytes<double>(), s>>>(
           static_cast<const SimtGroupItem<double>*>(g->d_items), (int)g->plans.size());
-      return launch_check("simt_gett_group");
+      if ((rc = launch_check("simt_gett_group"))) return rc;
+      return group_reduce<double>(g, s);
     default: {
       const bool x3 = g->prec == TCCG_PREC_BF16X3;
       if (x3)
@@ -1027,7 +1264,8 @@ extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
       else
         gett_tc_group_kernel<TC_BF16><<<g->grid, TcCfgT<TC_BF16>::NUM_THREADS,
                                         TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, st);
-      return launch_check("gett_tc_group");
+      if ((rc = launch_check("gett_tc_group"))) return rc;
+      return group_reduce<float>(g, s);
     }
   }
 }
@@ -1186,6 +1424,9 @@ extern "C" int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, c
   a.alpha = (float)alpha;
   a.beta = (float)beta;
   a.status = status;
+  a.ksplit = 1;  // no k-split: C written directly
+  a.kb_per_split = a.num_kb;
+  a.partial = nullptr;
   const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
   if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
   const int grid = (int)std::min<int64_t>(tiles, g_noalloc_sms[dev]);

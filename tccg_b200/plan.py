@@ -71,14 +71,30 @@ def gett_view(con: Contraction, strides: Optional[dict] = None) -> GettView:
     m = [(i.label, i.size) for i in con.m_indices]
     n = [(i.label, i.size) for i in con.n_indices]
     kset = [i.label for i in con.k_indices]
-    # K order: follow the operand whose stride-one index is contracted
-    if GA.indices[0].label in kset:
-        order = [l for l in GA.labels if l in kset]
-    elif GB.indices[0].label in kset:
-        order = [l for l in GB.labels if l in kset]
-    else:
-        order = [l for l in GA.labels if l in kset]
     sizes = {i.label: i.size for i in GA.indices + GB.indices}
+    # The packing pass reads an operand coalesced when its stride-one index
+    # is the first mode of its row order or of the K order. M keeps C's order
+    # (C's stride-one index first: coalesced epilogue stores). N is free
+    # (the epilogue's lanes run along m): GB's smallest-stride N mode first.
+    nb = [l for l, e in n if e > 1]
+    if nb:
+        first = min(nb, key=lambda l: abs(st(GB, nameB, l)))
+        n = [x for x in n if x[0] == first] + [x for x in n if x[0] != first]
+    # K order: the operand whose stride-one index is contracted leads; when
+    # both are, the larger operand.
+    def lead(T: Tensor) -> Optional[str]:
+        real = [i for i in T.indices if i.size > 1]
+        return real[0].label if real and real[0].label in kset else None
+    la, lb = lead(GA), lead(GB)
+    if la and lb and la != lb:
+        owner = GA if GA.num_elements() >= GB.num_elements() else GB
+    elif la:
+        owner = GA
+    elif lb:
+        owner = GB
+    else:
+        owner = GA
+    order = [l for l in owner.labels if l in kset]
     k = [(l, sizes[l]) for l in order]
     v = GettView(
         swap_ab=swap, m=m, n=n, k=k,
@@ -128,11 +144,12 @@ def operand_dtype(precision: str, bf16_inputs: bool = False) -> str:
 @dataclass
 class Tuning:
     method: str = "gett"
-    ksplit: int = 1
+    ksplit: int = 0  # 0: automatic (split K when the C tiles cannot fill the GPU)
     raster: int = 0
     max_ctas: int = 0
     variant: int = 0
     pair: int = 0
+    direct: int = 0  # CUDA-core kernels: 0 auto, 1 no packing pass, -1 always pack
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -142,11 +159,12 @@ class Tuning:
         t.max_ctas = int(self.max_ctas)
         t.variant = int(self.variant)
         t.pair = int(self.pair)
+        t.direct = int(self.direct)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d" % (self.method, self.ksplit, self.raster, self.max_ctas,
-                                           self.variant, self.pair)
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d" % (self.method, self.ksplit, self.raster, self.max_ctas,
+                                               self.variant, self.pair, self.direct)
 
 
 class Plan:
@@ -154,12 +172,14 @@ class Plan:
     specialised ``gett()``)."""
 
     def __init__(self, con: Contraction, precision: str = "fp32", dtype: Optional[str] = None,
-                 tuning: Optional[Tuning] = None, strides: Optional[dict] = None):
+                 tuning: Optional[Tuning] = None, strides: Optional[dict] = None,
+                 view: Optional[GettView] = None):
         self.con = con
         self.precision = precision
         self.dtype = dtype or operand_dtype(precision)
         self.tuning = tuning or Tuning()
-        self.view = gett_view(con, strides)
+        # ``view``: a hand-made GETT view of ``con`` (mode orders of one's own)
+        self.view = view if view is not None else gett_view(con, strides)
         self._desc = native_desc(self.view)
         self._lib = N.lib()
         h = ctypes.c_void_p()

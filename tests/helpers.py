@@ -23,11 +23,11 @@ def seeded_normal(n: int, seed: int) -> np.ndarray:
     return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
 
 
-def run_gpu(con, precision, A, B, C, alpha=None, beta=None, tuning=None, dtype=None):
+def run_gpu(con, precision, A, B, C, alpha=None, beta=None, tuning=None, dtype=None, view=None):
     """Run one contraction through the native plan; returns C as float64 numpy."""
     import torch
     from tccg_b200.plan import Plan
-    p = Plan(con, precision=precision, tuning=tuning, dtype=dtype)
+    p = Plan(con, precision=precision, tuning=tuning, dtype=dtype, view=view)
     tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}
     dA = torch.from_numpy(np.ascontiguousarray(A)).to("cuda").to(tdt[p.dtype])
     dB = torch.from_numpy(np.ascontiguousarray(B)).to("cuda").to(tdt[p.dtype])

@@ -18,7 +18,7 @@ import pytest
 from helpers import seeded_normal
 from oracle import LoopNest, error_metrics
 from tccg_b200 import _native as N
-from tccg_b200.plan import Plan, gett_view, native_desc
+from tccg_b200.plan import Plan, Tuning, gett_view, native_desc
 from tccg_b200.spec import make_contraction
 
 CASES = [
@@ -51,7 +51,9 @@ def test_noalloc_matches_plan_run_twice(cuda):
         dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
         c_plan = torch.from_numpy(C).cuda()
         c_free = torch.from_numpy(C).cuda()
-        Plan(con, precision="bf16x3").run(dA, dB, c_plan, alpha, beta)
+        # the allocation-free entry point never splits K: compare with the
+        # plan's unsplit schedule
+        Plan(con, precision="bf16x3", tuning=Tuning(ksplit=1)).run(dA, dB, c_plan, alpha, beta)
         _noalloc(con, dA, dB, c_free, alpha, beta)
         torch.cuda.synchronize()
         out_plan = c_plan.double().cpu().numpy()
