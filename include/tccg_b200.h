@@ -97,9 +97,10 @@ typedef struct tccg_desc {
 /* Kernel choices the autotuner searches over; zero-initialised = defaults. */
 typedef struct tccg_tuning {
   int32_t method;      /* TCCG_METHOD_* */
-  int32_t variant;     /* BF16X3: k-blocks (of 32) per TMEM accumulation chunk (0 = 16);
-                          BF16/BF16X3: < 0 selects the CUDA-core kernel (operands rounded
-                          to bf16 for BF16, FP32 FFMA) for bandwidth-bound shapes */
+  int32_t variant;     /* BF16/BF16X3 kernel family: 0 = chosen by a bandwidth/compute model,
+                          > 0 = tensor cores (BF16X3: k-blocks of 32 per TMEM accumulation
+                          chunk, default 16), < 0 = CUDA cores (operands rounded to bf16 for
+                          BF16, FP32 FFMA) */
   int32_t ksplit;      /* k-split factor: 0 = automatic (split K over CTAs when the C tiles
                           cannot fill the GPU), 1 = none, > 1 = that many slices
                           (the CTA-pair kernel never splits) */

@@ -6,8 +6,9 @@ generated harness and keeps the results in SQLite keyed on the contraction,
 the sizes, the CPU and the types (sql_util.py:206-306; lookup tccg.py:192-221).
 
 Here the candidates are kernel choices of one native plan -- method (GETT or
-TTGT), k-split for the SIMT kernels, tile-raster group and K-chunk length for
-the tcgen05 kernels -- ordered by a simple model (defaults first), timed on
+TTGT), k-split for the SIMT kernels, CUDA-core or tensor-core kernel for the
+BF16 precisions, tile-raster group and K-chunk length for the tcgen05
+kernels -- ordered by a simple model (defaults first), timed on
 the device with CUDA events (minimum over repetitions, L2 flushed in between
 like TCCG's trashCache, tccg.py:725-737), and the winner is stored in SQLite
 keyed on (contraction, extents, precision, operand type, beta != 0, GPU name,
@@ -109,13 +110,14 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             splits.sort(key=lambda s: abs(tiles * s - 2 * num_sms))
             out += [Tuning(method=method, ksplit=s) for s in splits]
         else:
+            # variant > 0 forces the tensor cores (BF16X3: k-blocks per
+            # accumulation chunk), < 0 the CUDA cores; the library's own
+            # choice (variant 0) goes first
             rasters = [8, 4, 16]
-            chunks = [16, 32, 8] if precision == "bf16x3" else [0]
+            chunks = [16, 32, 8] if precision == "bf16x3" else [1]
             tc = [Tuning(method=method, raster=r, variant=c) for r in rasters for c in chunks]
-            # a short K makes the contraction bandwidth-bound: the CUDA-core
-            # kernel (variant < 0) streams C faster than the tensor-core epilogue
             simt = [Tuning(method=method, variant=-1)]
-            out += (simt + tc) if K <= 128 else (tc + simt)
+            out += [Tuning(method=method)] + ((simt + tc) if K <= 128 else (tc + simt))
     return out
 
 

@@ -72,7 +72,7 @@ template <typename T>
 constexpr size_t simt_smem_bytes() {
   using Cfg = SimtCfg<T>;
   size_t pipe = (size_t)Cfg::STAGES * Cfg::BK * (Cfg::BM + Cfg::BN) * sizeof(T);
-  size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T);
+  size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T) + Cfg::EPN * sizeof(int64_t);
   return pipe > epi ? pipe : epi;
 }
 
@@ -96,7 +96,13 @@ __device__ __forceinline__ Vec4<T> lds4(const T* p) {
 }
 
 // One BM x BN tile (bx, by) of split bz; all 256 threads of the CTA take part.
-template <typename T>
+// Operand loading of simt_gett_tile: packed operands only, direct gathers
+// only, or either by a.direct at run time (the grouped kernel). The packed
+// instantiation carries none of the gather code, so its register allocation
+// and epilogue stay those of a pure packed kernel.
+enum SimtLoad : int { SIMT_PACKED = 0, SIMT_DIRECT = 1, SIMT_EITHER = 2 };
+
+template <typename T, int LOAD = SIMT_EITHER>
 __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int by, int bz) {
   using Cfg = SimtCfg<T>;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
@@ -126,7 +132,8 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   const int dcol_b = tid % BN, drow_b = tid / BN;
   constexpr int64_t NONE = INT64_MIN;  // offsets may be negative (negative strides)
   int64_t dm_off = NONE, dn_off = NONE;
-  if (a.direct) {
+  const bool direct = LOAD == SIMT_DIRECT || (LOAD == SIMT_EITHER && a.direct);
+  if (direct) {
     if (m0 + dcol_a < a.M) dm_off = a.a_m_off[m0 + dcol_a];
     if (n0 + dcol_b < a.N) dn_off = a.b_n_off[n0 + dcol_b];
   }
@@ -135,7 +142,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     T* as = As + (size_t)stage * BK * BM;
     T* bs = Bs + (size_t)stage * BK * BN;
     const int64_t krow = (int64_t)kt * BK;
-    if (a.direct) {
+    if (direct) {
       // all k offsets first (independent loads), then the copies: an offset
       // load between two asynchronous copies would serialise them
       constexpr int JA = BK * BM / 256, JB = BK * BN / 256;
@@ -267,6 +274,10 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   constexpr int CPI = 256 / QPC;           // columns per iteration
   constexpr int ITER = EPN / CPI;
   T* Cs = reinterpret_cast<T*>(smem_raw);  // [EPN][LDC]
+  // C offsets of the pass's columns, staged once: the C loads of a chunk then
+  // depend on shared memory only, not on a table load from L2
+  int64_t* Cn = reinterpret_cast<int64_t*>(smem_raw + (size_t)EPN * LDC * sizeof(T));
+  static_assert((EPN * LDC * sizeof(T)) % 8 == 0 && EPN <= 256, "column offset staging");
   const int q = tid % QPC, cl = tid / QPC;
   const int64_t mq = m0 + 4 * q;
   int64_t cmo[4];
@@ -287,6 +298,10 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
         for (int i = 0; i < TM; ++i) Cs[nl * LDC + mloc(i)] = acc[i][j];
       }
     }
+    if (tid < EPN) {
+      const int64_t n = n0 + p * EPN + tid;
+      Cn[tid] = n < a.N ? a.c_n_off[n] : 0;
+    }
     __syncthreads();
     if (mok[0]) {
       constexpr int CH = sizeof(T) == 8 ? 4 : 8;  // columns whose C loads are in flight together
@@ -298,7 +313,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
         for (int u = 0; u < CH; ++u) {
           const int64_t n = n0 + p * EPN + (it0 + u) * CPI + cl;
           nok[u] = (it0 + u < ITER) && n < a.N;
-          coff[u] = nok[u] ? a.c_n_off[n] : 0;
+          coff[u] = nok[u] ? Cn[(it0 + u) * CPI + cl] : 0;
         }
         T old[CH][4];
         if (beta != T(0)) {
@@ -345,9 +360,9 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   }
 }
 
-template <typename T>
+template <typename T, int LOAD>
 __global__ void __launch_bounds__(256, 2) simt_gett_kernel(const SimtArgs<T> a) {
-  simt_gett_tile<T>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  simt_gett_tile<T, LOAD>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Grouped launch: item i owns CTAs [tile_begin[i], tile_begin[i+1]); the CTA

@@ -82,17 +82,40 @@ struct tccg_plan {
   int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0, chunk_kb = 1, bn = 256;
   int32_t kb_per_split = 0;
   bool direct = false;  // CUDA-core kernel gathers operands without a packing pass
+  bool simt = false;    // CUDA-core kernels (else tcgen05)
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
   char describe[512] = "";
 };
 
-// The CUDA-core (SIMT) kernels run FP32 and FP64, and -- when the tuning asks
-// for it with variant < 0 -- the BF16 precisions too (operands rounded to bf16
-// by the pack for TCCG_PREC_BF16, FP32 FFMA accumulation), which is the faster
-// choice for bandwidth-bound contractions with a short K.
-static bool simt_path(const tccg_plan* p) {
-  return p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64 || p->tune.variant < 0;
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+static int64_t cdiv(int64_t x, int64_t a) { return (x + a - 1) / a; }
+
+// The CUDA-core (SIMT) kernels run FP32 and FP64, and the BF16 precisions too
+// when that is faster (operands rounded to bf16 by the pack for
+// TCCG_PREC_BF16; FP32 FFMA accumulation, more accurate than split-BF16x3):
+// tuning.variant < 0 asks for them, > 0 for the tensor cores, 0 lets a
+// bandwidth/compute model decide.
+static bool simt_path(const tccg_plan* p) { return p->simt; }
+
+static bool choose_simt(const tccg_plan* p) {
+  if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) return true;
+  if (p->tune.pair || p->tune.variant > 0) return false;
+  if (p->tune.variant < 0) return true;
+  // Model fitted on B200 timings of mixed contractions (the 256-item
+  // batched workload): tensor cores at 0.6 PFLOP/s effective (x3 for
+  // split-BF16x3) on 128 x 192 tiles with a C epilogue at 3 TB/s; CUDA cores
+  // at 35 TFLOP/s on 128 x 128 tiles; operands streamed three times (pack
+  // read, packed write, GEMM read) at 4.5 TB/s. Tile padding counts as work.
+  const double M = (double)p->M, N = (double)p->N, K = (double)p->K;
+  const double Mt = (double)round_up(p->M, 128), Nt = (double)round_up(p->N, 192);
+  const double Ms = (double)round_up(p->M, 128), Ns = (double)round_up(p->N, 128);
+  const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
+  const double t_tc = std::max(2.0 * Mt * Nt * K * (p->prec == TCCG_PREC_BF16X3 ? 3.0 : 1.0) / 0.6e15,
+                               cb / 3e12 + 3.0 * op / 4.5e12);
+  const double t_simt = std::max(2.0 * Ms * Ns * K / 35e12, (cb + 3.0 * op) / 4.5e12);
+  return t_simt < t_tc;
 }
 
 // First mode of extent > 1 has unit stride (or no such mode).
@@ -113,6 +136,9 @@ static bool choose_direct(const tccg_plan* p) {
   if (p->dtype == TCCG_BF16 || p->prec == TCCG_PREC_BF16) return false;
   if (p->tune.direct > 0) return true;
   if (p->K > 256) return false;
+  // the pack's extra traffic (2 x the operands) must matter next to C's;
+  // otherwise the 16-byte loads of packed operands win
+  if (4 * (p->M + p->N) * p->K < p->M * p->N) return false;
   const int64_t es = p->prec == TCCG_PREC_FP64 ? 8 : 4, small = 4 << 20;
   const tccg_desc& d = p->d;
   const bool a_ok = unit_first(d.nm, d.m_ext, d.a_m_stride) || p->M * p->K * es <= small;
@@ -120,9 +146,6 @@ static bool choose_direct(const tccg_plan* p) {
   return a_ok && b_ok;
 }
 
-static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-static int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
-static int64_t cdiv(int64_t x, int64_t a) { return (x + a - 1) / a; }
 
 // K slices for `tiles` C tiles over `kblocks` k-blocks when `slots` CTAs run
 // at once: the requested count, or (requested == 0) as many slices as fill
@@ -318,6 +341,7 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
     if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int32_t));
     if (e != cudaSuccess) rc = fail(TCCG_ERR_CUDA, "status word: %s", cudaGetErrorString(e));
   }
+  p->simt = choose_simt(p);
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
   if (!rc && !simt_path(p)) {  // tensor-core packs: rows along the unit-stride mode
@@ -493,10 +517,14 @@ static cudaError_t g_attr_err = cudaSuccess;
 static void set_attrs() {
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) { if (e == cudaSuccess && x != cudaSuccess) e = x; };
-  chk(cudaFuncSetAttribute(simt_gett_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)simt_smem_bytes<float>()));
-  chk(cudaFuncSetAttribute(simt_gett_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(simt_gett_kernel<float, SIMT_PACKED>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<float>()));
+  chk(cudaFuncSetAttribute(simt_gett_kernel<float, SIMT_DIRECT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<float>()));
+  chk(cudaFuncSetAttribute(simt_gett_kernel<double, SIMT_PACKED>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(simt_gett_kernel<double, SIMT_DIRECT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -693,7 +721,10 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   dim3 grid((unsigned)(p->Mp / Cfg::BM), (unsigned)(p->Np / Cfg::BN), (unsigned)p->ksplit);
   if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
   mark(1, 0, s);
-  simt_gett_kernel<T><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+  if (p->direct)
+    simt_gett_kernel<T, SIMT_DIRECT><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+  else
+    simt_gett_kernel<T, SIMT_PACKED><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
   mark(1, 1, s);
   rc = launch_check("simt_gett");
   if (rc) return rc;
@@ -949,20 +980,30 @@ extern "C" int tccg_transpose(int32_t dtype, int32_t dim, const int32_t* perm,
 }
 
 // --------------------------------------------------------------------------
-// grouped launches (implemented in grouped.cu)
+// grouped launches
 // --------------------------------------------------------------------------
 struct tccg_group {
   std::vector<const tccg_plan*> plans;
   int32_t prec = 0, dtype = 0;
   int device = 0, num_sms = 148;
-  std::vector<size_t> ws_off;  // per item: start of its packed operands
+  std::vector<size_t> ws_off;  // per item: start of its workspace
   size_t ws_bytes = 0;
-  void* d_items = nullptr;     // SimtGroupItem<T>[] or TcGroupItem[]
-  PackJob* d_jobs = nullptr;
-  int32_t n_jobs = 0;
-  int64_t pack_ctas = 0, total_tiles = 0;
-  int32_t grid = 0;
-  void* d_reduce = nullptr;    // ReduceJob<T>[] of the items with a k-split
+  // CUDA-core lane (FP32/FP64 groups, and BF16-precision items that plan for
+  // the CUDA cores): SimtGroupItem<T>[], T = double for FP64 groups else float
+  void* d_simt = nullptr;
+  int32_t n_simt = 0;
+  int64_t simt_tiles = 0;
+  PackJob* d_simt_jobs = nullptr;
+  int64_t simt_pack_ctas = 0;
+  // tensor-core lane (BF16 / BF16X3 groups)
+  TcGroupItem* d_tc = nullptr;
+  int32_t n_tc = 0;
+  int64_t tc_tiles = 0;
+  PackJob* d_tc_jobs = nullptr;
+  int64_t tc_pack_ctas = 0;
+  int32_t* tc_status = nullptr;
+  // k-split reductions: ReduceJob<T>[] (same T as the CUDA-core lane)
+  void* d_reduce = nullptr;
   int32_t n_reduce = 0;
   int64_t reduce_ctas = 0;
   bool bound = false;
@@ -970,9 +1011,9 @@ struct tccg_group {
 
 static void group_free(tccg_group* g) {
   if (!g) return;
-  if (g->d_items) cudaFree(g->d_items);
-  if (g->d_jobs) cudaFree(g->d_jobs);
-  if (g->d_reduce) cudaFree(g->d_reduce);
+  void* ps[] = {g->d_simt, g->d_simt_jobs, g->d_tc, g->d_tc_jobs, g->d_reduce};
+  for (void* q : ps)
+    if (q) cudaFree(q);
   delete g;
 }
 
@@ -984,8 +1025,8 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
   g->dtype = plans[0]->dtype;
   g->device = plans[0]->device;
   g->num_sms = plans[0]->num_sms;
+  const bool dbl = g->prec == TCCG_PREC_FP64;
   size_t ws = 0;
-  int64_t tiles = 0;
   for (int i = 0; i < count; ++i) {
     const tccg_plan* p = plans[i];
     if (!p) { group_free(g); return fail(TCCG_ERR_INVALID, "plan %d is null", i); }
@@ -993,32 +1034,39 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "all plans of a group need the same precision, dtype and device");
     }
-    if (p->tune.method != TCCG_METHOD_GETT || p->tune.pair ||
-        (simt_path(p) && p->prec != TCCG_PREC_FP32 && p->prec != TCCG_PREC_FP64)) {
+    if (p->tune.method != TCCG_METHOD_GETT || p->tune.pair) {
       group_free(g);
-      return fail(TCCG_ERR_UNSUPPORTED,
-                  "grouped plans must be GETT on the one-SM kernel of their precision (plan %d)", i);
+      return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without the CTA-pair kernel (plan %d)", i);
     }
     g->plans.push_back(p);
     g->ws_off.push_back(ws);
     ws = align_up(ws + p->ws_bytes, 256);
-    if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) {
-      const int BM = p->prec == TCCG_PREC_FP64 ? SimtCfg<double>::BM : SimtCfg<float>::BM;
-      const int BN = p->prec == TCCG_PREC_FP64 ? SimtCfg<double>::BN : SimtCfg<float>::BN;
-      tiles += (p->Mp / BM) * (p->Np / BN) * p->ksplit;
+    if (simt_path(p)) {
+      const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
+      const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+      g->simt_tiles += (p->Mp / BM) * (p->Np / BN) * p->ksplit;
+      ++g->n_simt;
     } else {
-      tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
+      g->tc_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
+      if (!g->tc_status) g->tc_status = p->d_status;
+      ++g->n_tc;
     }
   }
-  if (tiles > INT32_MAX) { group_free(g); return fail(TCCG_ERR_UNSUPPORTED, "too many tiles"); }
+  if (g->simt_tiles > INT32_MAX || g->tc_tiles > INT32_MAX) {
+    group_free(g);
+    return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
+  }
   g->ws_bytes = ws;
-  g->total_tiles = tiles;
-  g->n_jobs = 2 * count;
-  size_t item_bytes = (g->prec == TCCG_PREC_FP64)   ? sizeof(SimtGroupItem<double>)
-                      : (g->prec == TCCG_PREC_FP32) ? sizeof(SimtGroupItem<float>)
-                                                    : sizeof(TcGroupItem);
-  cudaError_t e = cudaMalloc(&g->d_items, item_bytes * count);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_jobs, sizeof(PackJob) * g->n_jobs);
+  const size_t simt_item = dbl ? sizeof(SimtGroupItem<double>) : sizeof(SimtGroupItem<float>);
+  cudaError_t e = cudaSuccess;
+  if (g->n_simt) {
+    e = cudaMalloc(&g->d_simt, simt_item * g->n_simt);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_simt_jobs, sizeof(PackJob) * 2 * g->n_simt);
+  }
+  if (e == cudaSuccess && g->n_tc) {
+    e = cudaMalloc((void**)&g->d_tc, sizeof(TcGroupItem) * g->n_tc);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_tc_jobs, sizeof(PackJob) * 2 * g->n_tc);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&g->d_reduce, sizeof(ReduceJob<double>) * count);
   if (e != cudaSuccess) {
     group_free(g);
@@ -1086,6 +1134,133 @@ static int64_t reduce_ctas(const ReduceJob<T>& j) {
   return (int64_t)j.mblocks * cdiv(j.N, REDUCE_NCOLS);
 }
 
+// Items of one lane, the most k-blocks per tile first: CTAs take tiles in
+// index order (round robin in the persistent tensor-core kernel, launch order
+// in the CUDA-core one), so the longest tiles start first and the short ones
+// fill in behind them.
+static std::vector<size_t> by_tile_cost(const tccg_group* g, bool simt) {
+  std::vector<size_t> idx;
+  for (size_t i = 0; i < g->plans.size(); ++i)
+    if (simt_path(g->plans[i]) == simt) idx.push_back(i);
+  auto cost = [&](size_t i) {
+    const tccg_plan* p = g->plans[i];
+    return simt ? (int64_t)p->ktiles_per_split : (int64_t)p->kb_per_split;
+  };
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+  return idx;
+}
+
+// Two pack jobs (A, B) of one item; a direct item's jobs own no CTAs.
+static void add_pack_jobs(std::vector<PackJob>& jobs, int64_t& ctas, const PackOperand& oa,
+                          const PackOperand& ob, int ktile, bool active) {
+  for (const PackOperand* o : {&oa, &ob}) {
+    PackJob jb;
+    jb.op = *o;
+    jb.begin = ctas;
+    jb.ktiles = cdiv(o->Kcover, ktile);
+    if (active) ctas += jb.ktiles * cdiv(o->Rcover, 32);
+    jobs.push_back(jb);
+  }
+}
+
+// The CUDA-core lane of a bind; T = the lane's element type.
+template <typename T>
+static int bind_simt(tccg_group* g, const void* const* A, const void* const* B, void* const* C,
+                     const double* alpha, const double* beta, char* ws,
+                     std::vector<ReduceJob<T>>& red, int64_t& rctas) {
+  std::vector<SimtGroupItem<T>> items;
+  std::vector<PackJob> jobs;
+  int64_t tile = 0, pctas = 0;
+  for (size_t i : by_tile_cost(g, true)) {
+    const tccg_plan* p = g->plans[i];
+    char* w = ws + g->ws_off[i];
+    const void* GA = p->d.swap_ab ? B[i] : A[i];
+    const void* GB = p->d.swap_ab ? A[i] : B[i];
+    add_pack_jobs(jobs, pctas,
+                  pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, w + p->off_a, p->Mp,
+                          p->read_k_fast_a),
+                  pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, w + p->off_b, p->Np,
+                          p->read_k_fast_b),
+                  pack_k_tile<PACK_MN>(), !p->direct);
+    SimtGroupItem<T> it;
+    it.args = simt_args_for<T>(p, w, GA, GB, C[i], alpha[i], beta[i]);
+    it.tile_begin = tile;
+    it.tiles_m = (int32_t)(p->Mp / SimtCfg<T>::BM);
+    it.tiles_n = (int32_t)(p->Np / SimtCfg<T>::BN);
+    tile += (int64_t)it.tiles_m * it.tiles_n * p->ksplit;
+    items.push_back(it);
+    if (p->ksplit > 1) {
+      red.push_back(reduce_job_for<T>(it.args.partial, p->ksplit, p->Mp, p->Np, p, C[i], alpha[i],
+                                      beta[i], rctas));
+      rctas += reduce_ctas(red.back());
+    }
+  }
+  if (items.empty()) return TCCG_OK;
+  if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
+  CUDA_TRY(cudaMemcpy(g->d_simt, items.data(), sizeof(items[0]) * items.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(g->d_simt_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
+  g->simt_pack_ctas = pctas;
+  return TCCG_OK;
+}
+
+static int bind_tc(tccg_group* g, const void* const* A, const void* const* B, void* const* C,
+                   const double* alpha, const double* beta, char* ws,
+                   std::vector<ReduceJob<float>>& red, int64_t& rctas) {
+  std::vector<TcGroupItem> items;
+  std::vector<PackJob> jobs;
+  int64_t tile = 0, pctas = 0;
+  for (size_t i : by_tile_cost(g, false)) {
+    const tccg_plan* p = g->plans[i];
+    char* w = ws + g->ws_off[i];
+    const void* GA = p->d.swap_ab ? B[i] : A[i];
+    const void* GB = p->d.swap_ab ? A[i] : B[i];
+    const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
+    add_pack_jobs(jobs, pctas,
+                  with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, w + p->off_a,
+                                     p->Kc, p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst),
+                  with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b,
+                                     p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
+                  pack_k_tile<PACK_K_BF16>(), true);
+    TcGroupItem it;
+    memset(&it, 0, sizeof(it));
+    int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, 128);
+    if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, p->bn);
+    if (rc) return rc;
+    TcArgs& a = it.args;
+    a.M = (int32_t)p->M;
+    a.N = (int32_t)p->N;
+    a.K = (int32_t)p->K;
+    a.num_kb = p->num_kb;
+    a.tiles_m = p->tiles_m;
+    a.tiles_n = p->tiles_n;
+    a.raster = p->raster;
+    a.chunk_kb = p->chunk_kb;
+    a.C = static_cast<float*>(C[i]);
+    a.c_m_off = p->t_c_m;
+    a.c_n_off = p->t_c_n;
+    a.alpha = (float)alpha[i];
+    a.beta = (float)beta[i];
+    a.status = p->d_status;
+    a.ksplit = p->ksplit;
+    a.kb_per_split = p->kb_per_split;
+    a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
+    it.tile_begin = tile;
+    tile += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
+    items.push_back(it);
+    if (p->ksplit > 1) {
+      red.push_back(reduce_job_for<float>(a.partial, p->ksplit, p->M, p->N, p, C[i], alpha[i],
+                                          beta[i], rctas));
+      rctas += reduce_ctas(red.back());
+    }
+  }
+  if (items.empty()) return TCCG_OK;
+  if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
+  CUDA_TRY(cudaMemcpy(g->d_tc, items.data(), sizeof(items[0]) * items.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(g->d_tc_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
+  g->tc_pack_ctas = pctas;
+  return TCCG_OK;
+}
+
 extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* const* B,
                                void* const* C, const double* alpha, const double* beta, void* ws,
                                size_t ws_bytes) {
@@ -1093,125 +1268,37 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
   if (ws_bytes < g->ws_bytes || (g->ws_bytes && !ws))
     return fail(TCCG_ERR_WORKSPACE, "group workspace of %zu bytes needed, %zu given", g->ws_bytes, ws_bytes);
   if ((reinterpret_cast<uintptr_t>(ws) & 255u) != 0) return fail(TCCG_ERR_ALIGNMENT, "workspace must be 256-byte aligned");
-  const int n = (int)g->plans.size();
-  std::vector<PackJob> jobs(2 * n);
-  int64_t pack_ctas = 0;
-  const bool simt = g->prec == TCCG_PREC_FP32 || g->prec == TCCG_PREC_FP64;
-  std::vector<SimtGroupItem<float>> sf;
-  std::vector<SimtGroupItem<double>> sd;
-  std::vector<TcGroupItem> tc;
-  std::vector<ReduceJob<float>> rf;
-  std::vector<ReduceJob<double>> rd;
-  int64_t tile = 0, rctas = 0;
-  for (int i = 0; i < n; ++i) {
-    const tccg_plan* p = g->plans[i];
-    if (!A[i] || !B[i] || !C[i]) return fail(TCCG_ERR_INVALID, "null operand pointer for item %d", i);
-    char* w = static_cast<char*>(ws) + g->ws_off[i];
-    const void* GA = p->d.swap_ab ? B[i] : A[i];
-    const void* GB = p->d.swap_ab ? A[i] : B[i];
-    PackOperand oa, ob;
-    if (simt) {
-      oa = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, w + p->off_a, p->Mp, p->read_k_fast_a);
-      ob = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, w + p->off_b, p->Np, p->read_k_fast_b);
-    } else {
-      const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
-      oa = with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, w + p->off_a, p->Kc,
-                              p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst);
-      ob = with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b, p->Kc,
-                              p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst);
-    }
-    PackOperand ops[2] = {oa, ob};
-    const int kt = simt ? pack_k_tile<PACK_MN>() : pack_k_tile<PACK_K_BF16>();
-    for (int j = 0; j < 2; ++j) {
-      PackJob& jb = jobs[2 * i + j];
-      jb.op = ops[j];
-      jb.begin = pack_ctas;
-      jb.ktiles = cdiv(ops[j].Kcover, kt);
-      if (!p->direct)  // a direct item's jobs own no CTAs
-        pack_ctas += jb.ktiles * cdiv(ops[j].Rcover, 32);
-    }
-    if (g->prec == TCCG_PREC_FP32) {
-      SimtGroupItem<float> it;
-      it.args = simt_args_for<float>(p, w, GA, GB, C[i], alpha[i], beta[i]);
-      it.tile_begin = tile;
-      it.tiles_m = (int32_t)(p->Mp / SimtCfg<float>::BM);
-      it.tiles_n = (int32_t)(p->Np / SimtCfg<float>::BN);
-      tile += (int64_t)it.tiles_m * it.tiles_n * p->ksplit;
-      sf.push_back(it);
-      if (p->ksplit > 1) {
-        rf.push_back(reduce_job_for<float>(it.args.partial, p->ksplit, p->Mp, p->Np, p, C[i],
-                                           alpha[i], beta[i], rctas));
-        rctas += reduce_ctas(rf.back());
-      }
-    } else if (g->prec == TCCG_PREC_FP64) {
-      SimtGroupItem<double> it;
-      it.args = simt_args_for<double>(p, w, GA, GB, C[i], alpha[i], beta[i]);
-      it.tile_begin = tile;
-      it.tiles_m = (int32_t)(p->Mp / SimtCfg<double>::BM);
-      it.tiles_n = (int32_t)(p->Np / SimtCfg<double>::BN);
-      tile += (int64_t)it.tiles_m * it.tiles_n * p->ksplit;
-      sd.push_back(it);
-      if (p->ksplit > 1) {
-        rd.push_back(reduce_job_for<double>(it.args.partial, p->ksplit, p->Mp, p->Np, p, C[i],
-                                            alpha[i], beta[i], rctas));
-        rctas += reduce_ctas(rd.back());
-      }
-    } else {
-      TcGroupItem it;
-      memset(&it, 0, sizeof(it));
-      int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, 128);
-      if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, p->bn);
-      if (rc) return rc;
-      TcArgs& a = it.args;
-      a.M = (int32_t)p->M;
-      a.N = (int32_t)p->N;
-      a.K = (int32_t)p->K;
-      a.num_kb = p->num_kb;
-      a.tiles_m = p->tiles_m;
-      a.tiles_n = p->tiles_n;
-      a.raster = p->raster;
-      a.chunk_kb = p->chunk_kb;
-      a.C = static_cast<float*>(C[i]);
-      a.c_m_off = p->t_c_m;
-      a.c_n_off = p->t_c_n;
-      a.alpha = (float)alpha[i];
-      a.beta = (float)beta[i];
-      a.status = p->d_status;
-      a.ksplit = p->ksplit;
-      a.kb_per_split = p->kb_per_split;
-      a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
-      it.tile_begin = tile;
-      tile += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
-      tc.push_back(it);
-      if (p->ksplit > 1) {
-        rf.push_back(reduce_job_for<float>(a.partial, p->ksplit, p->M, p->N, p, C[i], alpha[i],
-                                           beta[i], rctas));
-        rctas += reduce_ctas(rf.back());
-      }
-    }
+  for (size_t i = 0; i < g->plans.size(); ++i)
+    if (!A[i] || !B[i] || !C[i]) return fail(TCCG_ERR_INVALID, "null operand pointer for item %zu", i);
+  g->bound = false;
+  char* w = static_cast<char*>(ws);
+  int64_t rctas = 0;
+  int rc;
+  size_t nred = 0;
+  if (g->prec == TCCG_PREC_FP64) {
+    std::vector<ReduceJob<double>> red;
+    if ((rc = bind_simt<double>(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
+    if (!red.empty())
+      CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
+    nred = red.size();
+  } else {
+    std::vector<ReduceJob<float>> red;
+    if ((rc = bind_simt<float>(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
+    if ((rc = bind_tc(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
+    if (!red.empty())
+      CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
+    nred = red.size();
   }
-  if (pack_ctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
-  CUDA_TRY(cudaMemcpy(g->d_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
-  if (g->prec == TCCG_PREC_FP32)
-    CUDA_TRY(cudaMemcpy(g->d_items, sf.data(), sizeof(sf[0]) * sf.size(), cudaMemcpyHostToDevice));
-  else if (g->prec == TCCG_PREC_FP64)
-    CUDA_TRY(cudaMemcpy(g->d_items, sd.data(), sizeof(sd[0]) * sd.size(), cudaMemcpyHostToDevice));
-  else
-    CUDA_TRY(cudaMemcpy(g->d_items, tc.data(), sizeof(tc[0]) * tc.size(), cudaMemcpyHostToDevice));
-  if (!rf.empty())
-    CUDA_TRY(cudaMemcpy(g->d_reduce, rf.data(), sizeof(rf[0]) * rf.size(), cudaMemcpyHostToDevice));
-  if (!rd.empty())
-    CUDA_TRY(cudaMemcpy(g->d_reduce, rd.data(), sizeof(rd[0]) * rd.size(), cudaMemcpyHostToDevice));
   if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
-  g->n_reduce = (int32_t)(rf.size() + rd.size());
+  g->n_reduce = (int32_t)nred;
   g->reduce_ctas = rctas;
-  g->pack_ctas = pack_ctas;
-  g->grid = simt ? (int32_t)g->total_tiles : (int32_t)std::min<int64_t>(g->total_tiles, g->num_sms);
   g->bound = true;
   return TCCG_OK;
 }
 
-// Third launch of a group, only when some item has a k-split.
+// Launches of a group run, in order: packing (CUDA-core lane, tensor-core
+// lane), the two grouped GETT kernels, and the k-split reduction -- each only
+// when it has work.
 template <typename T>
 static int group_reduce(const tccg_group* g, cudaStream_t s) {
   if (g->n_reduce == 0) return TCCG_OK;
@@ -1226,48 +1313,56 @@ extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
   int rc = ensure_attrs();
   if (rc) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const dim3 pgrid((unsigned)g->pack_ctas);
-  const int nj = g->n_jobs;
-  const bool pack = g->pack_ctas > 0;  // all items direct: no packing launch
-  switch (g->prec) {
-    case TCCG_PREC_FP32:
-      if (pack) pack_group_kernel<float, float, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
-      if ((rc = launch_check("pack_group"))) return rc;
-      simt_gett_group_kernel<float><<<g->grid, 256, simt_smem_bytes<float>(), s>>>(
-          static_cast<const SimtGroupItem<float>*>(g->d_items), (int)g->plans.size());
-      if ((rc = launch_check("simt_gett_group"))) return rc;
-      return group_reduce<float>(g, s);
-    case TCCG_PREC_FP64:
-      if (pack) pack_group_kernel<double, double, PACK_MN><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
-      if ((rc = launch_check("pack_group"))) return rc;
-      simt_gett_group_kernel<double><<<g->grid, 256, simt_smem_bytes<double>(), s>>>(
-          static_cast<const SimtGroupItem<double>*>(g->d_items), (int)g->plans.size());
-      if ((rc = launch_check("simt_gett_group"))) return rc;
-      return group_reduce<double>(g, s);
-    default: {
-      const bool x3 = g->prec == TCCG_PREC_BF16X3;
-      if (x3)
-        pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
-      else if (g->dtype == TCCG_BF16)
-        pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
-      else
-        pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pgrid, dim3(32, 8), 0, s>>>(g->d_jobs, nj);
-      if ((rc = launch_check("pack_group"))) return rc;
-      TcGroup tg;
-      tg.items = static_cast<const TcGroupItem*>(g->d_items);
-      tg.n_items = (int32_t)g->plans.size();
-      tg.total_tiles = (int32_t)g->total_tiles;
-      int32_t* st = g->plans[0]->d_status;
-      if (x3)
-        gett_tc_group_kernel<TC_BF16X3><<<g->grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
-                                          TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tg, st);
-      else
-        gett_tc_group_kernel<TC_BF16><<<g->grid, TcCfgT<TC_BF16>::NUM_THREADS,
-                                        TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, st);
-      if ((rc = launch_check("gett_tc_group"))) return rc;
-      return group_reduce<float>(g, s);
-    }
+  const int sj = 2 * g->n_simt, tj = 2 * g->n_tc;
+  const dim3 blk(32, 8);
+  // CUDA-core lane packing (layout by precision and operand type)
+  if (g->simt_pack_ctas > 0) {
+    const dim3 pg((unsigned)g->simt_pack_ctas);
+    if (g->prec == TCCG_PREC_FP64)
+      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+    else if (g->dtype == TCCG_BF16)
+      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+    else if (g->prec == TCCG_PREC_BF16)
+      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+    else
+      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+    if ((rc = launch_check("pack_group"))) return rc;
   }
+  const bool x3 = g->prec == TCCG_PREC_BF16X3;
+  if (g->tc_pack_ctas > 0) {
+    const dim3 pg((unsigned)g->tc_pack_ctas);
+    if (x3)
+      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pg, blk, 0, s>>>(g->d_tc_jobs, tj);
+    else if (g->dtype == TCCG_BF16)
+      pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, tj);
+    else
+      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, tj);
+    if ((rc = launch_check("pack_group"))) return rc;
+  }
+  if (g->n_simt > 0) {
+    if (g->prec == TCCG_PREC_FP64)
+      simt_gett_group_kernel<double><<<(unsigned)g->simt_tiles, 256, simt_smem_bytes<double>(), s>>>(
+          static_cast<const SimtGroupItem<double>*>(g->d_simt), g->n_simt);
+    else
+      simt_gett_group_kernel<float><<<(unsigned)g->simt_tiles, 256, simt_smem_bytes<float>(), s>>>(
+          static_cast<const SimtGroupItem<float>*>(g->d_simt), g->n_simt);
+    if ((rc = launch_check("simt_gett_group"))) return rc;
+  }
+  if (g->n_tc > 0) {
+    TcGroup tg;
+    tg.items = g->d_tc;
+    tg.n_items = g->n_tc;
+    tg.total_tiles = (int32_t)g->tc_tiles;
+    const unsigned grid = (unsigned)std::min<int64_t>(g->tc_tiles, g->num_sms);
+    if (x3)
+      gett_tc_group_kernel<TC_BF16X3><<<grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
+                                        TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tg, g->tc_status);
+    else
+      gett_tc_group_kernel<TC_BF16><<<grid, TcCfgT<TC_BF16>::NUM_THREADS,
+                                      TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, g->tc_status);
+    if ((rc = launch_check("gett_tc_group"))) return rc;
+  }
+  return g->prec == TCCG_PREC_FP64 ? group_reduce<double>(g, s) : group_reduce<float>(g, s);
 }
 
 extern "C" int tccg_group_destroy(tccg_group* g) {

@@ -75,11 +75,16 @@ def gett_view(con: Contraction, strides: Optional[dict] = None) -> GettView:
     # The packing pass reads an operand coalesced when its stride-one index
     # is the first mode of its row order or of the K order. M keeps C's order
     # (C's stride-one index first: coalesced epilogue stores). N is free
-    # (the epilogue's lanes run along m): GB's smallest-stride N mode first.
+    # (the epilogue's lanes run along m).
+    # GB's unit-stride N mode leads when GB is large next to C (K >= M/4);
+    # otherwise C's order stays (its stores then sweep C's own layout)
     nb = [l for l, e in n if e > 1]
-    if nb:
+    K = _prod(i.size for i in con.k_indices)
+    M = _prod(e for _, e in m)
+    if nb and 4 * K >= M:
         first = min(nb, key=lambda l: abs(st(GB, nameB, l)))
-        n = [x for x in n if x[0] == first] + [x for x in n if x[0] != first]
+        if abs(st(GB, nameB, first)) == 1:
+            n = [x for x in n if x[0] == first] + [x for x in n if x[0] != first]
     # K order: the operand whose stride-one index is contracted leads; when
     # both are, the larger operand.
     def lead(T: Tensor) -> Optional[str]:

@@ -67,9 +67,13 @@ def test_direct_with_k_split(cuda, precision):
 
 def test_automatic_choice(cuda):
     from tccg_b200.plan import Plan
-    short = make_contraction("abcd", "aeb", "edc", dict(a=96, b=96, c=96, d=96, e=16))
-    assert "pack=none" in Plan(short, precision="fp32").describe()
+    # skinny C, short K: the operands are a large share of the traffic
+    skinny = make_contraction("abn", "abk", "kn", dict(a=300, b=400, n=12, k=20))
+    assert "pack=none" in Plan(skinny, precision="fp32").describe()
+    # configuration 2: C dominates, packing the small operands costs nothing
+    cfg2 = make_contraction("abcd", "aeb", "edc", dict(a=96, b=96, c=96, d=96, e=16))
+    assert "pack=MN" in Plan(cfg2, precision="fp32").describe()
     long_k = make_contraction("mn", "mk", "kn", dict(m=512, n=512, k=4096))
     assert "pack=MN" in Plan(long_k, precision="fp32").describe()
     # BF16 rounding needs the pack
-    assert "pack=MN" in Plan(short, precision="bf16", tuning=Tuning(variant=-1)).describe()
+    assert "pack=MN" in Plan(skinny, precision="bf16", tuning=Tuning(variant=-1)).describe()

@@ -16,6 +16,7 @@ import pytest
 
 from helpers import labels, run_gpu, seeded_normal, splitmix_uniform
 from oracle import LoopNest, error_metrics, tccg_inputs
+from tccg_b200.plan import Tuning
 from tccg_b200.spec import make_contraction, parse_text
 
 pytestmark = pytest.mark.gpu
@@ -75,20 +76,29 @@ def test_fp64_vs_loopnest(cuda, name):
     assert m["normwise"] <= 1e-13, m
 
 
+# BF16 precisions: the library's own kernel choice and the tensor-core kernel
+# forced (tuning.variant > 0), so both paths are checked on every case
+KERNELS = {"auto": 0, "tensor_core": 16}
+
+
+@pytest.mark.parametrize("kernel", sorted(KERNELS))
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_bf16x3_vs_fp64(cuda, name):
+def test_bf16x3_vs_fp64(cuda, name, kernel):
     lc, la, lb, sizes, alpha, beta = CASES[name]
     con = make_contraction(lc, la, lb, sizes, alpha, beta)
     ln, A, B, C = _inputs(lc, la, lb, sizes, seed=3, dist="normal")
     A32, B32, C32 = A.astype(np.float32), B.astype(np.float32), C.astype(np.float32)
-    out, _ = run_gpu(con, "bf16x3", A32, B32, C32)
+    out, p = run_gpu(con, "bf16x3", A32, B32, C32, tuning=Tuning(variant=KERNELS[kernel]))
+    if kernel == "tensor_core":
+        assert "gett_tc<BF16X3>" in p.describe()
     ref = ln.run(A32.astype(np.float64), B32.astype(np.float64), C32.astype(np.float64), alpha, beta)
     m = error_metrics(out, ref)
     assert m["normwise"] <= 1e-5, m
 
 
+@pytest.mark.parametrize("kernel", sorted(KERNELS))
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_bf16_vs_fp64(cuda, name):
+def test_bf16_vs_fp64(cuda, name, kernel):
     import torch
     lc, la, lb, sizes, alpha, beta = CASES[name]
     con = make_contraction(lc, la, lb, sizes, alpha, beta)
@@ -97,13 +107,18 @@ def test_bf16_vs_fp64(cuda, name):
     Ab = torch.from_numpy(A.astype(np.float32)).bfloat16().float().numpy()
     Bb = torch.from_numpy(B.astype(np.float32)).bfloat16().float().numpy()
     C32 = C.astype(np.float32)
-    out, _ = run_gpu(con, "bf16", Ab, Bb, C32)
+    # the same kernel for f32 and bf16 operand tensors (the automatic choice
+    # looks at the operand bytes): forced with variant -1 or 1
+    t = Tuning(variant=1 if kernel == "tensor_core" else -1)
+    out, _ = run_gpu(con, "bf16", Ab, Bb, C32, tuning=t)
     ref = ln.run(Ab.astype(np.float64), Bb.astype(np.float64), C32.astype(np.float64), alpha, beta)
     m = error_metrics(out, ref)
     assert m["normwise"] <= 1e-5, m
     # and with bf16 tensors as inputs
-    out2, _ = run_gpu(con, "bf16", Ab, Bb, C32, dtype="bf16")
+    out2, _ = run_gpu(con, "bf16", Ab, Bb, C32, dtype="bf16", tuning=t)
     assert np.array_equal(out, out2)
+    out3, _ = run_gpu(con, "bf16", Ab, Bb, C32)
+    assert error_metrics(out3, ref)["normwise"] <= 1e-5
 
 
 def test_tccg_formula_inputs_example(cuda):
@@ -126,8 +141,8 @@ def test_beta_zero_ignores_nan_in_c(cuda):
     con = make_contraction(lc, la, lb, sizes, alpha, 0.0)
     ln, A, B, C = _inputs(lc, la, lb, sizes, seed=5)
     Cn = np.full(ln.size_c, np.nan, dtype=np.float32)
-    for prec in ("fp32", "bf16x3"):
-        out, _ = run_gpu(con, prec, A.astype(np.float32), B.astype(np.float32), Cn)
+    for prec, t in (("fp32", None), ("bf16x3", None), ("bf16x3", Tuning(variant=16))):
+        out, _ = run_gpu(con, prec, A.astype(np.float32), B.astype(np.float32), Cn, tuning=t)
         assert np.isfinite(out).all(), prec
 
 

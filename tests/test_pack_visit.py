@@ -34,7 +34,7 @@ def test_visit_order_for_the_m_operand(cuda, precision):
     if precision == "bf16":
         A = torch.from_numpy(A).bfloat16().float().numpy()
         B = torch.from_numpy(B).bfloat16().float().numpy()
-    out, p = run_gpu(con, precision, A, B, C)
+    out, p = run_gpu(con, precision, A, B, C, tuning=Tuning(variant=16))
     assert "visit a=1" in p.describe(), p.describe()
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 1.5, 0.5)
     assert error_metrics(out, ref)["normwise"] <= 1e-5
@@ -50,7 +50,7 @@ def test_visit_order_for_the_n_operand(cuda):
     assert v.b_n[0] == 1  # the library's own order starts with B's stride-one mode p
     v = dataclasses.replace(v, n=v.n[::-1], b_n=v.b_n[::-1], c_n=v.c_n[::-1])
     ln, A, B, C = _data(lc, la, lb, sizes, 102)
-    out, p = run_gpu(con, "bf16x3", A, B, C, view=v)
+    out, p = run_gpu(con, "bf16x3", A, B, C, view=v, tuning=Tuning(variant=16))
     assert "visit a=0 b=1" in p.describe(), p.describe()
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 1.0, 0.0)
     assert error_metrics(out, ref)["normwise"] <= 1e-5

@@ -51,9 +51,10 @@ def test_noalloc_matches_plan_run_twice(cuda):
         dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
         c_plan = torch.from_numpy(C).cuda()
         c_free = torch.from_numpy(C).cuda()
-        # the allocation-free entry point never splits K: compare with the
-        # plan's unsplit schedule
-        Plan(con, precision="bf16x3", tuning=Tuning(ksplit=1)).run(dA, dB, c_plan, alpha, beta)
+        # the allocation-free entry point never splits K and always runs the
+        # tensor-core kernel: compare with the plan's schedule of the same kind
+        Plan(con, precision="bf16x3", tuning=Tuning(ksplit=1, variant=16)).run(dA, dB, c_plan,
+                                                                               alpha, beta)
         _noalloc(con, dA, dB, c_free, alpha, beta)
         torch.cuda.synchronize()
         out_plan = c_plan.double().cpu().numpy()
