@@ -404,6 +404,7 @@ __global__ void __launch_bounds__(256) simt_reduce_kernel(const T* __restrict__ 
   const int64_t cmo = c_m_off[m];
   for (int64_t n = blockIdx.y; n < N; n += gridDim.y) {
     T s = T(0);
+#pragma unroll 4
     for (int z = 0; z < splits; ++z) s += partial[(size_t)z * Np * Mp + n * Mp + m];
     T* dst = C + cmo + c_n_off[n];
     T v = alpha * s;
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(256) simt_reduce_kernel(const T* __restrict__ 
 
 // Grouped k-split reduction: job j (one contraction with a k-split) owns the
 // CTAs [begin, begin + mblocks * nblocks); CTA (mb, nb) sums the slices of
-// 256 rows over columns [64 nb, 64 nb + 64) in split order.
+// 256 rows over columns [ncols nb, ncols nb + ncols) in split order.
 template <typename T>
 struct ReduceJob {
   const T* partial;
@@ -425,9 +426,8 @@ struct ReduceJob {
   T alpha, beta;
   int64_t begin;
   int32_t splits, mblocks;
+  int32_t ncols;  // columns per CTA: fewer when there are many slices
 };
-
-constexpr int REDUCE_NCOLS = 64;
 
 template <typename T>
 __global__ void __launch_bounds__(256) reduce_group_kernel(const ReduceJob<T>* jobs, int n_jobs) {
@@ -441,11 +441,12 @@ __global__ void __launch_bounds__(256) reduce_group_kernel(const ReduceJob<T>* j
   const int64_t local = t - j.begin;
   const int64_t m = (local % j.mblocks) * 256 + threadIdx.x;
   if (m >= j.M) return;
-  const int64_t n0 = (local / j.mblocks) * REDUCE_NCOLS;
-  const int64_t n1 = n0 + REDUCE_NCOLS < j.N ? n0 + REDUCE_NCOLS : j.N;
+  const int64_t n0 = (local / j.mblocks) * j.ncols;
+  const int64_t n1 = n0 + j.ncols < j.N ? n0 + j.ncols : j.N;
   const int64_t cmo = j.c_m_off[m];
   for (int64_t n = n0; n < n1; ++n) {
     T s = T(0);
+#pragma unroll 4
     for (int z = 0; z < j.splits; ++z) s += j.partial[(size_t)z * j.Np * j.Mp + n * j.Mp + m];
     T* dst = j.C + cmo + j.c_n_off[n];
     T v = j.alpha * s;

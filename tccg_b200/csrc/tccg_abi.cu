@@ -218,6 +218,14 @@ static void plan_free(tccg_plan* p) {
 static int plan_layout(tccg_plan* p);
 static int pair_clusters(bool x3, int* clusters);
 
+// Smallest |stride| of the modes of extent > 1 (INT64_MAX if none).
+static long long min_stride(int n, const int64_t* ext, const int64_t* str) {
+  long long best = INT64_MAX;
+  for (int i = 0; i < n; ++i)
+    if (ext[i] > 1) best = std::min(best, std::llabs(str[i]));
+  return best;
+}
+
 // For a K-major pack whose rows are read one per lane: if a later row mode
 // has a smaller stride than the first (non-unit) mode, visit the rows with
 // that mode fastest. vsrc[v] = source offset, vdst[v] = destination row of
@@ -344,13 +352,24 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   p->simt = choose_simt(p);
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
-  if (!rc && !simt_path(p)) {  // tensor-core packs: rows along the unit-stride mode
+  if (!rc && !simt_path(p)) {
+    // tensor-core packs: walk the rows along the smallest-stride row mode when
+    // that beats both the first row mode and reading along k
     std::vector<int64_t> vs, vd;
-    if (!p->read_k_fast_a && build_visit(d.nm, d.m_ext, d.a_m_stride, vs, vd)) {
+    auto kstride = [&](const int64_t* kst) {
+      for (int i = 0; i < d.nk; ++i)
+        if (d.k_ext[i] > 1) return std::llabs(kst[i]);
+      return (long long)INT64_MAX;
+    };
+    if (min_stride(d.nm, d.m_ext, d.a_m_stride) < kstride(d.a_k_stride) &&
+        build_visit(d.nm, d.m_ext, d.a_m_stride, vs, vd)) {
+      p->read_k_fast_a = 0;
       rc = upload(vs, &p->t_a_vsrc);
       if (!rc) rc = upload(vd, &p->t_a_vdst);
     }
-    if (!rc && !p->read_k_fast_b && build_visit(d.nn, d.n_ext, d.b_n_stride, vs, vd)) {
+    if (!rc && min_stride(d.nn, d.n_ext, d.b_n_stride) < kstride(d.b_k_stride) &&
+        build_visit(d.nn, d.n_ext, d.b_n_stride, vs, vd)) {
+      p->read_k_fast_b = 0;
       rc = upload(vs, &p->t_b_vsrc);
       if (!rc) rc = upload(vd, &p->t_b_vdst);
     }
@@ -1126,12 +1145,14 @@ static ReduceJob<T> reduce_job_for(const T* partial, int32_t splits, int64_t Mp,
   j.begin = begin;
   j.splits = splits;
   j.mblocks = (int32_t)cdiv(p->M, 256);
+  // about 2048 loads per thread: many slices -> few columns per CTA
+  j.ncols = (int32_t)std::max<int64_t>(1, std::min<int64_t>(64, 2048 / splits));
   return j;
 }
 
 template <typename T>
 static int64_t reduce_ctas(const ReduceJob<T>& j) {
-  return (int64_t)j.mblocks * cdiv(j.N, REDUCE_NCOLS);
+  return (int64_t)j.mblocks * cdiv(j.N, j.ncols);
 }
 
 // Items of one lane, the most k-blocks per tile first: CTAs take tiles in
