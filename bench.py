@@ -432,7 +432,9 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": world * flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e,
-                    "path": "Compiled.run_host: pinned host A, B -> device, tccg_plan_run, C -> pinned host"},
+                    "path": "Compiled.run_host: pinned host A, B -> device, tccg_plan_run per slab of "
+                            "C's last index (%d slabs), C -> pinned host; copies overlap the compute on "
+                            "two copy streams" % x3._auto_slabs(Ch)},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
             "device_status": status,

@@ -69,26 +69,125 @@ class Compiled:
         self.plan.run(A, B, C, alpha, beta, workspace=self.workspace(C.device), stream=stream)
         return C
 
-    def run_host(self, A_host, B_host, C_host, alpha=None, beta=None, device="cuda", stream=None):
+    def run_host(self, A_host, B_host, C_host, alpha=None, beta=None, device="cuda", stream=None,
+                 slabs: Optional[int] = None):
         """End-to-end call on HOST buffers (torch CPU tensors, ideally pinned):
         copies A, B (and C when beta != 0) to the device, runs, copies C back.
-        Returns (h2d_bytes, d2h_bytes)."""
+        Returns (h2d_bytes, d2h_bytes); the work is queued on ``stream`` (the
+        current one by default), which the caller synchronises.
+
+        With ``slabs`` > 1 (default: automatic for C >= 256 MiB) C is computed
+        in slabs of its last index, and the copies overlap the compute on two
+        copy streams: the operand without that index goes up first, the other
+        one (when that index is its last) slab by slab, and each C slab comes
+        back while the next one is computed. Slab plans use the full tensors'
+        strides (the multi-GPU slab machinery of ``shard``)."""
         import torch
         beta_v = self.beta if beta is None else beta
+        alpha_v = self.alpha if alpha is None else alpha
         dev = torch.device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
         s = stream or torch.cuda.current_stream(dev)
-        with torch.cuda.stream(s):
-            dA = A_host.to(dev, non_blocking=True)
-            dB = B_host.to(dev, non_blocking=True)
-            h2d = dA.numel() * dA.element_size() + dB.numel() * dB.element_size()
-            if beta_v != 0:
-                dC = C_host.to(dev, non_blocking=True)
-                h2d += dC.numel() * dC.element_size()
+        n_slabs = self._auto_slabs(C_host) if slabs is None else max(1, int(slabs))
+        bufs = self._device_buffers(A_host, B_host, C_host, dev)
+        dA, dB, dC = bufs
+        es = lambda t: t.numel() * t.element_size()
+        h2d = es(A_host) + es(B_host) + (es(C_host) if beta_v != 0 else 0)
+        d2h = es(C_host)
+        if n_slabs <= 1 or not isinstance(self.plan, Plan):
+            with torch.cuda.stream(s):
+                dA.copy_(A_host, non_blocking=True)
+                dB.copy_(B_host, non_blocking=True)
+                if beta_v != 0:
+                    dC.copy_(C_host, non_blocking=True)
+                self.plan.run(dA, dB, dC, alpha, beta, workspace=self.workspace(dev), stream=s)
+                C_host.copy_(dC, non_blocking=True)
+            return h2d, d2h
+        from .shard import shard
+        con = self.contraction
+        label = con.C0.indices[-1].label
+        parts = [shard(con, r, n_slabs, label) for r in range(n_slabs)]
+        plans = [self._slab_plan(sh) for sh in parts]
+        ws_bytes = max(p.workspace_bytes for p in plans)
+        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev) if ws_bytes else None
+        up, down = self._copy_streams(dev)
+        up.wait_stream(s)    # buffers free: earlier work on the caller's stream is done
+        down.wait_stream(s)
+        # operands: the one carrying `label` as its last index goes slab by slab
+        per_slab = {}
+        for name, host, d in (("A", A_host, dA), ("B", B_host, dB)):
+            t = con.A0 if name == "A" else con.B0
+            if t.has(label) and t.indices[-1].label == label:
+                per_slab[name] = (host, d)
             else:
-                dC = torch.empty(C_host.shape, dtype=C_host.dtype, device=dev)
-            self.plan.run(dA, dB, dC, alpha, beta, workspace=self.workspace(dev), stream=s)
-            C_host.copy_(dC, non_blocking=True)
-        return h2d, dC.numel() * dC.element_size()
+                with torch.cuda.stream(up):
+                    d.copy_(host, non_blocking=True)
+        whole_ready = torch.cuda.Event()
+        whole_ready.record(up)
+        done = None
+        for sh, plan in zip(parts, plans):
+            n_c = sh.contraction.C0.num_elements()
+            c0 = sh.offsets["C"]
+            with torch.cuda.stream(up):
+                for name, (host, d) in per_slab.items():
+                    t = sh.contraction.A0 if name == "A" else sh.contraction.B0
+                    o, n = sh.offsets[name], t.num_elements()
+                    d[o:o + n].copy_(host[o:o + n], non_blocking=True)
+                if beta_v != 0:
+                    dC[c0:c0 + n_c].copy_(C_host[c0:c0 + n_c], non_blocking=True)
+                ready = torch.cuda.Event()
+                ready.record(up)
+            s.wait_event(whole_ready)
+            s.wait_event(ready)
+            ptr = lambda t, k: t.data_ptr() + sh.offsets[k] * t.element_size()
+            plan.run_ptr(ptr(dA, "A"), ptr(dB, "B"), ptr(dC, "C"), alpha_v, beta_v,
+                         ws.data_ptr() if ws is not None else 0,
+                         ws.numel() if ws is not None else 0, s.cuda_stream)
+            computed = torch.cuda.Event()
+            computed.record(s)
+            down.wait_event(computed)
+            with torch.cuda.stream(down):
+                C_host[c0:c0 + n_c].copy_(dC[c0:c0 + n_c], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(down)
+        s.wait_event(done)  # the caller's stream completes with the last copy
+        if ws is not None:
+            ws.record_stream(s)
+        return h2d, d2h
+
+    # -- helpers of run_host ------------------------------------------------
+    def _auto_slabs(self, C_host) -> int:
+        ext = self.contraction.C0.indices[-1].size
+        big = C_host.numel() * C_host.element_size() >= (256 << 20)
+        return min(16, ext) if big and ext >= 2 else 1
+
+    def _device_buffers(self, A_host, B_host, C_host, dev):
+        import torch
+        key = (dev, A_host.numel(), A_host.dtype, B_host.numel(), B_host.dtype, C_host.numel(),
+               C_host.dtype)
+        cached = getattr(self, "_host_bufs", None)
+        if cached is None or cached[0] != key:
+            mk = lambda h: torch.empty(h.numel(), dtype=h.dtype, device=dev)
+            cached = (key, (mk(A_host), mk(B_host), mk(C_host)))
+            self._host_bufs = cached
+        return cached[1]
+
+    def _copy_streams(self, dev):
+        import torch
+        st = getattr(self, "_streams", None)
+        if st is None or st[0] != dev:
+            st = (dev, torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+            self._streams = st
+        return st[1], st[2]
+
+    def _slab_plan(self, sh):
+        cache = self.__dict__.setdefault("_slab_plans", {})
+        key = (sh.label, sh.hi - sh.lo)
+        if key not in cache:
+            cache[key] = Plan(sh.contraction, precision=self.precision, tuning=self.plan.tuning,
+                              dtype=self.plan.dtype, strides=sh.strides)
+        return cache[key]
 
     def describe(self) -> str:
         return self.plan.describe()
