@@ -64,3 +64,58 @@ def test_group_matches_oracle_and_per_item(cuda, precision):
         ref = ln.sample64(An, Bn, None, 1.0, 0.0, lins)
         m = error_metrics(C.cpu().double().numpy()[lins], ref)
         assert m["normwise"] <= tol, (str(con), m)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16", "fp64"])
+def test_group_with_both_lanes_and_k_splits(cuda, precision):
+    """Items forced onto both kernel families (BF16 precisions: CUDA-core
+    lane and tensor-core lane in one group), with long-K items that split K
+    and short-K items that skip the pack; grouped results equal the per-item
+    plan runs bit for bit and match the FP64 oracle."""
+    import torch
+    from tccg_b200.grouped import Group
+    from tccg_b200.plan import Tuning
+    from tccg_b200.spec import make_contraction
+    shapes = [
+        ("ab", "akl", "lkb", dict(a=20, b=30, k=300, l=200)),          # long K, one tile: split
+        ("abn", "abk", "kn", dict(a=300, b=40, n=12, k=20)),           # short K, skinny: direct
+        ("mn", "mk", "kn", dict(m=700, n=500, k=1100)),
+        ("pqr", "qs", "spr", dict(p=37, q=29, r=11, s=53)),
+    ]
+    items = [make_contraction(lc, la, lb, sz, 1.0, 0.0) for lc, la, lb, sz in shapes] * 2
+    if precision == "fp64":
+        tunings = None
+    else:
+        tunings = [Tuning(variant=-1)] * 4 + [Tuning(variant=16 if precision == "bf16x3" else 1)] * 4
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    g = torch.Generator(device="cuda").manual_seed(9)
+    As = [torch.randn(c.A0.num_elements(), generator=g, device="cuda", dtype=dt) for c in items]
+    Bs = [torch.randn(c.B0.num_elements(), generator=g, device="cuda", dtype=dt) for c in items]
+    if precision == "bf16":  # exact products on either kernel family
+        As = [a.bfloat16().float() for a in As]
+        Bs = [b.bfloat16().float() for b in Bs]
+    Cs = [torch.zeros(c.C0.num_elements(), device="cuda", dtype=dt) for c in items]
+    grp = Group(items, precision, tunings=tunings)
+    descs = [p.describe() for p in grp.plans]
+    if precision != "fp64":
+        assert any("simt_gett" in d for d in descs) and any("gett_tc" in d for d in descs)
+    assert any("ksplit=1 " not in d for d in descs)
+    grp.bind(As, Bs, Cs)
+    grp.capture()
+    grp.replay()
+    torch.cuda.synchronize()
+    grouped = [c.clone() for c in Cs]
+    for c in Cs:
+        c.zero_()
+    grp.run_per_item()
+    torch.cuda.synchronize()
+    for a, b in zip(grouped, Cs):
+        assert torch.equal(a, b)
+    tol = 1e-13 if precision == "fp64" else 1e-5
+    for con, A, B, C in zip(items, As, Bs, grouped):
+        ln = LoopNest(con.C0.labels, con.A0.labels, con.B0.labels,
+                      {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices})
+        ref = ln.run(A.double().cpu().numpy(), B.double().cpu().numpy(),
+                     np.zeros(ln.size_c), 1.0, 0.0)
+        assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= tol, str(con)
