@@ -321,12 +321,20 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
         }
         tc_fence_after();
         const uint32_t tsrc = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * Cfg::ACC_STRIDE + h * HC);
+        // columns of this warp's half that exist in C (warp-uniform): the
+        // TMEM reads stop at the last 32-column group holding one of them
+        const int last = nlim >= HC ? HC - 32 : (nlim > 0 ? (int)((nlim - 1) / 32) * 32 : -32);
+        if (last < 0) {  // nothing to store: hand the accumulator straight back
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[acc]);
+        }
 #pragma unroll 1
-        for (int cc = 0; cc < HC; cc += 32) {
+        for (int cc = 0; cc <= last; cc += 32) {
           uint32_t r[32];
           tmem_ld_32x32b_x32(tsrc + (uint32_t)cc, r);
           tmem_ld_wait();
-          if (cc == HC - 32) {  // accumulator fully read: hand it back to the MMA warp
+          if (cc == last) {  // accumulator read: hand it back to the MMA warp
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce[acc]);
@@ -372,13 +380,15 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
           const uint32_t tsrc = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * Cfg::ACC_STRIDE + h * HC);
 #pragma unroll
           for (int cc = 0; cc < HC; cc += 16) {
-            uint32_t r[16];
-            tmem_ld_32x32b_x16(tsrc + (uint32_t)cc, r);
-            tmem_ld_wait();
+            if (cc < nlim) {  // warp-uniform: groups past C's last column are not read
+              uint32_t r[16];
+              tmem_ld_32x32b_x16(tsrc + (uint32_t)cc, r);
+              tmem_ld_wait();
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-              sum[cc + j] = (ch == 0) ? __uint_as_float(r[j])
-                                      : __fadd_rn(sum[cc + j], __uint_as_float(r[j]));
+              for (int j = 0; j < 16; ++j)
+                sum[cc + j] = (ch == 0) ? __uint_as_float(r[j])
+                                        : __fadd_rn(sum[cc + j], __uint_as_float(r[j]));
+            }
           }
           tc_fence_before();
           __syncwarp();
