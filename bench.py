@@ -446,7 +446,8 @@ def run_ours(args, world, rank, local):
 
 
 # --------------------------------------------------------------------------
-# every configuration (python bench.py --suite): the tables of DESIGN.md
+# every configuration (python bench.py --suite): per-precision timings, rooflines,
+# errors and the CPU baselines of configurations 1-5
 # --------------------------------------------------------------------------
 SUITE = {
     "cfg1": "C[a,b,i,j] = A[i,m,a] * B[m,j,b]\na=48\nb=48\ni=48\nj=48\nm=48\n",

@@ -11,12 +11,12 @@
 //   bit cleared), whose producer arrives with the byte count of the pair;
 //   the even CTA's MMA thread issues tcgen05.mma.cta_group::2 (M = 256),
 //   which reads the halves from both SMs and writes D rows [128r, 128r+128)
-//   into CTA r's TMEM; its commits arrive on both CTAs' barriers (multicast).
+//   into CTA r's TMEM; each of its commits is issued once per CTA's barrier.
 // Each CTA's epilogue drains its own TMEM rows; the odd CTA's epilogue warps
 // release the accumulator with remote arrives on the even CTA's barrier.
 // K is accumulated in chunks (as in tc_gemm.cuh) for BF16X3.
 //
-// No TMA multicast is used: every CTA loads its own operand halves.
+// No multicast of any kind: every CTA loads its own operand halves.
 #pragma once
 #include "tc_gemm.cuh"
 
@@ -76,12 +76,19 @@ __device__ __forceinline__ void tc_mma_f16_pair(uint32_t d_tmem, uint64_t adesc,
       : "memory");
 }
 
-// Arrive on `bar` in both CTAs of the pair once the prior MMAs completed.
+// Arrive on `bar` in both CTAs of the pair once the prior MMAs completed:
+// one commit per barrier (this CTA's, then the peer's at the same offset,
+// addressed through mapa); each commit tracks all prior MMAs of this thread.
 __device__ __forceinline__ void tc_commit_pair(uint64_t* bar) {
   asm volatile(
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
-      " [%0], %1;" ::"r"(smem_u32(bar)),
-      "h"((uint16_t)0x3)
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+  asm volatile(
+      "{\n\t.reg .b32 ra;\n\t"
+      "mapa.shared::cluster.u32 ra, %0, 1;\n\t"
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [ra];\n\t}" ::"r"(
+          smem_u32(bar))
       : "memory");
 }
 
