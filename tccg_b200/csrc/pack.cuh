@@ -60,116 +60,28 @@ __device__ __forceinline__ float load_as_acc<__nv_bfloat16>(const __nv_bfloat16*
   return __bfloat162float(*p);
 }
 
-// One 32 (rows) x 32 (k) tile of operand o; block = (32, 8).
-template <typename Tin, typename Tout, int LAYOUT>
-__device__ __forceinline__ void pack_tile(const PackOperand& o, int64_t kt, int64_t rt) {
-  using Acc = typename AccOf<Tin>::type;
-  const int64_t k0 = kt * 32, r0 = rt * 32;
-  if (k0 >= o.Kcover || r0 >= o.Rcover) return;
-  __shared__ Acc tile[32][33];  // [k_local][r_local]
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const Tin* src = static_cast<const Tin*>(o.src);
-  if (o.read_k_fast) {
-    const int64_t k = k0 + tx;
-    const int64_t coff = (k < o.Kk) ? o.col_off[k] : 0;
-#pragma unroll
-    for (int i = ty; i < 32; i += 8) {
-      const int64_t r = r0 + i;
-      Acc v = 0;
-      if (r < o.R && k < o.Kk) v = load_as_acc<Tin>(src + o.row_off[r] + coff);
-      tile[tx][i] = v;
-    }
-  } else {
-    const int64_t r = r0 + tx;
-    const int64_t roff = (r < o.R) ? o.row_off[r] : 0;
-#pragma unroll
-    for (int i = ty; i < 32; i += 8) {
-      const int64_t k = k0 + i;
-      Acc v = 0;
-      if (r < o.R && k < o.Kk) v = load_as_acc<Tin>(src + roff + o.col_off[k]);
-      tile[i][tx] = v;
-    }
-  }
-  __syncthreads();
-  Tout* dst = static_cast<Tout*>(o.dst);
-  if constexpr (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16) {
-    const int64_t r = r0 + tx;
-#pragma unroll
-    for (int i = ty; i < 32; i += 8) {
-      const int64_t k = k0 + i;
-      if (k < o.Kcover && r < o.Rcover) {
-        if constexpr (LAYOUT == PACK_MN_BF16)
-          dst[k * o.ld + r] = static_cast<Tout>(__bfloat162float(__float2bfloat16_rn((float)tile[i][tx])));
-        else
-          dst[k * o.ld + r] = static_cast<Tout>(tile[i][tx]);
-      }
-    }
-  } else {
-    // K-major bf16 rows: thread t packs 4 consecutive k of row t/8 and writes
-    // them as one 8-byte store (two for BF16X3: hi and lo). Reads of
-    // tile[kq + j][row] hit 32 distinct banks across the warp.
-    const int t = ty * 32 + tx;
-    const int rl = t >> 3, kq = (t & 7) * 4;
-    const int64_t r = r0 + rl;
-    __nv_bfloat16* base = reinterpret_cast<__nv_bfloat16*>(dst) + r * o.ld;
-    if (r < o.Rcover) {
-      if constexpr (LAYOUT == PACK_K_BF16) {
-        const int64_t k = k0 + kq;
-        if (k + 3 < o.Kcover && (o.ld & 3) == 0) {
-          __nv_bfloat162 p0 = __floats2bfloat162_rn((float)tile[kq][rl], (float)tile[kq + 1][rl]);
-          __nv_bfloat162 p1 = __floats2bfloat162_rn((float)tile[kq + 2][rl], (float)tile[kq + 3][rl]);
-          uint2 u;
-          u.x = *reinterpret_cast<uint32_t*>(&p0);
-          u.y = *reinterpret_cast<uint32_t*>(&p1);
-          *reinterpret_cast<uint2*>(base + k) = u;
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (k + j < o.Kcover) base[k + j] = __float2bfloat16_rn((float)tile[kq + j][rl]);
-        }
-      } else {  // PACK_K_BF16X3: each 32-wide k block becomes [hi x32 | lo x32]
-        float v[4];
-        __nv_bfloat16 hi[4], lo[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          v[j] = (float)tile[kq + j][rl];
-          hi[j] = __float2bfloat16_rn(v[j]);
-          lo[j] = __float2bfloat16_rn(v[j] - __bfloat162float(hi[j]));
-        }
-        __nv_bfloat16* row = base + (k0 / 32) * 64;  // 16-byte aligned: ld % 64 == 0
-        uint2 uh, ul;
-        __nv_bfloat162 h0 = __halves2bfloat162(hi[0], hi[1]), h1 = __halves2bfloat162(hi[2], hi[3]);
-        __nv_bfloat162 l0 = __halves2bfloat162(lo[0], lo[1]), l1 = __halves2bfloat162(lo[2], lo[3]);
-        uh.x = *reinterpret_cast<uint32_t*>(&h0);
-        uh.y = *reinterpret_cast<uint32_t*>(&h1);
-        ul.x = *reinterpret_cast<uint32_t*>(&l0);
-        ul.y = *reinterpret_cast<uint32_t*>(&l1);
-        *reinterpret_cast<uint2*>(row + kq) = uh;
-        *reinterpret_cast<uint2*>(row + 32 + kq) = ul;
-      }
-    }
-  }
-}
-
-// K-major layouts: one CTA packs 32 rows x 128 k. All 16 loads of a thread are
-// issued before the first shared-memory store, so each thread keeps 16
-// global loads in flight (the 32x32 tile left the pass latency-bound).
+// One CTA (32 x 8 threads) packs 32 rows x 128 k of an operand. All 16 loads
+// of a thread are issued before the first shared-memory store, so each thread
+// keeps 16 global loads in flight (32 x 32 tiles left the pass
+// latency-bound). Reads run along the operand's fast direction (k or rows);
+// writes along the destination's: rows for the MN layouts, k for K-major.
 constexpr int PACK_KT_WIDE = 128;
 
 template <int LAYOUT>
 __host__ __device__ constexpr int pack_k_tile() {
-  return (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16) ? 32 : PACK_KT_WIDE;
+  return PACK_KT_WIDE;
 }
 
-template <typename Tin, int LAYOUT>
-__device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t kt, int64_t rt) {
+template <typename Tin, typename Tout, int LAYOUT>
+__device__ __forceinline__ void pack_tile_wide(const PackOperand& o, int64_t kt, int64_t rt) {
+  using Acc = typename AccOf<Tin>::type;
   constexpr int KT = PACK_KT_WIDE, SB = KT / 32;
   const int64_t k0 = kt * KT, r0 = rt * 32;
   if (k0 >= o.Kcover || r0 >= o.Rcover) return;
-  __shared__ float tile[KT][33];  // [k_local][r_local]
+  __shared__ Acc tile[KT][33];  // [k_local][r_local]
   const int tx = threadIdx.x, ty = threadIdx.y;
   const Tin* src = static_cast<const Tin*>(o.src);
-  float v[SB][4];
+  Acc v[SB][4];
   if (o.read_k_fast) {
     int64_t roff[4];
 #pragma unroll
@@ -183,7 +95,7 @@ __device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t k
       const int64_t coff = (k < o.Kk) ? o.col_off[k] : -1;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
-        v[sb][i] = (roff[i] >= 0 && coff >= 0) ? load_as_acc<Tin>(src + roff[i] + coff) : 0.0f;
+        v[sb][i] = (roff[i] >= 0 && coff >= 0) ? load_as_acc<Tin>(src + roff[i] + coff) : Acc(0);
     }
 #pragma unroll
     for (int sb = 0; sb < SB; ++sb)
@@ -197,7 +109,7 @@ __device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t k
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int64_t k = k0 + sb * 32 + ty + 8 * i;
-        v[sb][i] = (roff >= 0 && k < o.Kk) ? load_as_acc<Tin>(src + roff + o.col_off[k]) : 0.0f;
+        v[sb][i] = (roff >= 0 && k < o.Kk) ? load_as_acc<Tin>(src + roff + o.col_off[k]) : Acc(0);
       }
 #pragma unroll
     for (int sb = 0; sb < SB; ++sb)
@@ -205,7 +117,25 @@ __device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t k
       for (int i = 0; i < 4; ++i) tile[sb * 32 + ty + 8 * i][tx] = v[sb][i];
   }
   __syncthreads();
-  // write: thread t packs 4 consecutive k of row t/8 per 32-wide k block
+  if constexpr (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16) {
+    // MN layouts: dst[k * ld + r], lanes along r (32 consecutive rows)
+    const int64_t r = r0 + tx;
+    if (r >= o.Rcover) return;
+    Tout* dst = static_cast<Tout*>(o.dst);
+#pragma unroll
+    for (int i = 0; i < KT / 8; ++i) {
+      const int kl = ty + 8 * i;
+      const int64_t k = k0 + kl;
+      if (k < o.Kcover) {
+        if constexpr (LAYOUT == PACK_MN_BF16)
+          dst[k * o.ld + r] = static_cast<Tout>(__bfloat162float(__float2bfloat16_rn((float)tile[kl][tx])));
+        else
+          dst[k * o.ld + r] = static_cast<Tout>(tile[kl][tx]);
+      }
+    }
+    return;
+  }
+  // K-major: thread t packs 4 consecutive k of row t/8 per 32-wide k block
   const int t = ty * 32 + tx;
   const int rl = t >> 3, kq = (t & 7) * 4;
   const int64_t r = r0 + rl;
@@ -254,10 +184,7 @@ __device__ __forceinline__ void pack_tile_kmajor(const PackOperand& o, int64_t k
 
 template <typename Tin, typename Tout, int LAYOUT>
 __device__ __forceinline__ void pack_any(const PackOperand& o, int64_t kt, int64_t rt) {
-  if constexpr (LAYOUT == PACK_MN || LAYOUT == PACK_MN_BF16)
-    pack_tile<Tin, Tout, LAYOUT>(o, kt, rt);
-  else
-    pack_tile_kmajor<Tin, LAYOUT>(o, kt, rt);
+  pack_tile_wide<Tin, Tout, LAYOUT>(o, kt, rt);
 }
 
 // grid = (ktiles * rtiles, 1, 2) with ktiles = ceil(Kcover / pack_k_tile),

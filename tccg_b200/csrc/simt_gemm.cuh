@@ -173,17 +173,17 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
         else
           *dst = T(0);
       }
-      return;
-    }
+    } else if constexpr (LOAD != SIMT_DIRECT) {
 #pragma unroll
-    for (int c = tid; c < A_CHUNKS; c += 256) {
-      const int row = c / A_ROW_CHUNKS, col = (c % A_ROW_CHUNKS) * VEC;
-      cp_async_16(as + row * BM + col, a.Ap + (krow + row) * a.Mp + m0 + col);
-    }
+      for (int c = tid; c < A_CHUNKS; c += 256) {
+        const int row = c / A_ROW_CHUNKS, col = (c % A_ROW_CHUNKS) * VEC;
+        cp_async_16(as + row * BM + col, a.Ap + (krow + row) * a.Mp + m0 + col);
+      }
 #pragma unroll
-    for (int c = tid; c < B_CHUNKS; c += 256) {
-      const int row = c / B_ROW_CHUNKS, col = (c % B_ROW_CHUNKS) * VEC;
-      cp_async_16(bs + row * BN + col, a.Bp + (krow + row) * a.Np + n0 + col);
+      for (int c = tid; c < B_CHUNKS; c += 256) {
+        const int row = c / B_ROW_CHUNKS, col = (c % B_ROW_CHUNKS) * VEC;
+        cp_async_16(bs + row * BN + col, a.Bp + (krow + row) * a.Np + n0 + col);
+      }
     }
   };
 
