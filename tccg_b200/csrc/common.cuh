@@ -13,6 +13,19 @@
 
 namespace tccg {
 
+// Grouped launches: index of the last segment whose first CTA/tile begin[i]
+// is <= t, in the ascending array begin[0..n) (begin[0] == 0). The array is
+// compact (8 bytes per segment), so the search stays in L1 after the first
+// CTAs of an SM touched it.
+__device__ __forceinline__ int find_segment(const int64_t* __restrict__ begin, int n, int64_t t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(begin + mid) <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));

@@ -205,14 +205,10 @@ struct PackJob {
 };
 
 template <typename Tin, typename Tout, int LAYOUT>
-__global__ void __launch_bounds__(256) pack_group_kernel(const PackJob* jobs, int n_jobs) {
+__global__ void __launch_bounds__(256) pack_group_kernel(const PackJob* jobs, const int64_t* begin,
+                                                         int n_jobs) {
   const int64_t t = blockIdx.x + (int64_t)gridDim.x * blockIdx.y;
-  int lo = 0, hi = n_jobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].begin <= t) lo = mid; else hi = mid - 1;
-  }
-  const PackJob& j = jobs[lo];
+  const PackJob& j = jobs[find_segment(begin, n_jobs, t)];
   const int64_t local = t - j.begin;
   pack_any<Tin, Tout, LAYOUT>(j.op, local % j.ktiles, local / j.ktiles);
 }

@@ -376,14 +376,10 @@ struct SimtGroupItem {
 
 template <typename T>
 __global__ void __launch_bounds__(256, 2) simt_gett_group_kernel(const SimtGroupItem<T>* items,
+                                                                  const int64_t* begin,
                                                                   int n_items) {
   const int64_t t = blockIdx.x;
-  int lo = 0, hi = n_items - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (items[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
-  }
-  const SimtGroupItem<T>& it = items[lo];
+  const SimtGroupItem<T>& it = items[find_segment(begin, n_items, t)];
   const int64_t local = t - it.tile_begin;
   const int64_t mn = (int64_t)it.tiles_m * it.tiles_n;
   const int64_t rem = local % mn;
@@ -430,14 +426,10 @@ struct ReduceJob {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) reduce_group_kernel(const ReduceJob<T>* jobs, int n_jobs) {
+__global__ void __launch_bounds__(256) reduce_group_kernel(const ReduceJob<T>* jobs,
+                                                           const int64_t* begin, int n_jobs) {
   const int64_t t = blockIdx.x;
-  int lo = 0, hi = n_jobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].begin <= t) lo = mid; else hi = mid - 1;
-  }
-  const ReduceJob<T>& j = jobs[lo];
+  const ReduceJob<T>& j = jobs[find_segment(begin, n_jobs, t)];
   const int64_t local = t - j.begin;
   const int64_t m = (local % j.mblocks) * 256 + threadIdx.x;
   if (m >= j.M) return;

@@ -90,6 +90,7 @@ struct __align__(64) TcGroupItem {
 
 struct TcGroup {
   const TcGroupItem* items;
+  const int64_t* tile_begin;  // items[i].tile_begin, compact, for the tile search
   int32_t n_items;
   int32_t total_tiles;
 };
@@ -133,12 +134,7 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
                                                 const TcGroup& g) {
   TileRef r;
   if constexpr (GROUPED) {
-    int lo = 0, hi = g.n_items - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (g.items[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
-    }
-    const TcGroupItem& it = g.items[lo];
+    const TcGroupItem& it = g.items[find_segment(g.tile_begin, g.n_items, tile)];
     r.a = &it.args;
     r.tA = &it.tmA;
     r.tB = &it.tmB;
@@ -438,7 +434,7 @@ template <int MODE>
 __global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
     gett_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                    const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
-  TcGroup g{nullptr, 0, 0};
+  TcGroup g{nullptr, nullptr, 0, 0};
   gett_tc_body<MODE, false>(&tmA, &tmB, &a, g, a.status);
 }
 

@@ -1023,6 +1023,11 @@ struct tccg_group {
   int32_t* tc_status = nullptr;
   // k-split reductions: ReduceJob<T>[] (same T as the CUDA-core lane)
   void* d_reduce = nullptr;
+  // compact first-CTA / first-tile arrays of the jobs and items above (one
+  // allocation): what the kernels binary-search instead of the large structs
+  int64_t* d_begin = nullptr;
+  int64_t *b_simt_jobs = nullptr, *b_tc_jobs = nullptr, *b_simt_items = nullptr,
+          *b_tc_items = nullptr, *b_reduce = nullptr;
   int32_t n_reduce = 0;
   int64_t reduce_ctas = 0;
   bool bound = false;
@@ -1030,7 +1035,7 @@ struct tccg_group {
 
 static void group_free(tccg_group* g) {
   if (!g) return;
-  void* ps[] = {g->d_simt, g->d_simt_jobs, g->d_tc, g->d_tc_jobs, g->d_reduce};
+  void* ps[] = {g->d_simt, g->d_simt_jobs, g->d_tc, g->d_tc_jobs, g->d_reduce, g->d_begin};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete g;
@@ -1087,6 +1092,14 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_tc_jobs, sizeof(PackJob) * 2 * g->n_tc);
   }
   if (e == cudaSuccess) e = cudaMalloc(&g->d_reduce, sizeof(ReduceJob<double>) * count);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_begin, sizeof(int64_t) * 4 * count);
+  if (e == cudaSuccess) {
+    g->b_simt_jobs = g->d_begin;
+    g->b_tc_jobs = g->b_simt_jobs + 2 * g->n_simt;
+    g->b_simt_items = g->b_tc_jobs + 2 * g->n_tc;
+    g->b_tc_items = g->b_simt_items + g->n_simt;
+    g->b_reduce = g->b_tc_items + g->n_tc;
+  }
   if (e != cudaSuccess) {
     group_free(g);
     return fail(TCCG_ERR_CUDA, "group tables: %s", cudaGetErrorString(e));
@@ -1171,6 +1184,16 @@ static std::vector<size_t> by_tile_cost(const tccg_group* g, bool simt) {
   return idx;
 }
 
+// Uploads the `begin` fields of `v` as a compact int64 array.
+template <typename V, typename F>
+static int upload_begins(const std::vector<V>& v, F field, int64_t* dst) {
+  if (v.empty()) return TCCG_OK;
+  std::vector<int64_t> b(v.size());
+  for (size_t i = 0; i < v.size(); ++i) b[i] = field(v[i]);
+  CUDA_TRY(cudaMemcpy(dst, b.data(), sizeof(int64_t) * b.size(), cudaMemcpyHostToDevice));
+  return TCCG_OK;
+}
+
 // Two pack jobs (A, B) of one item; a direct item's jobs own no CTAs.
 static void add_pack_jobs(std::vector<PackJob>& jobs, int64_t& ctas, const PackOperand& oa,
                           const PackOperand& ob, int ktile, bool active) {
@@ -1220,6 +1243,9 @@ static int bind_simt(tccg_group* g, const void* const* A, const void* const* B, 
   if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
   CUDA_TRY(cudaMemcpy(g->d_simt, items.data(), sizeof(items[0]) * items.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(g->d_simt_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
+  int rc = upload_begins(items, [](const SimtGroupItem<T>& x) { return x.tile_begin; }, g->b_simt_items);
+  if (!rc) rc = upload_begins(jobs, [](const PackJob& x) { return x.begin; }, g->b_simt_jobs);
+  if (rc) return rc;
   g->simt_pack_ctas = pctas;
   return TCCG_OK;
 }
@@ -1278,6 +1304,9 @@ static int bind_tc(tccg_group* g, const void* const* A, const void* const* B, vo
   if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
   CUDA_TRY(cudaMemcpy(g->d_tc, items.data(), sizeof(items[0]) * items.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(g->d_tc_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
+  int rc2 = upload_begins(items, [](const TcGroupItem& x) { return x.tile_begin; }, g->b_tc_items);
+  if (!rc2) rc2 = upload_begins(jobs, [](const PackJob& x) { return x.begin; }, g->b_tc_jobs);
+  if (rc2) return rc2;
   g->tc_pack_ctas = pctas;
   return TCCG_OK;
 }
@@ -1301,6 +1330,8 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     if ((rc = bind_simt<double>(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
     if (!red.empty())
       CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
+    if ((rc = upload_begins(red, [](const ReduceJob<double>& x) { return x.begin; }, g->b_reduce)))
+      return rc;
     nred = red.size();
   } else {
     std::vector<ReduceJob<float>> red;
@@ -1308,6 +1339,8 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     if ((rc = bind_tc(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
     if (!red.empty())
       CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
+    if ((rc = upload_begins(red, [](const ReduceJob<float>& x) { return x.begin; }, g->b_reduce)))
+      return rc;
     nred = red.size();
   }
   if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
@@ -1324,7 +1357,7 @@ template <typename T>
 static int group_reduce(const tccg_group* g, cudaStream_t s) {
   if (g->n_reduce == 0) return TCCG_OK;
   reduce_group_kernel<T><<<(unsigned)g->reduce_ctas, 256, 0, s>>>(
-      static_cast<const ReduceJob<T>*>(g->d_reduce), g->n_reduce);
+      static_cast<const ReduceJob<T>*>(g->d_reduce), g->b_reduce, g->n_reduce);
   return launch_check("reduce_group");
 }
 
@@ -1340,38 +1373,39 @@ extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
   if (g->simt_pack_ctas > 0) {
     const dim3 pg((unsigned)g->simt_pack_ctas);
     if (g->prec == TCCG_PREC_FP64)
-      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
     else if (g->dtype == TCCG_BF16)
-      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
     else if (g->prec == TCCG_PREC_BF16)
-      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
     else
-      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, sj);
+      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
     if ((rc = launch_check("pack_group"))) return rc;
   }
   const bool x3 = g->prec == TCCG_PREC_BF16X3;
   if (g->tc_pack_ctas > 0) {
     const dim3 pg((unsigned)g->tc_pack_ctas);
     if (x3)
-      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pg, blk, 0, s>>>(g->d_tc_jobs, tj);
+      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pg, blk, 0, s>>>(g->d_tc_jobs, g->b_tc_jobs, tj);
     else if (g->dtype == TCCG_BF16)
-      pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, tj);
+      pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, g->b_tc_jobs, tj);
     else
-      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, tj);
+      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, g->b_tc_jobs, tj);
     if ((rc = launch_check("pack_group"))) return rc;
   }
   if (g->n_simt > 0) {
     if (g->prec == TCCG_PREC_FP64)
       simt_gett_group_kernel<double><<<(unsigned)g->simt_tiles, 256, simt_smem_bytes<double>(), s>>>(
-          static_cast<const SimtGroupItem<double>*>(g->d_simt), g->n_simt);
+          static_cast<const SimtGroupItem<double>*>(g->d_simt), g->b_simt_items, g->n_simt);
     else
       simt_gett_group_kernel<float><<<(unsigned)g->simt_tiles, 256, simt_smem_bytes<float>(), s>>>(
-          static_cast<const SimtGroupItem<float>*>(g->d_simt), g->n_simt);
+          static_cast<const SimtGroupItem<float>*>(g->d_simt), g->b_simt_items, g->n_simt);
     if ((rc = launch_check("simt_gett_group"))) return rc;
   }
   if (g->n_tc > 0) {
     TcGroup tg;
     tg.items = g->d_tc;
+    tg.tile_begin = g->b_tc_items;
     tg.n_items = g->n_tc;
     tg.total_tiles = (int32_t)g->tc_tiles;
     const unsigned grid = (unsigned)std::min<int64_t>(g->tc_tiles, g->num_sms);
