@@ -1005,21 +1005,17 @@ struct tccg_group {
   std::vector<const tccg_plan*> plans;
   int32_t prec = 0, dtype = 0;
   int device = 0, num_sms = 148;
-  std::vector<size_t> ws_off;  // per item: start of its workspace
+  std::vector<size_t> ws_off;  // per item: start of its workspace within its wave's region
   size_t ws_bytes = 0;
   // CUDA-core lane (FP32/FP64 groups, and BF16-precision items that plan for
   // the CUDA cores): SimtGroupItem<T>[], T = double for FP64 groups else float
   void* d_simt = nullptr;
   int32_t n_simt = 0;
-  int64_t simt_tiles = 0;
   PackJob* d_simt_jobs = nullptr;
-  int64_t simt_pack_ctas = 0;
   // tensor-core lane (BF16 / BF16X3 groups)
   TcGroupItem* d_tc = nullptr;
   int32_t n_tc = 0;
-  int64_t tc_tiles = 0;
   PackJob* d_tc_jobs = nullptr;
-  int64_t tc_pack_ctas = 0;
   int32_t* tc_status = nullptr;
   // k-split reductions: ReduceJob<T>[] (same T as the CUDA-core lane)
   void* d_reduce = nullptr;
@@ -1028,10 +1024,26 @@ struct tccg_group {
   int64_t* d_begin = nullptr;
   int64_t *b_simt_jobs = nullptr, *b_tc_jobs = nullptr, *b_simt_items = nullptr,
           *b_tc_items = nullptr, *b_reduce = nullptr;
-  int32_t n_reduce = 0;
-  int64_t reduce_ctas = 0;
+  // Waves: the items run in sets whose workspaces together stay within
+  // kGroupWaveBytes (an item above it is a set of its own). Each wave is
+  // packed and multiplied before the next one reuses the same workspace
+  // region, so the group's workspace is that of its largest wave, not the sum
+  // over its items. On the 256-item batched workload 4 GiB waves take the
+  // time of one wave (22.0 vs 22.1 ms BF16x3) with 4.0 instead of 12.8 GiB of
+  // workspace; 512 MiB waves cost 8 % more time (more, shorter launches).
+  struct Wave {
+    std::vector<size_t> items;  // plan indices
+    int32_t simt0 = 0, n_simt = 0, tc0 = 0, n_tc = 0, red0 = 0, n_red = 0;
+    int64_t simt_tiles = 0, tc_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0, red_ctas = 0;
+  };
+  std::vector<Wave> waves;
   bool bound = false;
 };
+
+#ifndef TCCG_GROUP_WAVE_MB
+#define TCCG_GROUP_WAVE_MB 4096
+#endif
+static constexpr size_t kGroupWaveBytes = size_t(TCCG_GROUP_WAVE_MB) << 20;
 
 static void group_free(tccg_group* g) {
   if (!g) return;
@@ -1063,24 +1075,44 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
       return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without the CTA-pair kernel (plan %d)", i);
     }
     g->plans.push_back(p);
-    g->ws_off.push_back(ws);
-    ws = align_up(ws + p->ws_bytes, 256);
     if (simt_path(p)) {
-      const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
-      const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
-      g->simt_tiles += (p->Mp / BM) * (p->Np / BN) * p->ksplit;
       ++g->n_simt;
     } else {
-      g->tc_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
       if (!g->tc_status) g->tc_status = p->d_status;
       ++g->n_tc;
     }
   }
-  if (g->simt_tiles > INT32_MAX || g->tc_tiles > INT32_MAX) {
-    group_free(g);
-    return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
+  // waves, largest workspaces first (next fit under kGroupWaveBytes)
+  std::vector<size_t> order(count);
+  for (int i = 0; i < count; ++i) order[i] = (size_t)i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    return g->plans[a]->ws_bytes > g->plans[b]->ws_bytes;
+  });
+  g->ws_off.assign(count, 0);
+  for (size_t i : order) {
+    const tccg_plan* p = g->plans[i];
+    const size_t need = align_up(p->ws_bytes, 256);
+    if (g->waves.empty() || ws + need > kGroupWaveBytes) {
+      g->waves.emplace_back();
+      ws = 0;
+    }
+    tccg_group::Wave& wv = g->waves.back();
+    wv.items.push_back(i);
+    g->ws_off[i] = ws;
+    ws += need;
+    g->ws_bytes = std::max(g->ws_bytes, ws);
+    if (simt_path(p)) {
+      const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
+      const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+      wv.simt_tiles += (p->Mp / BM) * (p->Np / BN) * p->ksplit;
+    } else {
+      wv.tc_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
+    }
+    if (wv.simt_tiles > INT32_MAX || wv.tc_tiles > INT32_MAX) {
+      group_free(g);
+      return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
+    }
   }
-  g->ws_bytes = ws;
   const size_t simt_item = dbl ? sizeof(SimtGroupItem<double>) : sizeof(SimtGroupItem<float>);
   cudaError_t e = cudaSuccess;
   if (g->n_simt) {
@@ -1172,9 +1204,9 @@ static int64_t reduce_ctas(const ReduceJob<T>& j) {
 // index order (round robin in the persistent tensor-core kernel, launch order
 // in the CUDA-core one), so the longest tiles start first and the short ones
 // fill in behind them.
-static std::vector<size_t> by_tile_cost(const tccg_group* g, bool simt) {
+static std::vector<size_t> by_tile_cost(const tccg_group* g, const tccg_group::Wave& wv, bool simt) {
   std::vector<size_t> idx;
-  for (size_t i = 0; i < g->plans.size(); ++i)
+  for (size_t i : wv.items)
     if (simt_path(g->plans[i]) == simt) idx.push_back(i);
   auto cost = [&](size_t i) {
     const tccg_plan* p = g->plans[i];
@@ -1207,15 +1239,17 @@ static void add_pack_jobs(std::vector<PackJob>& jobs, int64_t& ctas, const PackO
   }
 }
 
-// The CUDA-core lane of a bind; T = the lane's element type.
+// The CUDA-core lane of one wave of a bind, appended to `items` / `jobs` /
+// `red` (first CTAs and tiles counted from 0 within the wave); T = the lane's
+// element type.
 template <typename T>
-static int bind_simt(tccg_group* g, const void* const* A, const void* const* B, void* const* C,
-                     const double* alpha, const double* beta, char* ws,
-                     std::vector<ReduceJob<T>>& red, int64_t& rctas) {
-  std::vector<SimtGroupItem<T>> items;
-  std::vector<PackJob> jobs;
+static int bind_simt(tccg_group* g, tccg_group::Wave& wv, const void* const* A,
+                     const void* const* B, void* const* C, const double* alpha,
+                     const double* beta, char* ws, std::vector<SimtGroupItem<T>>& items,
+                     std::vector<PackJob>& jobs, std::vector<ReduceJob<T>>& red, int64_t& rctas) {
+  wv.simt0 = (int32_t)items.size();
   int64_t tile = 0, pctas = 0;
-  for (size_t i : by_tile_cost(g, true)) {
+  for (size_t i : by_tile_cost(g, wv, true)) {
     const tccg_plan* p = g->plans[i];
     char* w = ws + g->ws_off[i];
     const void* GA = p->d.swap_ab ? B[i] : A[i];
@@ -1239,24 +1273,19 @@ static int bind_simt(tccg_group* g, const void* const* A, const void* const* B, 
       rctas += reduce_ctas(red.back());
     }
   }
-  if (items.empty()) return TCCG_OK;
   if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
-  CUDA_TRY(cudaMemcpy(g->d_simt, items.data(), sizeof(items[0]) * items.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(g->d_simt_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
-  int rc = upload_begins(items, [](const SimtGroupItem<T>& x) { return x.tile_begin; }, g->b_simt_items);
-  if (!rc) rc = upload_begins(jobs, [](const PackJob& x) { return x.begin; }, g->b_simt_jobs);
-  if (rc) return rc;
-  g->simt_pack_ctas = pctas;
+  wv.n_simt = (int32_t)items.size() - wv.simt0;
+  wv.simt_pack_ctas = pctas;
   return TCCG_OK;
 }
 
-static int bind_tc(tccg_group* g, const void* const* A, const void* const* B, void* const* C,
-                   const double* alpha, const double* beta, char* ws,
+static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, const void* const* B,
+                   void* const* C, const double* alpha, const double* beta, char* ws,
+                   std::vector<TcGroupItem>& items, std::vector<PackJob>& jobs,
                    std::vector<ReduceJob<float>>& red, int64_t& rctas) {
-  std::vector<TcGroupItem> items;
-  std::vector<PackJob> jobs;
+  wv.tc0 = (int32_t)items.size();
   int64_t tile = 0, pctas = 0;
-  for (size_t i : by_tile_cost(g, false)) {
+  for (size_t i : by_tile_cost(g, wv, false)) {
     const tccg_plan* p = g->plans[i];
     char* w = ws + g->ws_off[i];
     const void* GA = p->d.swap_ab ? B[i] : A[i];
@@ -1300,14 +1329,9 @@ static int bind_tc(tccg_group* g, const void* const* A, const void* const* B, vo
       rctas += reduce_ctas(red.back());
     }
   }
-  if (items.empty()) return TCCG_OK;
   if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
-  CUDA_TRY(cudaMemcpy(g->d_tc, items.data(), sizeof(items[0]) * items.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(g->d_tc_jobs, jobs.data(), sizeof(PackJob) * jobs.size(), cudaMemcpyHostToDevice));
-  int rc2 = upload_begins(items, [](const TcGroupItem& x) { return x.tile_begin; }, g->b_tc_items);
-  if (!rc2) rc2 = upload_begins(jobs, [](const PackJob& x) { return x.begin; }, g->b_tc_jobs);
-  if (rc2) return rc2;
-  g->tc_pack_ctas = pctas;
+  wv.n_tc = (int32_t)items.size() - wv.tc0;
+  wv.tc_pack_ctas = pctas;
   return TCCG_OK;
 }
 
@@ -1322,93 +1346,112 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     if (!A[i] || !B[i] || !C[i]) return fail(TCCG_ERR_INVALID, "null operand pointer for item %zu", i);
   g->bound = false;
   char* w = static_cast<char*>(ws);
-  int64_t rctas = 0;
   int rc;
-  size_t nred = 0;
+  // all waves' items, jobs and reductions in one array per kind, wave after
+  // wave; each wave's kernels see their slice (first CTAs from 0)
+  auto bind_all = [&](auto tag, auto& simt_items, auto& red) -> int {
+    using T = decltype(tag);
+    std::vector<PackJob> sjobs, tjobs;
+    std::vector<TcGroupItem> titems;
+    int r = TCCG_OK;
+    for (tccg_group::Wave& wv : g->waves) {
+      int64_t rctas = 0;
+      wv.red0 = (int32_t)red.size();
+      r = bind_simt<T>(g, wv, A, B, C, alpha, beta, w, simt_items, sjobs, red, rctas);
+      if (r) return r;
+      if constexpr (sizeof(T) == 4) {
+        r = bind_tc(g, wv, A, B, C, alpha, beta, w, titems, tjobs, red, rctas);
+        if (r) return r;
+      }
+      if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
+      wv.n_red = (int32_t)red.size() - wv.red0;
+      wv.red_ctas = rctas;
+    }
+    if (!simt_items.empty()) {
+      CUDA_TRY(cudaMemcpy(g->d_simt, simt_items.data(), sizeof(simt_items[0]) * simt_items.size(),
+                          cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(g->d_simt_jobs, sjobs.data(), sizeof(PackJob) * sjobs.size(),
+                          cudaMemcpyHostToDevice));
+    }
+    if (!titems.empty()) {
+      CUDA_TRY(cudaMemcpy(g->d_tc, titems.data(), sizeof(TcGroupItem) * titems.size(),
+                          cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(g->d_tc_jobs, tjobs.data(), sizeof(PackJob) * tjobs.size(),
+                          cudaMemcpyHostToDevice));
+    }
+    if (!red.empty())
+      CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
+    auto item_begin = [](const auto& x) { return x.tile_begin; };
+    auto job_begin = [](const auto& x) { return x.begin; };
+    r = upload_begins(simt_items, item_begin, g->b_simt_items);
+    if (!r) r = upload_begins(sjobs, job_begin, g->b_simt_jobs);
+    if (!r) r = upload_begins(titems, item_begin, g->b_tc_items);
+    if (!r) r = upload_begins(tjobs, job_begin, g->b_tc_jobs);
+    if (!r) r = upload_begins(red, job_begin, g->b_reduce);
+    return r;
+  };
   if (g->prec == TCCG_PREC_FP64) {
+    std::vector<SimtGroupItem<double>> items;
     std::vector<ReduceJob<double>> red;
-    if ((rc = bind_simt<double>(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
-    if (!red.empty())
-      CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
-    if ((rc = upload_begins(red, [](const ReduceJob<double>& x) { return x.begin; }, g->b_reduce)))
-      return rc;
-    nred = red.size();
+    rc = bind_all(double(0), items, red);
   } else {
+    std::vector<SimtGroupItem<float>> items;
     std::vector<ReduceJob<float>> red;
-    if ((rc = bind_simt<float>(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
-    if ((rc = bind_tc(g, A, B, C, alpha, beta, w, red, rctas))) return rc;
-    if (!red.empty())
-      CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
-    if ((rc = upload_begins(red, [](const ReduceJob<float>& x) { return x.begin; }, g->b_reduce)))
-      return rc;
-    nred = red.size();
+    rc = bind_all(float(0), items, red);
   }
-  if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
-  g->n_reduce = (int32_t)nred;
-  g->reduce_ctas = rctas;
+  if (rc) return rc;
   g->bound = true;
   return TCCG_OK;
 }
 
-// Launches of a group run, in order: packing (CUDA-core lane, tensor-core
-// lane), the two grouped GETT kernels, and the k-split reduction -- each only
-// when it has work.
+// Launches of a group run, wave by wave: packing (CUDA-core lane,
+// tensor-core lane), the two grouped GETT kernels and the k-split reduction
+// -- each only when the wave has work for it.
 template <typename T>
-static int group_reduce(const tccg_group* g, cudaStream_t s) {
-  if (g->n_reduce == 0) return TCCG_OK;
-  reduce_group_kernel<T><<<(unsigned)g->reduce_ctas, 256, 0, s>>>(
-      static_cast<const ReduceJob<T>*>(g->d_reduce), g->b_reduce, g->n_reduce);
-  return launch_check("reduce_group");
-}
-
-extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
-  if (!g) return fail(TCCG_ERR_INVALID, "null group");
-  if (!g->bound) return fail(TCCG_ERR_INVALID, "tccg_group_bind must be called before tccg_group_run");
-  int rc = ensure_attrs();
-  if (rc) return rc;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int sj = 2 * g->n_simt, tj = 2 * g->n_tc;
+static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_t s) {
+  int rc;
   const dim3 blk(32, 8);
-  // CUDA-core lane packing (layout by precision and operand type)
-  if (g->simt_pack_ctas > 0) {
-    const dim3 pg((unsigned)g->simt_pack_ctas);
+  const int sj = 2 * wv.n_simt, tj = 2 * wv.n_tc;
+  const PackJob* sjobs = g->d_simt_jobs + 2 * wv.simt0;
+  const int64_t* sb = g->b_simt_jobs + 2 * wv.simt0;
+  if (wv.simt_pack_ctas > 0) {
+    const dim3 pg((unsigned)wv.simt_pack_ctas);
     if (g->prec == TCCG_PREC_FP64)
-      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
+      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s>>>(sjobs, sb, sj);
     else if (g->dtype == TCCG_BF16)
-      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
+      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s>>>(sjobs, sb, sj);
     else if (g->prec == TCCG_PREC_BF16)
-      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
+      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s>>>(sjobs, sb, sj);
     else
-      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s>>>(g->d_simt_jobs, g->b_simt_jobs, sj);
+      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s>>>(sjobs, sb, sj);
     if ((rc = launch_check("pack_group"))) return rc;
   }
   const bool x3 = g->prec == TCCG_PREC_BF16X3;
-  if (g->tc_pack_ctas > 0) {
-    const dim3 pg((unsigned)g->tc_pack_ctas);
+  const PackJob* tjobs = g->d_tc_jobs + 2 * wv.tc0;
+  const int64_t* tb = g->b_tc_jobs + 2 * wv.tc0;
+  if (wv.tc_pack_ctas > 0) {
+    const dim3 pg((unsigned)wv.tc_pack_ctas);
     if (x3)
-      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pg, blk, 0, s>>>(g->d_tc_jobs, g->b_tc_jobs, tj);
+      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16X3><<<pg, blk, 0, s>>>(tjobs, tb, tj);
     else if (g->dtype == TCCG_BF16)
-      pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, g->b_tc_jobs, tj);
+      pack_group_kernel<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(tjobs, tb, tj);
     else
-      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(g->d_tc_jobs, g->b_tc_jobs, tj);
+      pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(tjobs, tb, tj);
     if ((rc = launch_check("pack_group"))) return rc;
   }
-  if (g->n_simt > 0) {
-    if (g->prec == TCCG_PREC_FP64)
-      simt_gett_group_kernel<double><<<(unsigned)g->simt_tiles, 256, simt_smem_bytes<double>(), s>>>(
-          static_cast<const SimtGroupItem<double>*>(g->d_simt), g->b_simt_items, g->n_simt);
-    else
-      simt_gett_group_kernel<float><<<(unsigned)g->simt_tiles, 256, simt_smem_bytes<float>(), s>>>(
-          static_cast<const SimtGroupItem<float>*>(g->d_simt), g->b_simt_items, g->n_simt);
+  if (wv.n_simt > 0) {
+    simt_gett_group_kernel<T><<<(unsigned)wv.simt_tiles, 256, simt_smem_bytes<T>(), s>>>(
+        static_cast<const SimtGroupItem<T>*>(g->d_simt) + wv.simt0, g->b_simt_items + wv.simt0,
+        wv.n_simt);
     if ((rc = launch_check("simt_gett_group"))) return rc;
   }
-  if (g->n_tc > 0) {
+  if (wv.n_tc > 0) {
     TcGroup tg;
-    tg.items = g->d_tc;
-    tg.tile_begin = g->b_tc_items;
-    tg.n_items = g->n_tc;
-    tg.total_tiles = (int32_t)g->tc_tiles;
-    const unsigned grid = (unsigned)std::min<int64_t>(g->tc_tiles, g->num_sms);
+    tg.items = g->d_tc + wv.tc0;
+    tg.tile_begin = g->b_tc_items + wv.tc0;
+    tg.n_items = wv.n_tc;
+    tg.total_tiles = (int32_t)wv.tc_tiles;
+    const unsigned grid = (unsigned)std::min<int64_t>(wv.tc_tiles, g->num_sms);
     if (x3)
       gett_tc_group_kernel<TC_BF16X3><<<grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
                                         TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tg, g->tc_status);
@@ -1417,7 +1460,25 @@ extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
                                       TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, g->tc_status);
     if ((rc = launch_check("gett_tc_group"))) return rc;
   }
-  return g->prec == TCCG_PREC_FP64 ? group_reduce<double>(g, s) : group_reduce<float>(g, s);
+  if (wv.n_red > 0) {
+    reduce_group_kernel<T><<<(unsigned)wv.red_ctas, 256, 0, s>>>(
+        static_cast<const ReduceJob<T>*>(g->d_reduce) + wv.red0, g->b_reduce + wv.red0, wv.n_red);
+    if ((rc = launch_check("reduce_group"))) return rc;
+  }
+  return TCCG_OK;
+}
+
+extern "C" int tccg_group_run(const tccg_group* g, void* stream) {
+  if (!g) return fail(TCCG_ERR_INVALID, "null group");
+  if (!g->bound) return fail(TCCG_ERR_INVALID, "tccg_group_bind must be called before tccg_group_run");
+  int rc = ensure_attrs();
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  for (const tccg_group::Wave& wv : g->waves) {
+    rc = g->prec == TCCG_PREC_FP64 ? run_wave<double>(g, wv, s) : run_wave<float>(g, wv, s);
+    if (rc) return rc;
+  }
+  return TCCG_OK;
 }
 
 extern "C" int tccg_group_destroy(tccg_group* g) {

@@ -2,11 +2,16 @@
 (new in this build; TCCG has one function per contraction).
 
 ``Group([con...], precision)`` creates one native plan per contraction and a
-native group. ``bind(As, Bs, Cs)`` fixes the operand pointers and the
-workspace (uploading the device work list once); after that ``run()`` issues
-exactly two kernel launches (grouped packing + grouped GETT) and
-``capture()`` records them into a CUDA graph that ``replay()`` re-launches.
-``run_per_item()`` is the baseline: one tccg_plan_run per contraction.
+native group. The items run in waves whose workspaces together fit a 4 GiB
+region (an item above that is a wave of its own): each wave is packed and
+multiplied before the next reuses the region, so the group's workspace is
+that of its largest wave rather than the sum over all items.
+``bind(As, Bs, Cs)`` fixes the operand pointers and the workspace (uploading
+the device work lists once); after that ``run()`` issues, per wave, the
+grouped packing, the grouped GETT kernels (CUDA-core and tensor-core lanes)
+and the k-split reduction that have work, and ``capture()`` records them into
+a CUDA graph that ``replay()`` re-launches. ``run_per_item()`` is the
+baseline: one tccg_plan_run per contraction.
 """
 from __future__ import annotations
 
@@ -69,7 +74,7 @@ class Group:
         N.check(self._lib.tccg_group_run(self._h, ctypes.c_void_p(s.cuda_stream)))
 
     def capture(self):
-        """Record run() into a CUDA graph (two kernel nodes)."""
+        """Record run() into a CUDA graph."""
         import torch
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(device=self._bound[2][0].device)
