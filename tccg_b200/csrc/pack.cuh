@@ -208,7 +208,9 @@ template <typename Tin, typename Tout, int LAYOUT>
 __global__ void __launch_bounds__(256) pack_group_kernel(const PackJob* jobs, const int64_t* begin,
                                                          int n_jobs) {
   const int64_t t = blockIdx.x + (int64_t)gridDim.x * blockIdx.y;
-  const PackJob& j = jobs[find_segment(begin, n_jobs, t)];
+  // the job's fields by value: loaded together up front instead of one
+  // dependent global load at a time inside the tile code
+  const PackJob j = jobs[find_segment(begin, n_jobs, t)];
   const int64_t local = t - j.begin;
   pack_any<Tin, Tout, LAYOUT>(j.op, local % j.ktiles, local / j.ktiles);
 }

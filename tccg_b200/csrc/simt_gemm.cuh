@@ -429,7 +429,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) reduce_group_kernel(const ReduceJob<T>* jobs,
                                                            const int64_t* begin, int n_jobs) {
   const int64_t t = blockIdx.x;
-  const ReduceJob<T>& j = jobs[find_segment(begin, n_jobs, t)];
+  const ReduceJob<T> j = jobs[find_segment(begin, n_jobs, t)];  // fields loaded up front
   const int64_t local = t - j.begin;
   const int64_t m = (local % j.mblocks) * 256 + threadIdx.x;
   if (m >= j.M) return;

@@ -1190,8 +1190,8 @@ static ReduceJob<T> reduce_job_for(const T* partial, int32_t splits, int64_t Mp,
   j.begin = begin;
   j.splits = splits;
   j.mblocks = (int32_t)cdiv(p->M, 256);
-  // about 2048 loads per thread: many slices -> few columns per CTA
-  j.ncols = (int32_t)std::max<int64_t>(1, std::min<int64_t>(64, 2048 / splits));
+  // about 256 loads per thread: many slices -> few columns per CTA
+  j.ncols = (int32_t)std::max<int64_t>(1, std::min<int64_t>(64, 256 / splits));
   return j;
 }
 
