@@ -199,11 +199,13 @@ int tccg_transpose(int32_t dtype, int32_t dim, const int32_t* perm, const int64_
                    double beta, void* B, void* stream);
 
 /*
- * Grouped launch: many plans of the same precision run by ONE persistent
- * kernel launch (plus one packing launch). tccg_group_bind fixes the operand
- * pointers and workspace (it uploads the work list, synchronously), after
- * which tccg_group_run only launches kernels and can be captured in a CUDA
- * graph.
+ * Grouped launch: many plans of the same precision run by a few launches per
+ * wave (waves of at most 4 GiB of workspace): grouped packing, one grouped
+ * GETT kernel per kernel family (CUDA cores, tcgen05 persistent) and the
+ * grouped k-split reduction, each only when it has work. tccg_group_bind fixes
+ * the operand pointers and workspace (it uploads the work lists,
+ * synchronously), after which tccg_group_run only launches kernels and can be
+ * captured in a CUDA graph.
  */
 typedef struct tccg_group tccg_group; /* opaque */
 int tccg_group_create(const tccg_plan* const* plans, int32_t count, tccg_group** out);

@@ -917,42 +917,85 @@ extern "C" int tccg_plan_run_timed(const tccg_plan* p, const void* A, const void
 static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s) {
   PermArgs pa = pa0;
   if (pa.dim < 1 || pa.dim > PERM_MAX_DIMS) return fail(TCCG_ERR_INVALID, "bad dimension count");
-  // put the output dim with the smallest B stride first
+  // drop unit extents, then fuse neighbouring output dims that are contiguous
+  // in both tensors (fewer, longer dims: longer coalesced runs, less decoding)
+  int n = 0;
+  for (int d = 0; d < pa.dim; ++d) {
+    if (pa.ext[d] == 1) continue;
+    if (n > 0 && pa.sa[d] == pa.sa[n - 1] * pa.ext[n - 1] && pa.sb[d] == pa.sb[n - 1] * pa.ext[n - 1]) {
+      pa.ext[n - 1] *= pa.ext[d];
+      continue;
+    }
+    pa.ext[n] = pa.ext[d];
+    pa.sa[n] = pa.sa[d];
+    pa.sb[n] = pa.sb[d];
+    ++n;
+  }
+  if (n == 0) {  // a single element
+    pa.ext[0] = 1;
+    pa.sa[0] = pa.sb[0] = 1;
+    n = 1;
+  }
+  pa.dim = n;
+  // the output dim with the smallest B stride first
   int b0 = 0;
   for (int d = 1; d < pa.dim; ++d)
-    if (pa.sb[d] < pa.sb[b0]) b0 = d;
+    if (std::llabs(pa.sb[d]) < std::llabs(pa.sb[b0])) b0 = d;
   std::swap(pa.ext[0], pa.ext[b0]);
   std::swap(pa.sa[0], pa.sa[b0]);
   std::swap(pa.sb[0], pa.sb[b0]);
   int da = 0;
   for (int d = 1; d < pa.dim; ++d)
-    if (pa.sa[d] < pa.sa[da]) da = d;
-  if (pa.sa[da] == pa.sa[0]) da = 0;
+    if (std::llabs(pa.sa[d]) < std::llabs(pa.sa[da])) da = d;
+  if (std::llabs(pa.sa[da]) == std::llabs(pa.sa[0])) da = 0;
   pa.da = da;
   int64_t rest = 1;
   for (int d = 1; d < pa.dim; ++d)
     if (d != da) rest *= pa.ext[d];
   pa.rest = rest;
-  dim3 grid;
+  // tile edge: 64 unless that pads dim 0 x dim da by more than 5 % over 32
+  const auto padded = [&](int64_t t) {
+    return (double)(cdiv(pa.ext[0], t) * t) * (double)(cdiv(pa.ext[da], t) * t);
+  };
+  const bool t64 = da != 0 && padded(64) <= 1.05 * padded(32);
+  const int te = t64 ? 64 : 32, rows = t64 ? 1 : 4;
+  const bool along0 = !t64 && rest < 64;  // few rows: group tiles along dim 0 instead
   if (da == 0) {
-    pa.nt0 = cdiv(pa.ext[0], 256);
+    pa.nt0 = cdiv(pa.ext[0], 256 * PERM_STREAM);
     pa.nta = 1;
-    grid.x = (unsigned)pa.nt0;
   } else {
-    pa.nt0 = cdiv(pa.ext[0], 32);
-    pa.nta = cdiv(pa.ext[da], 32);
-    if (pa.nt0 * pa.nta > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "transpose too large");
-    grid.x = (unsigned)(pa.nt0 * pa.nta);
+    pa.nt0 = cdiv(pa.ext[0], (int64_t)te * (along0 ? rows : 1));
+    pa.nta = cdiv(pa.ext[da], te);
   }
-  grid.y = (unsigned)std::min<int64_t>(rest, 65535);
-  grid.z = (unsigned)std::min<int64_t>(cdiv(rest, grid.y), 1024);
+  if (pa.nt0 * pa.nta > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "transpose too large");
+  const int64_t groups = (da == 0 || along0) ? rest : cdiv(rest, rows);
+  dim3 grid;
+  grid.x = (unsigned)(pa.nt0 * pa.nta);
+  grid.y = (unsigned)std::min<int64_t>(groups, 65535);
+  grid.z = (unsigned)std::min<int64_t>(cdiv(groups, grid.y), 1024);
   mark(2, 0, s);
-  if (dtype == TCCG_F64)
-    permute_kernel<double><<<grid, dim3(32, 8), 0, s>>>(pa);
-  else if (dtype == TCCG_F32)
-    permute_kernel<float><<<grid, dim3(32, 8), 0, s>>>(pa);
-  else
+  const dim3 blk(32, 8);
+  if (dtype == TCCG_F64) {
+    if (da == 0)
+      permute_stream_kernel<double><<<grid, blk, 0, s>>>(pa);
+    else if (t64)
+      permute_kernel<double, 64, 1, false><<<grid, blk, 0, s>>>(pa);
+    else if (along0)
+      permute_kernel<double, 32, 4, true><<<grid, blk, 0, s>>>(pa);
+    else
+      permute_kernel<double, 32, 4, false><<<grid, blk, 0, s>>>(pa);
+  } else if (dtype == TCCG_F32) {
+    if (da == 0)
+      permute_stream_kernel<float><<<grid, blk, 0, s>>>(pa);
+    else if (t64)
+      permute_kernel<float, 64, 1, false><<<grid, blk, 0, s>>>(pa);
+    else if (along0)
+      permute_kernel<float, 32, 4, true><<<grid, blk, 0, s>>>(pa);
+    else
+      permute_kernel<float, 32, 4, false><<<grid, blk, 0, s>>>(pa);
+  } else {
     return fail(TCCG_ERR_UNSUPPORTED, "transpose supports TCCG_F32 and TCCG_F64");
+  }
   mark(2, 1, s);
   return launch_check("permute");
 }

@@ -52,18 +52,29 @@ def test_ksplit(cuda, ksplit, precision):
     assert error_metrics(out, ref)["normwise"] <= (1e-13 if precision == "fp64" else 1e-6)
 
 
+PERMS = {
+    "mixed": ([5, 7, 3, 4], [2, 0, 3, 1], True),
+    "reverse": ([70, 9, 33, 66], [3, 2, 1, 0], False),
+    "stream": ([130, 6, 5, 70], [0, 1, 3, 2], False),      # dim 0 stays first: streaming copy
+    "identity": ([17, 3, 1, 40], [0, 1, 2, 3], False),     # fuses to one dimension
+    "padded_stream": ([65, 3, 4, 2], [0, 2, 1, 3], True),  # padding blocks fusion
+    "few_rows": ([300, 70, 2, 1], [1, 0, 2, 3], False),    # tiles grouped along dim 0
+    "wide_tiles": ([128, 128, 3, 2], [1, 0, 3, 2], False), # 64 x 64 tiles
+}
+
+
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(PERMS))
 @pytest.mark.parametrize("dtype", ["f32", "f64"])
-def test_transpose_entry_point(cuda, dtype):
+def test_transpose_entry_point(cuda, dtype, case):
     """tccg_transpose: B[perm] = alpha * A + beta * B with outer (padded) sizes,
     HPTT's semantics (dimension j of B is dimension perm[j] of A)."""
     import torch
     from tccg_b200 import _native as N
     tdt = torch.float32 if dtype == "f32" else torch.float64
-    size = [5, 7, 3, 4]
-    outer_a = [6, 7, 4, 4]
-    perm = [2, 0, 3, 1]
-    outer_b = [size[perm[j]] + (1 if j == 1 else 0) for j in range(4)]
+    size, perm, padded = PERMS[case]
+    outer_a = [e + (1 if padded and i % 2 == 0 else 0) for i, e in enumerate(size)]
+    outer_b = [size[perm[j]] + (1 if padded and j == 1 else 0) for j in range(4)]
     g = torch.Generator(device="cuda").manual_seed(1)
     A = torch.randn(int(np.prod(outer_a)), generator=g, device="cuda", dtype=tdt)
     B = torch.randn(int(np.prod(outer_b)), generator=g, device="cuda", dtype=tdt)
@@ -83,6 +94,14 @@ def test_transpose_entry_point(cuda, dtype):
     want[sl] = 2.0 * np.transpose(An, perm) + 0.5 * Bv[sl]
     got = B.cpu().numpy().reshape(outer_b[::-1]).transpose()
     assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
+    # beta == 0 never reads B (NaN there stays out of the result)
+    B.fill_(float("nan"))
+    N.check(N.lib().tccg_transpose(N.F32 if dtype == "f32" else N.F64, 4, i32, i64(size),
+                                   i64(outer_a), i64(outer_b), 2.0, ctypes.c_void_p(A.data_ptr()),
+                                   0.0, ctypes.c_void_p(B.data_ptr()), None))
+    torch.cuda.synchronize()
+    got = B.cpu().numpy().reshape(outer_b[::-1]).transpose()[sl]
+    assert np.allclose(got, 2.0 * np.transpose(An, perm), rtol=1e-6, atol=1e-6)
 
 
 @pytest.mark.gpu
