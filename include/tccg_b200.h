@@ -109,7 +109,9 @@ typedef struct tccg_tuning {
   int32_t pair;        /* tensor-core precisions: 1 = CTA-pair kernel (cta_group::2, 256-row tiles) */
   int32_t direct;      /* CUDA-core kernels: 0 = automatic (no packing pass when K <= 256 and the
                           operand loads stay coalesced), 1 = always, -1 = never (GETT only) */
-  int32_t reserved[1];
+  int32_t shortk;      /* CUDA-core kernels, K <= 32 (FP64: 16): the kernel that prefetches each
+                          tile's C block under its FMA phase. 0 = automatic (C a 2-D matrix
+                          moved by TMA, at least two tiles per SM), 1 = always, -1 = never */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

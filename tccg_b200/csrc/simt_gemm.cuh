@@ -16,6 +16,7 @@
 // double path) and applies alpha/beta, like TCCG's k-split with one private C
 // per k-group and a final sum (tccg/gett.py:755-781).
 #pragma once
+#include <cuda.h>
 #include "common.cuh"
 
 namespace tccg {
@@ -66,6 +67,7 @@ struct SimtArgs {
   const int64_t* a_k_off;
   const int64_t* b_n_off;
   const int64_t* b_k_off;
+  int32_t* status;  // device error word (bounded waits of the short-K kernel)
 };
 
 template <typename T>
@@ -95,6 +97,67 @@ __device__ __forceinline__ Vec4<T> lds4(const T* p) {
   return r;
 }
 
+// Thread fragment geometry of the 256-thread CUDA-core tiles: warps WARPS_M x
+// WARPS_N, lanes 8 (m) x 4 (n), each thread TMG groups of 4 m and TNG groups of
+// 4 n. A fragment: per group g of 32 m, a thread owns 4 m. FP32: m = 4 lm + i,
+// one 16-byte load. FP64: two 16-byte loads at m = 2 lm + {0,1} and
+// 16 + 2 lm + {0,1}, so the 8 lane groups of each load read 128 contiguous
+// bytes (4 consecutive doubles per lane would put lanes lm and lm + 4 on
+// the same banks: a 2-way conflict on every A load).
+template <typename T>
+struct SimtFrag {
+  using Cfg = SimtCfg<T>;
+  static constexpr int TM = Cfg::TMG * 4, TN = Cfg::TNG * 4;
+  static constexpr bool PAIRS = sizeof(T) == 8;
+  int a_off, b_off;
+  __device__ __forceinline__ explicit SimtFrag(int tid) {
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
+    a_off = wm * (Cfg::TMG * 32) + (lane & 7) * (PAIRS ? 2 : 4);
+    b_off = wn * (Cfg::TNG * 16) + (lane >> 3) * 4;
+  }
+  // tile-local m of accumulator row i and n of accumulator column j
+  __device__ __forceinline__ int m(int i) const {
+    return PAIRS ? a_off + (i / 4) * 32 + ((i % 4) / 2) * 16 + (i % 2) : a_off + (i / 4) * 32 + (i % 4);
+  }
+  __device__ __forceinline__ int n(int j) const { return b_off + (j / 4) * 16 + (j % 4); }
+};
+
+// One k-tile: acc += A[k][m] * B[k][n] over the BK rows of the stage's
+// A [BK][BM] and B [BK][BN] panels, k in increasing order.
+template <typename T>
+__device__ __forceinline__ void simt_fma_ktile(const T* as, const T* bs, int a_off, int b_off,
+                                               T (&acc)[SimtFrag<T>::TM][SimtFrag<T>::TN]) {
+  using Cfg = SimtCfg<T>;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
+  constexpr int TM = SimtFrag<T>::TM, TN = SimtFrag<T>::TN;
+#pragma unroll
+  for (int k = 0; k < BK; ++k) {
+    T av[TM], bv[TN];
+#pragma unroll
+    for (int g = 0; g < Cfg::TMG; ++g) {
+      Vec4<T> x;
+      if constexpr (SimtFrag<T>::PAIRS) {
+        const double2 lo = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32);
+        const double2 hi = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32 + 16);
+        x.v[0] = lo.x; x.v[1] = lo.y; x.v[2] = hi.x; x.v[3] = hi.y;
+      } else {
+        x = lds4<T>(as + k * BM + a_off + g * 32);
+      }
+      av[g * 4 + 0] = x.v[0]; av[g * 4 + 1] = x.v[1]; av[g * 4 + 2] = x.v[2]; av[g * 4 + 3] = x.v[3];
+    }
+#pragma unroll
+    for (int g = 0; g < Cfg::TNG; ++g) {
+      Vec4<T> x = lds4<T>(bs + k * BN + b_off + g * 16);
+      bv[g * 4 + 0] = x.v[0]; bv[g * 4 + 1] = x.v[1]; bv[g * 4 + 2] = x.v[2]; bv[g * 4 + 3] = x.v[3];
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+  }
+}
+
 // One BM x BN tile (bx, by) of split bz; all 256 threads of the CTA take part.
 // Operand loading of simt_gett_tile: packed operands only, direct gathers
 // only, or either by a.direct at run time (the grouped kernel). The packed
@@ -117,9 +180,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   T* As = reinterpret_cast<T*>(smem_raw);              // [STAGES][BK][BM]
   T* Bs = As + (size_t)STAGES * BK * BM;               // [STAGES][BK][BN]
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
-  const int lm = lane & 7, ln = lane >> 3;
+  const int tid = threadIdx.x;
   const int64_t m0 = (int64_t)bx * BM, n0 = (int64_t)by * BN;
   const int kt_begin = bz * a.ktiles_per_split;
   int kt_end = kt_begin + a.ktiles_per_split;
@@ -199,14 +260,8 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     cp_async_commit();
   }
 
-  // A fragment: per group g of 32 m, a thread owns 4 m. FP32: m = 4 lm + i,
-  // one 16-byte load. FP64: two 16-byte loads at m = 2 lm + {0,1} and
-  // 16 + 2 lm + {0,1}, so the 8 lane groups of each load read 128 contiguous
-  // bytes (4 consecutive doubles per lane would put lanes lm and lm + 4 on
-  // the same banks: a 2-way conflict on every A load).
-  constexpr bool PAIRS = sizeof(T) == 8;
-  const int a_off = wm * (Cfg::TMG * 32) + lm * (PAIRS ? 2 : 4);
-  const int b_off = wn * (Cfg::TNG * 16) + ln * 4;
+  const SimtFrag<T> frag(tid);
+  const int a_off = frag.a_off, b_off = frag.b_off;
   for (int kt = kt_begin; kt < kt_end; ++kt) {
     cp_async_wait<STAGES - 2>();
     __syncthreads();
@@ -218,40 +273,13 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     const int stage = (kt - kt_begin) % STAGES;
     const T* as = As + (size_t)stage * BK * BM;
     const T* bs = Bs + (size_t)stage * BK * BN;
-#pragma unroll
-    for (int k = 0; k < BK; ++k) {
-      T av[TM], bv[TN];
-#pragma unroll
-      for (int g = 0; g < Cfg::TMG; ++g) {
-        Vec4<T> x;
-        if constexpr (PAIRS) {
-          const double2 lo = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32);
-          const double2 hi = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32 + 16);
-          x.v[0] = lo.x; x.v[1] = lo.y; x.v[2] = hi.x; x.v[3] = hi.y;
-        } else {
-          x = lds4<T>(as + k * BM + a_off + g * 32);
-        }
-        av[g * 4 + 0] = x.v[0]; av[g * 4 + 1] = x.v[1]; av[g * 4 + 2] = x.v[2]; av[g * 4 + 3] = x.v[3];
-      }
-#pragma unroll
-      for (int g = 0; g < Cfg::TNG; ++g) {
-        Vec4<T> x = lds4<T>(bs + k * BN + b_off + g * 16);
-        bv[g * 4 + 0] = x.v[0]; bv[g * 4 + 1] = x.v[1]; bv[g * 4 + 2] = x.v[2]; bv[g * 4 + 3] = x.v[3];
-      }
-#pragma unroll
-      for (int i = 0; i < TM; ++i)
-#pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-    }
+    simt_fma_ktile<T>(as, bs, a_off, b_off, acc);
   }
   cp_async_wait<0>();
   __syncthreads();
 
-  // thread fragment coordinates (tile-local)
-  auto mloc = [&](int i) {
-    return PAIRS ? a_off + (i / 4) * 32 + ((i % 4) / 2) * 16 + (i % 2) : a_off + (i / 4) * 32 + (i % 4);
-  };
-  auto nloc = [&](int j) { return b_off + (j / 4) * 16 + (j % 4); };
+  auto mloc = [&](int i) { return frag.m(i); };
+  auto nloc = [&](int j) { return frag.n(j); };
 
   if (a.partial != nullptr) {
     T* P = a.partial + (size_t)bz * a.Np * a.Mp;
@@ -363,6 +391,195 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
 template <typename T, int LOAD>
 __global__ void __launch_bounds__(256, 2) simt_gett_kernel(const SimtArgs<T> a) {
   simt_gett_tile<T, LOAD>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------
+// Short-K kernel (packed operands, K <= KP, no k-split). For K = 16 a tile's
+// FMA work (16 FMAs per C element) is short next to its C traffic, and
+// simt_gett_tile reads C only in its epilogue, where the loads' latency
+// stalls the CTA, then spends its own issue slots on the stores. Here the CTA
+// brings its C block into shared memory right after the operand panels, so
+// the read runs under the FMA phase; the epilogue combines in shared memory
+// (alpha * acc + beta * C, 16-byte accesses at the fragment positions) and
+// the block leaves as one bulk store.
+//   TMA = true  (C is a 2-D matrix in the GETT view: unit M stride, one N
+//               stride): the C block comes in and goes out by TMA -- one
+//               instruction each, the store draining while the next CTA on
+//               the SM computes.
+//   TMA = false (any layout): cp.async per thread through the offset tables,
+//               stores from the threads (16-byte vectors where 4 consecutive
+//               m are contiguous and aligned in C).
+// Two CTAs per SM. Same k order and epilogue arithmetic as simt_gett_tile:
+// the results are bitwise equal.
+template <typename T>
+struct SimtShortKCfg {
+  using Cfg = SimtCfg<T>;
+  static constexpr int KP = sizeof(T) == 4 ? 32 : 16;  // longest padded K it takes
+  static constexpr size_t C_BYTES = (size_t)Cfg::BN * Cfg::BM * sizeof(T);  // [BN][BM], dense
+  static constexpr size_t N_BYTES = (size_t)Cfg::BN * sizeof(int64_t);
+  static constexpr size_t A_BYTES = (size_t)KP * Cfg::BM * sizeof(T);
+  static constexpr size_t B_BYTES = (size_t)KP * Cfg::BN * sizeof(T);
+  static constexpr size_t USED = C_BYTES + N_BYTES + A_BYTES + B_BYTES + 16;  // + mbarrier
+  static constexpr size_t SMEM_BYTES = USED + 128;  // slack to align the C block to 128 bytes
+  static_assert(C_BYTES % 128 == 0 && N_BYTES % 16 == 0 && A_BYTES % 16 == 0, "aligned panels");
+  static_assert(2 * (SMEM_BYTES + 1024) <= 228 * 1024, "two CTAs per SM");
+};
+
+template <typename T, bool TMA>
+__global__ void __launch_bounds__(256, 2)
+    simt_shortk_kernel(const SimtArgs<T> a, const __grid_constant__ CUtensorMap tmC) {
+  using Cfg = SimtCfg<T>;
+  using SC = SimtShortKCfg<T>;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
+  constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte access
+  constexpr int QPC = BM / 4, CPI = 256 / QPC, ITER = BN / CPI;
+  constexpr int TM = SimtFrag<T>::TM, TN = SimtFrag<T>::TN;
+  constexpr int64_t NONE = INT64_MIN;  // offsets may be negative (negative strides)
+  static_assert(BN <= 256, "one column offset per thread");
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + (((raw_addr + 127u) & ~127u) - raw_addr);  // TMA: 128-byte aligned
+  T* Cs = reinterpret_cast<T*>(smem);                                  // [BN][BM]
+  int64_t* Cn = reinterpret_cast<int64_t*>(smem + SC::C_BYTES);        // [BN]
+  T* As = reinterpret_cast<T*>(smem + SC::C_BYTES + SC::N_BYTES);      // [KP][BM]
+  T* Bs = As + (size_t)SC::KP * BM;                                    // [KP][BN]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + SC::USED - 16);
+  const int tid = threadIdx.x;
+  const SimtFrag<T> frag(tid);
+  const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
+  const int kp = a.ktiles * BK;
+  const T alpha = a.alpha, beta = a.beta;
+  const bool read_c = beta != T(0);
+
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+  }
+  // operand panels first: their latency runs under the offset loads
+  for (int c = tid; c < kp * (BM / VEC); c += 256) {
+    const int row = c / (BM / VEC), col = (c % (BM / VEC)) * VEC;
+    cp_async_16(As + row * BM + col, a.Ap + (int64_t)row * a.Mp + m0 + col);
+  }
+  for (int c = tid; c < kp * (BN / VEC); c += 256) {
+    const int row = c / (BN / VEC), col = (c % (BN / VEC)) * VEC;
+    cp_async_16(Bs + row * BN + col, a.Bp + (int64_t)row * a.Np + n0 + col);
+  }
+  cp_async_commit();
+  // element path: the thread's 4 m (quad q) of columns cl + u * CPI
+  const int q = tid % QPC, cl = tid / QPC;
+  int64_t cmo[4] = {NONE, NONE, NONE, NONE};
+  bool vq = false;
+  if constexpr (!TMA) {
+    if (tid < BN) Cn[tid] = n0 + tid < a.N ? __ldg(a.c_n_off + n0 + tid) : NONE;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t m = m0 + 4 * q + i;
+      cmo[i] = m < a.M ? __ldg(a.c_m_off + m) : NONE;
+    }
+    vq = cmo[3] != NONE && cmo[1] == cmo[0] + 1 && cmo[2] == cmo[0] + 2 && cmo[3] == cmo[0] + 3;
+  }
+  auto aligned16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  __syncthreads();  // mbarrier initialised, Cn staged
+  if constexpr (TMA) {
+    if (read_c && tid == 0) {
+      mbar_arrive_expect_tx(bar, (uint32_t)SC::C_BYTES);
+      tma_load_2d(Cs, &tmC, (int32_t)m0, (int32_t)n0, bar);
+    }
+  } else if (read_c && cmo[0] != NONE) {
+#pragma unroll
+    for (int u = 0; u < ITER; ++u) {
+      const int col = u * CPI + cl;
+      const int64_t no = Cn[col];
+      if (no == NONE) continue;
+      T* dst = Cs + col * BM + 4 * q;
+      const T* src = a.C + cmo[0] + no;
+      if (vq && aligned16(src)) {
+        cp_async_16(dst, src);
+        if constexpr (sizeof(T) == 8) cp_async_16(dst + 2, src + 2);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (cmo[i] != NONE) cp_async_elem<sizeof(T)>(dst + i, a.C + cmo[i] + no);
+      }
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<1>();  // operand panels in place; the C block may still be in flight
+  __syncthreads();
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+  for (int kt = 0; kt < a.ktiles; ++kt)
+    simt_fma_ktile<T>(As + kt * BK * BM, Bs + kt * BK * BN, frag.a_off, frag.b_off, acc);
+  if constexpr (TMA) {
+    if (read_c && !mbar_wait(bar, 0)) {
+      record_error(a.status, 4);
+      return;  // nothing stored; the block's load never completed
+    }
+  } else {
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+  // combine at the fragment positions: runs of VEC consecutive m (16 bytes)
+#pragma unroll
+  for (int j = 0; j < TN; ++j)
+#pragma unroll
+    for (int i0 = 0; i0 < TM; i0 += VEC) {
+      T* c = Cs + frag.n(j) * BM + frag.m(i0);
+      T v[VEC];
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) v[e] = alpha * acc[i0 + e][j];
+      if (read_c) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 o = *reinterpret_cast<const float4*>(c);
+          v[0] = fma(beta, o.x, v[0]); v[1] = fma(beta, o.y, v[1]);
+          v[2] = fma(beta, o.z, v[2]); v[3] = fma(beta, o.w, v[3]);
+        } else {
+          const double2 o = *reinterpret_cast<const double2*>(c);
+          v[0] = fma(beta, o.x, v[0]); v[1] = fma(beta, o.y, v[1]);
+        }
+      }
+      if constexpr (sizeof(T) == 4)
+        *reinterpret_cast<float4*>(c) = make_float4(v[0], v[1], v[2], v[3]);
+      else
+        *reinterpret_cast<double2*>(c) = make_double2(v[0], v[1]);
+    }
+  if constexpr (TMA) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store_2d(&tmC, Cs, (int32_t)m0, (int32_t)n0);
+      bulk_commit();
+      bulk_wait_read_all();  // shared memory stays valid until the store has read it
+    }
+    return;
+  }
+  __syncthreads();
+  if (cmo[0] == NONE) return;
+#pragma unroll
+  for (int u = 0; u < ITER; ++u) {
+    const int col = u * CPI + cl;
+    const int64_t no = Cn[col];
+    if (no == NONE) continue;
+    const T* src = Cs + col * BM + 4 * q;
+    T* d = a.C + cmo[0] + no;
+    if (vq && aligned16(d)) {
+      if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(d) = *reinterpret_cast<const float4*>(src);
+      } else {
+        reinterpret_cast<double2*>(d)[0] = reinterpret_cast<const double2*>(src)[0];
+        reinterpret_cast<double2*>(d)[1] = reinterpret_cast<const double2*>(src)[1];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (cmo[i] != NONE) a.C[cmo[i] + no] = src[i];
+    }
+  }
 }
 
 // Grouped launch: item i owns CTAs [tile_begin[i], tile_begin[i+1]); the CTA

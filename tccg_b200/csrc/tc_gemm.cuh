@@ -95,10 +95,6 @@ struct TcGroup {
   int32_t total_tiles;
 };
 
-__device__ __forceinline__ void record_error(int32_t* status, int32_t code) {
-  if (status) atomicCAS(status, 0, code);
-}
-
 __device__ __forceinline__ void tile_coords(int tile, const TcArgs& a, int& tm, int& tn) {
   const int group = a.raster * a.tiles_n;
   const int gid = tile / group;

@@ -74,6 +74,7 @@ struct tccg_plan {
   int32_t* d_status = nullptr;
   int32_t read_k_fast_a = 0, read_k_fast_b = 0;
   bool c_is_mn_dense = false;  // C is already the column-major [M-modes][N-modes] matrix
+  int64_t c_ldc = 0;  // > 0: C(m, n) = C[m + c_ldc * n] (a 2-D matrix in the GETT view)
   // SIMT geometry
   int64_t Mp = 0, Np = 0, Kp = 0;
   int32_t ktiles = 0, ksplit = 1, ktiles_per_split = 0;
@@ -82,6 +83,7 @@ struct tccg_plan {
   int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0, chunk_kb = 1, bn = 256;
   int32_t kb_per_split = 0;
   bool direct = false;  // CUDA-core kernel gathers operands without a packing pass
+  bool shortk = false;  // short-K CUDA-core kernel prefetching C (simt_shortk_kernel)
   bool simt = false;    // CUDA-core kernels (else tcgen05)
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
@@ -135,6 +137,7 @@ static bool choose_direct(const tccg_plan* p) {
   if (!simt_path(p) || p->tune.method != TCCG_METHOD_GETT || p->tune.direct < 0) return false;
   if (p->dtype == TCCG_BF16 || p->prec == TCCG_PREC_BF16) return false;
   if (p->tune.direct > 0) return true;
+  if (p->tune.shortk > 0) return false;  // the short-K kernel reads packed operands
   if (p->K > 256) return false;
   // the pack's extra traffic (2 x the operands) must matter next to C's;
   // otherwise the 16-byte loads of packed operands win
@@ -146,6 +149,31 @@ static bool choose_direct(const tccg_plan* p) {
   return a_ok && b_ok;
 }
 
+// The short-K kernel moves its C block by TMA when C is a 2-D matrix
+// C[m + ldc n] with a 16-byte column stride and at least one full tile in
+// each direction (else by cp.async through the offset tables).
+static bool shortk_tma(const tccg_plan* p, int64_t ldc) {
+  const bool dbl = p->prec == TCCG_PREC_FP64;
+  const int64_t es = dbl ? 8 : 4;
+  const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
+  const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
+  return ldc > 0 && (ldc * es) % 16 == 0 && p->M >= BM && p->N >= BN &&
+         p->M < (int64_t(1) << 31) && p->N < (int64_t(1) << 31);
+}
+
+// The short-K kernel that prefetches its C block under the FMA phase:
+// packed operands, the whole K in one panel, no k-split. Automatically only
+// with the TMA C block (the cp.async one measured no faster than the tile
+// kernel) and at least two tiles per SM. TTGT writes the contiguous C'
+// (ldc = M).
+static bool choose_shortk(const tccg_plan* p, int64_t tiles) {
+  if (p->direct || p->ksplit > 1 || p->tune.shortk < 0) return false;
+  const int kp = p->prec == TCCG_PREC_FP64 ? SimtShortKCfg<double>::KP : SimtShortKCfg<float>::KP;
+  if (p->Kp > kp) return false;
+  if (p->tune.shortk > 0) return true;
+  const int64_t ldc = p->tune.method == TCCG_METHOD_TTGT ? p->M : p->c_ldc;
+  return shortk_tma(p, ldc) && tiles >= 2 * (int64_t)p->num_sms;
+}
 
 // K slices for `tiles` C tiles over `kblocks` k-blocks when `slots` CTAs run
 // at once: the requested count, or (requested == 0) as many slices as fill
@@ -341,8 +369,16 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
     for (int i = 0; i < d.nn; ++i) { dense &= d.c_n_stride[i] == s; s *= d.n_ext[i]; }
     p->c_is_mn_dense = dense;
   }
+  bool m_unit = true;
+  for (size_t m = 0; m < h.size() && m_unit; ++m) m_unit = h[m] == (int64_t)m;
   if (!rc) rc = upload(h, &p->t_c_m);
   build_offsets(d.nn, d.n_ext, d.c_n_stride, h);
+  if (m_unit) {
+    const int64_t ldc = h.size() > 1 ? h[1] : std::max<int64_t>(p->M, 1);
+    bool two_d = ldc > 0;
+    for (size_t n = 0; n < h.size() && two_d; ++n) two_d = h[n] == (int64_t)n * ldc;
+    p->c_ldc = two_d ? ldc : 0;
+  }
   if (!rc) rc = upload(h, &p->t_c_n);
   if (!rc) {
     e = cudaMalloc((void**)&p->d_status, sizeof(int32_t));
@@ -401,6 +437,7 @@ static int plan_layout(tccg_plan* p) {
     p->ktiles_per_split = (int32_t)choose_ksplit(p->tune.ksplit, tiles, p->ktiles,
                                                  2 * (int64_t)p->num_sms, 8, &p->ksplit);
     p->direct = choose_direct(p);
+    p->shortk = choose_shortk(p, tiles);
     p->off_a = 0;
     if (!p->direct) {
       ws = align_up((size_t)(p->Kp * p->Mp) * es, 256);
@@ -413,11 +450,13 @@ static int plan_layout(tccg_plan* p) {
     }
     static const char* pn[] = {"fp32", "fp64", "bf16", "bf16x3"};
     snprintf(p->describe, sizeof(p->describe),
-             "method=%s prec=%s kernel=simt_gett<%s> tile=%dx%dx%d M=%lld N=%lld K=%lld "
-             "ksplit=%d pack=%s%s(read_k_fast a=%d b=%d)",
-             ttgt ? "TTGT" : "GETT", pn[p->prec], dbl ? "f64" : "f32", BM, BN, BK,
+             "method=%s prec=%s kernel=simt_%s<%s> tile=%dx%dx%d M=%lld N=%lld K=%lld "
+             "ksplit=%d pack=%s%s%s(read_k_fast a=%d b=%d)",
+             ttgt ? "TTGT" : "GETT", pn[p->prec], p->shortk ? "shortk" : "gett", dbl ? "f64" : "f32",
+             BM, BN, BK,
              (long long)p->M, (long long)p->N, (long long)p->K, p->ksplit,
              p->direct ? "none" : "MN", p->prec == TCCG_PREC_BF16 ? " bf16-rounded" : "",
+             !p->shortk ? "" : shortk_tma(p, ttgt ? p->M : p->c_ldc) ? " cblock=tma" : " cblock=cp.async",
              p->read_k_fast_a, p->read_k_fast_b);
   } else {
     const bool x3 = p->prec == TCCG_PREC_BF16X3;
@@ -544,6 +583,14 @@ static void set_attrs() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
   chk(cudaFuncSetAttribute(simt_gett_kernel<double, SIMT_DIRECT>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(simt_shortk_kernel<float, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SimtShortKCfg<float>::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(simt_shortk_kernel<float, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SimtShortKCfg<float>::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(simt_shortk_kernel<double, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SimtShortKCfg<double>::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(simt_shortk_kernel<double, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SimtShortKCfg<double>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -626,6 +673,26 @@ static int encode_kmajor(CUtensorMap* tm, const void* base, int64_t rows, int64_
   return TCCG_OK;
 }
 
+// 2-D C matrix C[m + ldc * n] (FP32 or FP64), box {box_m, box_n}, no swizzle:
+// the block lands in shared memory as a dense [box_n][box_m] array. Returns
+// false (no map) when the base or the column stride is not 16-byte aligned.
+template <typename T>
+static bool encode_c2d(CUtensorMap* tm, const T* base, int64_t M, int64_t N, int64_t ldc,
+                       int box_m, int box_n) {
+  if (get_encode() != TCCG_OK) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (ldc * (int64_t)sizeof(T)) % 16 != 0)
+    return false;
+  cuuint64_t gdim[2] = {(cuuint64_t)M, (cuuint64_t)N};
+  cuuint64_t gstride[1] = {(cuuint64_t)(ldc * (int64_t)sizeof(T))};
+  cuuint32_t box[2] = {(cuuint32_t)box_m, (cuuint32_t)box_n};
+  cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapDataType dt =
+      sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return g_encode(tm, dt, 2, const_cast<T*>(base), gdim, gstride, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // --------------------------------------------------------------------------
 // launches
 // --------------------------------------------------------------------------
@@ -699,8 +766,8 @@ static void set_direct(SimtArgs<T>& a, const tccg_plan* p, const void* GA, const
 
 template <typename T>
 static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
-                    const int64_t* c_m, const int64_t* c_n, T alpha, T beta, char* ws,
-                    cudaStream_t s) {
+                    const int64_t* c_m, const int64_t* c_n, int64_t c_ldc, T alpha, T beta,
+                    char* ws, cudaStream_t s) {
   using Cfg = SimtCfg<T>;
   T* Ap = reinterpret_cast<T*>(ws + p->off_a);
   T* Bp = reinterpret_cast<T*>(ws + p->off_b);
@@ -737,10 +804,17 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   a.beta = beta;
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(ws + p->off_part) : nullptr;
   set_direct(a, p, GA, GB);
+  a.status = p->d_status;
   dim3 grid((unsigned)(p->Mp / Cfg::BM), (unsigned)(p->Np / Cfg::BN), (unsigned)p->ksplit);
   if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
   mark(1, 0, s);
-  if (p->direct)
+  CUtensorMap tmC{};
+  if (p->shortk && shortk_tma(p, c_ldc) &&
+      encode_c2d<T>(&tmC, Cout, p->M, p->N, c_ldc, Cfg::BM, Cfg::BN))
+    simt_shortk_kernel<T, true><<<grid, 256, SimtShortKCfg<T>::SMEM_BYTES, s>>>(a, tmC);
+  else if (p->shortk)
+    simt_shortk_kernel<T, false><<<grid, 256, SimtShortKCfg<T>::SMEM_BYTES, s>>>(a, tmC);
+  else if (p->direct)
     simt_gett_kernel<T, SIMT_DIRECT><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
   else
     simt_gett_kernel<T, SIMT_PACKED><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
@@ -854,10 +928,13 @@ extern "C" int tccg_plan_run(const tccg_plan* p, const void* A, const void* B, v
   const int64_t* cn = direct && !ttgt ? p->t_c_n : p->t_id_n;
   void* Cdst = direct ? C : (void*)(w + p->off_cprime);
   const double ga = direct ? alpha : 1.0, gb = direct ? beta : 0.0;
+  // C(m, n) = Cdst[m + ldc n]: C itself (GETT on a 2-D C) or the contiguous C'
+  const int64_t ldc = cm == p->t_id_m ? p->M : p->c_ldc;
   if (p->prec == TCCG_PREC_FP64)
-    rc = run_simt<double>(p, GA, GB, static_cast<double*>(Cdst), cm, cn, ga, gb, w, s);
+    rc = run_simt<double>(p, GA, GB, static_cast<double*>(Cdst), cm, cn, ldc, ga, gb, w, s);
   else if (simt_path(p))
-    rc = run_simt<float>(p, GA, GB, static_cast<float*>(Cdst), cm, cn, (float)ga, (float)gb, w, s);
+    rc = run_simt<float>(p, GA, GB, static_cast<float*>(Cdst), cm, cn, ldc, (float)ga, (float)gb,
+                         w, s);
   else
     rc = run_tc(p, GA, GB, static_cast<float*>(Cdst), cm, cn, (float)ga, (float)gb, w, s);
   if (rc || direct) return rc;
@@ -1211,6 +1288,7 @@ static SimtArgs<T> simt_args_for(const tccg_plan* p, char* w, const void* GA, co
   a.beta = (T)beta;
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(w + p->off_part) : nullptr;
   set_direct(a, p, GA, GB);
+  a.status = p->d_status;
   return a;
 }
 

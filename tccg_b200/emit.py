@@ -50,7 +50,7 @@ def source(con: Contraction, precision: str, tuning: Tuning, float_type: str) ->
 #include "gett.h"
 
 static const tccg_desc kDesc = %(desc)s;
-static const tccg_tuning kTuning = {%(method)s, %(variant)d, %(ksplit)d, %(raster)d, %(max_ctas)d, %(pair)d, %(direct)d, {0}};
+static const tccg_tuning kTuning = {%(method)s, %(variant)d, %(ksplit)d, %(raster)d, %(max_ctas)d, %(pair)d, %(direct)d, %(shortk)d};
 
 static tccg_plan* g_plan = NULL;
 static void* g_ws = NULL;
@@ -88,7 +88,8 @@ void gett(%(T)s* A, %(T)s* B, %(T)s* C, const %(T)s alpha, const %(T)s beta) {
 int gett_last_status(void) { return g_status; }
 ''' % dict(spec=spec, precision=precision, tkey=tuning.key(), desc=desc, method=method,
            variant=tuning.variant, ksplit=tuning.ksplit, raster=tuning.raster,
-           max_ctas=tuning.max_ctas, pair=tuning.pair, direct=tuning.direct, dt=dt, prec=prec, T=T)
+           max_ctas=tuning.max_ctas, pair=tuning.pair, direct=tuning.direct,
+           shortk=tuning.shortk, dt=dt, prec=prec, T=T)
 
 
 def header(float_type: str) -> str:

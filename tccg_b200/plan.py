@@ -155,6 +155,7 @@ class Tuning:
     variant: int = 0
     pair: int = 0
     direct: int = 0  # CUDA-core kernels: 0 auto, 1 no packing pass, -1 always pack
+    shortk: int = 0  # CUDA-core kernels, K <= 32: 0 auto, 1 kernel prefetching C, -1 never
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -165,11 +166,13 @@ class Tuning:
         t.variant = int(self.variant)
         t.pair = int(self.pair)
         t.direct = int(self.direct)
+        t.shortk = int(self.shortk)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d" % (self.method, self.ksplit, self.raster, self.max_ctas,
-                                               self.variant, self.pair, self.direct)
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d" % (self.method, self.ksplit, self.raster,
+                                                   self.max_ctas, self.variant, self.pair,
+                                                   self.direct, self.shortk)
 
 
 class Plan:
