@@ -71,6 +71,11 @@ struct tccg_plan {
   int64_t* t_a_vdst = nullptr;
   int64_t* t_b_vsrc = nullptr;
   int64_t* t_b_vdst = nullptr;
+  // tensor-core packs: k-block tiles {kb_lo, kb_run, kb_rows} (PackOperand), or zeros
+  int32_t kb_a[5] = {0, 0, 0, 0, 0}, kb_b[5] = {0, 0, 0, 0, 0};  // {lo, run, rows, ext, step}
+  // offset tables allow the streaming K-major pack (every quad of k is 4
+  // consecutive elements, every quad start and row offset a multiple of 4)
+  bool ks_a = false, ks_b = false;
   int32_t* d_status = nullptr;
   int32_t read_k_fast_a = 0, read_k_fast_b = 0;
   bool c_is_mn_dense = false;  // C is already the column-major [M-modes][N-modes] matrix
@@ -254,6 +259,51 @@ static long long min_stride(int n, const int64_t* ext, const int64_t* str) {
   return best;
 }
 
+// Streaming K-major pack: every row offset is a multiple of 4 elements, and
+// every quad of k (k % 4 == 0, k + 3 < K) starts at a multiple of 4 and runs
+// over 4 consecutive elements -- 16-byte loads once the base is aligned.
+static bool rows_by_4(const std::vector<int64_t>& roff) {
+  for (int64_t o : roff)
+    if (o % 4 != 0) return false;
+  return true;
+}
+static bool k_quads(const std::vector<int64_t>& coff) {
+  if (coff.size() < 4) return false;
+  for (size_t k = 0; k + 3 < coff.size(); k += 4) {
+    if (coff[k] % 4 != 0) return false;
+    for (size_t j = 1; j < 4; ++j)
+      if (coff[k + j] != coff[k] + (int64_t)j) return false;
+  }
+  return true;
+}
+
+// k-block tiles of a K-major pack (PackOperand::kb_*) when the operand's
+// unit-stride mode is a K mode u other than the first K mode of extent > 1:
+// tiles of kb_lo * kb_run consecutive k (kb_lo = product of the extents of
+// the K modes before u, kb_run values of u) x kb_rows rows, at most
+// PACK_KB_ELEMS elements. Needs runs of at least 8 along u, at most 1024 k
+// per tile and whole quads of k (4 | kb_lo * kb_run).
+static void kblock_tiles(int nk, const int64_t* kext, const int64_t* kstr, int32_t (&kb)[5]) {
+  kb[0] = kb[1] = kb[2] = kb[3] = kb[4] = 0;
+  int first = -1, u = -1;
+  for (int i = 0; i < nk; ++i) {
+    if (kext[i] <= 1) continue;
+    if (first < 0) first = i;
+    if (std::llabs(kstr[i]) == 1) u = i;
+  }
+  if (u < 0 || u == first || kext[u] < 8) return;
+  int64_t lo = 1;
+  for (int i = 0; i < u; ++i) lo *= kext[i];
+  if (lo > 128) return;
+  const int64_t run = std::min<int64_t>(kext[u], 1024 / lo), t = lo * run;
+  if (run < 8 || t % 4 != 0) return;
+  kb[0] = (int32_t)lo;
+  kb[1] = (int32_t)run;
+  kb[2] = (int32_t)std::max<int64_t>(1, std::min<int64_t>(32, PACK_KB_ELEMS / t));
+  kb[3] = (int32_t)kext[u];
+  kb[4] = kstr[u] > 0 ? 1 : -1;
+}
+
 // For a K-major pack whose rows are read one per lane: if a later row mode
 // has a smaller stride than the first (non-unit) mode, visit the rows with
 // that mode fastest. vsrc[v] = source offset, vdst[v] = destination row of
@@ -352,12 +402,16 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   std::vector<int64_t> h;
   int rc = TCCG_OK;
   build_offsets(d.nm, d.m_ext, d.a_m_stride, h);
+  p->ks_a = rows_by_4(h);
   if (!rc) rc = upload(h, &p->t_a_m);
   build_offsets(d.nk, d.k_ext, d.a_k_stride, h);
+  p->ks_a = p->ks_a && k_quads(h);
   if (!rc) rc = upload(h, &p->t_a_k);
   build_offsets(d.nn, d.n_ext, d.b_n_stride, h);
+  p->ks_b = rows_by_4(h);
   if (!rc) rc = upload(h, &p->t_b_n);
   build_offsets(d.nk, d.k_ext, d.b_k_stride, h);
+  p->ks_b = p->ks_b && k_quads(h);
   if (!rc) rc = upload(h, &p->t_b_k);
   build_offsets(d.nm, d.m_ext, d.c_m_stride, h);
   // C is "already [M][N]" when its M modes are dense from stride 1 and the N
@@ -389,21 +443,25 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
   if (!rc && !simt_path(p)) {
-    // tensor-core packs: walk the rows along the smallest-stride row mode when
+    // tensor-core packs: unit stride on a later K mode -> k-block tiles read
+    // along it; else walk the rows along the smallest-stride row mode when
     // that beats both the first row mode and reading along k
+    // (FP32 sources only: the tiles move 4-byte elements by cp.async)
+    if (!p->ks_a && p->dtype != TCCG_BF16) kblock_tiles(d.nk, d.k_ext, d.a_k_stride, p->kb_a);
+    if (!p->ks_b && p->dtype != TCCG_BF16) kblock_tiles(d.nk, d.k_ext, d.b_k_stride, p->kb_b);
     std::vector<int64_t> vs, vd;
     auto kstride = [&](const int64_t* kst) {
       for (int i = 0; i < d.nk; ++i)
         if (d.k_ext[i] > 1) return std::llabs(kst[i]);
       return (long long)INT64_MAX;
     };
-    if (min_stride(d.nm, d.m_ext, d.a_m_stride) < kstride(d.a_k_stride) &&
+    if (!p->ks_a && p->kb_a[0] == 0 && min_stride(d.nm, d.m_ext, d.a_m_stride) < kstride(d.a_k_stride) &&
         build_visit(d.nm, d.m_ext, d.a_m_stride, vs, vd)) {
       p->read_k_fast_a = 0;
       rc = upload(vs, &p->t_a_vsrc);
       if (!rc) rc = upload(vd, &p->t_a_vdst);
     }
-    if (!rc && min_stride(d.nn, d.n_ext, d.b_n_stride) < kstride(d.b_k_stride) &&
+    if (!rc && !p->ks_b && p->kb_b[0] == 0 && min_stride(d.nn, d.n_ext, d.b_n_stride) < kstride(d.b_k_stride) &&
         build_visit(d.nn, d.n_ext, d.b_n_stride, vs, vd)) {
       p->read_k_fast_b = 0;
       rc = upload(vs, &p->t_b_vsrc);
@@ -506,13 +564,15 @@ static int plan_layout(tccg_plan* p) {
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=gett_tc%s<%s> tile=%dx%d stages=%d M=%lld N=%lld K=%lld "
              "kblocks=%d chunk=%d ksplit=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
-             "visit a=%d b=%d)",
+             "visit a=%d b=%d kblock a=%dx%dx%d b=%dx%dx%d kstream a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", pair ? "2" : "", x3 ? "BF16X3" : "BF16",
              pair ? 256 : 128, p->bn,
              pair ? (x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES)
-                  : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES), (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit, p->grid,
-             p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
-             p->t_a_vsrc ? 1 : 0, p->t_b_vsrc ? 1 : 0);
+                  : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES),
+             (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit,
+             p->grid, p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
+             p->t_a_vsrc ? 1 : 0, p->t_b_vsrc ? 1 : 0, p->kb_a[0], p->kb_a[1], p->kb_a[2], p->kb_b[0],
+             p->kb_b[1], p->kb_b[2], p->ks_a ? 1 : 0, p->ks_b ? 1 : 0);
   }
   if (ttgt) {
     // contiguous C' = [M][N] (column-major) in the workspace, then C' -> C
@@ -726,7 +786,42 @@ static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* 
   o.read_k_fast = kfast;
   o.active = 1;
   o.row_dst = nullptr;
+  o.kb_lo = o.kb_run = o.kb_rows = o.kb_ext = o.kb_step = 0;
+  o.kstream = 0;
+  o.ktiles = o.tiles = 0;
   return o;
+}
+
+// The read schedule of a K-major pack chosen at plan creation: the streaming
+// pass (when the source is aligned for its vector loads; es = source element
+// bytes) or k-block tiles, else unchanged.
+static PackOperand with_kread(PackOperand o, bool kstream, const int32_t (&kb)[5], size_t es) {
+  if (kstream && (reinterpret_cast<uintptr_t>(o.src) % (4 * es)) == 0) {
+    o.kstream = 1;
+  } else if (kb[0] > 0) {
+    o.kb_lo = kb[0];
+    o.kb_run = kb[1];
+    o.kb_rows = kb[2];
+    o.kb_ext = kb[3];
+    o.kb_step = kb[4];
+  }
+  return o;
+}
+
+// Tile grid of one operand: k-block tiles, or 32 rows x `ktile` k.
+static void pack_geometry(PackOperand& o, int ktile) {
+  if (o.kstream) {  // one tile along k; 256 threads x PACK_KS_Q quads per CTA
+    o.ktiles = 1;
+    o.tiles = cdiv(o.Rcover * (o.Kcover / 4), 256 * PACK_KS_Q);
+    return;
+  }
+  int64_t kt = ktile, rows = 32;
+  if (o.kb_lo > 0) {
+    kt = (int64_t)o.kb_lo * o.kb_run;
+    rows = o.kb_rows;
+  }
+  o.ktiles = cdiv(o.Kcover, kt);
+  o.tiles = o.ktiles * cdiv(o.Rcover, rows);
 }
 
 // Row visit order of a K-major pack (tables built at plan creation).
@@ -738,16 +833,39 @@ static PackOperand with_visit(PackOperand o, const int64_t* vsrc, const int64_t*
   return o;
 }
 
+// Read schedule of one operand (PackRead).
+static int pack_read(const PackOperand& o) {
+  return o.kstream ? PACK_READ_STREAM : o.kb_lo > 0 ? PACK_READ_KBLOCK : PACK_READ_WIDE;
+}
+
+// One launch for both operands, with the kernel of their common read
+// schedule, or the kernel holding all schedules when they differ (a second
+// launch costs more than the wider kernel's extra registers).
 template <typename Tin, typename Tout, int LAYOUT>
-static int launch_pack(const PackArgs& pa, cudaStream_t s) {
-  const int64_t kx = std::max(pa.op[0].Kcover, pa.op[1].Kcover);
-  const int64_t ry = std::max(pa.op[0].Rcover, pa.op[1].Rcover);
-  const int64_t ktiles = cdiv(kx, pack_k_tile<LAYOUT>());
-  const int64_t ctas = ktiles * cdiv(ry, 32);
+static int launch_pack(PackArgs pa, cudaStream_t s) {
+  int64_t ctas = 0;
+  int read = -1;
+  for (PackOperand& o : pa.op) {
+    pack_geometry(o, pack_k_tile<LAYOUT>());
+    if (!o.active) continue;
+    ctas = std::max(ctas, o.tiles);
+    read = read < 0 || read == pack_read(o) ? pack_read(o) : PACK_READ_ANY;
+  }
   if (ctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "operand too large to pack (%lld tiles)", (long long)ctas);
-  dim3 grid((unsigned)ctas, 1, 2);
+  if (ctas == 0) return TCCG_OK;
+  const dim3 grid((unsigned)ctas, 1, 2), block(32, 8);
+  constexpr bool KMAJOR = LAYOUT == PACK_K_BF16 || LAYOUT == PACK_K_BF16X3;
   mark(0, 0, s);
-  pack_kernel<Tin, Tout, LAYOUT><<<grid, dim3(32, 8), 0, s>>>(pa, ktiles);
+  if (!KMAJOR || read == PACK_READ_WIDE)
+    pack_kernel<Tin, Tout, LAYOUT, PACK_READ_WIDE><<<grid, block, 0, s>>>(pa);
+  else if constexpr (KMAJOR) {
+    if (read == PACK_READ_STREAM)
+      pack_kernel<Tin, Tout, LAYOUT, PACK_READ_STREAM><<<grid, block, 0, s>>>(pa);
+    else if (read == PACK_READ_KBLOCK)
+      pack_kernel<Tin, Tout, LAYOUT, PACK_READ_KBLOCK><<<grid, block, 0, s>>>(pa);
+    else
+      pack_kernel<Tin, Tout, LAYOUT, PACK_READ_ANY><<<grid, block, 0, s>>>(pa);
+  }
   mark(0, 1, s);
   return launch_check("pack");
 }
@@ -840,10 +958,13 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   void* Bp = ws + p->off_b;
   PackArgs pa;
   const int64_t kcover = x3 ? round_up(p->K, 32) : p->Kc;
-  pa.op[0] = with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap, p->Kc,
-                                p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst);
-  pa.op[1] = with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp, p->Kc,
-                                p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst);
+  const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
+  pa.op[0] = with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap,
+                                           p->Kc, p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst),
+                        p->ks_a, p->kb_a, es);
+  pa.op[1] = with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp,
+                                           p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
+                        p->ks_b, p->kb_b, es);
   int rc;
   if (x3)
     rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s);
@@ -1353,9 +1474,9 @@ static void add_pack_jobs(std::vector<PackJob>& jobs, int64_t& ctas, const PackO
   for (const PackOperand* o : {&oa, &ob}) {
     PackJob jb;
     jb.op = *o;
+    pack_geometry(jb.op, ktile);
     jb.begin = ctas;
-    jb.ktiles = cdiv(o->Kcover, ktile);
-    if (active) ctas += jb.ktiles * cdiv(o->Rcover, 32);
+    if (active) ctas += jb.op.tiles;
     jobs.push_back(jb);
   }
 }
@@ -1412,11 +1533,14 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
     const void* GA = p->d.swap_ab ? B[i] : A[i];
     const void* GB = p->d.swap_ab ? A[i] : B[i];
     const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
+    const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
     add_pack_jobs(jobs, pctas,
-                  with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, w + p->off_a,
-                                     p->Kc, p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst),
-                  with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, w + p->off_b,
-                                     p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
+                  with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover,
+                                                w + p->off_a, p->Kc, p->read_k_fast_a),
+                                        p->t_a_vsrc, p->t_a_vdst), p->ks_a, p->kb_a, es),
+                  with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover,
+                                                w + p->off_b, p->Kc, p->read_k_fast_b),
+                                        p->t_b_vsrc, p->t_b_vdst), p->ks_b, p->kb_b, es),
                   pack_k_tile<PACK_K_BF16>(), true);
     TcGroupItem it;
     memset(&it, 0, sizeof(it));
