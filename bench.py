@@ -565,6 +565,10 @@ def run_suite(args):
         byts = (nA + nB) * 4 + nC * 4 * (2 if con.beta else 1)
         res = {"flop": flops, "algorithmic_bytes_fp32": byts}
         modes = [("fp32", "gett", 0), ("bf16x3", "gett", 0), ("bf16", "gett", 0), ("fp64", "gett", 0)]
+        if name == "cfg2":
+            # the general CUDA-core tile kernel beside the short-K kernel the
+            # library picks for K = 16
+            modes += [("fp32", "gett", 0, {"shortk": -1})]
         if name in ("cfg1", "cfg2"):
             # short K: the BF16 precisions on each kernel family as well
             # (variant 0 is the library's own choice)
@@ -572,9 +576,11 @@ def run_suite(args):
                       ("bf16x3", "gett", 16), ("bf16", "gett", 1)]
         if name == "cfg2":
             modes += [("fp32", "ttgt", 0), ("bf16", "ttgt", 0), ("bf16x3", "ttgt", 0)]
-        for prec, method, variant in modes:
+        for mode in modes:
+            prec, method, variant = mode[:3]
+            extra = mode[3] if len(mode) > 3 else {}
             dbl = prec == "fp64"
-            tune = Tuning(method=method, variant=variant)
+            tune = Tuning(method=method, variant=variant, **extra)
             c = Compiled(con, prec, tune)
             Ai, Bi = (A.double(), B.double()) if dbl else (A, B)
             if prec == "bf16" and name == "cfg2":
@@ -588,8 +594,9 @@ def run_suite(args):
             c.plan.run(Ai, Bi, Cw, workspace=ws)
             torch.cuda.synchronize()
             e = errs(Cw, C64) if not dbl else errs(Cw, C64)
-            key = "%s_%s%s" % (prec, method, "_cuda_core" if variant < 0 else
-                               "_tensor_core" if variant > 0 else "")
+            key = "%s_%s%s%s" % (prec, method, "_cuda_core" if variant < 0 else
+                                 "_tensor_core" if variant > 0 else "",
+                                 "_tile_kernel" if extra.get("shortk") == -1 else "")
             gbps = (byts * (2 if dbl else 1) if prec != "bf16" else byts - (nA + nB) * 2) / (ms * 1e-3) / 1e9
             res[key] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "gbs": gbps,
                         "hbm_frac": gbps / peaks["hbm_gbs"], "normwise_vs_fp64": e,

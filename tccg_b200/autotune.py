@@ -109,6 +109,10 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
                         splits.append(s)
             splits.sort(key=lambda s: abs(tiles * s - 2 * num_sms))
             out += [Tuning(method=method, ksplit=s) for s in splits]
+            # short K: the C-prefetching kernel forced on and off
+            if K <= (16 if precision == "fp64" else 32):
+                out += [Tuning(method=method, ksplit=1, shortk=1),
+                        Tuning(method=method, ksplit=1, shortk=-1)]
         else:
             # variant > 0 forces the tensor cores (BF16X3: k-blocks per
             # accumulation chunk), < 0 the CUDA cores; the library's own
@@ -117,6 +121,9 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             chunks = [16, 32, 8] if precision == "bf16x3" else [1]
             tc = [Tuning(method=method, raster=r, variant=c) for r in rasters for c in chunks]
             simt = [Tuning(method=method, variant=-1)]
+            if K <= 32:
+                simt += [Tuning(method=method, variant=-1, shortk=1),
+                         Tuning(method=method, variant=-1, shortk=-1)]
             out += [Tuning(method=method)] + ((simt + tc) if K <= 128 else (tc + simt))
     return out
 
