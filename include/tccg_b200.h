@@ -112,6 +112,9 @@ typedef struct tccg_tuning {
   int32_t shortk;      /* CUDA-core kernels, K <= 32 (FP64: 16): the kernel that prefetches each
                           tile's C block under its FMA phase. 0 = automatic (C a 2-D matrix
                           moved by TMA, at least two tiles per SM), 1 = always, -1 = never */
+  int32_t simt_tile;   /* CUDA-core tile shape, FP32 accumulation: 0 = the least padded work
+                          (narrow tiles counted at 1.6x), 1 = 128x128, 2 = 128x32 (small N),
+                          3 = 32x128 (small M); FP64 always 128x64 */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

@@ -62,7 +62,8 @@ class Tuning(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("variant", ctypes.c_int32),
                 ("ksplit", ctypes.c_int32), ("raster", ctypes.c_int32),
                 ("max_ctas", ctypes.c_int32), ("pair", ctypes.c_int32),
-                ("direct", ctypes.c_int32), ("shortk", ctypes.c_int32)]
+                ("direct", ctypes.c_int32), ("shortk", ctypes.c_int32),
+                ("simt_tile", ctypes.c_int32)]
 
 
 _lib = None

@@ -21,27 +21,56 @@
 
 namespace tccg {
 
-template <typename T>
+// Tile shapes S: 0 = the square tile; FP32 also 1 = 128 x 32 (small N) and
+// 2 = 32 x 128 (small M), for contractions whose small extent would leave
+// most of a 128 x 128 tile empty (4 x 4 per thread instead of 8 x 8).
+enum SimtShape : int { SIMT_SQUARE = 0, SIMT_NARROW_N = 1, SIMT_NARROW_M = 2 };
+
+template <typename T, int S = SIMT_SQUARE>
 struct SimtCfg;
 
 template <>
-struct SimtCfg<float> {
+struct SimtCfg<float, SIMT_SQUARE> {
   static constexpr int BM = 128, BN = 128, BK = 16;
   static constexpr int WARPS_M = 2, WARPS_N = 4;
   static constexpr int TMG = 2, TNG = 2;  // 4-wide groups per thread along m / n
   static constexpr int STAGES = 4;
   static constexpr int EPN = 128;         // epilogue columns per pass (the whole tile)
   static constexpr int PAD = 4;
+  static constexpr int MIN_BLOCKS = 2;    // CTAs per SM the register budget allows
 };
 
 template <>
-struct SimtCfg<double> {
+struct SimtCfg<float, SIMT_NARROW_N> {
+  static constexpr int BM = 128, BN = 32, BK = 16;
+  static constexpr int WARPS_M = 4, WARPS_N = 2;
+  static constexpr int TMG = 1, TNG = 1;
+  static constexpr int STAGES = 4;
+  static constexpr int EPN = 32;
+  static constexpr int PAD = 4;
+  static constexpr int MIN_BLOCKS = 3;
+};
+
+template <>
+struct SimtCfg<float, SIMT_NARROW_M> {
+  static constexpr int BM = 32, BN = 128, BK = 16;
+  static constexpr int WARPS_M = 1, WARPS_N = 8;
+  static constexpr int TMG = 1, TNG = 1;
+  static constexpr int STAGES = 4;
+  static constexpr int EPN = 128;
+  static constexpr int PAD = 4;
+  static constexpr int MIN_BLOCKS = 3;
+};
+
+template <>
+struct SimtCfg<double, SIMT_SQUARE> {
   static constexpr int BM = 128, BN = 64, BK = 8;
   static constexpr int WARPS_M = 2, WARPS_N = 4;
   static constexpr int TMG = 2, TNG = 1;
   static constexpr int STAGES = 4;
   static constexpr int EPN = 64;
   static constexpr int PAD = 2;
+  static constexpr int MIN_BLOCKS = 2;
 };
 
 template <typename T>
@@ -70,9 +99,9 @@ struct SimtArgs {
   int32_t* status;  // device error word (bounded waits of the short-K kernel)
 };
 
-template <typename T>
+template <typename T, int S = SIMT_SQUARE>
 constexpr size_t simt_smem_bytes() {
-  using Cfg = SimtCfg<T>;
+  using Cfg = SimtCfg<T, S>;
   size_t pipe = (size_t)Cfg::STAGES * Cfg::BK * (Cfg::BM + Cfg::BN) * sizeof(T);
   size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T) + Cfg::EPN * sizeof(int64_t);
   return pipe > epi ? pipe : epi;
@@ -104,9 +133,9 @@ __device__ __forceinline__ Vec4<T> lds4(const T* p) {
 // 16 + 2 lm + {0,1}, so the 8 lane groups of each load read 128 contiguous
 // bytes (4 consecutive doubles per lane would put lanes lm and lm + 4 on
 // the same banks: a 2-way conflict on every A load).
-template <typename T>
+template <typename T, int S = SIMT_SQUARE>
 struct SimtFrag {
-  using Cfg = SimtCfg<T>;
+  using Cfg = SimtCfg<T, S>;
   static constexpr int TM = Cfg::TMG * 4, TN = Cfg::TNG * 4;
   static constexpr bool PAIRS = sizeof(T) == 8;
   int a_off, b_off;
@@ -125,19 +154,19 @@ struct SimtFrag {
 
 // One k-tile: acc += A[k][m] * B[k][n] over the BK rows of the stage's
 // A [BK][BM] and B [BK][BN] panels, k in increasing order.
-template <typename T>
+template <typename T, int S = SIMT_SQUARE>
 __device__ __forceinline__ void simt_fma_ktile(const T* as, const T* bs, int a_off, int b_off,
-                                               T (&acc)[SimtFrag<T>::TM][SimtFrag<T>::TN]) {
-  using Cfg = SimtCfg<T>;
+                                               T (&acc)[SimtFrag<T, S>::TM][SimtFrag<T, S>::TN]) {
+  using Cfg = SimtCfg<T, S>;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
-  constexpr int TM = SimtFrag<T>::TM, TN = SimtFrag<T>::TN;
+  constexpr int TM = SimtFrag<T, S>::TM, TN = SimtFrag<T, S>::TN;
 #pragma unroll
   for (int k = 0; k < BK; ++k) {
     T av[TM], bv[TN];
 #pragma unroll
     for (int g = 0; g < Cfg::TMG; ++g) {
       Vec4<T> x;
-      if constexpr (SimtFrag<T>::PAIRS) {
+      if constexpr (SimtFrag<T, S>::PAIRS) {
         const double2 lo = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32);
         const double2 hi = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32 + 16);
         x.v[0] = lo.x; x.v[1] = lo.y; x.v[2] = hi.x; x.v[3] = hi.y;
@@ -165,9 +194,9 @@ __device__ __forceinline__ void simt_fma_ktile(const T* as, const T* bs, int a_o
 // and epilogue stay those of a pure packed kernel.
 enum SimtLoad : int { SIMT_PACKED = 0, SIMT_DIRECT = 1, SIMT_EITHER = 2 };
 
-template <typename T, int LOAD = SIMT_EITHER>
+template <typename T, int LOAD = SIMT_EITHER, int S = SIMT_SQUARE>
 __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int by, int bz) {
-  using Cfg = SimtCfg<T>;
+  using Cfg = SimtCfg<T, S>;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
   constexpr int TM = Cfg::TMG * 4, TN = Cfg::TNG * 4;
   constexpr int VEC = 16 / sizeof(T);                 // elements per 16-byte chunk
@@ -260,7 +289,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     cp_async_commit();
   }
 
-  const SimtFrag<T> frag(tid);
+  const SimtFrag<T, S> frag(tid);
   const int a_off = frag.a_off, b_off = frag.b_off;
   for (int kt = kt_begin; kt < kt_end; ++kt) {
     cp_async_wait<STAGES - 2>();
@@ -273,7 +302,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     const int stage = (kt - kt_begin) % STAGES;
     const T* as = As + (size_t)stage * BK * BM;
     const T* bs = Bs + (size_t)stage * BK * BN;
-    simt_fma_ktile<T>(as, bs, a_off, b_off, acc);
+    simt_fma_ktile<T, S>(as, bs, a_off, b_off, acc);
   }
   cp_async_wait<0>();
   __syncthreads();
@@ -388,9 +417,9 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   }
 }
 
-template <typename T, int LOAD>
-__global__ void __launch_bounds__(256, 2) simt_gett_kernel(const SimtArgs<T> a) {
-  simt_gett_tile<T, LOAD>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+template <typename T, int LOAD, int S = SIMT_SQUARE>
+__global__ void __launch_bounds__(256, SimtCfg<T, S>::MIN_BLOCKS) simt_gett_kernel(const SimtArgs<T> a) {
+  simt_gett_tile<T, LOAD, S>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -589,7 +618,20 @@ struct SimtGroupItem {
   SimtArgs<T> args;
   int64_t tile_begin;
   int32_t tiles_m, tiles_n;  // tiles of one k-split slice
+  int32_t shape;             // SimtShape (FP32 items)
 };
+
+// Shared memory of the grouped kernel: the largest of its tile shapes.
+template <typename T>
+constexpr size_t simt_group_smem_bytes() {
+  if constexpr (sizeof(T) == 4) {
+    constexpr size_t a = simt_smem_bytes<T, SIMT_SQUARE>(), b = simt_smem_bytes<T, SIMT_NARROW_N>(),
+                     c = simt_smem_bytes<T, SIMT_NARROW_M>();
+    return a > b ? (a > c ? a : c) : (b > c ? b : c);
+  } else {
+    return simt_smem_bytes<T, SIMT_SQUARE>();
+  }
+}
 
 template <typename T>
 __global__ void __launch_bounds__(256, 2) simt_gett_group_kernel(const SimtGroupItem<T>* items,
@@ -600,7 +642,18 @@ __global__ void __launch_bounds__(256, 2) simt_gett_group_kernel(const SimtGroup
   const int64_t local = t - it.tile_begin;
   const int64_t mn = (int64_t)it.tiles_m * it.tiles_n;
   const int64_t rem = local % mn;
-  simt_gett_tile<T>(it.args, (int)(rem % it.tiles_m), (int)(rem / it.tiles_m), (int)(local / mn));
+  const int bx = (int)(rem % it.tiles_m), by = (int)(rem / it.tiles_m), bz = (int)(local / mn);
+  if constexpr (sizeof(T) == 4) {  // the item's tile shape (uniform over the CTA)
+    if (it.shape == SIMT_NARROW_N) {
+      simt_gett_tile<T, SIMT_EITHER, SIMT_NARROW_N>(it.args, bx, by, bz);
+      return;
+    }
+    if (it.shape == SIMT_NARROW_M) {
+      simt_gett_tile<T, SIMT_EITHER, SIMT_NARROW_M>(it.args, bx, by, bz);
+      return;
+    }
+  }
+  simt_gett_tile<T>(it.args, bx, by, bz);
 }
 
 // C = alpha * sum_z partial[z] + beta * C.

@@ -89,6 +89,8 @@ struct tccg_plan {
   int32_t kb_per_split = 0;
   bool direct = false;  // CUDA-core kernel gathers operands without a packing pass
   bool shortk = false;  // short-K CUDA-core kernel prefetching C (simt_shortk_kernel)
+  int32_t simt_shape = 0;             // SimtShape of the CUDA-core tiles
+  int32_t simt_bm = 0, simt_bn = 0;   // its tile extents
   bool simt = false;    // CUDA-core kernels (else tcgen05)
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
@@ -106,6 +108,45 @@ static int64_t cdiv(int64_t x, int64_t a) { return (x + a - 1) / a; }
 // bandwidth/compute model decide.
 static bool simt_path(const tccg_plan* p) { return p->simt; }
 
+// CUDA-core tile extents of a shape (FP64: the square tile only).
+static void simt_dims(bool dbl, int shape, int* bm, int* bn, int* bk) {
+  if (dbl) {
+    *bm = SimtCfg<double>::BM, *bn = SimtCfg<double>::BN, *bk = SimtCfg<double>::BK;
+  } else if (shape == SIMT_NARROW_N) {
+    *bm = SimtCfg<float, SIMT_NARROW_N>::BM, *bn = SimtCfg<float, SIMT_NARROW_N>::BN;
+    *bk = SimtCfg<float, SIMT_NARROW_N>::BK;
+  } else if (shape == SIMT_NARROW_M) {
+    *bm = SimtCfg<float, SIMT_NARROW_M>::BM, *bn = SimtCfg<float, SIMT_NARROW_M>::BN;
+    *bk = SimtCfg<float, SIMT_NARROW_M>::BK;
+  } else {
+    *bm = SimtCfg<float>::BM, *bn = SimtCfg<float>::BN, *bk = SimtCfg<float>::BK;
+  }
+}
+
+// CUDA-core tile shape: the tuning's, or the one with the least padded work,
+// the narrow tiles' work counted at NARROW_COST per element (their 4 x 4
+// fragments do fewer FMAs per shared-memory load). FP64: square only.
+static constexpr double NARROW_COST = 1.6;
+static int choose_simt_shape(const tccg_plan* p, double* padded_work) {
+  const bool dbl = p->prec == TCCG_PREC_FP64;
+  int best = SIMT_SQUARE;
+  double best_w = 0;
+  for (int sh = SIMT_SQUARE; sh <= (dbl ? SIMT_SQUARE : SIMT_NARROW_M); ++sh) {
+    int bm, bn, bk;
+    simt_dims(dbl, sh, &bm, &bn, &bk);
+    const double w = (double)round_up(p->M, bm) * (double)round_up(p->N, bn) *
+                     (sh == SIMT_SQUARE ? 1.0 : NARROW_COST);
+    const bool forced = !dbl && p->tune.simt_tile == sh + 1;
+    if (forced || (p->tune.simt_tile == 0 && (sh == SIMT_SQUARE || w < best_w))) {
+      best = sh;
+      best_w = w;
+      if (forced) break;
+    }
+  }
+  if (padded_work) *padded_work = best_w;
+  return best;
+}
+
 static bool choose_simt(const tccg_plan* p) {
   if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) return true;
   if (p->tune.pair || p->tune.variant > 0) return false;
@@ -113,15 +154,17 @@ static bool choose_simt(const tccg_plan* p) {
   // Model fitted on B200 timings of mixed contractions (the 256-item
   // batched workload): tensor cores at 0.6 PFLOP/s effective (x3 for
   // split-BF16x3) on 128 x 192 tiles with a C epilogue at 3 TB/s; CUDA cores
-  // at 35 TFLOP/s on 128 x 128 tiles; operands streamed three times (pack
-  // read, packed write, GEMM read) at 4.5 TB/s. Tile padding counts as work.
+  // at 35 TFLOP/s; operands streamed three times (pack
+  // read, packed write, GEMM read) at 4.5 TB/s. Tile padding counts as work
+  // (CUDA cores: that of the shape choose_simt_shape picks).
   const double M = (double)p->M, N = (double)p->N, K = (double)p->K;
   const double Mt = (double)round_up(p->M, 128), Nt = (double)round_up(p->N, 192);
-  const double Ms = (double)round_up(p->M, 128), Ns = (double)round_up(p->N, 128);
+  double simt_work = 0;  // padded M x N of the CUDA-core tile shape it would use
+  (void)choose_simt_shape(p, &simt_work);
   const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
   const double t_tc = std::max(2.0 * Mt * Nt * K * (p->prec == TCCG_PREC_BF16X3 ? 3.0 : 1.0) / 0.6e15,
                                cb / 3e12 + 3.0 * op / 4.5e12);
-  const double t_simt = std::max(2.0 * Ms * Ns * K / 35e12, (cb + 3.0 * op) / 4.5e12);
+  const double t_simt = std::max(2.0 * simt_work * K / 35e12, (cb + 3.0 * op) / 4.5e12);
   return t_simt < t_tc;
 }
 
@@ -172,7 +215,7 @@ static bool shortk_tma(const tccg_plan* p, int64_t ldc) {
 // kernel) and at least two tiles per SM. TTGT writes the contiguous C'
 // (ldc = M).
 static bool choose_shortk(const tccg_plan* p, int64_t tiles) {
-  if (p->direct || p->ksplit > 1 || p->tune.shortk < 0) return false;
+  if (p->direct || p->ksplit > 1 || p->tune.shortk < 0 || p->simt_shape != SIMT_SQUARE) return false;
   const int kp = p->prec == TCCG_PREC_FP64 ? SimtShortKCfg<double>::KP : SimtShortKCfg<float>::KP;
   if (p->Kp > kp) return false;
   if (p->tune.shortk > 0) return true;
@@ -482,18 +525,24 @@ static int plan_layout(tccg_plan* p) {
   const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
   if (simt_path(p)) {
     const bool dbl = p->prec == TCCG_PREC_FP64;
-    const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
-    const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
-    const int BK = dbl ? SimtCfg<double>::BK : SimtCfg<float>::BK;
+    // the short-K kernel keeps the square tile: a tuning that asks for it
+    // settles the shape
+    p->simt_shape = p->tune.shortk > 0 ? SIMT_SQUARE : choose_simt_shape(p, nullptr);
+    int BM, BN, BK;
+    simt_dims(dbl, p->simt_shape, &BM, &BN, &BK);
+    p->simt_bm = BM;
+    p->simt_bn = BN;
+    const int min_blocks = p->simt_shape == SIMT_SQUARE ? SimtCfg<float>::MIN_BLOCKS
+                                                        : SimtCfg<float, SIMT_NARROW_N>::MIN_BLOCKS;
     const size_t es = dbl ? 8 : 4;
     p->Mp = round_up(p->M, BM);
     p->Np = round_up(p->N, BN);
     p->Kp = round_up(p->K, BK);
     p->ktiles = (int32_t)(p->Kp / BK);
     const int64_t tiles = (p->Mp / BM) * (p->Np / BN);
-    // two CTAs per SM; a slice is at least 8 k-tiles
+    // min_blocks CTAs per SM; a slice is at least 8 k-tiles
     p->ktiles_per_split = (int32_t)choose_ksplit(p->tune.ksplit, tiles, p->ktiles,
-                                                 2 * (int64_t)p->num_sms, 8, &p->ksplit);
+                                                 min_blocks * (int64_t)p->num_sms, 8, &p->ksplit);
     p->direct = choose_direct(p);
     p->shortk = choose_shortk(p, tiles);
     p->off_a = 0;
@@ -655,10 +704,10 @@ static void set_attrs() {
                            (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(simt_gett_group_kernel<float>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<float>()));
-  chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)simt_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(simt_gett_group_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)simt_group_smem_bytes<float>()));
+  chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)simt_group_smem_bytes<double>()));
   chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)Tc2Cfg<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -882,6 +931,22 @@ static void set_direct(SimtArgs<T>& a, const tccg_plan* p, const void* GA, const
   a.b_k_off = p->t_b_k;
 }
 
+// simt_gett_kernel with the plan's tile shape (FP32: three shapes).
+template <typename T, int LOAD>
+static void launch_simt_tiles(const tccg_plan* p, const SimtArgs<T>& a, dim3 grid, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    if (p->simt_shape == SIMT_NARROW_N) {
+      simt_gett_kernel<T, LOAD, SIMT_NARROW_N><<<grid, 256, simt_smem_bytes<T, SIMT_NARROW_N>(), s>>>(a);
+      return;
+    }
+    if (p->simt_shape == SIMT_NARROW_M) {
+      simt_gett_kernel<T, LOAD, SIMT_NARROW_M><<<grid, 256, simt_smem_bytes<T, SIMT_NARROW_M>(), s>>>(a);
+      return;
+    }
+  }
+  simt_gett_kernel<T, LOAD><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+}
+
 template <typename T>
 static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
                     const int64_t* c_m, const int64_t* c_n, int64_t c_ldc, T alpha, T beta,
@@ -923,7 +988,7 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(ws + p->off_part) : nullptr;
   set_direct(a, p, GA, GB);
   a.status = p->d_status;
-  dim3 grid((unsigned)(p->Mp / Cfg::BM), (unsigned)(p->Np / Cfg::BN), (unsigned)p->ksplit);
+  dim3 grid((unsigned)(p->Mp / p->simt_bm), (unsigned)(p->Np / p->simt_bn), (unsigned)p->ksplit);
   if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
   mark(1, 0, s);
   CUtensorMap tmC{};
@@ -933,9 +998,9 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   else if (p->shortk)
     simt_shortk_kernel<T, false><<<grid, 256, SimtShortKCfg<T>::SMEM_BYTES, s>>>(a, tmC);
   else if (p->direct)
-    simt_gett_kernel<T, SIMT_DIRECT><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+    launch_simt_tiles<T, SIMT_DIRECT>(p, a, grid, s);
   else
-    simt_gett_kernel<T, SIMT_PACKED><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+    launch_simt_tiles<T, SIMT_PACKED>(p, a, grid, s);
   mark(1, 1, s);
   rc = launch_check("simt_gett");
   if (rc) return rc;
@@ -1343,9 +1408,7 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     ws += need;
     g->ws_bytes = std::max(g->ws_bytes, ws);
     if (simt_path(p)) {
-      const int BM = dbl ? SimtCfg<double>::BM : SimtCfg<float>::BM;
-      const int BN = dbl ? SimtCfg<double>::BN : SimtCfg<float>::BN;
-      wv.simt_tiles += (p->Mp / BM) * (p->Np / BN) * p->ksplit;
+      wv.simt_tiles += (p->Mp / p->simt_bm) * (p->Np / p->simt_bn) * p->ksplit;
     } else {
       wv.tc_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
@@ -1505,8 +1568,9 @@ static int bind_simt(tccg_group* g, tccg_group::Wave& wv, const void* const* A,
     SimtGroupItem<T> it;
     it.args = simt_args_for<T>(p, w, GA, GB, C[i], alpha[i], beta[i]);
     it.tile_begin = tile;
-    it.tiles_m = (int32_t)(p->Mp / SimtCfg<T>::BM);
-    it.tiles_n = (int32_t)(p->Np / SimtCfg<T>::BN);
+    it.tiles_m = (int32_t)(p->Mp / p->simt_bm);
+    it.tiles_n = (int32_t)(p->Np / p->simt_bn);
+    it.shape = p->simt_shape;
     tile += (int64_t)it.tiles_m * it.tiles_n * p->ksplit;
     items.push_back(it);
     if (p->ksplit > 1) {
@@ -1685,7 +1749,7 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
     if ((rc = launch_check("pack_group"))) return rc;
   }
   if (wv.n_simt > 0) {
-    simt_gett_group_kernel<T><<<(unsigned)wv.simt_tiles, 256, simt_smem_bytes<T>(), s>>>(
+    simt_gett_group_kernel<T><<<(unsigned)wv.simt_tiles, 256, simt_group_smem_bytes<T>(), s>>>(
         static_cast<const SimtGroupItem<T>*>(g->d_simt) + wv.simt0, g->b_simt_items + wv.simt0,
         wv.n_simt);
     if ((rc = launch_check("simt_gett_group"))) return rc;

@@ -156,6 +156,7 @@ class Tuning:
     pair: int = 0
     direct: int = 0  # CUDA-core kernels: 0 auto, 1 no packing pass, -1 always pack
     shortk: int = 0  # CUDA-core kernels, K <= 32: 0 auto, 1 kernel prefetching C, -1 never
+    simt_tile: int = 0  # CUDA-core tiles: 0 auto, 1 128x128, 2 128x32, 3 32x128
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -167,12 +168,13 @@ class Tuning:
         t.pair = int(self.pair)
         t.direct = int(self.direct)
         t.shortk = int(self.shortk)
+        t.simt_tile = int(self.simt_tile)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d" % (self.method, self.ksplit, self.raster,
-                                                   self.max_ctas, self.variant, self.pair,
-                                                   self.direct, self.shortk)
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d" % (self.method, self.ksplit, self.raster,
+                                                       self.max_ctas, self.variant, self.pair,
+                                                       self.direct, self.shortk, self.simt_tile)
 
 
 class Plan:
