@@ -113,6 +113,9 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             if K <= (16 if precision == "fp64" else 32):
                 out += [Tuning(method=method, ksplit=1, shortk=1),
                         Tuning(method=method, ksplit=1, shortk=-1)]
+            # FP32: each CUDA-core tile shape (square, small N, small M)
+            if precision == "fp32":
+                out += [Tuning(method=method, simt_tile=t) for t in (1, 2, 3)]
         else:
             # variant > 0 forces the tensor cores (BF16X3: k-blocks per
             # accumulation chunk), < 0 the CUDA cores; the library's own
