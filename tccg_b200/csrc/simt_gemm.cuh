@@ -10,6 +10,10 @@
 // That is GETT's defining property (TCCG's micro-kernel stores into C's
 // original layout, tccg/gett.py:192-223) -- there is no C transposition.
 //
+// FP32 tiles come in three shapes (128x128, and 128x32 / 32x128 for a small
+// N / M); simt_shortk_kernel is the K <= 32 variant that reads the tile's C
+// block under the FMA phase (below).
+//
 // beta == 0 writes C without reading it (TCCG's update = 0 path,
 // tccg/gett.py:516-525). With a k-split the CTAs of split z write raw partial
 // sums to a workspace and simt_reduce_kernel adds them (in T: FP64 for the
