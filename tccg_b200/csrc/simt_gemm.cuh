@@ -42,6 +42,7 @@ struct SimtCfg<float, SIMT_SQUARE> {
   static constexpr int EPN = 128;         // epilogue columns per pass (the whole tile)
   static constexpr int PAD = 4;
   static constexpr int MIN_BLOCKS = 2;    // CTAs per SM the register budget allows
+  static constexpr int LDA = BM, LDB = BN;  // stage row strides (elements)
 };
 
 template <>
@@ -53,6 +54,9 @@ struct SimtCfg<float, SIMT_NARROW_N> {
   static constexpr int EPN = 32;
   static constexpr int PAD = 4;
   static constexpr int MIN_BLOCKS = 3;
+  // padded stage rows: gathers along k (lanes 4 elements apart in k) spread
+  // over the banks
+  static constexpr int LDA = BM + 4, LDB = BN + 4;
 };
 
 template <>
@@ -64,6 +68,7 @@ struct SimtCfg<float, SIMT_NARROW_M> {
   static constexpr int EPN = 128;
   static constexpr int PAD = 4;
   static constexpr int MIN_BLOCKS = 3;
+  static constexpr int LDA = BM + 4, LDB = BN + 4;
 };
 
 template <>
@@ -75,6 +80,7 @@ struct SimtCfg<double, SIMT_SQUARE> {
   static constexpr int EPN = 64;
   static constexpr int PAD = 2;
   static constexpr int MIN_BLOCKS = 2;
+  static constexpr int LDA = BM, LDB = BN;
 };
 
 template <typename T>
@@ -93,6 +99,9 @@ struct SimtArgs {
   // Asrc[a_m_off[m] + a_k_off[k]] and B[k][n] = Bsrc[b_n_off[n] + b_k_off[k]]
   // element by element (zeros beyond M, N, K)
   int32_t direct;
+  // narrow tiles, direct: 1 = the operand is gathered along k (its unit
+  // stride is a K mode)
+  int32_t a_kfast, b_kfast;
   int64_t K;
   const T* Asrc;
   const T* Bsrc;
@@ -106,7 +115,7 @@ struct SimtArgs {
 template <typename T, int S = SIMT_SQUARE>
 constexpr size_t simt_smem_bytes() {
   using Cfg = SimtCfg<T, S>;
-  size_t pipe = (size_t)Cfg::STAGES * Cfg::BK * (Cfg::BM + Cfg::BN) * sizeof(T);
+  size_t pipe = (size_t)Cfg::STAGES * Cfg::BK * (Cfg::LDA + Cfg::LDB) * sizeof(T);
   size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T) + Cfg::EPN * sizeof(int64_t);
   return pipe > epi ? pipe : epi;
 }
@@ -157,12 +166,12 @@ struct SimtFrag {
 };
 
 // One k-tile: acc += A[k][m] * B[k][n] over the BK rows of the stage's
-// A [BK][BM] and B [BK][BN] panels, k in increasing order.
+// A [BK][LDA] and B [BK][LDB] panels, k in increasing order.
 template <typename T, int S = SIMT_SQUARE>
 __device__ __forceinline__ void simt_fma_ktile(const T* as, const T* bs, int a_off, int b_off,
                                                T (&acc)[SimtFrag<T, S>::TM][SimtFrag<T, S>::TN]) {
   using Cfg = SimtCfg<T, S>;
-  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
+  constexpr int BK = Cfg::BK;
   constexpr int TM = SimtFrag<T, S>::TM, TN = SimtFrag<T, S>::TN;
 #pragma unroll
   for (int k = 0; k < BK; ++k) {
@@ -171,17 +180,17 @@ __device__ __forceinline__ void simt_fma_ktile(const T* as, const T* bs, int a_o
     for (int g = 0; g < Cfg::TMG; ++g) {
       Vec4<T> x;
       if constexpr (SimtFrag<T, S>::PAIRS) {
-        const double2 lo = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32);
-        const double2 hi = *reinterpret_cast<const double2*>(as + k * BM + a_off + g * 32 + 16);
+        const double2 lo = *reinterpret_cast<const double2*>(as + k * Cfg::LDA + a_off + g * 32);
+        const double2 hi = *reinterpret_cast<const double2*>(as + k * Cfg::LDA + a_off + g * 32 + 16);
         x.v[0] = lo.x; x.v[1] = lo.y; x.v[2] = hi.x; x.v[3] = hi.y;
       } else {
-        x = lds4<T>(as + k * BM + a_off + g * 32);
+        x = lds4<T>(as + k * Cfg::LDA + a_off + g * 32);
       }
       av[g * 4 + 0] = x.v[0]; av[g * 4 + 1] = x.v[1]; av[g * 4 + 2] = x.v[2]; av[g * 4 + 3] = x.v[3];
     }
 #pragma unroll
     for (int g = 0; g < Cfg::TNG; ++g) {
-      Vec4<T> x = lds4<T>(bs + k * BN + b_off + g * 16);
+      Vec4<T> x = lds4<T>(bs + k * Cfg::LDB + b_off + g * 16);
       bv[g * 4 + 0] = x.v[0]; bv[g * 4 + 1] = x.v[1]; bv[g * 4 + 2] = x.v[2]; bv[g * 4 + 3] = x.v[3];
     }
 #pragma unroll
@@ -202,6 +211,7 @@ template <typename T, int LOAD = SIMT_EITHER, int S = SIMT_SQUARE>
 __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int by, int bz) {
   using Cfg = SimtCfg<T, S>;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, STAGES = Cfg::STAGES;
+  constexpr int LDA = Cfg::LDA, LDB = Cfg::LDB;
   constexpr int TM = Cfg::TMG * 4, TN = Cfg::TNG * 4;
   constexpr int VEC = 16 / sizeof(T);                 // elements per 16-byte chunk
   constexpr int A_CHUNKS = BK * BM / VEC, B_CHUNKS = BK * BN / VEC;
@@ -210,8 +220,8 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   static_assert(Cfg::WARPS_N * Cfg::TNG * 16 == BN, "tile N");
 
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);              // [STAGES][BK][BM]
-  T* Bs = As + (size_t)STAGES * BK * BM;               // [STAGES][BK][BN]
+  T* As = reinterpret_cast<T*>(smem_raw);              // [STAGES][BK][LDA]
+  T* Bs = As + (size_t)STAGES * BK * LDA;              // [STAGES][BK][LDB]
 
   const int tid = threadIdx.x;
   const int64_t m0 = (int64_t)bx * BM, n0 = (int64_t)by * BN;
@@ -231,12 +241,81 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     if (m0 + dcol_a < a.M) dm_off = a.a_m_off[m0 + dcol_a];
     if (n0 + dcol_b < a.N) dn_off = a.b_n_off[n0 + dcol_b];
   }
+  // Narrow tiles: an operand whose unit stride is along k (a_kfast /
+  // b_kfast) is gathered with lanes along k instead -- thread tid fills
+  // k = tid % BK of rows tid / BK + j * (256 / BK) -- so each warp reads two
+  // 64-byte runs; the rows' offsets are loaded once per tile.
+  constexpr bool KFAST = S != SIMT_SQUARE;
+  constexpr int KR = 256 / BK;  // rows per pass of the k-fast gather
+  constexpr int JAK = KFAST ? BM / KR : 1, JBK = KFAST ? BN / KR : 1;
+  const int kk = tid % BK, kr = tid / BK;
+  int64_t kfa[JAK], kfb[JBK];
+  const bool kfast_a = KFAST && direct && a.a_kfast, kfast_b = KFAST && direct && a.b_kfast;
+  if constexpr (KFAST) {
+    static_assert(BM % KR == 0 && BN % KR == 0, "k-fast gather layout");
+#pragma unroll
+    for (int j = 0; j < JAK; ++j) {
+      const int64_t m = m0 + kr + j * KR;
+      kfa[j] = kfast_a && m < a.M ? a.a_m_off[m] : NONE;
+    }
+#pragma unroll
+    for (int j = 0; j < JBK; ++j) {
+      const int64_t n = n0 + kr + j * KR;
+      kfb[j] = kfast_b && n < a.N ? a.b_n_off[n] : NONE;
+    }
+  }
 
   auto load_stage = [&](int stage, int kt) {
-    T* as = As + (size_t)stage * BK * BM;
-    T* bs = Bs + (size_t)stage * BK * BN;
+    T* as = As + (size_t)stage * BK * LDA;
+    T* bs = Bs + (size_t)stage * BK * LDB;
     const int64_t krow = (int64_t)kt * BK;
-    if (direct) {
+    if (KFAST && (kfast_a || kfast_b)) {
+      // one operand (or both) along k; the other, if any, along its rows
+      const int64_t k = krow + kk;
+      const int64_t koa = k < a.K ? __ldg(a.a_k_off + k) : NONE;
+      const int64_t kob = k < a.K ? __ldg(a.b_k_off + k) : NONE;
+      constexpr int JA = BK * BM / 256, JB = BK * BN / 256;
+      if (kfast_a) {
+#pragma unroll
+        for (int j = 0; j < JAK; ++j) {
+          T* dst = as + kk * LDA + kr + j * KR;
+          if (kfa[j] != NONE && koa != NONE)
+            cp_async_elem<sizeof(T)>(dst, a.Asrc + kfa[j] + koa);
+          else
+            *dst = T(0);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < JA; ++j) {
+          const int64_t kj = krow + drow_a + j * (256 / BM);
+          T* dst = as + (drow_a + j * (256 / BM)) * LDA + dcol_a;
+          if (dm_off != NONE && kj < a.K)
+            cp_async_elem<sizeof(T)>(dst, a.Asrc + dm_off + __ldg(a.a_k_off + kj));
+          else
+            *dst = T(0);
+        }
+      }
+      if (kfast_b) {
+#pragma unroll
+        for (int j = 0; j < JBK; ++j) {
+          T* dst = bs + kk * LDB + kr + j * KR;
+          if (kfb[j] != NONE && kob != NONE)
+            cp_async_elem<sizeof(T)>(dst, a.Bsrc + kfb[j] + kob);
+          else
+            *dst = T(0);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < JB; ++j) {
+          const int64_t kj = krow + drow_b + j * (256 / BN);
+          T* dst = bs + (drow_b + j * (256 / BN)) * LDB + dcol_b;
+          if (dn_off != NONE && kj < a.K)
+            cp_async_elem<sizeof(T)>(dst, a.Bsrc + dn_off + __ldg(a.b_k_off + kj));
+          else
+            *dst = T(0);
+        }
+      }
+    } else if (direct) {
       // all k offsets first (independent loads), then the copies: an offset
       // load between two asynchronous copies would serialise them
       constexpr int JA = BK * BM / 256, JB = BK * BN / 256;
@@ -253,7 +332,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       }
 #pragma unroll
       for (int j = 0; j < JA; ++j) {
-        T* dst = as + (drow_a + j * (256 / BM)) * BM + dcol_a;
+        T* dst = as + (drow_a + j * (256 / BM)) * LDA + dcol_a;
         if (dm_off != NONE && koa[j] != NONE)
           cp_async_elem<sizeof(T)>(dst, a.Asrc + dm_off + koa[j]);
         else
@@ -261,7 +340,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       }
 #pragma unroll
       for (int j = 0; j < JB; ++j) {
-        T* dst = bs + (drow_b + j * (256 / BN)) * BN + dcol_b;
+        T* dst = bs + (drow_b + j * (256 / BN)) * LDB + dcol_b;
         if (dn_off != NONE && kob[j] != NONE)
           cp_async_elem<sizeof(T)>(dst, a.Bsrc + dn_off + kob[j]);
         else
@@ -271,12 +350,12 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
 #pragma unroll
       for (int c = tid; c < A_CHUNKS; c += 256) {
         const int row = c / A_ROW_CHUNKS, col = (c % A_ROW_CHUNKS) * VEC;
-        cp_async_16(as + row * BM + col, a.Ap + (krow + row) * a.Mp + m0 + col);
+        cp_async_16(as + row * LDA + col, a.Ap + (krow + row) * a.Mp + m0 + col);
       }
 #pragma unroll
       for (int c = tid; c < B_CHUNKS; c += 256) {
         const int row = c / B_ROW_CHUNKS, col = (c % B_ROW_CHUNKS) * VEC;
-        cp_async_16(bs + row * BN + col, a.Bp + (krow + row) * a.Np + n0 + col);
+        cp_async_16(bs + row * LDB + col, a.Bp + (krow + row) * a.Np + n0 + col);
       }
     }
   };
@@ -304,8 +383,8 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       cp_async_commit();
     }
     const int stage = (kt - kt_begin) % STAGES;
-    const T* as = As + (size_t)stage * BK * BM;
-    const T* bs = Bs + (size_t)stage * BK * BN;
+    const T* as = As + (size_t)stage * BK * LDA;
+    const T* bs = Bs + (size_t)stage * BK * LDB;
     simt_fma_ktile<T, S>(as, bs, a_off, b_off, acc);
   }
   cp_async_wait<0>();

@@ -88,6 +88,7 @@ struct tccg_plan {
   int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0, chunk_kb = 1, bn = 256;
   int32_t kb_per_split = 0;
   bool direct = false;  // CUDA-core kernel gathers operands without a packing pass
+  bool gather_k_a = false, gather_k_b = false;  // direct, narrow tiles: gathers along k
   bool shortk = false;  // short-K CUDA-core kernel prefetching C (simt_shortk_kernel)
   int32_t simt_shape = 0;             // SimtShape of the CUDA-core tiles
   int32_t simt_bm = 0, simt_bn = 0;   // its tile extents
@@ -186,15 +187,31 @@ static bool choose_direct(const tccg_plan* p) {
   if (p->dtype == TCCG_BF16 || p->prec == TCCG_PREC_BF16) return false;
   if (p->tune.direct > 0) return true;
   if (p->tune.shortk > 0) return false;  // the short-K kernel reads packed operands
-  if (p->K > 256) return false;
+  // narrow tiles gather along k too (lanes along the operand's unit-stride
+  // K mode), so they take long K as well
+  const bool narrow = p->simt_shape != SIMT_SQUARE;
+  if (p->K > 256 && !narrow) return false;
   // the pack's extra traffic (2 x the operands) must matter next to C's;
   // otherwise the 16-byte loads of packed operands win
   if (4 * (p->M + p->N) * p->K < p->M * p->N) return false;
   const int64_t es = p->prec == TCCG_PREC_FP64 ? 8 : 4, small = 4 << 20;
   const tccg_desc& d = p->d;
-  const bool a_ok = unit_first(d.nm, d.m_ext, d.a_m_stride) || p->M * p->K * es <= small;
-  const bool b_ok = unit_first(d.nn, d.n_ext, d.b_n_stride) || p->N * p->K * es <= small;
+  const bool a_ok = unit_first(d.nm, d.m_ext, d.a_m_stride) || p->M * p->K * es <= small ||
+                    (narrow && unit_first(d.nk, d.k_ext, d.a_k_stride));
+  const bool b_ok = unit_first(d.nn, d.n_ext, d.b_n_stride) || p->N * p->K * es <= small ||
+                    (narrow && unit_first(d.nk, d.k_ext, d.b_k_stride));
   return a_ok && b_ok;
+}
+
+// Narrow tiles, direct loads: gather an operand along k when its unit
+// stride is a K mode and not a row mode.
+static void choose_gather_k(tccg_plan* p) {
+  const tccg_desc& d = p->d;
+  const bool narrow = p->simt_shape != SIMT_SQUARE;
+  p->gather_k_a = p->direct && narrow && !unit_first(d.nm, d.m_ext, d.a_m_stride) &&
+                  unit_first(d.nk, d.k_ext, d.a_k_stride);
+  p->gather_k_b = p->direct && narrow && !unit_first(d.nn, d.n_ext, d.b_n_stride) &&
+                  unit_first(d.nk, d.k_ext, d.b_k_stride);
 }
 
 // The short-K kernel moves its C block by TMA when C is a 2-D matrix
@@ -544,6 +561,7 @@ static int plan_layout(tccg_plan* p) {
     p->ktiles_per_split = (int32_t)choose_ksplit(p->tune.ksplit, tiles, p->ktiles,
                                                  min_blocks * (int64_t)p->num_sms, 8, &p->ksplit);
     p->direct = choose_direct(p);
+    choose_gather_k(p);
     p->shortk = choose_shortk(p, tiles);
     p->off_a = 0;
     if (!p->direct) {
@@ -558,13 +576,15 @@ static int plan_layout(tccg_plan* p) {
     static const char* pn[] = {"fp32", "fp64", "bf16", "bf16x3"};
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=simt_%s<%s> tile=%dx%dx%d M=%lld N=%lld K=%lld "
-             "ksplit=%d pack=%s%s%s(read_k_fast a=%d b=%d)",
+             "ksplit=%d pack=%s%s%s(%s a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", pn[p->prec], p->shortk ? "shortk" : "gett", dbl ? "f64" : "f32",
              BM, BN, BK,
              (long long)p->M, (long long)p->N, (long long)p->K, p->ksplit,
              p->direct ? "none" : "MN", p->prec == TCCG_PREC_BF16 ? " bf16-rounded" : "",
              !p->shortk ? "" : shortk_tma(p, ttgt ? p->M : p->c_ldc) ? " cblock=tma" : " cblock=cp.async",
-             p->read_k_fast_a, p->read_k_fast_b);
+             p->direct ? "gather_k" : "read_k_fast",
+             p->direct ? (int)p->gather_k_a : p->read_k_fast_a,
+             p->direct ? (int)p->gather_k_b : p->read_k_fast_b);
   } else {
     const bool x3 = p->prec == TCCG_PREC_BF16X3;
     if (x3) {
@@ -922,6 +942,8 @@ static int launch_pack(PackArgs pa, cudaStream_t s) {
 template <typename T>
 static void set_direct(SimtArgs<T>& a, const tccg_plan* p, const void* GA, const void* GB) {
   a.direct = p->direct ? 1 : 0;
+  a.a_kfast = p->gather_k_a ? 1 : 0;
+  a.b_kfast = p->gather_k_b ? 1 : 0;
   a.K = p->K;
   a.Asrc = static_cast<const T*>(GA);
   a.Bsrc = static_cast<const T*>(GB);

@@ -2,7 +2,8 @@
 a small N and 32 x 128 for a small M, 4 x 4 per thread. Same k order and
 epilogue arithmetic as the 128 x 128 tile, so without a k-split the results
 are bitwise equal to it; all against the FP64 loop nest. Cases: packed and
-pack-free loads, tails in M, N and K, k-splits, beta, the automatic choice,
+pack-free loads (gathered along rows or, where an operand's unit stride is a
+K mode, along k), tails in M, N and K, k-splits, beta, the automatic choice,
 and a grouped run that mixes the three shapes."""
 import numpy as np
 import pytest
@@ -20,11 +21,18 @@ CASES = {
     "narrow_n": ("mn", "mk", "kn", dict(m=1000, n=20, k=700), 1.0, 0.0, 2),
     # small N spread over two modes, beta, C's stride-one index in M
     "narrow_n_modes": ("abn", "akb", "nk", dict(a=37, b=29, n=45, k=300), 0.5, -1.0, 2),
-    # small M, N over several tiles with a tail
+    # small N, A's unit stride along k (pack-free: A gathered along k)
+    "narrow_n_kfast": ("mn", "km", "kn", dict(m=1000, n=20, k=700), 1.0, 0.0, 2),
+    # small M, N over several tiles with a tail (pack-free: both along k)
     "narrow_m": ("mn", "km", "kn", dict(m=11, n=900, k=500), 1.0, 0.5, 3),
     # small M from two modes, K a product of two modes with a tail
     "narrow_m_modes": ("abnp", "akbl", "nlkp", dict(a=5, b=4, n=60, p=7, k=13, l=9), 2.0, 0.0, 3),
 }
+
+
+# pack-free narrow tiles: which operands are gathered along k
+GATHER_K = {"narrow_n": "gather_k a=0 b=1", "narrow_n_kfast": "gather_k a=1 b=1",
+            "narrow_m": "gather_k a=1 b=1", "narrow_n_modes": "gather_k a=0 b=0"}
 
 
 def _data(lc, la, lb, sizes, seed):
@@ -49,6 +57,8 @@ def test_narrow_tile_matches_square_and_oracle(cuda, name, direct, precision):
                          tuning=Tuning(variant=v, simt_tile=1, ksplit=1, direct=direct))
     want = "tile=128x32x16" if tile == 2 else "tile=32x128x16"
     assert want in pn.describe() and "tile=128x128x16" in ps.describe(), pn.describe()
+    if direct == 1 and name in GATHER_K:
+        assert GATHER_K[name] in pn.describe(), pn.describe()
     assert np.array_equal(narrow, square)
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
     assert error_metrics(narrow, ref)["normwise"] <= 1e-6
