@@ -64,3 +64,14 @@ def test_null_arguments():
     size = (ctypes.c_int64 * 2)(2, 2)
     assert L.tccg_transpose(N.F32, 2, perm, size, None, None, 1.0, ctypes.c_void_p(8), 0.0,
                             ctypes.c_void_p(8), None) == N.ERR_INVALID
+
+
+def test_tuning_struct_matches_the_header():
+    """The ctypes mirror of tccg_tuning has the header's fields, in order,
+    and its size (every field an int32_t)."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct tccg_tuning \{(.*?)\} tccg_tuning;", src, re.S).group(1)
+    fields = re.findall(r"int32_t\s+([a-z_0-9]+)\s*;", body)
+    assert len(fields) == len(re.findall(r";", body)), "tccg_tuning holds int32_t fields only"
+    assert [f[0] for f in N.Tuning._fields_] == fields
+    assert ctypes.sizeof(N.Tuning) == 4 * len(fields)
