@@ -148,6 +148,8 @@ static int choose_simt_shape(const tccg_plan* p, double* padded_work) {
   return best;
 }
 
+static bool direct_eligible(const tccg_plan* p, int shape);
+
 static bool choose_simt(const tccg_plan* p) {
   if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) return true;
   if (p->tune.pair || p->tune.variant > 0) return false;
@@ -156,16 +158,18 @@ static bool choose_simt(const tccg_plan* p) {
   // batched workload): tensor cores at 0.6 PFLOP/s effective (x3 for
   // split-BF16x3) on 128 x 192 tiles with a C epilogue at 3 TB/s; CUDA cores
   // at 35 TFLOP/s; operands streamed three times (pack
-  // read, packed write, GEMM read) at 4.5 TB/s. Tile padding counts as work
+  // read, packed write, GEMM read) at 4.5 TB/s, once where the CUDA-core
+  // kernel reads them in place. Tile padding counts as work
   // (CUDA cores: that of the shape choose_simt_shape picks).
   const double M = (double)p->M, N = (double)p->N, K = (double)p->K;
   const double Mt = (double)round_up(p->M, 128), Nt = (double)round_up(p->N, 192);
   double simt_work = 0;  // padded M x N of the CUDA-core tile shape it would use
-  (void)choose_simt_shape(p, &simt_work);
+  const int shape = choose_simt_shape(p, &simt_work);
+  const double simt_passes = direct_eligible(p, shape) ? 1.0 : 3.0;  // operand reads
   const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
   const double t_tc = std::max(2.0 * Mt * Nt * K * (p->prec == TCCG_PREC_BF16X3 ? 3.0 : 1.0) / 0.6e15,
                                cb / 3e12 + 3.0 * op / 4.5e12);
-  const double t_simt = std::max(2.0 * simt_work * K / 35e12, (cb + 3.0 * op) / 4.5e12);
+  const double t_simt = std::max(2.0 * simt_work * K / 35e12, (cb + simt_passes * op) / 4.5e12);
   return t_simt < t_tc;
 }
 
@@ -176,20 +180,19 @@ static bool unit_first(int n, const int64_t* ext, const int64_t* str) {
   return true;
 }
 
-// The CUDA-core kernel reads the operands in place (no packing pass) when the
-// tuning asks for it, or -- automatically -- for a short K (bandwidth-bound:
-// the pack would triple the operand traffic) as long as each operand's
-// gather runs along a unit-stride mode or the operand is small enough to stay
-// cached. Not for TTGT (whose point is the transposition) and not where the
-// pack converts (bf16 operands, BF16 rounding).
-static bool choose_direct(const tccg_plan* p) {
-  if (!simt_path(p) || p->tune.method != TCCG_METHOD_GETT || p->tune.direct < 0) return false;
+// Whether the CUDA-core kernel with tile shape `shape` reads the operands in
+// place (no packing pass): asked for by the tuning, or -- automatically --
+// when the pack's extra traffic matters and each operand's gather runs along
+// a unit-stride mode (narrow tiles: a row mode or a K mode) or the operand is
+// small enough to stay cached; short K only for the square tile. Not for
+// TTGT (whose point is the transposition) and not where the pack converts
+// (bf16 operands, BF16 rounding).
+static bool direct_eligible(const tccg_plan* p, int shape) {
+  if (p->tune.method != TCCG_METHOD_GETT || p->tune.direct < 0) return false;
   if (p->dtype == TCCG_BF16 || p->prec == TCCG_PREC_BF16) return false;
   if (p->tune.direct > 0) return true;
   if (p->tune.shortk > 0) return false;  // the short-K kernel reads packed operands
-  // narrow tiles gather along k too (lanes along the operand's unit-stride
-  // K mode), so they take long K as well
-  const bool narrow = p->simt_shape != SIMT_SQUARE;
+  const bool narrow = shape != SIMT_SQUARE;
   if (p->K > 256 && !narrow) return false;
   // the pack's extra traffic (2 x the operands) must matter next to C's;
   // otherwise the 16-byte loads of packed operands win
@@ -201,6 +204,10 @@ static bool choose_direct(const tccg_plan* p) {
   const bool b_ok = unit_first(d.nn, d.n_ext, d.b_n_stride) || p->N * p->K * es <= small ||
                     (narrow && unit_first(d.nk, d.k_ext, d.b_k_stride));
   return a_ok && b_ok;
+}
+
+static bool choose_direct(const tccg_plan* p) {
+  return simt_path(p) && direct_eligible(p, p->simt_shape);
 }
 
 // Narrow tiles, direct loads: gather an operand along k when its unit
