@@ -41,8 +41,11 @@ struct PackOperand {
   // rows x (kb_lo * kb_run) consecutive k -- kb_lo = the product of the extents
   // of the K modes before u, kb_run consecutive values of u -- and is read with
   // u fastest (coalesced), reordered in shared memory and written K-major.
-  // kb_ext = u's extent, kb_step = u's stride (+1 or -1).
-  int32_t kb_lo, kb_run, kb_rows, kb_ext, kb_step;
+  // kb_ext = u's extent, kb_step = u's stride (+1 or -1). kb_quad = 1: every
+  // 4 consecutive u (u % 4 == 0) are 4 consecutive, 16-byte aligned source
+  // elements, and kb_lo, kb_run and kb_ext are multiples of 4: the tile
+  // moves them as one 16-byte copy.
+  int32_t kb_lo, kb_run, kb_rows, kb_ext, kb_step, kb_quad;
   // K-major layouts only: 1 = every quad of k (k % 4 == 0) is 4 consecutive,
   // 16-byte aligned source elements (the first K mode has unit stride): the
   // pass streams 16-byte loads straight into K-major stores.
@@ -287,6 +290,61 @@ __device__ __forceinline__ void pack_kblock(const PackOperand& o, int64_t kt, in
   }
 }
 
+// k-block tile with 16-byte copies (kb_quad): the tile is kept as the source
+// lays it out, raw[r][l][u] (u contiguous), 4 consecutive u per cp.async; the
+// 16-byte chunks of row (r, l) are rotated by l / 4 so that the write-out,
+// which reads 4 consecutive l of one u per quad of k, spreads over the banks.
+// Quads past K or the last row are read element by element (or zero).
+template <int LAYOUT>
+__device__ __forceinline__ void pack_kblock_quad(const PackOperand& o, int64_t kt, int64_t rt,
+                                                 float* tile) {
+  constexpr int NQ = PACK_KB_ELEMS / 4 / 256;  // 16-byte copies per thread at most
+  const int lo = o.kb_lo, run = o.kb_run, T = lo * run, R = o.kb_rows;
+  const int nch = run / 4;  // 16-byte chunks per (r, l) row
+  const int64_t k0 = kt * T, r0 = rt * R;
+  if (k0 >= o.Kcover || r0 >= o.Rcover) return;
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  const float* src = static_cast<const float*>(o.src);
+  const int u0 = (int)((kt * run) % o.kb_ext);  // u of the tile's first run (a multiple of 4)
+  // chunk c of row (r, l) lives at raw position ((r lo + l) run + 4 ((c + l/4) % nch))
+  auto chunk = [&](int r, int l, int c) {
+    return tile + (r * lo + l) * run + 4 * ((c + (l >> 2)) % nch);
+  };
+#pragma unroll
+  for (int i = 0; i < NQ; ++i) {
+    const int f = tid + 256 * i;  // f = (r lo + l) nch + c
+    if (f >= R * lo * nch) break;
+    const int c = f % nch, rl = f / nch, l = rl % lo, r = rl / lo;
+    const int u = 4 * c;
+    const int64_t row = r0 + r, k = k0 + l + (int64_t)lo * u;
+    float* d = chunk(r, l, c);
+    if (row < o.R && k + 3 * (int64_t)lo < o.Kk) {
+      const int64_t coff = u0 + u < o.kb_ext ? o.col_off[k0 + l] + u : o.col_off[k];
+      cp_async_16(d, src + o.row_off[row] + coff);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t kj = k + (int64_t)lo * j;
+        d[j] = (row < o.R && kj < o.Kk) ? src[o.row_off[row] + o.col_off[kj]] : 0.f;
+      }
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  const int Q = T / 4;  // quads of k per row: 4 consecutive l (lo % 4 == 0) of one u
+  for (int f = tid; f < R * Q; f += 256) {
+    const int r = f / Q, kq = (f - r * Q) * 4;
+    const int64_t k = k0 + kq, row = r0 + r;
+    if (row >= o.Rcover || k >= o.Kcover) continue;
+    const int l = kq % lo, u = kq / lo;
+    float x[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = chunk(r, l + j, u >> 2)[u & 3];
+    store_k4<LAYOUT>(static_cast<__nv_bfloat16*>(o.dst) + row * o.ld, k, o.Kcover, o.ld, x);
+  }
+}
+
 // Streaming K-major pack (kstream): quad q of the operand (quads numbered
 // row-major over Rcover x Kcover / 4) is k .. k+3 of one row, 4 consecutive
 // source elements (16 bytes, 8 for bf16 sources). A CTA moves 256 x
@@ -373,7 +431,10 @@ __device__ __forceinline__ void pack_any(const PackOperand& o, int64_t kt, int64
   }
   if constexpr (KMAJOR && sizeof(Tin) == 4 && (READ == PACK_READ_KBLOCK || READ == PACK_READ_ANY)) {
     if (READ == PACK_READ_KBLOCK || o.kb_lo > 0) {
-      pack_kblock<Tin, LAYOUT>(o, kt, rt, &tile[0][0]);
+      if (o.kb_quad)
+        pack_kblock_quad<LAYOUT>(o, kt, rt, &tile[0][0]);
+      else
+        pack_kblock<Tin, LAYOUT>(o, kt, rt, &tile[0][0]);
       return;
     }
   }

@@ -76,6 +76,8 @@ struct tccg_plan {
   // offset tables allow the streaming K-major pack (every quad of k is 4
   // consecutive elements, every quad start and row offset a multiple of 4)
   bool ks_a = false, ks_b = false;
+  // the k-block tiles of A / B may move 16-byte quads along u (kb_quad)
+  bool kbq_a = false, kbq_b = false;
   int32_t* d_status = nullptr;
   int32_t read_k_fast_a = 0, read_k_fast_b = 0;
   bool c_is_mn_dense = false;  // C is already the column-major [M-modes][N-modes] matrix
@@ -371,6 +373,26 @@ static void kblock_tiles(int nk, const int64_t* kext, const int64_t* kstr, int32
   kb[4] = kstr[u] > 0 ? 1 : -1;
 }
 
+// The k-block tiles of an operand (kblock_tiles) may move 4 consecutive u at
+// once: kb_lo, the run and u's extent multiples of 4, u's stride +1, and in
+// the column table every quad of u (u % 4 == 0) starts at a multiple of 4 and
+// runs over 4 consecutive elements.
+static bool kblock_quads(int nk, const int64_t* kext, const int64_t* kstr,
+                         const std::vector<int64_t>& coff) {
+  int32_t kb[5];
+  kblock_tiles(nk, kext, kstr, kb);
+  const int64_t lo = kb[0], run = kb[1], ext = kb[3];
+  if (lo == 0 || lo % 4 != 0 || run % 4 != 0 || ext % 4 != 0 || kb[4] != 1) return false;
+  const int64_t K = (int64_t)coff.size();
+  for (int64_t k = 0; k < K; ++k) {
+    if (((k / lo) % ext) % 4 != 0) continue;  // not the first u of a quad
+    if (coff[(size_t)k] % 4 != 0) return false;
+    for (int64_t j = 1; j < 4 && k + j * lo < K; ++j)
+      if (coff[(size_t)(k + j * lo)] != coff[(size_t)k] + j) return false;
+  }
+  return true;
+}
+
 // For a K-major pack whose rows are read one per lane: if a later row mode
 // has a smaller stride than the first (non-unit) mode, visit the rows with
 // that mode fastest. vsrc[v] = source offset, vdst[v] = destination row of
@@ -468,17 +490,21 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   }
   std::vector<int64_t> h;
   int rc = TCCG_OK;
+  // row offsets that are multiples of 4 and quads of k: the 16-byte pack
+  // reads (streaming pass, 16-byte k-block tiles)
   build_offsets(d.nm, d.m_ext, d.a_m_stride, h);
-  p->ks_a = rows_by_4(h);
+  const bool rows4_a = rows_by_4(h);
   if (!rc) rc = upload(h, &p->t_a_m);
   build_offsets(d.nk, d.k_ext, d.a_k_stride, h);
-  p->ks_a = p->ks_a && k_quads(h);
+  p->ks_a = rows4_a && k_quads(h);
+  p->kbq_a = rows4_a && kblock_quads(d.nk, d.k_ext, d.a_k_stride, h);
   if (!rc) rc = upload(h, &p->t_a_k);
   build_offsets(d.nn, d.n_ext, d.b_n_stride, h);
-  p->ks_b = rows_by_4(h);
+  const bool rows4_b = rows_by_4(h);
   if (!rc) rc = upload(h, &p->t_b_n);
   build_offsets(d.nk, d.k_ext, d.b_k_stride, h);
-  p->ks_b = p->ks_b && k_quads(h);
+  p->ks_b = rows4_b && k_quads(h);
+  p->kbq_b = rows4_b && kblock_quads(d.nk, d.k_ext, d.b_k_stride, h);
   if (!rc) rc = upload(h, &p->t_b_k);
   build_offsets(d.nm, d.m_ext, d.c_m_stride, h);
   // C is "already [M][N]" when its M modes are dense from stride 1 and the N
@@ -640,15 +666,16 @@ static int plan_layout(tccg_plan* p) {
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=gett_tc%s<%s> tile=%dx%d stages=%d M=%lld N=%lld K=%lld "
              "kblocks=%d chunk=%d ksplit=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
-             "visit a=%d b=%d kblock a=%dx%dx%d b=%dx%dx%d kstream a=%d b=%d)",
+             "visit a=%d b=%d kblock a=%dx%dx%d%s b=%dx%dx%d%s kstream a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", pair ? "2" : "", x3 ? "BF16X3" : "BF16",
              pair ? 256 : 128, p->bn,
              pair ? (x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES)
                   : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES),
              (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit,
              p->grid, p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
-             p->t_a_vsrc ? 1 : 0, p->t_b_vsrc ? 1 : 0, p->kb_a[0], p->kb_a[1], p->kb_a[2], p->kb_b[0],
-             p->kb_b[1], p->kb_b[2], p->ks_a ? 1 : 0, p->ks_b ? 1 : 0);
+             p->t_a_vsrc ? 1 : 0, p->t_b_vsrc ? 1 : 0, p->kb_a[0], p->kb_a[1], p->kb_a[2],
+             p->kb_a[0] && p->kbq_a ? " x16B" : "", p->kb_b[0], p->kb_b[1], p->kb_b[2],
+             p->kb_b[0] && p->kbq_b ? " x16B" : "", p->ks_a ? 1 : 0, p->ks_b ? 1 : 0);
   }
   if (ttgt) {
     // contiguous C' = [M][N] (column-major) in the workspace, then C' -> C
@@ -862,7 +889,7 @@ static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* 
   o.read_k_fast = kfast;
   o.active = 1;
   o.row_dst = nullptr;
-  o.kb_lo = o.kb_run = o.kb_rows = o.kb_ext = o.kb_step = 0;
+  o.kb_lo = o.kb_run = o.kb_rows = o.kb_ext = o.kb_step = o.kb_quad = 0;
   o.kstream = 0;
   o.ktiles = o.tiles = 0;
   return o;
@@ -871,8 +898,10 @@ static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* 
 // The read schedule of a K-major pack chosen at plan creation: the streaming
 // pass (when the source is aligned for its vector loads; es = source element
 // bytes) or k-block tiles, else unchanged.
-static PackOperand with_kread(PackOperand o, bool kstream, const int32_t (&kb)[5], size_t es) {
-  if (kstream && (reinterpret_cast<uintptr_t>(o.src) % (4 * es)) == 0) {
+static PackOperand with_kread(PackOperand o, bool kstream, const int32_t (&kb)[5], bool kb_quad,
+                              size_t es) {
+  const bool aligned = (reinterpret_cast<uintptr_t>(o.src) % (4 * es)) == 0;
+  if (kstream && aligned) {
     o.kstream = 1;
   } else if (kb[0] > 0) {
     o.kb_lo = kb[0];
@@ -880,6 +909,7 @@ static PackOperand with_kread(PackOperand o, bool kstream, const int32_t (&kb)[5
     o.kb_rows = kb[2];
     o.kb_ext = kb[3];
     o.kb_step = kb[4];
+    o.kb_quad = kb_quad && aligned ? 1 : 0;
   }
   return o;
 }
@@ -1055,10 +1085,10 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
   pa.op[0] = with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap,
                                            p->Kc, p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst),
-                        p->ks_a, p->kb_a, es);
+                        p->ks_a, p->kb_a, p->kbq_a, es);
   pa.op[1] = with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp,
                                            p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
-                        p->ks_b, p->kb_b, es);
+                        p->ks_b, p->kb_b, p->kbq_b, es);
   int rc;
   if (x3)
     rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s);
@@ -1630,10 +1660,10 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
     add_pack_jobs(jobs, pctas,
                   with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover,
                                                 w + p->off_a, p->Kc, p->read_k_fast_a),
-                                        p->t_a_vsrc, p->t_a_vdst), p->ks_a, p->kb_a, es),
+                                        p->t_a_vsrc, p->t_a_vdst), p->ks_a, p->kb_a, p->kbq_a, es),
                   with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover,
                                                 w + p->off_b, p->Kc, p->read_k_fast_b),
-                                        p->t_b_vsrc, p->t_b_vdst), p->ks_b, p->kb_b, es),
+                                        p->t_b_vsrc, p->t_b_vdst), p->ks_b, p->kb_b, p->kbq_b, es),
                   pack_k_tile<PACK_K_BF16>(), true);
     TcGroupItem it;
     memset(&it, 0, sizeof(it));

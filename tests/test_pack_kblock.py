@@ -4,7 +4,8 @@ reads runs along that mode (kb_lo * kb_run consecutive k per tile, kb_rows
 rows), reorders them in shared memory and writes K-major rows. Parity with
 the FP64 loop nest and with the CUDA-core kernel (which packs without them)
 for BF16x3 and BF16, on either operand, with K tails, runs that wrap into
-the next value of the higher K modes, and row tails."""
+the next value of the higher K modes, and row tails; element-wise and
+16-byte (4 consecutive u per copy) tiles."""
 import numpy as np
 import pytest
 
@@ -38,6 +39,11 @@ CASES = {
 }
 
 
+# tiles that move 16-byte quads along u (kb_lo, run and u's extent multiples
+# of 4, u's stride +1, aligned quads)
+QUAD = {"cfg4_small": True, "odd": False, "wrap": True, "long_lo": False, "third": True}
+
+
 def _run(name, precision, seed):
     import torch
     lc, la, lb, sizes, tag = CASES[name]
@@ -52,6 +58,7 @@ def _run(name, precision, seed):
     out, p = run_gpu(con, precision, A, B, C, tuning=Tuning(variant=16))
     assert "kernel=gett_tc<" in p.describe(), p.describe()
     assert "kblock " in p.describe() and tag in p.describe(), p.describe()
+    assert (" x16B" in p.describe()) == QUAD[name], p.describe()
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 1.25, 0.5)
     cc, _ = run_gpu(con, precision, A, B, C, tuning=Tuning(variant=-1))
     return out, ref, cc
