@@ -16,7 +16,8 @@
 // release the accumulator with remote arrives on the even CTA's barrier.
 // K is accumulated in chunks (as in tc_gemm.cuh) for BF16X3.
 //
-// No multicast of any kind: every CTA loads its own operand halves.
+// Every CTA loads its own operand halves with its own TMA loads (no load is
+// shared between the two CTAs of a pair).
 #pragma once
 #include "tc_gemm.cuh"
 
