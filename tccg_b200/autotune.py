@@ -25,7 +25,9 @@ from typing import List, Optional, Tuple
 from .plan import Plan, Tuning
 from .spec import Contraction
 
-CODE_VERSION = "tccg_b200-0.1"
+# Part of every cache key: cached winners measured on older kernels (or
+# without the tuning fields a newer build searches) are not reused.
+CODE_VERSION = "tccg_b200-0.2"
 
 
 def default_db_path() -> str:
