@@ -115,6 +115,9 @@ typedef struct tccg_tuning {
   int32_t simt_tile;   /* CUDA-core tile shape, FP32 accumulation: 0 = the least padded work
                           (narrow tiles counted at 1.6x), 1 = 128x128, 2 = 128x32 (small N),
                           3 = 32x128 (small M); FP64 always 128x64 */
+  int32_t tail_split;  /* tcgen05, automatic k-split: 0 = run the tiles of a short last round of
+                          the persistent grid as k slices where that pays, -1 = never (grouped
+                          runs never split that way) */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */
@@ -210,7 +213,9 @@ int tccg_transpose(int32_t dtype, int32_t dim, const int32_t* perm, const int64_
  * grouped k-split reduction, each only when it has work. tccg_group_bind fixes
  * the operand pointers and workspace (it uploads the work lists,
  * synchronously), after which tccg_group_run only launches kernels and can be
- * captured in a CUDA graph.
+ * captured in a CUDA graph. Groups run a plan's tcgen05 tiles without its tail
+ * split (tuning.tail_split); plans made with tail_split = -1 give the same
+ * sums in a group as alone.
  */
 typedef struct tccg_group tccg_group; /* opaque */
 int tccg_group_create(const tccg_plan* const* plans, int32_t count, tccg_group** out);

@@ -77,6 +77,15 @@ struct TcArgs {
   // alpha/beta. ksplit == 1 writes C directly.
   int32_t ksplit, kb_per_split;
   float* partial;
+  // Tail split (ksplit == 1, tail_split > 1): tiles [0, full_tiles) of the
+  // tile order run over all of K; each of the remaining tail = tiles -
+  // full_tiles tiles runs as tail_split slices of tail_kb k-blocks (tile index
+  // full_tiles + z * tail + t) that write raw sums to
+  // tail_partial[((z * tail + t) * BN + n_local) * 128 + m_local];
+  // tc_tail_reduce_kernel adds the slices and applies alpha/beta. It fills the
+  // last round of the persistent grid instead of leaving it mostly idle.
+  int32_t full_tiles, tail_split, tail_kb;
+  float* tail_partial;
 };
 
 // Grouped launch: one entry per contraction, in device memory. The tensor maps
@@ -114,10 +123,21 @@ struct TileRef {
   const CUtensorMap* tB;
   int tm, tn;
   int z, kb_begin, kb_end;
+  int tail;  // index among the tail tiles (a slice of it), or -1
 };
 
 __device__ __forceinline__ void split_coords(int local, const TcArgs& a, TileRef& r) {
   const int mn = a.tiles_m * a.tiles_n;
+  r.tail = -1;
+  if (a.tail_split > 1 && local >= a.full_tiles) {
+    const int tail = mn - a.full_tiles, u = local - a.full_tiles;
+    r.z = u / tail;
+    r.tail = u - r.z * tail;
+    tile_coords(a.full_tiles + r.tail, a, r.tm, r.tn);
+    r.kb_begin = r.z * a.tail_kb;
+    r.kb_end = r.kb_begin + a.tail_kb < a.num_kb ? r.kb_begin + a.tail_kb : a.num_kb;
+    return;
+  }
   r.z = local / mn;
   tile_coords(local - r.z * mn, a, r.tm, r.tn);
   r.kb_begin = r.z * a.kb_per_split;
@@ -163,7 +183,11 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int num_tiles = GROUPED ? g.total_tiles : a1->tiles_m * a1->tiles_n * a1->ksplit;
+  const int num_tiles =
+      GROUPED ? g.total_tiles
+              : (a1->tail_split > 1
+                     ? a1->full_tiles + (a1->tiles_m * a1->tiles_n - a1->full_tiles) * a1->tail_split
+                     : a1->tiles_m * a1->tiles_n * a1->ksplit);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -303,8 +327,21 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       const int64_t n0 = (int64_t)t.tn * Cfg::BN + h * HC;
       const int64_t nlim = a.N - n0;
       const float alpha = a.alpha, beta = a.beta;
-      // k-split slice: raw sums to partial[z][n][M] (coalesced along m)
-      float* part = a.partial ? a.partial + (size_t)t.z * a.N * a.M + m : nullptr;
+      // k-split slice: raw sums to partial[z][n][M], a tail slice to its
+      // tile's block of tail_partial (both coalesced along m): element
+      // (m, column c of this warp's half) at part[(pc0 + c) * pld]
+      float* part = nullptr;
+      int64_t pld = 0, pc0 = 0;
+      if (t.tail >= 0) {
+        const int tail = a.tiles_m * a.tiles_n - a.full_tiles;
+        part = a.tail_partial + ((size_t)(t.z * tail + t.tail) * Cfg::BN) * Cfg::BM + q * 32 + lane;
+        pld = Cfg::BM;
+        pc0 = h * HC;
+      } else if (a.partial) {
+        part = a.partial + (size_t)t.z * a.N * a.M + m;
+        pld = a.M;
+        pc0 = n0;
+      }
       if constexpr (MODE == TC_BF16) {
         // one accumulator per tile: stream TMEM -> C
         if (!mbar_wait(&accf[acc], acc_phase)) {
@@ -334,7 +371,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
           if (m_ok && part) {
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-              if (cc + j < nlim) part[(size_t)(n0 + cc + j) * a.M] = __uint_as_float(r[j]);
+              if (cc + j < nlim) part[(size_t)(pc0 + cc + j) * pld] = __uint_as_float(r[j]);
           } else if (m_ok) {
             if (beta != 0.0f) {
               float old[32];
@@ -394,7 +431,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
         if (m_ok && part) {
 #pragma unroll
           for (int j = 0; j < HC; ++j)
-            if (j < nlim) part[(size_t)(n0 + j) * a.M] = sum[j];
+            if (j < nlim) part[(size_t)(pc0 + j) * pld] = sum[j];
         } else if (m_ok) {
           if (beta != 0.0f) {
 #pragma unroll
@@ -438,6 +475,29 @@ template <int MODE>
 __global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
     gett_tc_group_kernel(const TcGroup g, int32_t* status) {
   gett_tc_body<MODE, true>(nullptr, nullptr, nullptr, g, status);
+}
+
+// Tail split: C = alpha * (slice 0 + slice 1 + ...) + beta * C over the tail
+// tiles (RN adds in slice order). grid = (tail tiles, BM * BN / 256), block
+// 256: thread e of a tile takes element (m_local = e % BM, n_local = e / BM).
+template <int MODE>
+__global__ void __launch_bounds__(256) tc_tail_reduce_kernel(const TcArgs a) {
+  using Cfg = TcCfgT<MODE>;
+  const int tail = a.tiles_m * a.tiles_n - a.full_tiles;
+  const int tl = blockIdx.x;
+  const int e = blockIdx.y * 256 + threadIdx.x;
+  if (tl >= tail || e >= Cfg::BM * Cfg::BN) return;
+  const int ml = e % Cfg::BM, nl = e / Cfg::BM;
+  int tm, tn;
+  tile_coords(a.full_tiles + tl, a, tm, tn);
+  const int64_t m = (int64_t)tm * Cfg::BM + ml, n = (int64_t)tn * Cfg::BN + nl;
+  if (m >= a.M || n >= a.N) return;
+  const float* p = a.tail_partial + ((size_t)tl * Cfg::BN + nl) * Cfg::BM + ml;
+  const size_t slice = (size_t)tail * Cfg::BN * Cfg::BM;
+  float s = p[0];
+  for (int z = 1; z < a.tail_split; ++z) s = __fadd_rn(s, p[z * slice]);
+  float* c = a.C + a.c_m_off[m] + a.c_n_off[n];
+  *c = a.beta != 0.0f ? fmaf(a.beta, *c, a.alpha * s) : a.alpha * s;
 }
 
 }  // namespace tccg

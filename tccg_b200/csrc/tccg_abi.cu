@@ -89,6 +89,9 @@ struct tccg_plan {
   int64_t Kc = 0;
   int32_t num_kb = 0, tiles_m = 0, tiles_n = 0, raster = 8, grid = 0, chunk_kb = 1, bn = 256;
   int32_t kb_per_split = 0;
+  // tail split of the tcgen05 tile order (TcArgs): tiles [0, full_tiles) over
+  // all of K, the rest as tail_split slices of tail_kb k-blocks; 1 = none
+  int32_t full_tiles = 0, tail_split = 1, tail_kb = 0;
   bool direct = false;  // CUDA-core kernel gathers operands without a packing pass
   bool gather_k_a = false, gather_k_b = false;  // direct, narrow tiles: gathers along k
   bool shortk = false;  // short-K CUDA-core kernel prefetching C (simt_shortk_kernel)
@@ -96,7 +99,7 @@ struct tccg_plan {
   int32_t simt_bm = 0, simt_bn = 0;   // its tile extents
   bool simt = false;    // CUDA-core kernels (else tcgen05)
   // workspace layout
-  size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, ws_bytes = 0;
+  size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, off_tail = 0, ws_bytes = 0;
   char describe[512] = "";
 };
 
@@ -646,6 +649,36 @@ static int plan_layout(tccg_plan* p) {
     p->kb_per_split = (int32_t)choose_ksplit(pair ? 1 : p->tune.ksplit, tiles, p->num_kb, ctas,
                                              x3 ? p->chunk_kb : 8, &p->ksplit);
     tiles *= p->ksplit;
+    // Tail split: whole rounds of the persistent grid plus a short tail (at
+    // most half a round) -- the tail's tiles run as k slices that fill the
+    // last round while the full tiles keep all of K. It saves (1 - 1/slices)
+    // of a tile's time and costs the slices' partial sums (written, read back,
+    // C written) and a launch, so it is taken only for long tiles: a tile at
+    // about 0.52 us per k-block (BF16X3, 128 x 192) or 0.47 us (BF16,
+    // 128 x 256), the partial sums at 6.5 TB/s, 5 us fixed. Automatic k-split
+    // only (not with an explicit ksplit, nor for the CTA-pair kernel).
+    const int64_t mn = (int64_t)p->tiles_m * p->tiles_n;
+    p->full_tiles = 0;
+    p->tail_split = 1;
+    p->tail_kb = 0;
+    if (!pair && p->ksplit == 1 && p->tune.ksplit == 0 && p->tune.tail_split >= 0 && mn > ctas) {
+      const int64_t full = mn / ctas * ctas, tail = mn - full;
+      const int64_t min_kb = x3 ? p->chunk_kb : 8;
+      const int64_t want = tail > 0 ? std::min<int64_t>(ctas / tail, p->num_kb / min_kb) : 0;
+      if (tail > 0 && 2 * tail <= ctas && want >= 2) {
+        const int64_t per = cdiv(p->num_kb, want);  // no empty slice
+        const int64_t splits = cdiv(p->num_kb, per);
+        const double t_tile = p->num_kb * (x3 ? 0.52e-6 : 0.47e-6);
+        const double t_sum =
+            5e-6 + (double)tail * 128 * p->bn * 4 * (2.0 * splits + 2.0) / 6.5e12;
+        if ((1.0 - 1.0 / splits) * t_tile > t_sum) {
+          p->tail_kb = (int32_t)per;
+          p->tail_split = (int32_t)splits;
+          p->full_tiles = (int32_t)full;
+          tiles = full + tail * p->tail_split;
+        }
+      }
+    }
     if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
     if (pair) {  // clusters of two CTAs, one pair tile per cluster at a time
       int resident = 0;
@@ -663,16 +696,21 @@ static int plan_layout(tccg_plan* p) {
       p->off_part = ws;
       ws = align_up(ws + (size_t)p->ksplit * p->N * p->M * 4, 256);
     }
+    if (p->tail_split > 1) {  // FP32 tail slices [split][tail tile][BN][128]
+      p->off_tail = ws;
+      ws = align_up(ws + (size_t)p->tail_split * (size_t)(mn - p->full_tiles) * p->bn * 128 * 4, 256);
+    }
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=gett_tc%s<%s> tile=%dx%d stages=%d M=%lld N=%lld K=%lld "
-             "kblocks=%d chunk=%d ksplit=%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
+             "kblocks=%d chunk=%d ksplit=%d tail=%dx%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
              "visit a=%d b=%d kblock a=%dx%dx%d%s b=%dx%dx%d%s kstream a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", pair ? "2" : "", x3 ? "BF16X3" : "BF16",
              pair ? 256 : 128, p->bn,
              pair ? (x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES)
                   : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES),
              (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit,
-             p->grid, p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
+             p->tail_split > 1 ? (int)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles) : 0,
+             p->tail_split, p->grid, p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
              p->t_a_vsrc ? 1 : 0, p->t_b_vsrc ? 1 : 0, p->kb_a[0], p->kb_a[1], p->kb_a[2],
              p->kb_a[0] && p->kbq_a ? " x16B" : "", p->kb_b[0], p->kb_b[1], p->kb_b[2],
              p->kb_b[0] && p->kbq_b ? " x16B" : "", p->ks_a ? 1 : 0, p->ks_b ? 1 : 0);
@@ -1103,7 +1141,7 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   if (rc) return rc;
   rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, pair ? p->bn / 2 : p->bn);
   if (rc) return rc;
-  TcArgs a;
+  TcArgs a{};
   a.M = (int32_t)p->M;
   a.N = (int32_t)p->N;
   a.K = (int32_t)p->K;
@@ -1121,6 +1159,10 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.ksplit = p->ksplit;
   a.kb_per_split = p->kb_per_split;
   a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(ws + p->off_part) : nullptr;
+  a.full_tiles = p->full_tiles;
+  a.tail_split = p->tail_split;
+  a.tail_kb = p->tail_kb;
+  a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
   mark(1, 0, s);
   if (pair && x3)
     gett_tc2_kernel<TC_BF16X3><<<p->grid, Tc2Cfg<TC_BF16X3>::NUM_THREADS,
@@ -1136,7 +1178,20 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
                               s>>>(tmA, tmB, a);
   mark(1, 1, s);
   rc = launch_check("gett_tc");
-  if (rc || p->ksplit == 1) return rc;
+  if (rc) return rc;
+  if (p->tail_split > 1) {
+    const unsigned tail = (unsigned)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles);
+    mark(2, 0, s);
+    if (x3)
+      tc_tail_reduce_kernel<TC_BF16X3>
+          <<<dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), 256, 0, s>>>(a);
+    else
+      tc_tail_reduce_kernel<TC_BF16>
+          <<<dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), 256, 0, s>>>(a);
+    mark(2, 1, s);
+    return launch_check("tc_tail_reduce");
+  }
+  if (p->ksplit == 1) return rc;
   dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
   mark(2, 0, s);
   simt_reduce_kernel<float><<<g2, 256, 0, s>>>(a.partial, p->ksplit, p->M, p->N, p->M, p->N, Cout,
@@ -1988,7 +2043,7 @@ extern "C" int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, c
   CUtensorMap tmA, tmB;
   if ((rc = encode_kmajor(&tmA, w + o_pa, M, Kc, Cfg::BM))) return rc;
   if ((rc = encode_kmajor(&tmB, w + o_pb, N, Kc, Cfg::BN))) return rc;
-  TcArgs a;
+  TcArgs a{};
   a.M = (int32_t)M;
   a.N = (int32_t)N;
   a.K = (int32_t)K;

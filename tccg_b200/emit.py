@@ -50,7 +50,7 @@ def source(con: Contraction, precision: str, tuning: Tuning, float_type: str) ->
 #include "gett.h"
 
 static const tccg_desc kDesc = %(desc)s;
-static const tccg_tuning kTuning = {%(method)s, %(variant)d, %(ksplit)d, %(raster)d, %(max_ctas)d, %(pair)d, %(direct)d, %(shortk)d, %(simt_tile)d};
+static const tccg_tuning kTuning = {%(method)s, %(variant)d, %(ksplit)d, %(raster)d, %(max_ctas)d, %(pair)d, %(direct)d, %(shortk)d, %(simt_tile)d, %(tail_split)d};
 
 static tccg_plan* g_plan = NULL;
 static void* g_ws = NULL;
@@ -89,7 +89,8 @@ int gett_last_status(void) { return g_status; }
 ''' % dict(spec=spec, precision=precision, tkey=tuning.key(), desc=desc, method=method,
            variant=tuning.variant, ksplit=tuning.ksplit, raster=tuning.raster,
            max_ctas=tuning.max_ctas, pair=tuning.pair, direct=tuning.direct,
-           shortk=tuning.shortk, simt_tile=tuning.simt_tile, dt=dt, prec=prec, T=T)
+           shortk=tuning.shortk, simt_tile=tuning.simt_tile,
+           tail_split=tuning.tail_split, dt=dt, prec=prec, T=T)
 
 
 def header(float_type: str) -> str:

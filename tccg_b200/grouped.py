@@ -16,6 +16,7 @@ baseline: one tccg_plan_run per contraction.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from typing import List, Optional, Sequence
 
 from . import _native as N
@@ -28,7 +29,11 @@ class Group:
                  tunings: Optional[Sequence[Tuning]] = None, dtype: Optional[str] = None):
         self.contractions = list(contractions)
         self.precision = precision
-        tunings = tunings or [None] * len(self.contractions)
+        # the grouped kernels do not run the tcgen05 tail split (the other
+        # items' tiles fill the persistent grid's rounds anyway): plans made
+        # without it, so that grouped and per-item runs compute the same sums
+        tunings = [dataclasses.replace(t or Tuning(), tail_split=-1)
+                   for t in (tunings or [None] * len(self.contractions))]
         self.plans: List[Plan] = [Plan(c, precision=precision, tuning=t, dtype=dtype)
                                   for c, t in zip(self.contractions, tunings)]
         self._lib = N.lib()

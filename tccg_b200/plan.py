@@ -157,6 +157,7 @@ class Tuning:
     direct: int = 0  # CUDA-core kernels: 0 auto, 1 no packing pass, -1 always pack
     shortk: int = 0  # CUDA-core kernels, K <= 32: 0 auto, 1 kernel prefetching C, -1 never
     simt_tile: int = 0  # CUDA-core tiles: 0 auto, 1 128x128, 2 128x32, 3 32x128
+    tail_split: int = 0  # tcgen05: 0 auto (k slices for a short last round), -1 never
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -169,12 +170,13 @@ class Tuning:
         t.direct = int(self.direct)
         t.shortk = int(self.shortk)
         t.simt_tile = int(self.simt_tile)
+        t.tail_split = int(self.tail_split)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d" % (self.method, self.ksplit, self.raster,
-                                                       self.max_ctas, self.variant, self.pair,
-                                                       self.direct, self.shortk, self.simt_tile)
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d" % (
+            self.method, self.ksplit, self.raster, self.max_ctas, self.variant, self.pair,
+            self.direct, self.shortk, self.simt_tile, self.tail_split)
 
 
 class Plan:
