@@ -129,6 +129,8 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             if K <= 32:
                 simt += [Tuning(method=method, variant=-1, shortk=1),
                          Tuning(method=method, variant=-1, shortk=-1)]
+            # the tcgen05 tail split off (it is on where the model expects a gain)
+            tc.append(Tuning(method=method, tail_split=-1))
             out += [Tuning(method=method)] + ((simt + tc) if K <= 128 else (tc + simt))
     return out
 
