@@ -242,7 +242,6 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
-    constexpr uint32_t idesc = idesc_bf16_f32(Cfg::BM, Cfg::BN);
     int stage = 0;
     uint32_t phase = 0;
     int acc = 0;
@@ -251,6 +250,12 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
       const int nkb = t.kb_end, K = t.a->K, ckb = t.a->chunk_kb;
+      // the MMAs stop at the tile's last column of C, rounded up to 32 (the
+      // epilogue reads no further): a narrow C, or the last column tile,
+      // costs only the tensor work its columns need
+      const int64_t ncols = t.a->N - (int64_t)t.tn * Cfg::BN;
+      const uint32_t idesc =
+          idesc_bf16_f32(Cfg::BM, ncols >= Cfg::BN ? Cfg::BN : (int)((ncols + 31) / 32) * 32);
       for (int kb0 = t.kb_begin; kb0 < nkb && ok; kb0 += ckb) {
         if (!mbar_wait(&acce[acc], acc_phase ^ 1)) {
           record_error(status, 2);
