@@ -120,6 +120,18 @@ __device__ __forceinline__ void record_error(int32_t* status, int32_t code) {
   if (status) atomicCAS(status, 0, code);
 }
 
+// ---- programmatic dependent launch ------------------------------------------
+// A kernel launched with the programmatic-stream-serialization attribute may
+// start while the kernel before it on the stream is still running. It calls
+// grid_dep_wait() before reading anything that kernel writes: the wait returns
+// once that grid has completed and its writes are visible (at once for an
+// ordinary launch). grid_dep_launch() lets the next kernel's CTAs start as
+// soon as every CTA of this grid has issued it.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---- tcgen05 ---------------------------------------------------------------
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -446,6 +446,7 @@ __device__ __forceinline__ void pack_any(const PackOperand& o, int64_t kt, int64
 // k tile x % ktiles of row tile x / ktiles of operand z.
 template <typename Tin, typename Tout, int LAYOUT, int READ>
 __global__ void __launch_bounds__(256) pack_kernel(const PackArgs args) {
+  grid_dep_launch();  // the GETT kernel may launch now; it waits for this grid's writes
   const PackOperand& o = args.op[blockIdx.z];
   if (!o.active || (int64_t)blockIdx.x >= o.tiles) return;
   pack_any<Tin, Tout, LAYOUT, READ>(o, (int64_t)blockIdx.x % o.ktiles, (int64_t)blockIdx.x / o.ktiles);

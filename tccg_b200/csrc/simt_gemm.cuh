@@ -502,6 +502,7 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
 
 template <typename T, int LOAD, int S = SIMT_SQUARE>
 __global__ void __launch_bounds__(256, SimtCfg<T, S>::MIN_BLOCKS) simt_gett_kernel(const SimtArgs<T> a) {
+  grid_dep_wait();  // packed operands written by the kernel before
   simt_gett_tile<T, LOAD, S>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -568,7 +569,15 @@ __global__ void __launch_bounds__(256, 2)
       mbar_init(bar, 1);
       fence_mbar_init();
     }
+    __syncthreads();
+    // the packing kernel before this one does not write C: the block comes
+    // in while that kernel may still run
+    if (read_c && tid == 0) {
+      mbar_arrive_expect_tx(bar, (uint32_t)SC::C_BYTES);
+      tma_load_2d(Cs, &tmC, (int32_t)m0, (int32_t)n0, bar);
+    }
   }
+  grid_dep_wait();  // packed operands written by the kernel before
   // operand panels first: their latency runs under the offset loads
   for (int c = tid; c < kp * (BM / VEC); c += 256) {
     const int row = c / (BM / VEC), col = (c % (BM / VEC)) * VEC;
@@ -593,27 +602,24 @@ __global__ void __launch_bounds__(256, 2)
     vq = cmo[3] != NONE && cmo[1] == cmo[0] + 1 && cmo[2] == cmo[0] + 2 && cmo[3] == cmo[0] + 3;
   }
   auto aligned16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-  __syncthreads();  // mbarrier initialised, Cn staged
-  if constexpr (TMA) {
-    if (read_c && tid == 0) {
-      mbar_arrive_expect_tx(bar, (uint32_t)SC::C_BYTES);
-      tma_load_2d(Cs, &tmC, (int32_t)m0, (int32_t)n0, bar);
-    }
-  } else if (read_c && cmo[0] != NONE) {
+  if constexpr (!TMA) {
+    __syncthreads();  // Cn staged
+    if (read_c && cmo[0] != NONE) {
 #pragma unroll
-    for (int u = 0; u < ITER; ++u) {
-      const int col = u * CPI + cl;
-      const int64_t no = Cn[col];
-      if (no == NONE) continue;
-      T* dst = Cs + col * BM + 4 * q;
-      const T* src = a.C + cmo[0] + no;
-      if (vq && aligned16(src)) {
-        cp_async_16(dst, src);
-        if constexpr (sizeof(T) == 8) cp_async_16(dst + 2, src + 2);
-      } else {
+      for (int u = 0; u < ITER; ++u) {
+        const int col = u * CPI + cl;
+        const int64_t no = Cn[col];
+        if (no == NONE) continue;
+        T* dst = Cs + col * BM + 4 * q;
+        const T* src = a.C + cmo[0] + no;
+        if (vq && aligned16(src)) {
+          cp_async_16(dst, src);
+          if constexpr (sizeof(T) == 8) cp_async_16(dst + 2, src + 2);
+        } else {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if (cmo[i] != NONE) cp_async_elem<sizeof(T)>(dst + i, a.C + cmo[i] + no);
+          for (int i = 0; i < 4; ++i)
+            if (cmo[i] != NONE) cp_async_elem<sizeof(T)>(dst + i, a.C + cmo[i] + no);
+        }
       }
     }
   }
@@ -748,6 +754,7 @@ __global__ void __launch_bounds__(256) simt_reduce_kernel(const T* __restrict__ 
                                                           const int64_t* c_m_off,
                                                           const int64_t* c_n_off, T alpha,
                                                           T beta) {
+  grid_dep_wait();  // partial sums written by the GETT kernel before
   const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
   if (m >= M) return;
   const int64_t cmo = c_m_off[m];

@@ -155,6 +155,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Tc2Cfg<MODE>::NUM_TH
   cluster_sync();  // barriers of both CTAs initialised, TMEM allocated
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
+  grid_dep_wait();  // packed operands written by the kernel before
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer (both CTAs) ----------------

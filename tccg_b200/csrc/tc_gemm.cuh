@@ -210,6 +210,9 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
+  // barriers and TMEM were set up while the packing kernel may still run:
+  // its operands (and nothing else this kernel reads) come from it
+  grid_dep_wait();
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
@@ -488,6 +491,7 @@ __global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
 template <int MODE>
 __global__ void __launch_bounds__(256) tc_tail_reduce_kernel(const TcArgs a) {
   using Cfg = TcCfgT<MODE>;
+  grid_dep_wait();  // partial sums written by the GETT kernel before
   const int tail = a.tiles_m * a.tiles_n - a.full_tiles;
   const int tl = blockIdx.x;
   const int e = blockIdx.y * 256 + threadIdx.x;

@@ -6,10 +6,12 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/tccg_b200.h"
@@ -911,6 +913,35 @@ static int launch_check(const char* what) {
   return TCCG_OK;
 }
 
+// Programmatic dependent launch of a kernel that directly follows one of this
+// library's own kernels on the stream (packing -> GETT, GETT -> reduction):
+// its CTAs may start, and set up barriers and TMEM, while that kernel drains;
+// they call grid_dep_wait() before reading its output, and read nothing
+// before it that an earlier kernel of the call could still be writing. Off
+// under per-kernel event timing (an event between the two kernels) and with
+// TCCG_B200_PDL=0 in the environment.
+static bool pdl_enabled() {
+  if (g_events) return false;
+  const char* e = std::getenv("TCCG_B200_PDL");
+  return !(e && e[0] == '0');
+}
+
+template <typename... P, typename... A>
+static void launch_after(bool after_own_kernel, void (*kernel)(P...), dim3 grid, dim3 block,
+                         size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = after_own_kernel && pdl_enabled() ? 1 : 0;
+  (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);  // launch_check reads the error
+}
+
 static PackOperand pack_op(const void* src, const int64_t* roff, const int64_t* coff, int64_t R,
                            int64_t Kk, int64_t Rcover, int64_t Kcover, void* dst, int64_t ld,
                            int32_t kfast) {
@@ -986,7 +1017,8 @@ static int pack_read(const PackOperand& o) {
 // schedule, or the kernel holding all schedules when they differ (a second
 // launch costs more than the wider kernel's extra registers).
 template <typename Tin, typename Tout, int LAYOUT>
-static int launch_pack(PackArgs pa, cudaStream_t s) {
+static int launch_pack(PackArgs pa, cudaStream_t s, bool* launched = nullptr) {
+  if (launched) *launched = false;
   int64_t ctas = 0;
   int read = -1;
   for (PackOperand& o : pa.op) {
@@ -997,6 +1029,7 @@ static int launch_pack(PackArgs pa, cudaStream_t s) {
   }
   if (ctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "operand too large to pack (%lld tiles)", (long long)ctas);
   if (ctas == 0) return TCCG_OK;
+  if (launched) *launched = true;
   const dim3 grid((unsigned)ctas, 1, 2), block(32, 8);
   constexpr bool KMAJOR = LAYOUT == PACK_K_BF16 || LAYOUT == PACK_K_BF16X3;
   mark(0, 0, s);
@@ -1030,18 +1063,21 @@ static void set_direct(SimtArgs<T>& a, const tccg_plan* p, const void* GA, const
 
 // simt_gett_kernel with the plan's tile shape (FP32: three shapes).
 template <typename T, int LOAD>
-static void launch_simt_tiles(const tccg_plan* p, const SimtArgs<T>& a, dim3 grid, cudaStream_t s) {
+static void launch_simt_tiles(const tccg_plan* p, const SimtArgs<T>& a, dim3 grid, bool after,
+                              cudaStream_t s) {
   if constexpr (sizeof(T) == 4) {
     if (p->simt_shape == SIMT_NARROW_N) {
-      simt_gett_kernel<T, LOAD, SIMT_NARROW_N><<<grid, 256, simt_smem_bytes<T, SIMT_NARROW_N>(), s>>>(a);
+      launch_after(after, simt_gett_kernel<T, LOAD, SIMT_NARROW_N>, grid, dim3(256),
+                   simt_smem_bytes<T, SIMT_NARROW_N>(), s, a);
       return;
     }
     if (p->simt_shape == SIMT_NARROW_M) {
-      simt_gett_kernel<T, LOAD, SIMT_NARROW_M><<<grid, 256, simt_smem_bytes<T, SIMT_NARROW_M>(), s>>>(a);
+      launch_after(after, simt_gett_kernel<T, LOAD, SIMT_NARROW_M>, grid, dim3(256),
+                   simt_smem_bytes<T, SIMT_NARROW_M>(), s, a);
       return;
     }
   }
-  simt_gett_kernel<T, LOAD><<<grid, 256, simt_smem_bytes<T>(), s>>>(a);
+  launch_after(after, simt_gett_kernel<T, LOAD>, grid, dim3(256), simt_smem_bytes<T>(), s, a);
 }
 
 template <typename T>
@@ -1055,17 +1091,18 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   pa.op[0] = pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->Mp, p->Kp, Ap, p->Mp, p->read_k_fast_a);
   pa.op[1] = pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->Np, p->Kp, Bp, p->Np, p->read_k_fast_b);
   int rc = TCCG_OK;
+  bool packed = false;  // the packing kernel is the last launch on s
   if (p->direct) {
     // no packing pass
   } else if constexpr (sizeof(T) == 8) {
-    rc = launch_pack<T, T, PACK_MN>(pa, s);
+    rc = launch_pack<T, T, PACK_MN>(pa, s, &packed);
   } else {
     if (p->dtype == TCCG_BF16)
-      rc = launch_pack<__nv_bfloat16, float, PACK_MN>(pa, s);
+      rc = launch_pack<__nv_bfloat16, float, PACK_MN>(pa, s, &packed);
     else if (p->prec == TCCG_PREC_BF16)
-      rc = launch_pack<float, float, PACK_MN_BF16>(pa, s);
+      rc = launch_pack<float, float, PACK_MN_BF16>(pa, s, &packed);
     else
-      rc = launch_pack<float, float, PACK_MN>(pa, s);
+      rc = launch_pack<float, float, PACK_MN>(pa, s, &packed);
   }
   if (rc) return rc;
   SimtArgs<T> a;
@@ -1091,21 +1128,23 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   CUtensorMap tmC{};
   if (p->shortk && shortk_tma(p, c_ldc) &&
       encode_c2d<T>(&tmC, Cout, p->M, p->N, c_ldc, Cfg::BM, Cfg::BN))
-    simt_shortk_kernel<T, true><<<grid, 256, SimtShortKCfg<T>::SMEM_BYTES, s>>>(a, tmC);
+    launch_after(packed, simt_shortk_kernel<T, true>, grid, dim3(256),
+                 SimtShortKCfg<T>::SMEM_BYTES, s, a, tmC);
   else if (p->shortk)
-    simt_shortk_kernel<T, false><<<grid, 256, SimtShortKCfg<T>::SMEM_BYTES, s>>>(a, tmC);
+    launch_after(packed, simt_shortk_kernel<T, false>, grid, dim3(256),
+                 SimtShortKCfg<T>::SMEM_BYTES, s, a, tmC);
   else if (p->direct)
-    launch_simt_tiles<T, SIMT_DIRECT>(p, a, grid, s);
+    launch_simt_tiles<T, SIMT_DIRECT>(p, a, grid, false, s);
   else
-    launch_simt_tiles<T, SIMT_PACKED>(p, a, grid, s);
+    launch_simt_tiles<T, SIMT_PACKED>(p, a, grid, packed, s);
   mark(1, 1, s);
   rc = launch_check("simt_gett");
   if (rc) return rc;
   if (p->ksplit > 1) {
     dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
     mark(2, 0, s);
-    simt_reduce_kernel<T><<<g2, 256, 0, s>>>(a.partial, p->ksplit, p->Mp, p->Np, p->M, p->N,
-                                             Cout, c_m, c_n, alpha, beta);
+    launch_after(true, simt_reduce_kernel<T>, g2, dim3(256), 0, s, a.partial, (int)p->ksplit,
+                 p->Mp, p->Np, p->M, p->N, Cout, c_m, c_n, alpha, beta);
     mark(2, 1, s);
     rc = launch_check("simt_reduce");
   }
@@ -1128,12 +1167,13 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
                                            p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
                         p->ks_b, p->kb_b, p->kbq_b, es);
   int rc;
+  bool packed = false;  // the packing kernel is the last launch on s
   if (x3)
-    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s);
+    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s, &packed);
   else if (p->dtype == TCCG_BF16)
-    rc = launch_pack<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16>(pa, s);
+    rc = launch_pack<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16>(pa, s, &packed);
   else
-    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s);
+    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s, &packed);
   if (rc) return rc;
   CUtensorMap tmA, tmB;
   const bool pair = p->tune.pair != 0;
@@ -1165,17 +1205,17 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
   mark(1, 0, s);
   if (pair && x3)
-    gett_tc2_kernel<TC_BF16X3><<<p->grid, Tc2Cfg<TC_BF16X3>::NUM_THREADS,
-                                 Tc2Cfg<TC_BF16X3>::SMEM_BYTES, s>>>(tmA, tmB, a);
+    launch_after(packed, gett_tc2_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16X3>::NUM_THREADS),
+                 Tc2Cfg<TC_BF16X3>::SMEM_BYTES, s, tmA, tmB, a);
   else if (pair)
-    gett_tc2_kernel<TC_BF16><<<p->grid, Tc2Cfg<TC_BF16>::NUM_THREADS, Tc2Cfg<TC_BF16>::SMEM_BYTES,
-                               s>>>(tmA, tmB, a);
+    launch_after(packed, gett_tc2_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16>::NUM_THREADS),
+                 Tc2Cfg<TC_BF16>::SMEM_BYTES, s, tmA, tmB, a);
   else if (x3)
-    gett_tc_kernel<TC_BF16X3><<<p->grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
-                                TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tmA, tmB, a);
+    launch_after(packed, gett_tc_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16X3>::NUM_THREADS),
+                 TcCfgT<TC_BF16X3>::SMEM_BYTES, s, tmA, tmB, a);
   else
-    gett_tc_kernel<TC_BF16><<<p->grid, TcCfgT<TC_BF16>::NUM_THREADS, TcCfgT<TC_BF16>::SMEM_BYTES,
-                              s>>>(tmA, tmB, a);
+    launch_after(packed, gett_tc_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16>::NUM_THREADS),
+                 TcCfgT<TC_BF16>::SMEM_BYTES, s, tmA, tmB, a);
   mark(1, 1, s);
   rc = launch_check("gett_tc");
   if (rc) return rc;
@@ -1183,19 +1223,20 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
     const unsigned tail = (unsigned)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles);
     mark(2, 0, s);
     if (x3)
-      tc_tail_reduce_kernel<TC_BF16X3>
-          <<<dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), 256, 0, s>>>(a);
+      launch_after(true, tc_tail_reduce_kernel<TC_BF16X3>,
+                   dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), dim3(256), 0, s, a);
     else
-      tc_tail_reduce_kernel<TC_BF16>
-          <<<dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), 256, 0, s>>>(a);
+      launch_after(true, tc_tail_reduce_kernel<TC_BF16>,
+                   dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), dim3(256), 0, s, a);
     mark(2, 1, s);
     return launch_check("tc_tail_reduce");
   }
   if (p->ksplit == 1) return rc;
   dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
   mark(2, 0, s);
-  simt_reduce_kernel<float><<<g2, 256, 0, s>>>(a.partial, p->ksplit, p->M, p->N, p->M, p->N, Cout,
-                                               c_m, c_n, alpha, beta);
+  launch_after(true, simt_reduce_kernel<float>, g2, dim3(256), 0, s, (const float*)a.partial,
+               (int)p->ksplit, (int64_t)p->M, (int64_t)p->N, (int64_t)p->M, (int64_t)p->N, Cout, c_m,
+               c_n, alpha, beta);
   mark(2, 1, s);
   return launch_check("tc_reduce");
 }
