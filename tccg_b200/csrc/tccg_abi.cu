@@ -917,18 +917,24 @@ static int launch_check(const char* what) {
 // library's own kernels on the stream (packing -> GETT, GETT -> reduction):
 // its CTAs may start, and set up barriers and TMEM, while that kernel drains;
 // they call grid_dep_wait() before reading its output, and read nothing
-// before it that an earlier kernel of the call could still be writing. Off
-// under per-kernel event timing (an event between the two kernels) and with
-// TCCG_B200_PDL=0 in the environment.
-static bool pdl_enabled() {
+// before it that an earlier kernel of the call could still be writing.
+// Automatic for short runs only (2MNK <= 2^36 FLOP, about 0.1 ms on the
+// tensor cores), where the 2 us it saves per kernel boundary shows: the
+// 8.8e12-FLOP persistent tcgen05 run (operands far larger than L2) measured
+// 20 % slower with it, and kernels right after such runs slower too (the cause
+// is not established). TCCG_B200_PDL=1 / =0 in the environment forces it on /
+// off; always off under per-kernel event timing (an event between the kernels).
+static bool pdl_enabled(const tccg_plan* p) {
   if (g_events) return false;
   const char* e = std::getenv("TCCG_B200_PDL");
-  return !(e && e[0] == '0');
+  if (e && e[0] == '0') return false;
+  if (e && e[0] == '1') return true;
+  return 2.0 * (double)p->M * (double)p->N * (double)p->K <= 68719476736.0;
 }
 
 template <typename... P, typename... A>
-static void launch_after(bool after_own_kernel, void (*kernel)(P...), dim3 grid, dim3 block,
-                         size_t smem, cudaStream_t s, A&&... args) {
+static void launch_after(bool after_own_kernel, const tccg_plan* p, void (*kernel)(P...),
+                         dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -938,7 +944,7 @@ static void launch_after(bool after_own_kernel, void (*kernel)(P...), dim3 grid,
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cfg.attrs = attr;
-  cfg.numAttrs = after_own_kernel && pdl_enabled() ? 1 : 0;
+  cfg.numAttrs = after_own_kernel && pdl_enabled(p) ? 1 : 0;
   (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);  // launch_check reads the error
 }
 
@@ -1067,17 +1073,17 @@ static void launch_simt_tiles(const tccg_plan* p, const SimtArgs<T>& a, dim3 gri
                               cudaStream_t s) {
   if constexpr (sizeof(T) == 4) {
     if (p->simt_shape == SIMT_NARROW_N) {
-      launch_after(after, simt_gett_kernel<T, LOAD, SIMT_NARROW_N>, grid, dim3(256),
+      launch_after(after, p, simt_gett_kernel<T, LOAD, SIMT_NARROW_N>, grid, dim3(256),
                    simt_smem_bytes<T, SIMT_NARROW_N>(), s, a);
       return;
     }
     if (p->simt_shape == SIMT_NARROW_M) {
-      launch_after(after, simt_gett_kernel<T, LOAD, SIMT_NARROW_M>, grid, dim3(256),
+      launch_after(after, p, simt_gett_kernel<T, LOAD, SIMT_NARROW_M>, grid, dim3(256),
                    simt_smem_bytes<T, SIMT_NARROW_M>(), s, a);
       return;
     }
   }
-  launch_after(after, simt_gett_kernel<T, LOAD>, grid, dim3(256), simt_smem_bytes<T>(), s, a);
+  launch_after(after, p, simt_gett_kernel<T, LOAD>, grid, dim3(256), simt_smem_bytes<T>(), s, a);
 }
 
 template <typename T>
@@ -1128,10 +1134,10 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   CUtensorMap tmC{};
   if (p->shortk && shortk_tma(p, c_ldc) &&
       encode_c2d<T>(&tmC, Cout, p->M, p->N, c_ldc, Cfg::BM, Cfg::BN))
-    launch_after(packed, simt_shortk_kernel<T, true>, grid, dim3(256),
+    launch_after(packed, p, simt_shortk_kernel<T, true>, grid, dim3(256),
                  SimtShortKCfg<T>::SMEM_BYTES, s, a, tmC);
   else if (p->shortk)
-    launch_after(packed, simt_shortk_kernel<T, false>, grid, dim3(256),
+    launch_after(packed, p, simt_shortk_kernel<T, false>, grid, dim3(256),
                  SimtShortKCfg<T>::SMEM_BYTES, s, a, tmC);
   else if (p->direct)
     launch_simt_tiles<T, SIMT_DIRECT>(p, a, grid, false, s);
@@ -1143,7 +1149,7 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   if (p->ksplit > 1) {
     dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
     mark(2, 0, s);
-    launch_after(true, simt_reduce_kernel<T>, g2, dim3(256), 0, s, a.partial, (int)p->ksplit,
+    launch_after(true, p, simt_reduce_kernel<T>, g2, dim3(256), 0, s, a.partial, (int)p->ksplit,
                  p->Mp, p->Np, p->M, p->N, Cout, c_m, c_n, alpha, beta);
     mark(2, 1, s);
     rc = launch_check("simt_reduce");
@@ -1205,16 +1211,16 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
   mark(1, 0, s);
   if (pair && x3)
-    launch_after(packed, gett_tc2_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16X3>::NUM_THREADS),
+    launch_after(packed, p, gett_tc2_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16X3>::NUM_THREADS),
                  Tc2Cfg<TC_BF16X3>::SMEM_BYTES, s, tmA, tmB, a);
   else if (pair)
-    launch_after(packed, gett_tc2_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16>::NUM_THREADS),
+    launch_after(packed, p, gett_tc2_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16>::NUM_THREADS),
                  Tc2Cfg<TC_BF16>::SMEM_BYTES, s, tmA, tmB, a);
   else if (x3)
-    launch_after(packed, gett_tc_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16X3>::NUM_THREADS),
+    launch_after(packed, p, gett_tc_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16X3>::NUM_THREADS),
                  TcCfgT<TC_BF16X3>::SMEM_BYTES, s, tmA, tmB, a);
   else
-    launch_after(packed, gett_tc_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16>::NUM_THREADS),
+    launch_after(packed, p, gett_tc_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16>::NUM_THREADS),
                  TcCfgT<TC_BF16>::SMEM_BYTES, s, tmA, tmB, a);
   mark(1, 1, s);
   rc = launch_check("gett_tc");
@@ -1223,10 +1229,10 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
     const unsigned tail = (unsigned)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles);
     mark(2, 0, s);
     if (x3)
-      launch_after(true, tc_tail_reduce_kernel<TC_BF16X3>,
+      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16X3>,
                    dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), dim3(256), 0, s, a);
     else
-      launch_after(true, tc_tail_reduce_kernel<TC_BF16>,
+      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16>,
                    dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), dim3(256), 0, s, a);
     mark(2, 1, s);
     return launch_check("tc_tail_reduce");
@@ -1234,7 +1240,7 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   if (p->ksplit == 1) return rc;
   dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
   mark(2, 0, s);
-  launch_after(true, simt_reduce_kernel<float>, g2, dim3(256), 0, s, (const float*)a.partial,
+  launch_after(true, p, simt_reduce_kernel<float>, g2, dim3(256), 0, s, (const float*)a.partial,
                (int)p->ksplit, (int64_t)p->M, (int64_t)p->N, (int64_t)p->M, (int64_t)p->N, Cout, c_m,
                c_n, alpha, beta);
   mark(2, 1, s);

@@ -1,8 +1,9 @@
 """Programmatic dependent launch: the GETT kernel of a plan run may start
 while the packing kernel before it drains (and a reduction while its GETT
 kernel drains); each waits for that kernel's writes before reading them.
-Results must be bitwise equal with it switched off (TCCG_B200_PDL=0) on every
-launch path that uses it -- CUDA-core tiles (square, narrow), the short-K
+It is automatic for short runs only (2MNK <= 2^36 FLOP); these tests force it
+on (TCCG_B200_PDL=1) and off (=0). Results must be bitwise equal either way on
+every launch path that uses it -- CUDA-core tiles (square, narrow), the short-K
 kernel with TMA and cp.async C blocks, tcgen05 (BF16x3, BF16, CTA pairs),
 k-split and tail-split reductions -- and for back-to-back runs captured in
 one CUDA graph, where each run's beta reads the C of the run before."""
