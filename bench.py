@@ -26,7 +26,6 @@ import json
 import os
 import statistics
 import sys
-import tempfile
 import threading
 import time
 

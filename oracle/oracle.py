@@ -28,7 +28,7 @@ import ctypes
 import os
 import subprocess
 import threading
-from typing import Dict, List, Sequence, Tuple
+from typing import Dict, Sequence, Tuple
 
 import numpy as np
 

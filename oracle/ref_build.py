@@ -29,7 +29,7 @@ import subprocess
 import sys
 import tempfile
 import warnings
-from typing import Dict, List, Tuple
+from typing import List
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(_HERE, "_ref")

@@ -15,7 +15,7 @@ flat one. The output C has the reversed shape of C's indices.
 """
 from __future__ import annotations
 
-from typing import Dict, Optional, Tuple
+from typing import Dict, Tuple
 
 from .plan import Plan
 from .spec import Contraction, make_contraction

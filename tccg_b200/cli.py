@@ -17,7 +17,6 @@ fp32|fp64|bf16|bf16x3`` and ``--outdir``.
 from __future__ import annotations
 
 import argparse
-import os
 import sys
 
 from .spec import TccgSyntaxError, TccgUnsupported, parse_file
@@ -74,8 +73,6 @@ def main(argv=None) -> int:
               file=sys.stderr)
         return 2
     try:
-        import copy
-        from .spec import fuse_indices, parse_text
         con = parse_file(args.filename)
         con.validate()
     except (TccgSyntaxError, TccgUnsupported) as e:

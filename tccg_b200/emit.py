@@ -14,10 +14,9 @@ from __future__ import annotations
 
 import os
 import subprocess
-from typing import Optional
 
 from . import build as B
-from .plan import DTYPES, Tuning, gett_view, native_desc, operand_dtype
+from .plan import Tuning, gett_view, native_desc, operand_dtype
 from .spec import Contraction, to_tccg_text
 from . import _native as N
 

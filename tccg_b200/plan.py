@@ -12,8 +12,8 @@ plain device buffers (torch is only the allocator and stream provider here).
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
-from typing import List, Optional, Sequence, Tuple
+from dataclasses import dataclass
+from typing import List, Optional, Tuple
 
 from . import _native as N
 from .spec import Contraction, Tensor

@@ -1,13 +1,11 @@
 """Grouped launch (configuration 5 pattern): many contractions of uneven
 extents in one persistent launch, captured in a CUDA graph, against one
 launch per contraction and the FP64 oracle."""
-import random
-
 import numpy as np
 import pytest
 
 from oracle import LoopNest, error_metrics
-from tccg_b200.workloads import batched_workload, random_contraction
+from tccg_b200.workloads import batched_workload
 
 
 def test_workload_generator_properties():

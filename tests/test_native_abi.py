@@ -4,8 +4,6 @@ import ctypes
 import os
 import re
 
-import pytest
-
 from tccg_b200 import _native as N
 
 HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
