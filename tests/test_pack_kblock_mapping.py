@@ -1,4 +1,4 @@
-"""Index mapping of the 16-byte k-block pack, on the CPU. A restatement of
+"""Index mapping of the k-block packs, on the CPU. A restatement of
 the plan-time tile choice (tccg_abi.cu: ``kblock_tiles``, ``kblock_quads``)
 and of ``pack_kblock_quad`` (pack.cuh) -- 256 threads copy 4 consecutive u
 of one (row, l) as one 16-byte chunk into a shared tile whose chunks are
@@ -7,8 +7,13 @@ into K-major rows -- replayed with numpy on the layouts the GPU tests use:
 every chunk lands inside the tile and is written once, every 16-byte copy
 reads 4 source elements that are k, k + lo, k + 2 lo, k + 3 lo of the
 operand, every slot the write-out reads was written, and the packed rows
-equal the operand gathered through its offset tables (zeros past K). The
-kernel itself is checked on a B200 by test_pack_kblock.py."""
+equal the operand gathered through its offset tables (zeros past K). Likewise the
+element-wise tiles (``pack_kblock`` and its division-free ``KbWalk``): every
+(row, l, u) copied once into its padded slot inside the kernel's shared
+tile, the run's column shortcut (including runs that wrap into the next
+value of the higher modes and u of stride -1) reading the right element, and
+each quad of the write-out inside one 32-element group. The kernels
+themselves are checked on a B200 by test_pack_kblock.py."""
 import numpy as np
 import pytest
 
@@ -185,3 +190,95 @@ def test_quads_refused_where_a_copy_would_straddle():
     assert not kblock_quads(kext, kstr, offsets(kext, kstr))
     # u on the first K mode is the streaming pass, not a k-block tile
     assert kblock_tiles([16, 8], [1, 16]) is None
+
+
+def kb_walk(f, step, lo, run):
+    """KbWalk: (r, l, u) of element f = r lo run + l run + u, then steps of
+    ``step`` elements without divisions."""
+    T = lo * run
+    r = f // T
+    l = (f - r * T) // run
+    u = f - r * T - l * run
+    dr = step // T
+    dl = (step - dr * T) // run
+    du = step - dr * T - dl * run
+    while True:
+        yield r, l, u
+        u += du
+        l += dl
+        if u >= run:
+            u -= run
+            l += 1
+        if l >= lo:
+            l -= lo
+            r += 1
+        r += dr
+
+
+def replay_elementwise(rext, rstr, kext, kstr, kcover_multiple):
+    """``pack_kblock``: one 4-byte copy per (r, l, u) into the padded slot of
+    k_local = l + lo u, then quads of k_local read back out."""
+    roff, coff = offsets(rext, rstr), offsets(kext, kstr)
+    R, K = len(roff), len(coff)
+    lo, run, rows, ext, step = kblock_tiles(kext, kstr)
+    T, TP = lo * run, lo * run + lo * run // 32
+    assert rows * TP <= 128 * 33  # the kernel's shared tile
+    kcover = -(-K // kcover_multiple) * kcover_multiple
+    # negative strides give negative offsets: index from the lowest element
+    base0 = -int(roff.min() + coff.min())
+    src = np.random.default_rng(1).standard_normal(int(roff.max() + coff.max()) + base0 + 1)
+    out = np.full((R, kcover), np.nan)
+    for kt in range(-(-kcover // T)):
+        for rt in range(-(-R // rows)):
+            k0, r0 = kt * T, rt * rows
+            u0 = (kt * run) % ext
+            tile = np.full(128 * 33, np.nan)
+            written = np.zeros(128 * 33, dtype=int)
+            for tid in range(THREADS):
+                w = kb_walk(tid, THREADS, lo, run)
+                for i in range(PACK_KB_ELEMS // THREADS):
+                    r, l, u = next(w)
+                    assert (r * lo + l) * run + u == tid + THREADS * i
+                    if r >= rows:
+                        continue
+                    row, k = r0 + r, k0 + l + lo * u
+                    kl = l + lo * u
+                    slot = r * TP + kl + kl // 32
+                    if k >= K or row >= R:
+                        tile[slot] = 0.0
+                    else:
+                        co = coff[k0 + l] + step * u if u0 + u < ext else coff[k]
+                        assert co == coff[k]  # the run's shortcut reads the right element
+                        tile[slot] = src[base0 + roff[row] + co]
+                    written[slot] += 1
+            assert written.max() <= 1
+            q = T // 4
+            for f in range(rows * q):
+                r, kq = f // q, (f % q) * 4
+                row, k = r0 + r, k0 + kq
+                if row >= R or k >= kcover:
+                    continue
+                base = r * TP + kq + kq // 32
+                assert (kq + 3) // 32 == kq // 32  # a quad stays inside one 32-group
+                assert written[base:base + 4].tolist() == [1, 1, 1, 1]
+                out[row, k:k + 4] = tile[base:base + 4]
+    ref = np.zeros((R, kcover))
+    ref[:, :K] = src[base0 + roff[:, None] + coff[None, :]]
+    return out, ref
+
+
+# (row extents, row strides, K extents in K order, K strides): u = the K
+# mode of stride +-1 after the first
+ELEMENTWISE = {
+    "u_extent_10": ([37], [10 * 16 * 3], [16, 10, 3], [10, 1, 160]),
+    "wrap": ([5], [3200], [16, 100, 2], [100, 1, 1600]),
+    "negative_step": ([9], [2000], [6, 24], [24, -1]),
+    "cfg4_small": ([8, 40], [32 * 40 * 32, 32], [32, 32], [32 * 40, 1]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(ELEMENTWISE))
+def test_kblock_elementwise_mapping(name):
+    rext, rstr, kext, kstr = ELEMENTWISE[name]
+    out, ref = replay_elementwise(rext, rstr, kext, kstr, 32)
+    assert np.array_equal(out, ref)
