@@ -161,7 +161,9 @@ int tccg_plan_run_timed(const tccg_plan* plan, const void* A, const void* B, voi
                         double alpha, double beta, void* ws, size_t ws_bytes, void* stream,
                         float* kernel_ms);
 
-/* Human-readable plan summary (method, kernels, tiles, workspace). */
+/* Human-readable plan summary (method, kernels, tiles, launch=dependent|plain
+ * for programmatic dependent launch as the environment now selects it,
+ * workspace). */
 int tccg_plan_describe(const tccg_plan* plan, char* buf, size_t len);
 
 /* FLOPs of one run by TCCG's count (tccg/tccg.py:1230-1234): 2MNK (+3MN if beta != 0). */

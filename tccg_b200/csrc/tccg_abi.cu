@@ -743,9 +743,23 @@ extern "C" int tccg_plan_workspace(const tccg_plan* p, size_t* bytes) {
   return TCCG_OK;
 }
 
+// Programmatic dependent launch (launch_after): on by default for runs of at
+// most 2^36 FLOP; TCCG_B200_PDL=1 / =0 in the environment forces it on / off.
+static bool pdl_by_size(const tccg_plan* p) {
+  return 2.0 * (double)p->M * (double)p->N * (double)p->K <= 68719476736.0;
+}
+static int pdl_forced() {  // 1 on, 0 off, -1 the size rule
+  const char* e = std::getenv("TCCG_B200_PDL");
+  if (e && e[0] == '0') return 0;
+  if (e && e[0] == '1') return 1;
+  return -1;
+}
+
 extern "C" int tccg_plan_describe(const tccg_plan* p, char* buf, size_t len) {
   if (!p || !buf || len == 0) return fail(TCCG_ERR_INVALID, "null argument");
-  snprintf(buf, len, "%s ws=%zu", p->describe, p->ws_bytes);
+  const int f = pdl_forced();
+  snprintf(buf, len, "%s launch=%s ws=%zu", p->describe,
+           (f < 0 ? pdl_by_size(p) : f == 1) ? "dependent" : "plain", p->ws_bytes);
   return TCCG_OK;
 }
 
@@ -926,10 +940,8 @@ static int launch_check(const char* what) {
 // off; always off under per-kernel event timing (an event between the kernels).
 static bool pdl_enabled(const tccg_plan* p) {
   if (g_events) return false;
-  const char* e = std::getenv("TCCG_B200_PDL");
-  if (e && e[0] == '0') return false;
-  if (e && e[0] == '1') return true;
-  return 2.0 * (double)p->M * (double)p->N * (double)p->K <= 68719476736.0;
+  const int f = pdl_forced();
+  return f < 0 ? pdl_by_size(p) : f == 1;
 }
 
 template <typename... P, typename... A>

@@ -110,3 +110,16 @@ def test_dependent_launch_in_cuda_graph(cuda, monkeypatch, name):
     assert p.status() == 0
     assert np.array_equal(eager, dC.cpu().numpy())
     del g
+
+
+def test_describe_reports_the_launch(cuda, monkeypatch):
+    small = Plan(make_contraction("mn", "mk", "kn", dict(m=1024, n=1024, k=1024)), "bf16x3")
+    # configuration 3's size (8.8e12 FLOP): ordinary launches by default
+    big = Plan(make_contraction("abcijk", "ambnc", "minjk",
+                                dict(a=32, b=32, c=32, i=32, j=32, k=32, m=64, n=64)), "bf16x3")
+    monkeypatch.delenv("TCCG_B200_PDL", raising=False)
+    assert "launch=dependent" in small.describe() and "launch=plain" in big.describe()
+    monkeypatch.setenv("TCCG_B200_PDL", "1")
+    assert "launch=dependent" in big.describe()
+    monkeypatch.setenv("TCCG_B200_PDL", "0")
+    assert "launch=plain" in small.describe()
