@@ -170,6 +170,60 @@ def read_traffic(name: str):
     return None
 
 
+def host_threads() -> int:
+    """Host CPUs this process may run on (its affinity mask)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def set_omp_threads(n: int) -> dict:
+    """Sets the thread count of the process's OpenMP runtime (libgomp.so.1:
+    torch loads its own copy under that name first, and the oracle's and the
+    reference-emitted loop nests bind to whichever is loaded) for the calling
+    thread, and reports what the runtime then uses. torch's first parallel CPU
+    operation sets it to its own intra-op default, so it is set explicitly
+    right before every timed CPU call."""
+    import ctypes
+    info = {"requested": int(n)}
+    try:
+        g = ctypes.CDLL("libgomp.so.1")
+        g.omp_set_num_threads(int(n))
+        g.omp_get_max_threads.restype = ctypes.c_int
+        info["omp_get_max_threads"] = int(g.omp_get_max_threads())
+    except OSError as e:
+        info["error"] = str(e)
+    for k in ("OMP_NUM_THREADS", "GOMP_CPU_AFFINITY", "OMP_PROC_BIND", "OMP_PLACES"):
+        if os.environ.get(k):
+            info[k] = os.environ[k]
+    info["affinity_cpus"] = host_threads()
+    return info
+
+
+def oracle_errors(con, A_np, B_np, lins, samples):
+    """The checker: errors of sampled output entries (``samples``: name ->
+    values at the column-major indices ``lins``) against the FP64 oracle, the
+    C restatement of TCCG's loop-nest reference evaluated in FP64 on the same
+    FP32 inputs. Four metrics per output: max abs, normwise, max relative
+    error over |ref| > 1e-3 max|ref|, and TCCG's equal() criterion
+    min(abs, rel) (tccg.py:843-881) with its sign blindness fixed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import LoopNest, error_metrics  # noqa: E402
+    sizes = {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices}
+    ln = LoopNest(con.C0.labels, con.A0.labels, con.B0.labels, sizes)
+    ref = ln.sample64(A_np, B_np, None, con.alpha, 0.0, lins, host_threads())
+    out = {"oracle": "FP64 loop nest (oracle/loopnest.c) on %d entries of C spread evenly over "
+                     "its %d" % (len(lins), ln.size_c)}
+    for name, v in samples.items():
+        m = error_metrics(v, ref)
+        out[name] = {"max_abs": m["max_abs"], "normwise": m["normwise"],
+                     "max_rel_over_1e-3_max_ref": m["max_rel"],
+                     "tccg_min_abs_rel": m["tccg_equal_worst"],
+                     "max_abs_over_max_ref": m["max_abs_over_max_ref"]}
+    return out
+
+
 def cpu_loopnest_sample(con, A_np, B_np, seconds=10.0, threads=0, gpu_C=None):
     """Time the oracle loop nest (TCCG's referenceVersion restated) on the first
     S column-major entries of C, S sized for about `seconds`; optionally check
@@ -177,7 +231,8 @@ def cpu_loopnest_sample(con, A_np, B_np, seconds=10.0, threads=0, gpu_C=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     from oracle import LoopNest, error_metrics, lib  # noqa: E402
-    threads = threads or os.cpu_count() or 1
+    threads = threads or host_threads()
+    omp = set_omp_threads(threads)
     c, a, b = con.C0.labels, con.A0.labels, con.B0.labels
     sizes = {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices}
     ln = LoopNest(c, a, b, sizes)
@@ -198,7 +253,7 @@ def cpu_loopnest_sample(con, A_np, B_np, seconds=10.0, threads=0, gpu_C=None):
     out = {"value": flops / t / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
            "sample": "first %d column-major entries of C (%.2e of the %d) through the oracle's C "
                      "restatement of TCCG's loop-nest reference, %d OpenMP threads, %.1f s"
-                     % (S, S / ln.size_c, ln.size_c, threads, t)}
+                     % (S, S / ln.size_c, ln.size_c, threads, t), "openmp": omp}
     if gpu_C is not None:
         lins = np.arange(0, S, max(1, S // 4096), dtype=np.int64)
         ref = ln.sample64(A_np, B_np, None, 1.0, 0.0, lins, threads)
@@ -223,14 +278,16 @@ def reference_impl_sample(con, A_np, B_np, seconds, threads):
                                    ctypes.c_float, ctypes.c_float]
     # slab: all of a,b,c,i for j=k=0 -> 2^20 entries of K=4096 each
     Cs = np.zeros(32 ** 4, dtype=np.float32)
+    omp = set_omp_threads(threads)
     t0 = time.perf_counter()
     L.referenceVersion(A_np.ctypes.data, B_np.ctypes.data, Cs.ctypes.data, 1.0, 0.0)
     t = time.perf_counter() - t0
     flops = 2.0 * Cs.size * 4096
-    return {"value": flops / t / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+    return {"value": flops / t / 1e12, "unit": "TFLOP/s", "cores": omp.get("omp_get_max_threads", threads),
+            "kind": "reference",
             "sample": "slab C[:,:,:,:,0,0] (2^20 entries, 1/1024 of C) computed by the loop nest "
                       "TCCG's generator emits for this contraction, g++ -O3 -fopenmp, %d threads, "
-                      "%.2f s" % (threads, t)}
+                      "%.2f s" % (omp.get("omp_get_max_threads", threads), t), "openmp": omp}
 
 
 # --------------------------------------------------------------------------
@@ -244,11 +301,10 @@ def run_reference(args, world, rank):
     import torch
     from tccg_b200 import parse_text
     con = parse_text(workload(args.k_extent))
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     g = torch.Generator().manual_seed(0)
     A = torch.randn(con.A0.num_elements(), generator=g).numpy()
     B = torch.randn(con.B0.num_elements(), generator=g).numpy()
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     vals = []
     info = None
     per_step = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
@@ -269,7 +325,8 @@ def run_reference(args, world, rank):
         "config": {"workload": workload_name(args.k_extent), "precision": "fp32 (CPU loop nest)",
                    "parallelism": "host cores of rank 0"},
         "cpu_baseline": {"kind": info["kind"], "cores": info["cores"], "sample": info["sample"],
-                         "value": v, "unit": "TFLOP/s"},
+                         "value": v, "unit": "TFLOP/s", "openmp": info.get("openmp"),
+                         "steps_tflops": vals},
         "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -299,6 +356,12 @@ def run_ours(args, world, rank, local):
     # ---- headline: split-BF16x3, device-resident -------------------------
     for _ in range(args.warmup):
         x3.plan.run(A, B, C, workspace=ws)
+    # CUDA events around each kernel of every timed step (created and
+    # recorded once here, outside the timed region)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(args.steps)]
+    for evs in ev:
+        for e in evs:
+            e.record()
     torch.cuda.synchronize()
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
@@ -307,8 +370,8 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
-        x3.plan.run(A, B, C, workspace=ws)
+    for i in range(args.steps):
+        x3.plan.run_events(A, B, C, ev[i], workspace=ws)
     e1.record()
     torch.cuda.synchronize()
     barrier(world)
@@ -317,15 +380,19 @@ def run_ours(args, world, rank, local):
     ms_step = max_over_ranks(ms_total / args.steps, world)
     value = world * flops / (ms_step * 1e-3) / 1e12
     status = x3.plan.status()
-
-    # per-kernel breakdown (same stream, CUDA events around each kernel)
-    kt = [x3.plan.run_timed(A, B, C, workspace=ws) for _ in range(max(2, min(args.steps, 5)))]
-    pack_ms = statistics.mean(k[0] for k in kt)
-    gemm_ms = statistics.mean(k[1] for k in kt)
+    # per-kernel times of the same timed steps (pack, then the GETT kernel)
+    pack_steps = [evs[0].elapsed_time(evs[1]) for evs in ev]
+    gemm_steps = [evs[2].elapsed_time(evs[3]) for evs in ev]
+    pack_ms = statistics.mean(pack_steps)
+    gemm_ms = statistics.mean(gemm_steps)
     achieved = flops / (gemm_ms * 1e-3) / 1e12
     bf16_peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
     peak = bf16_peak / 3.0
+    burst = peaks.get("bf16_tflops", bf16_peak) / 3.0
     traffic = read_traffic("gett_tc_bf16x3_cfg3.txt")
+    # sampled output entries for the error check against the oracle
+    lins = torch.from_numpy(np.unique(np.linspace(0, nC - 1, 4096).astype(np.int64))).to(dev)
+    samples = {"bf16x3": C[lins].double().cpu().numpy()}
 
     # ---- plain FP32 GETT on the same inputs --------------------------------
     res = {}
@@ -345,34 +412,39 @@ def run_ours(args, world, rank, local):
         res["fp32"] = {"value": world * flops / (ms32 * 1e-3) / 1e12, "unit": "TFLOP/s",
                        "ms_per_step": ms32,
                        "kernel_frac_of_fp32_simt_peak": flops / (k32[1] * 1e-3) / 1e12 / FP32_SIMT_PEAK_TFLOPS}
+        samples["fp32"] = C32[lins].double().cpu().numpy()
         f32._ws = None
     else:
         C32 = None
 
-    # ---- errors against the FP64 path --------------------------------------
+    # ---- errors: the FP64 oracle on sampled entries, and the FP64 path -----
     if not args.skip_errors:
         f64 = Compiled(con, "fp64")
         C64 = torch.empty(nC, device=dev, dtype=torch.float64)
         f64.plan.run(A.double(), B.double(), C64, workspace=f64.workspace(dev))
         torch.cuda.synchronize()
+        samples["fp64_path"] = C64[lins].cpu().numpy()
         nrm = torch.linalg.vector_norm(C64).item()
-        err = {"reference": "this library's FP64 path (DFMA), itself checked against the FP64 oracle in tests/",
-               "bf16x3_normwise": (torch.linalg.vector_norm(C.double() - C64).item() / nrm)}
-        err["bf16x3_max_abs_over_max_ref"] = ((C.double() - C64).abs().max().item()
-                                              / C64.abs().max().item())
+        err = {"bf16x3_normwise_vs_fp64_path_all_entries":
+               torch.linalg.vector_norm(C.double() - C64).item() / nrm}
         if C32 is not None:
-            err["fp32_normwise"] = torch.linalg.vector_norm(C32.double() - C64).item() / nrm
+            err["fp32_normwise_vs_fp64_path_all_entries"] = (
+                torch.linalg.vector_norm(C32.double() - C64).item() / nrm)
         res["errors"] = err
         del C64, f64
     del C32
     torch.cuda.empty_cache()
 
     # ---- end to end through the public API with host buffers -------------
+    if not args.skip_errors:
+        res["errors"].update(oracle_errors(con, A.cpu().numpy(), B.cpu().numpy(),
+                                           lins.cpu().numpy(), samples))
     if args.skip_e2e:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "TFLOP/s",
                               "ms_per_step": ms_step, "roofline_kernel_ms": gemm_ms,
-                              "pack_ms": pack_ms, "partial": "--skip-e2e"}), flush=True)
+                              "pack_ms": pack_ms, "partial": "--skip-e2e",
+                              "errors": res.get("errors")}), flush=True)
         return 0
     Ah = A.cpu().pin_memory()
     Bh = B.cpu().pin_memory()
@@ -401,7 +473,7 @@ def run_ours(args, world, rank, local):
         ref = None
         if args.k_extent == 32:
             ref = reference_impl_sample(con, Ah.numpy(), Bh.numpy(), args.cpu_seconds,
-                                        os.cpu_count() or 1)
+                                        host_threads())
         if ref is not None:
             ref["check_vs_fp64_oracle"] = cpu.pop("check_vs_fp64_oracle", None)
             ref["port"] = {"value": cpu["value"], "sample": cpu["sample"]}
@@ -423,11 +495,14 @@ def run_ours(args, world, rank, local):
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "gett_tc_kernel<BF16X3>",
                          "kernel_ms": gemm_ms, "pack_ms": pack_ms,
+                         "kernel_ms_min_max": [min(gemm_steps), max(gemm_steps)],
+                         "timing": "CUDA events around the pack and GETT kernels of every timed step "
+                                   "(the same steps as ms_per_step)",
+                         "frac_of_burst": achieved / burst,
                          "peak_note": "%s sustained dense BF16 %.1f TFLOP/s / 3 (three BF16 MMAs per "
                                       "algorithmic multiply-add); frac = tensor-pipe share of measured "
-                                      "peak; of burst (%.1f/3): %.3f"
-                                      % (peak_src, bf16_peak, peaks.get("bf16_tflops", bf16_peak),
-                                         achieved / (peaks.get("bf16_tflops", bf16_peak) / 3.0))},
+                                      "peak; frac_of_burst against %.1f/3"
+                                      % (peak_src, bf16_peak, peaks.get("bf16_tflops", bf16_peak))},
             "e2e": {"value": world * flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e,

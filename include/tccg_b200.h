@@ -161,6 +161,19 @@ int tccg_plan_run_timed(const tccg_plan* plan, const void* A, const void* B, voi
                         double alpha, double beta, void* ws, size_t ws_bytes, void* stream,
                         float* kernel_ms);
 
+/*
+ * tccg_plan_run that records caller-created CUDA events around each kernel it
+ * launches, without synchronising: events[2*i] / events[2*i+1] bracket kernel
+ * slot i (0 = operand packing, 1 = the GEMM kernel, 2 = k-split reduction or
+ * TTGT output transposition; all six are recorded first, so a slot without a
+ * kernel measures 0 ms). For timing every kernel of a run inside a loop of
+ * runs; the kernels are launched as by tccg_plan_run_timed (never with
+ * programmatic dependent launch).
+ */
+int tccg_plan_run_events(const tccg_plan* plan, const void* A, const void* B, void* C,
+                         double alpha, double beta, void* ws, size_t ws_bytes, void* stream,
+                         void* const* events);
+
 /* Human-readable plan summary (method, kernels, tiles, launch=dependent|plain
  * for programmatic dependent launch as the environment now selects it,
  * workspace). */
@@ -192,14 +205,41 @@ int tccg_plan_status(const tccg_plan* plan, int32_t* device_status);
  * process exits; a contraction needing more is rejected with
  * TCCG_ERR_WORKSPACE and a message (use tccg_plan_run then). The first call
  * on each device looks up the array's device address with that device
- * current; make that first call before any stream capture. All calls share
- * the array (each clears what must start at zero), so calls whose kernels
- * overlap on the GPU -- e.g. on two streams -- race; serialise them.
+ * current (and clears the status word); make that first call before any
+ * stream capture. All calls share the array (each call rebuilds the tables
+ * and packed operands it reads), so calls whose kernels overlap on the GPU --
+ * e.g. on two streams -- race; serialise them.
  * A, B, C: device pointers, float, in the caller's (file) order as for
  * tccg_plan_run; desc as for tccg_plan_create.
  */
 int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, const float* B, float* C,
                              double alpha, double beta, void* stream);
+
+/*
+ * Device-side status of the allocation-free entry point on the current
+ * device: 0, or the first TCCG_DEVSTAT_* code one of its kernels recorded
+ * since the last query (a bounded wait that ran out means C is incomplete).
+ * The word lives in the same static scratch array; calls do not clear it, so
+ * a code stays until this query. Synchronises the device, reads and clears
+ * the word. No counterpart in the reference (its calls return void).
+ */
+int tccg_gett_bf16x3_noalloc_status(int32_t* device_status);
+
+/*
+ * Testing of the bounded device waits (no counterpart in the reference).
+ * Arms a one-shot trigger on the calling host thread: the next tcgen05 GETT
+ * launch this thread makes (tccg_plan_run of a tensor-core plan without the
+ * CTA-pair kernel, or tccg_gett_bf16x3_noalloc) bounds every device wait by
+ * wait_ms instead of 4 s, and its producer does not load the first k-block of
+ * tile `tile` of the tile order. The MMA warp's wait for that block runs out,
+ * the CTA that owns the tile records TCCG_DEVSTAT_TIMEOUT_* and winds down
+ * (in-flight copies and MMAs are waited for, tensor memory is released), and
+ * the launch leaves that CTA's tiles of C unwritten. Nothing faults and no
+ * wait is unbounded; tccg_plan_status / tccg_gett_bf16x3_noalloc_status then
+ * report the code. tile >= 0 (a tile past the last one skips nothing),
+ * wait_ms in [1, 4000].
+ */
+int tccg_debug_inject_timeout(int32_t tile, int32_t wait_ms);
 
 /*
  * HPTT-style out-of-place transposition (the call TCCG emits at

@@ -30,9 +30,10 @@ METHODS = {"gett": METHOD_GETT, "ttgt": METHOD_TTGT, "log": METHOD_LOG}
 
 EXPORTED = [
     "tccg_version", "tccg_last_error", "tccg_plan_create", "tccg_plan_workspace",
-    "tccg_plan_run", "tccg_plan_run_timed", "tccg_plan_describe", "tccg_plan_flops", "tccg_plan_destroy",
+    "tccg_plan_run", "tccg_plan_run_timed", "tccg_plan_run_events", "tccg_plan_describe", "tccg_plan_flops", "tccg_plan_destroy",
     "tccg_plan_status", "tccg_transpose", "tccg_group_create", "tccg_group_workspace",
     "tccg_group_bind", "tccg_group_run", "tccg_group_destroy", "tccg_gett_bf16x3_noalloc",
+    "tccg_gett_bf16x3_noalloc_status", "tccg_debug_inject_timeout",
 ]
 
 
@@ -80,6 +81,8 @@ def _declare(L):
     L.tccg_plan_run.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, sz, vp]
     L.tccg_plan_run_timed.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, sz,
                                       vp, ctypes.POINTER(ctypes.c_float)]
+    L.tccg_plan_run_events.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, sz,
+                                       vp, ctypes.POINTER(vp)]
     L.tccg_plan_describe.argtypes = [vp, ctypes.c_char_p, sz]
     L.tccg_plan_flops.argtypes = [vp, ctypes.c_double]
     L.tccg_plan_flops.restype = ctypes.c_double
@@ -96,6 +99,8 @@ def _declare(L):
     L.tccg_group_destroy.argtypes = [vp]
     L.tccg_gett_bf16x3_noalloc.argtypes = [ctypes.POINTER(Desc), vp, vp, vp, ctypes.c_double,
                                            ctypes.c_double, vp]
+    L.tccg_gett_bf16x3_noalloc_status.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+    L.tccg_debug_inject_timeout.argtypes = [i32, i32]
     for name in EXPORTED:
         if name not in ("tccg_version", "tccg_last_error", "tccg_plan_flops"):
             getattr(L, name).restype = ctypes.c_int

@@ -68,14 +68,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity to complete. Returns false
-// when TCCG_DEVICE_WAIT_NS elapsed first (the caller records an error).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// when limit_ns elapsed first (the caller records an error).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint64_t limit_ns = TCCG_DEVICE_WAIT_NS) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   uint32_t spins = 0;
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > TCCG_DEVICE_WAIT_NS) return false;
+    if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 

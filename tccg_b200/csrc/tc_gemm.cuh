@@ -31,9 +31,10 @@
 // With a k-split (contractions whose C tiles cannot fill the GPU), tile
 // indices run over (split, tile) and each split's epilogue writes raw sums to
 // a workspace slice; simt_reduce_kernel adds the slices in split order.
-// Every mbarrier wait is bounded (TCCG_DEVICE_WAIT_NS); a wait that runs out
-// records an error code in *status and the CTA winds down: in-flight TMA loads
-// and MMAs are waited for (bounded) and TMEM is released before returning.
+// Every mbarrier wait is bounded (TcArgs::wait_ns, by default
+// TCCG_DEVICE_WAIT_NS = 4 s); a wait that runs out records an error code in
+// *status and the CTA winds down: in-flight TMA loads and MMAs are waited for
+// (bounded) and TMEM is released before returning.
 #pragma once
 #include <cuda.h>
 #include "common.cuh"
@@ -86,6 +87,12 @@ struct TcArgs {
   // last round of the persistent grid instead of leaving it mostly idle.
   int32_t full_tiles, tail_split, tail_kb;
   float* tail_partial;
+  // Bound of every mbarrier wait of the launch (0 = TCCG_DEVICE_WAIT_NS).
+  uint64_t wait_ns;
+  // Testing of the abort path (0 = off): the producer does not load the
+  // first k-block of tile skip_tile1 - 1, so the MMA warp's wait for it runs
+  // out and the CTA winds down with a status code.
+  int32_t skip_tile1;
 };
 
 // Grouped launch: one entry per contraction, in device memory. The tensor maps
@@ -188,6 +195,8 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
               : (a1->tail_split > 1
                      ? a1->full_tiles + (a1->tiles_m * a1->tiles_n - a1->full_tiles) * a1->tail_split
                      : a1->tiles_m * a1->tiles_n * a1->ksplit);
+  const uint64_t wait_ns = (GROUPED || a1->wait_ns == 0) ? TCCG_DEVICE_WAIT_NS : a1->wait_ns;
+  const int skip_tile1 = GROUPED ? 0 : a1->skip_tile1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -224,15 +233,17 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
       for (int kb = t.kb_begin; kb < t.kb_end; ++kb) {
-        if (!mbar_wait(&empty[stage], phase ^ 1)) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, wait_ns)) {
           record_error(status, 1);
           ok = false;
           break;
         }
-        mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
-        tma_load_2d(sA + stage * Cfg::A_STAGE, t.tA, kb * 64, t.tm * Cfg::BM, &full[stage]);
-        tma_load_2d(sB + stage * Cfg::B_STAGE, t.tB, kb * 64, t.tn * Cfg::BN, &full[stage]);
-        issued_phase[stage] = (int)phase;
+        if (tile + 1 != skip_tile1 || kb != t.kb_begin) {
+          mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
+          tma_load_2d(sA + stage * Cfg::A_STAGE, t.tA, kb * 64, t.tm * Cfg::BM, &full[stage]);
+          tma_load_2d(sB + stage * Cfg::B_STAGE, t.tB, kb * 64, t.tn * Cfg::BN, &full[stage]);
+          issued_phase[stage] = (int)phase;
+        }
         if (++stage == Cfg::STAGES) {
           stage = 0;
           phase ^= 1;
@@ -241,7 +252,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     }
     if (!ok) {  // let in-flight copies land before the CTA's smem goes away
       for (int s = 0; s < Cfg::STAGES; ++s)
-        if (issued_phase[s] >= 0) (void)mbar_wait(&full[s], (uint32_t)issued_phase[s]);
+        if (issued_phase[s] >= 0) (void)mbar_wait(&full[s], (uint32_t)issued_phase[s], wait_ns);
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
@@ -260,7 +271,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       const uint32_t idesc =
           idesc_bf16_f32(Cfg::BM, ncols >= Cfg::BN ? Cfg::BN : (int)((ncols + 31) / 32) * 32);
       for (int kb0 = t.kb_begin; kb0 < nkb && ok; kb0 += ckb) {
-        if (!mbar_wait(&acce[acc], acc_phase ^ 1)) {
+        if (!mbar_wait(&acce[acc], acc_phase ^ 1, wait_ns)) {
           record_error(status, 2);
           ok = false;
           break;
@@ -270,7 +281,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
         uint32_t accumulate = 0;
         const int kend = (kb0 + ckb < nkb) ? kb0 + ckb : nkb;
         for (int kb = kb0; kb < kend; ++kb) {
-          if (!mbar_wait(&full[stage], phase)) {
+          if (!mbar_wait(&full[stage], phase, wait_ns)) {
             record_error(status, 2);
             ok = false;
             break;
@@ -316,7 +327,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     }
     if (!ok && issued_any) {  // wait for outstanding MMAs before TMEM is released
       tc_commit(drain);
-      (void)mbar_wait(drain, 0);
+      (void)mbar_wait(drain, 0, wait_ns);
     }
   } else if (warp >= 2) {
     // ---------------- epilogue ----------------
@@ -352,7 +363,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       }
       if constexpr (MODE == TC_BF16) {
         // one accumulator per tile: stream TMEM -> C
-        if (!mbar_wait(&accf[acc], acc_phase)) {
+        if (!mbar_wait(&accf[acc], acc_phase, wait_ns)) {
           record_error(status, 3);
           break;
         }
@@ -408,7 +419,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
         const int nchunks = (t.kb_end - t.kb_begin + a.chunk_kb - 1) / a.chunk_kb;
         float sum[HC];
         for (int ch = 0; ch < nchunks; ++ch) {
-          if (!mbar_wait(&accf[acc], acc_phase)) {
+          if (!mbar_wait(&accf[acc], acc_phase, wait_ns)) {
             record_error(status, 3);
             ok = false;
             break;

@@ -442,6 +442,21 @@ static bool build_visit(int n, const int64_t* ext, const int64_t* str, std::vect
   return true;
 }
 
+// Product of the n extents of one index class (M, N or K). Each extent must
+// be >= 1 and the running product may never exceed 2^31 (checked before each
+// multiplication, so that huge extents cannot wrap to a small product).
+static int mode_product(const char* cls, int n, const int64_t* ext, int64_t* out) {
+  int64_t p = 1;
+  for (int i = 0; i < n; ++i) {
+    if (ext[i] < 1) return fail(TCCG_ERR_INVALID, "%s extent %d is %lld", cls, i, (long long)ext[i]);
+    if (ext[i] > ((int64_t)1 << 31) / p)
+      return fail(TCCG_ERR_UNSUPPORTED, "%s (the product of its extents) must be <= 2^31", cls);
+    p *= ext[i];
+  }
+  *out = p;
+  return TCCG_OK;
+}
+
 extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t precision,
                                 const tccg_tuning* tuning, tccg_plan** out) {
   if (!desc || !out) return fail(TCCG_ERR_INVALID, "null descriptor or output pointer");
@@ -460,20 +475,10 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   if (dtype == TCCG_BF16 && precision != TCCG_PREC_BF16)
     return fail(TCCG_ERR_UNSUPPORTED, "BF16 operands are supported with TCCG_PREC_BF16 only");
   int64_t M = 1, N = 1, K = 1;
-  for (int i = 0; i < d.nm; ++i) {
-    if (d.m_ext[i] < 1) return fail(TCCG_ERR_INVALID, "M extent %d is %lld", i, (long long)d.m_ext[i]);
-    M *= d.m_ext[i];
-  }
-  for (int i = 0; i < d.nn; ++i) {
-    if (d.n_ext[i] < 1) return fail(TCCG_ERR_INVALID, "N extent %d is %lld", i, (long long)d.n_ext[i]);
-    N *= d.n_ext[i];
-  }
-  for (int i = 0; i < d.nk; ++i) {
-    if (d.k_ext[i] < 1) return fail(TCCG_ERR_INVALID, "K extent %d is %lld", i, (long long)d.k_ext[i]);
-    K *= d.k_ext[i];
-  }
-  if (M > (int64_t)1 << 31 || N > (int64_t)1 << 31 || K > (int64_t)1 << 31)
-    return fail(TCCG_ERR_UNSUPPORTED, "M, N and K must each be <= 2^31");
+  int rc0 = mode_product("M", d.nm, d.m_ext, &M);
+  if (!rc0) rc0 = mode_product("N", d.nn, d.n_ext, &N);
+  if (!rc0) rc0 = mode_product("K", d.nk, d.k_ext, &K);
+  if (rc0) return rc0;
 
   tccg_plan* p = new tccg_plan();
   p->d = d;
@@ -754,12 +759,18 @@ static int pdl_forced() {  // 1 on, 0 off, -1 the size rule
   if (e && e[0] == '1') return 1;
   return -1;
 }
+// Whether tccg_plan_run launches this plan's kernels with programmatic
+// dependent launch; tccg_plan_run_timed never does (an event sits between
+// the kernels), see pdl_enabled.
+static bool pdl_selected(const tccg_plan* p) {
+  const int f = pdl_forced();
+  return f < 0 ? pdl_by_size(p) : f == 1;
+}
 
 extern "C" int tccg_plan_describe(const tccg_plan* p, char* buf, size_t len) {
   if (!p || !buf || len == 0) return fail(TCCG_ERR_INVALID, "null argument");
-  const int f = pdl_forced();
   snprintf(buf, len, "%s launch=%s ws=%zu", p->describe,
-           (f < 0 ? pdl_by_size(p) : f == 1) ? "dependent" : "plain", p->ws_bytes);
+           pdl_selected(p) ? "dependent(plain when timed per kernel)" : "plain", p->ws_bytes);
   return TCCG_OK;
 }
 
@@ -784,12 +795,15 @@ extern "C" int tccg_plan_status(const tccg_plan* p, int32_t* device_status) {
 }
 
 // --------------------------------------------------------------------------
-// kernel attributes (once per process)
+// kernel attributes (once per device)
 // --------------------------------------------------------------------------
-static std::once_flag g_attr_once;
-static cudaError_t g_attr_err = cudaSuccess;
+// cudaFuncSetAttribute acts on the current device's context, so the large
+// shared-memory sizes are set once for each device the process uses.
+#define TCCG_MAX_DEVICES 64
+static std::once_flag g_attr_once[TCCG_MAX_DEVICES];
+static cudaError_t g_attr_err[TCCG_MAX_DEVICES];
 
-static void set_attrs() {
+static cudaError_t set_attrs() {
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) { if (e == cudaSuccess && x != cudaSuccess) e = x; };
   chk(cudaFuncSetAttribute(simt_gett_kernel<float, SIMT_PACKED>,
@@ -825,13 +839,18 @@ static void set_attrs() {
   chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
-  g_attr_err = e;
+  return e;
 }
 
 static int ensure_attrs() {
-  std::call_once(g_attr_once, set_attrs);
-  if (g_attr_err != cudaSuccess)
-    return fail(TCCG_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(g_attr_err));
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= TCCG_MAX_DEVICES)
+    return fail(TCCG_ERR_UNSUPPORTED, "device index %d (at most %d devices)", dev, TCCG_MAX_DEVICES);
+  std::call_once(g_attr_once[dev], [dev] { g_attr_err[dev] = set_attrs(); });
+  if (g_attr_err[dev] != cudaSuccess)
+    return fail(TCCG_ERR_CUDA, "cudaFuncSetAttribute on device %d: %s", dev,
+                cudaGetErrorString(g_attr_err[dev]));
   return TCCG_OK;
 }
 
@@ -921,6 +940,26 @@ static void mark(int slot, int end, cudaStream_t s) {
   if (g_events) cudaEventRecord(g_events[2 * slot + end], s);
 }
 
+// Test trigger of the bounded device waits (tccg_debug_inject_timeout):
+// armed per host thread, taken by the next launch of gett_tc_kernel.
+static thread_local int32_t g_inject_tile1 = 0;
+static thread_local uint64_t g_inject_wait_ns = 0;
+
+static void take_injection(TcArgs& a) {
+  a.skip_tile1 = g_inject_tile1;
+  a.wait_ns = g_inject_wait_ns;
+  g_inject_tile1 = 0;
+  g_inject_wait_ns = 0;
+}
+
+extern "C" int tccg_debug_inject_timeout(int32_t tile, int32_t wait_ms) {
+  if (tile < 0 || wait_ms < 1 || wait_ms > 4000)
+    return fail(TCCG_ERR_INVALID, "tile must be >= 0 and wait_ms in [1, 4000]");
+  g_inject_tile1 = tile + 1;
+  g_inject_wait_ns = (uint64_t)wait_ms * 1000000ull;
+  return TCCG_OK;
+}
+
 static int launch_check(const char* what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TCCG_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
@@ -938,11 +977,7 @@ static int launch_check(const char* what) {
 // 20 % slower with it, and kernels right after such runs slower too (the cause
 // is not established). TCCG_B200_PDL=1 / =0 in the environment forces it on /
 // off; always off under per-kernel event timing (an event between the kernels).
-static bool pdl_enabled(const tccg_plan* p) {
-  if (g_events) return false;
-  const int f = pdl_forced();
-  return f < 0 ? pdl_by_size(p) : f == 1;
-}
+static bool pdl_enabled(const tccg_plan* p) { return !g_events && pdl_selected(p); }
 
 template <typename... P, typename... A>
 static void launch_after(bool after_own_kernel, const tccg_plan* p, void (*kernel)(P...),
@@ -1221,6 +1256,7 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   a.tail_split = p->tail_split;
   a.tail_kb = p->tail_kb;
   a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
+  if (!pair) take_injection(a);
   mark(1, 0, s);
   if (pair && x3)
     launch_after(packed, p, gett_tc2_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16X3>::NUM_THREADS),
@@ -1343,6 +1379,24 @@ extern "C" int tccg_plan_run_timed(const tccg_plan* p, const void* A, const void
   if (rc) return rc;
   if (e != cudaSuccess) return fail(TCCG_ERR_CUDA, "stream sync: %s", cudaGetErrorString(e));
   return TCCG_OK;
+}
+
+extern "C" int tccg_plan_run_events(const tccg_plan* p, const void* A, const void* B, void* C,
+                                    double alpha, double beta, void* ws, size_t ws_bytes,
+                                    void* stream, void* const* events) {
+  if (!events) return fail(TCCG_ERR_INVALID, "null events");
+  cudaEvent_t ev[6];
+  for (int i = 0; i < 6; ++i) {
+    ev[i] = reinterpret_cast<cudaEvent_t>(events[i]);
+    if (!ev[i]) return fail(TCCG_ERR_INVALID, "event %d is null", i);
+  }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  // pre-record every event so that slots without a kernel read as 0 ms
+  for (int i = 0; i < 6; ++i) CUDA_TRY(cudaEventRecord(ev[i], s));
+  g_events = ev;
+  int rc = tccg_plan_run(p, A, B, C, alpha, beta, ws, ws_bytes, stream);
+  g_events = nullptr;
+  return rc;
 }
 
 // --------------------------------------------------------------------------
@@ -1979,7 +2033,8 @@ extern "C" int tccg_group_destroy(tccg_group* g) {
 // PREC_BF16X3, but everything it needs besides the caller's A, B and C -- the
 // offset tables, the packed operands and the status word -- lives in the
 // static device array below: TCCG_NOALLOC_SCRATCH_BYTES (64 MiB) on every GPU
-// that loads the library, held until the process exits.
+// that loads the library, held until the process exits. The status word is
+// read (and cleared) by tccg_gett_bf16x3_noalloc_status.
 #define TCCG_NOALLOC_SCRATCH_BYTES (64ull << 20)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[TCCG_NOALLOC_SCRATCH_BYTES];
 
@@ -1998,6 +2053,8 @@ static int noalloc_setup(int dev) {
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e == cudaSuccess)
       e = cudaDeviceGetAttribute(&g_noalloc_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaMemset(ptr, 0, sizeof(int32_t));  // the status word
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     g_noalloc_ptr[dev] = (e == cudaSuccess) ? ptr : nullptr;
     g_noalloc_err[dev] = e;
   });
@@ -2046,11 +2103,10 @@ extern "C" int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, c
     return fail(TCCG_ERR_INVALID, "mode counts (nm=%d nn=%d nk=%d) must be in [1,%d]", d.nm, d.nn,
                 d.nk, TCCG_MAX_MODES);
   int64_t M = 1, N = 1, K = 1;
-  for (int i = 0; i < d.nm; ++i) { if (d.m_ext[i] < 1) return fail(TCCG_ERR_INVALID, "bad M extent"); M *= d.m_ext[i]; }
-  for (int i = 0; i < d.nn; ++i) { if (d.n_ext[i] < 1) return fail(TCCG_ERR_INVALID, "bad N extent"); N *= d.n_ext[i]; }
-  for (int i = 0; i < d.nk; ++i) { if (d.k_ext[i] < 1) return fail(TCCG_ERR_INVALID, "bad K extent"); K *= d.k_ext[i]; }
-  if (M > (int64_t)1 << 31 || N > (int64_t)1 << 31 || K > (int64_t)1 << 31)
-    return fail(TCCG_ERR_UNSUPPORTED, "M, N and K must each be <= 2^31");
+  int rc0 = mode_product("M", d.nm, d.m_ext, &M);
+  if (!rc0) rc0 = mode_product("N", d.nn, d.n_ext, &N);
+  if (!rc0) rc0 = mode_product("K", d.nk, d.k_ext, &K);
+  if (rc0) return rc0;
   // scratch layout: status | a_m | a_k | b_n | b_k | c_m | c_n | A' | B'
   const int64_t Kc = 2 * round_up(K, 32);
   size_t off = 256;
@@ -2083,8 +2139,8 @@ extern "C" int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, c
   int64_t* t_bk = reinterpret_cast<int64_t*>(w + o_bk);
   int64_t* t_cm = reinterpret_cast<int64_t*>(w + o_cm);
   int64_t* t_cn = reinterpret_cast<int64_t*>(w + o_cn);
-  // the previous call's status word may be left over: clear it
-  CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int32_t), s));
+  // the status word keeps the first code a kernel recorded (from this or an
+  // earlier call) until tccg_gett_bf16x3_noalloc_status reads and clears it
   const int64_t ntab = 2 * (M + N + K);
   noalloc_tables_kernel<<<(unsigned)std::min<int64_t>(cdiv(ntab, 256), 4096), 256, 0, s>>>(
       d, t_am, t_ak, t_bn, t_bk, t_cm, t_cn, M, N, K);
@@ -2123,6 +2179,21 @@ extern "C" int tccg_gett_bf16x3_noalloc(const tccg_desc* desc, const float* A, c
   const int64_t tiles = (int64_t)a.tiles_m * a.tiles_n;
   if (tiles > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
   const int grid = (int)std::min<int64_t>(tiles, g_noalloc_sms[dev]);
+  take_injection(a);
   gett_tc_kernel<TC_BF16X3><<<grid, Cfg::NUM_THREADS, Cfg::SMEM_BYTES, s>>>(tmA, tmB, a);
   return launch_check("gett_tc (allocation-free)");
+}
+
+extern "C" int tccg_gett_bf16x3_noalloc_status(int32_t* device_status) {
+  if (!device_status) return fail(TCCG_ERR_INVALID, "null argument");
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= TCCG_NOALLOC_MAX_DEVICES) return fail(TCCG_ERR_UNSUPPORTED, "device index %d", dev);
+  int rc = noalloc_setup(dev);
+  if (rc) return rc;
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(device_status, g_noalloc_ptr[dev], sizeof(int32_t), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemset(g_noalloc_ptr[dev], 0, sizeof(int32_t)));
+  CUDA_TRY(cudaDeviceSynchronize());
+  return TCCG_OK;
 }

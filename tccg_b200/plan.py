@@ -272,6 +272,31 @@ class Plan:
             ctypes.c_size_t(ws_n), ctypes.c_void_p(stream.cuda_stream), ms))
         return float(ms[0]), float(ms[1]), float(ms[2])
 
+    def run_events(self, A, B, C, events, alpha: Optional[float] = None,
+                   beta: Optional[float] = None, workspace=None, stream=None) -> None:
+        """``run`` that records the six ``torch.cuda.Event`` objects ``events``
+        (created with enable_timing=True) around its kernels without
+        synchronising: events[2i], events[2i+1] bracket packing (i = 0), the
+        GEMM kernel (1) and the reduction/transposition (2)."""
+        import torch
+        alpha = self.con.alpha if alpha is None else alpha
+        beta = self.con.beta if beta is None else beta
+        if stream is None:
+            stream = torch.cuda.current_stream(C.device)
+        if workspace is None and self.workspace_bytes:
+            workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=C.device)
+        handles = (ctypes.c_void_p * 6)()
+        for i, ev in enumerate(events):
+            if not ev.cuda_event:
+                ev.record(stream)  # torch creates the event on its first record
+            handles[i] = ev.cuda_event
+        N.check(self._lib.tccg_plan_run_events(
+            self._h, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(B.data_ptr()),
+            ctypes.c_void_p(C.data_ptr()), float(alpha), float(beta),
+            ctypes.c_void_p(workspace.data_ptr() if workspace is not None else 0),
+            ctypes.c_size_t(workspace.numel() if workspace is not None else 0),
+            ctypes.c_void_p(stream.cuda_stream), handles))
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

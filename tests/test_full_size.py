@@ -64,6 +64,77 @@ def test_configuration_sampled_vs_fp64(cuda, cfg, precision):
     assert m["normwise"] <= tol, m
 
 
+def _sampled_metrics(con, A, B, C0, out, n=4096):
+    """error_metrics of ``out`` on n entries spread over C against the FP64
+    oracle evaluated on the values of A, B (and C0 when beta != 0) as given
+    (bf16 operands are widened exactly to FP32 first)."""
+    import torch
+    ln = _loopnest(con)
+    lins = np.unique(np.linspace(0, ln.size_c - 1, n).astype(np.int64))
+    wide = lambda t: (t.float() if t.dtype == torch.bfloat16 else t).cpu().numpy()
+    Cn = wide(C0) if con.beta != 0 else None
+    ref = ln.sample64(wide(A), wide(B), Cn, con.alpha, con.beta, lins)
+    return error_metrics(out[torch.from_numpy(lins).to(out.device)].double().cpu().numpy(), ref)
+
+
+# BF16 products of bf16 operands are exact in FP32; what remains is the FP32
+# accumulation. On the tensor cores each MMA (16 k) adds into the FP32
+# accumulator with truncation, up to one ulp (2^-23 relative) per add,
+# biased toward zero, so over K/16 adds the normwise error stays below
+# (K/16) * 2^-23; on the CUDA cores it is FP32 round-to-nearest FFMA.
+def _bf16_bound(K):
+    return max(1e-5, (K / 16) * 2.0 ** -23)
+
+
+@pytest.mark.parametrize("method", ["gett", "ttgt"])
+def test_configuration2_bf16_inputs(cuda, method):
+    """Configuration 2 with BF16 operands (bf16 precision: bf16 products,
+    FP32 accumulation; beta = 1 with C preloaded), GETT and TTGT: 4096
+    entries against the FP64 oracle of the same bf16 values."""
+    import torch
+    from tccg_b200.api import Compiled
+    from tccg_b200.plan import Tuning
+    con = parse_text(CFG[2])
+    A, B, C0 = _data(con, torch.float32, 210)
+    Ab, Bb = A.bfloat16(), B.bfloat16()
+    c = Compiled(con, "bf16", Tuning(method=method), dtype="bf16")
+    C = C0.clone()
+    c(Ab, Bb, C)
+    torch.cuda.synchronize()
+    assert c.plan.status() == 0
+    m = _sampled_metrics(con, Ab, Bb, C0, C)
+    assert m["normwise"] <= _bf16_bound(con.sizeK), m
+    assert m["tccg_equal_pass"], m
+
+
+@pytest.mark.parametrize("precision", ["bf16", "fp64"])
+def test_configuration3_bf16_fp64_vs_oracle(cuda, precision):
+    """Configuration 3 at full size (M = N = 32768, K = 4096) in BF16 (bf16
+    operands, tensor cores) and in FP64 (DFMA): 4096 entries against the FP64
+    oracle. FP64 sums of 4096 products: normwise within 1e-13, and TCCG's
+    equal() at its double tolerance 1e-9 (tccg.py:869-873)."""
+    import torch
+    from tccg_b200.api import Compiled
+    con = parse_text(CFG[3])
+    if precision == "fp64":
+        A, B, _ = _data(con, torch.float64, 220)
+        c = Compiled(con, "fp64")
+    else:
+        A, B, _ = _data(con, torch.float32, 221)
+        A, B = A.bfloat16(), B.bfloat16()
+        c = Compiled(con, "bf16", dtype="bf16")
+    C = c(A, B)
+    torch.cuda.synchronize()
+    assert c.plan.status() == 0
+    m = _sampled_metrics(con, A, B, None, C)
+    del C
+    if precision == "fp64":
+        assert m["normwise"] <= 1e-13, m
+        assert m["tccg_equal_worst"] <= 1e-9, m
+    else:
+        assert m["normwise"] <= _bf16_bound(con.sizeK), m
+
+
 @pytest.mark.parametrize("precision", ["bf16x3", "fp32", "fp64"])
 def test_configuration3_scaling_is_exact(cuda, precision):
     """Scaling A by 4 and B by 0.5 scales every product by exactly 2 (powers

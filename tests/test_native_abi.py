@@ -73,3 +73,31 @@ def test_tuning_struct_matches_the_header():
     assert len(fields) == len(re.findall(r";", body)), "tccg_tuning holds int32_t fields only"
     assert [f[0] for f in N.Tuning._fields_] == fields
     assert ctypes.sizeof(N.Tuning) == 4 * len(fields)
+
+
+def test_extent_products_cannot_wrap():
+    """Extents whose product passes 2^63 (or wraps to a small number) are
+    rejected before any table is built: the running product is checked
+    before each multiplication."""
+    L = N.lib()
+    h = ctypes.c_void_p()
+    for exts in ([1 << 32, 1 << 32], [1 << 31, 2], [3, 1 << 30]):
+        d = N.Desc()
+        d.nm, d.nn, d.nk = len(exts), 1, 1
+        for i, e in enumerate(exts):
+            d.m_ext[i] = e
+        d.n_ext[0] = d.k_ext[0] = 4
+        rc = L.tccg_plan_create(ctypes.byref(d), N.F32, N.PREC_FP32, None, ctypes.byref(h))
+        assert rc == N.ERR_UNSUPPORTED and not h.value, exts
+        assert b"2^31" in L.tccg_last_error()
+        rc = L.tccg_gett_bf16x3_noalloc(ctypes.byref(d), ctypes.c_void_p(16), ctypes.c_void_p(16),
+                                        ctypes.c_void_p(16), 1.0, 0.0, None)
+        assert rc == N.ERR_UNSUPPORTED, exts
+
+
+def test_debug_trigger_validates_its_arguments():
+    L = N.lib()
+    assert L.tccg_debug_inject_timeout(-1, 100) == N.ERR_INVALID
+    assert L.tccg_debug_inject_timeout(0, 0) == N.ERR_INVALID
+    assert L.tccg_debug_inject_timeout(0, 5000) == N.ERR_INVALID
+    assert L.tccg_gett_bf16x3_noalloc_status(None) == N.ERR_INVALID

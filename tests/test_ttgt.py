@@ -131,14 +131,12 @@ def test_loops_over_gemm(cuda, precision, case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["bf16", "bf16x3"])
-@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+@pytest.mark.parametrize("precision,dtype", [("bf16", "f32"), ("bf16", "bf16"), ("bf16x3", "f32")])
 def test_cuda_core_variant_of_bf16_precisions(cuda, precision, dtype):
     """variant < 0: BF16 precisions on the CUDA-core kernel (bandwidth-bound
-    shapes); BF16 keeps its semantics (operands rounded to bf16)."""
+    shapes); BF16 keeps its semantics (operands rounded to bf16). BF16
+    operands go with the bf16 precision only."""
     import torch
-    if precision == "bf16x3" and dtype == "bf16":
-        pytest.skip("BF16 operands go with the bf16 precision only")
     lc, la, lb, sizes, alpha, beta = CASES[0]
     con = make_contraction(lc, la, lb, sizes, alpha, beta)
     ln = LoopNest(lc, la, lb, sizes)
