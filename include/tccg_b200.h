@@ -118,6 +118,10 @@ typedef struct tccg_tuning {
   int32_t tail_split;  /* tcgen05, automatic k-split: 0 = run the tiles of a short last round of
                           the persistent grid as k slices where that pays, -1 = never (grouped
                           runs never split that way) */
+  int32_t load;        /* tcgen05 BF16X3 with FP32 operands: 0 = chosen by the model, 1 = packing
+                          pass + TMA loads (128x192 tiles), 2 = gather: producer warps read the
+                          caller's tensors through the offset tables and split them into the
+                          swizzled bf16 stages themselves (128x128 tiles, no packing pass) */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

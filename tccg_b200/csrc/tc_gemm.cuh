@@ -43,23 +43,60 @@ namespace tccg {
 
 enum TcMode : int { TC_BF16 = 0, TC_BF16X3 = 1 };
 
+// How the operand stages are filled.
+//   TC_LOAD_TMA   : one thread issues 2-D TMA loads of operands packed K-major
+//                   by pack_kernel (a separate pass through HBM before the GETT).
+//   TC_LOAD_GATHER: four producer warps gather FP32 elements straight from the
+//                   caller's tensors through the offset tables (cp.async into
+//                   an FP32 staging ring), split them into bf16 hi/lo and write
+//                   the same 128-byte-swizzled K-major stage TMA would deliver
+//                   -- no packing pass, each operand element crosses HBM once
+//                   per tile that reads it. BF16X3 only.
+enum TcLoad : int { TC_LOAD_TMA = 0, TC_LOAD_GATHER = 1 };
+
+// Gather read schedule of one operand (chosen at plan creation).
+enum GatherRead : int {
+  GATHER_ROWS = 0,   // lanes along rows, 4-byte copies (rows have the smallest stride)
+  GATHER_K = 1,      // lanes along k, 4-byte copies
+  GATHER_KQUAD = 2,  // lanes along k, 16-byte copies of 4 consecutive, aligned k
+};
+
 // Tile configuration per mode. BF16X3 uses 128x192 tiles so that each of the 8
 // epilogue warps keeps its 96-column running chunk sum in registers (a 10-warp
 // CTA has at most 168 registers per thread: 3 warps share one SM sub-partition).
-template <int MODE>
+// The gather variant has 13 warps (4 producers, the MMA warp, 8 epilogue
+// warps: at most 152 registers each), so its tiles are 128x128 (64 running
+// sums per epilogue warp).
+template <int MODE, int LOAD = TC_LOAD_TMA>
 struct TcCfgT {
+  static constexpr bool GATHER = LOAD == TC_LOAD_GATHER;
+  static_assert(!GATHER || MODE == TC_BF16X3, "the gather loader serves split-BF16x3");
   static constexpr int BM = 128;
-  static constexpr int BN = (MODE == TC_BF16X3) ? 192 : 256;
+  static constexpr int BN = GATHER ? 128 : (MODE == TC_BF16X3) ? 192 : 256;
   static constexpr int ROW_BYTES = 128;  // one swizzle row per operand row per stage
-  static constexpr int STAGES = (MODE == TC_BF16X3) ? 5 : 4;
+  static constexpr int STAGES = GATHER ? 2 : (MODE == TC_BF16X3) ? 5 : 4;
   static constexpr int A_STAGE = BM * ROW_BYTES;   // 16 KB
-  static constexpr int B_STAGE = BN * ROW_BYTES;   // 24 / 32 KB
+  static constexpr int B_STAGE = BN * ROW_BYTES;   // 16 / 24 / 32 KB
   static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-  static constexpr int TMEM_COLS = 512;            // two accumulators of BN columns
-  static constexpr int ACC_STRIDE = 256;           // accumulator b starts at column 256*b
-  static constexpr int NUM_THREADS = 320;
+  static constexpr int ACC_STRIDE = GATHER ? 128 : 256;  // accumulator b starts at column ACC_STRIDE*b
+  static constexpr int TMEM_COLS = 2 * ACC_STRIDE;       // two accumulators of BN columns
+  static constexpr int PRODUCER_WARPS = GATHER ? 4 : 1;
+  static constexpr int MMA_WARP = PRODUCER_WARPS;
+  static constexpr int EPI_WARP0 = PRODUCER_WARPS + 1;
   static constexpr int EPI_WARPS = 8;
-  static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
+  static constexpr int NUM_THREADS = 32 * (PRODUCER_WARPS + 1 + EPI_WARPS);
+  // gather: FP32 staging ring of STG_SLOTS k-blocks (copies run STG_SLOTS - 1
+  // k-blocks ahead of the conversion); a staging row holds the 32 source
+  // elements of one operand row, 36 floats apart (16-byte copies stay
+  // aligned, conversion reads are bank-conflict free) or 33 (4-byte copies
+  // along rows are bank-conflict free)
+  static constexpr int KB_ELEMS = 32;
+  static constexpr int STG_LD = 36;
+  static constexpr int STG_SLOTS = GATHER ? 3 : 0;
+  static constexpr int STG_SLOT_BYTES = (BM + BN) * STG_LD * 4;
+  static constexpr int ROWCACHE_BYTES = GATHER ? (BM + BN) * 8 : 0;
+  static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES +
+                                       (size_t)STG_SLOTS * STG_SLOT_BYTES + ROWCACHE_BYTES + 256;
 };
 
 struct TcArgs {
@@ -93,6 +130,12 @@ struct TcArgs {
   // first k-block of tile skip_tile1 - 1, so the MMA warp's wait for it runs
   // out and the CTA winds down with a status code.
   int32_t skip_tile1;
+  // TC_LOAD_GATHER: operand o (0 = GA, rows m; 1 = GB, rows n) element (r, k)
+  // is gsrc[o][grow[o][r] + gk[o][k]] (FP32), read with schedule gread[o]
+  const float* gsrc[2];
+  const int64_t* grow[2];
+  const int64_t* gk[2];
+  int32_t gread[2];
 };
 
 // Grouped launch: one entry per contraction, in device memory. The tensor maps
@@ -171,17 +214,252 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
   return r;
 }
 
+// ---- gather loader (TC_LOAD_GATHER) ------------------------------------------
+// The producer warps walk this CTA's (tile, k-block) jobs in the order the MMA
+// warp consumes them, twice: copies run STG_SLOTS - 1 jobs ahead of the
+// conversion into MMA stages.
+struct GatherJob {
+  int tile, kb;
+  bool valid;
+  TileRef t;
+};
+
+template <bool GROUPED>
+__device__ __forceinline__ void gjob_seek(GatherJob& j, int num_tiles, const TcArgs* a1,
+                                          const TcGroup& g) {
+  while (j.tile < num_tiles) {
+    j.t = resolve_tile<GROUPED>(j.tile, nullptr, nullptr, a1, g);
+    if (j.t.kb_begin < j.t.kb_end) {
+      j.kb = j.t.kb_begin;
+      j.valid = true;
+      return;
+    }
+    j.tile += gridDim.x;
+  }
+  j.valid = false;
+}
+
+template <bool GROUPED>
+__device__ __forceinline__ void gjob_next(GatherJob& j, int num_tiles, const TcArgs* a1,
+                                          const TcGroup& g) {
+  if (++j.kb < j.t.kb_end) return;
+  j.tile += gridDim.x;
+  gjob_seek<GROUPED>(j, num_tiles, a1, g);
+}
+
+// Staging row stride of an operand (floats): 33 for copies along rows (the 32
+// lanes' 4-byte writes land in 32 banks), 36 for copies along k (16-byte
+// aligned rows; the conversion reads 8 rows x 32 bytes per phase conflict free).
+__device__ __forceinline__ int gather_ld(int read) { return read == GATHER_ROWS ? 33 : 36; }
+
+// Producer barrier over the 128 producer threads (named barrier 1) that also
+// ANDs a flag across them, so that every producer takes the same branch.
+__device__ __forceinline__ bool producers_and(bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, 1, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)v)
+      : "memory");
+  return out != 0;
+}
+
+// Row offsets of the job's tile (A rows then B rows) into the shared cache.
+template <int BM, int BN>
+__device__ __forceinline__ void gather_rows(const GatherJob& j, int64_t* rowc, int ptid) {
+  const TcArgs& a = *j.t.a;
+  for (int r = ptid; r < BM + BN; r += 128) {
+    const int o = r >= BM;
+    const int64_t row = o ? (int64_t)j.t.tn * BN + (r - BM) : (int64_t)j.t.tm * BM + r;
+    const int64_t R = o ? a.N : a.M;
+    rowc[r] = row < R ? __ldg(a.grow[o] + row) : 0;
+  }
+}
+
+// Asynchronous copies of one job's source elements into a staging slot:
+// operand o's element (r, k) of the k-block goes to slot_o[r * ld + k].
+template <int BM, int BN>
+__device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, const int64_t* rowc,
+                                             int ptid) {
+  const TcArgs& a = *j.t.a;
+  const int pw = ptid >> 5, lane = ptid & 31;
+  const int k0 = j.kb * 32;
+  const int kn = a.K - k0 < 32 ? a.K - k0 : 32;  // k of this block inside K
+#pragma unroll 1
+  for (int o = 0; o < 2; ++o) {
+    const float* src = a.gsrc[o];
+    const int64_t R = o ? a.N : a.M;
+    const int64_t r0 = o ? (int64_t)j.t.tn * BN : (int64_t)j.t.tm * BM;
+    const int rows = o ? BN : BM;
+    const int nr = R - r0 < rows ? (int)(R - r0) : rows;
+    const int64_t* rc = rowc + (o ? BM : 0);
+    const int read = a.gread[o];
+    const int ld = gather_ld(read);
+    float* dst = slot + (o ? BM * 36 : 0);
+    const int64_t* gk = a.gk[o] + k0;
+    if (read == GATHER_ROWS) {
+#pragma unroll 1
+      for (int k = 0; k < kn; ++k) {
+        const int64_t ko = __ldg(gk + k);
+        for (int r = ptid; r < nr; r += 128) cp_async_elem<4>(dst + r * ld + k, src + rc[r] + ko);
+      }
+    } else if (read == GATHER_K) {
+      if (lane < kn) {
+        const int64_t ko = __ldg(gk + lane);
+#pragma unroll 4
+        for (int r = pw; r < nr; r += 4) cp_async_elem<4>(dst + r * ld + lane, src + rc[r] + ko);
+      }
+    } else {  // GATHER_KQUAD
+      const int kq = 4 * (lane & 7), sub = lane >> 3;
+      if (kq + 3 < kn) {
+        const int64_t ko = __ldg(gk + kq);
+#pragma unroll 4
+        for (int r = pw * 4 + sub; r < nr; r += 16) cp_async_16(dst + r * ld + kq, src + rc[r] + ko);
+      } else {
+        for (int e = 0; e < 4 && kq + e < kn; ++e) {
+          const int64_t ko = __ldg(gk + kq + e);
+          for (int r = pw * 4 + sub; r < nr; r += 16)
+            cp_async_elem<4>(dst + r * ld + kq + e, src + rc[r] + ko);
+        }
+      }
+    }
+  }
+}
+
+// Converts one job's staging slot into an MMA stage: element (r, k) becomes
+// hi = bf16(x), lo = bf16(x - hi) in the K-major [hi(32 k) | lo(32 k)] row r,
+// 16-byte chunk c stored at chunk c ^ (r & 7) (the 128-byte swizzle TMA
+// applies); rows past the operand and k past K are zero, as TMA's
+// out-of-bounds fill and the packing pass leave them.
+template <int BM, int BN>
+__device__ __forceinline__ void gather_convert(const GatherJob& j, const float* slot, uint8_t* stA,
+                                               uint8_t* stB, int ptid) {
+  const TcArgs& a = *j.t.a;
+  const int pw = ptid >> 5, lane = ptid & 31;
+  const int k0 = j.kb * 32;
+  const int kn = a.K - k0 < 32 ? a.K - k0 : 32;
+  const int k8 = lane >> 3;
+#pragma unroll 1
+  for (int rg = pw; rg < (BM + BN) / 8; rg += 4) {
+    const int r = rg * 8 + (lane & 7);
+    const int o = r >= BM;
+    const int rr = r - (o ? BM : 0);
+    const int64_t R = o ? a.N : a.M;
+    const int64_t r0 = o ? (int64_t)j.t.tn * BN : (int64_t)j.t.tm * BM;
+    const bool row_ok = r0 + rr < R;
+    const int ld = gather_ld(a.gread[o]);
+    const float* srow = slot + (o ? BM * 36 : 0) + rr * ld + k8 * 8;
+    float v[8];
+    if (ld == 36) {
+      const float4 x0 = *reinterpret_cast<const float4*>(srow);
+      const float4 x1 = *reinterpret_cast<const float4*>(srow + 4);
+      v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
+      v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] = srow[e];
+    }
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int e = 0; e < 8; e += 2) {
+      const float x0 = (row_ok && k8 * 8 + e < kn) ? v[e] : 0.0f;
+      const float x1 = (row_ok && k8 * 8 + e + 1 < kn) ? v[e + 1] : 0.0f;
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+      const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+      const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+      const __nv_bfloat162 hp = __halves2bfloat162(h0, h1), lp = __halves2bfloat162(l0, l1);
+      hw[e / 2] = *reinterpret_cast<const uint32_t*>(&hp);
+      lw[e / 2] = *reinterpret_cast<const uint32_t*>(&lp);
+    }
+    uint8_t* drow = (o ? stB : stA) + rr * 128;
+    const int sw = rr & 7;
+    *reinterpret_cast<uint4*>(drow + ((k8 ^ sw) << 4)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4*>(drow + (((4 + k8) ^ sw) << 4)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+  }
+}
+
+// The four producer warps of the gather variant.
 template <int MODE, bool GROUPED>
+__device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup& g, int num_tiles,
+                                                uint8_t* sA, uint8_t* sB, float* stg,
+                                                int64_t* rowc, uint64_t* full, uint64_t* empty,
+                                                uint64_t wait_ns, int skip_tile1,
+                                                int32_t* status) {
+  using Cfg = TcCfgT<MODE, TC_LOAD_GATHER>;
+  constexpr int S = Cfg::STG_SLOTS;
+  constexpr int SLOT = Cfg::STG_SLOT_BYTES / 4;  // floats per staging slot
+  const int ptid = threadIdx.x;                  // 0..127
+  GatherJob ji, jc;                              // issue / conversion iterators
+  ji.tile = jc.tile = blockIdx.x;
+  gjob_seek<GROUPED>(ji, num_tiles, a1, g);
+  gjob_seek<GROUPED>(jc, num_tiles, a1, g);
+  int cached = -1;  // tile whose row offsets are in rowc
+  auto issue = [&](int slot) {
+    if (ji.valid) {
+      if (ji.tile != cached) {  // every producer is past its copies of the old tile
+        named_barrier_sync(1, 128);
+        gather_rows<Cfg::BM, Cfg::BN>(ji, rowc, ptid);
+        named_barrier_sync(1, 128);
+        cached = ji.tile;
+      }
+      gather_issue<Cfg::BM, Cfg::BN>(ji, stg + slot * SLOT, rowc, ptid);
+      gjob_next<GROUPED>(ji, num_tiles, a1, g);
+    }
+    cp_async_commit();  // one group per job (empty past the last), so waits count jobs
+  };
+  int islot = 0;
+  for (int d = 0; d < S - 1; ++d) {
+    issue(islot);
+    islot = islot + 1 == S ? 0 : islot + 1;
+  }
+  int stage = 0, cslot = 0;
+  uint32_t phase = 0;
+  while (jc.valid) {
+    const bool free_stage = mbar_wait(&empty[stage], phase ^ 1, wait_ns);
+    cp_async_wait<S - 2>();  // this thread's copies of job jc landed
+    // all producers' copies of jc landed, their previous conversion is done
+    if (!producers_and(free_stage)) {
+      record_error(status, 1);
+      break;
+    }
+    issue(islot);
+    islot = islot + 1 == S ? 0 : islot + 1;
+    if (jc.tile + 1 != skip_tile1 || jc.kb != jc.t.kb_begin) {
+      gather_convert<Cfg::BM, Cfg::BN>(jc, stg + cslot * SLOT, sA + stage * Cfg::A_STAGE,
+                                       sB + stage * Cfg::B_STAGE, ptid);
+      fence_proxy_async_smem();  // the stage is read by the tensor cores (async proxy)
+      mbar_arrive(&full[stage]);
+    }
+    cslot = cslot + 1 == S ? 0 : cslot + 1;
+    if (++stage == Cfg::STAGES) {
+      stage = 0;
+      phase ^= 1;
+    }
+    gjob_next<GROUPED>(jc, num_tiles, a1, g);
+  }
+  cp_async_wait<0>();  // no copy in flight when the producers leave
+}
+
+template <int MODE, int LOAD, bool GROUPED>
 __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUtensorMap* tmB,
                                              const TcArgs* a1, const TcGroup& g,
                                              int32_t* status) {
-  using Cfg = TcCfgT<MODE>;
+  using Cfg = TcCfgT<MODE, LOAD>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_addr = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + (((raw_addr + 1023u) & ~1023u) - raw_addr);
   uint8_t* sA = smem;                                   // STAGES x 16 KB
-  uint8_t* sB = smem + Cfg::STAGES * Cfg::A_STAGE;      // STAGES x 32 KB
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
+  uint8_t* sB = smem + Cfg::STAGES * Cfg::A_STAGE;      // STAGES x B_STAGE
+  // gather: FP32 staging slots and the row-offset cache after the stages
+  float* stg = reinterpret_cast<float*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
+  int64_t* rowc = reinterpret_cast<int64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES +
+                                             Cfg::STG_SLOTS * Cfg::STG_SLOT_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES +
+                                               Cfg::STG_SLOTS * Cfg::STG_SLOT_BYTES +
+                                               Cfg::ROWCACHE_BYTES);
   uint64_t* full = bars;                   // [STAGES]
   uint64_t* empty = bars + Cfg::STAGES;    // [STAGES]
   uint64_t* accf = bars + 2 * Cfg::STAGES; // [2] accumulator ready
@@ -200,7 +478,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
-      mbar_init(&full[s], 1);
+      mbar_init(&full[s], Cfg::GATHER ? 32 * Cfg::PRODUCER_WARPS : 1);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -209,12 +487,12 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     }
     mbar_init(drain, 1);
     fence_mbar_init();
-    if (!GROUPED) {
+    if (!GROUPED && !Cfg::GATHER) {
       tma_prefetch_desc(tmA);
       tma_prefetch_desc(tmB);
     }
   }
-  if (warp == 1) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+  if (warp == Cfg::MMA_WARP) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -223,7 +501,12 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   // its operands (and nothing else this kernel reads) come from it
   grid_dep_wait();
 
-  if (warp == 0 && lane == 0) {
+  if (Cfg::GATHER && warp < Cfg::PRODUCER_WARPS) {
+    // ---------------- gather producers (4 warps) ----------------
+    if constexpr (Cfg::GATHER)
+      gather_producer<MODE, GROUPED>(a1, g, num_tiles, sA, sB, stg, rowc, full, empty, wait_ns,
+                                     skip_tile1, status);
+  } else if (!Cfg::GATHER && warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
     int stage = 0;
     uint32_t phase = 0;
@@ -254,7 +537,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       for (int s = 0; s < Cfg::STAGES; ++s)
         if (issued_phase[s] >= 0) (void)mbar_wait(&full[s], (uint32_t)issued_phase[s], wait_ns);
     }
-  } else if (warp == 1 && lane == 0) {
+  } else if (warp == Cfg::MMA_WARP && lane == 0) {
     // ---------------- MMA issuer ----------------
     int stage = 0;
     uint32_t phase = 0;
@@ -329,10 +612,10 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       tc_commit(drain);
       (void)mbar_wait(drain, 0, wait_ns);
     }
-  } else if (warp >= 2) {
+  } else if (warp >= Cfg::EPI_WARP0) {
     // ---------------- epilogue ----------------
     const int q = warp & 3;             // TMEM lanes [32q, 32q+32) are accessible to this warp
-    const int h = (warp - 2) >> 2;      // column half of the tile
+    const int h = (warp - Cfg::EPI_WARP0) >> 2;  // column half of the tile
     constexpr int HC = Cfg::BN / 2;     // columns per epilogue warp
     int acc = 0;
     uint32_t acc_phase = 0;
@@ -476,32 +759,32 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
 
   tc_fence_before();
   __syncthreads();
-  if (warp == 1) {
+  if (warp == Cfg::MMA_WARP) {
     tc_fence_after();
     tmem_dealloc(tbase, Cfg::TMEM_COLS);
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
+template <int MODE, int LOAD = TC_LOAD_TMA>
+__global__ void __launch_bounds__(TcCfgT<MODE, LOAD>::NUM_THREADS, 1)
     gett_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                    const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
   TcGroup g{nullptr, nullptr, 0, 0};
-  gett_tc_body<MODE, false>(&tmA, &tmB, &a, g, a.status);
+  gett_tc_body<MODE, LOAD, false>(&tmA, &tmB, &a, g, a.status);
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(TcCfgT<MODE>::NUM_THREADS, 1)
+template <int MODE, int LOAD = TC_LOAD_TMA>
+__global__ void __launch_bounds__(TcCfgT<MODE, LOAD>::NUM_THREADS, 1)
     gett_tc_group_kernel(const TcGroup g, int32_t* status) {
-  gett_tc_body<MODE, true>(nullptr, nullptr, nullptr, g, status);
+  gett_tc_body<MODE, LOAD, true>(nullptr, nullptr, nullptr, g, status);
 }
 
 // Tail split: C = alpha * (slice 0 + slice 1 + ...) + beta * C over the tail
 // tiles (RN adds in slice order). grid = (tail tiles, BM * BN / 256), block
 // 256: thread e of a tile takes element (m_local = e % BM, n_local = e / BM).
-template <int MODE>
+template <int MODE, int LOAD = TC_LOAD_TMA>
 __global__ void __launch_bounds__(256) tc_tail_reduce_kernel(const TcArgs a) {
-  using Cfg = TcCfgT<MODE>;
+  using Cfg = TcCfgT<MODE, LOAD>;
   grid_dep_wait();  // partial sums written by the GETT kernel before
   const int tail = a.tiles_m * a.tiles_n - a.full_tiles;
   const int tl = blockIdx.x;

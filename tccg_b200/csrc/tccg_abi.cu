@@ -100,6 +100,10 @@ struct tccg_plan {
   int32_t simt_shape = 0;             // SimtShape of the CUDA-core tiles
   int32_t simt_bm = 0, simt_bn = 0;   // its tile extents
   bool simt = false;    // CUDA-core kernels (else tcgen05)
+  // tcgen05 BF16X3: gather loader (operands read straight from the caller's
+  // tensors, no packing pass) and its read schedule per operand (GatherRead)
+  bool gather = false;
+  int32_t gread_a = 0, gread_b = 0;
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, off_tail = 0, ws_bytes = 0;
   char describe[512] = "";
@@ -156,26 +160,62 @@ static int choose_simt_shape(const tccg_plan* p, double* padded_work) {
 }
 
 static bool direct_eligible(const tccg_plan* p, int shape);
+static bool unit_first(int n, const int64_t* ext, const int64_t* str);
+
+// The gather loader of the tcgen05 BF16X3 kernel (TC_LOAD_GATHER) can serve
+// the plan: FP32 operands, GETT, one-SM tiles, and each operand read
+// coalesced along its gather direction (k quads, a unit-stride first K mode
+// read along k, a unit-stride first row mode read along rows) or small
+// enough (<= 4 MiB) to stay in L2 across its re-reads.
+static bool gather_eligible(const tccg_plan* p) {
+  if (p->prec != TCCG_PREC_BF16X3 || p->dtype != TCCG_F32 || p->tune.method != TCCG_METHOD_GETT ||
+      p->tune.pair || p->tune.load == 1)
+    return false;
+  if (p->tune.load == 2) return true;
+  const tccg_desc& d = p->d;
+  const int64_t small = 4 << 20;
+  const bool a_ok = p->ks_a || unit_first(d.nk, d.k_ext, d.a_k_stride) ||
+                    unit_first(d.nm, d.m_ext, d.a_m_stride) || p->M * p->K * 4 <= small;
+  const bool b_ok = p->ks_b || unit_first(d.nk, d.k_ext, d.b_k_stride) ||
+                    unit_first(d.nn, d.n_ext, d.b_n_stride) || p->N * p->K * 4 <= small;
+  return a_ok && b_ok;
+}
+
+// Tensor-core time model (seconds), fitted on B200 timings of the 256-item
+// batched workload: tensor cores at 0.6 PFLOP/s effective (x3 for
+// split-BF16x3) on 128 x 192 tiles, the C epilogue at 3 TB/s, operands
+// streamed at 4.5 TB/s three times with the packing pass (pack read, packed
+// write, GEMM read); the gather loader's 128 x 128 tiles at 0.5 PFLOP/s with
+// one operand pass. Tile padding counts as work.
+static double tc_time(const tccg_plan* p, bool gather) {
+  const double M = (double)p->M, N = (double)p->N, K = (double)p->K;
+  const double Mt = (double)round_up(p->M, 128), Nt = (double)round_up(p->N, gather ? 128 : 192);
+  const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
+  const double x3 = p->prec == TCCG_PREC_BF16X3 ? 3.0 : 1.0;
+  return std::max(2.0 * Mt * Nt * K * x3 / (gather ? 0.5e15 : 0.6e15),
+                  cb / 3e12 + (gather ? 1.0 : 3.0) * op / 4.5e12);
+}
+
+static bool choose_gather(const tccg_plan* p) {
+  if (!gather_eligible(p)) return false;
+  return p->tune.load == 2 || tc_time(p, true) < tc_time(p, false);
+}
 
 static bool choose_simt(const tccg_plan* p) {
   if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) return true;
-  if (p->tune.pair || p->tune.variant > 0) return false;
+  if (p->tune.pair || p->tune.variant > 0 || p->tune.load > 0) return false;
   if (p->tune.variant < 0) return true;
-  // Model fitted on B200 timings of mixed contractions (the 256-item
-  // batched workload): tensor cores at 0.6 PFLOP/s effective (x3 for
-  // split-BF16x3) on 128 x 192 tiles with a C epilogue at 3 TB/s; CUDA cores
-  // at 35 TFLOP/s; operands streamed three times (pack
-  // read, packed write, GEMM read) at 4.5 TB/s, once where the CUDA-core
-  // kernel reads them in place. Tile padding counts as work
-  // (CUDA cores: that of the shape choose_simt_shape picks).
+  // Against the tensor-core model (tc_time, the faster of its two loaders):
+  // CUDA cores at 35 TFLOP/s on the tile shape choose_simt_shape picks (its
+  // padding counted as work), operands streamed at 4.5 TB/s three times
+  // with a packing pass, once where the CUDA-core kernel reads them in place.
   const double M = (double)p->M, N = (double)p->N, K = (double)p->K;
-  const double Mt = (double)round_up(p->M, 128), Nt = (double)round_up(p->N, 192);
   double simt_work = 0;  // padded M x N of the CUDA-core tile shape it would use
   const int shape = choose_simt_shape(p, &simt_work);
   const double simt_passes = direct_eligible(p, shape) ? 1.0 : 3.0;  // operand reads
   const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
-  const double t_tc = std::max(2.0 * Mt * Nt * K * (p->prec == TCCG_PREC_BF16X3 ? 3.0 : 1.0) / 0.6e15,
-                               cb / 3e12 + 3.0 * op / 4.5e12);
+  double t_tc = tc_time(p, false);
+  if (gather_eligible(p)) t_tc = std::min(t_tc, tc_time(p, true));
   const double t_simt = std::max(2.0 * simt_work * K / 35e12, (cb + simt_passes * op) / 4.5e12);
   return t_simt < t_tc;
 }
@@ -545,7 +585,14 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   p->simt = choose_simt(p);
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
-  if (!rc && !simt_path(p)) {
+  if (!simt_path(p) && choose_gather(p)) {
+    // gather schedules: 16-byte k quads, else along the operand's faster
+    // direction (k or rows)
+    p->gather = true;
+    p->gread_a = p->ks_a ? GATHER_KQUAD : p->read_k_fast_a ? GATHER_K : GATHER_ROWS;
+    p->gread_b = p->ks_b ? GATHER_KQUAD : p->read_k_fast_b ? GATHER_K : GATHER_ROWS;
+  }
+  if (!rc && !simt_path(p) && !p->gather) {
     // tensor-core packs: unit stride on a later K mode -> k-block tiles read
     // along it; else walk the rows along the smallest-stride row mode when
     // that beats both the first row mode and reading along k
@@ -644,6 +691,8 @@ static int plan_layout(tccg_plan* p) {
     const bool pair = p->tune.pair != 0;
     if (pair)
       p->bn = x3 ? Tc2Cfg<TC_BF16X3>::BN : Tc2Cfg<TC_BF16>::BN;
+    else if (p->gather)
+      p->bn = TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::BN;
     else
       p->bn = x3 ? TcCfgT<TC_BF16X3>::BN : TcCfgT<TC_BF16>::BN;
     p->tiles_m = (int32_t)cdiv(p->M, pair ? 256 : 128);
@@ -696,9 +745,11 @@ static int plan_layout(tccg_plan* p) {
     } else
       p->grid = (int32_t)std::min<int64_t>(tiles, ctas);
     p->off_a = 0;
-    ws = align_up((size_t)(p->M * p->Kc) * 2, 256);
-    p->off_b = ws;
-    ws = align_up(ws + (size_t)(p->N * p->Kc) * 2, 256);
+    if (!p->gather) {  // packed operands
+      ws = align_up((size_t)(p->M * p->Kc) * 2, 256);
+      p->off_b = ws;
+      ws = align_up(ws + (size_t)(p->N * p->Kc) * 2, 256);
+    }
     if (p->ksplit > 1) {  // FP32 slices [split][N][M]
       p->off_part = ws;
       ws = align_up(ws + (size_t)p->ksplit * p->N * p->M * 4, 256);
@@ -707,6 +758,17 @@ static int plan_layout(tccg_plan* p) {
       p->off_tail = ws;
       ws = align_up(ws + (size_t)p->tail_split * (size_t)(mn - p->full_tiles) * p->bn * 128 * 4, 256);
     }
+    static const char* gr[] = {"rows", "k", "kquad"};
+    if (p->gather)
+      snprintf(p->describe, sizeof(p->describe),
+               "method=GETT prec=bf16x3 kernel=gett_tc<BF16X3,gather> tile=128x%d stages=%d M=%lld "
+               "N=%lld K=%lld kblocks=%d chunk=%d ksplit=%d tail=%dx%d grid=%d raster=%d pack=none "
+               "(gather a=%s b=%s)",
+               p->bn, TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::STAGES, (long long)p->M, (long long)p->N,
+               (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit,
+               p->tail_split > 1 ? (int)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles) : 0,
+               p->tail_split, p->grid, p->raster, gr[p->gread_a], gr[p->gread_b]);
+    else
     snprintf(p->describe, sizeof(p->describe),
              "method=%s prec=%s kernel=gett_tc%s<%s> tile=%dx%d stages=%d M=%lld N=%lld K=%lld "
              "kblocks=%d chunk=%d ksplit=%d tail=%dx%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
@@ -826,6 +888,12 @@ static cudaError_t set_attrs() {
                            (int)TcCfgT<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3, TC_LOAD_GATHER>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::SMEM_BYTES));
+  chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3, TC_LOAD_GATHER>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)simt_group_smem_bytes<float>()));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1204,10 +1272,103 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   return rc;
 }
 
+// Arguments of the tcgen05 kernels common to both loaders (k-split partial
+// sums and tail slices in the workspace `ws`).
+static TcArgs tc_args(const tccg_plan* p, float* Cout, const int64_t* c_m, const int64_t* c_n,
+                      float alpha, float beta, char* ws) {
+  TcArgs a{};
+  a.M = (int32_t)p->M;
+  a.N = (int32_t)p->N;
+  a.K = (int32_t)p->K;
+  a.num_kb = p->num_kb;
+  a.tiles_m = p->tiles_m;
+  a.tiles_n = p->tiles_n;
+  a.raster = p->raster;
+  a.chunk_kb = p->chunk_kb;
+  a.C = Cout;
+  a.c_m_off = c_m;
+  a.c_n_off = c_n;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.status = p->d_status;
+  a.ksplit = p->ksplit;
+  a.kb_per_split = p->kb_per_split;
+  a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(ws + p->off_part) : nullptr;
+  a.full_tiles = p->full_tiles;
+  a.tail_split = p->tail_split;
+  a.tail_kb = p->tail_kb;
+  a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
+  return a;
+}
+
+// Gather loader: the kernel reads GA and GB through the plan's offset tables.
+// 16-byte copies need a 16-byte aligned operand; an unaligned one is read
+// along k 4 bytes at a time (the same elements, the same stages).
+static void set_gather(TcArgs& a, const tccg_plan* p, const void* GA, const void* GB) {
+  a.gsrc[0] = static_cast<const float*>(GA);
+  a.gsrc[1] = static_cast<const float*>(GB);
+  a.grow[0] = p->t_a_m;
+  a.grow[1] = p->t_b_n;
+  a.gk[0] = p->t_a_k;
+  a.gk[1] = p->t_b_k;
+  const bool al_a = (reinterpret_cast<uintptr_t>(GA) & 15u) == 0;
+  const bool al_b = (reinterpret_cast<uintptr_t>(GB) & 15u) == 0;
+  a.gread[0] = p->gread_a == GATHER_KQUAD && !al_a ? GATHER_K : p->gread_a;
+  a.gread[1] = p->gread_b == GATHER_KQUAD && !al_b ? GATHER_K : p->gread_b;
+}
+
+// Reduction after the tcgen05 kernel: tail slices or k-split slices.
+template <int LOAD>
+static int tc_reduce(const tccg_plan* p, const TcArgs& a, float* Cout, const int64_t* c_m,
+                     const int64_t* c_n, float alpha, float beta, cudaStream_t s) {
+  const bool x3 = p->prec == TCCG_PREC_BF16X3;
+  if (p->tail_split > 1) {
+    const unsigned tail = (unsigned)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles);
+    mark(2, 0, s);
+    if constexpr (LOAD == TC_LOAD_GATHER) {
+      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16X3, TC_LOAD_GATHER>,
+                   dim3(tail, TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::BM *
+                                  TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::BN / 256),
+                   dim3(256), 0, s, a);
+    } else if (x3) {
+      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16X3>,
+                   dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), dim3(256), 0, s, a);
+    } else {
+      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16>,
+                   dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), dim3(256), 0, s, a);
+    }
+    mark(2, 1, s);
+    return launch_check("tc_tail_reduce");
+  }
+  if (p->ksplit == 1) return TCCG_OK;
+  dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
+  mark(2, 0, s);
+  launch_after(true, p, simt_reduce_kernel<float>, g2, dim3(256), 0, s, (const float*)a.partial,
+               (int)p->ksplit, (int64_t)p->M, (int64_t)p->N, (int64_t)p->M, (int64_t)p->N, Cout, c_m,
+               c_n, alpha, beta);
+  mark(2, 1, s);
+  return launch_check("tc_reduce");
+}
+
 static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cout,
                   const int64_t* c_m, const int64_t* c_n, float alpha, float beta, char* ws,
                   cudaStream_t s) {
   const bool x3 = p->prec == TCCG_PREC_BF16X3;
+  TcArgs a = tc_args(p, Cout, c_m, c_n, alpha, beta, ws);
+  if (p->gather) {
+    using Cfg = TcCfgT<TC_BF16X3, TC_LOAD_GATHER>;
+    set_gather(a, p, GA, GB);
+    take_injection(a);
+    CUtensorMap none;
+    memset(&none, 0, sizeof(none));
+    mark(1, 0, s);
+    launch_after(false, p, gett_tc_kernel<TC_BF16X3, TC_LOAD_GATHER>, dim3((unsigned)p->grid),
+                 dim3(Cfg::NUM_THREADS), Cfg::SMEM_BYTES, s, none, none, a);
+    mark(1, 1, s);
+    const int rc = launch_check("gett_tc (gather)");
+    if (rc) return rc;
+    return tc_reduce<TC_LOAD_GATHER>(p, a, Cout, c_m, c_n, alpha, beta, s);
+  }
   void* Ap = ws + p->off_a;
   void* Bp = ws + p->off_b;
   PackArgs pa;
@@ -1234,28 +1395,6 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   if (rc) return rc;
   rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, pair ? p->bn / 2 : p->bn);
   if (rc) return rc;
-  TcArgs a{};
-  a.M = (int32_t)p->M;
-  a.N = (int32_t)p->N;
-  a.K = (int32_t)p->K;
-  a.num_kb = p->num_kb;
-  a.tiles_m = p->tiles_m;
-  a.tiles_n = p->tiles_n;
-  a.raster = p->raster;
-  a.chunk_kb = p->chunk_kb;
-  a.C = Cout;
-  a.c_m_off = c_m;
-  a.c_n_off = c_n;
-  a.alpha = alpha;
-  a.beta = beta;
-  a.status = p->d_status;
-  a.ksplit = p->ksplit;
-  a.kb_per_split = p->kb_per_split;
-  a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(ws + p->off_part) : nullptr;
-  a.full_tiles = p->full_tiles;
-  a.tail_split = p->tail_split;
-  a.tail_kb = p->tail_kb;
-  a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
   if (!pair) take_injection(a);
   mark(1, 0, s);
   if (pair && x3)
@@ -1273,26 +1412,7 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   mark(1, 1, s);
   rc = launch_check("gett_tc");
   if (rc) return rc;
-  if (p->tail_split > 1) {
-    const unsigned tail = (unsigned)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles);
-    mark(2, 0, s);
-    if (x3)
-      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16X3>,
-                   dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), dim3(256), 0, s, a);
-    else
-      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16>,
-                   dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), dim3(256), 0, s, a);
-    mark(2, 1, s);
-    return launch_check("tc_tail_reduce");
-  }
-  if (p->ksplit == 1) return rc;
-  dim3 g2((unsigned)cdiv(p->M, 256), (unsigned)std::min<int64_t>(p->N, 65535));
-  mark(2, 0, s);
-  launch_after(true, p, simt_reduce_kernel<float>, g2, dim3(256), 0, s, (const float*)a.partial,
-               (int)p->ksplit, (int64_t)p->M, (int64_t)p->N, (int64_t)p->M, (int64_t)p->N, Cout, c_m,
-               c_n, alpha, beta);
-  mark(2, 1, s);
-  return launch_check("tc_reduce");
+  return tc_reduce<TC_LOAD_TMA>(p, a, Cout, c_m, c_n, alpha, beta, s);
 }
 
 static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s);
@@ -1564,10 +1684,14 @@ struct tccg_group {
   // over its items. On the 256-item batched workload 4 GiB waves take the
   // time of one wave (22.0 vs 22.1 ms BF16x3) with 4.0 instead of 12.8 GiB of
   // workspace; 512 MiB waves cost 8 % more time (more, shorter launches).
+  // The tensor-core items of a wave form two lanes: packed operands with TMA
+  // loads (tc0, n_tc) and the gather loader (tcg0, n_tcg), adjacent in d_tc.
   struct Wave {
     std::vector<size_t> items;  // plan indices
-    int32_t simt0 = 0, n_simt = 0, tc0 = 0, n_tc = 0, red0 = 0, n_red = 0;
-    int64_t simt_tiles = 0, tc_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0, red_ctas = 0;
+    int32_t simt0 = 0, n_simt = 0, tc0 = 0, n_tc = 0, tcg0 = 0, n_tcg = 0, red0 = 0, n_red = 0;
+    int32_t tcj0 = 0;  // first pack job of the TMA lane (two per item)
+    int64_t simt_tiles = 0, tc_tiles = 0, tcg_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0,
+            red_ctas = 0;
   };
   std::vector<Wave> waves;
   bool bound = false;
@@ -1636,10 +1760,12 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     g->ws_bytes = std::max(g->ws_bytes, ws);
     if (simt_path(p)) {
       wv.simt_tiles += (p->Mp / p->simt_bm) * (p->Np / p->simt_bn) * p->ksplit;
+    } else if (p->gather) {
+      wv.tcg_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     } else {
       wv.tc_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
-    if (wv.simt_tiles > INT32_MAX || wv.tc_tiles > INT32_MAX) {
+    if (wv.simt_tiles > INT32_MAX || wv.tc_tiles > INT32_MAX || wv.tcg_tiles > INT32_MAX) {
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
     }
@@ -1736,10 +1862,11 @@ static int64_t reduce_ctas(const ReduceJob<T>& j) {
 // index order (round robin in the persistent tensor-core kernel, launch order
 // in the CUDA-core one), so the longest tiles start first and the short ones
 // fill in behind them.
-static std::vector<size_t> by_tile_cost(const tccg_group* g, const tccg_group::Wave& wv, bool simt) {
+static std::vector<size_t> by_tile_cost(const tccg_group* g, const tccg_group::Wave& wv, bool simt,
+                                        bool gather = false) {
   std::vector<size_t> idx;
   for (size_t i : wv.items)
-    if (simt_path(g->plans[i]) == simt) idx.push_back(i);
+    if (simt_path(g->plans[i]) == simt && (simt || g->plans[i]->gather == gather)) idx.push_back(i);
   auto cost = [&](size_t i) {
     const tccg_plan* p = g->plans[i];
     return simt ? (int64_t)p->ktiles_per_split : (int64_t)p->kb_per_split;
@@ -1816,57 +1943,55 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
                    void* const* C, const double* alpha, const double* beta, char* ws,
                    std::vector<TcGroupItem>& items, std::vector<PackJob>& jobs,
                    std::vector<ReduceJob<float>>& red, int64_t& rctas) {
-  wv.tc0 = (int32_t)items.size();
-  int64_t tile = 0, pctas = 0;
-  for (size_t i : by_tile_cost(g, wv, false)) {
-    const tccg_plan* p = g->plans[i];
-    char* w = ws + g->ws_off[i];
-    const void* GA = p->d.swap_ab ? B[i] : A[i];
-    const void* GB = p->d.swap_ab ? A[i] : B[i];
-    const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
-    const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
-    add_pack_jobs(jobs, pctas,
-                  with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover,
-                                                w + p->off_a, p->Kc, p->read_k_fast_a),
-                                        p->t_a_vsrc, p->t_a_vdst), p->ks_a, p->kb_a, p->kbq_a, es),
-                  with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover,
-                                                w + p->off_b, p->Kc, p->read_k_fast_b),
-                                        p->t_b_vsrc, p->t_b_vdst), p->ks_b, p->kb_b, p->kbq_b, es),
-                  pack_k_tile<PACK_K_BF16>(), true);
-    TcGroupItem it;
-    memset(&it, 0, sizeof(it));
-    int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, 128);
-    if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, p->bn);
-    if (rc) return rc;
-    TcArgs& a = it.args;
-    a.M = (int32_t)p->M;
-    a.N = (int32_t)p->N;
-    a.K = (int32_t)p->K;
-    a.num_kb = p->num_kb;
-    a.tiles_m = p->tiles_m;
-    a.tiles_n = p->tiles_n;
-    a.raster = p->raster;
-    a.chunk_kb = p->chunk_kb;
-    a.C = static_cast<float*>(C[i]);
-    a.c_m_off = p->t_c_m;
-    a.c_n_off = p->t_c_n;
-    a.alpha = (float)alpha[i];
-    a.beta = (float)beta[i];
-    a.status = p->d_status;
-    a.ksplit = p->ksplit;
-    a.kb_per_split = p->kb_per_split;
-    a.partial = p->ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
-    it.tile_begin = tile;
-    tile += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
-    items.push_back(it);
-    if (p->ksplit > 1) {
-      red.push_back(reduce_job_for<float>(a.partial, p->ksplit, p->M, p->N, p, C[i], alpha[i],
-                                          beta[i], rctas));
-      rctas += reduce_ctas(red.back());
+  int64_t pctas = 0;
+  wv.tcj0 = (int32_t)jobs.size();
+  for (int lane = 0; lane < 2; ++lane) {  // 0: packed operands + TMA, 1: gather loader
+    const bool gather = lane == 1;
+    (gather ? wv.tcg0 : wv.tc0) = (int32_t)items.size();
+    int64_t tile = 0;
+    for (size_t i : by_tile_cost(g, wv, false, gather)) {
+      const tccg_plan* p = g->plans[i];
+      char* w = ws + g->ws_off[i];
+      const void* GA = p->d.swap_ab ? B[i] : A[i];
+      const void* GB = p->d.swap_ab ? A[i] : B[i];
+      TcGroupItem it;
+      memset(&it, 0, sizeof(it));
+      it.args = tc_args(p, static_cast<float*>(C[i]), p->t_c_m, p->t_c_n, (float)alpha[i],
+                        (float)beta[i], w);
+      // grouped tiles run over all of K or their k-split slices, never a tail split
+      it.args.full_tiles = 0;
+      it.args.tail_split = 1;
+      it.args.tail_kb = 0;
+      it.args.tail_partial = nullptr;
+      if (gather) {
+        set_gather(it.args, p, GA, GB);
+      } else {
+        const int64_t kcover = p->prec == TCCG_PREC_BF16X3 ? round_up(p->K, 32) : p->Kc;
+        const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
+        add_pack_jobs(jobs, pctas,
+                      with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover,
+                                                    w + p->off_a, p->Kc, p->read_k_fast_a),
+                                            p->t_a_vsrc, p->t_a_vdst), p->ks_a, p->kb_a, p->kbq_a, es),
+                      with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover,
+                                                    w + p->off_b, p->Kc, p->read_k_fast_b),
+                                            p->t_b_vsrc, p->t_b_vdst), p->ks_b, p->kb_b, p->kbq_b, es),
+                      pack_k_tile<PACK_K_BF16>(), true);
+        int rc = encode_kmajor(&it.tmA, w + p->off_a, p->M, p->Kc, 128);
+        if (!rc) rc = encode_kmajor(&it.tmB, w + p->off_b, p->N, p->Kc, p->bn);
+        if (rc) return rc;
+      }
+      it.tile_begin = tile;
+      tile += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
+      items.push_back(it);
+      if (p->ksplit > 1) {
+        red.push_back(reduce_job_for<float>(it.args.partial, p->ksplit, p->M, p->N, p, C[i],
+                                            alpha[i], beta[i], rctas));
+        rctas += reduce_ctas(red.back());
+      }
     }
+    (gather ? wv.n_tcg : wv.n_tc) = (int32_t)items.size() - (gather ? wv.tcg0 : wv.tc0);
   }
   if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
-  wv.n_tc = (int32_t)items.size() - wv.tc0;
   wv.tc_pack_ctas = pctas;
   return TCCG_OK;
 }
@@ -1963,8 +2088,8 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
     if ((rc = launch_check("pack_group"))) return rc;
   }
   const bool x3 = g->prec == TCCG_PREC_BF16X3;
-  const PackJob* tjobs = g->d_tc_jobs + 2 * wv.tc0;
-  const int64_t* tb = g->b_tc_jobs + 2 * wv.tc0;
+  const PackJob* tjobs = g->d_tc_jobs + wv.tcj0;
+  const int64_t* tb = g->b_tc_jobs + wv.tcj0;
   if (wv.tc_pack_ctas > 0) {
     const dim3 pg((unsigned)wv.tc_pack_ctas);
     if (x3)
@@ -1995,6 +2120,18 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
       gett_tc_group_kernel<TC_BF16><<<grid, TcCfgT<TC_BF16>::NUM_THREADS,
                                       TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, g->tc_status);
     if ((rc = launch_check("gett_tc_group"))) return rc;
+  }
+  if (wv.n_tcg > 0) {
+    using Cfg = TcCfgT<TC_BF16X3, TC_LOAD_GATHER>;
+    TcGroup tg;
+    tg.items = g->d_tc + wv.tcg0;
+    tg.tile_begin = g->b_tc_items + wv.tcg0;
+    tg.n_items = wv.n_tcg;
+    tg.total_tiles = (int32_t)wv.tcg_tiles;
+    const unsigned grid = (unsigned)std::min<int64_t>(wv.tcg_tiles, g->num_sms);
+    gett_tc_group_kernel<TC_BF16X3, TC_LOAD_GATHER><<<grid, Cfg::NUM_THREADS, Cfg::SMEM_BYTES, s>>>(
+        tg, g->tc_status);
+    if ((rc = launch_check("gett_tc_group (gather)"))) return rc;
   }
   if (wv.n_red > 0) {
     reduce_group_kernel<T><<<(unsigned)wv.red_ctas, 256, 0, s>>>(

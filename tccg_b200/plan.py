@@ -158,6 +158,7 @@ class Tuning:
     shortk: int = 0  # CUDA-core kernels, K <= 32: 0 auto, 1 kernel prefetching C, -1 never
     simt_tile: int = 0  # CUDA-core tiles: 0 auto, 1 128x128, 2 128x32, 3 32x128
     tail_split: int = 0  # tcgen05: 0 auto (k slices for a short last round), -1 never
+    load: int = 0  # tcgen05 BF16x3, FP32 operands: 0 auto, 1 packing pass + TMA, 2 gather
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -171,12 +172,13 @@ class Tuning:
         t.shortk = int(self.shortk)
         t.simt_tile = int(self.simt_tile)
         t.tail_split = int(self.tail_split)
+        t.load = int(self.load)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d" % (
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d" % (
             self.method, self.ksplit, self.raster, self.max_ctas, self.variant, self.pair,
-            self.direct, self.shortk, self.simt_tile, self.tail_split)
+            self.direct, self.shortk, self.simt_tile, self.tail_split, self.load)
 
 
 class Plan:

@@ -88,3 +88,48 @@ def test_cli_end_to_end(cuda, tmp_path):
                           capture_output=True, text=True, env=env,
                           cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     assert out2.returncode == 0 and "tuning cache hit" in out2.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spec,precision", [
+    (EXAMPLE, "fp32"),
+    # configuration 2 (beta = 1, C of 340 MB: 16 slabs of its last index d,
+    # B copied whole, C copied up and down per slab)
+    ("C[a,b,c,d] = A[a,e,b] * B[e,d,c] + C[a,b,c,d]\na=96\nb=96\nc=96\nd=96\ne=16\n", "bf16x3"),
+])
+def test_emitted_gett_with_host_buffers(cuda, tmp_path, spec, precision):
+    """TCCG's callers pass host buffers (tccg.py:910-919, 1040): the emitted
+    gett() called with numpy arrays copies them to the GPU and back (in slabs
+    when C is large) and matches the FP64 oracle; called again with device
+    pointers it gives the same C (bit for bit when no slabs are used)."""
+    import torch
+    from oracle import LoopNest, error_metrics
+    con = parse_text(spec)
+    paths = emit(con, precision, Tuning(), "s", str(tmp_path / "impl"))
+    src = open(paths["cu"]).read()
+    L = ctypes.CDLL(paths["so"])
+    L.gett.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_float] * 2
+    L.gett_last_status.restype = ctypes.c_int
+    sizes = {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices}
+    ln = LoopNest(con.C0.labels, con.A0.labels, con.B0.labels, sizes)
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal(ln.size_a, dtype=np.float32)
+    B = rng.standard_normal(ln.size_b, dtype=np.float32)
+    C0 = rng.standard_normal(ln.size_c, dtype=np.float32)
+    C = C0.copy()
+    L.gett(A.ctypes.data, B.ctypes.data, C.ctypes.data, con.alpha, con.beta)
+    assert L.gett_last_status() == 0
+    big = ln.size_c * 4 >= (256 << 20)
+    assert ("#define NSLAB 16" in src) == big
+    lins = np.unique(np.linspace(0, ln.size_c - 1, 4096).astype(np.int64))
+    ref = ln.sample64(A, B, C0 if con.beta != 0 else None, con.alpha, con.beta, lins)
+    tol = 1e-5 if precision == "bf16x3" else 1e-6
+    assert error_metrics(C[lins], ref)["normwise"] <= tol
+    dA, dB, dC = (torch.from_numpy(x).cuda() for x in (A, B, C0))
+    torch.cuda.synchronize()
+    L.gett(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), con.alpha, con.beta)
+    assert L.gett_last_status() == 0
+    if not big:  # the same plan on the same data
+        assert np.array_equal(dC.cpu().numpy(), C)
+    else:  # slab plans and the whole-tensor plan may tile differently
+        assert error_metrics(dC.cpu().numpy()[lins], ref)["normwise"] <= tol
