@@ -178,6 +178,27 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def host_operand(x):
+    """The CPU baseline's copy of an operand: a fresh 64-byte aligned array
+    written by this thread (as TCCG's harness allocates with posix_memalign
+    and initialises serially, tccg.py:910-919, 957-971), so that both bench
+    arms time the loop nest on memory placed the same way -- on the wide
+    strides of this contraction the loop nest is bound by address
+    translation, and pinned or torch-allocated buffers measured up to 4x
+    apart on the same slab."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import aligned_copy  # noqa: E402
+    return aligned_copy(x)
+
+
+def thp_mode():
+    try:
+        with open("/sys/kernel/mm/transparent_hugepage/enabled") as f:
+            return f.read().strip()
+    except OSError:
+        return None
+
+
 def set_omp_threads(n: int) -> dict:
     """Sets the thread count of the process's OpenMP runtime (libgomp.so.1:
     torch loads its own copy under that name first, and the oracle's and the
@@ -198,6 +219,7 @@ def set_omp_threads(n: int) -> dict:
         if os.environ.get(k):
             info[k] = os.environ[k]
     info["affinity_cpus"] = host_threads()
+    info["transparent_hugepage"] = thp_mode()
     return info
 
 
@@ -303,8 +325,8 @@ def run_reference(args, world, rank):
     con = parse_text(workload(args.k_extent))
     threads = host_threads()
     g = torch.Generator().manual_seed(0)
-    A = torch.randn(con.A0.num_elements(), generator=g).numpy()
-    B = torch.randn(con.B0.num_elements(), generator=g).numpy()
+    A = host_operand(torch.randn(con.A0.num_elements(), generator=g).numpy())
+    B = host_operand(torch.randn(con.B0.num_elements(), generator=g).numpy())
     vals = []
     info = None
     per_step = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
@@ -468,12 +490,12 @@ def run_ours(args, world, rank, local):
         # the port times the sample and checks the GPU result against FP64;
         # the reference's own emitted loop nest, where it was built, is the
         # reported baseline (the port's figure stays beside it)
-        cpu = cpu_loopnest_sample(con, Ah.numpy(), Bh.numpy(), seconds=args.cpu_seconds,
-                                  gpu_C=Cx3)
+        An, Bn = host_operand(Ah.numpy()), host_operand(Bh.numpy())
+        cpu = cpu_loopnest_sample(con, An, Bn, seconds=args.cpu_seconds, gpu_C=Cx3)
         ref = None
         if args.k_extent == 32:
-            ref = reference_impl_sample(con, Ah.numpy(), Bh.numpy(), args.cpu_seconds,
-                                        host_threads())
+            ref = reference_impl_sample(con, An, Bn, args.cpu_seconds, host_threads())
+        del An, Bn
         if ref is not None:
             ref["check_vs_fp64_oracle"] = cpu.pop("check_vs_fp64_oracle", None)
             ref["port"] = {"value": cpu["value"], "sample": cpu["sample"]}
