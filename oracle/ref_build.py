@@ -33,7 +33,11 @@ from typing import List
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(_HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# The reference checkout: $TCCG_REFERENCE_ROOT, else a directory named
+# "reference" beside the repository; where neither exists the reference-built
+# checkers are skipped (the committed fixtures and prebuilt files are used).
+DEFAULT_REF = os.environ.get("TCCG_REFERENCE_ROOT") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "reference")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 

@@ -30,7 +30,11 @@ import sys
 import tokenize
 from typing import Dict
 
-DEFAULT_REF = "/root/reference"
+# The reference checkout: $TCCG_REFERENCE_ROOT, else a directory named
+# "reference" beside the repository; where neither exists the reference-built
+# checkers are skipped (the committed fixtures and prebuilt files are used).
+DEFAULT_REF = os.environ.get("TCCG_REFERENCE_ROOT") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "reference")
 _HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(_HERE, "_ref", "py3")
 

@@ -15,12 +15,17 @@ flat one. The output C has the reversed shape of C's indices.
 """
 from __future__ import annotations
 
+from collections import OrderedDict
 from typing import Dict, Tuple
 
 from .plan import Plan
 from .spec import Contraction, make_contraction
 
-_PLANS: Dict[Tuple, Plan] = {}
+# Plans shared across contraction objects with the same text, least recently
+# used first; at most _MAX_PLANS are kept (each holds its device offset
+# tables), the oldest is dropped past that.
+_MAX_PLANS = 256
+_PLANS: "OrderedDict[Tuple, Plan]" = OrderedDict()
 
 
 def _sizes(con: Contraction) -> Dict[str, int]:
@@ -57,6 +62,10 @@ def _plan(con: Contraction, precision: str, dtype: str, role: str) -> Plan:
     if p is None:
         p = Plan(con, precision=precision, dtype=dtype)
         _PLANS[key] = p
+        while len(_PLANS) > _MAX_PLANS:
+            _PLANS.popitem(last=False)
+    else:
+        _PLANS.move_to_end(key)
     local[(precision, dtype, role)] = p
     return p
 
