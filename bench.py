@@ -736,6 +736,24 @@ def run_suite(args):
     return out
 
 
+def _kernel_mix(grp):
+    """How many items of a group run on each kernel family / loader."""
+    mix = {}
+    for p in grp.plans:
+        d = p.describe()
+        k = ("cuda_core" if "simt" in d else "tcgen05_gather" if "gather" in d else "tcgen05_packed")
+        mix[k] = mix.get(k, 0) + 1
+    return mix
+
+
+def _tuning_mix(grp):
+    mix = {}
+    for p in grp.plans:
+        k = p.tuning.key()
+        mix[k] = mix.get(k, 0) + 1
+    return dict(sorted(mix.items(), key=lambda kv: -kv[1]))
+
+
 def _suite_cfg5(out, gen, flush, dev):
     """Configuration 5: 256 mixed contractions, one grouped launch in a CUDA
     graph, against one plan run (pack + GETT launch) per contraction."""
@@ -757,7 +775,25 @@ def _suite_cfg5(out, gen, flush, dev):
         res[prec] = {"graph_ms": t_graph, "graph_tflops": tot / (t_graph * 1e-3) / 1e12,
                      "per_item_launches_ms": t_items,
                      "per_item_tflops": tot / (t_items * 1e-3) / 1e12,
-                     "workspace_gib": grp.workspace_bytes / 2 ** 30}
+                     "workspace_gib": grp.workspace_bytes / 2 ** 30,
+                     "kernels": _kernel_mix(grp)}
+        del grp
+        torch.cuda.empty_cache()
+    if os.environ.get("TCCG_SUITE_AUTOTUNE", "1") != "0":
+        # every item tuned (GETT, no tail split) from a fresh cache, then the
+        # grouped run of the tuned plans
+        import tempfile
+        db = os.path.join(tempfile.mkdtemp(), "cfg5.db")
+        t0 = time.perf_counter()
+        grp = Group(items, "bf16x3", autotune=True, max_implementations=6, cache_path=db)
+        t_tune = time.perf_counter() - t0
+        grp.bind(As, Bs, Cs)
+        grp.capture()
+        t_graph = _time(grp.replay, 3, 10, flush)
+        res["bf16x3_autotuned"] = {"graph_ms": t_graph, "graph_tflops": tot / (t_graph * 1e-3) / 1e12,
+                                   "tuning_s": t_tune, "candidates_per_item": 6,
+                                   "kernels": _kernel_mix(grp),
+                                   "tunings": _tuning_mix(grp)}
         del grp
         torch.cuda.empty_cache()
     out["cfg5"] = res

@@ -104,7 +104,9 @@ typedef struct tccg_tuning {
   int32_t ksplit;      /* k-split factor: 0 = automatic (split K over CTAs when the C tiles
                           cannot fill the GPU), 1 = none, > 1 = that many slices
                           (the CTA-pair kernel never splits) */
-  int32_t raster;      /* tile-raster group size of the persistent tcgen05 kernel (0 = default) */
+  int32_t raster;      /* tile order of the persistent tcgen05 kernel (TCCG's two loop orders,
+                          tccg/gett.py:52-55): > 0 = groups of that many tile rows, m fastest;
+                          < 0 = groups of -raster tile columns, n fastest; 0 = default (8) */
   int32_t max_ctas;    /* persistent grid size cap (0 = one CTA per SM) */
   int32_t pair;        /* tensor-core precisions: 1 = CTA-pair kernel (cta_group::2, 256-row tiles) */
   int32_t direct;      /* CUDA-core kernels: 0 = automatic (no packing pass when K <= 256 and the

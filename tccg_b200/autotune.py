@@ -5,14 +5,28 @@ the best ``--maxImplementations`` of them with make, times them in a
 generated harness and keeps the results in SQLite keyed on the contraction,
 the sizes, the CPU and the types (sql_util.py:206-306; lookup tccg.py:192-221).
 
-Here the candidates are kernel choices of one native plan -- method (GETT or
-TTGT), k-split for the SIMT kernels, CUDA-core or tensor-core kernel for the
-BF16 precisions, tile-raster group and K-chunk length for the tcgen05
-kernels -- ordered by a simple model (defaults first), timed on
-the device with CUDA events (minimum over repetitions, L2 flushed in between
-like TCCG's trashCache, tccg.py:725-737), and the winner is stored in SQLite
-keyed on (contraction, extents, precision, operand type, beta != 0, GPU name,
-SM count, library version). A cache hit skips the search.
+Here the candidates are kernel choices of one native plan, TCCG's search
+dimensions restated for the GPU:
+
+* method: GETT or TTGT (TCCG also weighs TTGT and LoG, tccg.py:188-430);
+* loop order (TCCG's two GEMM variants, panel-matrix and matrix-panel,
+  gett.py:52-55): the persistent tile order, groups of tile rows (raster > 0)
+  or of tile columns (raster < 0), and the group size;
+* blockings (TCCG's mc/nc/kc, gett.py:1023-1062): the tcgen05 tile shape
+  through the operand loader (128x192 tiles after a packing pass, or 128x128
+  tiles gathered from the caller's tensors), the K-chunk of the split-BF16x3
+  accumulation, k-split (CUDA cores) and the CUDA-core tile shape;
+* mode orders of the GETT view (the index permutations TCCG searches with
+  its index splits, gett.py:1063-1110): the N order (C's, or GB's unit-stride
+  mode first) and the K order (GA's or GB's), where they change the view;
+* kernel family for the BF16 precisions (tensor cores or CUDA cores).
+
+They are ordered by a simple model (defaults first, then one dimension
+varied at a time), timed on the device with CUDA events (minimum over
+repetitions, L2 flushed in between like TCCG's trashCache,
+tccg.py:725-737), and the winner is stored in SQLite keyed on (contraction,
+extents, precision, operand type, beta != 0, GPU name, SM count, library
+version). A cache hit skips the search.
 """
 from __future__ import annotations
 
@@ -27,7 +41,7 @@ from .spec import Contraction
 
 # Part of every cache key: cached winners measured on older kernels (or
 # without the tuning fields a newer build searches) are not reused.
-CODE_VERSION = "tccg_b200-0.2"
+CODE_VERSION = "tccg_b200-0.3"
 
 
 def default_db_path() -> str:
@@ -92,11 +106,29 @@ def tuning_key(con: Contraction, precision: str, dtype: str, gpu: str) -> str:
                      gpu, CODE_VERSION])
 
 
-def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_sms: int = 148
-               ) -> List[Tuning]:
+def order_variants(con: Contraction):
+    """(n_order, k_order) pairs whose GETT views differ, the heuristic (0, 0)
+    first."""
+    from .plan import gett_view
+    seen, out = set(), []
+    for no, ko in ((0, 0), (1, 0), (2, 0), (0, 1), (0, 2)):
+        v = gett_view(con, n_order=no, k_order=ko)
+        key = (tuple(v.m), tuple(v.n), tuple(v.k))
+        if key not in seen:
+            seen.add(key)
+            out.append((no, ko))
+    return out
+
+
+def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_sms: int = 148,
+               dtype: str = "f32", grouped: bool = False) -> List[Tuning]:
     """Candidate tunings, the model's favourite first: the defaults, then
-    variations that matter for this shape."""
+    variations that matter for this shape. ``grouped``: for an item of a
+    grouped launch (GETT, no tcgen05 tail split)."""
     M, N, K = con.sizeM, con.sizeN, max(1, con.sizeK)
+    if grouped:
+        methods = ("gett",)
+    orders = order_variants(con)
     out: List[Tuning] = []
     for method in methods:
         if precision in ("fp32", "fp64"):
@@ -118,25 +150,64 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             # FP32: each CUDA-core tile shape (square, small N, small M)
             if precision == "fp32":
                 out += [Tuning(method=method, simt_tile=t) for t in (1, 2, 3)]
+            out += [Tuning(method=method, n_order=no, k_order=ko) for no, ko in orders[1:]]
         else:
             # variant > 0 forces the tensor cores (BF16X3: k-blocks per
             # accumulation chunk), < 0 the CUDA cores; the library's own
-            # choice (variant 0) goes first
-            rasters = [8, 4, 16]
+            # choice (variant 0) goes first, then each kernel family: the
+            # CUDA cores and, for BF16x3 with FP32 operands, both tcgen05
+            # loaders (128x192 tiles packed, 128x128 tiles gathered); then
+            # accumulation chunks, tile orders and mode orders.
+            loads = [1, 2] if precision == "bf16x3" and dtype == "f32" and method == "gett" else [0]
             chunks = [16, 32, 8] if precision == "bf16x3" else [1]
-            tc = [Tuning(method=method, raster=r, variant=c) for r in rasters for c in chunks]
-            simt = [Tuning(method=method, variant=-1)]
+            first = [Tuning(method=method)]
+            if len(loads) > 1:
+                first += [Tuning(method=method, load=ld) for ld in loads]
+            else:
+                first.append(Tuning(method=method, variant=chunks[0]))  # tensor cores
+            first.append(Tuning(method=method, variant=-1))
+            more = []
+            for ld in loads:
+                more += [Tuning(method=method, load=ld, raster=r) for r in (-8, 4, 16, -2)]
+                more += [Tuning(method=method, load=ld, variant=c) for c in chunks[1:]]
+            more += [Tuning(method=method, n_order=no, k_order=ko) for no, ko in orders[1:]]
             if K <= 32:
-                simt += [Tuning(method=method, variant=-1, shortk=1),
+                more += [Tuning(method=method, variant=-1, shortk=1),
                          Tuning(method=method, variant=-1, shortk=-1)]
-            # the tcgen05 tail split off (it is on where the model expects a gain)
-            tc.append(Tuning(method=method, tail_split=-1))
-            out += [Tuning(method=method)] + ((simt + tc) if K <= 128 else (tc + simt))
-    return out
+            if not grouped:
+                # the tcgen05 tail split off (it is on where the model expects a gain)
+                more.append(Tuning(method=method, tail_split=-1))
+            out += first + more
+    if grouped:
+        for t in out:
+            t.tail_split = -1
+    # drop repeats, keeping the first of each
+    seen, uniq = set(), []
+    for t in out:
+        if t.key() not in seen:
+            seen.add(t.key())
+            uniq.append(t)
+    return uniq
 
 
 def _flush_l2(buf):
     buf.add_(1.0)
+
+
+def _inputs(con: Contraction, dtype: str, c_dtype: str):
+    """Seeded operands of ``con`` on the current device, shared by all the
+    candidates of one search."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}
+    g = torch.Generator(device=dev).manual_seed(0)
+    A = torch.randn(con.A0.num_elements(), generator=g, device=dev).to(tdt[dtype])
+    B = torch.randn(con.B0.num_elements(), generator=g, device=dev).to(tdt[dtype])
+    C = torch.randn(con.C0.num_elements(), generator=g, device=dev).to(tdt[c_dtype])
+    return A, B, C
+
+
+_TRASH = {}
 
 
 def measure(plan: Plan, reps: int = 5, inputs=None) -> float:
@@ -154,7 +225,9 @@ def measure(plan: Plan, reps: int = 5, inputs=None) -> float:
     else:
         A, B, C = inputs
     ws = torch.empty(max(plan.workspace_bytes, 1), dtype=torch.uint8, device=dev)
-    trash = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    trash = _TRASH.get(dev)
+    if trash is None:
+        trash = _TRASH[dev] = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     plan.run(A, B, C, workspace=ws)  # warm-up
     torch.cuda.synchronize()
     best = float("inf")
@@ -174,31 +247,39 @@ def measure(plan: Plan, reps: int = 5, inputs=None) -> float:
 def autotune(con: Contraction, precision: str, max_implementations: int = 16,
              cache_path: Optional[str] = None, dtype: Optional[str] = None,
              ignore_cache: bool = False, methods=("gett", "ttgt"), verbose: bool = False,
-             max_workspace_gb: Optional[float] = None) -> Tuning:
+             max_workspace_gb: Optional[float] = None, grouped: bool = False,
+             db: Optional[TuningDB] = None, stats: Optional[dict] = None) -> Tuning:
     """Best tuning for ``con``: from the cache, else by timing up to
-    ``max_implementations`` candidates (-1 = all)."""
+    ``max_implementations`` candidates (-1 = all). ``grouped``: tune an item
+    of a grouped launch (GETT, no tail split; cached under its own key).
+    ``stats`` (optional dict) counts cache "hits" and "tuned" contractions."""
     import torch
     from .plan import operand_dtype
     dtype = dtype or operand_dtype(precision)
-    db = TuningDB(cache_path)
-    key = tuning_key(con, precision, dtype, gpu_signature())
+    db = db or TuningDB(cache_path)
+    key = tuning_key(con, precision, dtype, gpu_signature()) + ("|grouped" if grouped else "")
     if not ignore_cache:
         hit = db.lookup(key)
         if hit is not None:
             if verbose:
                 print("[tccg_b200] tuning cache hit: %s (%.2f GFLOPS)" % (hit[0].key(), hit[1]))
+            if stats is not None:
+                stats["hits"] = stats.get("hits", 0) + 1
             return hit[0]
+    if stats is not None:
+        stats["tuned"] = stats.get("tuned", 0) + 1
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    cands = candidates(con, precision, methods, sms)
+    cands = candidates(con, precision, methods, sms, dtype=dtype, grouped=grouped)
     if max_implementations >= 0:
         cands = cands[:max(1, max_implementations)]
     best, best_ms = None, float("inf")
     flops = con.flop_count()
+    inputs = _inputs(con, dtype, "f64" if precision == "fp64" else "f32")
     for t in cands:
         p = Plan(con, precision=precision, tuning=t, dtype=dtype)
         if max_workspace_gb is not None and p.workspace_bytes > max_workspace_gb * 2 ** 30:
             continue
-        ms = measure(p)
+        ms = measure(p, inputs=inputs)
         gf = flops / (ms * 1e-3) / 1e9
         db.record(key, t, ms, gf)
         if verbose:

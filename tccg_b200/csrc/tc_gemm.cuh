@@ -154,7 +154,24 @@ struct TcGroup {
   int32_t total_tiles;
 };
 
+// Tile order of the persistent grid (TCCG's two GEMM loop orders,
+// tccg/gett.py:52-55): raster > 0 walks groups of `raster` tile rows (m),
+// m fastest inside a group and the group's columns after each other -- the
+// group's A rows stay in L2 while B streams (matrix-panel); raster < 0 walks
+// groups of -raster tile columns (n), n fastest -- B's rows stay (panel-matrix).
 __device__ __forceinline__ void tile_coords(int tile, const TcArgs& a, int& tm, int& tn) {
+  if (a.raster < 0) {
+    const int R = -a.raster;
+    const int group = R * a.tiles_m;
+    const int gid = tile / group;
+    const int first_n = gid * R;
+    int gn = a.tiles_n - first_n;
+    if (gn > R) gn = R;
+    const int r = tile - gid * group;
+    tn = first_n + r % gn;
+    tm = r / gn;
+    return;
+  }
   const int group = a.raster * a.tiles_n;
   const int gid = tile / group;
   const int first_m = gid * a.raster;

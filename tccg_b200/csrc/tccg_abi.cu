@@ -697,7 +697,9 @@ static int plan_layout(tccg_plan* p) {
       p->bn = x3 ? TcCfgT<TC_BF16X3>::BN : TcCfgT<TC_BF16>::BN;
     p->tiles_m = (int32_t)cdiv(p->M, pair ? 256 : 128);
     p->tiles_n = (int32_t)cdiv(p->N, p->bn);
-    p->raster = p->tune.raster > 0 ? p->tune.raster : 8;
+    // tile order: groups of `raster` tile rows (> 0, default 8) or of
+    // -raster tile columns (< 0), the two GEMM loop orders
+    p->raster = p->tune.raster != 0 ? p->tune.raster : 8;
     int64_t tiles = (int64_t)p->tiles_m * p->tiles_n;
     int ctas = p->tune.max_ctas > 0 ? std::min(p->tune.max_ctas, p->num_sms) : p->num_sms;
     // one CTA per SM; a slice is at least one accumulation chunk (BF16X3) or

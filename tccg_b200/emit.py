@@ -41,7 +41,7 @@ def _desc_c(d) -> str:
                 _arr(d.c_n_stride, d.nn)))
 
 
-def host_slabs(con: Contraction, elem_bytes: int):
+def host_slabs(con: Contraction, elem_bytes: int, tuning: Tuning = None):
     """Slabs of C's last index for the host-buffer path: 16 (at most the
     extent) when C holds >= 256 MiB, else one. Per slab: its descriptor (the
     full tensors' strides), element offsets into A, B, C and element counts
@@ -56,13 +56,13 @@ def host_slabs(con: Contraction, elem_bytes: int):
     out = []
     for r in range(n):
         if n == 1:
-            d = native_desc(gett_view(con))
+            d = native_desc(_view(con, tuning))
             out.append((d, (0, 0, 0), (con.A0.num_elements(), con.B0.num_elements(),
                                        con.C0.num_elements())))
             continue
         sh = shard(con, r, n, label)
         sc = sh.contraction
-        d = native_desc(gett_view(sc, strides=sh.strides))
+        d = native_desc(_view(sc, tuning, sh.strides))
         out.append((d, (sh.offsets["A"], sh.offsets["B"], sh.offsets["C"]),
                     (sc.A0.num_elements(), sc.B0.num_elements(), sc.C0.num_elements())))
     if n == 1:
@@ -70,10 +70,16 @@ def host_slabs(con: Contraction, elem_bytes: int):
     return out, per
 
 
+def _view(con: Contraction, tuning: Tuning = None, strides=None):
+    """GETT view with the tuning's mode orders."""
+    t = tuning or Tuning()
+    return gett_view(con, strides, n_order=t.n_order, k_order=t.k_order)
+
+
 def source(con: Contraction, precision: str, tuning: Tuning, float_type: str) -> str:
-    d = native_desc(gett_view(con))
+    d = native_desc(_view(con, tuning))
     T = "double" if float_type == "d" else "float"
-    slabs, per = host_slabs(con, 8 if float_type == "d" else 4)
+    slabs, per = host_slabs(con, 8 if float_type == "d" else 4, tuning)
     slab_desc = ",\n".join(_desc_c(sd) for sd, _, _ in slabs)
     slab_off = ", ".join("{%d, %d, %d}" % o for _, o, _ in slabs)
     slab_len = ", ".join("{%d, %d, %d}" % l for _, _, l in slabs)

@@ -25,10 +25,27 @@ from .spec import Contraction
 
 
 class Group:
+    """``autotune=True`` picks each item's kernels with the autotuner: its
+    tuning comes from the SQLite cache (``cache_path``, default as
+    ``autotune``), and items that miss are tuned on the device (up to
+    ``max_implementations`` candidates each, GETT without the tail split, as
+    grouped kernels run them) and stored. ``tune_stats`` then counts cache
+    hits and tuned items."""
+
     def __init__(self, contractions: Sequence[Contraction], precision: str = "bf16x3",
-                 tunings: Optional[Sequence[Tuning]] = None, dtype: Optional[str] = None):
+                 tunings: Optional[Sequence[Tuning]] = None, dtype: Optional[str] = None,
+                 autotune: bool = False, max_implementations: int = 8,
+                 cache_path: Optional[str] = None):
         self.contractions = list(contractions)
         self.precision = precision
+        self.tune_stats = {}
+        if autotune:
+            if tunings is not None:
+                raise ValueError("give tunings or autotune=True, not both")
+            from .autotune import TuningDB, autotune as _autotune
+            db = TuningDB(cache_path)
+            tunings = [_autotune(c, precision, max_implementations, dtype=dtype, grouped=True,
+                                 db=db, stats=self.tune_stats) for c in self.contractions]
         # the grouped kernels do not run the tcgen05 tail split (the other
         # items' tiles fill the persistent grid's rounds anyway): plans made
         # without it, so that grouped and per-item runs compute the same sums

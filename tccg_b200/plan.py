@@ -54,9 +54,14 @@ def _prod(it) -> int:
     return p
 
 
-def gett_view(con: Contraction, strides: Optional[dict] = None) -> GettView:
+def gett_view(con: Contraction, strides: Optional[dict] = None, n_order: int = 0,
+              k_order: int = 0) -> GettView:
     """GETT view of ``con``. ``strides`` may override the dense column-major
-    strides: {'A': {label: stride}, 'B': ..., 'C': ...} (elements)."""
+    strides: {'A': {label: stride}, 'B': ..., 'C': ...} (elements).
+
+    Mode orders (the autotuner searches them; 0 = the heuristics below):
+    ``n_order`` 1 = N modes in C's order, 2 = GB's unit-stride N mode first;
+    ``k_order`` 1 = K modes in GA's order, 2 = in GB's order."""
     con.validate()
     A, B, C = con.A, con.B, con.C
     swap = not A.has(C.indices[0].label)
@@ -81,7 +86,7 @@ def gett_view(con: Contraction, strides: Optional[dict] = None) -> GettView:
     nb = [l for l, e in n if e > 1]
     K = _prod(i.size for i in con.k_indices)
     M = _prod(e for _, e in m)
-    if nb and 4 * K >= M:
+    if nb and (n_order == 2 or (n_order == 0 and 4 * K >= M)):
         first = min(nb, key=lambda l: abs(st(GB, nameB, l)))
         if abs(st(GB, nameB, first)) == 1:
             n = [x for x in n if x[0] == first] + [x for x in n if x[0] != first]
@@ -91,7 +96,9 @@ def gett_view(con: Contraction, strides: Optional[dict] = None) -> GettView:
         real = [i for i in T.indices if i.size > 1]
         return real[0].label if real and real[0].label in kset else None
     la, lb = lead(GA), lead(GB)
-    if la and lb and la != lb:
+    if k_order in (1, 2):
+        owner = GA if k_order == 1 else GB
+    elif la and lb and la != lb:
         owner = GA if GA.num_elements() >= GB.num_elements() else GB
     elif la:
         owner = GA
@@ -159,6 +166,9 @@ class Tuning:
     simt_tile: int = 0  # CUDA-core tiles: 0 auto, 1 128x128, 2 128x32, 3 32x128
     tail_split: int = 0  # tcgen05: 0 auto (k slices for a short last round), -1 never
     load: int = 0  # tcgen05 BF16x3, FP32 operands: 0 auto, 1 packing pass + TMA, 2 gather
+    # mode orders of the GETT view (gett_view): 0 = heuristic
+    n_order: int = 0  # 1 = C's order, 2 = GB's unit-stride N mode first
+    k_order: int = 0  # 1 = GA's order, 2 = GB's order
 
     def native(self) -> N.Tuning:
         t = N.Tuning()
@@ -176,9 +186,10 @@ class Tuning:
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d" % (
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d/o%d%d" % (
             self.method, self.ksplit, self.raster, self.max_ctas, self.variant, self.pair,
-            self.direct, self.shortk, self.simt_tile, self.tail_split, self.load)
+            self.direct, self.shortk, self.simt_tile, self.tail_split, self.load, self.n_order,
+            self.k_order)
 
 
 class Plan:
@@ -193,7 +204,8 @@ class Plan:
         self.dtype = dtype or operand_dtype(precision)
         self.tuning = tuning or Tuning()
         # ``view``: a hand-made GETT view of ``con`` (mode orders of one's own)
-        self.view = view if view is not None else gett_view(con, strides)
+        self.view = view if view is not None else gett_view(
+            con, strides, n_order=self.tuning.n_order, k_order=self.tuning.k_order)
         self._desc = native_desc(self.view)
         self._lib = N.lib()
         h = ctypes.c_void_p()

@@ -54,8 +54,49 @@ def test_bf16_candidates_start_with_the_library_choice(precision):
         cs = candidates(_con(name), precision, methods=("gett",))
         assert cs[0] == Tuning(method="gett")
         # both kernel families and the tail split switched off are searched
-        assert any(t.variant < 0 for t in cs) and any(t.variant > 0 for t in cs)
+        assert any(t.variant < 0 for t in cs) and any(t.variant > 0 or t.load > 0 for t in cs)
         assert any(t.tail_split == -1 for t in cs)
+        # both tile orders (TCCG's two loop orders)
+        assert any(t.raster < 0 for t in cs) and any(t.raster > 0 for t in cs)
+
+
+def test_split_bf16x3_searches_both_loaders_first():
+    """BF16x3 with FP32 operands: right after the library's own choice, the
+    packed 128x192 tiles (load 1), the gathered 128x128 tiles (load 2) and
+    the CUDA cores, so that --maxImplementations=4 already compares them."""
+    for name in SHAPES:
+        cs = candidates(_con(name), "bf16x3", methods=("gett",))
+        assert [(t.load, t.variant) for t in cs[:4]] == [(0, 0), (1, 0), (2, 0), (0, -1)]
+    # not for TTGT (its GEMM reads the transposed operands) nor BF16 operands
+    cs = candidates(_con("square"), "bf16x3", methods=("ttgt",))
+    assert all(t.load == 0 for t in cs)
+    assert all(t.load == 0 for t in candidates(_con("square"), "bf16", dtype="bf16"))
+
+
+def test_mode_order_candidates_change_the_view():
+    """The N/K mode-order candidates are kept only where they give another
+    GETT view (configuration 4's pattern has two K modes led by either
+    operand)."""
+    from tccg_b200.autotune import order_variants
+    from tccg_b200.plan import gett_view
+    con = make_contraction("xyzw", "pxqw", "qzpy", dict(x=64, w=64, y=64, z=64, p=32, q=32))
+    orders = order_variants(con)
+    assert orders[0] == (0, 0) and len(orders) >= 2
+    views = {(tuple(v.m), tuple(v.n), tuple(v.k))
+             for v in (gett_view(con, n_order=a, k_order=b) for a, b in orders)}
+    assert len(views) == len(orders)
+    cs = candidates(con, "bf16x3", methods=("gett",))
+    assert {(t.n_order, t.k_order) for t in cs} >= set(orders)
+
+
+def test_grouped_candidates():
+    """Items of a grouped launch: GETT only and never the tail split."""
+    for name in SHAPES:
+        for prec in PRECISIONS:
+            cs = candidates(_con(name), prec, grouped=True)
+            assert cs and all(t.method == "gett" for t in cs)
+            if prec in ("bf16", "bf16x3"):
+                assert all(t.tail_split == -1 for t in cs)
 
 
 def test_ksplit_candidates_follow_the_tile_count():

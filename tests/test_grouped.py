@@ -117,3 +117,38 @@ def test_group_with_both_lanes_and_k_splits(cuda, precision):
         ref = ln.run(A.double().cpu().numpy(), B.double().cpu().numpy(),
                      np.zeros(ln.size_c), 1.0, 0.0)
         assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= tol, str(con)
+
+
+@pytest.mark.gpu
+def test_group_autotune_consults_the_cache_per_item(cuda, tmp_path):
+    """Group(autotune=True): the first group tunes every item (GETT, no tail
+    split) and stores the winners in the SQLite cache; a second group over
+    the same items finds every item in the cache, builds the same plans, and
+    its grouped run equals its per-item runs bit for bit."""
+    import torch
+    from tccg_b200.autotune import TuningDB, gpu_signature, tuning_key
+    from tccg_b200.grouped import Group
+    items = batched_workload(6, seed=21, fmax=2e8)
+    db = str(tmp_path / "group.db")
+    g1 = Group(items, "bf16x3", autotune=True, max_implementations=4, cache_path=db)
+    assert g1.tune_stats == {"tuned": len(items)}
+    g2 = Group(items, "bf16x3", autotune=True, max_implementations=4, cache_path=db)
+    assert g2.tune_stats == {"hits": len(items)}
+    store = TuningDB(db)
+    for con, p1, p2 in zip(items, g1.plans, g2.plans):
+        hit = store.lookup(tuning_key(con, "bf16x3", "f32", gpu_signature()) + "|grouped")
+        assert hit is not None and hit[0].tail_split == -1
+        assert p1.describe() == p2.describe()
+        assert p2.tuning.key() == hit[0].key()
+    g = torch.Generator(device="cuda").manual_seed(2)
+    As = [torch.randn(c.A0.num_elements(), generator=g, device="cuda") for c in items]
+    Bs = [torch.randn(c.B0.num_elements(), generator=g, device="cuda") for c in items]
+    Cs = [torch.zeros(c.C0.num_elements(), device="cuda") for c in items]
+    g2.bind(As, Bs, Cs)
+    g2.run()
+    torch.cuda.synchronize()
+    grouped = [c.clone() for c in Cs]
+    g2.run_per_item()
+    torch.cuda.synchronize()
+    for a, b in zip(grouped, Cs):
+        assert torch.equal(a, b)

@@ -19,6 +19,14 @@ def cdiv(a, b):
 
 
 def tile_coords(tile, tiles_m, tiles_n, raster):
+    if raster < 0:  # groups of -raster tile columns, n fastest
+        R = -raster
+        group = R * tiles_m
+        gid = tile // group
+        first_n = gid * R
+        gn = min(tiles_n - first_n, R)
+        r = tile - gid * group
+        return r // gn, first_n + r % gn
     group = raster * tiles_n
     gid = tile // group
     first_m = gid * raster
@@ -122,3 +130,17 @@ def test_random_shapes(seed):
                  ctas=rng.choice([148, 132, 100]))
         split += check(p)
     assert split > 20  # the split case is exercised, not just the plain tile order
+
+
+@pytest.mark.parametrize("raster", [8, 1, 5, 16, -8, -1, -3])
+@pytest.mark.parametrize("tiles_m,tiles_n", [(1, 1), (7, 3), (13, 40), (64, 9), (3, 100)])
+def test_tile_order_is_a_permutation(raster, tiles_m, tiles_n):
+    """Both loop orders (groups of tile rows, raster > 0; groups of tile
+    columns, raster < 0) visit every (tm, tn) of the grid exactly once, and
+    a group's tiles are consecutive in the order."""
+    seen = [tile_coords(t, tiles_m, tiles_n, raster) for t in range(tiles_m * tiles_n)]
+    assert sorted(seen) == [(m, n) for m in range(tiles_m) for n in range(tiles_n)]
+    R = abs(raster)
+    key = (lambda mn: mn[0] // R) if raster > 0 else (lambda mn: mn[1] // R)
+    groups = [key(x) for x in seen]
+    assert groups == sorted(groups)
