@@ -95,8 +95,12 @@ struct TcCfgT {
   static constexpr int STG_SLOTS = GATHER ? 3 : 0;
   static constexpr int STG_SLOT_BYTES = (BM + BN) * STG_LD * 4;
   static constexpr int ROWCACHE_BYTES = GATHER ? (BM + BN) * 8 : 0;
+  // staged C stores (TcArgs::crun): 32 rows x 16 columns per epilogue warp
+  static constexpr int EPI_LD = 33;
+  static constexpr int EPI_STG_BYTES = EPI_WARPS * 16 * EPI_LD * 4;
   static constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES +
-                                       (size_t)STG_SLOTS * STG_SLOT_BYTES + ROWCACHE_BYTES + 256;
+                                       (size_t)STG_SLOTS * STG_SLOT_BYTES + ROWCACHE_BYTES +
+                                       EPI_STG_BYTES + 256;
 };
 
 struct TcArgs {
@@ -136,6 +140,12 @@ struct TcArgs {
   const int64_t* grow[2];
   const int64_t* gk[2];
   int32_t gread[2];
+  // C layout: 0 = the epilogue's lanes store along m (C's stride-one run
+  // along m is >= 32 elements, or partial sums); e0 in [2, 31] = C's
+  // stride-one index is the first M mode, of extent e0, directly followed in
+  // C by the first N mode: stores go through shared memory in runs of e0 m
+  // by 32 / e0 columns, which are consecutive addresses of C
+  int32_t crun;
 };
 
 // Grouped launch: one entry per contraction, in device memory. The tensor maps
@@ -229,6 +239,33 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
     split_coords(tile, *a1, r);
   }
   return r;
+}
+
+// Staged C store of one epilogue warp (TcArgs::crun = e0): stg holds the
+// warp's 32 rows (m0 ...) x ncols <= 16 columns (nb ...) as [column][row], 33
+// floats per column. Lane (i, j) = (lane % e0, lane / e0) stores element
+// (run start + i, column j + q*k), q = 32 / e0: one store instruction covers
+// q consecutive columns of a run of e0 consecutive m, consecutive addresses
+// of C. Same arithmetic as the register epilogue (alpha*acc, fmaf with beta).
+__device__ __forceinline__ void store_runs(const float* stg, const TcArgs& a, int64_t m0,
+                                           int64_t nb, int ncols, int e0, float alpha, float beta,
+                                           int lane) {
+  const int q = 32 / e0;
+  const int i = lane % e0, j = lane / e0;
+  if (j >= q) return;
+#pragma unroll 1
+  for (int64_t rs = (m0 / e0) * e0; rs < m0 + 32; rs += e0) {
+    const int64_t m = rs + i;
+    if (m < m0 || m >= m0 + 32 || m >= a.M) continue;
+    const int64_t cmo = a.c_m_off[m];
+    const float* col = stg + (m - m0);
+#pragma unroll 1
+    for (int c = j; c < ncols; c += q) {
+      float* dst = a.C + cmo + __ldg(a.c_n_off + nb + c);
+      const float v = alpha * col[c * 33];
+      *dst = beta != 0.0f ? fmaf(beta, *dst, v) : v;
+    }
+  }
 }
 
 // ---- gather loader (TC_LOAD_GATHER) ------------------------------------------
@@ -474,9 +511,12 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   float* stg = reinterpret_cast<float*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
   int64_t* rowc = reinterpret_cast<int64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES +
                                              Cfg::STG_SLOTS * Cfg::STG_SLOT_BYTES);
+  float* epi_stg = reinterpret_cast<float*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES +
+                                            Cfg::STG_SLOTS * Cfg::STG_SLOT_BYTES +
+                                            Cfg::ROWCACHE_BYTES);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES +
                                                Cfg::STG_SLOTS * Cfg::STG_SLOT_BYTES +
-                                               Cfg::ROWCACHE_BYTES);
+                                               Cfg::ROWCACHE_BYTES + Cfg::EPI_STG_BYTES);
   uint64_t* full = bars;                   // [STAGES]
   uint64_t* empty = bars + Cfg::STAGES;    // [STAGES]
   uint64_t* accf = bars + 2 * Cfg::STAGES; // [2] accumulator ready
@@ -634,6 +674,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     const int q = warp & 3;             // TMEM lanes [32q, 32q+32) are accessible to this warp
     const int h = (warp - Cfg::EPI_WARP0) >> 2;  // column half of the tile
     constexpr int HC = Cfg::BN / 2;     // columns per epilogue warp
+    float* wstg = epi_stg + (warp - Cfg::EPI_WARP0) * 16 * Cfg::EPI_LD;  // staged C stores
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
@@ -691,6 +732,19 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
 #pragma unroll
             for (int j = 0; j < 32; ++j)
               if (cc + j < nlim) part[(size_t)(pc0 + cc + j) * pld] = __uint_as_float(r[j]);
+          } else if (a.crun > 0 && !part) {
+#pragma unroll
+            for (int hh = 0; hh < 32; hh += 16) {
+              if (cc + hh < nlim) {  // warp-uniform
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) wstg[j * Cfg::EPI_LD + lane] = __uint_as_float(r[hh + j]);
+                __syncwarp();
+                const int64_t left = nlim - cc - hh;
+                store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, n0 + cc + hh,
+                           left < 16 ? (int)left : 16, a.crun, alpha, beta, lane);
+              }
+            }
           } else if (m_ok) {
             if (beta != 0.0f) {
               float old[32];
@@ -751,6 +805,19 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
 #pragma unroll
           for (int j = 0; j < HC; ++j)
             if (j < nlim) part[(size_t)(pc0 + j) * pld] = sum[j];
+        } else if (a.crun > 0 && !part) {
+#pragma unroll
+          for (int cc = 0; cc < HC; cc += 16) {
+            if (cc < nlim) {  // warp-uniform
+              __syncwarp();
+#pragma unroll
+              for (int j = 0; j < 16; ++j) wstg[j * Cfg::EPI_LD + lane] = sum[cc + j];
+              __syncwarp();
+              const int64_t left = nlim - cc;
+              store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, n0 + cc,
+                         left < 16 ? (int)left : 16, a.crun, alpha, beta, lane);
+            }
+          }
         } else if (m_ok) {
           if (beta != 0.0f) {
 #pragma unroll

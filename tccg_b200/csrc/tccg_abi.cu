@@ -104,6 +104,10 @@ struct tccg_plan {
   // tensors, no packing pass) and its read schedule per operand (GatherRead)
   bool gather = false;
   int32_t gread_a = 0, gread_b = 0;
+  // tcgen05 epilogue: C's stride-one index is the first M mode of extent
+  // crun < 32, directly followed in C by the first N mode (staged C stores,
+  // TcArgs::crun), or 0
+  int32_t crun = 0;
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, off_tail = 0, ws_bytes = 0;
   char describe[512] = "";
@@ -582,6 +586,10 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
     if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int32_t));
     if (e != cudaSuccess) rc = fail(TCCG_ERR_CUDA, "status word: %s", cudaGetErrorString(e));
   }
+  p->crun = (d.c_m_stride[0] == 1 && d.m_ext[0] >= 2 && d.m_ext[0] < 32 && d.n_ext[0] > 1 &&
+             d.c_n_stride[0] == d.m_ext[0])
+                ? (int32_t)d.m_ext[0]
+                : 0;
   p->simt = choose_simt(p);
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
@@ -1300,6 +1308,7 @@ static TcArgs tc_args(const tccg_plan* p, float* Cout, const int64_t* c_m, const
   a.tail_split = p->tail_split;
   a.tail_kb = p->tail_kb;
   a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
+  a.crun = c_m == p->t_c_m ? p->crun : 0;  // not for TTGT's contiguous C'
   return a;
 }
 
