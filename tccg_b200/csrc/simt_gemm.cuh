@@ -110,6 +110,11 @@ struct SimtArgs {
   const int64_t* b_n_off;
   const int64_t* b_k_off;
   int32_t* status;  // device error word (bounded waits of the short-K kernel)
+  // C layout (as TcArgs::crun): e0 in [2, 31] = C's stride-one index is the
+  // first M mode, of extent e0, directly followed in C by the first N mode;
+  // the epilogue then stores runs of e0 m by 32 / e0 columns per warp
+  // instruction (consecutive addresses); 0 = quads along m
+  int32_t crun;
 };
 
 template <typename T, int S = SIMT_SQUARE>
@@ -443,7 +448,32 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       Cn[tid] = n < a.N ? a.c_n_off[n] : 0;
     }
     __syncthreads();
-    if (mok[0]) {
+    if (a.crun > 0) {
+      // lane (i, j) = (lane % e0, lane / e0) of warp w stores element
+      // (run start + i, column block start + j) for every (run, column
+      // block) pair w, w + 8, ...: one store instruction covers q columns
+      // of a run of e0 consecutive m, consecutive addresses of C. Same
+      // arithmetic as the quad path (alpha * acc, then fma with beta).
+      const int e0 = a.crun, qn = 32 / e0;
+      const int lane = tid & 31, w = tid >> 5;
+      const int i = lane % e0, jj = lane / e0;
+      if (jj < qn) {
+        const int64_t rfirst = (m0 / e0) * e0;
+        const int nruns = (int)((m0 + BM - rfirst + e0 - 1) / e0);
+        const int ncb = (EPN + qn - 1) / qn;
+#pragma unroll 1
+        for (int u = w; u < nruns * ncb; u += 8) {
+          const int ri = u % nruns, cb = u / nruns;
+          const int64_t m = rfirst + (int64_t)ri * e0 + i;
+          const int nl = cb * qn + jj;
+          if (m < m0 || m >= m0 + BM || m >= a.M || nl >= EPN || n0 + p * EPN + nl >= a.N) continue;
+          T* d = a.C + a.c_m_off[m] + Cn[nl];
+          T v = alpha * Cs[nl * LDC + (int)(m - m0)];
+          if (beta != T(0)) v = fma(beta, *d, v);
+          *d = v;
+        }
+      }
+    } else if (mok[0]) {
       constexpr int CH = sizeof(T) == 8 ? 4 : 8;  // columns whose C loads are in flight together
 #pragma unroll 1
       for (int it0 = 0; it0 < ITER; it0 += CH) {

@@ -1253,6 +1253,7 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(ws + p->off_part) : nullptr;
   set_direct(a, p, GA, GB);
   a.status = p->d_status;
+  a.crun = c_m == p->t_c_m ? p->crun : 0;  // not for TTGT's contiguous C'
   dim3 grid((unsigned)(p->Mp / p->simt_bm), (unsigned)(p->Np / p->simt_bn), (unsigned)p->ksplit);
   if (grid.y > 65535u || grid.z > 65535u) return fail(TCCG_ERR_UNSUPPORTED, "grid too large");
   mark(1, 0, s);
@@ -1837,6 +1838,7 @@ static SimtArgs<T> simt_args_for(const tccg_plan* p, char* w, const void* GA, co
   a.partial = p->ksplit > 1 ? reinterpret_cast<T*>(w + p->off_part) : nullptr;
   set_direct(a, p, GA, GB);
   a.status = p->d_status;
+  a.crun = p->crun;
   return a;
 }
 

@@ -1,6 +1,7 @@
-"""The tcgen05 epilogue's staged C stores (C whose stride-one index is the
+"""The epilogues' staged C stores for a C whose stride-one index is the
 first M mode, of extent e0 < 32, directly followed in C by the first N mode:
-stores go through shared memory in runs of e0 m by 32 // e0 columns).
+stores go through shared memory in runs of e0 m by 32 // e0 columns, in the
+tcgen05 kernel (both loaders) and in the CUDA-core tile kernel.
 
 With alpha = 1 and beta = 0 the result must equal, bit for bit, the same
 contraction through TTGT, whose GEMM writes the contiguous C' with the
@@ -36,9 +37,10 @@ def _data(ln, seed):
 
 def _run(con, A, B, C, precision, tuning, alpha, beta):
     import torch
-    p = Plan(con, precision=precision, tuning=tuning, dtype="f32")
-    dC = torch.from_numpy(C).cuda()
-    p.run(torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda(), dC, alpha, beta)
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    p = Plan(con, precision=precision, tuning=tuning, dtype="f64" if precision == "fp64" else "f32")
+    dC = torch.from_numpy(C).cuda().to(dt)
+    p.run(torch.from_numpy(A).cuda().to(dt), torch.from_numpy(B).cuda().to(dt), dC, alpha, beta)
     torch.cuda.synchronize()
     assert p.status() == 0
     return dC, p
@@ -73,3 +75,27 @@ def test_staged_stores_with_beta(cuda, name, load):
     cg, _ = _run(con, A, B, C, "bf16x3", Tuning(load=load, variant=16), 0.5, -1.25)
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 0.5, -1.25)
     assert error_metrics(cg.double().cpu().numpy(), ref)["normwise"] <= 1e-5
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("precision,tuning", [("fp32", dict(shortk=-1)), ("fp32", dict(simt_tile=3)),
+                                              ("fp64", dict(shortk=-1))])
+def test_cuda_core_staged_stores_equal_ttgt(cuda, name, precision, tuning):
+    """CUDA-core tile kernel: the staged run stores of GETT equal TTGT (whose
+    GEMM writes the contiguous C' with quads along m) bit for bit, beta = 0;
+    with beta != 0 they match the FP64 oracle at the FP32 / FP64 bound."""
+    import torch
+    lc, la, lb, sizes = CASES[name]
+    con = make_contraction(lc, la, lb, sizes)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, C = _data(ln, 5)
+    t = dict(tuning, ksplit=1)
+    cg, pg = _run(con, A, B, C, precision, Tuning(**t), 1.0, 0.0)
+    ct, pt = _run(con, A, B, C, precision, Tuning(method="ttgt", **t), 1.0, 0.0)
+    assert "simt_gett" in pg.describe(), pg.describe()
+    assert torch.equal(cg, ct)
+    con2 = make_contraction(lc, la, lb, sizes, 0.5, -1.25)
+    cb, _ = _run(con2, A, B, C, precision, Tuning(**t), 0.5, -1.25)
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 0.5, -1.25)
+    tol = 1e-6 if precision == "fp32" else 1e-13
+    assert error_metrics(cb.double().cpu().numpy(), ref)["normwise"] <= tol
