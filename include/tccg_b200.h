@@ -124,6 +124,9 @@ typedef struct tccg_tuning {
                           pass + TMA loads (128x192 tiles), 2 = gather: producer warps read the
                           caller's tensors through the offset tables and split them into the
                           swizzled bf16 stages themselves (128x128 tiles, no packing pass) */
+  int32_t tile_n;      /* tcgen05 tile width (columns of C per tile): 0 = the loader's default
+                          (BF16 256, BF16X3 192, gather 128); 128, 192 or 256 (BF16), 128 or
+                          192 (BF16X3 with the packing pass) */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

@@ -166,7 +166,10 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             else:
                 first.append(Tuning(method=method, variant=chunks[0]))  # tensor cores
             first.append(Tuning(method=method, variant=-1))
-            more = []
+            # tcgen05 tile widths of the packed-operand loader
+            tiles = [128] if precision == "bf16x3" else [192, 128]
+            tl = 1 if len(loads) > 1 else 0
+            more = [Tuning(method=method, load=tl, variant=chunks[0], tile_n=w) for w in tiles]
             for ld in loads:
                 more += [Tuning(method=method, load=ld, raster=r) for r in (-8, 4, 16, -2)]
                 more += [Tuning(method=method, load=ld, variant=c) for c in chunks[1:]]

@@ -67,18 +67,29 @@ enum GatherRead : int {
 // The gather variant has 13 warps (4 producers, the MMA warp, 8 epilogue
 // warps: at most 152 registers each), so its tiles are 128x128 (64 running
 // sums per epilogue warp).
-template <int MODE, int LOAD = TC_LOAD_TMA>
+//
+// BNV != 0 sets the tile width of the TMA loader (a blocking the autotuner
+// searches: 128, 192 or 256 columns for BF16, 128 or 192 for BF16X3); the
+// operand ring then has as many stages as fit in shared memory (at most 6).
+template <int MODE, int LOAD = TC_LOAD_TMA, int BNV = 0>
 struct TcCfgT {
   static constexpr bool GATHER = LOAD == TC_LOAD_GATHER;
   static_assert(!GATHER || MODE == TC_BF16X3, "the gather loader serves split-BF16x3");
+  static_assert(!GATHER || BNV == 0 || BNV == 128, "the gather loader has 128-column tiles");
+  static_assert(BNV == 0 || BNV == 128 || BNV == 192 || (BNV == 256 && MODE == TC_BF16),
+                "tile widths: 128, 192 (and 256 for BF16)");
   static constexpr int BM = 128;
-  static constexpr int BN = GATHER ? 128 : (MODE == TC_BF16X3) ? 192 : 256;
+  static constexpr int BN = BNV ? BNV : GATHER ? 128 : (MODE == TC_BF16X3) ? 192 : 256;
   static constexpr int ROW_BYTES = 128;  // one swizzle row per operand row per stage
-  static constexpr int STAGES = GATHER ? 2 : (MODE == TC_BF16X3) ? 5 : 4;
   static constexpr int A_STAGE = BM * ROW_BYTES;   // 16 KB
   static constexpr int B_STAGE = BN * ROW_BYTES;   // 16 / 24 / 32 KB
   static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-  static constexpr int ACC_STRIDE = GATHER ? 128 : 256;  // accumulator b starts at column ACC_STRIDE*b
+  // default shapes keep their measured ring depths (BF16X3 5 x 40 KB, BF16
+  // 4 x 48 KB); other widths take what fits next to the epilogue staging
+  static constexpr int STAGES = GATHER ? 2
+                                : BNV == 0 ? ((MODE == TC_BF16X3) ? 5 : 4)
+                                : (200 * 1024 / STAGE_BYTES > 6 ? 6 : 200 * 1024 / STAGE_BYTES);
+  static constexpr int ACC_STRIDE = BN <= 128 ? 128 : 256;  // accumulator b starts at column ACC_STRIDE*b
   static constexpr int TMEM_COLS = 2 * ACC_STRIDE;       // two accumulators of BN columns
   static constexpr int PRODUCER_WARPS = GATHER ? 4 : 1;
   static constexpr int MMA_WARP = PRODUCER_WARPS;
@@ -497,11 +508,11 @@ __device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup&
   cp_async_wait<0>();  // no copy in flight when the producers leave
 }
 
-template <int MODE, int LOAD, bool GROUPED>
+template <int MODE, int LOAD, int BNV, bool GROUPED>
 __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUtensorMap* tmB,
                                              const TcArgs* a1, const TcGroup& g,
                                              int32_t* status) {
-  using Cfg = TcCfgT<MODE, LOAD>;
+  using Cfg = TcCfgT<MODE, LOAD, BNV>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_addr = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + (((raw_addr + 1023u) & ~1023u) - raw_addr);
@@ -849,26 +860,26 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   }
 }
 
-template <int MODE, int LOAD = TC_LOAD_TMA>
-__global__ void __launch_bounds__(TcCfgT<MODE, LOAD>::NUM_THREADS, 1)
+template <int MODE, int LOAD = TC_LOAD_TMA, int BNV = 0>
+__global__ void __launch_bounds__(TcCfgT<MODE, LOAD, BNV>::NUM_THREADS, 1)
     gett_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                    const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
   TcGroup g{nullptr, nullptr, 0, 0};
-  gett_tc_body<MODE, LOAD, false>(&tmA, &tmB, &a, g, a.status);
+  gett_tc_body<MODE, LOAD, BNV, false>(&tmA, &tmB, &a, g, a.status);
 }
 
-template <int MODE, int LOAD = TC_LOAD_TMA>
-__global__ void __launch_bounds__(TcCfgT<MODE, LOAD>::NUM_THREADS, 1)
+template <int MODE, int LOAD = TC_LOAD_TMA, int BNV = 0>
+__global__ void __launch_bounds__(TcCfgT<MODE, LOAD, BNV>::NUM_THREADS, 1)
     gett_tc_group_kernel(const TcGroup g, int32_t* status) {
-  gett_tc_body<MODE, LOAD, true>(nullptr, nullptr, nullptr, g, status);
+  gett_tc_body<MODE, LOAD, BNV, true>(nullptr, nullptr, nullptr, g, status);
 }
 
 // Tail split: C = alpha * (slice 0 + slice 1 + ...) + beta * C over the tail
 // tiles (RN adds in slice order). grid = (tail tiles, BM * BN / 256), block
 // 256: thread e of a tile takes element (m_local = e % BM, n_local = e / BM).
-template <int MODE, int LOAD = TC_LOAD_TMA>
+template <int MODE, int LOAD = TC_LOAD_TMA, int BNV = 0>
 __global__ void __launch_bounds__(256) tc_tail_reduce_kernel(const TcArgs a) {
-  using Cfg = TcCfgT<MODE, LOAD>;
+  using Cfg = TcCfgT<MODE, LOAD, BNV>;
   grid_dep_wait();  // partial sums written by the GETT kernel before
   const int tail = a.tiles_m * a.tiles_n - a.full_tiles;
   const int tl = blockIdx.x;

@@ -108,10 +108,57 @@ struct tccg_plan {
   // crun < 32, directly followed in C by the first N mode (staged C stores,
   // TcArgs::crun), or 0
   int32_t crun = 0;
+  int32_t tcv = 0;  // TcVariant of a tensor-core plan
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, off_tail = 0, ws_bytes = 0;
   char describe[512] = "";
 };
+
+// tcgen05 kernel variants: precision x operand loader x tile width (the
+// autotuner's tile-shape choices). A plan runs one; a grouped run launches
+// one grouped kernel per variant its items use.
+enum TcVariant : int {
+  TCV_X3 = 0,         // split-BF16x3, packing pass + TMA, 128 x 192
+  TCV_X3_N128,        // split-BF16x3, packing pass + TMA, 128 x 128
+  TCV_X3_GATHER,      // split-BF16x3, gather loader, 128 x 128
+  TCV_BF16,           // BF16, packing pass + TMA, 128 x 256
+  TCV_BF16_N192,      // BF16, packing pass + TMA, 128 x 192
+  TCV_BF16_N128,      // BF16, packing pass + TMA, 128 x 128
+  TCV_COUNT
+};
+
+template <int MODE, int LOAD, int BNV>
+struct TcKernels {
+  using Cfg = TcCfgT<MODE, LOAD, BNV>;
+  static constexpr bool GATHER = LOAD == TC_LOAD_GATHER;
+  static constexpr auto single = &gett_tc_kernel<MODE, LOAD, BNV>;
+  static constexpr auto group = &gett_tc_group_kernel<MODE, LOAD, BNV>;
+  static constexpr auto tail = &tc_tail_reduce_kernel<MODE, LOAD, BNV>;
+};
+
+// Calls f(TcKernels<...>{}) for variant v.
+template <typename F>
+static void with_tc_variant(int v, F&& f) {
+  switch (v) {
+    case TCV_X3: f(TcKernels<TC_BF16X3, TC_LOAD_TMA, 0>{}); break;
+    case TCV_X3_N128: f(TcKernels<TC_BF16X3, TC_LOAD_TMA, 128>{}); break;
+    case TCV_X3_GATHER: f(TcKernels<TC_BF16X3, TC_LOAD_GATHER, 0>{}); break;
+    case TCV_BF16: f(TcKernels<TC_BF16, TC_LOAD_TMA, 0>{}); break;
+    case TCV_BF16_N192: f(TcKernels<TC_BF16, TC_LOAD_TMA, 192>{}); break;
+    default: f(TcKernels<TC_BF16, TC_LOAD_TMA, 128>{}); break;
+  }
+}
+
+// The variant of a tensor-core plan: its precision, loader and the tuning's
+// tile width (0 = the loader's default); -1 when the width is not built.
+static int tc_variant(bool x3, bool gather, int32_t tile_n) {
+  if (gather) return (tile_n == 0 || tile_n == 128) ? TCV_X3_GATHER : -1;
+  if (x3) return tile_n == 0 || tile_n == 192 ? TCV_X3 : tile_n == 128 ? TCV_X3_N128 : -1;
+  return tile_n == 0 || tile_n == 256 ? TCV_BF16
+         : tile_n == 192              ? TCV_BF16_N192
+         : tile_n == 128              ? TCV_BF16_N128
+                                      : -1;
+}
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 static int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
@@ -173,7 +220,7 @@ static bool unit_first(int n, const int64_t* ext, const int64_t* str);
 // enough (<= 4 MiB) to stay in L2 across its re-reads.
 static bool gather_eligible(const tccg_plan* p) {
   if (p->prec != TCCG_PREC_BF16X3 || p->dtype != TCCG_F32 || p->tune.method != TCCG_METHOD_GETT ||
-      p->tune.pair || p->tune.load == 1)
+      p->tune.pair || p->tune.load == 1 || (p->tune.tile_n != 0 && p->tune.tile_n != 128))
     return false;
   if (p->tune.load == 2) return true;
   const tccg_desc& d = p->d;
@@ -697,12 +744,20 @@ static int plan_layout(tccg_plan* p) {
     p->chunk_kb = x3 ? (p->tune.variant > 0 ? p->tune.variant : 16) : p->num_kb;
     if (p->chunk_kb < 1) p->chunk_kb = 1;
     const bool pair = p->tune.pair != 0;
-    if (pair)
+    int stages = 0;
+    if (pair) {
       p->bn = x3 ? Tc2Cfg<TC_BF16X3>::BN : Tc2Cfg<TC_BF16>::BN;
-    else if (p->gather)
-      p->bn = TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::BN;
-    else
-      p->bn = x3 ? TcCfgT<TC_BF16X3>::BN : TcCfgT<TC_BF16>::BN;
+      stages = x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES;
+    } else {
+      p->tcv = tc_variant(x3, p->gather, p->tune.tile_n);
+      if (p->tcv < 0)
+        return fail(TCCG_ERR_UNSUPPORTED, "tile width %d is not built for %s%s", p->tune.tile_n,
+                    x3 ? "BF16X3" : "BF16", p->gather ? " with the gather loader" : "");
+      with_tc_variant(p->tcv, [&](auto k) {
+        p->bn = decltype(k)::Cfg::BN;
+        stages = decltype(k)::Cfg::STAGES;
+      });
+    }
     p->tiles_m = (int32_t)cdiv(p->M, pair ? 256 : 128);
     p->tiles_n = (int32_t)cdiv(p->N, p->bn);
     // tile order: groups of `raster` tile rows (> 0, default 8) or of
@@ -774,7 +829,7 @@ static int plan_layout(tccg_plan* p) {
                "method=GETT prec=bf16x3 kernel=gett_tc<BF16X3,gather> tile=128x%d stages=%d M=%lld "
                "N=%lld K=%lld kblocks=%d chunk=%d ksplit=%d tail=%dx%d grid=%d raster=%d pack=none "
                "(gather a=%s b=%s)",
-               p->bn, TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::STAGES, (long long)p->M, (long long)p->N,
+               p->bn, stages, (long long)p->M, (long long)p->N,
                (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit,
                p->tail_split > 1 ? (int)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles) : 0,
                p->tail_split, p->grid, p->raster, gr[p->gread_a], gr[p->gread_b]);
@@ -784,9 +839,7 @@ static int plan_layout(tccg_plan* p) {
              "kblocks=%d chunk=%d ksplit=%d tail=%dx%d grid=%d raster=%d pack=K-major bf16%s(read_k_fast a=%d b=%d "
              "visit a=%d b=%d kblock a=%dx%dx%d%s b=%dx%dx%d%s kstream a=%d b=%d)",
              ttgt ? "TTGT" : "GETT", x3 ? "bf16x3" : "bf16", pair ? "2" : "", x3 ? "BF16X3" : "BF16",
-             pair ? 256 : 128, p->bn,
-             pair ? (x3 ? Tc2Cfg<TC_BF16X3>::STAGES : Tc2Cfg<TC_BF16>::STAGES)
-                  : (x3 ? TcCfgT<TC_BF16X3>::STAGES : TcCfgT<TC_BF16>::STAGES),
+             pair ? 256 : 128, p->bn, stages,
              (long long)p->M, (long long)p->N, (long long)p->K, p->num_kb, p->chunk_kb, p->ksplit,
              p->tail_split > 1 ? (int)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles) : 0,
              p->tail_split, p->grid, p->raster, x3 ? " hi|lo " : " ", p->read_k_fast_a, p->read_k_fast_b,
@@ -894,16 +947,14 @@ static cudaError_t set_attrs() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SimtShortKCfg<double>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(simt_shortk_kernel<double, false>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SimtShortKCfg<double>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfgT<TC_BF16>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(gett_tc_kernel<TC_BF16X3, TC_LOAD_GATHER>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3, TC_LOAD_GATHER>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::SMEM_BYTES));
+  for (int v = 0; v < TCV_COUNT; ++v)
+    with_tc_variant(v, [&](auto k) {
+      using K = decltype(k);
+      chk(cudaFuncSetAttribute(K::single, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)K::Cfg::SMEM_BYTES));
+      chk(cudaFuncSetAttribute(K::group, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)K::Cfg::SMEM_BYTES));
+    });
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)simt_group_smem_bytes<float>()));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -912,11 +963,7 @@ static cudaError_t set_attrs() {
                            (int)Tc2Cfg<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)Tc2Cfg<TC_BF16X3>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfgT<TC_BF16>::SMEM_BYTES));
-  chk(cudaFuncSetAttribute(gett_tc_group_kernel<TC_BF16X3>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)TcCfgT<TC_BF16X3>::SMEM_BYTES));
+
   return e;
 }
 
@@ -1330,25 +1377,15 @@ static void set_gather(TcArgs& a, const tccg_plan* p, const void* GA, const void
 }
 
 // Reduction after the tcgen05 kernel: tail slices or k-split slices.
-template <int LOAD>
 static int tc_reduce(const tccg_plan* p, const TcArgs& a, float* Cout, const int64_t* c_m,
                      const int64_t* c_n, float alpha, float beta, cudaStream_t s) {
-  const bool x3 = p->prec == TCCG_PREC_BF16X3;
   if (p->tail_split > 1) {
     const unsigned tail = (unsigned)((int64_t)p->tiles_m * p->tiles_n - p->full_tiles);
     mark(2, 0, s);
-    if constexpr (LOAD == TC_LOAD_GATHER) {
-      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16X3, TC_LOAD_GATHER>,
-                   dim3(tail, TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::BM *
-                                  TcCfgT<TC_BF16X3, TC_LOAD_GATHER>::BN / 256),
-                   dim3(256), 0, s, a);
-    } else if (x3) {
-      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16X3>,
-                   dim3(tail, TcCfgT<TC_BF16X3>::BM * TcCfgT<TC_BF16X3>::BN / 256), dim3(256), 0, s, a);
-    } else {
-      launch_after(true, p, tc_tail_reduce_kernel<TC_BF16>,
-                   dim3(tail, TcCfgT<TC_BF16>::BM * TcCfgT<TC_BF16>::BN / 256), dim3(256), 0, s, a);
-    }
+    with_tc_variant(p->tcv, [&](auto k) {
+      using K = decltype(k);
+      launch_after(true, p, K::tail, dim3(tail, K::Cfg::BM * K::Cfg::BN / 256), dim3(256), 0, s, a);
+    });
     mark(2, 1, s);
     return launch_check("tc_tail_reduce");
   }
@@ -1367,64 +1404,58 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
                   cudaStream_t s) {
   const bool x3 = p->prec == TCCG_PREC_BF16X3;
   TcArgs a = tc_args(p, Cout, c_m, c_n, alpha, beta, ws);
-  if (p->gather) {
-    using Cfg = TcCfgT<TC_BF16X3, TC_LOAD_GATHER>;
-    set_gather(a, p, GA, GB);
-    take_injection(a);
-    CUtensorMap none;
-    memset(&none, 0, sizeof(none));
-    mark(1, 0, s);
-    launch_after(false, p, gett_tc_kernel<TC_BF16X3, TC_LOAD_GATHER>, dim3((unsigned)p->grid),
-                 dim3(Cfg::NUM_THREADS), Cfg::SMEM_BYTES, s, none, none, a);
-    mark(1, 1, s);
-    const int rc = launch_check("gett_tc (gather)");
-    if (rc) return rc;
-    return tc_reduce<TC_LOAD_GATHER>(p, a, Cout, c_m, c_n, alpha, beta, s);
-  }
-  void* Ap = ws + p->off_a;
-  void* Bp = ws + p->off_b;
-  PackArgs pa;
-  const int64_t kcover = x3 ? round_up(p->K, 32) : p->Kc;
-  const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
-  pa.op[0] = with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap,
-                                           p->Kc, p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst),
-                        p->ks_a, p->kb_a, p->kbq_a, es);
-  pa.op[1] = with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp,
-                                           p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
-                        p->ks_b, p->kb_b, p->kbq_b, es);
+  CUtensorMap tmA, tmB;
   int rc;
   bool packed = false;  // the packing kernel is the last launch on s
-  if (x3)
-    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s, &packed);
-  else if (p->dtype == TCCG_BF16)
-    rc = launch_pack<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16>(pa, s, &packed);
-  else
-    rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s, &packed);
-  if (rc) return rc;
-  CUtensorMap tmA, tmB;
   const bool pair = p->tune.pair != 0;
-  rc = encode_kmajor(&tmA, Ap, p->M, p->Kc, 128);
-  if (rc) return rc;
-  rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, pair ? p->bn / 2 : p->bn);
-  if (rc) return rc;
-  if (!pair) take_injection(a);
+  if (p->gather) {
+    // no packing pass: the kernel reads GA and GB through the offset tables
+    set_gather(a, p, GA, GB);
+    memset(&tmA, 0, sizeof(tmA));
+    memset(&tmB, 0, sizeof(tmB));
+  } else {
+    void* Ap = ws + p->off_a;
+    void* Bp = ws + p->off_b;
+    PackArgs pa;
+    const int64_t kcover = x3 ? round_up(p->K, 32) : p->Kc;
+    const size_t es = p->dtype == TCCG_BF16 ? 2 : 4;
+    pa.op[0] = with_kread(with_visit(pack_op(GA, p->t_a_m, p->t_a_k, p->M, p->K, p->M, kcover, Ap,
+                                             p->Kc, p->read_k_fast_a), p->t_a_vsrc, p->t_a_vdst),
+                          p->ks_a, p->kb_a, p->kbq_a, es);
+    pa.op[1] = with_kread(with_visit(pack_op(GB, p->t_b_n, p->t_b_k, p->N, p->K, p->N, kcover, Bp,
+                                             p->Kc, p->read_k_fast_b), p->t_b_vsrc, p->t_b_vdst),
+                          p->ks_b, p->kb_b, p->kbq_b, es);
+    if (x3)
+      rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s, &packed);
+    else if (p->dtype == TCCG_BF16)
+      rc = launch_pack<__nv_bfloat16, __nv_bfloat16, PACK_K_BF16>(pa, s, &packed);
+    else
+      rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16>(pa, s, &packed);
+    if (rc) return rc;
+    rc = encode_kmajor(&tmA, Ap, p->M, p->Kc, 128);
+    if (rc) return rc;
+    rc = encode_kmajor(&tmB, Bp, p->N, p->Kc, pair ? p->bn / 2 : p->bn);
+    if (rc) return rc;
+  }
   mark(1, 0, s);
-  if (pair && x3)
+  if (pair && x3) {
     launch_after(packed, p, gett_tc2_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16X3>::NUM_THREADS),
                  Tc2Cfg<TC_BF16X3>::SMEM_BYTES, s, tmA, tmB, a);
-  else if (pair)
+  } else if (pair) {
     launch_after(packed, p, gett_tc2_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(Tc2Cfg<TC_BF16>::NUM_THREADS),
                  Tc2Cfg<TC_BF16>::SMEM_BYTES, s, tmA, tmB, a);
-  else if (x3)
-    launch_after(packed, p, gett_tc_kernel<TC_BF16X3>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16X3>::NUM_THREADS),
-                 TcCfgT<TC_BF16X3>::SMEM_BYTES, s, tmA, tmB, a);
-  else
-    launch_after(packed, p, gett_tc_kernel<TC_BF16>, dim3((unsigned)p->grid), dim3(TcCfgT<TC_BF16>::NUM_THREADS),
-                 TcCfgT<TC_BF16>::SMEM_BYTES, s, tmA, tmB, a);
+  } else {
+    take_injection(a);
+    with_tc_variant(p->tcv, [&](auto k) {
+      using K = decltype(k);
+      launch_after(packed, p, K::single, dim3((unsigned)p->grid), dim3(K::Cfg::NUM_THREADS),
+                   K::Cfg::SMEM_BYTES, s, tmA, tmB, a);
+    });
+  }
   mark(1, 1, s);
-  rc = launch_check("gett_tc");
+  rc = launch_check(p->gather ? "gett_tc (gather)" : "gett_tc");
   if (rc) return rc;
-  return tc_reduce<TC_LOAD_TMA>(p, a, Cout, c_m, c_n, alpha, beta, s);
+  return tc_reduce(p, a, Cout, c_m, c_n, alpha, beta, s);
 }
 
 static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s);
@@ -1696,14 +1727,16 @@ struct tccg_group {
   // over its items. On the 256-item batched workload 4 GiB waves take the
   // time of one wave (22.0 vs 22.1 ms BF16x3) with 4.0 instead of 12.8 GiB of
   // workspace; 512 MiB waves cost 8 % more time (more, shorter launches).
-  // The tensor-core items of a wave form two lanes: packed operands with TMA
-  // loads (tc0, n_tc) and the gather loader (tcg0, n_tcg), adjacent in d_tc.
+  // The tensor-core items of a wave form one lane per kernel variant
+  // (TcVariant): lane v holds items [lane0[v], lane0[v] + nlane[v]) of d_tc
+  // and runs as one grouped launch of that variant's kernel.
   struct Wave {
     std::vector<size_t> items;  // plan indices
-    int32_t simt0 = 0, n_simt = 0, tc0 = 0, n_tc = 0, tcg0 = 0, n_tcg = 0, red0 = 0, n_red = 0;
-    int32_t tcj0 = 0;  // first pack job of the TMA lane (two per item)
-    int64_t simt_tiles = 0, tc_tiles = 0, tcg_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0,
-            red_ctas = 0;
+    int32_t simt0 = 0, n_simt = 0, red0 = 0, n_red = 0;
+    int32_t lane0[TCV_COUNT] = {}, nlane[TCV_COUNT] = {};
+    int64_t lane_tiles[TCV_COUNT] = {};
+    int32_t tcj0 = 0, ntcj = 0;  // pack jobs of the packed-operand lanes (two per item)
+    int64_t simt_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0, red_ctas = 0;
   };
   std::vector<Wave> waves;
   bool bound = false;
@@ -1772,12 +1805,12 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     g->ws_bytes = std::max(g->ws_bytes, ws);
     if (simt_path(p)) {
       wv.simt_tiles += (p->Mp / p->simt_bm) * (p->Np / p->simt_bn) * p->ksplit;
-    } else if (p->gather) {
-      wv.tcg_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     } else {
-      wv.tc_tiles += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
+      wv.lane_tiles[p->tcv] += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
-    if (wv.simt_tiles > INT32_MAX || wv.tc_tiles > INT32_MAX || wv.tcg_tiles > INT32_MAX) {
+    bool too_many = wv.simt_tiles > INT32_MAX;
+    for (int v = 0; v < TCV_COUNT; ++v) too_many |= wv.lane_tiles[v] > INT32_MAX;
+    if (too_many) {
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "too many tiles");
     }
@@ -1876,10 +1909,10 @@ static int64_t reduce_ctas(const ReduceJob<T>& j) {
 // in the CUDA-core one), so the longest tiles start first and the short ones
 // fill in behind them.
 static std::vector<size_t> by_tile_cost(const tccg_group* g, const tccg_group::Wave& wv, bool simt,
-                                        bool gather = false) {
+                                        int variant = -1) {
   std::vector<size_t> idx;
   for (size_t i : wv.items)
-    if (simt_path(g->plans[i]) == simt && (simt || g->plans[i]->gather == gather)) idx.push_back(i);
+    if (simt_path(g->plans[i]) == simt && (simt || g->plans[i]->tcv == variant)) idx.push_back(i);
   auto cost = [&](size_t i) {
     const tccg_plan* p = g->plans[i];
     return simt ? (int64_t)p->ktiles_per_split : (int64_t)p->kb_per_split;
@@ -1958,11 +1991,11 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
                    std::vector<ReduceJob<float>>& red, int64_t& rctas) {
   int64_t pctas = 0;
   wv.tcj0 = (int32_t)jobs.size();
-  for (int lane = 0; lane < 2; ++lane) {  // 0: packed operands + TMA, 1: gather loader
-    const bool gather = lane == 1;
-    (gather ? wv.tcg0 : wv.tc0) = (int32_t)items.size();
+  for (int lane = 0; lane < TCV_COUNT; ++lane) {  // one lane per kernel variant
+    const bool gather = lane == TCV_X3_GATHER;
+    wv.lane0[lane] = (int32_t)items.size();
     int64_t tile = 0;
-    for (size_t i : by_tile_cost(g, wv, false, gather)) {
+    for (size_t i : by_tile_cost(g, wv, false, lane)) {
       const tccg_plan* p = g->plans[i];
       char* w = ws + g->ws_off[i];
       const void* GA = p->d.swap_ab ? B[i] : A[i];
@@ -2002,9 +2035,10 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
         rctas += reduce_ctas(red.back());
       }
     }
-    (gather ? wv.n_tcg : wv.n_tc) = (int32_t)items.size() - (gather ? wv.tcg0 : wv.tc0);
+    wv.nlane[lane] = (int32_t)items.size() - wv.lane0[lane];
   }
   if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
+  wv.ntcj = (int32_t)jobs.size() - wv.tcj0;
   wv.tc_pack_ctas = pctas;
   return TCCG_OK;
 }
@@ -2085,7 +2119,7 @@ template <typename T>
 static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_t s) {
   int rc;
   const dim3 blk(32, 8);
-  const int sj = 2 * wv.n_simt, tj = 2 * wv.n_tc;
+  const int sj = 2 * wv.n_simt, tj = wv.ntcj;
   const PackJob* sjobs = g->d_simt_jobs + 2 * wv.simt0;
   const int64_t* sb = g->b_simt_jobs + 2 * wv.simt0;
   if (wv.simt_pack_ctas > 0) {
@@ -2119,32 +2153,19 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
         wv.n_simt);
     if ((rc = launch_check("simt_gett_group"))) return rc;
   }
-  if (wv.n_tc > 0) {
+  for (int v = 0; v < TCV_COUNT; ++v) {
+    if (wv.nlane[v] == 0) continue;
     TcGroup tg;
-    tg.items = g->d_tc + wv.tc0;
-    tg.tile_begin = g->b_tc_items + wv.tc0;
-    tg.n_items = wv.n_tc;
-    tg.total_tiles = (int32_t)wv.tc_tiles;
-    const unsigned grid = (unsigned)std::min<int64_t>(wv.tc_tiles, g->num_sms);
-    if (x3)
-      gett_tc_group_kernel<TC_BF16X3><<<grid, TcCfgT<TC_BF16X3>::NUM_THREADS,
-                                        TcCfgT<TC_BF16X3>::SMEM_BYTES, s>>>(tg, g->tc_status);
-    else
-      gett_tc_group_kernel<TC_BF16><<<grid, TcCfgT<TC_BF16>::NUM_THREADS,
-                                      TcCfgT<TC_BF16>::SMEM_BYTES, s>>>(tg, g->tc_status);
+    tg.items = g->d_tc + wv.lane0[v];
+    tg.tile_begin = g->b_tc_items + wv.lane0[v];
+    tg.n_items = wv.nlane[v];
+    tg.total_tiles = (int32_t)wv.lane_tiles[v];
+    const unsigned grid = (unsigned)std::min<int64_t>(wv.lane_tiles[v], g->num_sms);
+    with_tc_variant(v, [&](auto k) {
+      using K = decltype(k);
+      K::group<<<grid, K::Cfg::NUM_THREADS, K::Cfg::SMEM_BYTES, s>>>(tg, g->tc_status);
+    });
     if ((rc = launch_check("gett_tc_group"))) return rc;
-  }
-  if (wv.n_tcg > 0) {
-    using Cfg = TcCfgT<TC_BF16X3, TC_LOAD_GATHER>;
-    TcGroup tg;
-    tg.items = g->d_tc + wv.tcg0;
-    tg.tile_begin = g->b_tc_items + wv.tcg0;
-    tg.n_items = wv.n_tcg;
-    tg.total_tiles = (int32_t)wv.tcg_tiles;
-    const unsigned grid = (unsigned)std::min<int64_t>(wv.tcg_tiles, g->num_sms);
-    gett_tc_group_kernel<TC_BF16X3, TC_LOAD_GATHER><<<grid, Cfg::NUM_THREADS, Cfg::SMEM_BYTES, s>>>(
-        tg, g->tc_status);
-    if ((rc = launch_check("gett_tc_group (gather)"))) return rc;
   }
   if (wv.n_red > 0) {
     reduce_group_kernel<T><<<(unsigned)wv.red_ctas, 256, 0, s>>>(

@@ -98,7 +98,7 @@ def source(con: Contraction, precision: str, tuning: Tuning, float_type: str) ->
 #include "gett.h"
 
 static const tccg_desc kDesc = %(desc)s;
-static const tccg_tuning kTuning = {%(method)s, %(variant)d, %(ksplit)d, %(raster)d, %(max_ctas)d, %(pair)d, %(direct)d, %(shortk)d, %(simt_tile)d, %(tail_split)d, %(load)d};
+static const tccg_tuning kTuning = {%(method)s, %(variant)d, %(ksplit)d, %(raster)d, %(max_ctas)d, %(pair)d, %(direct)d, %(shortk)d, %(simt_tile)d, %(tail_split)d, %(load)d, %(tile_n)d};
 
 /* host-buffer path: slabs of C's last index (full tensors' strides), element
    offsets into A, B, C and element counts of the parts copied per slab */
@@ -239,7 +239,7 @@ int gett_last_status(void) { return g_status; }
            variant=tuning.variant, ksplit=tuning.ksplit, raster=tuning.raster,
            max_ctas=tuning.max_ctas, pair=tuning.pair, direct=tuning.direct,
            shortk=tuning.shortk, simt_tile=tuning.simt_tile,
-           tail_split=tuning.tail_split, load=tuning.load, dt=dt, prec=prec, T=T,
+           tail_split=tuning.tail_split, load=tuning.load, tile_n=tuning.tile_n, dt=dt, prec=prec, T=T,
            nslab=len(slabs), slab_desc=slab_desc, slab_off=slab_off, slab_len=slab_len,
            per_a=int(per["A"]), per_b=int(per["B"]), na=con.A0.num_elements(),
            nb=con.B0.num_elements(), nc=con.C0.num_elements())

@@ -166,6 +166,7 @@ class Tuning:
     simt_tile: int = 0  # CUDA-core tiles: 0 auto, 1 128x128, 2 128x32, 3 32x128
     tail_split: int = 0  # tcgen05: 0 auto (k slices for a short last round), -1 never
     load: int = 0  # tcgen05 BF16x3, FP32 operands: 0 auto, 1 packing pass + TMA, 2 gather
+    tile_n: int = 0  # tcgen05 tile width: 0 default, 128, 192 (BF16, BF16x3) or 256 (BF16)
     # mode orders of the GETT view (gett_view): 0 = heuristic
     n_order: int = 0  # 1 = C's order, 2 = GB's unit-stride N mode first
     k_order: int = 0  # 1 = GA's order, 2 = GB's order
@@ -183,13 +184,14 @@ class Tuning:
         t.simt_tile = int(self.simt_tile)
         t.tail_split = int(self.tail_split)
         t.load = int(self.load)
+        t.tile_n = int(self.tile_n)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d/o%d%d" % (
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d/n%d/o%d%d" % (
             self.method, self.ksplit, self.raster, self.max_ctas, self.variant, self.pair,
-            self.direct, self.shortk, self.simt_tile, self.tail_split, self.load, self.n_order,
-            self.k_order)
+            self.direct, self.shortk, self.simt_tile, self.tail_split, self.load, self.tile_n,
+            self.n_order, self.k_order)
 
 
 class Plan:

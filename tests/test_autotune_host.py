@@ -56,8 +56,9 @@ def test_bf16_candidates_start_with_the_library_choice(precision):
         # both kernel families and the tail split switched off are searched
         assert any(t.variant < 0 for t in cs) and any(t.variant > 0 or t.load > 0 for t in cs)
         assert any(t.tail_split == -1 for t in cs)
-        # both tile orders (TCCG's two loop orders)
+        # both tile orders (TCCG's two loop orders) and other tile widths
         assert any(t.raster < 0 for t in cs) and any(t.raster > 0 for t in cs)
+        assert {t.tile_n for t in cs} >= ({0, 128} if precision == "bf16x3" else {0, 128, 192})
 
 
 def test_split_bf16x3_searches_both_loaders_first():
