@@ -345,7 +345,10 @@ __device__ __forceinline__ void gather_rows(const GatherJob& j, int64_t* rowc, i
 }
 
 // Asynchronous copies of one job's source elements into a staging slot:
-// operand o's element (r, k) of the k-block goes to slot_o[r * ld + k].
+// operand o's element (r, k) of the k-block goes to slot_o[r * ld + k]. The
+// k-block's 32 k offsets are loaded once per lane and broadcast with warp
+// shuffles, row offsets come from the shared cache; the copy loops are
+// unrolled so that many copies of a thread are in flight at once.
 template <int BM, int BN>
 __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, const int64_t* rowc,
                                              int ptid) {
@@ -364,31 +367,49 @@ __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, co
     const int read = a.gread[o];
     const int ld = gather_ld(read);
     float* dst = slot + (o ? BM * 36 : 0);
-    const int64_t* gk = a.gk[o] + k0;
+    // k offset of k = lane (0 past K)
+    const int64_t ko_lane = lane < kn ? __ldg(a.gk[o] + k0 + lane) : 0;
     if (read == GATHER_ROWS) {
-#pragma unroll 1
-      for (int k = 0; k < kn; ++k) {
-        const int64_t ko = __ldg(gk + k);
-        for (int r = ptid; r < nr; r += 128) cp_async_elem<4>(dst + r * ld + k, src + rc[r] + ko);
+      // lanes along rows: thread ptid copies rows ptid (and ptid + 128)
+      const int r = ptid;
+      const bool ok = r < nr;
+      const float* srow = src + (ok ? rc[r] : 0);
+      float* drow = dst + r * ld;
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) {
+        const int64_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
+        if (ok && k < kn) cp_async_elem<4>(drow + k, srow + ko);
+      }
+      if (rows > 128) {
+        const int r2 = ptid + 128;
+        const bool ok2 = r2 < nr;
+        const float* srow2 = src + (ok2 ? rc[r2] : 0);
+        float* drow2 = dst + r2 * ld;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) {
+          const int64_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
+          if (ok2 && k < kn) cp_async_elem<4>(drow2 + k, srow2 + ko);
+        }
       }
     } else if (read == GATHER_K) {
       if (lane < kn) {
-        const int64_t ko = __ldg(gk + lane);
-#pragma unroll 4
-        for (int r = pw; r < nr; r += 4) cp_async_elem<4>(dst + r * ld + lane, src + rc[r] + ko);
+#pragma unroll 8
+        for (int r = pw; r < nr; r += 4) cp_async_elem<4>(dst + r * ld + lane, src + rc[r] + ko_lane);
       }
-    } else {  // GATHER_KQUAD
+    } else {  // GATHER_KQUAD: lane -> (row sub = lane / 8, quad = lane % 8)
       const int kq = 4 * (lane & 7), sub = lane >> 3;
+      int64_t koq[4];  // offsets of the quad's 4 k (every lane shuffles, before any branch)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) koq[e] = __shfl_sync(0xffffffffu, ko_lane, kq + e);
       if (kq + 3 < kn) {
-        const int64_t ko = __ldg(gk + kq);
-#pragma unroll 4
-        for (int r = pw * 4 + sub; r < nr; r += 16) cp_async_16(dst + r * ld + kq, src + rc[r] + ko);
+#pragma unroll 8
+        for (int r = pw * 4 + sub; r < nr; r += 16) cp_async_16(dst + r * ld + kq, src + rc[r] + koq[0]);
       } else {
-        for (int e = 0; e < 4 && kq + e < kn; ++e) {
-          const int64_t ko = __ldg(gk + kq + e);
-          for (int r = pw * 4 + sub; r < nr; r += 16)
-            cp_async_elem<4>(dst + r * ld + kq + e, src + rc[r] + ko);
-        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (kq + e < kn)
+            for (int r = pw * 4 + sub; r < nr; r += 16)
+              cp_async_elem<4>(dst + r * ld + kq + e, src + rc[r] + koq[e]);
       }
     }
   }
