@@ -640,6 +640,13 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
   p->simt = choose_simt(p);
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
+  if (!simt_path(p) && p->tune.load == 2 && p->prec == TCCG_PREC_BF16X3 && p->dtype == TCCG_F32 &&
+      p->tune.method == TCCG_METHOD_GETT && !p->tune.pair && p->tune.tile_n != 0 &&
+      p->tune.tile_n != 128) {
+    const int32_t tn = p->tune.tile_n;
+    plan_free(p);
+    return fail(TCCG_ERR_UNSUPPORTED, "the gather loader has 128-column tiles (tile_n %d)", tn);
+  }
   if (!simt_path(p) && choose_gather(p)) {
     // gather schedules: 16-byte k quads, else along the operand's faster
     // direction (k or rows)
