@@ -449,28 +449,42 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
     }
     __syncthreads();
     if (a.crun > 0) {
-      // lane (i, j) = (lane % e0, lane / e0) of warp w stores element
-      // (run start + i, column block start + j) for every (run, column
-      // block) pair w, w + 8, ...: one store instruction covers q columns
-      // of a run of e0 consecutive m, consecutive addresses of C. Same
-      // arithmetic as the quad path (alpha * acc, then fma with beta).
-      const int e0 = a.crun, qn = 32 / e0;
+      // runs of e0 consecutive m (clipped to the tile and M, length L), one
+      // per warp at a time: the run's L x ncols block is stored in C's
+      // address order, element f = i + L * j (row ma + i, column j) by lane
+      // f % 32, so a store instruction covers 32 consecutive positions of
+      // one contiguous stretch of C. Same arithmetic as the quad path
+      // (alpha * acc, then fma with beta).
+      const int e0 = a.crun;
       const int lane = tid & 31, w = tid >> 5;
-      const int i = lane % e0, jj = lane / e0;
-      if (jj < qn) {
-        const int64_t rfirst = (m0 / e0) * e0;
-        const int nruns = (int)((m0 + BM - rfirst + e0 - 1) / e0);
-        const int ncb = (EPN + qn - 1) / qn;
+      const int64_t rfirst = (m0 / e0) * e0;
+      const int nruns = (int)((m0 + BM - rfirst + e0 - 1) / e0);
+      const int64_t nleft = a.N - (n0 + p * EPN);
+      const int ncols = nleft < EPN ? (int)nleft : EPN;
 #pragma unroll 1
-        for (int u = w; u < nruns * ncb; u += 8) {
-          const int ri = u % nruns, cb = u / nruns;
-          const int64_t m = rfirst + (int64_t)ri * e0 + i;
-          const int nl = cb * qn + jj;
-          if (m < m0 || m >= m0 + BM || m >= a.M || nl >= EPN || n0 + p * EPN + nl >= a.N) continue;
-          T* d = a.C + a.c_m_off[m] + Cn[nl];
-          T v = alpha * Cs[nl * LDC + (int)(m - m0)];
+      for (int ri = w; ri < nruns; ri += 8) {
+        const int64_t rs = rfirst + (int64_t)ri * e0;
+        const int64_t ma = rs > m0 ? rs : m0;
+        int64_t mb = rs + e0 < m0 + BM ? rs + e0 : m0 + BM;
+        if (mb > a.M) mb = a.M;
+        const int L = (int)(mb - ma);
+        if (L <= 0 || ncols <= 0) continue;
+        const int total = L * ncols;
+        int i = lane % L, j = lane / L;
+        const int di = 32 % L, dj = 32 / L;
+        const int moff = (int)(ma - m0);
+#pragma unroll 1
+        for (int f = lane; f < total; f += 32) {
+          T* d = a.C + a.c_m_off[ma + i] + Cn[j];
+          T v = alpha * Cs[j * LDC + moff + i];
           if (beta != T(0)) v = fma(beta, *d, v);
           *d = v;
+          i += di;
+          j += dj;
+          if (i >= L) {
+            i -= L;
+            ++j;
+          }
         }
       }
     } else if (mok[0]) {

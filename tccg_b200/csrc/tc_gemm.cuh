@@ -254,27 +254,38 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
 
 // Staged C store of one epilogue warp (TcArgs::crun = e0): stg holds the
 // warp's 32 rows (m0 ...) x ncols <= 16 columns (nb ...) as [column][row], 33
-// floats per column. Lane (i, j) = (lane % e0, lane / e0) stores element
-// (run start + i, column j + q*k), q = 32 / e0: one store instruction covers
-// q consecutive columns of a run of e0 consecutive m, consecutive addresses
-// of C. Same arithmetic as the register epilogue (alpha*acc, fmaf with beta).
+// floats per column. For each run of e0 consecutive m (clipped to the warp's
+// rows and to M, length L) the block of L x ncols elements is stored in C's
+// address order, element f = i + L * j (row ma + i, column j) by lane f % 32:
+// a store instruction covers 32 consecutive positions of the block -- one
+// contiguous stretch of C for a whole run. The lanes step (i, j) by 32
+// positions without dividing. Same arithmetic as the register epilogue
+// (alpha * acc, fmaf with beta).
 __device__ __forceinline__ void store_runs(const float* stg, const TcArgs& a, int64_t m0,
                                            int64_t nb, int ncols, int e0, float alpha, float beta,
                                            int lane) {
-  const int q = 32 / e0;
-  const int i = lane % e0, j = lane / e0;
-  if (j >= q) return;
 #pragma unroll 1
   for (int64_t rs = (m0 / e0) * e0; rs < m0 + 32; rs += e0) {
-    const int64_t m = rs + i;
-    if (m < m0 || m >= m0 + 32 || m >= a.M) continue;
-    const int64_t cmo = a.c_m_off[m];
-    const float* col = stg + (m - m0);
+    const int64_t ma = rs > m0 ? rs : m0;
+    int64_t mb = rs + e0 < m0 + 32 ? rs + e0 : m0 + 32;
+    if (mb > a.M) mb = a.M;
+    const int L = (int)(mb - ma);
+    if (L <= 0) continue;  // warp-uniform
+    const int total = L * ncols;
+    int i = lane % L, j = lane / L;
+    const int di = 32 % L, dj = 32 / L;
+    const int moff = (int)(ma - m0);
 #pragma unroll 1
-    for (int c = j; c < ncols; c += q) {
-      float* dst = a.C + cmo + __ldg(a.c_n_off + nb + c);
-      const float v = alpha * col[c * 33];
+    for (int f = lane; f < total; f += 32) {
+      float* dst = a.C + a.c_m_off[ma + i] + __ldg(a.c_n_off + nb + j);
+      const float v = alpha * stg[j * 33 + moff + i];
       *dst = beta != 0.0f ? fmaf(beta, *dst, v) : v;
+      i += di;
+      j += dj;
+      if (i >= L) {
+        i -= L;
+        ++j;
+      }
     }
   }
 }
