@@ -121,7 +121,10 @@ template <typename T, int S = SIMT_SQUARE>
 constexpr size_t simt_smem_bytes() {
   using Cfg = SimtCfg<T, S>;
   size_t pipe = (size_t)Cfg::STAGES * Cfg::BK * (Cfg::LDA + Cfg::LDB) * sizeof(T);
-  size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T) + Cfg::EPN * sizeof(int64_t);
+  // epilogue: the C tile (one pass of EPN columns), C offsets of the pass's
+  // columns and of the tile's rows
+  size_t epi = (size_t)Cfg::EPN * (Cfg::BM + Cfg::PAD) * sizeof(T) +
+               (Cfg::EPN + Cfg::BM) * sizeof(int64_t);
   return pipe > epi ? pipe : epi;
 }
 
@@ -422,7 +425,10 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
   // C offsets of the pass's columns, staged once: the C loads of a chunk then
   // depend on shared memory only, not on a table load from L2
   int64_t* Cn = reinterpret_cast<int64_t*>(smem_raw + (size_t)EPN * LDC * sizeof(T));
+  int64_t* Cm = Cn + EPN;  // C offsets of the tile's rows (staged C stores)
   static_assert((EPN * LDC * sizeof(T)) % 8 == 0 && EPN <= 256, "column offset staging");
+  if (a.crun > 0)
+    for (int r = tid; r < BM; r += 256) Cm[r] = m0 + r < a.M ? a.c_m_off[m0 + r] : 0;
   const int q = tid % QPC, cl = tid / QPC;
   const int64_t mq = m0 + 4 * q;
   int64_t cmo[4];
@@ -453,8 +459,9 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
       // per warp at a time: the run's L x ncols block is stored in C's
       // address order, element f = i + L * j (row ma + i, column j) by lane
       // f % 32, so a store instruction covers 32 consecutive positions of
-      // one contiguous stretch of C. Same arithmetic as the quad path
-      // (alpha * acc, then fma with beta).
+      // one contiguous stretch of C; the C offsets of rows and columns come
+      // from shared memory. Same arithmetic as the quad path (alpha * acc,
+      // then fma with beta).
       const int e0 = a.crun;
       const int lane = tid & 31, w = tid >> 5;
       const int64_t rfirst = (m0 / e0) * e0;
@@ -473,9 +480,9 @@ __device__ __forceinline__ void simt_gett_tile(const SimtArgs<T>& a, int bx, int
         int i = lane % L, j = lane / L;
         const int di = 32 % L, dj = 32 / L;
         const int moff = (int)(ma - m0);
-#pragma unroll 1
+#pragma unroll 2
         for (int f = lane; f < total; f += 32) {
-          T* d = a.C + a.c_m_off[ma + i] + Cn[j];
+          T* d = a.C + Cm[moff + i] + Cn[j];
           T v = alpha * Cs[j * LDC + moff + i];
           if (beta != T(0)) v = fma(beta, *d, v);
           *d = v;

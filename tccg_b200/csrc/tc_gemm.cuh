@@ -253,33 +253,40 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
 }
 
 // Staged C store of one epilogue warp (TcArgs::crun = e0): stg holds the
-// warp's 32 rows (m0 ...) x ncols <= 16 columns (nb ...) as [column][row], 33
-// floats per column. For each run of e0 consecutive m (clipped to the warp's
-// rows and to M, length L) the block of L x ncols elements is stored in C's
-// address order, element f = i + L * j (row ma + i, column j) by lane f % 32:
-// a store instruction covers 32 consecutive positions of the block -- one
-// contiguous stretch of C for a whole run. The lanes step (i, j) by 32
-// positions without dividing. Same arithmetic as the register epilogue
-// (alpha * acc, fmaf with beta).
+// warp's 32 rows (m0 ...) x ncols <= 16 columns as [column][row], 33 floats
+// per column; cm_lane / cn_lane are C's offsets of row m0 + lane and of
+// column lane (lane < ncols) of the block, passed around by warp shuffles (no
+// memory access on the store path). For each run of e0 consecutive m
+// (clipped to the warp's rows and to M, length L) the block of L x ncols
+// elements is stored in C's address order, element f = i + L * j (row ma +
+// i, column j) by lane f % 32: a store instruction covers 32 consecutive
+// positions of the block -- one contiguous stretch of C for a whole run.
+// Every lane runs the same number of steps (the shuffles need the whole
+// warp), stepping (i, j) by 32 positions without dividing. Same arithmetic
+// as the register epilogue (alpha * acc, fmaf with beta).
 __device__ __forceinline__ void store_runs(const float* stg, const TcArgs& a, int64_t m0,
-                                           int64_t nb, int ncols, int e0, float alpha, float beta,
-                                           int lane) {
+                                           int ncols, int e0, float alpha, float beta, int lane,
+                                           int64_t cm_lane, int64_t cn_lane) {
+  int64_t mlim = a.M - m0;  // rows of this warp inside M
+  if (mlim > 32) mlim = 32;
 #pragma unroll 1
-  for (int64_t rs = (m0 / e0) * e0; rs < m0 + 32; rs += e0) {
-    const int64_t ma = rs > m0 ? rs : m0;
-    int64_t mb = rs + e0 < m0 + 32 ? rs + e0 : m0 + 32;
-    if (mb > a.M) mb = a.M;
-    const int L = (int)(mb - ma);
+  for (int rs = (int)((m0 / e0) * e0 - m0); rs < (int)mlim; rs += e0) {  // run starts, warp-relative
+    const int ma = rs > 0 ? rs : 0;
+    const int mb = rs + e0 < (int)mlim ? rs + e0 : (int)mlim;
+    const int L = mb - ma;
     if (L <= 0) continue;  // warp-uniform
     const int total = L * ncols;
     int i = lane % L, j = lane / L;
     const int di = 32 % L, dj = 32 / L;
-    const int moff = (int)(ma - m0);
-#pragma unroll 1
-    for (int f = lane; f < total; f += 32) {
-      float* dst = a.C + a.c_m_off[ma + i] + __ldg(a.c_n_off + nb + j);
-      const float v = alpha * stg[j * 33 + moff + i];
-      *dst = beta != 0.0f ? fmaf(beta, *dst, v) : v;
+#pragma unroll 2
+    for (int f0 = 0; f0 < total; f0 += 32) {
+      const int64_t cm = __shfl_sync(0xffffffffu, cm_lane, (ma + i) & 31);
+      const int64_t cn = __shfl_sync(0xffffffffu, cn_lane, j & 31);
+      if (f0 + lane < total) {
+        float* dst = a.C + cm + cn;
+        const float v = alpha * stg[j * 33 + ma + i];
+        *dst = beta != 0.0f ? fmaf(beta, *dst, v) : v;
+      }
       i += di;
       j += dj;
       if (i >= L) {
@@ -294,20 +301,41 @@ __device__ __forceinline__ void store_runs(const float* stg, const TcArgs& a, in
 // The producer warps walk this CTA's (tile, k-block) jobs in the order the MMA
 // warp consumes them, twice: copies run STG_SLOTS - 1 jobs ahead of the
 // conversion into MMA stages.
+// The fields a job's copies and conversion use are read from the kernel
+// arguments once per tile, into registers (the copy loops then touch no
+// argument memory).
 struct GatherJob {
   int tile, kb;
   bool valid;
   TileRef t;
+  int K;
+  const float* src[2];
+  const int64_t* gk[2];
+  int read[2];
+  int nr[2];       // rows of the tile inside the operand (0..128)
+  int64_t r0[2];   // first row of the tile
 };
 
-template <bool GROUPED>
+template <int BM, int BN, bool GROUPED>
 __device__ __forceinline__ void gjob_seek(GatherJob& j, int num_tiles, const TcArgs* a1,
                                           const TcGroup& g) {
   while (j.tile < num_tiles) {
     j.t = resolve_tile<GROUPED>(j.tile, nullptr, nullptr, a1, g);
     if (j.t.kb_begin < j.t.kb_end) {
+      const TcArgs& a = *j.t.a;
       j.kb = j.t.kb_begin;
       j.valid = true;
+      j.K = a.K;
+#pragma unroll
+      for (int o = 0; o < 2; ++o) {
+        j.src[o] = a.gsrc[o];
+        j.gk[o] = a.gk[o];
+        j.read[o] = a.gread[o];
+        const int64_t R = o ? a.N : a.M;
+        j.r0[o] = o ? (int64_t)j.t.tn * BN : (int64_t)j.t.tm * BM;
+        const int rows = o ? BN : BM;
+        j.nr[o] = R - j.r0[o] < rows ? (int)(R - j.r0[o]) : rows;
+      }
       return;
     }
     j.tile += gridDim.x;
@@ -315,12 +343,12 @@ __device__ __forceinline__ void gjob_seek(GatherJob& j, int num_tiles, const TcA
   j.valid = false;
 }
 
-template <bool GROUPED>
+template <int BM, int BN, bool GROUPED>
 __device__ __forceinline__ void gjob_next(GatherJob& j, int num_tiles, const TcArgs* a1,
                                           const TcGroup& g) {
   if (++j.kb < j.t.kb_end) return;
   j.tile += gridDim.x;
-  gjob_seek<GROUPED>(j, num_tiles, a1, g);
+  gjob_seek<BM, BN, GROUPED>(j, num_tiles, a1, g);
 }
 
 // Staging row stride of an operand (floats): 33 for copies along rows (the 32
@@ -363,25 +391,21 @@ __device__ __forceinline__ void gather_rows(const GatherJob& j, int64_t* rowc, i
 template <int BM, int BN>
 __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, const int64_t* rowc,
                                              int ptid) {
-  const TcArgs& a = *j.t.a;
   const int pw = ptid >> 5, lane = ptid & 31;
   const int k0 = j.kb * 32;
-  const int kn = a.K - k0 < 32 ? a.K - k0 : 32;  // k of this block inside K
-#pragma unroll 1
+  const int kn = j.K - k0 < 32 ? j.K - k0 : 32;  // k of this block inside K
+#pragma unroll
   for (int o = 0; o < 2; ++o) {
-    const float* src = a.gsrc[o];
-    const int64_t R = o ? a.N : a.M;
-    const int64_t r0 = o ? (int64_t)j.t.tn * BN : (int64_t)j.t.tm * BM;
-    const int rows = o ? BN : BM;
-    const int nr = R - r0 < rows ? (int)(R - r0) : rows;
+    const float* src = j.src[o];
+    const int nr = j.nr[o];
     const int64_t* rc = rowc + (o ? BM : 0);
-    const int read = a.gread[o];
+    const int read = j.read[o];
     const int ld = gather_ld(read);
     float* dst = slot + (o ? BM * 36 : 0);
     // k offset of k = lane (0 past K)
-    const int64_t ko_lane = lane < kn ? __ldg(a.gk[o] + k0 + lane) : 0;
+    const int64_t ko_lane = lane < kn ? __ldg(j.gk[o] + k0 + lane) : 0;
     if (read == GATHER_ROWS) {
-      // lanes along rows: thread ptid copies rows ptid (and ptid + 128)
+      // lanes along rows: thread ptid copies row ptid (every tile has <= 128 rows)
       const int r = ptid;
       const bool ok = r < nr;
       const float* srow = src + (ok ? rc[r] : 0);
@@ -390,17 +414,6 @@ __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, co
       for (int k = 0; k < 32; ++k) {
         const int64_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
         if (ok && k < kn) cp_async_elem<4>(drow + k, srow + ko);
-      }
-      if (rows > 128) {
-        const int r2 = ptid + 128;
-        const bool ok2 = r2 < nr;
-        const float* srow2 = src + (ok2 ? rc[r2] : 0);
-        float* drow2 = dst + r2 * ld;
-#pragma unroll 8
-        for (int k = 0; k < 32; ++k) {
-          const int64_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
-          if (ok2 && k < kn) cp_async_elem<4>(drow2 + k, srow2 + ko);
-        }
       }
     } else if (read == GATHER_K) {
       if (lane < kn) {
@@ -434,47 +447,49 @@ __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, co
 template <int BM, int BN>
 __device__ __forceinline__ void gather_convert(const GatherJob& j, const float* slot, uint8_t* stA,
                                                uint8_t* stB, int ptid) {
-  const TcArgs& a = *j.t.a;
   const int pw = ptid >> 5, lane = ptid & 31;
   const int k0 = j.kb * 32;
-  const int kn = a.K - k0 < 32 ? a.K - k0 : 32;
+  const int kn = j.K - k0 < 32 ? j.K - k0 : 32;
   const int k8 = lane >> 3;
+#pragma unroll
+  for (int o = 0; o < 2; ++o) {
+    const int ld = gather_ld(j.read[o]);
+    const int nr = j.nr[o];
+    const float* sop = slot + (o ? BM * 36 : 0);
+    uint8_t* stage = o ? stB : stA;
+    constexpr int GROUPS = 16;  // 8-row groups per operand (128 rows)
 #pragma unroll 1
-  for (int rg = pw; rg < (BM + BN) / 8; rg += 4) {
-    const int r = rg * 8 + (lane & 7);
-    const int o = r >= BM;
-    const int rr = r - (o ? BM : 0);
-    const int64_t R = o ? a.N : a.M;
-    const int64_t r0 = o ? (int64_t)j.t.tn * BN : (int64_t)j.t.tm * BM;
-    const bool row_ok = r0 + rr < R;
-    const int ld = gather_ld(a.gread[o]);
-    const float* srow = slot + (o ? BM * 36 : 0) + rr * ld + k8 * 8;
-    float v[8];
-    if (ld == 36) {
-      const float4 x0 = *reinterpret_cast<const float4*>(srow);
-      const float4 x1 = *reinterpret_cast<const float4*>(srow + 4);
-      v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
-      v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
-    } else {
+    for (int rg = pw; rg < GROUPS; rg += 4) {
+      const int rr = rg * 8 + (lane & 7);
+      const bool row_ok = rr < nr;
+      const float* srow = sop + rr * ld + k8 * 8;
+      float v[8];
+      if (ld == 36) {
+        const float4 x0 = *reinterpret_cast<const float4*>(srow);
+        const float4 x1 = *reinterpret_cast<const float4*>(srow + 4);
+        v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
+        v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
+      } else {
 #pragma unroll
-      for (int e = 0; e < 8; ++e) v[e] = srow[e];
-    }
-    uint32_t hw[4], lw[4];
+        for (int e = 0; e < 8; ++e) v[e] = srow[e];
+      }
+      uint32_t hw[4], lw[4];
 #pragma unroll
-    for (int e = 0; e < 8; e += 2) {
-      const float x0 = (row_ok && k8 * 8 + e < kn) ? v[e] : 0.0f;
-      const float x1 = (row_ok && k8 * 8 + e + 1 < kn) ? v[e + 1] : 0.0f;
-      const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-      const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-      const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-      const __nv_bfloat162 hp = __halves2bfloat162(h0, h1), lp = __halves2bfloat162(l0, l1);
-      hw[e / 2] = *reinterpret_cast<const uint32_t*>(&hp);
-      lw[e / 2] = *reinterpret_cast<const uint32_t*>(&lp);
+      for (int e = 0; e < 8; e += 2) {
+        const float x0 = (row_ok && k8 * 8 + e < kn) ? v[e] : 0.0f;
+        const float x1 = (row_ok && k8 * 8 + e + 1 < kn) ? v[e + 1] : 0.0f;
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+        const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+        const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+        const __nv_bfloat162 hp = __halves2bfloat162(h0, h1), lp = __halves2bfloat162(l0, l1);
+        hw[e / 2] = *reinterpret_cast<const uint32_t*>(&hp);
+        lw[e / 2] = *reinterpret_cast<const uint32_t*>(&lp);
+      }
+      uint8_t* drow = stage + rr * 128;
+      const int sw = rr & 7;
+      *reinterpret_cast<uint4*>(drow + ((k8 ^ sw) << 4)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(drow + (((4 + k8) ^ sw) << 4)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
-    uint8_t* drow = (o ? stB : stA) + rr * 128;
-    const int sw = rr & 7;
-    *reinterpret_cast<uint4*>(drow + ((k8 ^ sw) << 4)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-    *reinterpret_cast<uint4*>(drow + (((4 + k8) ^ sw) << 4)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
   }
 }
 
@@ -491,8 +506,8 @@ __device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup&
   const int ptid = threadIdx.x;                  // 0..127
   GatherJob ji, jc;                              // issue / conversion iterators
   ji.tile = jc.tile = blockIdx.x;
-  gjob_seek<GROUPED>(ji, num_tiles, a1, g);
-  gjob_seek<GROUPED>(jc, num_tiles, a1, g);
+  gjob_seek<Cfg::BM, Cfg::BN, GROUPED>(ji, num_tiles, a1, g);
+  gjob_seek<Cfg::BM, Cfg::BN, GROUPED>(jc, num_tiles, a1, g);
   int cached = -1;  // tile whose row offsets are in rowc
   auto issue = [&](int slot) {
     if (ji.valid) {
@@ -503,7 +518,7 @@ __device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup&
         cached = ji.tile;
       }
       gather_issue<Cfg::BM, Cfg::BN>(ji, stg + slot * SLOT, rowc, ptid);
-      gjob_next<GROUPED>(ji, num_tiles, a1, g);
+      gjob_next<Cfg::BM, Cfg::BN, GROUPED>(ji, num_tiles, a1, g);
     }
     cp_async_commit();  // one group per job (empty past the last), so waits count jobs
   };
@@ -535,7 +550,7 @@ __device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup&
       stage = 0;
       phase ^= 1;
     }
-    gjob_next<GROUPED>(jc, num_tiles, a1, g);
+    gjob_next<Cfg::BM, Cfg::BN, GROUPED>(jc, num_tiles, a1, g);
   }
   cp_async_wait<0>();  // no copy in flight when the producers leave
 }
@@ -784,8 +799,10 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
                 for (int j = 0; j < 16; ++j) wstg[j * Cfg::EPI_LD + lane] = __uint_as_float(r[hh + j]);
                 __syncwarp();
                 const int64_t left = nlim - cc - hh;
-                store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, n0 + cc + hh,
-                           left < 16 ? (int)left : 16, a.crun, alpha, beta, lane);
+                const int64_t cn_lane =
+                    lane < 16 && cc + hh + lane < nlim ? __ldg(a.c_n_off + n0 + cc + hh + lane) : 0;
+                store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, left < 16 ? (int)left : 16,
+                           a.crun, alpha, beta, lane, cmo, cn_lane);
               }
             }
           } else if (m_ok) {
@@ -857,8 +874,10 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
               for (int j = 0; j < 16; ++j) wstg[j * Cfg::EPI_LD + lane] = sum[cc + j];
               __syncwarp();
               const int64_t left = nlim - cc;
-              store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, n0 + cc,
-                         left < 16 ? (int)left : 16, a.crun, alpha, beta, lane);
+              const int64_t cn_lane =
+                  lane < 16 && cc + lane < nlim ? __ldg(a.c_n_off + n0 + cc + lane) : 0;
+              store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, left < 16 ? (int)left : 16,
+                         a.crun, alpha, beta, lane, cmo, cn_lane);
             }
           }
         } else if (m_ok) {

@@ -247,9 +247,12 @@ static double tc_time(const tccg_plan* p, bool gather) {
                   cb / 3e12 + (gather ? 1.0 : 3.0) * op / 4.5e12);
 }
 
+// The gather loader runs only when asked for (tuning.load = 2, which the
+// autotuner tries): measured on the 256-item batched workload, its producer
+// warps bring in 0.3-0.7 TB/s per kernel where the packing pass plus TMA
+// loads move operands at 3-5 TB/s, so the model never picks it.
 static bool choose_gather(const tccg_plan* p) {
-  if (!gather_eligible(p)) return false;
-  return p->tune.load == 2 || tc_time(p, true) < tc_time(p, false);
+  return p->tune.load == 2 && gather_eligible(p);
 }
 
 static bool choose_simt(const tccg_plan* p) {
@@ -265,8 +268,7 @@ static bool choose_simt(const tccg_plan* p) {
   const int shape = choose_simt_shape(p, &simt_work);
   const double simt_passes = direct_eligible(p, shape) ? 1.0 : 3.0;  // operand reads
   const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
-  double t_tc = tc_time(p, false);
-  if (gather_eligible(p)) t_tc = std::min(t_tc, tc_time(p, true));
+  double t_tc = tc_time(p, p->tune.load == 2 && gather_eligible(p));
   const double t_simt = std::max(2.0 * simt_work * K / 35e12, (cb + simt_passes * op) / 4.5e12);
   return t_simt < t_tc;
 }
