@@ -391,6 +391,7 @@ __device__ __forceinline__ void gather_rows(const GatherJob& j, int64_t* rowc, i
 template <int BM, int BN>
 __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, const int64_t* rowc,
                                              int ptid) {
+  static_assert(BM == 128 && BN == 128, "one row per producer thread along rows");
   const int pw = ptid >> 5, lane = ptid & 31;
   const int k0 = j.kb * 32;
   const int kn = j.K - k0 < 32 ? j.K - k0 : 32;  // k of this block inside K
@@ -447,6 +448,7 @@ __device__ __forceinline__ void gather_issue(const GatherJob& j, float* slot, co
 template <int BM, int BN>
 __device__ __forceinline__ void gather_convert(const GatherJob& j, const float* slot, uint8_t* stA,
                                                uint8_t* stB, int ptid) {
+  static_assert(BM == 128 && BN == 128, "the conversion walks 16 groups of 8 rows per operand");
   const int pw = ptid >> 5, lane = ptid & 31;
   const int k0 = j.kb * 32;
   const int kn = j.K - k0 < 32 ? j.K - k0 : 32;
