@@ -141,6 +141,13 @@ struct TcArgs {
   float* tail_partial;
   // Bound of every mbarrier wait of the launch (0 = TCCG_DEVICE_WAIT_NS).
   uint64_t wait_ns;
+  // Position of a CTA in the tile order: 0 = its launch index (blockIdx.x);
+  // 1 = the SM it runs on (%smid), when the grid has one CTA per SM id
+  // (%nsmid == gridDim.x, so the ids are exactly 0 .. grid-1). With the SM
+  // order, consecutive tiles -- which share operand rows -- run on
+  // consecutive SMs whatever order the CTAs were launched in (programmatic
+  // dependent launch places them as the previous kernel frees SMs).
+  int32_t sm_order;
   // Testing of the abort path (0 = off): the producer does not load the
   // first k-block of tile skip_tile1 - 1, so the MMA warp's wait for it runs
   // out and the CTA winds down with a status code.
@@ -498,7 +505,7 @@ __device__ __forceinline__ void gather_convert(const GatherJob& j, const float* 
 // The four producer warps of the gather variant.
 template <int MODE, bool GROUPED>
 __device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup& g, int num_tiles,
-                                                uint8_t* sA, uint8_t* sB, float* stg,
+                                                int cta, uint8_t* sA, uint8_t* sB, float* stg,
                                                 int64_t* rowc, uint64_t* full, uint64_t* empty,
                                                 uint64_t wait_ns, int skip_tile1,
                                                 int32_t* status) {
@@ -507,7 +514,7 @@ __device__ __forceinline__ void gather_producer(const TcArgs* a1, const TcGroup&
   constexpr int SLOT = Cfg::STG_SLOT_BYTES / 4;  // floats per staging slot
   const int ptid = threadIdx.x;                  // 0..127
   GatherJob ji, jc;                              // issue / conversion iterators
-  ji.tile = jc.tile = blockIdx.x;
+  ji.tile = jc.tile = cta;
   gjob_seek<Cfg::BM, Cfg::BN, GROUPED>(ji, num_tiles, a1, g);
   gjob_seek<Cfg::BM, Cfg::BN, GROUPED>(jc, num_tiles, a1, g);
   int cached = -1;  // tile whose row offsets are in rowc
@@ -592,6 +599,13 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
                      : a1->tiles_m * a1->tiles_n * a1->ksplit);
   const uint64_t wait_ns = (GROUPED || a1->wait_ns == 0) ? TCCG_DEVICE_WAIT_NS : a1->wait_ns;
   const int skip_tile1 = GROUPED ? 0 : a1->skip_tile1;
+  int cta = (int)blockIdx.x;  // position in the tile order (TcArgs::sm_order)
+  if (!GROUPED && a1->sm_order) {
+    uint32_t smid, nsmid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsmid));
+    if (nsmid == gridDim.x) cta = (int)smid;
+  }
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -621,8 +635,8 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
   if (Cfg::GATHER && warp < Cfg::PRODUCER_WARPS) {
     // ---------------- gather producers (4 warps) ----------------
     if constexpr (Cfg::GATHER)
-      gather_producer<MODE, GROUPED>(a1, g, num_tiles, sA, sB, stg, rowc, full, empty, wait_ns,
-                                     skip_tile1, status);
+      gather_producer<MODE, GROUPED>(a1, g, num_tiles, cta, sA, sB, stg, rowc, full, empty,
+                                     wait_ns, skip_tile1, status);
   } else if (!Cfg::GATHER && warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
     int stage = 0;
@@ -630,7 +644,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     int issued_phase[Cfg::STAGES];
     for (int s = 0; s < Cfg::STAGES; ++s) issued_phase[s] = -1;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+    for (int tile = cta; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
       for (int kb = t.kb_begin; kb < t.kb_end; ++kb) {
         if (!mbar_wait(&empty[stage], phase ^ 1, wait_ns)) {
@@ -661,7 +675,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true, issued_any = false;
-    for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+    for (int tile = cta; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
       const int nkb = t.kb_end, K = t.a->K, ckb = t.a->chunk_kb;
       // the MMAs stop at the tile's last column of C, rounded up to 32 (the
@@ -738,7 +752,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+    for (int tile = cta; tile < num_tiles && ok; tile += gridDim.x) {
       const TileRef t = resolve_tile<GROUPED>(tile, tmA, tmB, a1, g);
       const TcArgs& a = *t.a;
       const int64_t m = (int64_t)t.tm * Cfg::BM + q * 32 + lane;

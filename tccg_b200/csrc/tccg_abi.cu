@@ -1339,6 +1339,14 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   return rc;
 }
 
+// Tile order of the persistent tcgen05 grid by SM (TcArgs::sm_order): on,
+// unless TCCG_B200_CTA_ORDER=launch in the environment selects the launch
+// order (for comparisons).
+static bool sm_order_enabled() {
+  const char* e = std::getenv("TCCG_B200_CTA_ORDER");
+  return !(e && std::strcmp(e, "launch") == 0);
+}
+
 // Arguments of the tcgen05 kernels common to both loaders (k-split partial
 // sums and tail slices in the workspace `ws`).
 static TcArgs tc_args(const tccg_plan* p, float* Cout, const int64_t* c_m, const int64_t* c_n,
@@ -1366,6 +1374,7 @@ static TcArgs tc_args(const tccg_plan* p, float* Cout, const int64_t* c_m, const
   a.tail_kb = p->tail_kb;
   a.tail_partial = p->tail_split > 1 ? reinterpret_cast<float*>(ws + p->off_tail) : nullptr;
   a.crun = c_m == p->t_c_m ? p->crun : 0;  // not for TTGT's contiguous C'
+  a.sm_order = sm_order_enabled() ? 1 : 0;
   return a;
 }
 

@@ -123,3 +123,36 @@ def test_describe_reports_the_launch(cuda, monkeypatch):
     assert "launch=dependent" in big.describe()
     monkeypatch.setenv("TCCG_B200_PDL", "0")
     assert "launch=plain" in small.describe()
+
+
+@pytest.mark.parametrize("name,pdl", [("tc_x3", "1"), ("tc_x3", "0"), ("tc_bf16", "1"),
+                                      ("tc_tail", "1")])
+def test_sm_tile_order_bitwise(cuda, monkeypatch, name, pdl):
+    """The persistent tcgen05 grid takes tiles in SM order (%smid, when the
+    grid has one CTA per SM id) or in launch order
+    (TCCG_B200_CTA_ORDER=launch): the same tiles with the same sums, only on
+    other SMs -- bitwise equal, with and without dependent launch. The
+    shapes are widened so that the grid fills every SM for several rounds."""
+    import torch
+    lc, la, lb, sizes, beta, precision, tuning, tag = CASES[name]
+    big = dict(sizes, m=sizes["m"] * 8, n=sizes["n"] * 2)
+    con = make_contraction(lc, la, lb, big, 1.25, beta)
+    ln = LoopNest(lc, la, lb, big)
+    A = seeded_normal(ln.size_a, 5).astype(np.float32)
+    B = seeded_normal(ln.size_b, 6).astype(np.float32)
+    C = seeded_normal(ln.size_c, 7).astype(np.float32)
+    if precision == "bf16":
+        A = torch.from_numpy(A).bfloat16().float().numpy()
+        B = torch.from_numpy(B).bfloat16().float().numpy()
+    p = Plan(con, precision=precision, tuning=tuning)
+    assert "grid=148" in p.describe() or "grid=" in p.describe()
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    ws = torch.empty(max(p.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    monkeypatch.setenv("TCCG_B200_PDL", pdl)
+    outs = []
+    for order in ("sm", "launch"):
+        monkeypatch.setenv("TCCG_B200_CTA_ORDER", order)
+        outs.append(_run(p, dA, dB, C, ws))
+    assert np.array_equal(outs[0], outs[1])
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), 1.25, beta)
+    assert error_metrics(outs[0], ref)["normwise"] <= 1e-5
