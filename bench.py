@@ -801,6 +801,67 @@ def _suite_cfg5(out, gen, flush, dev):
     return out
 
 
+CASES = {
+    "cfg1": SUITE["cfg1"],
+    "cfg2": SUITE["cfg2"],
+    # configuration 2 with C's indices permuted against the GEMM's [M][N]
+    # order: TTGT then transposes C' into C (the permute kernel)
+    "cfg2t": "C[a,c,b,d] = A[a,e,b] * B[e,d,c] + C[a,c,b,d]\na=96\nb=96\nc=96\nd=96\ne=16\n",
+    "cfg3k2": workload(2),
+    "cfg3k4": workload(4),
+    "cfg3k8": workload(8),
+    "cfg4": SUITE["cfg4"],
+}
+
+
+def run_case(args):
+    """One named workload run a few times with no timing, for profiler
+    captures (ncu -k <kernel> -c <n> python bench.py --case ...):
+    configurations by name (cfg3kN: configuration 3's C slab k < N),
+    cfg5:N (the first N items of configuration 5 as one grouped run) or
+    item:I (item I of configuration 5 alone)."""
+    import torch
+    from tccg_b200 import parse_text
+    from tccg_b200.api import Compiled
+    from tccg_b200.plan import Plan, Tuning
+    from tccg_b200.workloads import batched_workload
+    dev = torch.device("cuda", 0)
+    tune = {}
+    for kv in filter(None, args.tuning.split(",")):
+        k, v = kv.split("=")
+        tune[k] = v if k == "method" else int(v)
+    t = Tuning(**tune)
+    g = torch.Generator(device=dev).manual_seed(5)
+    if args.case.startswith("cfg5:"):
+        from tccg_b200.grouped import Group
+        items = batched_workload(int(args.case.split(":")[1]), seed=0)
+        As = [torch.randn(c.A0.num_elements(), generator=g, device=dev) for c in items]
+        Bs = [torch.randn(c.B0.num_elements(), generator=g, device=dev) for c in items]
+        Cs = [torch.empty(c.C0.num_elements(), device=dev) for c in items]
+        grp = Group(items, args.precision, tunings=[t] * len(items) if tune else None)
+        grp.bind(As, Bs, Cs)
+        for _ in range(args.runs):
+            grp.run()
+        torch.cuda.synchronize()
+        print("case %s: %d items" % (args.case, len(items)), flush=True)
+        return 0
+    con = (batched_workload(int(args.case.split(":")[1]) + 1, seed=0)[-1]
+           if args.case.startswith("item:") else parse_text(CASES[args.case]))
+    dt = "bf16" if args.precision == "bf16" else None
+    c = Compiled(con, args.precision, t, dtype=dt)
+    tdt = {"fp32": torch.float32, "bf16x3": torch.float32, "bf16": torch.bfloat16,
+           "fp64": torch.float64}[args.precision]
+    A = torch.randn(con.A0.num_elements(), generator=g, device=dev).to(tdt)
+    B = torch.randn(con.B0.num_elements(), generator=g, device=dev).to(tdt)
+    C = torch.randn(con.C0.num_elements(), generator=g, device=dev).to(
+        torch.float64 if args.precision == "fp64" else torch.float32)
+    for _ in range(args.runs):
+        c(A, B, C)
+    torch.cuda.synchronize()
+    print("case %s %s: %s" % (args.case, args.precision, c.describe()), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -821,7 +882,15 @@ def main():
     ap.add_argument("--suite", action="store_true",
                     help="measure every configuration (one JSON line each) instead of the headline")
     ap.add_argument("--suite-configs", default="cfg1,cfg2,cfg3,cfg4,cfg5")
+    ap.add_argument("--case", default=None,
+                    help="run one named workload --runs times without timing (profiler captures): "
+                         + ", ".join(sorted(CASES)) + ", cfg5:N, item:I")
+    ap.add_argument("--precision", default="bf16x3", help="precision of --case")
+    ap.add_argument("--runs", type=int, default=2, help="runs of --case")
+    ap.add_argument("--tuning", default="", help="tuning of --case, e.g. raster=32,load=1")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     if args.suite:
         run_suite(args)
         return 0
