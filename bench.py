@@ -482,6 +482,19 @@ def run_ours(args, world, rank, local):
     e1.record()
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / ne2e, world)
+    # the host link's own rates, measured on the same pinned buffers: the
+    # end-to-end step cannot beat max(H2D bytes / H2D rate, D2H bytes / D2H
+    # rate) when the copies run concurrently on the two copy engines
+    link = {}
+    for name, src, dst in (("h2d_gbs", Ah, A), ("d2h_gbs", C, Ch)):
+        dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        link[name] = src.numel() * src.element_size() / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    e2e_bound_ms = max(h2d / (link["h2d_gbs"] * 1e9), d2h / (link["d2h_gbs"] * 1e9)) * 1e3
 
     # ---- CPU baseline (rank 0, single GPU only) ----------------------------
     cpu = None
@@ -528,6 +541,9 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": world * flops / (ms_e2e * 1e-3) / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e,
+                    "link": link,
+                    "bound_ms": e2e_bound_ms,
+                    "frac_of_link_bound": e2e_bound_ms / ms_e2e,
                     "path": "Compiled.run_host: pinned host A, B -> device, tccg_plan_run per slab of "
                             "C's last index (%d slabs), C -> pinned host; copies overlap the compute on "
                             "two copy streams" % x3._auto_slabs(Ch)},

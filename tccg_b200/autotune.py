@@ -180,6 +180,12 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             if not grouped:
                 # the tcgen05 tail split off (it is on where the model expects a gain)
                 more.append(Tuning(method=method, tail_split=-1))
+                # the CTA-pair kernel (256-row tiles, cta_group::2) where there
+                # are rows for it: measured 16 % slower per GHz than the one-SM
+                # kernel on configuration 3, searched so that a shape it serves
+                # better can pick it (grouped launches do not run it)
+                if M >= 512 and (precision != "bf16x3" or dtype == "f32"):
+                    more.append(Tuning(method=method, pair=1, variant=chunks[0]))
             out += first + more
     if grouped:
         for t in out:
