@@ -153,9 +153,10 @@ int tccg_plan_workspace(const tccg_plan* plan, size_t* bytes);
  * C = alpha * contract(A, B) + beta * C on `stream`. A and B are in the
  * caller's (file) order; ws must be 256-byte aligned when ws_bytes > 0.
  * With beta == 0, C is written without being read (as TCCG's update=0 path).
- * For contractions of at most 2^36 FLOP the kernels after the first one use
- * programmatic dependent launch (they start while the kernel before them
- * drains); TCCG_B200_PDL=1 or =0 in the environment forces it on or off.
+ * The kernels after the first one use programmatic dependent launch (they
+ * start while the kernel before them drains) on the CUDA cores, and on the
+ * tensor cores when the persistent grid runs at most four rounds of tiles;
+ * TCCG_B200_PDL=1 or =0 in the environment forces it on or off.
  */
 int tccg_plan_run(const tccg_plan* plan, const void* A, const void* B, void* C, double alpha,
                   double beta, void* ws, size_t ws_bytes, void* stream);

@@ -882,10 +882,24 @@ extern "C" int tccg_plan_workspace(const tccg_plan* p, size_t* bytes) {
   return TCCG_OK;
 }
 
-// Programmatic dependent launch (launch_after): on by default for runs of at
-// most 2^36 FLOP; TCCG_B200_PDL=1 / =0 in the environment forces it on / off.
-static bool pdl_by_size(const tccg_plan* p) {
-  return 2.0 * (double)p->M * (double)p->N * (double)p->K <= 68719476736.0;
+// Programmatic dependent launch (launch_after) lets a kernel start while the
+// one before it drains (about 2 us per kernel boundary). For the persistent
+// tcgen05 grid it also moves the CTAs: they start on SMs in the order the
+// previous kernel frees them instead of the hardware's own placement (pairs
+// of SMs round-robin over the GPCs), so the CTAs that share operand tiles
+// across the rounds of the tile order land elsewhere. Measured on
+// configuration 3 (37 rounds of 148 tiles): steps 20 % slower as the power
+// draw rose, while in SM order (tile positions from %smid, identical with
+// and without it) the steps were the same with and without -- the placement
+// is the cost. Default: on for the CUDA-core kernels (independent CTAs) and
+// for tcgen05 grids of at most 4 rounds (little reuse across rounds to
+// lose); TCCG_B200_PDL=1 / =0 in the environment forces it on / off.
+static bool pdl_auto(const tccg_plan* p) {
+  if (p->simt) return true;
+  const int64_t mn = (int64_t)p->tiles_m * p->tiles_n;
+  const int64_t tiles = p->tail_split > 1 ? p->full_tiles + (mn - p->full_tiles) * p->tail_split
+                                          : mn * p->ksplit;
+  return tiles <= 4 * (int64_t)std::max(p->grid, 1);
 }
 static int pdl_forced() {  // 1 on, 0 off, -1 the size rule
   const char* e = std::getenv("TCCG_B200_PDL");
@@ -898,7 +912,7 @@ static int pdl_forced() {  // 1 on, 0 off, -1 the size rule
 // the kernels), see pdl_enabled.
 static bool pdl_selected(const tccg_plan* p) {
   const int f = pdl_forced();
-  return f < 0 ? pdl_by_size(p) : f == 1;
+  return f < 0 ? pdl_auto(p) : f == 1;
 }
 
 extern "C" int tccg_plan_describe(const tccg_plan* p, char* buf, size_t len) {
@@ -1104,13 +1118,9 @@ static int launch_check(const char* what) {
 // library's own kernels on the stream (packing -> GETT, GETT -> reduction):
 // its CTAs may start, and set up barriers and TMEM, while that kernel drains;
 // they call grid_dep_wait() before reading its output, and read nothing
-// before it that an earlier kernel of the call could still be writing.
-// Automatic for short runs only (2MNK <= 2^36 FLOP, about 0.1 ms on the
-// tensor cores), where the 2 us it saves per kernel boundary shows: the
-// 8.8e12-FLOP persistent tcgen05 run (operands far larger than L2) measured
-// 20 % slower with it, and kernels right after such runs slower too (the cause
-// is not established). TCCG_B200_PDL=1 / =0 in the environment forces it on /
-// off; always off under per-kernel event timing (an event between the kernels).
+// before it that an earlier kernel of the call could still be writing. When
+// it is used: pdl_auto. Always off under per-kernel event timing (an event
+// sits between the kernels).
 static bool pdl_enabled(const tccg_plan* p) { return !g_events && pdl_selected(p); }
 
 template <typename... P, typename... A>
@@ -1339,12 +1349,15 @@ static int run_simt(const tccg_plan* p, const void* GA, const void* GB, T* Cout,
   return rc;
 }
 
-// Tile order of the persistent tcgen05 grid by SM (TcArgs::sm_order): on,
-// unless TCCG_B200_CTA_ORDER=launch in the environment selects the launch
-// order (for comparisons).
+// Tile order of the persistent tcgen05 grid by SM (TcArgs::sm_order) when
+// TCCG_B200_CTA_ORDER=sm in the environment; by default the launch order.
+// Measured on configuration 3: the SM order makes the placement independent
+// of programmatic dependent launch, but its placement (consecutive tiles on
+// consecutive SM ids) ran 13 % slower than the hardware's own (launch order
+// without dependent launch), which the default keeps.
 static bool sm_order_enabled() {
   const char* e = std::getenv("TCCG_B200_CTA_ORDER");
-  return !(e && std::strcmp(e, "launch") == 0);
+  return e && std::strcmp(e, "sm") == 0;
 }
 
 // Arguments of the tcgen05 kernels common to both loaders (k-split partial
@@ -1646,6 +1659,21 @@ static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s) {
   grid.z = (unsigned)std::min<int64_t>(cdiv(groups, grid.y), 1024);
   mark(2, 0, s);
   const dim3 blk(32, 8);
+  if (da == 0 && pa.ext[0] < PERM_ROWS_MAX) {  // short rows: one warp per row
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const dim3 g1((unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(rest, 8), (int64_t)sms * 8)));
+    if (dtype == TCCG_F64)
+      permute_rows_kernel<double><<<g1, blk, 0, s>>>(pa);
+    else if (dtype == TCCG_F32)
+      permute_rows_kernel<float><<<g1, blk, 0, s>>>(pa);
+    else
+      return fail(TCCG_ERR_UNSUPPORTED, "transpose supports TCCG_F32 and TCCG_F64");
+    mark(2, 1, s);
+    return launch_check("permute_rows");
+  }
   if (dtype == TCCG_F64) {
     if (da == 0)
       permute_stream_kernel<double><<<grid, blk, 0, s>>>(pa);

@@ -5,7 +5,8 @@
 // output dimensions that are contiguous in both tensors, and orders the
 // output dimensions so that dim 0 has B's smallest stride. Then:
 //   * dim 0 is also A's smallest stride: a streaming copy along dim 0, 8
-//     elements per thread with all loads issued before the stores;
+//     elements per thread with all loads issued before the stores (one
+//     warp per row when dim 0 is short);
 //   * otherwise shared-memory tiles over (dim 0, the dim `da` with A's
 //     smallest stride): reads along da, writes along dim 0, 16 loads in
 //     flight per thread (one 64 x 64 tile, or four 32 x 32 tiles of
@@ -83,6 +84,53 @@ __global__ void __launch_bounds__(256) permute_stream_kernel(const PermArgs p) {
     for (int u = 0; u < PERM_STREAM; ++u) {
       const int64_t i0 = base + u * 256 + tid;
       if (i0 < L) B[offb + i0 * sb0] = v[u];
+    }
+  }
+}
+
+// dim 0 has the smallest stride in both tensors and is short (< PERM_ROWS_MAX
+// elements): one warp per row of dim 0 (rows r = global warp index + k *
+// warps in the grid), lanes along dim 0, 4 x 32 elements per pass with all
+// loads issued before the stores. The chunked kernel above gives every row a
+// CTA of 256 x PERM_STREAM slots, most of them empty on short rows.
+constexpr int PERM_ROWS_MAX = 1024;
+
+template <typename T>
+__global__ void __launch_bounds__(256) permute_rows_kernel(const PermArgs p) {
+  const T alpha = (T)p.alpha, beta = (T)p.beta;
+  const T* A = static_cast<const T*>(p.A);
+  T* B = static_cast<T*>(p.B);
+  const int lane = threadIdx.x, w = threadIdx.y;  // block (32, 8)
+  const int64_t L = p.ext[0], sa0 = p.sa[0], sb0 = p.sb[0];
+  const int64_t warps = (int64_t)gridDim.x * 8;
+  for (int64_t r = (int64_t)blockIdx.x * 8 + w; r < p.rest; r += warps) {
+    int64_t offa, offb;
+    perm_decode(p, r, offa, offb);
+    for (int64_t c0 = 0; c0 < L; c0 += 128) {
+      T v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t i0 = c0 + u * 32 + lane;
+        v[u] = i0 < L ? A[offa + i0 * sa0] : T(0);
+      }
+      if (beta != T(0)) {
+        T old[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t i0 = c0 + u * 32 + lane;
+          old[u] = i0 < L ? B[offb + i0 * sb0] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = alpha * v[u] + beta * old[u];
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = alpha * v[u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t i0 = c0 + u * 32 + lane;
+        if (i0 < L) B[offb + i0 * sb0] = v[u];
+      }
     }
   }
 }

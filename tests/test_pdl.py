@@ -1,8 +1,8 @@
 """Programmatic dependent launch: the GETT kernel of a plan run may start
 while the packing kernel before it drains (and a reduction while its GETT
 kernel drains); each waits for that kernel's writes before reading them.
-It is automatic for short runs only (2MNK <= 2^36 FLOP); these tests force it
-on (TCCG_B200_PDL=1) and off (=0). Results must be bitwise equal either way on
+It is automatic for the CUDA-core kernels and for tcgen05 grids of at most
+four rounds of tiles; these tests force it on (TCCG_B200_PDL=1) and off (=0). Results must be bitwise equal either way on
 every launch path that uses it -- CUDA-core tiles (square, narrow), the short-K
 kernel with TMA and cp.async C blocks, tcgen05 (BF16x3, BF16, CTA pairs),
 k-split and tail-split reductions -- and for back-to-back runs captured in
@@ -117,8 +117,12 @@ def test_describe_reports_the_launch(cuda, monkeypatch):
     # configuration 3's size (8.8e12 FLOP): ordinary launches by default
     big = Plan(make_contraction("abcijk", "ambnc", "minjk",
                                 dict(a=32, b=32, c=32, i=32, j=32, k=32, m=64, n=64)), "bf16x3")
+    big32 = Plan(big.con, "fp32")
     monkeypatch.delenv("TCCG_B200_PDL", raising=False)
+    # a tcgen05 grid of one round: dependent; of 37 rounds: plain; the
+    # CUDA-core kernels (independent CTAs): dependent at any size
     assert "launch=dependent" in small.describe() and "launch=plain" in big.describe()
+    assert "launch=dependent" in big32.describe()
     monkeypatch.setenv("TCCG_B200_PDL", "1")
     assert "launch=dependent" in big.describe()
     monkeypatch.setenv("TCCG_B200_PDL", "0")
@@ -150,7 +154,7 @@ def test_sm_tile_order_bitwise(cuda, monkeypatch, name, pdl):
     ws = torch.empty(max(p.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
     monkeypatch.setenv("TCCG_B200_PDL", pdl)
     outs = []
-    for order in ("sm", "launch"):
+    for order in ("sm", "launch"):  # TCCG_B200_CTA_ORDER=sm: tile positions from %smid
         monkeypatch.setenv("TCCG_B200_CTA_ORDER", order)
         outs.append(_run(p, dA, dB, C, ws))
     assert np.array_equal(outs[0], outs[1])
