@@ -227,6 +227,19 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
          | ((uint32_t)(M >> 4) << 24);      // M / 16
 }
 
+// ---- split-BF16x3 representation ---------------------------------------------
+// hi = bf16_rn(x), lo = bf16_rn(x - hi) for two values, each pair converted
+// by one packed instruction (cvt.rn.bf16x2.f32): the same values as
+// converting every element alone, at half the conversion instructions (the
+// scalar conversion runs on the SM's narrow conversion pipe and bounded the
+// operand conversion). hi / lo hold x0 in the low and x1 in the high half.
+__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - __low2float(h), x1 - __high2float(h));
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
 // ---- cp.async (SIMT kernels) ------------------------------------------------
 __device__ __forceinline__ void cp_async_16(void* smem_dst, const void* gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc)

@@ -95,20 +95,10 @@ __device__ __forceinline__ void store_k4(__nv_bfloat16* base, int64_t k, int64_t
         if (k + j < kcover) base[k + j] = __float2bfloat16_rn(x[j]);
     }
   } else {  // PACK_K_BF16X3 (kcover is a multiple of 32)
-    __nv_bfloat16 hi[4], lo[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      hi[j] = __float2bfloat16_rn(x[j]);
-      lo[j] = __float2bfloat16_rn(x[j] - __bfloat162float(hi[j]));
-    }
     __nv_bfloat16* row = base + (k / 32) * 64;  // 16-byte aligned: ld % 64 == 0
-    __nv_bfloat162 h0 = __halves2bfloat162(hi[0], hi[1]), h1 = __halves2bfloat162(hi[2], hi[3]);
-    __nv_bfloat162 l0 = __halves2bfloat162(lo[0], lo[1]), l1 = __halves2bfloat162(lo[2], lo[3]);
     uint2 uh, ul;
-    uh.x = *reinterpret_cast<uint32_t*>(&h0);
-    uh.y = *reinterpret_cast<uint32_t*>(&h1);
-    ul.x = *reinterpret_cast<uint32_t*>(&l0);
-    ul.y = *reinterpret_cast<uint32_t*>(&l1);
+    split_bf16x2(x[0], x[1], uh.x, ul.x);
+    split_bf16x2(x[2], x[3], uh.y, ul.y);
     *reinterpret_cast<uint2*>(row + k % 32) = uh;
     *reinterpret_cast<uint2*>(row + 32 + k % 32) = ul;
   }

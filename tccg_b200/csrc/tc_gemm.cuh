@@ -487,12 +487,7 @@ __device__ __forceinline__ void gather_convert(const GatherJob& j, const float* 
       for (int e = 0; e < 8; e += 2) {
         const float x0 = (row_ok && k8 * 8 + e < kn) ? v[e] : 0.0f;
         const float x1 = (row_ok && k8 * 8 + e + 1 < kn) ? v[e + 1] : 0.0f;
-        const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-        const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-        const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-        const __nv_bfloat162 hp = __halves2bfloat162(h0, h1), lp = __halves2bfloat162(l0, l1);
-        hw[e / 2] = *reinterpret_cast<const uint32_t*>(&hp);
-        lw[e / 2] = *reinterpret_cast<const uint32_t*>(&lp);
+        split_bf16x2(x0, x1, hw[e / 2], lw[e / 2]);
       }
       uint8_t* drow = stage + rr * 128;
       const int sw = rr & 7;
