@@ -65,7 +65,8 @@ class Tuning(ctypes.Structure):
                 ("max_ctas", ctypes.c_int32), ("pair", ctypes.c_int32),
                 ("direct", ctypes.c_int32), ("shortk", ctypes.c_int32),
                 ("simt_tile", ctypes.c_int32), ("tail_split", ctypes.c_int32),
-                ("load", ctypes.c_int32), ("tile_n", ctypes.c_int32)]
+                ("load", ctypes.c_int32), ("tile_n", ctypes.c_int32),
+                ("skinny", ctypes.c_int32)]
 
 
 _lib = None

@@ -36,12 +36,13 @@ import sqlite3
 import time
 from typing import List, Optional, Tuple
 
+from ._native import TccgError
 from .plan import Plan, Tuning
 from .spec import Contraction
 
 # Part of every cache key: cached winners measured on older kernels (or
 # without the tuning fields a newer build searches) are not reused.
-CODE_VERSION = "tccg_b200-0.3"
+CODE_VERSION = "tccg_b200-0.4"
 
 
 def default_db_path() -> str:
@@ -130,6 +131,10 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
         methods = ("gett",)
     orders = order_variants(con)
     out: List[Tuning] = []
+    # the skinny kernel (one small free extent) forced on and off, right
+    # after the model's choice
+    skinny = (skinny_eligible(M, N, K, precision, dtype)
+              and [Tuning(method="gett", skinny=1), Tuning(method="gett", skinny=-1)] or [])
     for method in methods:
         if precision in ("fp32", "fp64"):
             bm, bn = (128, 128) if precision == "fp32" else (128, 64)
@@ -142,7 +147,10 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
                     if K >= 64 * s:
                         splits.append(s)
             splits.sort(key=lambda s: abs(tiles * s - 2 * num_sms))
-            out += [Tuning(method=method, ksplit=s) for s in splits]
+            out += [Tuning(method=method, ksplit=s) for s in splits[:1]]
+            if method == "gett" and precision == "fp32":
+                out += skinny
+            out += [Tuning(method=method, ksplit=s) for s in splits[1:]]
             # short K: the C-prefetching kernel forced on and off
             if K <= (16 if precision == "fp64" else 32):
                 out += [Tuning(method=method, ksplit=1, shortk=1),
@@ -160,7 +168,7 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             # accumulation chunks, tile orders and mode orders.
             loads = [1, 2] if precision == "bf16x3" and dtype == "f32" and method == "gett" else [0]
             chunks = [16, 32, 8] if precision == "bf16x3" else [1]
-            first = [Tuning(method=method)]
+            first = [Tuning(method=method)] + (skinny if method == "gett" else [])
             if len(loads) > 1:
                 first += [Tuning(method=method, load=ld) for ld in loads]
             else:
@@ -197,6 +205,15 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             seen.add(t.key())
             uniq.append(t)
     return uniq
+
+
+def skinny_eligible(M: int, N: int, K: int, precision: str, dtype: str = "f32") -> bool:
+    """Whether the skinny kernel can run a GETT of these extents (the C ABI's
+    rule: FP32 operands, FP32 or BF16x3 precision, min(M, N) <= 64, or <= 256
+    with K <= 32)."""
+    S = min(M, N)
+    return (dtype == "f32" and precision in ("fp32", "bf16x3")
+            and (S <= 64 or (S <= 256 and K <= 32)))
 
 
 def _flush_l2(buf):
@@ -285,7 +302,10 @@ def autotune(con: Contraction, precision: str, max_implementations: int = 16,
     flops = con.flop_count()
     inputs = _inputs(con, dtype, "f64" if precision == "fp64" else "f32")
     for t in cands:
-        p = Plan(con, precision=precision, tuning=t, dtype=dtype)
+        try:
+            p = Plan(con, precision=precision, tuning=t, dtype=dtype)
+        except TccgError:  # a kernel this contraction cannot take
+            continue
         if max_workspace_gb is not None and p.workspace_bytes > max_workspace_gb * 2 ** 30:
             continue
         ms = measure(p, inputs=inputs)

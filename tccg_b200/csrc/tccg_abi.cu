@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
@@ -18,6 +19,7 @@
 #include "common.cuh"
 #include "pack.cuh"
 #include "simt_gemm.cuh"
+#include "skinny_gett.cuh"
 #include "tc2_gemm.cuh"
 #include "tc_gemm.cuh"
 #include "transpose.cuh"
@@ -109,6 +111,13 @@ struct tccg_plan {
   // TcArgs::crun), or 0
   int32_t crun = 0;
   int32_t tcv = 0;  // TcVariant of a tensor-core plan
+  // skinny kernel (skinny_gett.cuh): geometry and tables in sk (operand, C
+  // and slice pointers are filled in per run); s_is_n: the narrow side is N
+  bool skinny = false, sk_s_is_n = false;
+  int32_t sk_ksplit = 1;
+  SkinnyArgs sk{};
+  int64_t* t_p_y = nullptr;
+  int64_t* t_c_y = nullptr;
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, off_tail = 0, ws_bytes = 0;
   char describe[512] = "";
@@ -255,22 +264,25 @@ static bool choose_gather(const tccg_plan* p) {
   return p->tune.load == 2 && gather_eligible(p);
 }
 
-static bool choose_simt(const tccg_plan* p) {
-  if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) return true;
-  if (p->tune.pair || p->tune.variant > 0 || p->tune.load > 0) return false;
-  if (p->tune.variant < 0) return true;
-  // Against the tensor-core model (tc_time, the faster of its two loaders):
-  // CUDA cores at 35 TFLOP/s on the tile shape choose_simt_shape picks (its
-  // padding counted as work), operands streamed at 4.5 TB/s three times
-  // with a packing pass, once where the CUDA-core kernel reads them in place.
+// CUDA-core tile kernel model (seconds): 35 TFLOP/s on the tile shape
+// choose_simt_shape picks (its padding counted as work), operands streamed
+// at 4.5 TB/s three times with a packing pass, once where the kernel reads
+// them in place.
+static double simt_time(const tccg_plan* p) {
   const double M = (double)p->M, N = (double)p->N, K = (double)p->K;
   double simt_work = 0;  // padded M x N of the CUDA-core tile shape it would use
   const int shape = choose_simt_shape(p, &simt_work);
   const double simt_passes = direct_eligible(p, shape) ? 1.0 : 3.0;  // operand reads
   const double op = (M + N) * K * (p->dtype == TCCG_BF16 ? 2.0 : 4.0), cb = M * N * 4.0;
-  double t_tc = tc_time(p, p->tune.load == 2 && gather_eligible(p));
-  const double t_simt = std::max(2.0 * simt_work * K / 35e12, (cb + simt_passes * op) / 4.5e12);
-  return t_simt < t_tc;
+  return std::max(2.0 * simt_work * K / 35e12, (cb + simt_passes * op) / 4.5e12);
+}
+
+static bool choose_simt(const tccg_plan* p) {
+  if (p->prec == TCCG_PREC_FP32 || p->prec == TCCG_PREC_FP64) return true;
+  if (p->tune.pair || p->tune.variant > 0 || p->tune.load > 0) return false;
+  if (p->tune.variant < 0) return true;
+  // against the tensor-core model (tc_time, with the loader the tuning asks for)
+  return simt_time(p) < tc_time(p, p->tune.load == 2 && gather_eligible(p));
 }
 
 // First mode of extent > 1 has unit stride (or no such mode).
@@ -405,10 +417,162 @@ static int32_t pick_read_k_fast(int nr, const int64_t* rext, const int64_t* rstr
   return ks < rs ? 1 : 0;
 }
 
+// ---- skinny kernel: eligibility, geometry and model ----------------------
+// FP32 operands (FP32 accumulation serves BF16X3 as well: more accurate
+// than its three-product split), GETT, a narrow side of at most 64 rows (any
+// K), or of at most 256 with K <= 32 (several passes over one chunk).
+static bool skinny_eligible(const tccg_plan* p) {
+  if (p->dtype != TCCG_F32 || (p->prec != TCCG_PREC_FP32 && p->prec != TCCG_PREC_BF16X3)) return false;
+  if (p->tune.method != TCCG_METHOD_GETT || p->tune.pair) return false;
+  const int64_t S = std::min(p->M, p->N);
+  return (S <= 64 || (S <= SK_SMAX && p->K <= SK_KC)) && p->K <= INT32_MAX;
+}
+
+static long long abs_ll(int64_t v) { return v < 0 ? -(long long)v : (long long)v; }
+
+// Smallest |stride| over modes of extent > 1 (LLONG_MAX when there is none).
+static long long min_abs_stride(int n, const int64_t* ext, const int64_t* str) {
+  long long m = LLONG_MAX;
+  for (int i = 0; i < n; ++i)
+    if (ext[i] > 1) m = std::min(m, abs_ll(str[i]));
+  return m;
+}
+
+// Geometry of the skinny kernel (SkinnyArgs without pointers) and the Y-space
+// mode list (W modes other than X, by increasing P stride). False when the
+// blocks would not fit one launch.
+static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
+  const tccg_desc& d = p->d;
+  const bool sn = p->N <= p->M;  // narrow side: N (W = M, P = GA) or M (W = N, P = GB)
+  p->sk_s_is_n = sn;
+  const int nw = sn ? d.nm : d.nn, nsm = sn ? d.nn : d.nm;
+  const int64_t* wext = sn ? d.m_ext : d.n_ext;
+  const int64_t* wp = sn ? d.a_m_stride : d.b_n_stride;
+  const int64_t* wc = sn ? d.c_m_stride : d.c_n_stride;
+  const int64_t* kp = sn ? d.a_k_stride : d.b_k_stride;
+  const int64_t* kq = sn ? d.b_k_stride : d.a_k_stride;
+  const int64_t* sext = sn ? d.n_ext : d.m_ext;
+  const int64_t* sq = sn ? d.b_n_stride : d.a_m_stride;
+  const int64_t* sc = sn ? d.c_n_stride : d.c_m_stride;
+  SkinnyArgs& a = p->sk;
+  a = SkinnyArgs{};
+  int X = -1;  // the W mode C stores contiguously
+  for (int i = 0; i < nw; ++i)
+    if (wext[i] > 1 && (X < 0 || abs_ll(wc[i]) < abs_ll(wc[X]))) X = i;
+  ym.clear();
+  for (int i = 0; i < nw; ++i)
+    if (i != X && wext[i] > 1) ym.push_back(i);
+  std::stable_sort(ym.begin(), ym.end(), [&](int u, int v) { return abs_ll(wp[u]) < abs_ll(wp[v]); });
+  *xmode = X;
+  a.ex = X >= 0 ? wext[X] : 1;
+  a.px = X >= 0 ? wp[X] : 0;
+  a.cx = X >= 0 ? wc[X] : 0;
+  a.ey = 1;
+  for (int i : ym) a.ey *= wext[i];
+  // P loads along its stride-one direction
+  const long long px = X >= 0 ? abs_ll(wp[X]) : LLONG_MAX;
+  const long long py = ym.empty() ? LLONG_MAX : abs_ll(wp[ym[0]]);
+  const long long pk = min_abs_stride(d.nk, d.k_ext, kp);
+  a.p_walk = pk < std::min(px, py) ? SK_P_K : py < px ? SK_P_Y : SK_P_X;
+  // box: along X (and the first Y modes) when P and C agree on X; a
+  // transposition needs runs both ways -- all of X up to 32, else 16 x 16
+  int64_t tx, ty;
+  if (a.p_walk == SK_P_Y) {
+    tx = a.ex <= 32 ? a.ex : a.ey <= 16 ? std::min<int64_t>(a.ex, SK_BW / a.ey) : 16;
+    ty = std::min<int64_t>(a.ey, SK_BW / tx);
+    tx = std::min<int64_t>(a.ex, SK_BW / ty);
+  } else {
+    tx = std::min<int64_t>(a.ex, SK_BW);
+    ty = std::min<int64_t>(a.ey, SK_BW / tx);
+  }
+  a.tx = (int32_t)tx;
+  a.ty = (int32_t)ty;
+  a.bxn = (int32_t)cdiv(a.ex, tx);
+  a.nblk = (int64_t)a.bxn * cdiv(a.ey, ty);
+  if (a.nblk > INT32_MAX) return false;
+  // C walk: C's stride-one index on the narrow side (runs of that S mode,
+  // when it is the first one), else X then the next C stride's side
+  const long long cs = min_abs_stride(nsm, sext, sc), cx = X >= 0 ? abs_ll(wc[X]) : LLONG_MAX;
+  long long cymin = LLONG_MAX;
+  for (int i : ym) cymin = std::min(cymin, abs_ll(wc[i]));
+  a.c_walk = cymin < cs ? SK_C_XY : SK_C_XS;
+  a.s_run = 0;
+  if (cs < cx) {
+    int s0 = -1;  // first S mode of extent > 1
+    for (int i = 0; i < nsm && s0 < 0; ++i)
+      if (sext[i] > 1) s0 = i;
+    if (s0 >= 0 && abs_ll(sc[s0]) == 1) {
+      a.c_walk = SK_C_SX;
+      a.s_run = (int32_t)sext[s0];
+    }
+  }
+  a.q_kfast = min_abs_stride(d.nk, d.k_ext, kq) < min_abs_stride(nsm, sext, sq) ? 1 : 0;
+  // rows per thread: one pass of the smallest of 16 / 32 / 48 / 64 rows; a
+  // longer S (K <= 32) passes of 32 or 64 rows, the least padding
+  const int64_t S = sn ? p->N : p->M;
+  if (S <= 64) {
+    a.rs = (int32_t)std::max<int64_t>(4, round_up(cdiv(S, 4), 4));
+    a.npass = 1;
+  } else {
+    const int64_t p32 = round_up(S, 32), p64 = round_up(S, 64);
+    a.rs = p64 <= p32 ? 16 : 8;
+    a.npass = (int32_t)cdiv(S, 4 * a.rs);
+  }
+  a.S = (int32_t)S;
+  a.K = (int32_t)p->K;
+  a.nchunks = (int32_t)cdiv(p->K, SK_KC);
+  int lg = 0;
+  while ((1 << lg) < std::min<int64_t>(p->K, SK_KC)) ++lg;
+  a.kr_log2 = lg;
+  // k-split: blocks that cannot fill two CTAs per SM, slices of >= 4 chunks
+  if (a.npass == 1) {
+    a.chunks_per_split = (int32_t)choose_ksplit(p->tune.ksplit, a.nblk, a.nchunks,
+                                                2 * (int64_t)p->num_sms, 4, &p->sk_ksplit);
+  } else {
+    a.chunks_per_split = a.nchunks;
+    p->sk_ksplit = 1;
+  }
+  a.alpha = 1.0f;
+  a.beta = 0.0f;
+  return true;
+}
+
+// Skinny kernel model (seconds): FP32 FMAs at 45 TFLOP/s over the blocks'
+// positions and padded rows; P and C at 5.5 TB/s, a run of fewer than 8
+// elements (32 bytes) in the load or store walk counted as a whole sector;
+// the k-split slices written and read back.
+static double skinny_time(const tccg_plan* p) {
+  const SkinnyArgs& a = p->sk;
+  const double W = (double)a.ex * (double)a.ey, K = (double)p->K, S = (double)a.S;
+  const double rows = 4.0 * a.rs * a.npass;
+  const double fma = 2.0 * (double)a.nblk * SK_BW * rows * K / 45e12;
+  const double run_p = a.p_walk == SK_P_K ? std::min<double>(K, SK_KC)
+                       : a.p_walk == SK_P_Y ? a.ty : a.tx;
+  const double run_c = a.c_walk == SK_C_SX ? a.s_run : a.tx;
+  auto waste = [](double run) { return run >= 8.0 ? 1.0 : 8.0 / std::max(run, 1.0); };
+  double bytes = 4.0 * W * K * waste(run_p) + 4.0 * W * S * waste(run_c);
+  if (p->sk_ksplit > 1) bytes += 8.0 * p->sk_ksplit * (double)a.nblk * 4.0 * a.rs * SK_BW;
+  return std::max(fma, bytes / 5.5e12) + (p->sk_ksplit > 1 ? 8e-6 : 4e-6);
+}
+
+// Whether the plan runs the skinny kernel: asked for, or -- unless the
+// tuning asks for another kernel family -- when its model beats the others'.
+static bool choose_skinny(const tccg_plan* p) {
+  if (p->tune.skinny > 0) return true;
+  if (p->tune.skinny < 0) return false;
+  const tccg_tuning& t = p->tune;
+  if (t.variant != 0 || t.load != 0 || t.direct != 0 || t.shortk != 0 || t.simt_tile != 0 ||
+      t.tile_n != 0)
+    return false;
+  double other = simt_time(p);
+  if (p->prec == TCCG_PREC_BF16X3) other = std::min(other, tc_time(p, false));
+  return skinny_time(p) < other;
+}
+
 static void plan_free(tccg_plan* p) {
   if (!p) return;
   int64_t* ts[] = {p->t_a_m, p->t_a_k, p->t_b_n, p->t_b_k, p->t_c_m, p->t_c_n, p->t_id_m, p->t_id_n,
-                   p->t_a_vsrc, p->t_a_vdst, p->t_b_vsrc, p->t_b_vdst};
+                   p->t_a_vsrc, p->t_a_vdst, p->t_b_vsrc, p->t_b_vdst, p->t_p_y, p->t_c_y};
   for (auto t : ts)
     if (t) cudaFree(t);
   if (p->d_status) cudaFree(p->d_status);
@@ -639,24 +803,50 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
              d.c_n_stride[0] == d.m_ext[0])
                 ? (int32_t)d.m_ext[0]
                 : 0;
-  p->simt = choose_simt(p);
+  if (!rc) {
+    // the skinny kernel: its geometry, the model's choice, its Y-space tables
+    std::vector<int> ym;
+    int xmode = -1;
+    const bool eligible = skinny_eligible(p) && skinny_geometry(p, ym, &xmode);
+    if (p->tune.skinny > 0 && !eligible) {
+      plan_free(p);
+      return fail(TCCG_ERR_UNSUPPORTED,
+                  "the skinny kernel needs FP32 operands, FP32 or BF16X3 precision, GETT and "
+                  "min(M, N) <= 64 (or <= 256 with K <= 32)");
+    }
+    p->skinny = eligible && choose_skinny(p);
+    if (p->skinny) {
+      const bool sn = p->sk_s_is_n;
+      int64_t ext[TCCG_MAX_MODES], sp[TCCG_MAX_MODES], scc[TCCG_MAX_MODES];
+      for (size_t i = 0; i < ym.size(); ++i) {
+        ext[i] = sn ? d.m_ext[ym[i]] : d.n_ext[ym[i]];
+        sp[i] = sn ? d.a_m_stride[ym[i]] : d.b_n_stride[ym[i]];
+        scc[i] = sn ? d.c_m_stride[ym[i]] : d.c_n_stride[ym[i]];
+      }
+      build_offsets((int)ym.size(), ext, sp, h);
+      rc = upload(h, &p->t_p_y);
+      build_offsets((int)ym.size(), ext, scc, h);
+      if (!rc) rc = upload(h, &p->t_c_y);
+    }
+  }
+  p->simt = !p->skinny && choose_simt(p);
   p->read_k_fast_a = pick_read_k_fast(d.nm, d.m_ext, d.a_m_stride, d.nk, d.k_ext, d.a_k_stride);
   p->read_k_fast_b = pick_read_k_fast(d.nn, d.n_ext, d.b_n_stride, d.nk, d.k_ext, d.b_k_stride);
-  if (!simt_path(p) && p->tune.load == 2 && p->prec == TCCG_PREC_BF16X3 && p->dtype == TCCG_F32 &&
+  if (!p->skinny && !simt_path(p) && p->tune.load == 2 && p->prec == TCCG_PREC_BF16X3 && p->dtype == TCCG_F32 &&
       p->tune.method == TCCG_METHOD_GETT && !p->tune.pair && p->tune.tile_n != 0 &&
       p->tune.tile_n != 128) {
     const int32_t tn = p->tune.tile_n;
     plan_free(p);
     return fail(TCCG_ERR_UNSUPPORTED, "the gather loader has 128-column tiles (tile_n %d)", tn);
   }
-  if (!simt_path(p) && choose_gather(p)) {
+  if (!p->skinny && !simt_path(p) && choose_gather(p)) {
     // gather schedules: 16-byte k quads, else along the operand's faster
     // direction (k or rows)
     p->gather = true;
     p->gread_a = p->ks_a ? GATHER_KQUAD : p->read_k_fast_a ? GATHER_K : GATHER_ROWS;
     p->gread_b = p->ks_b ? GATHER_KQUAD : p->read_k_fast_b ? GATHER_K : GATHER_ROWS;
   }
-  if (!rc && !simt_path(p) && !p->gather) {
+  if (!rc && !p->skinny && !simt_path(p) && !p->gather) {
     // tensor-core packs: unit stride on a later K mode -> k-block tiles read
     // along it; else walk the rows along the smallest-stride row mode when
     // that beats both the first row mode and reading along k
@@ -694,6 +884,26 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
 static int plan_layout(tccg_plan* p) {
   size_t ws = 0;
   const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
+  if (p->skinny) {
+    const SkinnyArgs& a = p->sk;
+    if (p->sk_ksplit > 1) {  // FP32 slices [split][block][row][position]
+      p->off_part = 0;
+      ws = align_up((size_t)p->sk_ksplit * (size_t)a.nblk * 4 * a.rs * SK_BW * 4, 256);
+    }
+    static const char* pw[] = {"x", "y", "k"};
+    static const char* cw[] = {"xs", "xy", "sx"};
+    snprintf(p->describe, sizeof(p->describe),
+             "method=GETT prec=%s kernel=skinny_gett<f32> M=%lld N=%lld K=%lld narrow=%s S=%d "
+             "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d load=%s%s "
+             "store=%s%s pack=none",
+             p->prec == TCCG_PREC_BF16X3 ? "bf16x3" : "fp32", (long long)p->M, (long long)p->N,
+             (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S, a.npass, 4 * a.rs, a.tx, a.ty,
+             (long long)a.ex, (long long)a.ey, (long long)a.nblk, a.nchunks, p->sk_ksplit,
+             pw[a.p_walk], a.q_kfast ? " q=k" : " q=s", cw[a.c_walk],
+             a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "");
+    p->ws_bytes = ws;
+    return TCCG_OK;
+  }
   if (simt_path(p)) {
     const bool dbl = p->prec == TCCG_PREC_FP64;
     // the short-K kernel keeps the square tile: a tuning that asks for it
@@ -895,7 +1105,7 @@ extern "C" int tccg_plan_workspace(const tccg_plan* p, size_t* bytes) {
 // for tcgen05 grids of at most 4 rounds (little reuse across rounds to
 // lose); TCCG_B200_PDL=1 / =0 in the environment forces it on / off.
 static bool pdl_auto(const tccg_plan* p) {
-  if (p->simt) return true;
+  if (p->simt || p->skinny) return true;
   const int64_t mn = (int64_t)p->tiles_m * p->tiles_n;
   const int64_t tiles = p->tail_split > 1 ? p->full_tiles + (mn - p->full_tiles) * p->tail_split
                                           : mn * p->ksplit;
@@ -982,6 +1192,14 @@ static cudaError_t set_attrs() {
                            (int)simt_group_smem_bytes<float>()));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)simt_group_smem_bytes<double>()));
+  chk(cudaFuncSetAttribute(skinny_gett_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SK_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SK_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SK_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_reduce_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SK_SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)Tc2Cfg<TC_BF16>::SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1489,6 +1707,43 @@ static int run_tc(const tccg_plan* p, const void* GA, const void* GB, float* Cou
   return tc_reduce(p, a, Cout, c_m, c_n, alpha, beta, s);
 }
 
+// Kernel arguments of a skinny plan for one call (P / Q by the narrow side).
+static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB, float* C,
+                              float alpha, float beta, char* w) {
+  SkinnyArgs a = p->sk;
+  const bool sn = p->sk_s_is_n;
+  a.P = static_cast<const float*>(sn ? GA : GB);
+  a.Q = static_cast<const float*>(sn ? GB : GA);
+  a.C = C;
+  a.p_y_off = p->t_p_y;
+  a.c_y_off = p->t_c_y;
+  a.p_k_off = sn ? p->t_a_k : p->t_b_k;
+  a.q_s_off = sn ? p->t_b_n : p->t_a_m;
+  a.q_k_off = sn ? p->t_b_k : p->t_a_k;
+  a.c_s_off = sn ? p->t_c_n : p->t_c_m;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.partial = p->sk_ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
+  return a;
+}
+
+static int run_skinny(const tccg_plan* p, const void* GA, const void* GB, float* C, float alpha,
+                      float beta, char* w, cudaStream_t s) {
+  const SkinnyArgs a = skinny_args(p, GA, GB, C, alpha, beta, w);
+  mark(1, 0, s);
+  launch_after(false, p, skinny_gett_kernel, dim3((unsigned)a.nblk, (unsigned)p->sk_ksplit),
+               dim3(SK_THREADS), SK_SMEM_BYTES, s, a);
+  int rc = launch_check("skinny_gett");
+  mark(1, 1, s);
+  if (rc || p->sk_ksplit == 1) return rc;
+  mark(2, 0, s);
+  launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)a.nblk), dim3(SK_THREADS),
+               SK_SMEM_BYTES, s, a, (int)p->sk_ksplit);
+  rc = launch_check("skinny_reduce");
+  mark(2, 1, s);
+  return rc;
+}
+
 static int permute_launch(int32_t dtype, const PermArgs& pa0, cudaStream_t s);
 
 extern "C" int tccg_plan_run(const tccg_plan* p, const void* A, const void* B, void* C,
@@ -1519,7 +1774,9 @@ extern "C" int tccg_plan_run(const tccg_plan* p, const void* A, const void* B, v
   const double ga = direct ? alpha : 1.0, gb = direct ? beta : 0.0;
   // C(m, n) = Cdst[m + ldc n]: C itself (GETT on a 2-D C) or the contiguous C'
   const int64_t ldc = cm == p->t_id_m ? p->M : p->c_ldc;
-  if (p->prec == TCCG_PREC_FP64)
+  if (p->skinny)
+    rc = run_skinny(p, GA, GB, static_cast<float*>(Cdst), (float)ga, (float)gb, w, s);
+  else if (p->prec == TCCG_PREC_FP64)
     rc = run_simt<double>(p, GA, GB, static_cast<double*>(Cdst), cm, cn, ldc, ga, gb, w, s);
   else if (simt_path(p))
     rc = run_simt<float>(p, GA, GB, static_cast<float*>(Cdst), cm, cn, ldc, (float)ga, (float)gb,
@@ -1761,11 +2018,16 @@ struct tccg_group {
   int32_t* tc_status = nullptr;
   // k-split reductions: ReduceJob<T>[] (same T as the CUDA-core lane)
   void* d_reduce = nullptr;
+  // skinny lane (FP32 operands): the items' contractions and the k-split
+  // reductions of those that split
+  SkinnyItem* d_sk = nullptr;
+  SkinnyItem* d_skr = nullptr;
+  int32_t n_sk = 0;
   // compact first-CTA / first-tile arrays of the jobs and items above (one
   // allocation): what the kernels binary-search instead of the large structs
   int64_t* d_begin = nullptr;
   int64_t *b_simt_jobs = nullptr, *b_tc_jobs = nullptr, *b_simt_items = nullptr,
-          *b_tc_items = nullptr, *b_reduce = nullptr;
+          *b_tc_items = nullptr, *b_reduce = nullptr, *b_sk = nullptr, *b_skr = nullptr;
   // Waves: the items run in sets whose workspaces together stay within
   // kGroupWaveBytes (an item above it is a set of its own). Each wave is
   // packed and multiplied before the next one reuses the same workspace
@@ -1783,6 +2045,8 @@ struct tccg_group {
     int64_t lane_tiles[TCV_COUNT] = {};
     int32_t tcj0 = 0, ntcj = 0;  // pack jobs of the packed-operand lanes (two per item)
     int64_t simt_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0, red_ctas = 0;
+    int32_t sk0 = 0, nsk = 0, skr0 = 0, nskr = 0;  // skinny items and their reductions
+    int64_t sk_ctas = 0, skr_ctas = 0;
   };
   std::vector<Wave> waves;
   bool bound = false;
@@ -1795,7 +2059,8 @@ static constexpr size_t kGroupWaveBytes = size_t(TCCG_GROUP_WAVE_MB) << 20;
 
 static void group_free(tccg_group* g) {
   if (!g) return;
-  void* ps[] = {g->d_simt, g->d_simt_jobs, g->d_tc, g->d_tc_jobs, g->d_reduce, g->d_begin};
+  void* ps[] = {g->d_simt, g->d_simt_jobs, g->d_tc, g->d_tc_jobs, g->d_reduce, g->d_begin,
+                g->d_sk, g->d_skr};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete g;
@@ -1823,7 +2088,9 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
       return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without the CTA-pair kernel (plan %d)", i);
     }
     g->plans.push_back(p);
-    if (simt_path(p)) {
+    if (p->skinny) {
+      ++g->n_sk;
+    } else if (simt_path(p)) {
       ++g->n_simt;
     } else {
       if (!g->tc_status) g->tc_status = p->d_status;
@@ -1849,12 +2116,14 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     g->ws_off[i] = ws;
     ws += need;
     g->ws_bytes = std::max(g->ws_bytes, ws);
-    if (simt_path(p)) {
+    if (p->skinny) {
+      wv.sk_ctas += p->sk.nblk * p->sk_ksplit;
+    } else if (simt_path(p)) {
       wv.simt_tiles += (p->Mp / p->simt_bm) * (p->Np / p->simt_bn) * p->ksplit;
     } else {
       wv.lane_tiles[p->tcv] += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
-    bool too_many = wv.simt_tiles > INT32_MAX;
+    bool too_many = wv.simt_tiles > INT32_MAX || wv.sk_ctas > INT32_MAX;
     for (int v = 0; v < TCV_COUNT; ++v) too_many |= wv.lane_tiles[v] > INT32_MAX;
     if (too_many) {
       group_free(g);
@@ -1871,14 +2140,21 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     e = cudaMalloc((void**)&g->d_tc, sizeof(TcGroupItem) * g->n_tc);
     if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_tc_jobs, sizeof(PackJob) * 2 * g->n_tc);
   }
+  if (e == cudaSuccess && g->n_sk) {
+    e = cudaMalloc((void**)&g->d_sk, sizeof(SkinnyItem) * g->n_sk);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_skr, sizeof(SkinnyItem) * g->n_sk);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&g->d_reduce, sizeof(ReduceJob<double>) * count);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_begin, sizeof(int64_t) * 4 * count);
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&g->d_begin, sizeof(int64_t) * (4 * (size_t)count + 2 * g->n_sk));
   if (e == cudaSuccess) {
     g->b_simt_jobs = g->d_begin;
     g->b_tc_jobs = g->b_simt_jobs + 2 * g->n_simt;
     g->b_simt_items = g->b_tc_jobs + 2 * g->n_tc;
     g->b_tc_items = g->b_simt_items + g->n_simt;
     g->b_reduce = g->b_tc_items + g->n_tc;
+    g->b_sk = g->b_reduce + count;
+    g->b_skr = g->b_sk + g->n_sk;
   }
   if (e != cudaSuccess) {
     group_free(g);
@@ -1958,7 +2234,9 @@ static std::vector<size_t> by_tile_cost(const tccg_group* g, const tccg_group::W
                                         int variant = -1) {
   std::vector<size_t> idx;
   for (size_t i : wv.items)
-    if (simt_path(g->plans[i]) == simt && (simt || g->plans[i]->tcv == variant)) idx.push_back(i);
+    if (!g->plans[i]->skinny && simt_path(g->plans[i]) == simt &&
+        (simt || g->plans[i]->tcv == variant))
+      idx.push_back(i);
   auto cost = [&](size_t i) {
     const tccg_plan* p = g->plans[i];
     return simt ? (int64_t)p->ktiles_per_split : (int64_t)p->kb_per_split;
@@ -2089,6 +2367,47 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
   return TCCG_OK;
 }
 
+// The skinny lane of one wave: its items (the longest k slices first) and
+// the reductions of those with a k-split, first CTAs counted from 0 within
+// the wave.
+static void bind_skinny(tccg_group* g, tccg_group::Wave& wv, const void* const* A,
+                        const void* const* B, void* const* C, const double* alpha,
+                        const double* beta, char* ws, std::vector<SkinnyItem>& items,
+                        std::vector<SkinnyItem>& red) {
+  wv.sk0 = (int32_t)items.size();
+  wv.skr0 = (int32_t)red.size();
+  std::vector<size_t> idx;
+  for (size_t i : wv.items)
+    if (g->plans[i]->skinny) idx.push_back(i);
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+    return g->plans[a]->sk.chunks_per_split > g->plans[b]->sk.chunks_per_split;
+  });
+  int64_t ctas = 0, rctas = 0;
+  for (size_t i : idx) {
+    const tccg_plan* p = g->plans[i];
+    const void* GA = p->d.swap_ab ? B[i] : A[i];
+    const void* GB = p->d.swap_ab ? A[i] : B[i];
+    SkinnyItem it;
+    memset(&it, 0, sizeof(it));
+    it.args = skinny_args(p, GA, GB, static_cast<float*>(C[i]), (float)alpha[i], (float)beta[i],
+                          ws + g->ws_off[i]);
+    it.begin = ctas;
+    it.ksplit = p->sk_ksplit;
+    ctas += p->sk.nblk * p->sk_ksplit;
+    items.push_back(it);
+    if (p->sk_ksplit > 1) {
+      SkinnyItem r = it;
+      r.begin = rctas;
+      rctas += p->sk.nblk;
+      red.push_back(r);
+    }
+  }
+  wv.nsk = (int32_t)items.size() - wv.sk0;
+  wv.nskr = (int32_t)red.size() - wv.skr0;
+  wv.sk_ctas = ctas;
+  wv.skr_ctas = rctas;
+}
+
 extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* const* B,
                                void* const* C, const double* alpha, const double* beta, void* ws,
                                size_t ws_bytes) {
@@ -2107,6 +2426,7 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     using T = decltype(tag);
     std::vector<PackJob> sjobs, tjobs;
     std::vector<TcGroupItem> titems;
+    std::vector<SkinnyItem> kitems, kred;
     int r = TCCG_OK;
     for (tccg_group::Wave& wv : g->waves) {
       int64_t rctas = 0;
@@ -2116,6 +2436,7 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       if constexpr (sizeof(T) == 4) {
         r = bind_tc(g, wv, A, B, C, alpha, beta, w, titems, tjobs, red, rctas);
         if (r) return r;
+        bind_skinny(g, wv, A, B, C, alpha, beta, w, kitems, kred);
       }
       if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
       wv.n_red = (int32_t)red.size() - wv.red0;
@@ -2135,6 +2456,12 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     }
     if (!red.empty())
       CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
+    if (!kitems.empty())
+      CUDA_TRY(cudaMemcpy(g->d_sk, kitems.data(), sizeof(SkinnyItem) * kitems.size(),
+                          cudaMemcpyHostToDevice));
+    if (!kred.empty())
+      CUDA_TRY(cudaMemcpy(g->d_skr, kred.data(), sizeof(SkinnyItem) * kred.size(),
+                          cudaMemcpyHostToDevice));
     auto item_begin = [](const auto& x) { return x.tile_begin; };
     auto job_begin = [](const auto& x) { return x.begin; };
     r = upload_begins(simt_items, item_begin, g->b_simt_items);
@@ -2142,6 +2469,8 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     if (!r) r = upload_begins(titems, item_begin, g->b_tc_items);
     if (!r) r = upload_begins(tjobs, job_begin, g->b_tc_jobs);
     if (!r) r = upload_begins(red, job_begin, g->b_reduce);
+    if (!r) r = upload_begins(kitems, job_begin, g->b_sk);
+    if (!r) r = upload_begins(kred, job_begin, g->b_skr);
     return r;
   };
   if (g->prec == TCCG_PREC_FP64) {
@@ -2212,6 +2541,18 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
       K::group<<<grid, K::Cfg::NUM_THREADS, K::Cfg::SMEM_BYTES, s>>>(tg, g->tc_status);
     });
     if ((rc = launch_check("gett_tc_group"))) return rc;
+  }
+  if constexpr (sizeof(T) == 4) {
+    if (wv.nsk > 0) {
+      skinny_group_kernel<<<(unsigned)wv.sk_ctas, SK_THREADS, SK_SMEM_BYTES, s>>>(
+          g->d_sk + wv.sk0, g->b_sk + wv.sk0, wv.nsk);
+      if ((rc = launch_check("skinny_group"))) return rc;
+    }
+    if (wv.nskr > 0) {
+      skinny_reduce_group_kernel<<<(unsigned)wv.skr_ctas, SK_THREADS, SK_SMEM_BYTES, s>>>(
+          g->d_skr + wv.skr0, g->b_skr + wv.skr0, wv.nskr);
+      if ((rc = launch_check("skinny_reduce_group"))) return rc;
+    }
   }
   if (wv.n_red > 0) {
     reduce_group_kernel<T><<<(unsigned)wv.red_ctas, 256, 0, s>>>(

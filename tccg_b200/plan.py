@@ -167,6 +167,7 @@ class Tuning:
     tail_split: int = 0  # tcgen05: 0 auto (k slices for a short last round), -1 never
     load: int = 0  # tcgen05 BF16x3, FP32 operands: 0 auto, 1 packing pass + TMA, 2 gather
     tile_n: int = 0  # tcgen05 tile width: 0 default, 128, 192 (BF16, BF16x3) or 256 (BF16)
+    skinny: int = 0  # FP32 operands, min(M, N) small: 0 auto, 1 the skinny kernel, -1 never
     # mode orders of the GETT view (gett_view): 0 = heuristic
     n_order: int = 0  # 1 = C's order, 2 = GB's unit-stride N mode first
     k_order: int = 0  # 1 = GA's order, 2 = GB's order
@@ -185,13 +186,14 @@ class Tuning:
         t.tail_split = int(self.tail_split)
         t.load = int(self.load)
         t.tile_n = int(self.tile_n)
+        t.skinny = int(self.skinny)
         return t
 
     def key(self) -> str:
-        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d/n%d/o%d%d" % (
+        return "%s/k%d/r%d/c%d/v%d/p%d/d%d/s%d/t%d/l%d/g%d/n%d/o%d%d/w%d" % (
             self.method, self.ksplit, self.raster, self.max_ctas, self.variant, self.pair,
             self.direct, self.shortk, self.simt_tile, self.tail_split, self.load, self.tile_n,
-            self.n_order, self.k_order)
+            self.n_order, self.k_order, self.skinny)
 
 
 class Plan:

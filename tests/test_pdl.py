@@ -4,8 +4,8 @@ kernel drains); each waits for that kernel's writes before reading them.
 It is automatic for the CUDA-core kernels and for tcgen05 grids of at most
 four rounds of tiles; these tests force it on (TCCG_B200_PDL=1) and off (=0). Results must be bitwise equal either way on
 every launch path that uses it -- CUDA-core tiles (square, narrow), the short-K
-kernel with TMA and cp.async C blocks, tcgen05 (BF16x3, BF16, CTA pairs),
-k-split and tail-split reductions -- and for back-to-back runs captured in
+kernel with TMA and cp.async C blocks, the skinny kernel's k-split reduction,
+tcgen05 (BF16x3, BF16, CTA pairs), k-split and tail-split reductions -- and for back-to-back runs captured in
 one CUDA graph, where each run's beta reads the C of the run before."""
 import numpy as np
 import pytest
@@ -29,6 +29,8 @@ CASES = {
                    "cblock=tma"),
     "shortk_cp": ("acbd", "aeb", "edc", dict(a=40, b=24, c=36, d=20, e=16), 1.0, "fp32",
                   Tuning(shortk=1), "cblock=cp.async"),
+    "skinny_ksplit": ("cdn", "dnxy", "yxc", dict(c=8, d=23, n=20, x=60, y=41), 0.5, "fp32",
+                      Tuning(skinny=1, ksplit=3), "kernel=skinny_gett<"),
     "tc_x3": ("mn", "mk", "kn", dict(m=1000, n=900, k=700), 0.5, "bf16x3", Tuning(variant=16),
               "kernel=gett_tc<"),
     "tc_bf16": ("mn", "km", "kn", dict(m=700, n=1100, k=500), -1.0, "bf16", Tuning(variant=16),
@@ -86,7 +88,7 @@ def test_dependent_launch_bitwise(cuda, monkeypatch, name):
     assert error_metrics(one.astype(np.float64), ref)["normwise"] <= 1e-5
 
 
-@pytest.mark.parametrize("name", ["shortk_tma", "tc_tail", "tc_ksplit", "simt"])
+@pytest.mark.parametrize("name", ["shortk_tma", "tc_tail", "tc_ksplit", "simt", "skinny_ksplit"])
 def test_dependent_launch_in_cuda_graph(cuda, monkeypatch, name):
     import torch
     con, ln, p, dA, dB, C, ws, beta = _setup(name, 172)

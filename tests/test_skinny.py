@@ -1,0 +1,137 @@
+"""The skinny kernel (tuning.skinny = 1; tccg_b200/csrc/skinny_gett.cuh):
+contractions with one small free extent, the narrow operand in shared memory
+and the wide one streamed in place, FP32 FMAs.
+
+Every case is checked against the FP64 oracle at the FP32 bound (normwise
+1e-6) for both precisions that can run it (FP32, and BF16x3 -- served in
+FP32, more accurate than its three-product split). The cases cover each P
+load walk (along x, along y for a transposition between P and C, along k),
+each C store walk (x then S, x then Y, runs of C's stride-one S mode), one
+and several passes over S, k-split slices and their reduction (with beta),
+the operand swap, a matrix-vector and an outer product; grouped runs equal
+per-item runs bit for bit, repeated runs are deterministic, and a plan that
+cannot take the kernel is refused when it is forced.
+"""
+import numpy as np
+import pytest
+
+from helpers import run_gpu, seeded_normal
+from oracle import LoopNest, error_metrics
+from tccg_b200.plan import Plan, Tuning
+from tccg_b200.spec import make_contraction
+
+pytestmark = pytest.mark.gpu
+
+# (C, A, B, extents, alpha, beta, describe tags)
+CASES = {
+    # P (= B after the swap) has d at stride one, C has v: boxes of 19 x 13
+    "transpose": ("vqud", "qe", "duve", dict(v=19, q=40, u=6, d=31, e=20), 1.0, 0.0,
+                  ["narrow=N", "load=y", "store=xs"]),
+    # C's stride-one index on the narrow side (runs of c), long K split over slices
+    "matvec_split": ("cdn", "dnxy", "yxc", dict(c=8, d=23, n=20, x=60, y=41), 0.5, -1.5,
+                     ["narrow=M", "store=sx run=8"]),
+    # P's stride-one index is contracted (u): loads along k
+    "kfast": ("fjr", "ufr", "ju", dict(f=10, j=28, r=46, u=8), 1.0, 0.25,
+              ["narrow=N", "load=k", "store=xs"]),
+    # S = 150 rows over several passes (K = 18 <= 32)
+    "passes": ("orak", "cok", "rac", dict(o=10, r=37, a=9, k=15, c=18), -0.75, 0.0,
+               ["narrow=M", "rows=5x32", "store=sx run=10"]),
+    # C's next stride after X is a W mode: (x, y) planes; K over three chunks
+    "xy": ("mpn", "pmk", "kn", dict(m=33, p=9, n=5, k=70), 1.0, 1.0,
+           ["narrow=N", "load=y", "store=xy"]),
+    "matvec": ("a", "ak", "k", dict(a=300, k=77), 1.0, 0.0, ["S=1 "]),
+    "outer": ("ab", "a", "b", dict(a=33, b=65), 1.5, 0.0, ["kchunks=1 "]),
+}
+
+
+def _data(ln, seed):
+    A = seeded_normal(ln.size_a, seed).astype(np.float32)
+    B = seeded_normal(ln.size_b, seed + 1).astype(np.float32)
+    C = seeded_normal(ln.size_c, seed + 2).astype(np.float32)
+    return A, B, C
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_skinny_matches_oracle(cuda, name, precision):
+    lc, la, lb, sizes, alpha, beta, tags = CASES[name]
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, C = _data(ln, 17)
+    out, p = run_gpu(con, precision, A, B, C, tuning=Tuning(skinny=1))
+    d = p.describe()
+    assert "kernel=skinny_gett<f32>" in d, d
+    for t in tags:
+        assert t in d, (t, d)
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    assert error_metrics(out, ref)["normwise"] <= 1e-6, d
+
+
+@pytest.mark.parametrize("ksplit", [1, 3, 0])
+def test_skinny_k_split_is_deterministic(cuda, ksplit):
+    """Slices added in order by the reduction: repeated runs are bitwise
+    equal, and an explicit split count is honoured."""
+    lc, la, lb, sizes, alpha, beta, _ = CASES["matvec_split"]
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, C = _data(ln, 23)
+    o1, p = run_gpu(con, "fp32", A, B, C, tuning=Tuning(skinny=1, ksplit=ksplit))
+    o2, _ = run_gpu(con, "fp32", A, B, C, tuning=Tuning(skinny=1, ksplit=ksplit))
+    assert np.array_equal(o1, o2)
+    if ksplit:
+        assert "ksplit=%d " % ksplit in p.describe(), p.describe()
+    else:
+        assert "ksplit=1 " not in p.describe(), p.describe()
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    assert error_metrics(o1, ref)["normwise"] <= 1e-6
+
+
+def test_skinny_grouped_equals_per_item(cuda):
+    """A grouped run with skinny items (one of them k-split) next to
+    tensor-core and CUDA-core items equals the per-item runs bit for bit."""
+    import torch
+    from tccg_b200.grouped import Group
+    names = ["transpose", "matvec_split", "kfast", "passes", "xy"]
+    items = [make_contraction(*CASES[n][:4], 1.0, 0.0) for n in names]
+    items.append(make_contraction("mn", "mk", "kn", dict(m=700, n=500, k=300), 1.0, 0.0))
+    tunings = [Tuning(skinny=1)] * len(names) + [Tuning(variant=16)]
+    g = torch.Generator(device="cuda").manual_seed(3)
+    As = [torch.randn(c.A0.num_elements(), generator=g, device="cuda") for c in items]
+    Bs = [torch.randn(c.B0.num_elements(), generator=g, device="cuda") for c in items]
+    Cs = [torch.zeros(c.C0.num_elements(), device="cuda") for c in items]
+    grp = Group(items, "bf16x3", tunings=tunings)
+    assert sum("skinny_gett" in p.describe() for p in grp.plans) == len(names)
+    grp.bind(As, Bs, Cs)
+    grp.capture()
+    grp.replay()
+    torch.cuda.synchronize()
+    grouped = [c.clone() for c in Cs]
+    for c in Cs:
+        c.zero_()
+    grp.run_per_item()
+    torch.cuda.synchronize()
+    for a, b in zip(grouped, Cs):
+        assert torch.equal(a, b)
+    for con, A, B, C in zip(items[:len(names)], As, Bs, grouped):
+        ln = LoopNest(con.C0.labels, con.A0.labels, con.B0.labels,
+                      {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices})
+        ref = ln.run(A.double().cpu().numpy(), B.double().cpu().numpy(), np.zeros(ln.size_c), 1.0, 0.0)
+        assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= 1e-6, str(con)
+
+
+def test_skinny_choice_and_refusal(cuda):
+    from tccg_b200._native import TccgError
+    # an item-69-like shape (N = 40, K = 20, P transposed against C): the model takes it
+    con = make_contraction("vqud", "qe", "duve", dict(v=19, q=40, u=600, d=31, e=20))
+    for precision in ("fp32", "bf16x3"):
+        assert "skinny_gett" in Plan(con, precision).describe()
+        assert "skinny_gett" not in Plan(con, precision, tuning=Tuning(skinny=-1)).describe()
+    # a square GEMM is not skinny; FP64 and BF16 are not served
+    sq = make_contraction("mn", "mk", "kn", dict(m=512, n=512, k=512))
+    assert "skinny_gett" not in Plan(sq, "fp32").describe()
+    with pytest.raises(TccgError):
+        Plan(sq, "fp32", tuning=Tuning(skinny=1))
+    with pytest.raises(TccgError):
+        Plan(con, "fp64", tuning=Tuning(skinny=1))
+    with pytest.raises(TccgError):
+        Plan(con, "bf16", tuning=Tuning(skinny=1))

@@ -1,0 +1,233 @@
+"""CPU replay of the skinny kernel's index arithmetic
+(tccg_b200/csrc/skinny_gett.cuh): the block boxes over the W positions, the
+three P load walks and both Q load walks of a k chunk, the epilogue's row
+staging over passes, and the three C store walks with their division-free
+(i, j) stepping. Each element is touched exactly once, and every store
+instruction of a whole run covers 32 consecutive C addresses.
+"""
+import itertools
+
+import pytest
+
+BW, KC, LDP, SUB, THREADS = 256, 32, 260, 32, 256
+P_X, P_Y, P_K = 0, 1, 2
+C_XS, C_XY, C_SX = 0, 1, 2
+
+
+def pos(p_walk, tx, ty, xl, yl):
+    return yl + ty * xl if p_walk == P_Y else xl + tx * yl
+
+
+def box(p_walk, tx, ty, bxn, ex, ey, b):
+    """skinny_box: {position: (x, y)} of block b (valid positions only)."""
+    ix, iy = b % bxn, b // bxn
+    out = {}
+    for w in range(BW):
+        if p_walk == P_Y:
+            yl, xl = w % ty, w // ty
+        else:
+            xl, yl = w % tx, w // tx
+        x, y = ix * tx + xl, iy * ty + yl
+        if w < tx * ty and x < ex and y < ey:
+            out[w] = (x, y)
+    return out
+
+
+@pytest.mark.parametrize("p_walk", [P_X, P_Y, P_K])
+@pytest.mark.parametrize("ex,ey,tx,ty", [(19, 262, 19, 13), (2627, 3, 256, 1), (10, 250, 10, 25),
+                                         (300, 300, 16, 16), (7, 5, 7, 5), (1, 40, 1, 40)])
+def test_boxes_cover_each_position_once(p_walk, ex, ey, tx, ty):
+    bxn = -(-ex // tx)
+    nblk = bxn * -(-ey // ty)
+    seen = {}
+    for b in range(nblk):
+        for w, xy in box(p_walk, tx, ty, bxn, ex, ey, b).items():
+            assert xy not in seen
+            seen[xy] = (b, w)
+            xl, yl = xy[0] - (b % bxn) * tx, xy[1] - (b // bxn) * ty
+            assert pos(p_walk, tx, ty, xl, yl) == w  # the store walks' numbering
+    assert len(seen) == ex * ey
+
+
+def p_loads(p_walk, kr_log2, kc, valid):
+    """skinny_load, P part: (k, w) of every copy or zero fill, per thread."""
+    out = []
+    for tid in range(THREADS):
+        if p_walk == P_K:
+            kl = tid & ((1 << kr_log2) - 1)
+            if kl < kc:
+                w = tid >> kr_log2
+                while w < BW:
+                    out.append((kl, w))
+                    w += THREADS >> kr_log2
+        else:
+            for k in range(kc):
+                out.append((k, tid))
+    return out
+
+
+@pytest.mark.parametrize("p_walk", [P_X, P_Y, P_K])
+@pytest.mark.parametrize("K", [1, 3, 8, 13, 20, 32, 45, 100])
+def test_p_chunk_loads_each_element_once(p_walk, K):
+    kr_log2 = 0
+    while (1 << kr_log2) < min(K, KC):
+        kr_log2 += 1
+    for c in range(-(-K // KC)):
+        kc = min(KC, K - c * KC)
+        got = p_loads(p_walk, kr_log2, kc, None)
+        assert sorted(got) == [(k, w) for k in range(kc) for w in range(BW)]
+        # lanes of a warp: along k (one 32-lane run of a position's k) or
+        # along consecutive positions
+        if p_walk == P_K and kc >= 8:
+            lanes = [(tid & ((1 << kr_log2) - 1), tid >> kr_log2) for tid in range(32)]
+            assert [k for k, _ in lanes[: 1 << kr_log2]] == list(range(1 << kr_log2))
+
+
+def q_loads(q_kfast, sq, kc):
+    out = []
+    for tid in range(THREADS):
+        if q_kfast:
+            kl = tid & 31
+            if kl < kc:
+                out += [(kl, s) for s in range(tid >> 5, sq, THREADS // 32)]
+        else:
+            s, k = tid % sq, tid // sq
+            while k < kc:
+                out.append((k, s))
+                s += THREADS % sq
+                k += THREADS // sq
+                if s >= sq:
+                    s -= sq
+                    k += 1
+    return out
+
+
+@pytest.mark.parametrize("q_kfast", [0, 1])
+@pytest.mark.parametrize("sq", [16, 32, 48, 64, 96, 128, 160, 192, 256])
+@pytest.mark.parametrize("kc", [1, 7, 20, 32])
+def test_q_chunk_loads_each_element_once(q_kfast, sq, kc):
+    got = q_loads(q_kfast, sq, kc)
+    assert sorted(got) == [(k, s) for k in range(kc) for s in range(sq)]
+    qld = sq + 4
+    assert all(k * qld + s < KC * (256 + 4) for k, s in got)  # inside the Q region
+
+
+def stage_rows(rs, S, npass):
+    """store_pass: the (pass, thread row i) -> staged (step s0, row r) map."""
+    sp = 4 * rs
+    out = {}
+    for p in range(npass):
+        for h in range(0, sp, SUB):
+            s0 = p * sp + h
+            if s0 >= S:
+                break
+            ns = min(sp - h, SUB, S - s0)
+            for sg in range(4):
+                for i in range(rs):
+                    r = sg * rs + i - h
+                    if 0 <= r < SUB:
+                        s = s0 + r
+                        assert (p, sg, i) not in out
+                        out[(p, sg, i)] = (s0, r, s < S and r < ns)
+    return out
+
+
+@pytest.mark.parametrize("rs,S,npass", [(4, 1, 1), (4, 16, 1), (8, 20, 1), (12, 40, 1), (12, 48, 1),
+                                        (16, 64, 1), (16, 150, 3), (8, 150, 5), (16, 256, 4),
+                                        (8, 65, 3)])
+def test_epilogue_stages_every_row_once(rs, S, npass):
+    st = stage_rows(rs, S, npass)
+    stored = sorted(s0 + r for (s0, r, ok) in st.values() if ok)
+    assert stored == list(range(S))
+    assert 4 * rs * npass <= 256  # Q rows in shared memory
+
+
+def store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns):
+    """skinny_store: [(warp, step, lane, w, r)] of one staged step."""
+    out = []
+
+    def plane(L0, L1, warp, elem):
+        total, di, dj = L0 * L1, 32 % L0, 32 // L0
+        for lane in range(32):
+            i, j, step = lane % L0, lane // L0, 0
+            f = lane
+            while f < total:
+                assert (i, j) == (f % L0, f // L0)
+                out.append((warp, elem(i, j), step, lane))
+                i += di
+                j += dj
+                if i >= L0:
+                    i -= L0
+                    j += 1
+                f += 32
+                step += 1
+
+    for warp in range(8):
+        if c_walk == C_XS:
+            for yl in range(warp, ty, 8):
+                plane(tx, ns, (warp, yl), lambda xl, r, yl=yl: (pos(p_walk, tx, ty, xl, yl), r))
+        elif c_walk == C_XY:
+            for r in range(warp, ns, 8):
+                plane(tx, ty, (warp, r), lambda xl, yl, r=r: (pos(p_walk, tx, ty, xl, yl), r))
+        else:
+            e0 = s_run
+            first = (s0 // e0) * e0
+            nruns = (s0 + ns - first + e0 - 1) // e0
+            for job in range(warp, nruns * ty, 8):
+                run, yl = job % nruns, job // nruns
+                rs_ = first + run * e0
+                ra, rb = max(rs_, s0), min(rs_ + e0, s0 + ns)
+                if rb <= ra:
+                    continue
+                plane(rb - ra, tx, (warp, job),
+                      lambda i, xl, yl=yl, ra=ra: (pos(p_walk, tx, ty, xl, yl), ra - s0 + i))
+    return out
+
+
+GEOMS = [(19, 13), (10, 25), (16, 16), (256, 1), (3, 5), (1, 1)]
+
+
+@pytest.mark.parametrize("c_walk", [C_XS, C_XY, C_SX])
+@pytest.mark.parametrize("p_walk", [P_X, P_Y])
+@pytest.mark.parametrize("tx,ty", GEOMS)
+@pytest.mark.parametrize("s0,ns,s_run", [(0, 32, 10), (32, 8, 10), (0, 20, 8), (64, 32, 19),
+                                         (0, 1, 1), (96, 22, 64)])
+def test_store_walk_covers_each_element_once(c_walk, p_walk, tx, ty, s0, ns, s_run):
+    st = store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns)
+    got = sorted(e for _, e, _, _ in st)
+    assert got == sorted((pos(p_walk, tx, ty, xl, yl), r)
+                         for xl in range(tx) for yl in range(ty) for r in range(ns))
+
+
+def test_store_instructions_are_contiguous():
+    """C(x, y, s) = x + 19 s + 760 y (item-69-like: X of 19, then S of 40):
+    the (x, s) walk's full steps write 32 consecutive addresses; the (s, x)
+    walk with C(x, s) = s + 10 x (a run of 10 rows, then X) likewise."""
+    tx, ty = 19, 13
+    st = store_walk(C_XS, P_Y, tx, ty, 0, 0, 32)
+    inv = {pos(P_Y, tx, ty, xl, yl): (xl, yl) for xl in range(tx) for yl in range(ty)}
+    steps = {}
+    for warp, (w, r), step, lane in st:
+        xl, yl = inv[w]
+        steps.setdefault((warp, step), []).append(xl + 19 * r + 760 * yl)
+    full = [sorted(a) for a in steps.values() if len(a) == 32]
+    assert full and all(a == list(range(a[0], a[0] + 32)) for a in full)
+    st = store_walk(C_SX, P_X, 256, 1, 10, 0, 30)
+    steps = {}
+    for warp, (w, r), step, lane in st:
+        steps.setdefault((warp, step), []).append(r + 10 * w)
+    full = [sorted(a) for a in steps.values() if len(a) == 32]
+    assert full and all(a == list(range(a[0], a[0] + 32)) for a in full)
+
+
+def test_partial_slices_round_trip():
+    """k-split: split z of block b writes row s, position w at
+    ((z nblk + b) SP + s) BW + w; the reduction reads slice z of its block at
+    b SP BW + z nblk SP BW + s BW + w -- the same element, for every (z, b, s, w)."""
+    for nblk, sp, splits in itertools.product((1, 3, 7), (16, 48), (2, 5)):
+        slice_ = nblk * sp * BW
+        for z, b, s in itertools.product(range(splits), range(nblk), range(sp)):
+            w = (z * 7 + s) % BW
+            wr = ((z * nblk + b) * sp + s) * BW + w
+            rd = b * sp * BW + w + s * BW + z * slice_
+            assert wr == rd
