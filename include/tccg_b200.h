@@ -127,11 +127,11 @@ typedef struct tccg_tuning {
   int32_t tile_n;      /* tcgen05 tile width (columns of C per tile): 0 = the loader's default
                           (BF16 256, BF16X3 192, gather 128); 128, 192 or 256 (BF16), 128 or
                           192 (BF16X3 with the packing pass) */
-  int32_t skinny;      /* FP32 operands, FP32 or BF16X3 precision, GETT, min(M, N) <= 64 (or
-                          <= 256 with K <= 32): the skinny kernel -- the narrow operand in
-                          shared memory, the wide one streamed once in place, C written once.
-                          0 = chosen by the model, 1 = always (an error where it does not
-                          apply), -1 = never */
+  int32_t skinny;      /* FP32 operands, FP32 or BF16X3 precision, GETT, min(M, N) <= 256,
+                          tensors of fewer than 2^31 elements: the skinny kernel -- chunks of
+                          the narrow operand in shared memory, the wide one streamed once in
+                          place, C written once. 0 = chosen by the model, 1 = always (an
+                          error where it does not apply), -1 = never */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

@@ -131,10 +131,11 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
         methods = ("gett",)
     orders = order_variants(con)
     out: List[Tuning] = []
-    # the skinny kernel (one small free extent) forced on and off, right
-    # after the model's choice
-    skinny = (skinny_eligible(M, N, K, precision, dtype)
-              and [Tuning(method="gett", skinny=1), Tuning(method="gett", skinny=-1)] or [])
+    # the skinny kernel (one small free extent) right after the model's
+    # choice; held off at the end of the search
+    elig = skinny_eligible(M, N, K, precision, dtype)
+    skinny = [Tuning(method="gett", skinny=1)] if elig else []
+    skinny_off = [Tuning(method="gett", skinny=-1)] if elig else []
     for method in methods:
         if precision in ("fp32", "fp64"):
             bm, bn = (128, 128) if precision == "fp32" else (128, 64)
@@ -159,6 +160,8 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             if precision == "fp32":
                 out += [Tuning(method=method, simt_tile=t) for t in (1, 2, 3)]
             out += [Tuning(method=method, n_order=no, k_order=ko) for no, ko in orders[1:]]
+            if method == "gett" and precision == "fp32":
+                out += skinny_off
         else:
             # variant > 0 forces the tensor cores (BF16X3: k-blocks per
             # accumulation chunk), < 0 the CUDA cores; the library's own
@@ -194,7 +197,7 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
                 # better can pick it (grouped launches do not run it)
                 if M >= 512 and (precision != "bf16x3" or dtype == "f32"):
                     more.append(Tuning(method=method, pair=1, variant=chunks[0]))
-            out += first + more
+            out += first + more + (skinny_off if method == "gett" else [])
     if grouped:
         for t in out:
             t.tail_split = -1
@@ -209,11 +212,10 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
 
 def skinny_eligible(M: int, N: int, K: int, precision: str, dtype: str = "f32") -> bool:
     """Whether the skinny kernel can run a GETT of these extents (the C ABI's
-    rule: FP32 operands, FP32 or BF16x3 precision, min(M, N) <= 64, or <= 256
-    with K <= 32)."""
-    S = min(M, N)
-    return (dtype == "f32" and precision in ("fp32", "bf16x3")
-            and (S <= 64 or (S <= 256 and K <= 32)))
+    rule: FP32 operands, FP32 or BF16x3 precision, min(M, N) <= 256; the C ABI
+    also wants tensors of fewer than 2^31 elements, and the search skips a
+    candidate it refuses)."""
+    return dtype == "f32" and precision in ("fp32", "bf16x3") and min(M, N) <= 256
 
 
 def _flush_l2(buf):

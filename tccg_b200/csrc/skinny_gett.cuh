@@ -4,11 +4,11 @@
 // contraction has few FMAs per byte: the wide operand P (W rows x K) and C
 // (W x S) dominate, and each should cross HBM once. The tile kernels pad S
 // to their tile width and, for most layouts, pay a packing pass that
-// transposes P first. This kernel keeps the narrow operand Q (S x K) in
-// shared memory chunk by chunk (every CTA reads it, from L2), streams P
-// straight from the caller's tensor and writes every element of C once, in
-// C's own layout -- the GETT property of TCCG's micro-kernel (C written in
-// its original layout, tccg/gett.py:192-223), with TCCG's packing step
+// transposes P first. This kernel keeps a chunk of the narrow operand Q
+// (S x K) in shared memory (every CTA reads it, from L2), streams P straight
+// from the caller's tensor and writes every element of C once, in C's own
+// layout -- the GETT property of TCCG's micro-kernel (C written in its
+// original layout, tccg/gett.py:192-223), with TCCG's packing step
 // (tccg/gett.py:440-470) replaced by loads that follow P's layout.
 //
 // W blocking. The W modes split into X -- the W mode C stores contiguously
@@ -23,20 +23,30 @@
 // the P loads run along y and the C stores along x, each over runs of the
 // box's extent.
 //
-// Per block (256 threads, two CTAs per SM): K in chunks of 32, double
-// buffered through element-wise cp.async (no packing pass, no alignment
-// requirement); thread (wg, sg) accumulates 4 positions x RS rows of S
-// (RS = 4, 8, 12 or 16; a pass covers 4 RS rows) in FP32 FMAs, k in
-// increasing order. S up to 64 takes one pass; up to 256 several passes over
-// one chunk when K <= 32. The epilogue stages 32 rows at a time in shared
-// memory and stores them in C's address order (SK_C_*), alpha * acc, then
-// fma with beta * C (not read when beta = 0).
+// Jobs. A job is one block x one pass over S (4 RS rows: RS = 4, 8 or 12
+// rows per thread) x one k slice; an S above 48 runs passes of 32 rows,
+// neighbouring jobs whose P chunks the later passes read from L2. The CTAs are persistent
+// (two per SM) and walk their jobs' k chunks (32 k each) as one sequence,
+// double buffered through element-wise cp.async: the copies of the next
+// chunk -- of the same job, or the first of the next job, whose box offsets
+// are computed then -- are in flight while the CTA multiplies the current
+// chunk and, after a job's last chunk, stores its C block. That keeps loads
+// in flight through the FMA and store phases of every block.
 //
-// With a k-split (few blocks, long K: a matrix-vector shape) split z writes
-// its raw sums densely to partial[z][block][row][position] and
-// skinny_reduce_kernel adds the slices in split order before the same store
-// walk. Results are deterministic: a fixed k order within a slice, slices in
-// order.
+// Per chunk thread (wg, sg) accumulates 4 positions x RS rows in FP32 FMAs, k
+// in increasing order. The epilogue stages 32 rows at a time in the P stage
+// just consumed and stores them in C's address order (SK_C_*): alpha * acc,
+// then fma with beta * C (not read when beta = 0).
+//
+// Offsets are 32-bit: the plan takes this kernel only for tensors whose
+// element offsets stay below 2^31 (8 GiB of FP32 each), which halves the
+// integer work of every load and store address and of the offset tables.
+//
+// With a k-split (few blocks, long K: a matrix-vector shape) the job of
+// slice z writes its raw sums densely to partial[z][block][row][position]
+// and skinny_reduce_kernel adds the slices in split order before the same
+// store walk. Results are deterministic: a fixed k order within a slice,
+// slices in order.
 #pragma once
 #include <cuda.h>
 #include "common.cuh"
@@ -48,14 +58,18 @@ constexpr int SK_BW = 256;             // box positions per block (one per threa
 constexpr int SK_KC = 32;              // k per chunk
 constexpr int SK_LDP = SK_BW + 4;      // P stage row stride (floats): [k][position]
 constexpr int SK_SMAX = 256;           // largest narrow extent
+constexpr int SK_SPMAX = 48;           // rows of one pass
+constexpr int SK_QLD = SK_SPMAX + 4;   // Q stage row stride (floats): [k][row]
 constexpr int SK_SUB = 32;             // rows of S staged per epilogue step
-constexpr int SK_QCAP = SK_KC * (SK_SMAX + 4);  // floats of the Q region
-// shared memory: P stages [2][KC][LDP], Q region, then position / row offsets
-constexpr size_t SK_P_BYTES = (size_t)2 * SK_KC * SK_LDP * 4;
-constexpr size_t SK_Q_BYTES = (size_t)SK_QCAP * 4;
-constexpr size_t SK_SMEM_BYTES = SK_P_BYTES + SK_Q_BYTES + (size_t)(2 * SK_BW + SK_SMAX) * 8;
+// shared memory: P stages [2][KC][LDP], Q stages [2][KC][QLD], then per job
+// slot (two) the box positions' P and C offsets and the pass rows' C offsets
+constexpr size_t SK_P_STAGE = (size_t)SK_KC * SK_LDP * 4;
+constexpr size_t SK_Q_STAGE = (size_t)SK_KC * SK_QLD * 4;
+constexpr size_t SK_OFF_TAB = 2 * (SK_P_STAGE + SK_Q_STAGE);
+constexpr size_t SK_SMEM_BYTES = SK_OFF_TAB + (size_t)(4 * SK_BW + 2 * SK_SPMAX) * 4;
+constexpr int SK_CTAS_PER_SM = 2;
 static_assert(SK_SUB == SK_KC, "the epilogue staging reuses one P stage");
-static_assert(2 * (SK_SMEM_BYTES + 1024) <= 228 * 1024, "two CTAs per SM");
+static_assert(SK_CTAS_PER_SM * (SK_SMEM_BYTES + 1024) <= 228 * 1024, "two CTAs per SM");
 
 // P load order: lanes along x (X is P's stride-one W mode), along y (the
 // first Y mode is), or along k (a K mode is). Box positions are numbered
@@ -70,19 +84,21 @@ struct SkinnyArgs {
   const float* P;
   const float* Q;
   float* C;
-  const int64_t* p_y_off;  // [ey]
-  const int64_t* c_y_off;  // [ey]
-  const int64_t* p_k_off;  // [K]
-  const int64_t* q_s_off;  // [S]
-  const int64_t* q_k_off;  // [K]
-  const int64_t* c_s_off;  // [S]
-  int64_t px, cx;          // P and C strides of X
-  int64_t ex, ey;          // extents of X and of the Y space
-  int64_t nblk;            // boxes: bxn along x, ceil(ey / ty) along y
+  const int32_t* p_y_off;  // [ey]
+  const int32_t* c_y_off;  // [ey]
+  const int32_t* p_k_off;  // [K]
+  const int32_t* q_s_off;  // [S]
+  const int32_t* q_k_off;  // [K]
+  const int32_t* c_s_off;  // [S]
+  int32_t px, cx;          // P and C strides of X
+  int32_t ex, ey;          // extents of X and of the Y space
+  int32_t nblk;            // boxes: bxn along x, ceil(ey / ty) along y
+  int32_t njobs;           // nblk x npass x ksplit
   int32_t tx, ty, bxn;
   int32_t S, K;
   int32_t rs;              // rows of S per thread; a pass covers 4 * rs rows
-  int32_t npass;           // passes over S (> 1 only with one chunk, no k-split)
+  int32_t npass;           // passes over S (> 1 only with one chunk and no k-split)
+  int32_t ksplit;
   int32_t nchunks, chunks_per_split;
   int32_t kr_log2;         // SK_P_K: log2 of the lanes along k per position
   int32_t p_walk, c_walk;
@@ -92,13 +108,40 @@ struct SkinnyArgs {
   float* partial;          // k-split slices (null: store to C)
 };
 
-constexpr int64_t SK_NONE = INT64_MIN;  // position outside the tensor (offsets may be negative)
+constexpr int32_t SK_NONE = INT32_MIN;  // position outside the tensor (offsets may be negative)
 
-// Offsets of this block's box positions (one per thread) into pw / cw.
-__device__ __forceinline__ void skinny_box(const SkinnyArgs& a, int64_t b, int64_t* pw,
-                                           int64_t* cw) {
+// Job J of an item: block b, pass p, k slice z over chunks [c0, c1).
+struct SkJob {
+  int b, p, z, c0, c1;
+};
+
+__device__ __forceinline__ SkJob skinny_job(const SkinnyArgs& a, int J) {
+  SkJob j;
+  if (a.ksplit == 1 && a.npass == 1) {  // the common case: a job is a block
+    j.b = J;
+    j.p = j.z = 0;
+  } else {
+    j.z = J % a.ksplit;
+    const int r = J / a.ksplit;
+    j.p = r % a.npass;
+    j.b = r / a.npass;
+  }
+  j.c0 = j.z * a.chunks_per_split;
+  j.c1 = j.c0 + a.chunks_per_split < a.nchunks ? j.c0 + a.chunks_per_split : a.nchunks;
+  return j;
+}
+
+__device__ __forceinline__ int skinny_kc(const SkinnyArgs& a, int c) {
+  const int64_t k0 = (int64_t)c * SK_KC;
+  return a.K - k0 < SK_KC ? (int)(a.K - k0) : SK_KC;
+}
+
+// Offsets of block b's box positions (one per thread) into pw / cw, and the
+// C offsets of pass p's rows into cs (when the job stores to C).
+__device__ __forceinline__ void skinny_begin(const SkinnyArgs& a, int b, int p, int sp,
+                                             int32_t* pw, int32_t* cw, int32_t* cs) {
   const int w = threadIdx.x;
-  const int64_t ix = b % a.bxn, iy = b / a.bxn;
+  const int ix = a.bxn == 1 ? 0 : b % a.bxn, iy = a.bxn == 1 ? b : b / a.bxn;
   int xl, yl;
   if (a.p_walk == SK_P_Y) {
     yl = w % a.ty;
@@ -107,33 +150,33 @@ __device__ __forceinline__ void skinny_box(const SkinnyArgs& a, int64_t b, int64
     xl = w % a.tx;
     yl = w / a.tx;
   }
-  const int64_t x = ix * a.tx + xl, y = iy * a.ty + yl;
+  const int x = ix * a.tx + xl, y = iy * a.ty + yl;
   const bool ok = w < a.tx * a.ty && x < a.ex && y < a.ey;
   pw[w] = ok ? x * a.px + __ldg(a.p_y_off + y) : SK_NONE;
   cw[w] = ok ? x * a.cx + __ldg(a.c_y_off + y) : SK_NONE;
+  if (!a.partial && w < sp) {
+    const int s = p * sp + w;
+    cs[w] = s < a.S ? __ldg(a.c_s_off + s) : 0;
+  }
 }
 
-// Box position of (xl, yl) in the block's numbering.
-__device__ __forceinline__ int skinny_pos(const SkinnyArgs& a, int xl, int yl) {
-  return a.p_walk == SK_P_Y ? yl + a.ty * xl : xl + a.tx * yl;
-}
-
-// Issues the copies of chunk c (P: [k][position], Q: [k][row], qld floats
-// per k) as one cp.async group; elements outside the tensors are zeros.
-__device__ __forceinline__ void skinny_load(const SkinnyArgs& a, int c, float* ps, float* qs,
-                                            int sq, int qld, const int64_t* pw) {
-  const int tid = threadIdx.x;
-  const int64_t k0 = (int64_t)c * SK_KC;
-  const int kc = a.K - k0 < SK_KC ? (int)(a.K - k0) : SK_KC;
+// Issues the copies of chunk c of job j (P: [k][position], Q: the pass's
+// rows, [k][row]) as one cp.async group; elements outside the tensors are
+// zeros. pw must hold the job's box offsets (visible to all threads).
+__device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j, int c, int sp,
+                                             float* ps, float* qs, const int32_t* pw) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int k0 = c * SK_KC;
+  const int kc = skinny_kc(a, c);
   if (a.p_walk == SK_P_K) {
-    // lanes along k: thread tid takes k = tid % kr of positions tid / kr + j * 256 / kr
+    // lanes along k: thread tid takes k = tid % kr of positions tid / kr + i * 256 / kr
     const int lg = a.kr_log2, kl = tid & ((1 << lg) - 1);
     if (kl < kc) {
-      const int64_t ko = __ldg(a.p_k_off + k0 + kl);
+      const int32_t ko = __ldg(a.p_k_off + k0 + kl);
       float* d = ps + kl * SK_LDP;
 #pragma unroll 4
       for (int w = tid >> lg; w < SK_BW; w += SK_THREADS >> lg) {
-        const int64_t po = pw[w];
+        const int32_t po = pw[w];
         if (po != SK_NONE)
           cp_async_elem<4>(d + w, a.P + po + ko);
         else
@@ -141,41 +184,46 @@ __device__ __forceinline__ void skinny_load(const SkinnyArgs& a, int c, float* p
       }
     }
   } else {
-    // lanes along the positions: thread tid takes position tid at every k
-    const int64_t po = pw[tid];
+    // lanes along the positions: thread tid takes position tid at every k;
+    // the chunk's k offsets are loaded once per warp (lane k) and passed
+    // around by shuffles, so no copy waits on a table load
+    const int32_t po = pw[tid];
+    const int32_t ko_lane = lane < kc ? __ldg(a.p_k_off + k0 + lane) : 0;
     float* d = ps + tid;
-    if (po != SK_NONE) {
-      const float* src = a.P + po;
+    const float* src = a.P + (po != SK_NONE ? po : 0);
 #pragma unroll 4
-      for (int k = 0; k < kc; ++k) cp_async_elem<4>(d + k * SK_LDP, src + __ldg(a.p_k_off + k0 + k));
-    } else {
-      for (int k = 0; k < kc; ++k) d[k * SK_LDP] = 0.0f;
+    for (int k = 0; k < kc; ++k) {
+      const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
+      if (po != SK_NONE)
+        cp_async_elem<4>(d + k * SK_LDP, src + ko);
+      else
+        d[k * SK_LDP] = 0.0f;
     }
   }
-  // Q rows [0, sq) of k [0, kc); rows >= S are zeros
+  // Q rows p sp .. p sp + sp - 1 of k [0, kc); rows >= S are zeros
+  const int s0 = j.p * sp;
   if (a.q_kfast) {
-    const int kl = tid & 31;
-    if (kl < kc) {
-      const int64_t ko = __ldg(a.q_k_off + k0 + kl);
-      for (int s = tid >> 5; s < sq; s += SK_THREADS / 32) {
-        float* d = qs + kl * qld + s;
-        if (s < a.S)
-          cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s) + ko);
+    if (lane < kc) {
+      const int32_t ko = __ldg(a.q_k_off + k0 + lane);
+      for (int r = tid >> 5; r < sp; r += SK_THREADS / 32) {
+        float* d = qs + lane * SK_QLD + r;
+        if (s0 + r < a.S)
+          cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s0 + r) + ko);
         else
           *d = 0.0f;
       }
     }
   } else {
-    for (int s = tid % sq, k = tid / sq; k < kc;) {
-      float* d = qs + k * qld + s;
-      if (s < a.S)
-        cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s) + __ldg(a.q_k_off + k0 + k));
+    for (int r = tid % sp, k = tid / sp; k < kc;) {
+      float* d = qs + k * SK_QLD + r;
+      if (s0 + r < a.S)
+        cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s0 + r) + __ldg(a.q_k_off + k0 + k));
       else
         *d = 0.0f;
-      s += SK_THREADS % sq;
-      k += SK_THREADS / sq;
-      if (s >= sq) {
-        s -= sq;
+      r += SK_THREADS % sp;
+      k += SK_THREADS / sp;
+      if (r >= sp) {
+        r -= sp;
         ++k;
       }
     }
@@ -183,183 +231,230 @@ __device__ __forceinline__ void skinny_load(const SkinnyArgs& a, int c, float* p
   cp_async_commit();
 }
 
-// Stores staged rows [s0, s0 + ns) of S (os[row - s0][position]) to C in
-// the walk's address order; 8 warps share the planes.
-__device__ __forceinline__ void skinny_store(const SkinnyArgs& a, const float* os,
-                                             const int64_t* cw, const int64_t* cs, int s0, int ns) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// One warp's share of a staged plane of L0 x L1 elements (i0 fastest, 32
+// consecutive elements per step): element (i, j) is box position w0 + wi i
+// + wj j of staged row r0 + ri i + rj j, stored at C + cw[w] + cs[r].
+// Positions and rows advance by fixed steps (one carry at most per step).
+__device__ __forceinline__ void skinny_plane(const SkinnyArgs& a, const float* os,
+                                             const int32_t* cw, const int32_t* cs, int L0, int L1,
+                                             int w0, int wi, int wj, int r0, int ri, int rj) {
+  const int lane = threadIdx.x & 31;
+  const int total = L0 * L1, di = 32 % L0, dj = 32 / L0;
+  int i = lane % L0;
+  const int j = lane / L0;
+  int w = w0 + wi * i + wj * j, r = r0 + ri * i + rj * j;
+  const int dw = wi * di + wj * dj, dr = ri * di + rj * dj;
+  const int cw_carry = wj - wi * L0, cr_carry = rj - ri * L0;
   const float alpha = a.alpha, beta = a.beta;
-  auto put = [&](int w, int r) {
-    const int64_t o = cw[w];
-    if (o == SK_NONE) return;
-    float* d = a.C + o + cs[s0 + r];
-    const float v = alpha * os[r * SK_LDP + w];
-    *d = beta != 0.0f ? fmaf(beta, *d, v) : v;
-  };
-  // plane of L0 x L1 elements (i0 fastest), 32 consecutive per step
-  auto plane = [&](int L0, int L1, auto&& elem) {
-    const int total = L0 * L1, di = 32 % L0, dj = 32 / L0;
-    int i = lane % L0, j = lane / L0;
-    for (int f = lane; f < total; f += 32) {
-      elem(i, j);
-      i += di;
-      j += dj;
-      if (i >= L0) {
-        i -= L0;
-        ++j;
-      }
+  for (int f = lane; f < total; f += 32) {
+    const int32_t o = cw[w];
+    if (o != SK_NONE) {
+      float* d = a.C + o + cs[r];
+      const float v = alpha * os[r * SK_LDP + w];
+      *d = beta != 0.0f ? fmaf(beta, *d, v) : v;
     }
-  };
+    i += di;
+    w += dw;
+    r += dr;
+    if (i >= L0) {
+      i -= L0;
+      w += cw_carry;
+      r += cr_carry;
+    }
+  }
+}
+
+// Stores staged rows [0, ns) (C rows s0 .. s0 + ns - 1; cs[r] = C offset of
+// row s0 + r) in the walk's address order; 8 warps share the planes.
+__device__ __forceinline__ void skinny_store(const SkinnyArgs& a, const float* os,
+                                             const int32_t* cw, const int32_t* cs, int s0, int ns) {
+  const int warp = threadIdx.x >> 5;
+  const bool py = a.p_walk == SK_P_Y;
+  const int tx = a.tx, ty = a.ty;
   if (a.c_walk == SK_C_XS) {
-    for (int yl = warp; yl < a.ty; yl += SK_THREADS / 32)
-      plane(a.tx, ns, [&](int xl, int r) { put(skinny_pos(a, xl, yl), r); });
+    for (int yl = warp; yl < ty; yl += SK_THREADS / 32)
+      skinny_plane(a, os, cw, cs, tx, ns, py ? yl : tx * yl, py ? ty : 1, 0, 0, 0, 1);
   } else if (a.c_walk == SK_C_XY) {
     for (int r = warp; r < ns; r += SK_THREADS / 32)
-      plane(a.tx, a.ty, [&](int xl, int yl) { put(skinny_pos(a, xl, yl), r); });
+      skinny_plane(a, os, cw, cs, tx, ty, 0, py ? ty : 1, py ? 1 : tx, r, 0, 0);
   } else {
     // runs of e0 consecutive rows (C stride one), clipped to [s0, s0 + ns)
     const int e0 = a.s_run;
     const int first = (s0 / e0) * e0;
     const int nruns = (s0 + ns - first + e0 - 1) / e0;
-    for (int job = warp; job < nruns * a.ty; job += SK_THREADS / 32) {
+    for (int job = warp; job < nruns * ty; job += SK_THREADS / 32) {
       const int run = job % nruns, yl = job / nruns;
       const int rs = first + run * e0;
       const int ra = rs > s0 ? rs : s0;
       const int rb = rs + e0 < s0 + ns ? rs + e0 : s0 + ns;
       if (rb <= ra) continue;
-      plane(rb - ra, a.tx, [&](int i, int xl) { put(skinny_pos(a, xl, yl), ra - s0 + i); });
+      skinny_plane(a, os, cw, cs, rb - ra, tx, py ? yl : tx * yl, 0, py ? ty : 1, ra - s0, 1, 0);
     }
   }
 }
 
-// One block of split z (partial != null) or of the whole K.
 template <int RS>
-__device__ __forceinline__ void skinny_block(const SkinnyArgs& a, int64_t b, int z, uint8_t* smem) {
-  constexpr int SP = 4 * RS;
-  float* Ps = reinterpret_cast<float*>(smem);
-  float* Qs = reinterpret_cast<float*>(smem + SK_P_BYTES);
-  int64_t* pw = reinterpret_cast<int64_t*>(smem + SK_P_BYTES + SK_Q_BYTES);
-  int64_t* cw = pw + SK_BW;
-  int64_t* cs = cw + SK_BW;
-  const int tid = threadIdx.x;
-  const int wg = tid & 63, sg = tid >> 6;  // positions 4 wg .. 4 wg + 3, rows sg RS .. sg RS + RS - 1
-  skinny_box(a, b, pw, cw);
-  if (!a.partial)
-    for (int s = tid; s < a.S; s += SK_THREADS) cs[s] = __ldg(a.c_s_off + s);
-  __syncthreads();
-
-  const int sq = SP * a.npass;  // rows of Q in shared memory
-  const int qld = sq + 4;
-  const int c0 = z * a.chunks_per_split;
-  const int c1 = c0 + a.chunks_per_split < a.nchunks ? c0 + a.chunks_per_split : a.nchunks;
-  float acc[RS][4];
-  auto clear = [&] {
+struct SkAcc {
+  float v[RS][4];
+  __device__ __forceinline__ void clear() {
 #pragma unroll
     for (int i = 0; i < RS; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-  };
-  auto fma_chunk = [&](const float* ps, const float* qs, int kc) {
-    const float* pp = ps + 4 * wg;
-    const float* qq = qs + sg * RS;
-#pragma unroll 2
-    for (int k = 0; k < kc; ++k) {
-      const float4 pv = *reinterpret_cast<const float4*>(pp + k * SK_LDP);
-      float q[RS];
-#pragma unroll
-      for (int i = 0; i < RS; i += 4) {
-        const float4 t = *reinterpret_cast<const float4*>(qq + k * qld + i);
-        q[i] = t.x; q[i + 1] = t.y; q[i + 2] = t.z; q[i + 3] = t.w;
-      }
-#pragma unroll
-      for (int i = 0; i < RS; ++i) {
-        acc[i][0] = fmaf(q[i], pv.x, acc[i][0]);
-        acc[i][1] = fmaf(q[i], pv.y, acc[i][1]);
-        acc[i][2] = fmaf(q[i], pv.z, acc[i][2]);
-        acc[i][3] = fmaf(q[i], pv.w, acc[i][3]);
-      }
-    }
-  };
-  auto kc_of = [&](int c) {
-    const int64_t k0 = (int64_t)c * SK_KC;
-    return a.K - k0 < SK_KC ? (int)(a.K - k0) : SK_KC;
-  };
-  // staged store of pass p's rows (32 at a time through P stage 1)
-  float* os = Ps + SK_KC * SK_LDP;
-  auto store_pass = [&](int p) {
-#pragma unroll 1
-    for (int h = 0; h < SP; h += SK_SUB) {
-      const int s0 = p * SP + h;
-      if (s0 >= a.S) break;
-      int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
-      if (ns > a.S - s0) ns = a.S - s0;
-      __syncthreads();  // the stage (and earlier staged rows) are no longer read
-#pragma unroll
-      for (int i = 0; i < RS; ++i) {
-        const int r = sg * RS + i - h;
-        if (r >= 0 && r < SK_SUB)
-          *reinterpret_cast<float4*>(os + r * SK_LDP + 4 * wg) =
-              make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-      }
-      __syncthreads();
-      skinny_store(a, os, cw, cs, s0, ns);
-    }
-  };
+      for (int j = 0; j < 4; ++j) v[i][j] = 0.0f;
+  }
+};
 
-  if (a.npass > 1) {
-    // one chunk (K <= 32), every row of Q at once, passes over S
-    skinny_load(a, 0, Ps, Qs, sq, qld, pw);
-    cp_async_wait<0>();
-    __syncthreads();
-    const int kc = kc_of(0);
-#pragma unroll 1
-    for (int p = 0; p < a.npass; ++p) {
-      clear();
-      fma_chunk(Ps, Qs + p * SP, kc);
-      store_pass(p);
+// acc += P chunk (positions 4 wg .. 4 wg + 3) x Q chunk (rows sg RS ..), k < kc
+template <int RS>
+__device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, const float* qs, int kc) {
+  const int tid = threadIdx.x;
+  const float* pp = ps + 4 * (tid & 63);
+  const float* qq = qs + (tid >> 6) * RS;
+#pragma unroll 2
+  for (int k = 0; k < kc; ++k) {
+    const float4 pv = *reinterpret_cast<const float4*>(pp + k * SK_LDP);
+    float q[RS];
+#pragma unroll
+    for (int i = 0; i < RS; i += 4) {
+      const float4 t = *reinterpret_cast<const float4*>(qq + k * SK_QLD + i);
+      q[i] = t.x; q[i + 1] = t.y; q[i + 2] = t.z; q[i + 3] = t.w;
     }
+#pragma unroll
+    for (int i = 0; i < RS; ++i) {
+      acc.v[i][0] = fmaf(q[i], pv.x, acc.v[i][0]);
+      acc.v[i][1] = fmaf(q[i], pv.y, acc.v[i][1]);
+      acc.v[i][2] = fmaf(q[i], pv.z, acc.v[i][2]);
+      acc.v[i][3] = fmaf(q[i], pv.w, acc.v[i][3]);
+    }
+  }
+}
+
+// The end of job j: raw sums to its k slice, or its pass's rows to C staged
+// 32 at a time through os (the P stage just consumed).
+template <int RS>
+__device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& j, const SkAcc<RS>& acc,
+                                              float* os, const int32_t* cw, const int32_t* cs) {
+  constexpr int SP = 4 * RS;
+  const int tid = threadIdx.x, wg = tid & 63, sg = tid >> 6;
+  if (a.partial) {
+    float* dst = a.partial + ((size_t)j.z * a.nblk + j.b) * SP * SK_BW + 4 * wg;
+#pragma unroll
+    for (int i = 0; i < RS; ++i)
+      *reinterpret_cast<float4*>(dst + (size_t)(sg * RS + i) * SK_BW) =
+          make_float4(acc.v[i][0], acc.v[i][1], acc.v[i][2], acc.v[i][3]);
     return;
   }
-
-  clear();
-  if (c0 < c1) skinny_load(a, c0, Ps, Qs, sq, qld, pw);
 #pragma unroll 1
-  for (int c = c0; c < c1; ++c) {
-    const int st = (c - c0) & 1;
-    if (c + 1 < c1) {
-      // the other stage was last read by chunk c - 1: all threads are past it
-      __syncthreads();
-      skinny_load(a, c + 1, Ps + (st ^ 1) * SK_KC * SK_LDP, Qs + (st ^ 1) * SK_KC * qld, sq, qld, pw);
+  for (int h = 0; h < SP; h += SK_SUB) {
+    const int s0 = j.p * SP + h;
+    if (s0 >= a.S) break;
+    int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
+    if (ns > a.S - s0) ns = a.S - s0;
+    __syncthreads();  // the stage's last reader (the FMAs, or the previous step's stores) is done
+#pragma unroll
+    for (int i = 0; i < RS; ++i) {
+      const int r = sg * RS + i - h;
+      if (r >= 0 && r < SK_SUB)
+        *reinterpret_cast<float4*>(os + r * SK_LDP + 4 * wg) =
+            make_float4(acc.v[i][0], acc.v[i][1], acc.v[i][2], acc.v[i][3]);
+    }
+    __syncthreads();
+    skinny_store(a, os, cw, cs + h, s0, ns);
+  }
+}
+
+// A CTA's sequence of jobs: global job indices j0, j0 + jstep, ... < njobs;
+// resolve(J) gives the job's item (its SkinnyArgs) and its index in the item.
+struct SkRef {
+  const SkinnyArgs* a;
+  int J;
+};
+
+template <int RS, typename Resolve>
+__device__ __forceinline__ void skinny_loop(int j0, int jstep, int njobs, Resolve&& resolve,
+                                            uint8_t* smem) {
+  constexpr int SP = 4 * RS;
+  float* Ps = reinterpret_cast<float*>(smem);
+  float* Qs = reinterpret_cast<float*>(smem + 2 * SK_P_STAGE);
+  int32_t* pw = reinterpret_cast<int32_t*>(smem + SK_OFF_TAB);  // [2][BW]
+  int32_t* cw = pw + 2 * SK_BW;                                  // [2][BW]
+  int32_t* cs = cw + 2 * SK_BW;                                  // [2][SPMAX]
+  if (j0 >= njobs) return;
+  // loop state: the current step (job jg of this CTA's sequence, chunk c of
+  // its [.., c1)), its P / Q stage st and its job's offset slot; the job's
+  // fields are recomputed where needed (fewer registers across the FMAs)
+  int jg = j0;
+  SkRef cur = resolve(jg);
+  int c, c1;
+  {
+    const SkJob job = skinny_job(*cur.a, cur.J);
+    c = job.c0;
+    c1 = job.c1;
+    skinny_begin(*cur.a, job.b, job.p, SP, pw, cw, cs);
+    __syncthreads();
+    skinny_issue(*cur.a, job, c, SP, Ps, Qs, pw);
+  }
+  int st = 0, slot = 0;
+  SkAcc<RS> acc;
+  acc.clear();
+#pragma unroll 1
+  while (true) {
+    // the step after: the job's next chunk, or the next job's first
+    const bool last = c + 1 >= c1;
+    const int jn = last ? jg + jstep : jg;
+    const bool has_next = jn < njobs;
+    SkRef nref = cur;
+    int nc = c + 1, nc1 = c1;
+    __syncthreads();  // stage st ^ 1 and job slot slot ^ 1 are free
+    if (has_next) {
+      const int ns = last ? slot ^ 1 : slot;
+      if (last) nref = resolve(jn);
+      const SkJob njob = skinny_job(*nref.a, nref.J);
+      if (last) {
+        nc = njob.c0;
+        nc1 = njob.c1;
+        skinny_begin(*nref.a, njob.b, njob.p, SP, pw + ns * SK_BW, cw + ns * SK_BW,
+                     cs + ns * SK_SPMAX);
+        __syncthreads();
+      }
+      skinny_issue(*nref.a, njob, nc, SP, Ps + (st ^ 1) * (SK_P_STAGE / 4),
+                   Qs + (st ^ 1) * (SK_Q_STAGE / 4), pw + ns * SK_BW);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
-    __syncthreads();
-    fma_chunk(Ps + st * SK_KC * SK_LDP, Qs + st * SK_KC * qld, kc_of(c));
+    __syncthreads();  // chunk c is in stage st
+    float* ps = Ps + st * (SK_P_STAGE / 4);
+    skinny_fma<RS>(acc, ps, Qs + st * (SK_Q_STAGE / 4), skinny_kc(*cur.a, c));
+    if (last) {
+      skinny_finish<RS>(*cur.a, skinny_job(*cur.a, cur.J), acc, ps, cw + slot * SK_BW,
+                        cs + slot * SK_SPMAX);
+      acc.clear();
+    }
+    if (!has_next) break;
+    if (last) {
+      slot ^= 1;
+      jg = jn;
+    }
+    cur = nref;
+    c = nc;
+    c1 = nc1;
+    st ^= 1;
   }
-  if (a.partial) {
-    float* dst = a.partial + ((size_t)z * a.nblk + b) * SP * SK_BW + 4 * wg;
-#pragma unroll
-    for (int i = 0; i < RS; ++i)
-      *reinterpret_cast<float4*>(dst + (size_t)(sg * RS + i) * SK_BW) =
-          make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-    return;
-  }
-  store_pass(0);
 }
 
 // C of block b = alpha * (slice 0 + slice 1 + ...) + beta * C, slices in order.
 template <int RS>
-__device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int64_t b, int splits,
-                                                    uint8_t* smem) {
+__device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int b, uint8_t* smem) {
   constexpr int SP = 4 * RS;
   float* os = reinterpret_cast<float*>(smem);
-  int64_t* pw = reinterpret_cast<int64_t*>(smem + SK_P_BYTES + SK_Q_BYTES);
-  int64_t* cw = pw + SK_BW;
-  int64_t* cs = cw + SK_BW;
+  int32_t* pw = reinterpret_cast<int32_t*>(smem + SK_OFF_TAB);
+  int32_t* cw = pw + 2 * SK_BW;
+  int32_t* cs = cw + 2 * SK_BW;
   const int tid = threadIdx.x;
-  skinny_box(a, b, pw, cw);
-  for (int s = tid; s < a.S; s += SK_THREADS) cs[s] = __ldg(a.c_s_off + s);
+  SkinnyArgs ac = a;
+  ac.partial = nullptr;  // stage the rows' C offsets
+  skinny_begin(ac, b, 0, SP, pw, cw, cs);
   const size_t slice = (size_t)a.nblk * SP * SK_BW;
   const float* src = a.partial + (size_t)b * SP * SK_BW + tid;
 #pragma unroll 1
@@ -371,11 +466,11 @@ __device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int64_t
     for (int r = 0; r < ns; ++r) {
       const float* p = src + (size_t)(h + r) * SK_BW;
       float v = p[0];
-      for (int zz = 1; zz < splits; ++zz) v = __fadd_rn(v, p[zz * slice]);
+      for (int z = 1; z < a.ksplit; ++z) v = __fadd_rn(v, p[z * slice]);
       os[r * SK_LDP + tid] = v;
     }
     __syncthreads();
-    skinny_store(a, os, cw, cs, h, ns);
+    skinny_store(a, os, cw, cs + h, h, ns);
   }
 }
 
@@ -384,52 +479,56 @@ __device__ __forceinline__ void skinny_dispatch(int rs, F&& f) {
   switch (rs) {
     case 4: f(std::integral_constant<int, 4>()); break;
     case 8: f(std::integral_constant<int, 8>()); break;
-    case 12: f(std::integral_constant<int, 12>()); break;
-    default: f(std::integral_constant<int, 16>()); break;
+    default: f(std::integral_constant<int, 12>()); break;
   }
 }
 
-// grid (blocks, k slices)
-__global__ void __launch_bounds__(SK_THREADS, 2) skinny_gett_kernel(const SkinnyArgs a) {
+// persistent grid (at most two CTAs per SM) over the plan's jobs; one
+// instantiation per rows-per-thread class (RS = a.rs)
+template <int RS>
+__global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
+    skinny_gett_kernel(const __grid_constant__ SkinnyArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   grid_dep_wait();
-  skinny_dispatch(a.rs, [&](auto r) { skinny_block<decltype(r)::value>(a, blockIdx.x, blockIdx.y, smem); });
+  auto resolve = [&](int J) { return SkRef{&a, J}; };
+  skinny_loop<RS>(blockIdx.x, gridDim.x, a.njobs, resolve, smem);
 }
 
 // grid (blocks)
-__global__ void __launch_bounds__(SK_THREADS, 2) skinny_reduce_kernel(const SkinnyArgs a, int splits) {
+__global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
+    skinny_reduce_kernel(const __grid_constant__ SkinnyArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   grid_dep_wait();  // slices written by the kernel before
-  skinny_dispatch(a.rs, [&](auto r) { skinny_reduce_block<decltype(r)::value>(a, blockIdx.x, splits, smem); });
+  skinny_dispatch(a.rs, [&](auto r) { skinny_reduce_block<decltype(r)::value>(a, blockIdx.x, smem); });
 }
 
-// Grouped launches: item i owns CTAs [begin[i], begin[i + 1]) -- (block,
-// slice) pairs of its contraction, or its blocks in the reduction.
+// Grouped launches. Contraction items: item i owns the global job indices
+// [begin[i], begin[i + 1]); one persistent launch per rows-per-thread class
+// (RS = the items' rs) walks all of them. Reduction items:
+// CTAs [begin[i], begin[i + 1]) are the blocks of a k-split item.
 struct SkinnyItem {
   SkinnyArgs args;
   int64_t begin;
-  int32_t ksplit;
 };
 
-__global__ void __launch_bounds__(SK_THREADS, 2) skinny_group_kernel(const SkinnyItem* items,
-                                                                      const int64_t* begin, int n) {
+template <int RS>
+__global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
+    skinny_group_kernel(const SkinnyItem* items, const int64_t* begin, int n, int njobs) {
   extern __shared__ __align__(16) uint8_t smem[];
-  const int64_t t = blockIdx.x;
-  const SkinnyItem& it = items[find_segment(begin, n, t)];
-  const int64_t local = t - it.begin;
-  const int64_t b = local % it.args.nblk;
-  const int z = (int)(local / it.args.nblk);
-  skinny_dispatch(it.args.rs, [&](auto r) { skinny_block<decltype(r)::value>(it.args, b, z, smem); });
+  auto resolve = [&](int J) {
+    const SkinnyItem& it = items[find_segment(begin, n, J)];
+    return SkRef{&it.args, (int)(J - it.begin)};
+  };
+  skinny_loop<RS>(blockIdx.x, gridDim.x, njobs, resolve, smem);
 }
 
-__global__ void __launch_bounds__(SK_THREADS, 2) skinny_reduce_group_kernel(const SkinnyItem* items,
-                                                                             const int64_t* begin,
-                                                                             int n) {
+__global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
+    skinny_reduce_group_kernel(const SkinnyItem* items, const int64_t* begin, int n) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int64_t t = blockIdx.x;
   const SkinnyItem& it = items[find_segment(begin, n, t)];
   skinny_dispatch(it.args.rs, [&](auto r) {
-    skinny_reduce_block<decltype(r)::value>(it.args, t - it.begin, it.ksplit, smem);
+    skinny_reduce_block<decltype(r)::value>(it.args, (int)(t - it.begin), smem);
   });
 }
 

@@ -116,8 +116,10 @@ struct tccg_plan {
   bool skinny = false, sk_s_is_n = false;
   int32_t sk_ksplit = 1;
   SkinnyArgs sk{};
-  int64_t* t_p_y = nullptr;
-  int64_t* t_c_y = nullptr;
+  // its 32-bit offset tables in one allocation: P and C offsets of the Y
+  // space, P's k, Q's rows and k, C's rows (start of each in sk_tab[])
+  int32_t* t_sk = nullptr;
+  size_t sk_tab[6] = {};
   // workspace layout
   size_t off_a = 0, off_b = 0, off_part = 0, off_cprime = 0, off_tail = 0, ws_bytes = 0;
   char describe[512] = "";
@@ -419,13 +421,12 @@ static int32_t pick_read_k_fast(int nr, const int64_t* rext, const int64_t* rstr
 
 // ---- skinny kernel: eligibility, geometry and model ----------------------
 // FP32 operands (FP32 accumulation serves BF16X3 as well: more accurate
-// than its three-product split), GETT, a narrow side of at most 64 rows (any
-// K), or of at most 256 with K <= 32 (several passes over one chunk).
+// than its three-product split), GETT, a narrow side of at most 256 rows (one
+// pass of up to 64 rows, or passes of 32 / 64 rows).
 static bool skinny_eligible(const tccg_plan* p) {
   if (p->dtype != TCCG_F32 || (p->prec != TCCG_PREC_FP32 && p->prec != TCCG_PREC_BF16X3)) return false;
   if (p->tune.method != TCCG_METHOD_GETT || p->tune.pair) return false;
-  const int64_t S = std::min(p->M, p->N);
-  return (S <= 64 || (S <= SK_SMAX && p->K <= SK_KC)) && p->K <= INT32_MAX;
+  return std::min(p->M, p->N) <= SK_SMAX && p->K <= INT32_MAX;
 }
 
 static long long abs_ll(int64_t v) { return v < 0 ? -(long long)v : (long long)v; }
@@ -464,11 +465,23 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
     if (i != X && wext[i] > 1) ym.push_back(i);
   std::stable_sort(ym.begin(), ym.end(), [&](int u, int v) { return abs_ll(wp[u]) < abs_ll(wp[v]); });
   *xmode = X;
-  a.ex = X >= 0 ? wext[X] : 1;
-  a.px = X >= 0 ? wp[X] : 0;
-  a.cx = X >= 0 ? wc[X] : 0;
-  a.ey = 1;
-  for (int i : ym) a.ey *= wext[i];
+  // 32-bit offsets: every element offset of P, Q and C below 2^31
+  auto span = [](int n, const int64_t* ext, const int64_t* str) {
+    long long t = 0;
+    for (int i = 0; i < n; ++i) t += (long long)(ext[i] - 1) * abs_ll(str[i]);
+    return t;
+  };
+  const long long lim = INT32_MAX;
+  if (span(nw, wext, wp) + span(d.nk, d.k_ext, kp) >= lim ||
+      span(nsm, sext, sq) + span(d.nk, d.k_ext, kq) >= lim ||
+      span(nw, wext, wc) + span(nsm, sext, sc) >= lim || p->K >= lim)
+    return false;
+  a.ex = (int32_t)(X >= 0 ? wext[X] : 1);
+  a.px = (int32_t)(X >= 0 ? wp[X] : 0);
+  a.cx = (int32_t)(X >= 0 ? wc[X] : 0);
+  int64_t ey = 1;
+  for (int i : ym) ey *= wext[i];
+  a.ey = (int32_t)ey;
   // P loads along its stride-one direction
   const long long px = X >= 0 ? abs_ll(wp[X]) : LLONG_MAX;
   const long long py = ym.empty() ? LLONG_MAX : abs_ll(wp[ym[0]]);
@@ -488,8 +501,9 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   a.tx = (int32_t)tx;
   a.ty = (int32_t)ty;
   a.bxn = (int32_t)cdiv(a.ex, tx);
-  a.nblk = (int64_t)a.bxn * cdiv(a.ey, ty);
-  if (a.nblk > INT32_MAX) return false;
+  const int64_t nblk = (int64_t)a.bxn * cdiv(a.ey, ty);
+  if (nblk > INT32_MAX / 4) return false;
+  a.nblk = (int32_t)nblk;
   // C walk: C's stride-one index on the narrow side (runs of that S mode,
   // when it is the first one), else X then the next C stride's side
   const long long cs = min_abs_stride(nsm, sext, sc), cx = X >= 0 ? abs_ll(wc[X]) : LLONG_MAX;
@@ -507,16 +521,17 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
     }
   }
   a.q_kfast = min_abs_stride(d.nk, d.k_ext, kq) < min_abs_stride(nsm, sext, sq) ? 1 : 0;
-  // rows per thread: one pass of the smallest of 16 / 32 / 48 / 64 rows; a
-  // longer S (K <= 32) passes of 32 or 64 rows, the least padding
+  // rows per thread: one pass of the smallest of 16 / 32 / 48 rows; a longer
+  // S runs passes of 32 rows (the passes of a block are neighbouring jobs:
+  // their P chunks come from L2). 64-row passes (16 rows per thread) need
+  // more than the 128 registers two CTAs per SM leave a thread.
   const int64_t S = sn ? p->N : p->M;
-  if (S <= 64) {
+  if (S <= 48) {
     a.rs = (int32_t)std::max<int64_t>(4, round_up(cdiv(S, 4), 4));
     a.npass = 1;
   } else {
-    const int64_t p32 = round_up(S, 32), p64 = round_up(S, 64);
-    a.rs = p64 <= p32 ? 16 : 8;
-    a.npass = (int32_t)cdiv(S, 4 * a.rs);
+    a.rs = 8;
+    a.npass = (int32_t)cdiv(S, 32);
   }
   a.S = (int32_t)S;
   a.K = (int32_t)p->K;
@@ -524,14 +539,19 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   int lg = 0;
   while ((1 << lg) < std::min<int64_t>(p->K, SK_KC)) ++lg;
   a.kr_log2 = lg;
-  // k-split: blocks that cannot fill two CTAs per SM, slices of >= 4 chunks
+  // k-split (one pass only): blocks that cannot fill the persistent CTAs,
+  // slices of >= 4 chunks
   if (a.npass == 1) {
-    a.chunks_per_split = (int32_t)choose_ksplit(p->tune.ksplit, a.nblk, a.nchunks,
-                                                2 * (int64_t)p->num_sms, 4, &p->sk_ksplit);
+    a.chunks_per_split = (int32_t)choose_ksplit(
+        p->tune.ksplit, a.nblk, a.nchunks, (int64_t)SK_CTAS_PER_SM * p->num_sms, 4, &p->sk_ksplit);
   } else {
     a.chunks_per_split = a.nchunks;
     p->sk_ksplit = 1;
   }
+  a.ksplit = p->sk_ksplit;
+  const int64_t njobs = (int64_t)a.nblk * a.npass * a.ksplit;
+  if (njobs > INT32_MAX) return false;
+  a.njobs = (int32_t)njobs;
   a.alpha = 1.0f;
   a.beta = 0.0f;
   return true;
@@ -555,6 +575,16 @@ static double skinny_time(const tccg_plan* p) {
   return std::max(fma, bytes / 5.5e12) + (p->sk_ksplit > 1 ? 8e-6 : 4e-6);
 }
 
+// The persistent skinny kernel of a rows-per-thread class (4, 8 or 12).
+template <typename F>
+static void with_skinny_rs(int rs, F&& f) {
+  switch (rs) {
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 8: f(std::integral_constant<int, 8>()); break;
+    default: f(std::integral_constant<int, 12>()); break;
+  }
+}
+
 // Whether the plan runs the skinny kernel: asked for, or -- unless the
 // tuning asks for another kernel family -- when its model beats the others'.
 static bool choose_skinny(const tccg_plan* p) {
@@ -572,10 +602,11 @@ static bool choose_skinny(const tccg_plan* p) {
 static void plan_free(tccg_plan* p) {
   if (!p) return;
   int64_t* ts[] = {p->t_a_m, p->t_a_k, p->t_b_n, p->t_b_k, p->t_c_m, p->t_c_n, p->t_id_m, p->t_id_n,
-                   p->t_a_vsrc, p->t_a_vdst, p->t_b_vsrc, p->t_b_vdst, p->t_p_y, p->t_c_y};
+                   p->t_a_vsrc, p->t_a_vdst, p->t_b_vsrc, p->t_b_vdst};
   for (auto t : ts)
     if (t) cudaFree(t);
   if (p->d_status) cudaFree(p->d_status);
+  if (p->t_sk) cudaFree(p->t_sk);
   delete p;
 }
 
@@ -811,8 +842,8 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
     if (p->tune.skinny > 0 && !eligible) {
       plan_free(p);
       return fail(TCCG_ERR_UNSUPPORTED,
-                  "the skinny kernel needs FP32 operands, FP32 or BF16X3 precision, GETT and "
-                  "min(M, N) <= 64 (or <= 256 with K <= 32)");
+                  "the skinny kernel needs FP32 operands, FP32 or BF16X3 precision, GETT, "
+                  "min(M, N) <= 256 and tensors of fewer than 2^31 elements");
     }
     p->skinny = eligible && choose_skinny(p);
     if (p->skinny) {
@@ -823,10 +854,26 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
         sp[i] = sn ? d.a_m_stride[ym[i]] : d.b_n_stride[ym[i]];
         scc[i] = sn ? d.c_m_stride[ym[i]] : d.c_n_stride[ym[i]];
       }
-      build_offsets((int)ym.size(), ext, sp, h);
-      rc = upload(h, &p->t_p_y);
-      build_offsets((int)ym.size(), ext, scc, h);
-      if (!rc) rc = upload(h, &p->t_c_y);
+      const int nsm = sn ? d.nn : d.nm;
+      const int64_t* sext = sn ? d.n_ext : d.m_ext;
+      // P / C offsets of the Y space, P's k, Q's rows and k, C's rows
+      std::vector<int32_t> tab;
+      auto add = [&](int n, const int64_t* e, const int64_t* st, int slot) {
+        build_offsets(n, e, st, h);
+        p->sk_tab[slot] = tab.size();
+        for (int64_t v : h) tab.push_back((int32_t)v);
+        while (tab.size() % 4) tab.push_back(0);  // 16-byte aligned starts
+      };
+      add((int)ym.size(), ext, sp, 0);
+      add((int)ym.size(), ext, scc, 1);
+      add(d.nk, d.k_ext, sn ? d.a_k_stride : d.b_k_stride, 2);
+      add(nsm, sext, sn ? d.b_n_stride : d.a_m_stride, 3);
+      add(d.nk, d.k_ext, sn ? d.b_k_stride : d.a_k_stride, 4);
+      add(nsm, sext, sn ? d.c_n_stride : d.c_m_stride, 5);
+      e = cudaMalloc((void**)&p->t_sk, tab.size() * sizeof(int32_t));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(p->t_sk, tab.data(), tab.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) rc = fail(TCCG_ERR_CUDA, "skinny tables: %s", cudaGetErrorString(e));
     }
   }
   p->simt = !p->skinny && choose_simt(p);
@@ -894,11 +941,13 @@ static int plan_layout(tccg_plan* p) {
     static const char* cw[] = {"xs", "xy", "sx"};
     snprintf(p->describe, sizeof(p->describe),
              "method=GETT prec=%s kernel=skinny_gett<f32> M=%lld N=%lld K=%lld narrow=%s S=%d "
-             "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d load=%s%s "
-             "store=%s%s pack=none",
+             "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
+             "grid=%lld load=%s%s store=%s%s pack=none",
              p->prec == TCCG_PREC_BF16X3 ? "bf16x3" : "fp32", (long long)p->M, (long long)p->N,
              (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S, a.npass, 4 * a.rs, a.tx, a.ty,
              (long long)a.ex, (long long)a.ey, (long long)a.nblk, a.nchunks, p->sk_ksplit,
+             (long long)a.njobs,
+             (long long)std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms),
              pw[a.p_walk], a.q_kfast ? " q=k" : " q=s", cw[a.c_walk],
              a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "");
     p->ws_bytes = ws;
@@ -1192,11 +1241,14 @@ static cudaError_t set_attrs() {
                            (int)simt_group_smem_bytes<float>()));
   chk(cudaFuncSetAttribute(simt_gett_group_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)simt_group_smem_bytes<double>()));
-  chk(cudaFuncSetAttribute(skinny_gett_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)SK_SMEM_BYTES));
+  for (int rs = 4; rs <= 12; rs += 4)
+    with_skinny_rs(rs, [&](auto r) {
+      chk(cudaFuncSetAttribute(skinny_gett_kernel<decltype(r)::value>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SK_SMEM_BYTES));
+      chk(cudaFuncSetAttribute(skinny_group_kernel<decltype(r)::value>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SK_SMEM_BYTES));
+    });
   chk(cudaFuncSetAttribute(skinny_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)SK_SMEM_BYTES));
-  chk(cudaFuncSetAttribute(skinny_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SK_SMEM_BYTES));
   chk(cudaFuncSetAttribute(skinny_reduce_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SK_SMEM_BYTES));
@@ -1715,12 +1767,12 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
   a.P = static_cast<const float*>(sn ? GA : GB);
   a.Q = static_cast<const float*>(sn ? GB : GA);
   a.C = C;
-  a.p_y_off = p->t_p_y;
-  a.c_y_off = p->t_c_y;
-  a.p_k_off = sn ? p->t_a_k : p->t_b_k;
-  a.q_s_off = sn ? p->t_b_n : p->t_a_m;
-  a.q_k_off = sn ? p->t_b_k : p->t_a_k;
-  a.c_s_off = sn ? p->t_c_n : p->t_c_m;
+  a.p_y_off = p->t_sk + p->sk_tab[0];
+  a.c_y_off = p->t_sk + p->sk_tab[1];
+  a.p_k_off = p->t_sk + p->sk_tab[2];
+  a.q_s_off = p->t_sk + p->sk_tab[3];
+  a.q_k_off = p->t_sk + p->sk_tab[4];
+  a.c_s_off = p->t_sk + p->sk_tab[5];
   a.alpha = alpha;
   a.beta = beta;
   a.partial = p->sk_ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
@@ -1730,15 +1782,18 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
 static int run_skinny(const tccg_plan* p, const void* GA, const void* GB, float* C, float alpha,
                       float beta, char* w, cudaStream_t s) {
   const SkinnyArgs a = skinny_args(p, GA, GB, C, alpha, beta, w);
+  const int64_t grid = std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms);
   mark(1, 0, s);
-  launch_after(false, p, skinny_gett_kernel, dim3((unsigned)a.nblk, (unsigned)p->sk_ksplit),
-               dim3(SK_THREADS), SK_SMEM_BYTES, s, a);
+  with_skinny_rs(a.rs, [&](auto r) {
+    launch_after(false, p, skinny_gett_kernel<decltype(r)::value>, dim3((unsigned)grid),
+                 dim3(SK_THREADS), SK_SMEM_BYTES, s, a);
+  });
   int rc = launch_check("skinny_gett");
   mark(1, 1, s);
   if (rc || p->sk_ksplit == 1) return rc;
   mark(2, 0, s);
   launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)a.nblk), dim3(SK_THREADS),
-               SK_SMEM_BYTES, s, a, (int)p->sk_ksplit);
+               SK_SMEM_BYTES, s, a);
   rc = launch_check("skinny_reduce");
   mark(2, 1, s);
   return rc;
@@ -2045,8 +2100,10 @@ struct tccg_group {
     int64_t lane_tiles[TCV_COUNT] = {};
     int32_t tcj0 = 0, ntcj = 0;  // pack jobs of the packed-operand lanes (two per item)
     int64_t simt_tiles = 0, simt_pack_ctas = 0, tc_pack_ctas = 0, red_ctas = 0;
-    int32_t sk0 = 0, nsk = 0, skr0 = 0, nskr = 0;  // skinny items and their reductions
-    int64_t sk_ctas = 0, skr_ctas = 0;
+    // skinny lanes, one per rows-per-thread class (rs / 4 - 1: 4, 8, 12): items
+    // [sk0[c], sk0[c] + nsk[c]) of d_sk with sk_jobs[c] jobs; reductions
+    int32_t sk0[3] = {}, nsk[3] = {}, skr0 = 0, nskr = 0;
+    int64_t sk_jobs[3] = {}, skr_ctas = 0;
   };
   std::vector<Wave> waves;
   bool bound = false;
@@ -2117,13 +2174,14 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     ws += need;
     g->ws_bytes = std::max(g->ws_bytes, ws);
     if (p->skinny) {
-      wv.sk_ctas += p->sk.nblk * p->sk_ksplit;
+      wv.sk_jobs[p->sk.rs / 4 - 1] += p->sk.njobs;
     } else if (simt_path(p)) {
       wv.simt_tiles += (p->Mp / p->simt_bm) * (p->Np / p->simt_bn) * p->ksplit;
     } else {
       wv.lane_tiles[p->tcv] += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
-    bool too_many = wv.simt_tiles > INT32_MAX || wv.sk_ctas > INT32_MAX;
+    bool too_many = wv.simt_tiles > INT32_MAX;
+    for (int c = 0; c < 3; ++c) too_many |= wv.sk_jobs[c] > INT32_MAX;
     for (int v = 0; v < TCV_COUNT; ++v) too_many |= wv.lane_tiles[v] > INT32_MAX;
     if (too_many) {
       group_free(g);
@@ -2367,44 +2425,47 @@ static int bind_tc(tccg_group* g, tccg_group::Wave& wv, const void* const* A, co
   return TCCG_OK;
 }
 
-// The skinny lane of one wave: its items (the longest k slices first) and
-// the reductions of those with a k-split, first CTAs counted from 0 within
-// the wave.
+// The skinny lanes of one wave (one per rows-per-thread class; in each the
+// items with the longest k slices first: a CTA takes jobs in index order)
+// and the reductions of the items with a k-split; job and CTA indices
+// counted from 0 within the lane.
 static void bind_skinny(tccg_group* g, tccg_group::Wave& wv, const void* const* A,
                         const void* const* B, void* const* C, const double* alpha,
                         const double* beta, char* ws, std::vector<SkinnyItem>& items,
                         std::vector<SkinnyItem>& red) {
-  wv.sk0 = (int32_t)items.size();
   wv.skr0 = (int32_t)red.size();
-  std::vector<size_t> idx;
-  for (size_t i : wv.items)
-    if (g->plans[i]->skinny) idx.push_back(i);
-  std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
-    return g->plans[a]->sk.chunks_per_split > g->plans[b]->sk.chunks_per_split;
-  });
-  int64_t ctas = 0, rctas = 0;
-  for (size_t i : idx) {
-    const tccg_plan* p = g->plans[i];
-    const void* GA = p->d.swap_ab ? B[i] : A[i];
-    const void* GB = p->d.swap_ab ? A[i] : B[i];
-    SkinnyItem it;
-    memset(&it, 0, sizeof(it));
-    it.args = skinny_args(p, GA, GB, static_cast<float*>(C[i]), (float)alpha[i], (float)beta[i],
-                          ws + g->ws_off[i]);
-    it.begin = ctas;
-    it.ksplit = p->sk_ksplit;
-    ctas += p->sk.nblk * p->sk_ksplit;
-    items.push_back(it);
-    if (p->sk_ksplit > 1) {
-      SkinnyItem r = it;
-      r.begin = rctas;
-      rctas += p->sk.nblk;
-      red.push_back(r);
+  int64_t rctas = 0;
+  for (int cls = 0; cls < 3; ++cls) {
+    wv.sk0[cls] = (int32_t)items.size();
+    std::vector<size_t> idx;
+    for (size_t i : wv.items)
+      if (g->plans[i]->skinny && g->plans[i]->sk.rs / 4 - 1 == cls) idx.push_back(i);
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+      return g->plans[a]->sk.chunks_per_split > g->plans[b]->sk.chunks_per_split;
+    });
+    int64_t jobs = 0;
+    for (size_t i : idx) {
+      const tccg_plan* p = g->plans[i];
+      const void* GA = p->d.swap_ab ? B[i] : A[i];
+      const void* GB = p->d.swap_ab ? A[i] : B[i];
+      SkinnyItem it;
+      memset(&it, 0, sizeof(it));
+      it.args = skinny_args(p, GA, GB, static_cast<float*>(C[i]), (float)alpha[i],
+                            (float)beta[i], ws + g->ws_off[i]);
+      it.begin = jobs;
+      jobs += p->sk.njobs;
+      items.push_back(it);
+      if (p->sk_ksplit > 1) {
+        SkinnyItem r = it;
+        r.begin = rctas;
+        rctas += p->sk.nblk;
+        red.push_back(r);
+      }
     }
+    wv.nsk[cls] = (int32_t)items.size() - wv.sk0[cls];
+    wv.sk_jobs[cls] = jobs;
   }
-  wv.nsk = (int32_t)items.size() - wv.sk0;
   wv.nskr = (int32_t)red.size() - wv.skr0;
-  wv.sk_ctas = ctas;
   wv.skr_ctas = rctas;
 }
 
@@ -2543,9 +2604,14 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
     if ((rc = launch_check("gett_tc_group"))) return rc;
   }
   if constexpr (sizeof(T) == 4) {
-    if (wv.nsk > 0) {
-      skinny_group_kernel<<<(unsigned)wv.sk_ctas, SK_THREADS, SK_SMEM_BYTES, s>>>(
-          g->d_sk + wv.sk0, g->b_sk + wv.sk0, wv.nsk);
+    for (int cls = 0; cls < 3; ++cls) {
+      if (wv.nsk[cls] == 0) continue;
+      const unsigned grid =
+          (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SK_CTAS_PER_SM * g->num_sms);
+      with_skinny_rs(4 * (cls + 1), [&](auto r) {
+        skinny_group_kernel<decltype(r)::value><<<grid, SK_THREADS, SK_SMEM_BYTES, s>>>(
+            g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], wv.sk_jobs[cls]);
+      });
       if ((rc = launch_check("skinny_group"))) return rc;
     }
     if (wv.nskr > 0) {

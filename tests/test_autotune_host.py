@@ -62,12 +62,16 @@ def test_bf16_candidates_start_with_the_library_choice(precision):
 
 
 def test_split_bf16x3_searches_both_loaders_first():
-    """BF16x3 with FP32 operands: right after the library's own choice, the
-    packed 128x192 tiles (load 1), the gathered 128x128 tiles (load 2) and
-    the CUDA cores, so that --maxImplementations=4 already compares them."""
+    """BF16x3 with FP32 operands: right after the library's own choice (and
+    the skinny kernel where it applies), the packed 128x192 tiles (load 1),
+    the gathered 128x128 tiles (load 2) and the CUDA cores, so that
+    --maxImplementations=5 already compares them."""
     for name in SHAPES:
         cs = candidates(_con(name), "bf16x3", methods=("gett",))
-        assert [(t.load, t.variant) for t in cs[:4]] == [(0, 0), (1, 0), (2, 0), (0, -1)]
+        con = _con(name)
+        sk = int(min(con.sizeM, con.sizeN) <= 256)
+        assert [t.skinny for t in cs[:1 + sk]] == [0] + [1] * sk
+        assert [(t.load, t.variant) for t in cs[sk:4 + sk]] == [(0, 0), (1, 0), (2, 0), (0, -1)]
     # not for TTGT (its GEMM reads the transposed operands) nor BF16 operands
     cs = candidates(_con("square"), "bf16x3", methods=("ttgt",))
     assert all(t.load == 0 for t in cs)

@@ -76,10 +76,13 @@ def test_narrow_tile_with_k_split(cuda, name):
 
 
 def test_automatic_shape(cuda):
+    # the tile kernel's own choice (the skinny kernel, which may take these
+    # shapes, held off)
+    off = Tuning(skinny=-1)
     small_n = make_contraction("mn", "mk", "kn", dict(m=4096, n=16, k=1024))
-    assert "tile=128x32x16" in Plan(small_n, precision="fp32").describe()
+    assert "tile=128x32x16" in Plan(small_n, precision="fp32", tuning=off).describe()
     small_m = make_contraction("mn", "mk", "kn", dict(m=24, n=4096, k=1024))
-    assert "tile=32x128x16" in Plan(small_m, precision="fp32").describe()
+    assert "tile=32x128x16" in Plan(small_m, precision="fp32", tuning=off).describe()
     square = make_contraction("mn", "mk", "kn", dict(m=1000, n=1000, k=64))
     assert "tile=128x128x16" in Plan(square, precision="fp32").describe()
     # FP64 keeps its one tile

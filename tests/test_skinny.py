@@ -33,7 +33,7 @@ CASES = {
     # P's stride-one index is contracted (u): loads along k
     "kfast": ("fjr", "ufr", "ju", dict(f=10, j=28, r=46, u=8), 1.0, 0.25,
               ["narrow=N", "load=k", "store=xs"]),
-    # S = 150 rows over several passes (K = 18 <= 32)
+    # S = 150 rows in five passes of 32
     "passes": ("orak", "cok", "rac", dict(o=10, r=37, a=9, k=15, c=18), -0.75, 0.0,
                ["narrow=M", "rows=5x32", "store=sx run=10"]),
     # C's next stride after X is a W mode: (x, y) planes; K over three chunks

@@ -1,9 +1,10 @@
 """CPU replay of the skinny kernel's index arithmetic
-(tccg_b200/csrc/skinny_gett.cuh): the block boxes over the W positions, the
+(tccg_b200/csrc/skinny_gett.cuh): the jobs (block x pass x k slice) and a
+persistent CTA's walk over them, the block boxes over the W positions, the
 three P load walks and both Q load walks of a k chunk, the epilogue's row
-staging over passes, and the three C store walks with their division-free
-(i, j) stepping. Each element is touched exactly once, and every store
-instruction of a whole run covers 32 consecutive C addresses.
+staging, and the three C store walks with their stepping of positions and
+rows. Each element is touched exactly once, and every store instruction of a
+whole run covers 32 consecutive C addresses.
 """
 import itertools
 
@@ -83,92 +84,164 @@ def test_p_chunk_loads_each_element_once(p_walk, K):
             assert [k for k, _ in lanes[: 1 << kr_log2]] == list(range(1 << kr_log2))
 
 
-def q_loads(q_kfast, sq, kc):
+QLD = 52
+
+
+def q_loads(q_kfast, sp, kc):
     out = []
     for tid in range(THREADS):
         if q_kfast:
-            kl = tid & 31
-            if kl < kc:
-                out += [(kl, s) for s in range(tid >> 5, sq, THREADS // 32)]
+            lane = tid & 31
+            if lane < kc:
+                out += [(lane, r) for r in range(tid >> 5, sp, THREADS // 32)]
         else:
-            s, k = tid % sq, tid // sq
+            r, k = tid % sp, tid // sp
             while k < kc:
-                out.append((k, s))
-                s += THREADS % sq
-                k += THREADS // sq
-                if s >= sq:
-                    s -= sq
+                out.append((k, r))
+                r += THREADS % sp
+                k += THREADS // sp
+                if r >= sp:
+                    r -= sp
                     k += 1
     return out
 
 
 @pytest.mark.parametrize("q_kfast", [0, 1])
-@pytest.mark.parametrize("sq", [16, 32, 48, 64, 96, 128, 160, 192, 256])
+@pytest.mark.parametrize("sp", [16, 32, 48])
 @pytest.mark.parametrize("kc", [1, 7, 20, 32])
-def test_q_chunk_loads_each_element_once(q_kfast, sq, kc):
-    got = q_loads(q_kfast, sq, kc)
-    assert sorted(got) == [(k, s) for k in range(kc) for s in range(sq)]
-    qld = sq + 4
-    assert all(k * qld + s < KC * (256 + 4) for k, s in got)  # inside the Q region
+def test_q_chunk_loads_each_element_once(q_kfast, sp, kc):
+    got = q_loads(q_kfast, sp, kc)
+    assert sorted(got) == [(k, r) for k in range(kc) for r in range(sp)]
+    assert all(k * QLD + r < KC * QLD for k, r in got)  # inside one Q stage
 
 
-def stage_rows(rs, S, npass):
-    """store_pass: the (pass, thread row i) -> staged (step s0, row r) map."""
+def jobs(nblk, npass, ksplit, nchunks, cps):
+    """skinny_job over J in [0, nblk npass ksplit): (b, p, z, c0, c1)."""
+    out = []
+    for J in range(nblk * npass * ksplit):
+        z = J % ksplit
+        r = J // ksplit
+        p, b = r % npass, r // npass
+        c0 = z * cps
+        out.append((b, p, z, c0, min(c0 + cps, nchunks)))
+    return out
+
+
+@pytest.mark.parametrize("nblk,npass,ksplit,nchunks", [(7, 1, 1, 1), (3, 5, 1, 1), (2, 1, 16, 77),
+                                                       (18, 1, 16, 3075), (5, 4, 1, 40), (1, 1, 3, 3)])
+def test_jobs_cover_blocks_passes_and_chunks(nblk, npass, ksplit, nchunks):
+    cps = -(-nchunks // ksplit)
+    js = jobs(nblk, npass, ksplit, nchunks, cps)
+    seen = {}
+    for b, p, z, c0, c1 in js:
+        assert c0 < c1  # no empty slice (the host picks ksplit = ceil(nchunks / cps))
+        for c in range(c0, c1):
+            assert (b, p, c) not in seen
+            seen[(b, p, c)] = z
+    assert len(seen) == nblk * npass * nchunks
+    # the passes of a block are neighbouring jobs (one slice): their P chunks
+    # are read by CTAs that run at the same time
+    if ksplit == 1:
+        assert [(b, p) for b, p, *_ in js] == [(b, p) for b in range(nblk) for p in range(npass)]
+
+
+@pytest.mark.parametrize("njobs,grid", [(1, 296), (296, 296), (1000, 296), (20198, 296), (5, 2)])
+def test_persistent_steps(njobs, grid):
+    """skinny_loop: CTA j0 takes jobs j0, j0 + grid, ...; its job slot
+    alternates per job and its stage per step (chunk), so the next step's
+    copies never land in the stage or slot the current step reads."""
+    chunks = lambda J: 1 + (J * 7) % 3
+    taken = []
+    for cta in range(min(grid, njobs)):
+        jg, slot, st, steps = cta, 0, 0, []
+        c, c1 = 0, chunks(jg)
+        while True:
+            last = c + 1 >= c1
+            jn = jg + grid if last else jg
+            has_next = jn < njobs
+            steps.append((jg, c, st, slot))
+            taken.append((jg, c))
+            if not has_next:
+                break
+            nslot = slot ^ 1 if last else slot
+            assert (st ^ 1) != st and (not last or nslot != slot)
+            if last:
+                slot, jg, c, c1 = nslot, jn, 0, chunks(jn)
+            else:
+                c += 1
+            st ^= 1
+        for (j1, _, s1, l1), (j2, _, s2, l2) in zip(steps, steps[1:]):
+            assert s1 != s2 and (l1 == l2) == (j1 == j2)
+    assert sorted(taken) == sorted((J, c) for J in range(njobs) for c in range(chunks(J)))
+
+
+def stage_rows(rs, S, p):
+    """skinny_finish of pass p: thread row (sg, i) -> staged (s0, r, stored)."""
     sp = 4 * rs
     out = {}
-    for p in range(npass):
-        for h in range(0, sp, SUB):
-            s0 = p * sp + h
-            if s0 >= S:
-                break
-            ns = min(sp - h, SUB, S - s0)
-            for sg in range(4):
-                for i in range(rs):
-                    r = sg * rs + i - h
-                    if 0 <= r < SUB:
-                        s = s0 + r
-                        assert (p, sg, i) not in out
-                        out[(p, sg, i)] = (s0, r, s < S and r < ns)
+    for h in range(0, sp, SUB):
+        s0 = p * sp + h
+        if s0 >= S:
+            break
+        ns = min(sp - h, SUB, S - s0)
+        for sg in range(4):
+            for i in range(rs):
+                r = sg * rs + i - h
+                if 0 <= r < SUB:
+                    assert (sg, i) not in out
+                    out[(sg, i)] = (s0, r, r < ns, h + r)  # cs index within the pass
     return out
 
 
 @pytest.mark.parametrize("rs,S,npass", [(4, 1, 1), (4, 16, 1), (8, 20, 1), (12, 40, 1), (12, 48, 1),
-                                        (16, 64, 1), (16, 150, 3), (8, 150, 5), (16, 256, 4),
+                                        (8, 49, 2), (8, 64, 2), (8, 150, 5), (8, 256, 8),
                                         (8, 65, 3)])
 def test_epilogue_stages_every_row_once(rs, S, npass):
-    st = stage_rows(rs, S, npass)
-    stored = sorted(s0 + r for (s0, r, ok) in st.values() if ok)
-    assert stored == list(range(S))
-    assert 4 * rs * npass <= 256  # Q rows in shared memory
+    sp = 4 * rs
+    stored = []
+    for p in range(npass):
+        for (s0, r, ok, ci) in stage_rows(rs, S, p).values():
+            if ok:
+                stored.append(s0 + r)
+                assert ci < sp and p * sp + ci == s0 + r  # the slot's row offsets
+    assert sorted(stored) == list(range(S))
+
+
+def plane(L0, L1, w0, wi, wj, r0, ri, rj, warp, out):
+    """skinny_plane: the (w, r) of every lane and step, stepped incrementally."""
+    total, di, dj = L0 * L1, 32 % L0, 32 // L0
+    dw, dr = wi * di + wj * dj, ri * di + rj * dj
+    cwc, crc = wj - wi * L0, rj - ri * L0
+    for lane in range(32):
+        i, j = lane % L0, lane // L0
+        w, r = w0 + wi * i + wj * j, r0 + ri * i + rj * j
+        f, step = lane, 0
+        while f < total:
+            fi, fj = f % L0, f // L0
+            assert (w, r) == (w0 + wi * fi + wj * fj, r0 + ri * fi + rj * fj)
+            out.append((warp, (w, r), step, lane))
+            i += di
+            w += dw
+            r += dr
+            if i >= L0:
+                i -= L0
+                w += cwc
+                r += crc
+            f += 32
+            step += 1
 
 
 def store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns):
-    """skinny_store: [(warp, step, lane, w, r)] of one staged step."""
+    """skinny_store: [(warp plane, (w, r), step, lane)] of one staged step."""
     out = []
-
-    def plane(L0, L1, warp, elem):
-        total, di, dj = L0 * L1, 32 % L0, 32 // L0
-        for lane in range(32):
-            i, j, step = lane % L0, lane // L0, 0
-            f = lane
-            while f < total:
-                assert (i, j) == (f % L0, f // L0)
-                out.append((warp, elem(i, j), step, lane))
-                i += di
-                j += dj
-                if i >= L0:
-                    i -= L0
-                    j += 1
-                f += 32
-                step += 1
-
+    py = p_walk == P_Y
     for warp in range(8):
         if c_walk == C_XS:
             for yl in range(warp, ty, 8):
-                plane(tx, ns, (warp, yl), lambda xl, r, yl=yl: (pos(p_walk, tx, ty, xl, yl), r))
+                plane(tx, ns, yl if py else tx * yl, ty if py else 1, 0, 0, 0, 1, (warp, yl), out)
         elif c_walk == C_XY:
             for r in range(warp, ns, 8):
-                plane(tx, ty, (warp, r), lambda xl, yl, r=r: (pos(p_walk, tx, ty, xl, yl), r))
+                plane(tx, ty, 0, ty if py else 1, 1 if py else tx, r, 0, 0, (warp, r), out)
         else:
             e0 = s_run
             first = (s0 // e0) * e0
@@ -179,8 +252,8 @@ def store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns):
                 ra, rb = max(rs_, s0), min(rs_ + e0, s0 + ns)
                 if rb <= ra:
                     continue
-                plane(rb - ra, tx, (warp, job),
-                      lambda i, xl, yl=yl, ra=ra: (pos(p_walk, tx, ty, xl, yl), ra - s0 + i))
+                plane(rb - ra, tx, yl if py else tx * yl, 0, ty if py else 1, ra - s0, 1, 0,
+                      (warp, job), out)
     return out
 
 
