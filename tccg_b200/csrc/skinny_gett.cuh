@@ -79,6 +79,11 @@ enum SkinnyPWalk : int { SK_P_X = 0, SK_P_Y = 1, SK_P_K = 2 };
 // X is S's); (x, y) planes per s (it is a Y mode's); runs of C's stride-one
 // S mode, then x, per y (C's stride-one index is on the narrow side).
 enum SkinnyCWalk : int { SK_C_XS = 0, SK_C_XY = 1, SK_C_SX = 2 };
+// Contiguous C rows of a box (each y of the box): C(x, y, s) = C(0, y, s0) +
+// x + ex (s - s0) with the box covering all of X (SK_CLIN_XS), or C(x0 + x,
+// y, s) = C(x0, y, 0) + s + S x with all of S in one staged step
+// (SK_CLIN_SX).
+enum SkinnyCLin : int { SK_CLIN_NONE = 0, SK_CLIN_XS = 1, SK_CLIN_SX = 2 };
 
 struct SkinnyArgs {
   const float* P;
@@ -104,6 +109,12 @@ struct SkinnyArgs {
   int32_t p_walk, c_walk;
   int32_t q_kfast;         // Q loads along k (its stride-one index is a K mode)
   int32_t s_run;           // SK_C_SX: extent of C's stride-one S mode
+  // SK_P_X with unit x stride, every k offset and P itself 16-byte aligned:
+  // four positions that are consecutive in P move as one 16-byte copy
+  int32_t p_vec;
+  // C of a box row is one contiguous range (SkinnyCLin): staged in that
+  // order and stored as a straight copy
+  int32_t c_lin;
   float alpha, beta;
   float* partial;          // k-split slices (null: store to C)
 };
@@ -181,6 +192,30 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
           cp_async_elem<4>(d + w, a.P + po + ko);
         else
           d[w] = 0.0f;
+      }
+    }
+  } else if (a.p_vec) {
+    // four consecutive positions per 16-byte copy where they are consecutive
+    // and aligned in P (else four element copies): thread tid takes
+    // positions 4 (tid % 64) .. + 3 at k = tid / 64, tid / 64 + 4, ...
+    const int g = 4 * (tid & 63);
+    const int32_t o0 = pw[g], o1 = pw[g + 1], o2 = pw[g + 2], o3 = pw[g + 3];
+    const bool vec = o0 != SK_NONE && (o0 & 3) == 0 && o1 == o0 + 1 && o2 == o0 + 2 && o3 == o0 + 3;
+    const int32_t ko_lane = lane < kc ? __ldg(a.p_k_off + k0 + lane) : 0;
+    for (int k = tid >> 6; k < kc; k += 4) {  // warp-uniform k
+      const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
+      float* d = ps + k * SK_LDP + g;
+      if (vec) {
+        cp_async_16(d, a.P + o0 + ko);
+      } else {
+        const int32_t o[4] = {o0, o1, o2, o3};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          if (o[e] != SK_NONE)
+            cp_async_elem<4>(d + e, a.P + o[e] + ko);
+          else
+            d[e] = 0.0f;
+        }
       }
     }
   } else {
@@ -329,6 +364,96 @@ __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, cons
   }
 }
 
+// Stores the staged range [0, n) of box row yl (os[f]) at C + base + f; one
+// warp per row when there are at least 8 rows, else the whole CTA per row.
+__device__ __forceinline__ void skinny_copy_rows(const SkinnyArgs& a, const float* os, int plane,
+                                                 const int32_t* cw, int32_t cs0, int n) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool py = a.p_walk == SK_P_Y;
+  const bool per_warp = a.ty >= SK_THREADS / 32;
+  const int y0 = per_warp ? warp : 0, ys = per_warp ? SK_THREADS / 32 : 1;
+  const int f0 = per_warp ? lane : tid, fs = per_warp ? 32 : SK_THREADS;
+  const float alpha = a.alpha, beta = a.beta;
+  for (int yl = y0; yl < a.ty; yl += ys) {
+    const int32_t o = cw[py ? yl : a.tx * yl];  // position (0, yl)
+    if (o == SK_NONE) continue;                 // y past the tensor (uniform per row)
+    float* c = a.C + o + cs0;
+    const float* src = os + yl * plane;
+    for (int f = f0; f < n; f += fs) {
+      const float v = alpha * src[f];
+      c[f] = beta != 0.0f ? fmaf(beta, c[f], v) : v;
+    }
+  }
+}
+
+// Linear C (SkinnyCLin): the pass's rows are staged per box row yl in C's own
+// order -- [s][x] (SK_CLIN_XS, one 32-row step at a time) or [x][s]
+// (SK_CLIN_SX, all of S at once) -- and leave as straight copies.
+template <int RS>
+__device__ __forceinline__ void skinny_finish_lin(const SkinnyArgs& a, const SkJob& j,
+                                                  const SkAcc<RS>& acc, float* os,
+                                                  const int32_t* cw, const int32_t* cs) {
+  constexpr int SP = 4 * RS;
+  const int tid = threadIdx.x, wg = tid & 63, sg = tid >> 6;
+  const bool py = a.p_walk == SK_P_Y;
+  const int tx = a.tx, ty = a.ty;
+  const bool xs = a.c_lin == SK_CLIN_XS;
+  const int plane = xs ? tx * SK_SUB : tx * a.S;
+  // staging index of row 0 of the thread's four positions 4 wg .. 4 wg + 3
+  // (-1: past the box): y plane + x (XS, rows tx apart) or + x S (SX, rows 1 apart)
+  int ob[4];
+  {
+    const int w = 4 * wg, npos = tx * ty;
+    int u = py ? w % ty : w % tx, v = py ? w / ty : w / tx;  // fast / slow index
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int x = py ? v : u, y = py ? u : v;
+      ob[e] = w + e < npos ? y * plane + (xs ? x : x * a.S) : -1;
+      if (++u == (py ? ty : tx)) {
+        u = 0;
+        ++v;
+      }
+    }
+  }
+  if (xs) {
+#pragma unroll 1
+    for (int h = 0; h < SP; h += SK_SUB) {
+      const int s0 = j.p * SP + h;
+      if (s0 >= a.S) break;
+      int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
+      if (ns > a.S - s0) ns = a.S - s0;
+      __syncthreads();  // the stage's last reader is done
+#pragma unroll
+      for (int i = 0; i < RS; ++i) {
+        const int r = sg * RS + i - h;
+        if (r >= 0 && r < SK_SUB) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (ob[e] >= 0) os[ob[e] + r * tx] = acc.v[i][e];
+        }
+      }
+      __syncthreads();
+      skinny_copy_rows(a, os, plane, cw, cs[h], tx * ns);
+    }
+  } else {  // SK_CLIN_SX: all of S (<= 32 rows) in one step
+    const int S = a.S;
+    const int ix = a.bxn == 1 ? 0 : j.b % a.bxn;
+    const int xn = a.ex - ix * tx < tx ? a.ex - ix * tx : tx;  // x of the box inside the tensor
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < RS; ++i) {
+      const int r = sg * RS + i;
+      if (r < S) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (ob[e] >= 0) os[ob[e] + r] = acc.v[i][e];
+      }
+    }
+    __syncthreads();
+    skinny_copy_rows(a, os, plane, cw, cs[0], xn * S);
+  }
+}
+
 // The end of job j: raw sums to its k slice, or its pass's rows to C staged
 // 32 at a time through os (the P stage just consumed).
 template <int RS>
@@ -342,6 +467,10 @@ __device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& 
     for (int i = 0; i < RS; ++i)
       *reinterpret_cast<float4*>(dst + (size_t)(sg * RS + i) * SK_BW) =
           make_float4(acc.v[i][0], acc.v[i][1], acc.v[i][2], acc.v[i][3]);
+    return;
+  }
+  if (a.c_lin != SK_CLIN_NONE) {
+    skinny_finish_lin<RS>(a, j, acc, os, cw, cs);
     return;
   }
 #pragma unroll 1

@@ -113,7 +113,7 @@ struct tccg_plan {
   int32_t tcv = 0;  // TcVariant of a tensor-core plan
   // skinny kernel (skinny_gett.cuh): geometry and tables in sk (operand, C
   // and slice pointers are filled in per run); s_is_n: the narrow side is N
-  bool skinny = false, sk_s_is_n = false;
+  bool skinny = false, sk_s_is_n = false, sk_p_vec = false;
   int32_t sk_ksplit = 1;
   SkinnyArgs sk{};
   // its 32-bit offset tables in one allocation: P and C offsets of the Y
@@ -552,6 +552,24 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   const int64_t njobs = (int64_t)a.nblk * a.npass * a.ksplit;
   if (njobs > INT32_MAX) return false;
   a.njobs = (int32_t)njobs;
+  // 16-byte P copies: x at unit stride, every k offset a multiple of 4 (the
+  // run checks P's alignment); linear C rows of a box (SkinnyCLin)
+  std::vector<int64_t> t;
+  build_offsets(d.nk, d.k_ext, kp, t);
+  bool k4 = true;
+  for (int64_t v : t) k4 &= v % 4 == 0;
+  p->sk_p_vec = a.p_walk == SK_P_X && a.px == 1 && k4;
+  build_offsets(nsm, sext, sc, t);
+  auto affine = [&](int64_t st) {
+    for (size_t i = 0; i < t.size(); ++i)
+      if (t[i] != t[0] + (int64_t)i * st) return false;
+    return true;
+  };
+  a.c_lin = SK_CLIN_NONE;
+  if (a.c_walk == SK_C_XS && a.cx == 1 && a.tx == a.ex && a.bxn == 1 && affine(a.ex))
+    a.c_lin = SK_CLIN_XS;
+  else if (a.c_walk == SK_C_SX && a.npass == 1 && S <= SK_SUB && a.cx == S && affine(1))
+    a.c_lin = SK_CLIN_SX;
   a.alpha = 1.0f;
   a.beta = 0.0f;
   return true;
@@ -942,14 +960,15 @@ static int plan_layout(tccg_plan* p) {
     snprintf(p->describe, sizeof(p->describe),
              "method=GETT prec=%s kernel=skinny_gett<f32> M=%lld N=%lld K=%lld narrow=%s S=%d "
              "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
-             "grid=%lld load=%s%s store=%s%s pack=none",
+             "grid=%lld load=%s%s%s store=%s%s%s pack=none",
              p->prec == TCCG_PREC_BF16X3 ? "bf16x3" : "fp32", (long long)p->M, (long long)p->N,
              (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S, a.npass, 4 * a.rs, a.tx, a.ty,
              (long long)a.ex, (long long)a.ey, (long long)a.nblk, a.nchunks, p->sk_ksplit,
              (long long)a.njobs,
              (long long)std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms),
-             pw[a.p_walk], a.q_kfast ? " q=k" : " q=s", cw[a.c_walk],
-             a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "");
+             pw[a.p_walk], p->sk_p_vec ? " x16B" : "", a.q_kfast ? " q=k" : " q=s", cw[a.c_walk],
+             a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "",
+             a.c_lin ? " linear" : "");
     p->ws_bytes = ws;
     return TCCG_OK;
   }
@@ -1776,6 +1795,7 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
   a.alpha = alpha;
   a.beta = beta;
   a.partial = p->sk_ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
+  a.p_vec = p->sk_p_vec && (reinterpret_cast<uintptr_t>(a.P) & 15) == 0;
   return a;
 }
 
