@@ -42,10 +42,10 @@
 // element offsets stay below 2^31 (8 GiB of FP32 each), which halves the
 // integer work of every load and store address and of the offset tables.
 //
-// With a k-split (few blocks, long K: a matrix-vector shape) the job of
-// slice z writes its raw sums densely to partial[z][block][row][position]
-// and skinny_reduce_kernel adds the slices in split order before the same
-// store walk. Results are deterministic: a fixed k order within a slice,
+// With a k-split (few jobs, long K: a matrix-vector shape) the job of slice
+// z writes its raw sums densely to partial[z][block][pass][row][position]
+// and skinny_reduce_kernel (one CTA per block and pass) adds the slices in
+// split order before the same store walk. Results are deterministic: a fixed k order within a slice,
 // slices in order.
 #pragma once
 #include <cuda.h>
@@ -462,7 +462,7 @@ __device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& 
   constexpr int SP = 4 * RS;
   const int tid = threadIdx.x, wg = tid & 63, sg = tid >> 6;
   if (a.partial) {
-    float* dst = a.partial + ((size_t)j.z * a.nblk + j.b) * SP * SK_BW + 4 * wg;
+    float* dst = a.partial + (((size_t)j.z * a.nblk + j.b) * a.npass + j.p) * SP * SK_BW + 4 * wg;
 #pragma unroll
     for (int i = 0; i < RS; ++i)
       *reinterpret_cast<float4*>(dst + (size_t)(sg * RS + i) * SK_BW) =
@@ -572,34 +572,37 @@ __device__ __forceinline__ void skinny_loop(int j0, int jstep, int njobs, Resolv
   }
 }
 
-// C of block b = alpha * (slice 0 + slice 1 + ...) + beta * C, slices in order.
+// C of pass p of block b = alpha * (slice 0 + slice 1 + ...) + beta * C,
+// slices in order; r = b npass + p.
 template <int RS>
-__device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int b, uint8_t* smem) {
+__device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int r, uint8_t* smem) {
   constexpr int SP = 4 * RS;
   float* os = reinterpret_cast<float*>(smem);
   int32_t* pw = reinterpret_cast<int32_t*>(smem + SK_OFF_TAB);
   int32_t* cw = pw + 2 * SK_BW;
   int32_t* cs = cw + 2 * SK_BW;
   const int tid = threadIdx.x;
+  const int b = r / a.npass, p = r % a.npass;
   SkinnyArgs ac = a;
   ac.partial = nullptr;  // stage the rows' C offsets
-  skinny_begin(ac, b, 0, SP, pw, cw, cs);
-  const size_t slice = (size_t)a.nblk * SP * SK_BW;
-  const float* src = a.partial + (size_t)b * SP * SK_BW + tid;
+  skinny_begin(ac, b, p, SP, pw, cw, cs);
+  const size_t slice = (size_t)a.nblk * a.npass * SP * SK_BW;
+  const float* src = a.partial + (size_t)r * SP * SK_BW + tid;
 #pragma unroll 1
   for (int h = 0; h < SP; h += SK_SUB) {
-    if (h >= a.S) break;
+    const int s0 = p * SP + h;
+    if (s0 >= a.S) break;
     int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
-    if (ns > a.S - h) ns = a.S - h;
+    if (ns > a.S - s0) ns = a.S - s0;
     __syncthreads();
-    for (int r = 0; r < ns; ++r) {
-      const float* p = src + (size_t)(h + r) * SK_BW;
-      float v = p[0];
-      for (int z = 1; z < a.ksplit; ++z) v = __fadd_rn(v, p[z * slice]);
-      os[r * SK_LDP + tid] = v;
+    for (int rr = 0; rr < ns; ++rr) {
+      const float* q = src + (size_t)(h + rr) * SK_BW;
+      float v = q[0];
+      for (int z = 1; z < a.ksplit; ++z) v = __fadd_rn(v, q[z * slice]);
+      os[rr * SK_LDP + tid] = v;
     }
     __syncthreads();
-    skinny_store(a, os, cw, cs + h, h, ns);
+    skinny_store(a, os, cw, cs + h, s0, ns);
   }
 }
 
@@ -623,7 +626,7 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
   skinny_loop<RS>(blockIdx.x, gridDim.x, a.njobs, resolve, smem);
 }
 
-// grid (blocks)
+// grid (blocks x passes)
 __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
     skinny_reduce_kernel(const __grid_constant__ SkinnyArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -634,7 +637,7 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
 // Grouped launches. Contraction items: item i owns the global job indices
 // [begin[i], begin[i + 1]); one persistent launch per rows-per-thread class
 // (RS = the items' rs) walks all of them. Reduction items:
-// CTAs [begin[i], begin[i + 1]) are the blocks of a k-split item.
+// CTAs [begin[i], begin[i + 1]) are the (block, pass) pairs of a k-split item.
 struct SkinnyItem {
   SkinnyArgs args;
   int64_t begin;

@@ -539,15 +539,11 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   int lg = 0;
   while ((1 << lg) < std::min<int64_t>(p->K, SK_KC)) ++lg;
   a.kr_log2 = lg;
-  // k-split (one pass only): blocks that cannot fill the persistent CTAs,
+  // k-split: (block, pass) jobs that cannot fill the persistent CTAs,
   // slices of >= 4 chunks
-  if (a.npass == 1) {
-    a.chunks_per_split = (int32_t)choose_ksplit(
-        p->tune.ksplit, a.nblk, a.nchunks, (int64_t)SK_CTAS_PER_SM * p->num_sms, 4, &p->sk_ksplit);
-  } else {
-    a.chunks_per_split = a.nchunks;
-    p->sk_ksplit = 1;
-  }
+  a.chunks_per_split = (int32_t)choose_ksplit(p->tune.ksplit, (int64_t)a.nblk * a.npass, a.nchunks,
+                                              (int64_t)SK_CTAS_PER_SM * p->num_sms, 4,
+                                              &p->sk_ksplit);
   a.ksplit = p->sk_ksplit;
   const int64_t njobs = (int64_t)a.nblk * a.npass * a.ksplit;
   if (njobs > INT32_MAX) return false;
@@ -575,22 +571,24 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   return true;
 }
 
-// Skinny kernel model (seconds): FP32 FMAs at 45 TFLOP/s over the blocks'
-// positions and padded rows; P and C at 5.5 TB/s, a run of fewer than 8
-// elements (32 bytes) in the load or store walk counted as a whole sector;
-// the k-split slices written and read back.
+// Skinny kernel model (seconds), fitted on B200 timings of eleven items of
+// the 256-item batched workload (0.08-1.4 ms; within 25 % of each): FP32
+// FMAs over the blocks' positions and padded rows at 18 TFLOP/s, C written at
+// 2.0 TB/s and P read at 6 TB/s (its copies overlap the FMAs and stores), as
+// a sum -- a job's phases follow one another in its CTA -- plus 4 us; a
+// k-split adds its slices' traffic and the reduction's launch.
 static double skinny_time(const tccg_plan* p) {
   const SkinnyArgs& a = p->sk;
   const double W = (double)a.ex * (double)a.ey, K = (double)p->K, S = (double)a.S;
   const double rows = 4.0 * a.rs * a.npass;
-  const double fma = 2.0 * (double)a.nblk * SK_BW * rows * K / 45e12;
-  const double run_p = a.p_walk == SK_P_K ? std::min<double>(K, SK_KC)
-                       : a.p_walk == SK_P_Y ? a.ty : a.tx;
-  const double run_c = a.c_walk == SK_C_SX ? a.s_run : a.tx;
-  auto waste = [](double run) { return run >= 8.0 ? 1.0 : 8.0 / std::max(run, 1.0); };
-  double bytes = 4.0 * W * K * waste(run_p) + 4.0 * W * S * waste(run_c);
-  if (p->sk_ksplit > 1) bytes += 8.0 * p->sk_ksplit * (double)a.nblk * 4.0 * a.rs * SK_BW;
-  return std::max(fma, bytes / 5.5e12) + (p->sk_ksplit > 1 ? 8e-6 : 4e-6);
+  const double fma = 2.0 * (double)a.nblk * SK_BW * rows * K;
+  double t = fma / 18e12 + 4.0 * W * S / 2.0e12 + 4.0 * W * K / 6e12;
+  // the rates need every persistent CTA busy
+  const double slots = (double)SK_CTAS_PER_SM * p->num_sms;
+  if ((double)a.njobs < slots) t *= slots / (double)a.njobs;
+  t += 4e-6;
+  if (p->sk_ksplit > 1) t += 8.0 * p->sk_ksplit * (double)a.nblk * rows * SK_BW / 3e12 + 5e-6;
+  return t;
 }
 
 // The persistent skinny kernel of a rows-per-thread class (4, 8 or 12).
@@ -604,7 +602,14 @@ static void with_skinny_rs(int rs, F&& f) {
 }
 
 // Whether the plan runs the skinny kernel: asked for, or -- unless the
-// tuning asks for another kernel family -- when its model beats the others'.
+// tuning asks for another kernel family -- where it was measured to win or
+// its model beats the others'. Measured on the 233 items of the 256-item
+// batched workload it can take (standalone runs, L2 flushed): with K <= 32,
+// a narrow side of at most 48 and at least 65536 positions on the wide side
+// it was the fastest kernel on 10 of 13 items (0.38-0.9x the time of the best
+// other one; 1.1-1.4x on the three others). There the tile kernels' models
+// undercount the packing pass, which must transpose the wide operand
+// (0.9 TB/s measured where they assume 4.5).
 static bool choose_skinny(const tccg_plan* p) {
   if (p->tune.skinny > 0) return true;
   if (p->tune.skinny < 0) return false;
@@ -612,6 +617,8 @@ static bool choose_skinny(const tccg_plan* p) {
   if (t.variant != 0 || t.load != 0 || t.direct != 0 || t.shortk != 0 || t.simt_tile != 0 ||
       t.tile_n != 0)
     return false;
+  const SkinnyArgs& a = p->sk;
+  if (p->K <= SK_KC && a.S <= 48 && (int64_t)a.ex * a.ey >= 65536) return true;
   double other = simt_time(p);
   if (p->prec == TCCG_PREC_BF16X3) other = std::min(other, tc_time(p, false));
   return skinny_time(p) < other;
@@ -951,9 +958,9 @@ static int plan_layout(tccg_plan* p) {
   const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
   if (p->skinny) {
     const SkinnyArgs& a = p->sk;
-    if (p->sk_ksplit > 1) {  // FP32 slices [split][block][row][position]
+    if (p->sk_ksplit > 1) {  // FP32 slices [split][block][pass][row][position]
       p->off_part = 0;
-      ws = align_up((size_t)p->sk_ksplit * (size_t)a.nblk * 4 * a.rs * SK_BW * 4, 256);
+      ws = align_up((size_t)p->sk_ksplit * (size_t)a.nblk * a.npass * 4 * a.rs * SK_BW * 4, 256);
     }
     static const char* pw[] = {"x", "y", "k"};
     static const char* cw[] = {"xs", "xy", "sx"};
@@ -1812,8 +1819,8 @@ static int run_skinny(const tccg_plan* p, const void* GA, const void* GB, float*
   mark(1, 1, s);
   if (rc || p->sk_ksplit == 1) return rc;
   mark(2, 0, s);
-  launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)a.nblk), dim3(SK_THREADS),
-               SK_SMEM_BYTES, s, a);
+  launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)(a.nblk * a.npass)),
+               dim3(SK_THREADS), SK_SMEM_BYTES, s, a);
   rc = launch_check("skinny_reduce");
   mark(2, 1, s);
   return rc;
@@ -2478,7 +2485,7 @@ static void bind_skinny(tccg_group* g, tccg_group::Wave& wv, const void* const* 
       if (p->sk_ksplit > 1) {
         SkinnyItem r = it;
         r.begin = rctas;
-        rctas += p->sk.nblk;
+        rctas += (int64_t)p->sk.nblk * p->sk.npass;
         red.push_back(r);
       }
     }

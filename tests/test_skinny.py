@@ -39,6 +39,10 @@ CASES = {
     # C's next stride after X is a W mode: (x, y) planes; K over three chunks
     "xy": ("mpn", "pmk", "kn", dict(m=33, p=9, n=5, k=70), 1.0, 1.0,
            ["narrow=N", "load=y", "store=xy"]),
+    # two passes of 32 rows over one block, K split over slices (the
+    # reduction runs per block and pass)
+    "passes_split": ("ab", "akl", "lkb", dict(a=56, b=93, k=60, l=50), 1.0, 0.5,
+                     ["narrow=M", "rows=2x32"]),
     "matvec": ("a", "ak", "k", dict(a=300, k=77), 1.0, 0.0, ["S=1 "]),
     "outer": ("ab", "a", "b", dict(a=33, b=65), 1.5, 0.0, ["kchunks=1 "]),
 }
@@ -121,8 +125,10 @@ def test_skinny_grouped_equals_per_item(cuda):
 
 def test_skinny_choice_and_refusal(cuda):
     from tccg_b200._native import TccgError
-    # an item-69-like shape (N = 40, K = 20, P transposed against C): the model takes it
-    con = make_contraction("vqud", "qe", "duve", dict(v=19, q=40, u=600, d=31, e=20))
+    # item 69 of the 256-item batched workload (N = 40, K = 20, 5.0e6 positions, P
+    # transposed against C): the library takes the skinny kernel
+    from tccg_b200.workloads import batched_workload
+    con = batched_workload(256, seed=0)[69]
     for precision in ("fp32", "bf16x3"):
         assert "skinny_gett" in Plan(con, precision).describe()
         assert "skinny_gett" not in Plan(con, precision, tuning=Tuning(skinny=-1)).describe()

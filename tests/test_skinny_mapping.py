@@ -294,13 +294,16 @@ def test_store_instructions_are_contiguous():
 
 
 def test_partial_slices_round_trip():
-    """k-split: split z of block b writes row s, position w at
-    ((z nblk + b) SP + s) BW + w; the reduction reads slice z of its block at
-    b SP BW + z nblk SP BW + s BW + w -- the same element, for every (z, b, s, w)."""
-    for nblk, sp, splits in itertools.product((1, 3, 7), (16, 48), (2, 5)):
-        slice_ = nblk * sp * BW
-        for z, b, s in itertools.product(range(splits), range(nblk), range(sp)):
-            w = (z * 7 + s) % BW
-            wr = ((z * nblk + b) * sp + s) * BW + w
-            rd = b * sp * BW + w + s * BW + z * slice_
+    """k-split: the job of slice z, block b, pass p writes row r, position w
+    at (((z nblk + b) npass + p) SP + r) BW + w; the reduction CTA of (b, p)
+    (index b npass + p) reads slice z at (b npass + p) SP BW + r BW + w +
+    z slice -- the same element, for every (z, b, p, r, w)."""
+    for nblk, npass, sp, splits in itertools.product((1, 3, 7), (1, 2, 5), (16, 32), (2, 5)):
+        slice_ = nblk * npass * sp * BW
+        for z, b, p, r in itertools.product(range(splits), range(nblk), range(npass), range(sp)):
+            w = (z * 7 + r) % BW
+            wr = (((z * nblk + b) * npass + p) * sp + r) * BW + w
+            cta = b * npass + p
+            assert (cta // npass, cta % npass) == (b, p)
+            rd = cta * sp * BW + w + r * BW + z * slice_
             assert wr == rd
