@@ -14,7 +14,7 @@
 // W blocking. The W modes split into X -- the W mode C stores contiguously
 // (its smallest C stride) -- and the Y space: all other W modes, linearised
 // in order of increasing P stride. A block is a box of tx x ty positions
-// (x, y), tx * ty <= 256:
+// (x, y), tx * ty <= SK_BW (256):
 //   P(x, y, k) = P[x px + p_y_off[y] + p_k_off[k]]
 //   Q(s, k)    = Q[q_s_off[s] + q_k_off[k]]
 //   C(x, y, s) = C[x cx + c_y_off[y] + c_s_off[s]]
@@ -26,7 +26,7 @@
 // Jobs. A job is one block x one pass over S (4 RS rows: RS = 4, 8 or 12
 // rows per thread) x one k slice; an S above 48 runs passes of 32 rows,
 // neighbouring jobs whose P chunks the later passes read from L2. The CTAs are persistent
-// (two per SM) and walk their jobs' k chunks (32 k each) as one sequence,
+// (two 256-thread CTAs per SM) and walk their jobs' k chunks (32 k each) as one sequence,
 // double buffered through element-wise cp.async: the copies of the next
 // chunk -- of the same job, or the first of the next job, whose box offsets
 // are computed then -- are in flight while the CTA multiplies the current
@@ -53,8 +53,17 @@
 
 namespace tccg {
 
-constexpr int SK_THREADS = 256;
-constexpr int SK_BW = 256;             // box positions per block (one per thread)
+// 256 threads (two CTAs per SM); 128-thread CTAs (four per SM, boxes of
+// 128 positions) measured 24 % slower on the largest transposing item and
+// faster only on multi-pass ones
+#ifndef TCCG_SK_THREADS
+#define TCCG_SK_THREADS 256
+#endif
+constexpr int SK_THREADS = TCCG_SK_THREADS;
+constexpr int SK_BW = SK_THREADS;      // box positions per block (one per thread)
+constexpr int SK_WG = SK_BW / 4;       // position groups of 4: a thread owns one ...
+constexpr int SK_SG = SK_THREADS / SK_WG;  // ... in one of 4 row groups
+static_assert(SK_SG == 4 && SK_WG % 32 == 0, "a warp's threads share one row group");
 constexpr int SK_KC = 32;              // k per chunk
 constexpr int SK_LDP = SK_BW + 4;      // P stage row stride (floats): [k][position]
 constexpr int SK_SMAX = 256;           // largest narrow extent
@@ -67,9 +76,9 @@ constexpr size_t SK_P_STAGE = (size_t)SK_KC * SK_LDP * 4;
 constexpr size_t SK_Q_STAGE = (size_t)SK_KC * SK_QLD * 4;
 constexpr size_t SK_OFF_TAB = 2 * (SK_P_STAGE + SK_Q_STAGE);
 constexpr size_t SK_SMEM_BYTES = SK_OFF_TAB + (size_t)(4 * SK_BW + 2 * SK_SPMAX) * 4;
-constexpr int SK_CTAS_PER_SM = 2;
+constexpr int SK_CTAS_PER_SM = SK_THREADS == 128 ? 4 : 2;
 static_assert(SK_SUB == SK_KC, "the epilogue staging reuses one P stage");
-static_assert(SK_CTAS_PER_SM * (SK_SMEM_BYTES + 1024) <= 228 * 1024, "two CTAs per SM");
+static_assert(SK_CTAS_PER_SM * (SK_SMEM_BYTES + 1024) <= 228 * 1024, "CTAs per SM");
 
 // P load order: lanes along x (X is P's stride-one W mode), along y (the
 // first Y mode is), or along k (a K mode is). Box positions are numbered
@@ -197,12 +206,12 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
   } else if (a.p_vec) {
     // four consecutive positions per 16-byte copy where they are consecutive
     // and aligned in P (else four element copies): thread tid takes
-    // positions 4 (tid % 64) .. + 3 at k = tid / 64, tid / 64 + 4, ...
-    const int g = 4 * (tid & 63);
+    // positions 4 (tid % WG) .. + 3 at k = tid / WG, tid / WG + 4, ...
+    const int g = 4 * (tid % SK_WG);
     const int32_t o0 = pw[g], o1 = pw[g + 1], o2 = pw[g + 2], o3 = pw[g + 3];
     const bool vec = o0 != SK_NONE && (o0 & 3) == 0 && o1 == o0 + 1 && o2 == o0 + 2 && o3 == o0 + 3;
     const int32_t ko_lane = lane < kc ? __ldg(a.p_k_off + k0 + lane) : 0;
-    for (int k = tid >> 6; k < kc; k += 4) {  // warp-uniform k
+    for (int k = tid / SK_WG; k < kc; k += SK_SG) {  // warp-uniform k
       const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
       float* d = ps + k * SK_LDP + g;
       if (vec) {
@@ -343,8 +352,8 @@ struct SkAcc {
 template <int RS>
 __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, const float* qs, int kc) {
   const int tid = threadIdx.x;
-  const float* pp = ps + 4 * (tid & 63);
-  const float* qq = qs + (tid >> 6) * RS;
+  const float* pp = ps + 4 * (tid % SK_WG);
+  const float* qq = qs + (tid / SK_WG) * RS;
 #pragma unroll 2
   for (int k = 0; k < kc; ++k) {
     const float4 pv = *reinterpret_cast<const float4*>(pp + k * SK_LDP);
@@ -394,7 +403,7 @@ __device__ __forceinline__ void skinny_finish_lin(const SkinnyArgs& a, const SkJ
                                                   const SkAcc<RS>& acc, float* os,
                                                   const int32_t* cw, const int32_t* cs) {
   constexpr int SP = 4 * RS;
-  const int tid = threadIdx.x, wg = tid & 63, sg = tid >> 6;
+  const int tid = threadIdx.x, wg = tid % SK_WG, sg = tid / SK_WG;
   const bool py = a.p_walk == SK_P_Y;
   const int tx = a.tx, ty = a.ty;
   const bool xs = a.c_lin == SK_CLIN_XS;
@@ -460,7 +469,7 @@ template <int RS>
 __device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& j, const SkAcc<RS>& acc,
                                               float* os, const int32_t* cw, const int32_t* cs) {
   constexpr int SP = 4 * RS;
-  const int tid = threadIdx.x, wg = tid & 63, sg = tid >> 6;
+  const int tid = threadIdx.x, wg = tid % SK_WG, sg = tid / SK_WG;
   if (a.partial) {
     float* dst = a.partial + (((size_t)j.z * a.nblk + j.b) * a.npass + j.p) * SP * SK_BW + 4 * wg;
 #pragma unroll
@@ -615,7 +624,7 @@ __device__ __forceinline__ void skinny_dispatch(int rs, F&& f) {
   }
 }
 
-// persistent grid (at most two CTAs per SM) over the plan's jobs; one
+// persistent grid (SK_CTAS_PER_SM CTAs per SM) over the plan's jobs; one
 // instantiation per rows-per-thread class (RS = a.rs)
 template <int RS>
 __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)

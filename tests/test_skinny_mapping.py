@@ -10,7 +10,8 @@ import itertools
 
 import pytest
 
-BW, KC, LDP, SUB, THREADS = 256, 32, 260, 32, 256
+BW, KC, LDP, SUB, THREADS = 256, 32, 260, 32, 256  # positions per block = threads
+WG, SG = BW // 4, 4  # a thread owns 4 positions of one of 4 row groups
 P_X, P_Y, P_K = 0, 1, 2
 C_XS, C_XY, C_SX = 0, 1, 2
 
@@ -65,6 +66,28 @@ def p_loads(p_walk, kr_log2, kc, valid):
             for k in range(kc):
                 out.append((k, tid))
     return out
+
+
+def p_vec_loads(kc):
+    """skinny_issue, 16-byte copies: thread tid takes positions 4 (tid % WG)
+    .. + 3 at k = tid / WG, tid / WG + SG, ..."""
+    out = []
+    for tid in range(THREADS):
+        g = 4 * (tid % WG)
+        k = tid // WG
+        while k < kc:
+            out += [(k, g + e) for e in range(4)]
+            k += SG
+    return out
+
+
+@pytest.mark.parametrize("kc", [1, 3, 4, 17, 32])
+def test_p_vector_loads_each_element_once(kc):
+    got = p_vec_loads(kc)
+    assert sorted(got) == [(k, w) for k in range(kc) for w in range(BW)]
+    # a warp's threads share k (the shuffled k offset comes from one lane)
+    for w0 in range(0, THREADS, 32):
+        assert len({tid // WG for tid in range(w0, w0 + 32)}) == 1
 
 
 @pytest.mark.parametrize("p_walk", [P_X, P_Y, P_K])
@@ -235,18 +258,19 @@ def store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns):
     """skinny_store: [(warp plane, (w, r), step, lane)] of one staged step."""
     out = []
     py = p_walk == P_Y
-    for warp in range(8):
+    NW = THREADS // 32
+    for warp in range(NW):
         if c_walk == C_XS:
-            for yl in range(warp, ty, 8):
+            for yl in range(warp, ty, NW):
                 plane(tx, ns, yl if py else tx * yl, ty if py else 1, 0, 0, 0, 1, (warp, yl), out)
         elif c_walk == C_XY:
-            for r in range(warp, ns, 8):
+            for r in range(warp, ns, NW):
                 plane(tx, ty, 0, ty if py else 1, 1 if py else tx, r, 0, 0, (warp, r), out)
         else:
             e0 = s_run
             first = (s0 // e0) * e0
             nruns = (s0 + ns - first + e0 - 1) // e0
-            for job in range(warp, nruns * ty, 8):
+            for job in range(warp, nruns * ty, NW):
                 run, yl = job % nruns, job // nruns
                 rs_ = first + run * e0
                 ra, rb = max(rs_, s0), min(rs_ + e0, s0 + ns)
