@@ -354,7 +354,7 @@ __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, cons
   const int tid = threadIdx.x;
   const float* pp = ps + 4 * (tid % SK_WG);
   const float* qq = qs + (tid / SK_WG) * RS;
-#pragma unroll 2
+#pragma unroll 4
   for (int k = 0; k < kc; ++k) {
     const float4 pv = *reinterpret_cast<const float4*>(pp + k * SK_LDP);
     float q[RS];
@@ -553,7 +553,9 @@ __device__ __forceinline__ void skinny_loop(int j0, int jstep, int njobs, Resolv
         nc1 = njob.c1;
         skinny_begin(*nref.a, njob.b, njob.p, SP, pw + ns * SK_BW, cw + ns * SK_BW,
                      cs + ns * SK_SPMAX);
-        __syncthreads();
+        // the copies below read other threads' box offsets only along k or
+        // in 16-byte groups; otherwise each thread reads its own
+        if (nref.a->p_walk == SK_P_K || nref.a->p_vec) __syncthreads();
       }
       skinny_issue(*nref.a, njob, nc, SP, Ps + (st ^ 1) * (SK_P_STAGE / 4),
                    Qs + (st ^ 1) * (SK_Q_STAGE / 4), pw + ns * SK_BW);
