@@ -607,9 +607,11 @@ static void with_skinny_rs(int rs, F&& f) {
 // batched workload it can take (standalone runs, L2 flushed): with K <= 32,
 // a narrow side of at most 48 and at least 65536 positions on the wide side
 // it was the fastest kernel on 10 of 13 items (0.38-0.9x the time of the best
-// other one; 1.1-1.4x on the three others). There the tile kernels' models
-// undercount the packing pass, which must transpose the wide operand
-// (0.9 TB/s measured where they assume 4.5).
+// other one; 1.1-1.4x on the three others), and with K <= 32 and over 2^20
+// positions on all three such items (any narrow side up to 256). There the
+// tile kernels' models undercount the packing pass, which must transpose the
+// wide operand (0.9 TB/s measured where they assume 4.5), and the tcgen05
+// epilogue's short C runs (0.4-0.5 TB/s measured where it assumes 3).
 static bool choose_skinny(const tccg_plan* p) {
   if (p->tune.skinny > 0) return true;
   if (p->tune.skinny < 0) return false;
@@ -618,7 +620,8 @@ static bool choose_skinny(const tccg_plan* p) {
       t.tile_n != 0)
     return false;
   const SkinnyArgs& a = p->sk;
-  if (p->K <= SK_KC && a.S <= 48 && (int64_t)a.ex * a.ey >= 65536) return true;
+  const int64_t W = (int64_t)a.ex * a.ey;
+  if (p->K <= SK_KC && ((a.S <= 48 && W >= 65536) || W >= (int64_t(1) << 20))) return true;
   double other = simt_time(p);
   if (p->prec == TCCG_PREC_BF16X3) other = std::min(other, tc_time(p, false));
   return skinny_time(p) < other;
