@@ -124,6 +124,10 @@ struct SkinnyArgs {
   // C of a box row is one contiguous range (SkinnyCLin): staged in that
   // order and stored as a straight copy
   int32_t c_lin;
+  // SK_CLIN_XS with beta = 0 and C 16-byte aligned: each box row's
+  // 16-byte-aligned range leaves as one bulk copy (cp.async.bulk) instead of
+  // per-element stores; alpha is applied when staging
+  int32_t c_bulk;
   float alpha, beta;
   float* partial;          // k-split slices (null: store to C)
 };
@@ -375,6 +379,11 @@ __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, cons
 
 // Stores the staged range [0, n) of box row yl (os[f]) at C + base + f; one
 // warp per row when there are at least 8 rows, else the whole CTA per row.
+// With c_bulk (staged values already scaled by alpha, beta = 0) a row whose
+// C start is 16-byte aligned leaves as one bulk copy of its first 4 [n / 4]
+// elements (issued by the row's first thread; every address and size a
+// multiple of 16 bytes: C, the staging rows and n / 4 quads), the rest by the
+// threads.
 __device__ __forceinline__ void skinny_copy_rows(const SkinnyArgs& a, const float* os, int plane,
                                                  const int32_t* cw, int32_t cs0, int n) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -383,16 +392,28 @@ __device__ __forceinline__ void skinny_copy_rows(const SkinnyArgs& a, const floa
   const int y0 = per_warp ? warp : 0, ys = per_warp ? SK_THREADS / 32 : 1;
   const int f0 = per_warp ? lane : tid, fs = per_warp ? 32 : SK_THREADS;
   const float alpha = a.alpha, beta = a.beta;
+  bool issued = false;
   for (int yl = y0; yl < a.ty; yl += ys) {
     const int32_t o = cw[py ? yl : a.tx * yl];  // position (0, yl)
     if (o == SK_NONE) continue;                 // y past the tensor (uniform per row)
     float* c = a.C + o + cs0;
     const float* src = os + yl * plane;
-    for (int f = f0; f < n; f += fs) {
-      const float v = alpha * src[f];
-      c[f] = beta != 0.0f ? fmaf(beta, c[f], v) : v;
+    if (a.c_bulk) {
+      const int body = ((o + cs0) & 3) == 0 ? (n & ~3) : 0;
+      if (body > 0 && f0 == 0) {
+        bulk_store_1d(c, src, (uint32_t)body * 4);
+        bulk_commit();
+        issued = true;
+      }
+      for (int f = body + f0; f < n; f += fs) c[f] = src[f];
+    } else {
+      for (int f = f0; f < n; f += fs) {
+        const float v = alpha * src[f];
+        c[f] = beta != 0.0f ? fmaf(beta, c[f], v) : v;
+      }
     }
   }
+  if (issued) bulk_wait_read_all();  // the staging is reused by the next copies
 }
 
 // Linear C (SkinnyCLin): the pass's rows are staged per box row yl in C's own
@@ -432,15 +453,17 @@ __device__ __forceinline__ void skinny_finish_lin(const SkinnyArgs& a, const SkJ
       int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
       if (ns > a.S - s0) ns = a.S - s0;
       __syncthreads();  // the stage's last reader is done
+      const float sc = a.c_bulk ? a.alpha : 1.0f;
 #pragma unroll
       for (int i = 0; i < RS; ++i) {
         const int r = sg * RS + i - h;
         if (r >= 0 && r < SK_SUB) {
 #pragma unroll
           for (int e = 0; e < 4; ++e)
-            if (ob[e] >= 0) os[ob[e] + r * tx] = acc.v[i][e];
+            if (ob[e] >= 0) os[ob[e] + r * tx] = sc * acc.v[i][e];
         }
       }
+      if (a.c_bulk) fence_proxy_async_smem();  // the bulk copies read the staging
       __syncthreads();
       skinny_copy_rows(a, os, plane, cw, cs[h], tx * ns);
     }
@@ -635,6 +658,7 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
   grid_dep_wait();
   auto resolve = [&](int J) { return SkRef{&a, J}; };
   skinny_loop<RS>(blockIdx.x, gridDim.x, a.njobs, resolve, smem);
+  bulk_wait_all();  // bulk C copies complete before the CTA exits
 }
 
 // grid (blocks x passes)
@@ -663,6 +687,7 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
     return SkRef{&it.args, (int)(J - it.begin)};
   };
   skinny_loop<RS>(blockIdx.x, gridDim.x, njobs, resolve, smem);
+  bulk_wait_all();  // bulk C copies complete before the CTA exits
 }
 
 __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)

@@ -622,6 +622,10 @@ static bool choose_skinny(const tccg_plan* p) {
   const SkinnyArgs& a = p->sk;
   const int64_t W = (int64_t)a.ex * a.ey;
   if (p->K <= SK_KC && ((a.S <= 48 && W >= 65536) || W >= (int64_t(1) << 20))) return true;
+  // FP32 precision (the CUDA-core tiles its only other choice): a narrow side
+  // of at most 48 and at least 4096 positions, any K -- on the 59 such items
+  // 2.6 ms less in sum than the CUDA-core tiles (21 % of their time)
+  if (p->prec == TCCG_PREC_FP32 && a.S <= 48 && W >= 4096) return true;
   double other = simt_time(p);
   if (p->prec == TCCG_PREC_BF16X3) other = std::min(other, tc_time(p, false));
   return skinny_time(p) < other;
@@ -1806,6 +1810,7 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
   a.beta = beta;
   a.partial = p->sk_ksplit > 1 ? reinterpret_cast<float*>(w + p->off_part) : nullptr;
   a.p_vec = p->sk_p_vec && (reinterpret_cast<uintptr_t>(a.P) & 15) == 0;
+  a.c_bulk = a.c_lin == SK_CLIN_XS && beta == 0.0f && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
   return a;
 }
 

@@ -25,8 +25,8 @@ pytestmark = pytest.mark.gpu
 # (C, A, B, extents, alpha, beta, describe tags)
 CASES = {
     # P (= B after the swap) has d at stride one, C has v: boxes of 19 x 13
-    "transpose": ("vqud", "qe", "duve", dict(v=19, q=40, u=6, d=31, e=20), 1.0, 0.0,
-                  ["narrow=N", "load=y", "store=xs"]),
+    "transpose": ("vqud", "qe", "duve", dict(v=19, q=40, u=6, d=31, e=20), 0.75, 0.0,
+                  ["narrow=N", "load=y", "store=xs linear"]),
     # C's stride-one index on the narrow side (runs of c), long K split over slices
     "matvec_split": ("cdn", "dnxy", "yxc", dict(c=8, d=23, n=20, x=60, y=41), 0.5, -1.5,
                      ["narrow=M", "store=sx run=8"]),
@@ -88,6 +88,31 @@ def test_skinny_k_split_is_deterministic(cuda, ksplit):
         assert "ksplit=1 " not in p.describe(), p.describe()
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
     assert error_metrics(o1, ref)["normwise"] <= 1e-6
+
+
+def test_skinny_bulk_and_element_stores_agree(cuda):
+    """Linear C rows with beta = 0 leave by bulk copies (alpha applied when
+    staging) when C is 16-byte aligned, else by element stores: a C one
+    element off a 16-byte boundary gives the same bits."""
+    import torch
+    lc, la, lb, sizes, alpha, beta, _ = CASES["transpose"]
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, _ = _data(ln, 29)
+    p = Plan(con, "fp32", tuning=Tuning(skinny=1))
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    outs = []
+    for off in (0, 1):
+        buf = torch.full((ln.size_c + 4,), float("nan"), device="cuda")
+        dC = buf[off:off + ln.size_c]
+        p.run(dA, dB, dC, alpha, beta)
+        torch.cuda.synchronize()
+        assert p.status() == 0
+        assert torch.isnan(buf[:off]).all() and torch.isnan(buf[off + ln.size_c:]).all()
+        outs.append(dC.clone())
+    assert torch.equal(outs[0], outs[1])
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), np.zeros(ln.size_c), alpha, 0.0)
+    assert error_metrics(outs[0].double().cpu().numpy(), ref)["normwise"] <= 1e-6
 
 
 def test_skinny_grouped_equals_per_item(cuda):
