@@ -313,24 +313,25 @@ __device__ __forceinline__ void skinny_plane(const SkinnyArgs& a, const float* o
 }
 
 // Stores staged rows [0, ns) (C rows s0 .. s0 + ns - 1; cs[r] = C offset of
-// row s0 + r) in the walk's address order; 8 warps share the planes.
+// row s0 + r) in the walk's address order; the NT / 32 warps share the planes.
+template <int NT = SK_THREADS>
 __device__ __forceinline__ void skinny_store(const SkinnyArgs& a, const float* os,
                                              const int32_t* cw, const int32_t* cs, int s0, int ns) {
   const int warp = threadIdx.x >> 5;
   const bool py = a.p_walk == SK_P_Y;
   const int tx = a.tx, ty = a.ty;
   if (a.c_walk == SK_C_XS) {
-    for (int yl = warp; yl < ty; yl += SK_THREADS / 32)
+    for (int yl = warp; yl < ty; yl += NT / 32)
       skinny_plane(a, os, cw, cs, tx, ns, py ? yl : tx * yl, py ? ty : 1, 0, 0, 0, 1);
   } else if (a.c_walk == SK_C_XY) {
-    for (int r = warp; r < ns; r += SK_THREADS / 32)
+    for (int r = warp; r < ns; r += NT / 32)
       skinny_plane(a, os, cw, cs, tx, ty, 0, py ? ty : 1, py ? 1 : tx, r, 0, 0);
   } else {
     // runs of e0 consecutive rows (C stride one), clipped to [s0, s0 + ns)
     const int e0 = a.s_run;
     const int first = (s0 / e0) * e0;
     const int nruns = (s0 + ns - first + e0 - 1) / e0;
-    for (int job = warp; job < nruns * ty; job += SK_THREADS / 32) {
+    for (int job = warp; job < nruns * ty; job += NT / 32) {
       const int run = job % nruns, yl = job / nruns;
       const int rs = first + run * e0;
       const int ra = rs > s0 ? rs : s0;
@@ -384,13 +385,14 @@ __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, cons
 // elements (issued by the row's first thread; every address and size a
 // multiple of 16 bytes: C, the staging rows and n / 4 quads), the rest by the
 // threads.
+template <int NT = SK_THREADS>
 __device__ __forceinline__ void skinny_copy_rows(const SkinnyArgs& a, const float* os, int plane,
                                                  const int32_t* cw, int32_t cs0, int n) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool py = a.p_walk == SK_P_Y;
-  const bool per_warp = a.ty >= SK_THREADS / 32;
-  const int y0 = per_warp ? warp : 0, ys = per_warp ? SK_THREADS / 32 : 1;
-  const int f0 = per_warp ? lane : tid, fs = per_warp ? 32 : SK_THREADS;
+  const bool per_warp = a.ty >= NT / 32;
+  const int y0 = per_warp ? warp : 0, ys = per_warp ? NT / 32 : 1;
+  const int f0 = per_warp ? lane : tid, fs = per_warp ? 32 : NT;
   const float alpha = a.alpha, beta = a.beta;
   bool issued = false;
   for (int yl = y0; yl < a.ty; yl += ys) {
@@ -649,6 +651,227 @@ __device__ __forceinline__ void skinny_dispatch(int rs, F&& f) {
   }
 }
 
+// A grouped launch's item (see the grouped kernels below).
+struct SkinnyItem {
+  SkinnyArgs args;
+  int64_t begin;
+};
+
+// ---- register path: a narrow side of at most 16 rows ------------------------
+// With 4 rows per thread the tile path reads each staged P value four times
+// from shared memory (once per row group): 5 shared-memory wavefronts per 16
+// FMAs of a warp, more than the FMA pipe's time for them, and its copies land
+// through the same L1 data path, so copies and FMAs queue behind each other.
+// Here P goes from global memory straight to registers: 128 threads, thread t
+// owns positions t and t + 128 of the block and all 16 rows (32 sums); each
+// step of 16 k loads the next step's 2 x 16 P values while it multiplies the
+// current ones with the step's Q values, broadcast from shared memory (4
+// wavefronts per 32 FMAs of a warp). Same boxes, jobs, k slices and C stores
+// as the tile path (rows staged in shared memory, then the store walks or the
+// linear / bulk copies); four CTAs per SM.
+constexpr int SKR_THREADS = 128;
+constexpr int SKR_ROWS = 16;
+constexpr int SKR_KR = 16;  // k per step
+constexpr size_t SKR_OFF_OS = (size_t)2 * SKR_KR * SKR_ROWS * 4;  // after Qs[2][KR][ROWS]
+constexpr size_t SKR_OFF_TAB = SKR_OFF_OS + (size_t)SKR_ROWS * SK_LDP * 4;
+constexpr size_t SKR_SMEM_BYTES = SKR_OFF_TAB + (size_t)(4 * SK_BW + 2 * SKR_ROWS) * 4;
+constexpr int SKR_CTAS_PER_SM = 4;
+static_assert(SK_BW == 2 * SKR_THREADS, "two positions per thread");
+static_assert(SKR_CTAS_PER_SM * (SKR_SMEM_BYTES + 1024) <= 228 * 1024, "CTAs per SM");
+
+// Box offsets of positions w = tid, tid + 128 and the C offsets of the 16 rows.
+__device__ __forceinline__ void skinny_reg_begin(const SkinnyArgs& a, int b, int32_t* pw,
+                                                 int32_t* cw, int32_t* cs) {
+  const int ix = a.bxn == 1 ? 0 : b % a.bxn, iy = a.bxn == 1 ? b : b / a.bxn;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int w = threadIdx.x + h * SKR_THREADS;
+    int xl, yl;
+    if (a.p_walk == SK_P_Y) {
+      yl = w % a.ty;
+      xl = w / a.ty;
+    } else {
+      xl = w % a.tx;
+      yl = w / a.tx;
+    }
+    const int x = ix * a.tx + xl, y = iy * a.ty + yl;
+    const bool ok = w < a.tx * a.ty && x < a.ex && y < a.ey;
+    pw[w] = ok ? x * a.px + __ldg(a.p_y_off + y) : SK_NONE;
+    cw[w] = ok ? x * a.cx + __ldg(a.c_y_off + y) : SK_NONE;
+  }
+  if (!a.partial && threadIdx.x < SKR_ROWS) {
+    const int s = threadIdx.x;
+    cs[s] = s < a.S ? __ldg(a.c_s_off + s) : 0;
+  }
+}
+
+// Q rows 0..15 of k [kb, kb + 16) into qs[k][row] (zeros past S or ke).
+__device__ __forceinline__ void skinny_reg_q(const SkinnyArgs& a, int kb, int ke, float* qs) {
+#pragma unroll
+  for (int i = 0; i < SKR_KR * SKR_ROWS / SKR_THREADS; ++i) {
+    const int e = threadIdx.x + i * SKR_THREADS;
+    const int kk = e / SKR_ROWS, r = e % SKR_ROWS;
+    float* d = qs + e;
+    if (r < a.S && kb + kk < ke)
+      cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + r) + __ldg(a.q_k_off + kb + kk));
+    else
+      *d = 0.0f;
+  }
+  cp_async_commit();
+}
+
+// P of the thread's two positions at k [kb, kb + 16) (zeros past ke or the box).
+__device__ __forceinline__ void skinny_reg_p(const SkinnyArgs& a, int kb, int ke, int32_t po0,
+                                             int32_t po1, float (&p0)[SKR_KR], float (&p1)[SKR_KR]) {
+  const int lane = threadIdx.x & 31;
+  const int32_t ko_lane = lane < SKR_KR && kb + lane < ke ? __ldg(a.p_k_off + kb + lane) : 0;
+#pragma unroll
+  for (int kk = 0; kk < SKR_KR; ++kk) {
+    const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, kk);
+    const bool kok = kb + kk < ke;
+    p0[kk] = kok && po0 != SK_NONE ? __ldg(a.P + po0 + ko) : 0.0f;
+    p1[kk] = kok && po1 != SK_NONE ? __ldg(a.P + po1 + ko) : 0.0f;
+  }
+}
+
+// The end of a job: raw sums to its k slice, or the rows to C (staged in os).
+__device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJob& j,
+                                                  const float (&acc)[2][SKR_ROWS], float* os,
+                                                  const int32_t* cw, const int32_t* cs) {
+  const int tid = threadIdx.x;
+  if (a.partial) {  // layout of the 16-row (RS = 4) tile path
+    float* dst = a.partial + (((size_t)j.z * a.nblk + j.b) * a.npass + j.p) * SKR_ROWS * SK_BW + tid;
+#pragma unroll
+    for (int r = 0; r < SKR_ROWS; ++r) {
+      dst[(size_t)r * SK_BW] = acc[0][r];
+      dst[(size_t)r * SK_BW + SKR_THREADS] = acc[1][r];
+    }
+    return;
+  }
+  const int S = a.S;
+  if (a.c_lin != SK_CLIN_NONE) {
+    // staged per box row in C's order: [s][x] (XS, rows tx apart) or [x][s] (SX)
+    const bool py = a.p_walk == SK_P_Y, xs = a.c_lin == SK_CLIN_XS;
+    const int tx = a.tx, ty = a.ty, plane = tx * (xs ? SKR_ROWS : S);
+    const float sc = a.c_bulk ? a.alpha : 1.0f;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int w = tid + h * SKR_THREADS;
+      if (w >= tx * ty) continue;
+      const int xl = py ? w / ty : w % tx, yl = py ? w % ty : w / tx;
+      float* o = os + yl * plane + (xs ? xl : xl * S);
+#pragma unroll
+      for (int r = 0; r < SKR_ROWS; ++r)
+        if (r < S) o[xs ? r * tx : r] = sc * acc[h][r];
+    }
+    if (a.c_bulk) fence_proxy_async_smem();
+    __syncthreads();
+    if (xs) {
+      skinny_copy_rows<SKR_THREADS>(a, os, plane, cw, cs[0], tx * S);
+    } else {
+      const int ix = a.bxn == 1 ? 0 : j.b % a.bxn;
+      const int xn = a.ex - ix * tx < tx ? a.ex - ix * tx : tx;
+      skinny_copy_rows<SKR_THREADS>(a, os, plane, cw, cs[0], xn * S);
+    }
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < SKR_ROWS; ++r) {
+    os[r * SK_LDP + tid] = acc[0][r];
+    os[r * SK_LDP + tid + SKR_THREADS] = acc[1][r];
+  }
+  __syncthreads();
+  skinny_store<SKR_THREADS>(a, os, cw, cs, 0, S);
+}
+
+template <typename Resolve>
+__device__ __forceinline__ void skinny_reg_loop(int j0, int jstep, int njobs, Resolve&& resolve,
+                                                uint8_t* smem) {
+  float* Qs = reinterpret_cast<float*>(smem);  // [2][KR][ROWS]
+  float* os = reinterpret_cast<float*>(smem + SKR_OFF_OS);
+  int32_t* pw = reinterpret_cast<int32_t*>(smem + SKR_OFF_TAB);
+  int32_t* cw = pw + SK_BW;
+  int32_t* cs = cw + SK_BW;
+  const int tid = threadIdx.x;
+#pragma unroll 1
+  for (int jg = j0; jg < njobs; jg += jstep) {
+    const SkRef ref = resolve(jg);
+    const SkinnyArgs& a = *ref.a;
+    const SkJob job = skinny_job(a, ref.J);
+    __syncthreads();  // the previous job's stores are done with os, pw, cw, cs
+    skinny_reg_begin(a, job.b, pw, cw, cs);
+    __syncthreads();
+    const int32_t po0 = pw[tid], po1 = pw[tid + SKR_THREADS];
+    const int kbeg = job.c0 * SK_KC;
+    const int kend = job.c1 * SK_KC < a.K ? job.c1 * SK_KC : a.K;
+    float acc[2][SKR_ROWS];
+#pragma unroll
+    for (int r = 0; r < SKR_ROWS; ++r) acc[0][r] = acc[1][r] = 0.0f;
+    float pc0[SKR_KR], pc1[SKR_KR];
+    skinny_reg_q(a, kbeg, kend, Qs);
+    skinny_reg_p(a, kbeg, kend, po0, po1, pc0, pc1);
+    int st = 0;
+#pragma unroll 1
+    for (int kb = kbeg; kb < kend; kb += SKR_KR) {
+      const int nb = kb + SKR_KR;
+      float pn0[SKR_KR], pn1[SKR_KR];
+      if (nb < kend) {
+        __syncthreads();  // stage st ^ 1 was read by the previous step
+        skinny_reg_q(a, nb, kend, Qs + (st ^ 1) * SKR_KR * SKR_ROWS);
+        skinny_reg_p(a, nb, kend, po0, po1, pn0, pn1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();  // Q of this step landed
+      const float* q = Qs + st * SKR_KR * SKR_ROWS;
+#pragma unroll
+      for (int kk = 0; kk < SKR_KR; ++kk) {
+        float qv[SKR_ROWS];
+#pragma unroll
+        for (int r = 0; r < SKR_ROWS; r += 4) {
+          const float4 t = *reinterpret_cast<const float4*>(q + kk * SKR_ROWS + r);
+          qv[r] = t.x; qv[r + 1] = t.y; qv[r + 2] = t.z; qv[r + 3] = t.w;
+        }
+#pragma unroll
+        for (int r = 0; r < SKR_ROWS; ++r) {
+          acc[0][r] = fmaf(qv[r], pc0[kk], acc[0][r]);
+          acc[1][r] = fmaf(qv[r], pc1[kk], acc[1][r]);
+        }
+      }
+      if (nb < kend) {
+#pragma unroll
+        for (int kk = 0; kk < SKR_KR; ++kk) {
+          pc0[kk] = pn0[kk];
+          pc1[kk] = pn1[kk];
+        }
+      }
+      st ^= 1;
+    }
+    skinny_reg_finish(a, job, acc, os, cw, cs);
+  }
+}
+
+__global__ void __launch_bounds__(SKR_THREADS, SKR_CTAS_PER_SM)
+    skinny_reg_kernel(const __grid_constant__ SkinnyArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  grid_dep_wait();
+  auto resolve = [&](int J) { return SkRef{&a, J}; };
+  skinny_reg_loop(blockIdx.x, gridDim.x, a.njobs, resolve, smem);
+  bulk_wait_all();  // bulk C copies complete before the CTA exits
+}
+
+__global__ void __launch_bounds__(SKR_THREADS, SKR_CTAS_PER_SM)
+    skinny_reg_group_kernel(const SkinnyItem* items, const int64_t* begin, int n, int njobs) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  auto resolve = [&](int J) {
+    const SkinnyItem& it = items[find_segment(begin, n, J)];
+    return SkRef{&it.args, (int)(J - it.begin)};
+  };
+  skinny_reg_loop(blockIdx.x, gridDim.x, njobs, resolve, smem);
+  bulk_wait_all();
+}
+
 // persistent grid (SK_CTAS_PER_SM CTAs per SM) over the plan's jobs; one
 // instantiation per rows-per-thread class (RS = a.rs)
 template <int RS>
@@ -673,10 +896,6 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
 // [begin[i], begin[i + 1]); one persistent launch per rows-per-thread class
 // (RS = the items' rs) walks all of them. Reduction items:
 // CTAs [begin[i], begin[i + 1]) are the (block, pass) pairs of a k-split item.
-struct SkinnyItem {
-  SkinnyArgs args;
-  int64_t begin;
-};
 
 template <int RS>
 __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)

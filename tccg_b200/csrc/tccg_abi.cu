@@ -114,6 +114,7 @@ struct tccg_plan {
   // skinny kernel (skinny_gett.cuh): geometry and tables in sk (operand, C
   // and slice pointers are filled in per run); s_is_n: the narrow side is N
   bool skinny = false, sk_s_is_n = false, sk_p_vec = false;
+  bool sk_reg = false;  // the register path (narrow side <= 16 rows)
   int32_t sk_ksplit = 1;
   SkinnyArgs sk{};
   // its 32-bit offset tables in one allocation: P and C offsets of the Y
@@ -566,6 +567,10 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
     a.c_lin = SK_CLIN_XS;
   else if (a.c_walk == SK_C_SX && a.npass == 1 && S <= SK_SUB && a.cx == S && affine(1))
     a.c_lin = SK_CLIN_SX;
+  // a narrow side of at most 16 rows: P straight to registers (skinny_reg_kernel);
+  // TCCG_B200_SKINNY_REG=0 keeps the shared-memory path
+  const char* reg_env = std::getenv("TCCG_B200_SKINNY_REG");
+  p->sk_reg = a.rs == 4 && a.npass == 1 && !(reg_env && std::strcmp(reg_env, "0") == 0);
   a.alpha = 1.0f;
   a.beta = 0.0f;
   return true;
@@ -974,15 +979,16 @@ static int plan_layout(tccg_plan* p) {
     snprintf(p->describe, sizeof(p->describe),
              "method=GETT prec=%s kernel=skinny_gett<f32> M=%lld N=%lld K=%lld narrow=%s S=%d "
              "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
-             "grid=%lld load=%s%s%s store=%s%s%s pack=none",
+             "grid=%lld load=%s%s%s store=%s%s%s%s pack=none",
              p->prec == TCCG_PREC_BF16X3 ? "bf16x3" : "fp32", (long long)p->M, (long long)p->N,
              (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S, a.npass, 4 * a.rs, a.tx, a.ty,
              (long long)a.ex, (long long)a.ey, (long long)a.nblk, a.nchunks, p->sk_ksplit,
              (long long)a.njobs,
-             (long long)std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms),
+             (long long)std::min<int64_t>(
+                 a.njobs, (int64_t)(p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM) * p->num_sms),
              pw[a.p_walk], p->sk_p_vec ? " x16B" : "", a.q_kfast ? " q=k" : " q=s", cw[a.c_walk],
              a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "",
-             a.c_lin ? " linear" : "");
+             a.c_lin ? " linear" : "", p->sk_reg ? " path=registers" : "");
     p->ws_bytes = ws;
     return TCCG_OK;
   }
@@ -1283,6 +1289,10 @@ static cudaError_t set_attrs() {
     });
   chk(cudaFuncSetAttribute(skinny_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SK_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_reg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SKR_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_reg_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SKR_SMEM_BYTES));
   chk(cudaFuncSetAttribute(skinny_reduce_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SK_SMEM_BYTES));
   chk(cudaFuncSetAttribute(gett_tc2_kernel<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1817,12 +1827,18 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
 static int run_skinny(const tccg_plan* p, const void* GA, const void* GB, float* C, float alpha,
                       float beta, char* w, cudaStream_t s) {
   const SkinnyArgs a = skinny_args(p, GA, GB, C, alpha, beta, w);
-  const int64_t grid = std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms);
   mark(1, 0, s);
-  with_skinny_rs(a.rs, [&](auto r) {
-    launch_after(false, p, skinny_gett_kernel<decltype(r)::value>, dim3((unsigned)grid),
-                 dim3(SK_THREADS), SK_SMEM_BYTES, s, a);
-  });
+  if (p->sk_reg) {
+    const int64_t grid = std::min<int64_t>(a.njobs, (int64_t)SKR_CTAS_PER_SM * p->num_sms);
+    launch_after(false, p, skinny_reg_kernel, dim3((unsigned)grid), dim3(SKR_THREADS),
+                 SKR_SMEM_BYTES, s, a);
+  } else {
+    const int64_t grid = std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms);
+    with_skinny_rs(a.rs, [&](auto r) {
+      launch_after(false, p, skinny_gett_kernel<decltype(r)::value>, dim3((unsigned)grid),
+                   dim3(SK_THREADS), SK_SMEM_BYTES, s, a);
+    });
+  }
   int rc = launch_check("skinny_gett");
   mark(1, 1, s);
   if (rc || p->sk_ksplit == 1) return rc;
@@ -2139,6 +2155,7 @@ struct tccg_group {
     // [sk0[c], sk0[c] + nsk[c]) of d_sk with sk_jobs[c] jobs; reductions
     int32_t sk0[3] = {}, nsk[3] = {}, skr0 = 0, nskr = 0;
     int64_t sk_jobs[3] = {}, skr_ctas = 0;
+    bool sk_reg[3] = {};  // the lane runs the register path
   };
   std::vector<Wave> waves;
   bool bound = false;
@@ -2499,6 +2516,7 @@ static void bind_skinny(tccg_group* g, tccg_group::Wave& wv, const void* const* 
     }
     wv.nsk[cls] = (int32_t)items.size() - wv.sk0[cls];
     wv.sk_jobs[cls] = jobs;
+    wv.sk_reg[cls] = !idx.empty() && g->plans[idx[0]]->sk_reg;
   }
   wv.nskr = (int32_t)red.size() - wv.skr0;
   wv.skr_ctas = rctas;
@@ -2641,12 +2659,19 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
   if constexpr (sizeof(T) == 4) {
     for (int cls = 0; cls < 3; ++cls) {
       if (wv.nsk[cls] == 0) continue;
-      const unsigned grid =
-          (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SK_CTAS_PER_SM * g->num_sms);
-      with_skinny_rs(4 * (cls + 1), [&](auto r) {
-        skinny_group_kernel<decltype(r)::value><<<grid, SK_THREADS, SK_SMEM_BYTES, s>>>(
-            g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], wv.sk_jobs[cls]);
-      });
+      if (wv.sk_reg[cls]) {  // the register path (its items all take it)
+        const unsigned grid =
+            (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SKR_CTAS_PER_SM * g->num_sms);
+        skinny_reg_group_kernel<<<grid, SKR_THREADS, SKR_SMEM_BYTES, s>>>(
+            g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], (int)wv.sk_jobs[cls]);
+      } else {
+        const unsigned grid =
+            (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SK_CTAS_PER_SM * g->num_sms);
+        with_skinny_rs(4 * (cls + 1), [&](auto r) {
+          skinny_group_kernel<decltype(r)::value><<<grid, SK_THREADS, SK_SMEM_BYTES, s>>>(
+              g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], wv.sk_jobs[cls]);
+        });
+      }
       if ((rc = launch_check("skinny_group"))) return rc;
     }
     if (wv.nskr > 0) {

@@ -90,6 +90,25 @@ def test_skinny_k_split_is_deterministic(cuda, ksplit):
     assert error_metrics(o1, ref)["normwise"] <= 1e-6
 
 
+@pytest.mark.parametrize("name", ["matvec_split", "matvec"])
+def test_skinny_register_and_shared_paths_agree(cuda, monkeypatch, name):
+    """A narrow side of at most 16 rows runs the register path (P straight
+    to registers, skinny_reg_kernel); TCCG_B200_SKINNY_REG=0 keeps the
+    shared-memory path. Both sum k in the same order per slice: the same
+    bits, and the oracle's values."""
+    lc, la, lb, sizes, alpha, beta, _ = CASES[name]
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, C = _data(ln, 31)
+    o_reg, p_reg = run_gpu(con, "fp32", A, B, C, tuning=Tuning(skinny=1))
+    monkeypatch.setenv("TCCG_B200_SKINNY_REG", "0")
+    o_smem, p_smem = run_gpu(con, "fp32", A, B, C, tuning=Tuning(skinny=1))
+    assert "path=registers" in p_reg.describe() and "path=registers" not in p_smem.describe()
+    assert np.array_equal(o_reg, o_smem)
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    assert error_metrics(o_reg, ref)["normwise"] <= 1e-6
+
+
 def test_skinny_bulk_and_element_stores_agree(cuda):
     """Linear C rows with beta = 0 leave by bulk copies (alpha applied when
     staging) when C is 16-byte aligned, else by element stores: a C one
