@@ -540,11 +540,15 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   int lg = 0;
   while ((1 << lg) < std::min<int64_t>(p->K, SK_KC)) ++lg;
   a.kr_log2 = lg;
+  // a narrow side of at most 16 rows: P straight to registers (skinny_reg_kernel);
+  // TCCG_B200_SKINNY_REG=0 keeps the shared-memory path
+  const char* reg_env = std::getenv("TCCG_B200_SKINNY_REG");
+  p->sk_reg = a.rs == 4 && a.npass == 1 && !(reg_env && std::strcmp(reg_env, "0") == 0);
   // k-split: (block, pass) jobs that cannot fill the persistent CTAs,
   // slices of >= 4 chunks
+  const int64_t per_sm = p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM;
   a.chunks_per_split = (int32_t)choose_ksplit(p->tune.ksplit, (int64_t)a.nblk * a.npass, a.nchunks,
-                                              (int64_t)SK_CTAS_PER_SM * p->num_sms, 4,
-                                              &p->sk_ksplit);
+                                              per_sm * p->num_sms, 4, &p->sk_ksplit);
   a.ksplit = p->sk_ksplit;
   const int64_t njobs = (int64_t)a.nblk * a.npass * a.ksplit;
   if (njobs > INT32_MAX) return false;
@@ -567,10 +571,6 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
     a.c_lin = SK_CLIN_XS;
   else if (a.c_walk == SK_C_SX && a.npass == 1 && S <= SK_SUB && a.cx == S && affine(1))
     a.c_lin = SK_CLIN_SX;
-  // a narrow side of at most 16 rows: P straight to registers (skinny_reg_kernel);
-  // TCCG_B200_SKINNY_REG=0 keeps the shared-memory path
-  const char* reg_env = std::getenv("TCCG_B200_SKINNY_REG");
-  p->sk_reg = a.rs == 4 && a.npass == 1 && !(reg_env && std::strcmp(reg_env, "0") == 0);
   a.alpha = 1.0f;
   a.beta = 0.0f;
   return true;
@@ -589,7 +589,7 @@ static double skinny_time(const tccg_plan* p) {
   const double fma = 2.0 * (double)a.nblk * SK_BW * rows * K;
   double t = fma / 18e12 + 4.0 * W * S / 2.0e12 + 4.0 * W * K / 6e12;
   // the rates need every persistent CTA busy
-  const double slots = (double)SK_CTAS_PER_SM * p->num_sms;
+  const double slots = (double)(p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM) * p->num_sms;
   if ((double)a.njobs < slots) t *= slots / (double)a.njobs;
   t += 4e-6;
   if (p->sk_ksplit > 1) t += 8.0 * p->sk_ksplit * (double)a.nblk * rows * SK_BW / 3e12 + 5e-6;

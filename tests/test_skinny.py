@@ -94,15 +94,17 @@ def test_skinny_k_split_is_deterministic(cuda, ksplit):
 def test_skinny_register_and_shared_paths_agree(cuda, monkeypatch, name):
     """A narrow side of at most 16 rows runs the register path (P straight
     to registers, skinny_reg_kernel); TCCG_B200_SKINNY_REG=0 keeps the
-    shared-memory path. Both sum k in the same order per slice: the same
-    bits, and the oracle's values."""
+    shared-memory path. With the same k slices (given explicitly: the
+    automatic count follows each path's CTAs per SM) both sum k in the same
+    order: the same bits, and the oracle's values."""
     lc, la, lb, sizes, alpha, beta, _ = CASES[name]
     con = make_contraction(lc, la, lb, sizes, alpha, beta)
     ln = LoopNest(lc, la, lb, sizes)
     A, B, C = _data(ln, 31)
-    o_reg, p_reg = run_gpu(con, "fp32", A, B, C, tuning=Tuning(skinny=1))
+    t = Tuning(skinny=1, ksplit=3 if name == "matvec_split" else 1)
+    o_reg, p_reg = run_gpu(con, "fp32", A, B, C, tuning=t)
     monkeypatch.setenv("TCCG_B200_SKINNY_REG", "0")
-    o_smem, p_smem = run_gpu(con, "fp32", A, B, C, tuning=Tuning(skinny=1))
+    o_smem, p_smem = run_gpu(con, "fp32", A, B, C, tuning=t)
     assert "path=registers" in p_reg.describe() and "path=registers" not in p_smem.describe()
     assert np.array_equal(o_reg, o_smem)
     ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
