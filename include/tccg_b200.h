@@ -131,7 +131,10 @@ typedef struct tccg_tuning {
                           tensors of fewer than 2^31 elements: the skinny kernel -- chunks of
                           the narrow operand in shared memory, the wide one streamed once in
                           place, C written once. 0 = chosen by the model, 1 = always (an
-                          error where it does not apply), -1 = never */
+                          error where it does not apply), -1 = never; 2 = its tensor-core
+                          form (BF16X3, min(M, N) <= 64, K <= 2^29: the wide operand split
+                          into bf16 hi / lo on the fly, tcgen05 MMAs; single plans only, a
+                          group refuses it) */
 } tccg_tuning;
 
 typedef struct tccg_plan tccg_plan; /* opaque */

@@ -181,6 +181,9 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             tiles = [128] if precision == "bf16x3" else [192, 128]
             tl = 1 if len(loads) > 1 else 0
             more = [Tuning(method=method, load=tl, variant=chunks[0], tile_n=w) for w in tiles]
+            # the tensor-core skinny kernel (single plans only)
+            if method == "gett" and not grouped and skinny_tc_eligible(M, N, K, precision, dtype):
+                more.insert(0, Tuning(method=method, skinny=2))
             for ld in loads:
                 more += [Tuning(method=method, load=ld, raster=r) for r in (-8, 4, 16, -2)]
                 more += [Tuning(method=method, load=ld, variant=c) for c in chunks[1:]]
@@ -216,6 +219,13 @@ def skinny_eligible(M: int, N: int, K: int, precision: str, dtype: str = "f32") 
     also wants tensors of fewer than 2^31 elements, and the search skips a
     candidate it refuses)."""
     return dtype == "f32" and precision in ("fp32", "bf16x3") and min(M, N) <= 256
+
+
+def skinny_tc_eligible(M: int, N: int, K: int, precision: str, dtype: str = "f32") -> bool:
+    """Whether the tensor-core skinny kernel (tuning.skinny = 2) can run a GETT
+    of these extents: split-BF16x3 with FP32 operands, min(M, N) <= 64,
+    K <= 2^29 (the C ABI's rule)."""
+    return dtype == "f32" and precision == "bf16x3" and min(M, N) <= 64 and K <= (1 << 29)
 
 
 def _flush_l2(buf):

@@ -184,19 +184,36 @@ __device__ __forceinline__ void skinny_begin(const SkinnyArgs& a, int b, int p, 
   }
 }
 
-// Issues the copies of chunk c of job j (P: [k][position], Q: the pass's
-// rows, [k][row]) as one cp.async group; elements outside the tensors are
-// zeros. pw must hold the job's box offsets (visible to all threads).
-__device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j, int c, int sp,
-                                             float* ps, float* qs, const int32_t* pw) {
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int k0 = c * SK_KC;
+// The P k offset thread tid's copies of chunk c start from: k = tid % kr
+// of the chunk for the walk along k, else k = lane (passed around the warp
+// by shuffles); 0 past the chunk's extent. A table load whose result the
+// copies wait for: callers load it a chunk ahead.
+__device__ __forceinline__ int32_t skinny_p_ko(const SkinnyArgs& a, int c) {
+  const int tid = threadIdx.x;
+  const int kl = a.p_walk == SK_P_K ? tid & ((1 << a.kr_log2) - 1) : tid & 31;
+  return kl < skinny_kc(a, c) ? __ldg(a.p_k_off + c * SK_KC + kl) : 0;
+}
+
+// Issues the P copies of chunk c ([k][position], k < the chunk's extent) of
+// the box whose offsets pw holds (visible to all threads; positions outside
+// the tensor are zeros); ko = skinny_p_ko(a, c). Threads 0 .. SK_THREADS - 1
+// take part; no commit. ZFILL: the zeros go through cp.async too (a
+// barrier that counts the copies' completion then covers them).
+template <bool ZFILL = false>
+__device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float* ps,
+                                               const int32_t* pw, int32_t ko) {
+  auto zero = [&](float* d) {
+    if (ZFILL)
+      cp_async_zero4(d, a.P);
+    else
+      *d = 0.0f;
+  };
+  const int tid = threadIdx.x;
   const int kc = skinny_kc(a, c);
   if (a.p_walk == SK_P_K) {
     // lanes along k: thread tid takes k = tid % kr of positions tid / kr + i * 256 / kr
     const int lg = a.kr_log2, kl = tid & ((1 << lg) - 1);
     if (kl < kc) {
-      const int32_t ko = __ldg(a.p_k_off + k0 + kl);
       float* d = ps + kl * SK_LDP;
 #pragma unroll 4
       for (int w = tid >> lg; w < SK_BW; w += SK_THREADS >> lg) {
@@ -204,7 +221,7 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
         if (po != SK_NONE)
           cp_async_elem<4>(d + w, a.P + po + ko);
         else
-          d[w] = 0.0f;
+          zero(d + w);
       }
     }
   } else if (a.p_vec) {
@@ -214,20 +231,19 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
     const int g = 4 * (tid % SK_WG);
     const int32_t o0 = pw[g], o1 = pw[g + 1], o2 = pw[g + 2], o3 = pw[g + 3];
     const bool vec = o0 != SK_NONE && (o0 & 3) == 0 && o1 == o0 + 1 && o2 == o0 + 2 && o3 == o0 + 3;
-    const int32_t ko_lane = lane < kc ? __ldg(a.p_k_off + k0 + lane) : 0;
     for (int k = tid / SK_WG; k < kc; k += SK_SG) {  // warp-uniform k
-      const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
+      const int32_t kok = __shfl_sync(0xffffffffu, ko, k);
       float* d = ps + k * SK_LDP + g;
       if (vec) {
-        cp_async_16(d, a.P + o0 + ko);
+        cp_async_16(d, a.P + o0 + kok);
       } else {
         const int32_t o[4] = {o0, o1, o2, o3};
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           if (o[e] != SK_NONE)
-            cp_async_elem<4>(d + e, a.P + o[e] + ko);
+            cp_async_elem<4>(d + e, a.P + o[e] + kok);
           else
-            d[e] = 0.0f;
+            zero(d + e);
         }
       }
     }
@@ -236,18 +252,29 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
     // the chunk's k offsets are loaded once per warp (lane k) and passed
     // around by shuffles, so no copy waits on a table load
     const int32_t po = pw[tid];
-    const int32_t ko_lane = lane < kc ? __ldg(a.p_k_off + k0 + lane) : 0;
     float* d = ps + tid;
     const float* src = a.P + (po != SK_NONE ? po : 0);
 #pragma unroll 4
     for (int k = 0; k < kc; ++k) {
-      const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, k);
+      const int32_t kok = __shfl_sync(0xffffffffu, ko, k);
       if (po != SK_NONE)
-        cp_async_elem<4>(d + k * SK_LDP, src + ko);
+        cp_async_elem<4>(d + k * SK_LDP, src + kok);
       else
-        d[k * SK_LDP] = 0.0f;
+        zero(d + k * SK_LDP);
     }
   }
+}
+
+// Issues the copies of chunk c of job j (P: [k][position], Q: the pass's
+// rows, [k][row]) as one cp.async group; elements outside the tensors are
+// zeros. pw must hold the job's box offsets (visible to all threads); ko =
+// skinny_p_ko(a, c).
+__device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j, int c, int sp,
+                                             float* ps, float* qs, const int32_t* pw, int32_t ko) {
+  skinny_issue_p(a, c, ps, pw, ko);
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int k0 = c * SK_KC;
+  const int kc = skinny_kc(a, c);
   // Q rows p sp .. p sp + sp - 1 of k [0, kc); rows >= S are zeros
   const int s0 = j.p * sp;
   if (a.q_kfast) {
@@ -316,8 +343,9 @@ __device__ __forceinline__ void skinny_plane(const SkinnyArgs& a, const float* o
 // row s0 + r) in the walk's address order; the NT / 32 warps share the planes.
 template <int NT = SK_THREADS>
 __device__ __forceinline__ void skinny_store(const SkinnyArgs& a, const float* os,
-                                             const int32_t* cw, const int32_t* cs, int s0, int ns) {
-  const int warp = threadIdx.x >> 5;
+                                             const int32_t* cw, const int32_t* cs, int s0, int ns,
+                                             int tid) {
+  const int warp = tid >> 5;
   const bool py = a.p_walk == SK_P_Y;
   const int tx = a.tx, ty = a.ty;
   if (a.c_walk == SK_C_XS) {
@@ -387,8 +415,8 @@ __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, cons
 // threads.
 template <int NT = SK_THREADS>
 __device__ __forceinline__ void skinny_copy_rows(const SkinnyArgs& a, const float* os, int plane,
-                                                 const int32_t* cw, int32_t cs0, int n) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+                                                 const int32_t* cw, int32_t cs0, int n, int tid) {
+  const int lane = tid & 31, warp = tid >> 5;
   const bool py = a.p_walk == SK_P_Y;
   const bool per_warp = a.ty >= NT / 32;
   const int y0 = per_warp ? warp : 0, ys = per_warp ? NT / 32 : 1;
@@ -467,7 +495,7 @@ __device__ __forceinline__ void skinny_finish_lin(const SkinnyArgs& a, const SkJ
       }
       if (a.c_bulk) fence_proxy_async_smem();  // the bulk copies read the staging
       __syncthreads();
-      skinny_copy_rows(a, os, plane, cw, cs[h], tx * ns);
+      skinny_copy_rows(a, os, plane, cw, cs[h], tx * ns, threadIdx.x);
     }
   } else {  // SK_CLIN_SX: all of S (<= 32 rows) in one step
     const int S = a.S;
@@ -484,7 +512,7 @@ __device__ __forceinline__ void skinny_finish_lin(const SkinnyArgs& a, const SkJ
       }
     }
     __syncthreads();
-    skinny_copy_rows(a, os, plane, cw, cs[0], xn * S);
+    skinny_copy_rows(a, os, plane, cw, cs[0], xn * S, threadIdx.x);
   }
 }
 
@@ -522,7 +550,7 @@ __device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& 
             make_float4(acc.v[i][0], acc.v[i][1], acc.v[i][2], acc.v[i][3]);
     }
     __syncthreads();
-    skinny_store(a, os, cw, cs + h, s0, ns);
+    skinny_store(a, os, cw, cs + h, s0, ns, threadIdx.x);
   }
 }
 
@@ -555,7 +583,7 @@ __device__ __forceinline__ void skinny_loop(int j0, int jstep, int njobs, Resolv
     c1 = job.c1;
     skinny_begin(*cur.a, job.b, job.p, SP, pw, cw, cs);
     __syncthreads();
-    skinny_issue(*cur.a, job, c, SP, Ps, Qs, pw);
+    skinny_issue(*cur.a, job, c, SP, Ps, Qs, pw, skinny_p_ko(*cur.a, c));
   }
   int st = 0, slot = 0;
   SkAcc<RS> acc;
@@ -583,7 +611,7 @@ __device__ __forceinline__ void skinny_loop(int j0, int jstep, int njobs, Resolv
         if (nref.a->p_walk == SK_P_K || nref.a->p_vec) __syncthreads();
       }
       skinny_issue(*nref.a, njob, nc, SP, Ps + (st ^ 1) * (SK_P_STAGE / 4),
-                   Qs + (st ^ 1) * (SK_Q_STAGE / 4), pw + ns * SK_BW);
+                   Qs + (st ^ 1) * (SK_Q_STAGE / 4), pw + ns * SK_BW, skinny_p_ko(*nref.a, nc));
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -613,6 +641,7 @@ __device__ __forceinline__ void skinny_loop(int j0, int jstep, int njobs, Resolv
 template <int RS>
 __device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int r, uint8_t* smem) {
   constexpr int SP = 4 * RS;
+  static_assert(SP <= 2 * SK_SPMAX, "the rows' C offsets fit the two offset slots");
   float* os = reinterpret_cast<float*>(smem);
   int32_t* pw = reinterpret_cast<int32_t*>(smem + SK_OFF_TAB);
   int32_t* cw = pw + 2 * SK_BW;
@@ -638,7 +667,7 @@ __device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int r, 
       os[rr * SK_LDP + tid] = v;
     }
     __syncthreads();
-    skinny_store(a, os, cw, cs + h, s0, ns);
+    skinny_store(a, os, cw, cs + h, s0, ns, threadIdx.x);
   }
 }
 
@@ -648,6 +677,18 @@ __device__ __forceinline__ void skinny_dispatch(int rs, F&& f) {
     case 4: f(std::integral_constant<int, 4>()); break;
     case 8: f(std::integral_constant<int, 8>()); break;
     default: f(std::integral_constant<int, 12>()); break;
+  }
+}
+
+// The reductions also serve the tensor-core kernel's slices (skinny_tc.cuh:
+// one pass of up to 64 rows, RS = 16).
+template <typename F>
+__device__ __forceinline__ void skinny_reduce_dispatch(int rs, F&& f) {
+  switch (rs) {
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 8: f(std::integral_constant<int, 8>()); break;
+    case 12: f(std::integral_constant<int, 12>()); break;
+    default: f(std::integral_constant<int, 16>()); break;
   }
 }
 
@@ -720,11 +761,18 @@ __device__ __forceinline__ void skinny_reg_q(const SkinnyArgs& a, int kb, int ke
   cp_async_commit();
 }
 
-// P of the thread's two positions at k [kb, kb + 16) (zeros past ke or the box).
-__device__ __forceinline__ void skinny_reg_p(const SkinnyArgs& a, int kb, int ke, int32_t po0,
-                                             int32_t po1, float (&p0)[SKR_KR], float (&p1)[SKR_KR]) {
+// The P k offset of k = kb + lane (lanes < 16, k < ke; else 0): loaded a
+// step ahead of the copies that use it.
+__device__ __forceinline__ int32_t skinny_reg_ko(const SkinnyArgs& a, int kb, int ke) {
   const int lane = threadIdx.x & 31;
-  const int32_t ko_lane = lane < SKR_KR && kb + lane < ke ? __ldg(a.p_k_off + kb + lane) : 0;
+  return lane < SKR_KR && kb + lane < ke ? __ldg(a.p_k_off + kb + lane) : 0;
+}
+
+// P of the thread's two positions at k [kb, kb + 16) (zeros past ke or the
+// box); ko_lane = skinny_reg_ko(a, kb, ke).
+__device__ __forceinline__ void skinny_reg_p(const SkinnyArgs& a, int kb, int ke, int32_t po0,
+                                             int32_t po1, float (&p0)[SKR_KR], float (&p1)[SKR_KR],
+                                             int32_t ko_lane) {
 #pragma unroll
   for (int kk = 0; kk < SKR_KR; ++kk) {
     const int32_t ko = __shfl_sync(0xffffffffu, ko_lane, kk);
@@ -767,11 +815,11 @@ __device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJ
     if (a.c_bulk) fence_proxy_async_smem();
     __syncthreads();
     if (xs) {
-      skinny_copy_rows<SKR_THREADS>(a, os, plane, cw, cs[0], tx * S);
+      skinny_copy_rows<SKR_THREADS>(a, os, plane, cw, cs[0], tx * S, tid);
     } else {
       const int ix = a.bxn == 1 ? 0 : j.b % a.bxn;
       const int xn = a.ex - ix * tx < tx ? a.ex - ix * tx : tx;
-      skinny_copy_rows<SKR_THREADS>(a, os, plane, cw, cs[0], xn * S);
+      skinny_copy_rows<SKR_THREADS>(a, os, plane, cw, cs[0], xn * S, tid);
     }
     return;
   }
@@ -781,7 +829,7 @@ __device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJ
     os[r * SK_LDP + tid + SKR_THREADS] = acc[1][r];
   }
   __syncthreads();
-  skinny_store<SKR_THREADS>(a, os, cw, cs, 0, S);
+  skinny_store<SKR_THREADS>(a, os, cw, cs, 0, S, tid);
 }
 
 template <typename Resolve>
@@ -809,7 +857,8 @@ __device__ __forceinline__ void skinny_reg_loop(int j0, int jstep, int njobs, Re
     for (int r = 0; r < SKR_ROWS; ++r) acc[0][r] = acc[1][r] = 0.0f;
     float pc0[SKR_KR], pc1[SKR_KR];
     skinny_reg_q(a, kbeg, kend, Qs);
-    skinny_reg_p(a, kbeg, kend, po0, po1, pc0, pc1);
+    skinny_reg_p(a, kbeg, kend, po0, po1, pc0, pc1, skinny_reg_ko(a, kbeg, kend));
+    int32_t ko_next = skinny_reg_ko(a, kbeg + SKR_KR, kend);  // the next step's
     int st = 0;
 #pragma unroll 1
     for (int kb = kbeg; kb < kend; kb += SKR_KR) {
@@ -818,7 +867,8 @@ __device__ __forceinline__ void skinny_reg_loop(int j0, int jstep, int njobs, Re
       if (nb < kend) {
         __syncthreads();  // stage st ^ 1 was read by the previous step
         skinny_reg_q(a, nb, kend, Qs + (st ^ 1) * SKR_KR * SKR_ROWS);
-        skinny_reg_p(a, nb, kend, po0, po1, pn0, pn1);
+        skinny_reg_p(a, nb, kend, po0, po1, pn0, pn1, ko_next);
+        ko_next = skinny_reg_ko(a, nb + SKR_KR, kend);
         cp_async_wait<1>();
       } else {
         cp_async_wait<0>();
@@ -889,7 +939,7 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
     skinny_reduce_kernel(const __grid_constant__ SkinnyArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   grid_dep_wait();  // slices written by the kernel before
-  skinny_dispatch(a.rs, [&](auto r) { skinny_reduce_block<decltype(r)::value>(a, blockIdx.x, smem); });
+  skinny_reduce_dispatch(a.rs, [&](auto r) { skinny_reduce_block<decltype(r)::value>(a, blockIdx.x, smem); });
 }
 
 // Grouped launches. Contraction items: item i owns the global job indices
@@ -914,7 +964,7 @@ __global__ void __launch_bounds__(SK_THREADS, SK_CTAS_PER_SM)
   extern __shared__ __align__(16) uint8_t smem[];
   const int64_t t = blockIdx.x;
   const SkinnyItem& it = items[find_segment(begin, n, t)];
-  skinny_dispatch(it.args.rs, [&](auto r) {
+  skinny_reduce_dispatch(it.args.rs, [&](auto r) {
     skinny_reduce_block<decltype(r)::value>(it.args, (int)(t - it.begin), smem);
   });
 }

@@ -20,6 +20,7 @@
 #include "pack.cuh"
 #include "simt_gemm.cuh"
 #include "skinny_gett.cuh"
+#include "skinny_tc.cuh"
 #include "tc2_gemm.cuh"
 #include "tc_gemm.cuh"
 #include "transpose.cuh"
@@ -115,6 +116,11 @@ struct tccg_plan {
   // and slice pointers are filled in per run); s_is_n: the narrow side is N
   bool skinny = false, sk_s_is_n = false, sk_p_vec = false;
   bool sk_reg = false;  // the register path (narrow side <= 16 rows)
+  // the tensor-core skinny kernel (skinny_tc.cuh, split-BF16x3): MMA N = S
+  // rounded up to 16; Q packed K-major [hi | lo] per 32 k at off_q
+  bool sk_tc = false;
+  int32_t sk_spad = 0;
+  size_t off_q = 0;
   int32_t sk_ksplit = 1;
   SkinnyArgs sk{};
   // its 32-bit offset tables in one allocation: P and C offsets of the Y
@@ -430,6 +436,14 @@ static bool skinny_eligible(const tccg_plan* p) {
   return std::min(p->M, p->N) <= SK_SMAX && p->K <= INT32_MAX;
 }
 
+// The tensor-core skinny kernel: split-BF16x3, a narrow side of at most 64
+// (its MMA N and the epilogue's register sums), K whose packed Q columns
+// (2 x K rounded up to 32) stay TMA coordinates.
+static bool skinny_tc_eligible(const tccg_plan* p) {
+  return skinny_eligible(p) && p->prec == TCCG_PREC_BF16X3 && std::min(p->M, p->N) <= SKT_SMAX &&
+         p->K <= (int64_t(1) << 29);
+}
+
 static long long abs_ll(int64_t v) { return v < 0 ? -(long long)v : (long long)v; }
 
 // Smallest |stride| over modes of extent > 1 (LLONG_MAX when there is none).
@@ -442,8 +456,9 @@ static long long min_abs_stride(int n, const int64_t* ext, const int64_t* str) {
 
 // Geometry of the skinny kernel (SkinnyArgs without pointers) and the Y-space
 // mode list (W modes other than X, by increasing P stride). False when the
-// blocks would not fit one launch.
-static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
+// blocks would not fit one launch. tc: the tensor-core kernel's rows (one
+// pass of S rounded up to 16) and k slices (one CTA per SM).
+static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode, bool tc = false) {
   const tccg_desc& d = p->d;
   const bool sn = p->N <= p->M;  // narrow side: N (W = M, P = GA) or M (W = N, P = GB)
   p->sk_s_is_n = sn;
@@ -527,7 +542,12 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   // their P chunks come from L2). 64-row passes (16 rows per thread) need
   // more than the 128 registers two CTAs per SM leave a thread.
   const int64_t S = sn ? p->N : p->M;
-  if (S <= 48) {
+  p->sk_tc = tc;
+  p->sk_spad = (int32_t)round_up(S, 16);
+  if (tc) {
+    a.rs = p->sk_spad / 4;
+    a.npass = 1;
+  } else if (S <= 48) {
     a.rs = (int32_t)std::max<int64_t>(4, round_up(cdiv(S, 4), 4));
     a.npass = 1;
   } else {
@@ -543,10 +563,10 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode) {
   // a narrow side of at most 16 rows: P straight to registers (skinny_reg_kernel);
   // TCCG_B200_SKINNY_REG=0 keeps the shared-memory path
   const char* reg_env = std::getenv("TCCG_B200_SKINNY_REG");
-  p->sk_reg = a.rs == 4 && a.npass == 1 && !(reg_env && std::strcmp(reg_env, "0") == 0);
+  p->sk_reg = !tc && a.rs == 4 && a.npass == 1 && !(reg_env && std::strcmp(reg_env, "0") == 0);
   // k-split: (block, pass) jobs that cannot fill the persistent CTAs,
   // slices of >= 4 chunks
-  const int64_t per_sm = p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM;
+  const int64_t per_sm = tc ? 1 : p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM;
   a.chunks_per_split = (int32_t)choose_ksplit(p->tune.ksplit, (int64_t)a.nblk * a.npass, a.nchunks,
                                               per_sm * p->num_sms, 4, &p->sk_ksplit);
   a.ksplit = p->sk_ksplit;
@@ -617,6 +637,10 @@ static void with_skinny_rs(int rs, F&& f) {
 // tile kernels' models undercount the packing pass, which must transpose the
 // wide operand (0.9 TB/s measured where they assume 4.5), and the tcgen05
 // epilogue's short C runs (0.4-0.5 TB/s measured where it assumes 3).
+// Whether a skinny plan runs the tensor-core kernel (skinny_tc.cuh): asked
+// for with tuning.skinny = 2; automatically not yet.
+static bool choose_skinny_tc(const tccg_plan* p) { return p->tune.skinny == 2; }
+
 static bool choose_skinny(const tccg_plan* p) {
   if (p->tune.skinny > 0) return true;
   if (p->tune.skinny < 0) return false;
@@ -882,7 +906,18 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
                   "the skinny kernel needs FP32 operands, FP32 or BF16X3 precision, GETT, "
                   "min(M, N) <= 256 and tensors of fewer than 2^31 elements");
     }
+    if (p->tune.skinny == 2 && !skinny_tc_eligible(p)) {
+      plan_free(p);
+      return fail(TCCG_ERR_UNSUPPORTED,
+                  "the tensor-core skinny kernel needs split-BF16x3 precision, min(M, N) <= 64 "
+                  "and K <= 2^29");
+    }
     p->skinny = eligible && choose_skinny(p);
+    if (p->skinny && skinny_tc_eligible(p) && choose_skinny_tc(p) &&
+        !skinny_geometry(p, ym, &xmode, true)) {
+      plan_free(p);
+      return fail(TCCG_ERR_UNSUPPORTED, "the tensor-core skinny kernel's jobs do not fit one launch");
+    }
     if (p->skinny) {
       const bool sn = p->sk_s_is_n;
       int64_t ext[TCCG_MAX_MODES], sp[TCCG_MAX_MODES], scc[TCCG_MAX_MODES];
@@ -970,12 +1005,32 @@ static int plan_layout(tccg_plan* p) {
   const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
   if (p->skinny) {
     const SkinnyArgs& a = p->sk;
+    if (p->sk_tc) {  // packed Q: spad rows x Kc bf16 (K-major, [hi | lo] per 32 k)
+      p->Kc = 2 * round_up(p->K, 32);
+      p->off_q = 0;
+      ws = align_up((size_t)p->sk_spad * (size_t)p->Kc * 2, 256);
+    }
     if (p->sk_ksplit > 1) {  // FP32 slices [split][block][pass][row][position]
-      p->off_part = 0;
-      ws = align_up((size_t)p->sk_ksplit * (size_t)a.nblk * a.npass * 4 * a.rs * SK_BW * 4, 256);
+      p->off_part = ws;
+      ws = align_up(ws + (size_t)p->sk_ksplit * (size_t)a.nblk * a.npass * 4 * a.rs * SK_BW * 4, 256);
     }
     static const char* pw[] = {"x", "y", "k"};
     static const char* cw[] = {"xs", "xy", "sx"};
+    if (p->sk_tc) {
+      snprintf(p->describe, sizeof(p->describe),
+               "method=GETT prec=bf16x3 kernel=skinny_tc<BF16X3> M=%lld N=%lld K=%lld narrow=%s "
+               "S=%d n=%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
+               "grid=%lld load=%s%s store=%s%s%s pack=q",
+               (long long)p->M, (long long)p->N, (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S,
+               p->sk_spad, a.tx, a.ty, (long long)a.ex, (long long)a.ey, (long long)a.nblk,
+               a.nchunks, p->sk_ksplit, (long long)a.njobs,
+               (long long)std::min<int64_t>(a.njobs, p->num_sms), pw[a.p_walk],
+               p->sk_p_vec ? " x16B" : "", cw[a.c_walk],
+               a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "",
+               a.c_lin ? " linear" : "");
+      p->ws_bytes = ws;
+      return TCCG_OK;
+    }
     snprintf(p->describe, sizeof(p->describe),
              "method=GETT prec=%s kernel=skinny_gett<f32> M=%lld N=%lld K=%lld narrow=%s S=%d "
              "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
@@ -1289,6 +1344,10 @@ static cudaError_t set_attrs() {
     });
   chk(cudaFuncSetAttribute(skinny_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SK_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SKT_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_tc_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SKT_SMEM_BYTES));
   chk(cudaFuncSetAttribute(skinny_reg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SKR_SMEM_BYTES));
   chk(cudaFuncSetAttribute(skinny_reg_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1824,8 +1883,55 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
   return a;
 }
 
+// The tensor-core skinny kernel's Q: the narrow operand packed K-major into
+// the workspace (spad rows, the rows past S zeros) and its tensor map (box of
+// 32 k x spad rows, 128-byte swizzle).
+static PackOperand skinny_tc_q(const tccg_plan* p, const void* GA, const void* GB, char* w) {
+  const bool sn = p->sk_s_is_n;
+  return pack_op(sn ? GB : GA, sn ? p->t_b_n : p->t_a_m, sn ? p->t_b_k : p->t_a_k,
+                 sn ? p->N : p->M, p->K, p->sk_spad, round_up(p->K, 32), w + p->off_q, p->Kc,
+                 sn ? p->read_k_fast_b : p->read_k_fast_a);
+}
+
+static SkinnyTcArgs skinny_tc_args(const tccg_plan* p, const void* GA, const void* GB, float* C,
+                                   float alpha, float beta, char* w) {
+  SkinnyTcArgs t;
+  t.sk = skinny_args(p, GA, GB, C, alpha, beta, w);
+  t.sk.Q = nullptr;
+  t.spad = p->sk_spad;
+  t.chunk_kb = 16;  // the tile kernel's chunked accumulation (512 k per TMEM round)
+  return t;
+}
+
+static int run_skinny_tc(const tccg_plan* p, const void* GA, const void* GB, float* C, float alpha,
+                         float beta, char* w, cudaStream_t s) {
+  PackArgs pa;
+  memset(&pa, 0, sizeof(pa));
+  pa.op[0] = skinny_tc_q(p, GA, GB, w);
+  bool packed = false;
+  int rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s, &packed);
+  if (rc) return rc;
+  CUtensorMap tmQ;
+  rc = encode_kmajor(&tmQ, w + p->off_q, p->sk_spad, p->Kc, p->sk_spad);
+  if (rc) return rc;
+  const SkinnyTcArgs a = skinny_tc_args(p, GA, GB, C, alpha, beta, w);
+  mark(1, 0, s);
+  launch_after(packed, p, skinny_tc_kernel, dim3((unsigned)std::min<int64_t>(a.sk.njobs, p->num_sms)),
+               dim3(SKT_THREADS), SKT_SMEM_BYTES, s, tmQ, a, p->d_status);
+  rc = launch_check("skinny_tc");
+  mark(1, 1, s);
+  if (rc || p->sk_ksplit == 1) return rc;
+  mark(2, 0, s);
+  launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)a.sk.nblk), dim3(SK_THREADS),
+               SK_SMEM_BYTES, s, a.sk);
+  rc = launch_check("skinny_reduce");
+  mark(2, 1, s);
+  return rc;
+}
+
 static int run_skinny(const tccg_plan* p, const void* GA, const void* GB, float* C, float alpha,
                       float beta, char* w, cudaStream_t s) {
+  if (p->sk_tc) return run_skinny_tc(p, GA, GB, C, alpha, beta, w, s);
   const SkinnyArgs a = skinny_args(p, GA, GB, C, alpha, beta, w);
   mark(1, 0, s);
   if (p->sk_reg) {
@@ -2195,6 +2301,11 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     if (p->tune.method != TCCG_METHOD_GETT || p->tune.pair) {
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without the CTA-pair kernel (plan %d)", i);
+    }
+    if (p->sk_tc) {
+      group_free(g);
+      return fail(TCCG_ERR_UNSUPPORTED,
+                  "the tensor-core skinny kernel (tuning.skinny = 2) runs as a single plan only (plan %d)", i);
     }
     g->plans.push_back(p);
     if (p->skinny) {

@@ -169,6 +169,63 @@ def test_skinny_grouped_equals_per_item(cuda):
         assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= 1e-6, str(con)
 
 
+# the tensor-core kernel (tuning.skinny = 2): every case with a narrow side <= 64
+TC_CASES = [n for n in sorted(CASES) if n != "passes"]
+# long K over several TMEM rounds (ksplit=1: 38 chunks = rounds of 16, 16, 6),
+# and a narrow side of exactly 64
+TC_EXTRA = {
+    "rounds": ("ab", "akl", "lkb", dict(a=900, b=24, k=40, l=30), 1.0, 0.5),
+    "s64": ("sw", "sk", "kw", dict(s=64, w=1000, k=300), -1.0, 0.0),
+}
+
+
+def _tc_case(name):
+    if name in TC_EXTRA:
+        return TC_EXTRA[name]
+    return CASES[name][:6]
+
+
+@pytest.mark.parametrize("ksplit", [0, 1])
+@pytest.mark.parametrize("name", TC_CASES + sorted(TC_EXTRA))
+def test_skinny_tc_matches_oracle(cuda, name, ksplit):
+    """tcgen05 MMAs of the split-BF16x3 products (P converted in shared
+    memory, Q packed once, FP32 sums over TMEM rounds) at the BF16x3 bound."""
+    lc, la, lb, sizes, alpha, beta = _tc_case(name)
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, C = _data(ln, 41)
+    out, p = run_gpu(con, "bf16x3", A, B, C, tuning=Tuning(skinny=2, ksplit=ksplit))
+    d = p.describe()
+    assert "kernel=skinny_tc<BF16X3>" in d, d
+    if ksplit == 1:
+        assert "ksplit=1 " in d, d
+    ref = ln.run(A.astype(np.float64), B.astype(np.float64), C.astype(np.float64), alpha, beta)
+    assert error_metrics(out, ref)["normwise"] <= 1e-5, d
+
+
+def test_skinny_tc_is_deterministic_and_refuses(cuda):
+    """Repeated runs (k slices added in order) are bitwise equal; the kernel
+    serves split-BF16x3 with a narrow side of at most 64 only."""
+    from tccg_b200._native import TccgError
+    lc, la, lb, sizes, alpha, beta = _tc_case("rounds")
+    con = make_contraction(lc, la, lb, sizes, alpha, beta)
+    ln = LoopNest(lc, la, lb, sizes)
+    A, B, C = _data(ln, 43)
+    o1, p = run_gpu(con, "bf16x3", A, B, C, tuning=Tuning(skinny=2))
+    o2, _ = run_gpu(con, "bf16x3", A, B, C, tuning=Tuning(skinny=2))
+    assert np.array_equal(o1, o2)
+    assert "ksplit=1 " not in p.describe(), p.describe()
+    with pytest.raises(TccgError):
+        Plan(con, "fp32", tuning=Tuning(skinny=2))
+    wide = make_contraction(*CASES["passes"][:4])
+    with pytest.raises(TccgError):
+        Plan(wide, "bf16x3", tuning=Tuning(skinny=2))
+    # single plans only: a group refuses it
+    from tccg_b200.grouped import Group
+    with pytest.raises(TccgError):
+        Group([con], "bf16x3", tunings=[Tuning(skinny=2)])
+
+
 def test_skinny_choice_and_refusal(cuda):
     from tccg_b200._native import TccgError
     # item 69 of the 256-item batched workload (N = 40, K = 20, 5.0e6 positions, P
