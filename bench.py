@@ -757,8 +757,8 @@ def _kernel_mix(grp):
     mix = {}
     for p in grp.plans:
         d = p.describe()
-        k = ("skinny" if "skinny_gett" in d else "cuda_core" if "simt" in d else
-             "tcgen05_gather" if "gather" in d else "tcgen05_packed")
+        k = ("skinny" if "skinny_gett" in d else "skinny_tc" if "skinny_tc" in d else
+             "cuda_core" if "simt" in d else "tcgen05_gather" if "gather" in d else "tcgen05_packed")
         mix[k] = mix.get(k, 0) + 1
     return mix
 

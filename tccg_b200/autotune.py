@@ -181,8 +181,8 @@ def candidates(con: Contraction, precision: str, methods=("gett", "ttgt"), num_s
             tiles = [128] if precision == "bf16x3" else [192, 128]
             tl = 1 if len(loads) > 1 else 0
             more = [Tuning(method=method, load=tl, variant=chunks[0], tile_n=w) for w in tiles]
-            # the tensor-core skinny kernel (single plans only)
-            if method == "gett" and not grouped and skinny_tc_eligible(M, N, K, precision, dtype):
+            # the tensor-core skinny kernel forced on
+            if method == "gett" and skinny_tc_eligible(M, N, K, precision, dtype):
                 more.insert(0, Tuning(method=method, skinny=2))
             for ld in loads:
                 more += [Tuning(method=method, load=ld, raster=r) for r in (-8, 4, 16, -2)]

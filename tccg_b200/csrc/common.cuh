@@ -277,12 +277,6 @@ __device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* gsrc) 
                "n"(BYTES)
                : "memory");
 }
-// 4 zero bytes through the same asynchronous path (source size 0: nothing is
-// read from gsrc, which must still be a valid global address)
-__device__ __forceinline__ void cp_async_zero4(void* smem_dst, const void* gsrc) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, 0;" ::"r"(smem_u32(smem_dst)), "l"(gsrc)
-               : "memory");
-}
 // Arrive on `bar` once all of this thread's earlier cp.async copies landed
 // (the barrier's expected count includes this arrival).
 __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {

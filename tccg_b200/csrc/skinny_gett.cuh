@@ -197,16 +197,13 @@ __device__ __forceinline__ int32_t skinny_p_ko(const SkinnyArgs& a, int c) {
 // Issues the P copies of chunk c ([k][position], k < the chunk's extent) of
 // the box whose offsets pw holds (visible to all threads; positions outside
 // the tensor are zeros); ko = skinny_p_ko(a, c). Threads 0 .. SK_THREADS - 1
-// take part; no commit. ZFILL: the zeros go through cp.async too (a
-// barrier that counts the copies' completion then covers them).
-template <bool ZFILL = false>
+// take part; no commit. SKIP: positions outside the tensor are left
+// unwritten (the consumer substitutes zeros for them).
+template <bool SKIP = false>
 __device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float* ps,
                                                const int32_t* pw, int32_t ko) {
   auto zero = [&](float* d) {
-    if (ZFILL)
-      cp_async_zero4(d, a.P);
-    else
-      *d = 0.0f;
+    if (!SKIP) *d = 0.0f;
   };
   const int tid = threadIdx.x;
   const int kc = skinny_kc(a, c);

@@ -95,6 +95,14 @@ struct SktRef {
   int J;
 };
 
+// Whether box position w of block b is inside the tensor.
+__device__ __forceinline__ bool skt_inside(const SkinnyArgs& a, int b, int w) {
+  const int ix = a.bxn == 1 ? 0 : b % a.bxn, iy = a.bxn == 1 ? b : b / a.bxn;
+  const int xl = a.p_walk == SK_P_Y ? w / a.ty : w % a.tx;
+  const int yl = a.p_walk == SK_P_Y ? w % a.ty : w / a.tx;
+  return w < a.tx * a.ty && ix * a.tx + xl < a.ex && iy * a.ty + yl < a.ey;
+}
+
 // Box position w's P offset (loaders) / C offset (epilogue); SK_NONE outside.
 __device__ __forceinline__ int32_t skt_box(const SkinnyArgs& a, int b, int w, bool c) {
   const int ix = a.bxn == 1 ? 0 : b % a.bxn, iy = a.bxn == 1 ? b : b / a.bxn;
@@ -132,7 +140,8 @@ __device__ __forceinline__ bool skt_epi_and(bool v) {
 // Converts position w's column of a staging slot ([k][position], k < kc
 // valid) into row w % 128 of half w / 128 of an MMA stage: hi = bf16(x), lo
 // = bf16(x - hi), K-major [hi(32 k) | lo(32 k)], 16-byte chunk j stored at
-// chunk j ^ (row & 7) (TMA's 128-byte swizzle); k past kc are zeros.
+// chunk j ^ (row & 7) (TMA's 128-byte swizzle); k past kc, and every k of a
+// position outside the tensor (kc = 0: the copies skip it), are zeros.
 __device__ __forceinline__ void skt_convert(const float* slot, uint8_t* stA, int w, int kc) {
   // shared-window addresses: the accesses stay shared-memory loads / stores
   const uint32_t src = smem_u32(slot + w);
@@ -352,6 +361,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
     // ---------------- converters ----------------
     const int w = threadIdx.x - SKT_COPY_THREADS;  // the thread's box position
     int cg = j0, cc = 0, cc1 = 0;
+    bool inside = false;  // the position is inside the tensor (else the copies skip it)
     SktRef cr{};
     auto cseek = [&]() {
       if (cg < njobs) {
@@ -359,6 +369,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         const SkJob jb = skinny_job(cr.a->sk, cr.J);
         cc = jb.c0;
         cc1 = jb.c1;
+        inside = skt_inside(cr.a->sk, jb.b, w);
       }
     };
     cseek();
@@ -378,7 +389,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         break;
       }
       skt_convert(slots + slot * (SKT_SLOT / 4), sA + stage * SKT_A_STAGE, w,
-                  skinny_kc(cr.a->sk, cc));
+                  inside ? skinny_kc(cr.a->sk, cc) : 0);
       mbar_arrive(&sempty[slot]);
       fence_proxy_async_smem();  // the stage is read by the tensor cores (async proxy)
       mbar_arrive(&full[stage]);

@@ -569,6 +569,21 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode, bool
   const int64_t per_sm = tc ? 1 : p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM;
   a.chunks_per_split = (int32_t)choose_ksplit(p->tune.ksplit, (int64_t)a.nblk * a.npass, a.nchunks,
                                               per_sm * p->num_sms, 4, &p->sk_ksplit);
+  if (tc && p->tune.ksplit == 0) {
+    // one CTA per SM runs whole jobs: the split whose busiest CTA has the
+    // fewest chunks, each slice counted two chunks more (its partial sums
+    // written and read again), slices of >= 4 chunks
+    double best = 1e300;
+    for (int64_t s = 1; s <= std::max<int64_t>(1, std::min<int64_t>(2 * p->num_sms, a.nchunks / 4)); ++s) {
+      const int64_t per = cdiv(a.nchunks, s), ns = cdiv(a.nchunks, per);
+      const double cost = (double)cdiv((int64_t)a.nblk * ns, p->num_sms) * (double)(per + (ns > 1 ? 2 : 0));
+      if (cost < best) {
+        best = cost;
+        a.chunks_per_split = (int32_t)per;
+        p->sk_ksplit = (int32_t)ns;
+      }
+    }
+  }
   a.ksplit = p->sk_ksplit;
   const int64_t njobs = (int64_t)a.nblk * a.npass * a.ksplit;
   if (njobs > INT32_MAX) return false;
@@ -637,9 +652,23 @@ static void with_skinny_rs(int rs, F&& f) {
 // tile kernels' models undercount the packing pass, which must transpose the
 // wide operand (0.9 TB/s measured where they assume 4.5), and the tcgen05
 // epilogue's short C runs (0.4-0.5 TB/s measured where it assumes 3).
-// Whether a skinny plan runs the tensor-core kernel (skinny_tc.cuh): asked
-// for with tuning.skinny = 2; automatically not yet.
-static bool choose_skinny_tc(const tccg_plan* p) { return p->tune.skinny == 2; }
+// Whether a plan runs the tensor-core skinny kernel (skinny_tc.cuh): asked
+// for with tuning.skinny = 2, or -- unless the tuning asks for something
+// else -- K > 32 (two chunks or more) and at least 48 blocks of positions
+// (enough CTAs without a deep k-split). Measured on the 169 items of the
+// 256-item batched workload it can take (standalone, L2 flushed): on the 26
+// such items it takes 10.96 ms in sum where the other kernels' choice took
+// 12.10 ms; it loses where K <= 32 (C stores dominate: 4 epilogue warps) and
+// on a few blocks with a very long K (few CTAs, deep k-splits).
+static bool choose_skinny_tc(const tccg_plan* p) {
+  if (p->tune.skinny == 2) return true;
+  if (p->tune.skinny != 0) return false;
+  const tccg_tuning& t = p->tune;
+  if (t.variant != 0 || t.load != 0 || t.direct != 0 || t.shortk != 0 || t.simt_tile != 0 ||
+      t.tile_n != 0 || t.ksplit != 0)
+    return false;
+  return p->K > SK_KC && p->sk.nblk >= 48;
+}
 
 static bool choose_skinny(const tccg_plan* p) {
   if (p->tune.skinny > 0) return true;
@@ -912,9 +941,9 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
                   "the tensor-core skinny kernel needs split-BF16x3 precision, min(M, N) <= 64 "
                   "and K <= 2^29");
     }
-    p->skinny = eligible && choose_skinny(p);
-    if (p->skinny && skinny_tc_eligible(p) && choose_skinny_tc(p) &&
-        !skinny_geometry(p, ym, &xmode, true)) {
+    const bool use_tc = eligible && skinny_tc_eligible(p) && choose_skinny_tc(p);
+    p->skinny = use_tc || (eligible && choose_skinny(p));
+    if (use_tc && !skinny_geometry(p, ym, &xmode, true)) {
       plan_free(p);
       return fail(TCCG_ERR_UNSUPPORTED, "the tensor-core skinny kernel's jobs do not fit one launch");
     }
@@ -2233,13 +2262,19 @@ struct tccg_group {
   // skinny lane (FP32 operands): the items' contractions and the k-split
   // reductions of those that split
   SkinnyItem* d_sk = nullptr;
-  SkinnyItem* d_skr = nullptr;
+  SkinnyItem* d_skr = nullptr;  // reductions of both skinny lanes
   int32_t n_sk = 0;
+  // tensor-core skinny lane (split-BF16x3): items with Q's tensor maps; Q's
+  // packs join the tensor-core lane's pack jobs
+  SkinnyTcItem* d_sktc = nullptr;
+  int32_t n_sktc = 0;
+  int32_t* sktc_status = nullptr;
   // compact first-CTA / first-tile arrays of the jobs and items above (one
   // allocation): what the kernels binary-search instead of the large structs
   int64_t* d_begin = nullptr;
   int64_t *b_simt_jobs = nullptr, *b_tc_jobs = nullptr, *b_simt_items = nullptr,
-          *b_tc_items = nullptr, *b_reduce = nullptr, *b_sk = nullptr, *b_skr = nullptr;
+          *b_tc_items = nullptr, *b_reduce = nullptr, *b_sk = nullptr, *b_skr = nullptr,
+          *b_sktc = nullptr;
   // Waves: the items run in sets whose workspaces together stay within
   // kGroupWaveBytes (an item above it is a set of its own). Each wave is
   // packed and multiplied before the next one reuses the same workspace
@@ -2262,6 +2297,9 @@ struct tccg_group {
     int32_t sk0[3] = {}, nsk[3] = {}, skr0 = 0, nskr = 0;
     int64_t sk_jobs[3] = {}, skr_ctas = 0;
     bool sk_reg[3] = {};  // the lane runs the register path
+    // the tensor-core skinny lane: items [sktc0, sktc0 + nsktc) of d_sktc
+    int32_t sktc0 = 0, nsktc = 0;
+    int64_t sktc_jobs = 0;
   };
   std::vector<Wave> waves;
   bool bound = false;
@@ -2275,7 +2313,7 @@ static constexpr size_t kGroupWaveBytes = size_t(TCCG_GROUP_WAVE_MB) << 20;
 static void group_free(tccg_group* g) {
   if (!g) return;
   void* ps[] = {g->d_simt, g->d_simt_jobs, g->d_tc, g->d_tc_jobs, g->d_reduce, g->d_begin,
-                g->d_sk, g->d_skr};
+                g->d_sk, g->d_skr, g->d_sktc};
   for (void* q : ps)
     if (q) cudaFree(q);
   delete g;
@@ -2302,13 +2340,11 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
       group_free(g);
       return fail(TCCG_ERR_UNSUPPORTED, "grouped plans must be GETT without the CTA-pair kernel (plan %d)", i);
     }
-    if (p->sk_tc) {
-      group_free(g);
-      return fail(TCCG_ERR_UNSUPPORTED,
-                  "the tensor-core skinny kernel (tuning.skinny = 2) runs as a single plan only (plan %d)", i);
-    }
     g->plans.push_back(p);
-    if (p->skinny) {
+    if (p->sk_tc) {
+      if (!g->sktc_status) g->sktc_status = p->d_status;
+      ++g->n_sktc;
+    } else if (p->skinny) {
       ++g->n_sk;
     } else if (simt_path(p)) {
       ++g->n_simt;
@@ -2336,14 +2372,16 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     g->ws_off[i] = ws;
     ws += need;
     g->ws_bytes = std::max(g->ws_bytes, ws);
-    if (p->skinny) {
+    if (p->sk_tc) {
+      wv.sktc_jobs += p->sk.njobs;
+    } else if (p->skinny) {
       wv.sk_jobs[p->sk.rs / 4 - 1] += p->sk.njobs;
     } else if (simt_path(p)) {
       wv.simt_tiles += (p->Mp / p->simt_bm) * (p->Np / p->simt_bn) * p->ksplit;
     } else {
       wv.lane_tiles[p->tcv] += (int64_t)p->tiles_m * p->tiles_n * p->ksplit;
     }
-    bool too_many = wv.simt_tiles > INT32_MAX;
+    bool too_many = wv.simt_tiles > INT32_MAX || wv.sktc_jobs > INT32_MAX;
     for (int c = 0; c < 3; ++c) too_many |= wv.sk_jobs[c] > INT32_MAX;
     for (int v = 0; v < TCV_COUNT; ++v) too_many |= wv.lane_tiles[v] > INT32_MAX;
     if (too_many) {
@@ -2357,25 +2395,28 @@ extern "C" int tccg_group_create(const tccg_plan* const* plans, int32_t count, t
     e = cudaMalloc(&g->d_simt, simt_item * g->n_simt);
     if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_simt_jobs, sizeof(PackJob) * 2 * g->n_simt);
   }
-  if (e == cudaSuccess && g->n_tc) {
-    e = cudaMalloc((void**)&g->d_tc, sizeof(TcGroupItem) * g->n_tc);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_tc_jobs, sizeof(PackJob) * 2 * g->n_tc);
-  }
-  if (e == cudaSuccess && g->n_sk) {
-    e = cudaMalloc((void**)&g->d_sk, sizeof(SkinnyItem) * g->n_sk);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_skr, sizeof(SkinnyItem) * g->n_sk);
-  }
+  // tensor-core pack jobs: two per tile item, Q's one per tensor-core skinny item
+  const int32_t n_tcj = 2 * g->n_tc + g->n_sktc;
+  if (e == cudaSuccess && n_tcj) e = cudaMalloc((void**)&g->d_tc_jobs, sizeof(PackJob) * n_tcj);
+  if (e == cudaSuccess && g->n_tc) e = cudaMalloc((void**)&g->d_tc, sizeof(TcGroupItem) * g->n_tc);
+  if (e == cudaSuccess && g->n_sk) e = cudaMalloc((void**)&g->d_sk, sizeof(SkinnyItem) * g->n_sk);
+  if (e == cudaSuccess && g->n_sktc)
+    e = cudaMalloc((void**)&g->d_sktc, sizeof(SkinnyTcItem) * g->n_sktc);
+  if (e == cudaSuccess && g->n_sk + g->n_sktc)
+    e = cudaMalloc((void**)&g->d_skr, sizeof(SkinnyItem) * (g->n_sk + g->n_sktc));
   if (e == cudaSuccess) e = cudaMalloc(&g->d_reduce, sizeof(ReduceJob<double>) * count);
-  if (e == cudaSuccess)
-    e = cudaMalloc((void**)&g->d_begin, sizeof(int64_t) * (4 * (size_t)count + 2 * g->n_sk));
+  const size_t nbegin = 2 * (size_t)g->n_simt + n_tcj + g->n_simt + g->n_tc + count + g->n_sk +
+                        (g->n_sk + g->n_sktc) + g->n_sktc;
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_begin, sizeof(int64_t) * nbegin);
   if (e == cudaSuccess) {
     g->b_simt_jobs = g->d_begin;
     g->b_tc_jobs = g->b_simt_jobs + 2 * g->n_simt;
-    g->b_simt_items = g->b_tc_jobs + 2 * g->n_tc;
+    g->b_simt_items = g->b_tc_jobs + n_tcj;
     g->b_tc_items = g->b_simt_items + g->n_simt;
     g->b_reduce = g->b_tc_items + g->n_tc;
     g->b_sk = g->b_reduce + count;
     g->b_skr = g->b_sk + g->n_sk;
+    g->b_sktc = g->b_skr + g->n_sk + g->n_sktc;
   }
   if (e != cudaSuccess) {
     group_free(g);
@@ -2602,7 +2643,8 @@ static void bind_skinny(tccg_group* g, tccg_group::Wave& wv, const void* const* 
     wv.sk0[cls] = (int32_t)items.size();
     std::vector<size_t> idx;
     for (size_t i : wv.items)
-      if (g->plans[i]->skinny && g->plans[i]->sk.rs / 4 - 1 == cls) idx.push_back(i);
+      if (g->plans[i]->skinny && !g->plans[i]->sk_tc && g->plans[i]->sk.rs / 4 - 1 == cls)
+        idx.push_back(i);
     std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
       return g->plans[a]->sk.chunks_per_split > g->plans[b]->sk.chunks_per_split;
     });
@@ -2633,6 +2675,60 @@ static void bind_skinny(tccg_group* g, tccg_group::Wave& wv, const void* const* 
   wv.skr_ctas = rctas;
 }
 
+// The tensor-core skinny lane of one wave: its items (Q's tensor map on the
+// item's workspace, longest k slices first), Q's pack jobs appended to the
+// tensor-core lane's (the same packing launch) and the k-split reductions
+// next to the CUDA-core skinny lane's.
+static int bind_sktc(tccg_group* g, tccg_group::Wave& wv, const void* const* A,
+                     const void* const* B, void* const* C, const double* alpha,
+                     const double* beta, char* ws, std::vector<SkinnyTcItem>& items,
+                     std::vector<PackJob>& jobs, std::vector<SkinnyItem>& red) {
+  wv.sktc0 = (int32_t)items.size();
+  std::vector<size_t> idx;
+  for (size_t i : wv.items)
+    if (g->plans[i]->sk_tc) idx.push_back(i);
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+    return g->plans[a]->sk.chunks_per_split > g->plans[b]->sk.chunks_per_split;
+  });
+  int64_t jobs_n = 0, pctas = wv.tc_pack_ctas, rctas = wv.skr_ctas;
+  for (size_t i : idx) {
+    const tccg_plan* p = g->plans[i];
+    char* w = ws + g->ws_off[i];
+    const void* GA = p->d.swap_ab ? B[i] : A[i];
+    const void* GB = p->d.swap_ab ? A[i] : B[i];
+    SkinnyTcItem it;
+    memset(&it, 0, sizeof(it));
+    int rc = encode_kmajor(&it.tmQ, w + p->off_q, p->sk_spad, p->Kc, p->sk_spad);
+    if (rc) return rc;
+    it.args = skinny_tc_args(p, GA, GB, static_cast<float*>(C[i]), (float)alpha[i], (float)beta[i], w);
+    it.begin = jobs_n;
+    jobs_n += p->sk.njobs;
+    items.push_back(it);
+    PackJob jb;
+    jb.op = skinny_tc_q(p, GA, GB, w);
+    pack_geometry(jb.op, pack_k_tile<PACK_K_BF16>());
+    jb.begin = pctas;
+    pctas += jb.op.tiles;
+    jobs.push_back(jb);
+    if (p->sk_ksplit > 1) {
+      SkinnyItem r;
+      memset(&r, 0, sizeof(r));
+      r.args = it.args.sk;
+      r.begin = rctas;
+      rctas += (int64_t)p->sk.nblk * p->sk.npass;
+      red.push_back(r);
+    }
+  }
+  if (pctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped packing grid too large");
+  wv.nsktc = (int32_t)items.size() - wv.sktc0;
+  wv.sktc_jobs = jobs_n;
+  wv.ntcj = (int32_t)jobs.size() - wv.tcj0;
+  wv.tc_pack_ctas = pctas;
+  wv.nskr = (int32_t)red.size() - wv.skr0;
+  wv.skr_ctas = rctas;
+  return TCCG_OK;
+}
+
 extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* const* B,
                                void* const* C, const double* alpha, const double* beta, void* ws,
                                size_t ws_bytes) {
@@ -2652,6 +2748,7 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     std::vector<PackJob> sjobs, tjobs;
     std::vector<TcGroupItem> titems;
     std::vector<SkinnyItem> kitems, kred;
+    std::vector<SkinnyTcItem> ktc;
     int r = TCCG_OK;
     for (tccg_group::Wave& wv : g->waves) {
       int64_t rctas = 0;
@@ -2662,6 +2759,8 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
         r = bind_tc(g, wv, A, B, C, alpha, beta, w, titems, tjobs, red, rctas);
         if (r) return r;
         bind_skinny(g, wv, A, B, C, alpha, beta, w, kitems, kred);
+        r = bind_sktc(g, wv, A, B, C, alpha, beta, w, ktc, tjobs, kred);
+        if (r) return r;
       }
       if (rctas > INT32_MAX) return fail(TCCG_ERR_UNSUPPORTED, "grouped reduction grid too large");
       wv.n_red = (int32_t)red.size() - wv.red0;
@@ -2673,12 +2772,12 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
       CUDA_TRY(cudaMemcpy(g->d_simt_jobs, sjobs.data(), sizeof(PackJob) * sjobs.size(),
                           cudaMemcpyHostToDevice));
     }
-    if (!titems.empty()) {
+    if (!titems.empty())
       CUDA_TRY(cudaMemcpy(g->d_tc, titems.data(), sizeof(TcGroupItem) * titems.size(),
                           cudaMemcpyHostToDevice));
+    if (!tjobs.empty())
       CUDA_TRY(cudaMemcpy(g->d_tc_jobs, tjobs.data(), sizeof(PackJob) * tjobs.size(),
                           cudaMemcpyHostToDevice));
-    }
     if (!red.empty())
       CUDA_TRY(cudaMemcpy(g->d_reduce, red.data(), sizeof(red[0]) * red.size(), cudaMemcpyHostToDevice));
     if (!kitems.empty())
@@ -2686,6 +2785,9 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
                           cudaMemcpyHostToDevice));
     if (!kred.empty())
       CUDA_TRY(cudaMemcpy(g->d_skr, kred.data(), sizeof(SkinnyItem) * kred.size(),
+                          cudaMemcpyHostToDevice));
+    if (!ktc.empty())
+      CUDA_TRY(cudaMemcpy(g->d_sktc, ktc.data(), sizeof(SkinnyTcItem) * ktc.size(),
                           cudaMemcpyHostToDevice));
     auto item_begin = [](const auto& x) { return x.tile_begin; };
     auto job_begin = [](const auto& x) { return x.begin; };
@@ -2696,6 +2798,7 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
     if (!r) r = upload_begins(red, job_begin, g->b_reduce);
     if (!r) r = upload_begins(kitems, job_begin, g->b_sk);
     if (!r) r = upload_begins(kred, job_begin, g->b_skr);
+    if (!r) r = upload_begins(ktc, job_begin, g->b_sktc);
     return r;
   };
   if (g->prec == TCCG_PREC_FP64) {
@@ -2784,6 +2887,12 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
         });
       }
       if ((rc = launch_check("skinny_group"))) return rc;
+    }
+    if (wv.nsktc > 0) {
+      const unsigned grid = (unsigned)std::min<int64_t>(wv.sktc_jobs, g->num_sms);
+      skinny_tc_group_kernel<<<grid, SKT_THREADS, SKT_SMEM_BYTES, s>>>(
+          g->d_sktc + wv.sktc0, g->b_sktc + wv.sktc0, wv.nsktc, (int)wv.sktc_jobs, g->sktc_status);
+      if ((rc = launch_check("skinny_tc_group"))) return rc;
     }
     if (wv.nskr > 0) {
       skinny_reduce_group_kernel<<<(unsigned)wv.skr_ctas, SK_THREADS, SK_SMEM_BYTES, s>>>(

@@ -220,10 +220,42 @@ def test_skinny_tc_is_deterministic_and_refuses(cuda):
     wide = make_contraction(*CASES["passes"][:4])
     with pytest.raises(TccgError):
         Plan(wide, "bf16x3", tuning=Tuning(skinny=2))
-    # single plans only: a group refuses it
+
+
+def test_skinny_tc_grouped_equals_per_item(cuda):
+    """A grouped run with tensor-core skinny items (Q packs next to the tile
+    items' packs, k-split items reduced with the CUDA-core skinny items')
+    equals the per-item runs bit for bit, within the BF16x3 bound."""
+    import torch
     from tccg_b200.grouped import Group
-    with pytest.raises(TccgError):
-        Group([con], "bf16x3", tunings=[Tuning(skinny=2)])
+    names = ["transpose", "matvec_split", "kfast", "xy", "passes_split"]
+    items = [make_contraction(*_tc_case(n)[:4], 1.0, 0.0) for n in names + sorted(TC_EXTRA)]
+    items.append(make_contraction(*CASES["passes"][:4], 1.0, 0.0))  # CUDA-core skinny
+    items.append(make_contraction("mn", "mk", "kn", dict(m=700, n=500, k=300), 1.0, 0.0))
+    tc = len(items) - 2
+    tunings = [Tuning(skinny=2)] * tc + [Tuning(skinny=1), Tuning(variant=16)]
+    g = torch.Generator(device="cuda").manual_seed(7)
+    As = [torch.randn(c.A0.num_elements(), generator=g, device="cuda") for c in items]
+    Bs = [torch.randn(c.B0.num_elements(), generator=g, device="cuda") for c in items]
+    Cs = [torch.zeros(c.C0.num_elements(), device="cuda") for c in items]
+    grp = Group(items, "bf16x3", tunings=tunings)
+    assert sum("skinny_tc" in p.describe() for p in grp.plans) == tc
+    grp.bind(As, Bs, Cs)
+    grp.capture()
+    grp.replay()
+    torch.cuda.synchronize()
+    grouped = [c.clone() for c in Cs]
+    for c in Cs:
+        c.zero_()
+    grp.run_per_item()
+    torch.cuda.synchronize()
+    for a, b in zip(grouped, Cs):
+        assert torch.equal(a, b)
+    for con, A, B, C in zip(items[:tc], As, Bs, grouped):
+        ln = LoopNest(con.C0.labels, con.A0.labels, con.B0.labels,
+                      {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices})
+        ref = ln.run(A.double().cpu().numpy(), B.double().cpu().numpy(), np.zeros(ln.size_c), 1.0, 0.0)
+        assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= 1e-5, str(con)
 
 
 def test_skinny_choice_and_refusal(cuda):
