@@ -23,11 +23,13 @@
 //               (tcgen05.mma kind::f16, M = 128, N = S rounded up to 16)
 //               into a TMEM accumulator; a job's chunks go into TMEM rounds
 //               of chunk_kb chunks, two accumulators alternating;
-//   warps 17-20 (128 threads, thread = TMEM lane, both halves) add each
-//               round into the job's running sums, kept in TMEM (RN adds:
-//               the tile kernel's chunked accumulation), then store the C
-//               block by the skinny kernel's store walks or linear copies,
-//               or its raw sums to the job's k slice.
+//   warps 17-24 (256 threads, thread = position = TMEM lane of its half)
+//               add each round into the job's running sums, kept in TMEM
+//               (RN adds: the tile kernel's chunked accumulation), then
+//               store the C block by the skinny kernel's store walks or
+//               linear copies, or its raw sums to the job's k slice (four
+//               warps, each thread both halves, measured 1.2-1.4x slower on
+//               items whose C stores dominate).
 //
 // Copies, conversion and MMAs run in separate warps: with one set of warps
 // issuing a chunk's copies, its Q load and its conversion in turn, a chunk
@@ -35,8 +37,8 @@
 // alone streams at 4.9-6.6 TB/s).
 //
 // One CTA per SM (214 KB of shared memory: three 33 KB staging slots, two
-// 40 KB MMA stages, the 33 KB epilogue staging and the offset tables); TMEM
-// 512 columns. Every wait is bounded (TCCG_DEVICE_WAIT_NS): a wait that
+// 40 KB MMA stages, the 33 KB epilogue staging and the offset tables; 25
+// warps); TMEM 512 columns. Every wait is bounded (TCCG_DEVICE_WAIT_NS): a wait that
 // runs out records a status code and the CTA winds down.
 #pragma once
 
@@ -51,8 +53,8 @@ constexpr int SKT_CONV_WARP0 = SKT_COPY_THREADS / 32;    // 8
 constexpr int SKT_CONV_THREADS = SK_BW;                  // 256, warps 8-15
 constexpr int SKT_MMA_WARP = SKT_CONV_WARP0 + SKT_CONV_THREADS / 32;  // 16
 constexpr int SKT_EPI_WARP0 = SKT_MMA_WARP + 1;          // 17
-constexpr int SKT_EPI_THREADS = 128;  // one TMEM lane each, both halves
-constexpr int SKT_THREADS = SKT_COPY_THREADS + SKT_CONV_THREADS + 32 + SKT_EPI_THREADS;  // 672
+constexpr int SKT_EPI_THREADS = SK_BW;  // one position each: TMEM lane of its half
+constexpr int SKT_THREADS = SKT_COPY_THREADS + SKT_CONV_THREADS + 32 + SKT_EPI_THREADS;  // 800
 constexpr int SKT_SMAX = 64;   // largest narrow extent
 constexpr int SKT_HALF = 128;  // MMA rows: positions per half box
 constexpr int SKT_SLOTS = 3;   // FP32 staging ring
@@ -167,24 +169,23 @@ __device__ __forceinline__ void skt_convert(const float* slot, uint8_t* stA, int
   }
 }
 
-// The end of job j in the epilogue, its sums in TMEM (tsum(h, g): columns
-// g * 16 .. + 15 of half h in this warp's lane quarter): raw sums to its k
-// slice, or the C block (staged in os, then the skinny kernel's store walks
-// or linear copies). Thread etid (0..127) holds positions w0 and w0 + 128.
+// The end of job j in the epilogue, its sums in TMEM (tsum(g): columns g *
+// 16 .. + 15 of the thread's half in its warp's lane quarter): raw sums to
+// its k slice, or the C block (staged in os, then the skinny kernel's store
+// walks or linear copies). Thread etid (0..255) holds position w.
 template <typename TSum>
 __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, int spad,
                                            TSum&& tsum, float* os, int32_t* cw, int32_t* cs,
-                                           int w0, int etid) {
+                                           int w, int etid) {
   const int S = a.S;
   if (a.partial) {  // the skinny layout with one pass of spad (= 4 rs) rows
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      float* dst = a.partial + ((size_t)j.z * a.nblk + j.b) * (size_t)spad * SK_BW + w0 + h * SKT_HALF;
+    {
+      float* dst = a.partial + ((size_t)j.z * a.nblk + j.b) * (size_t)spad * SK_BW + w;
 #pragma unroll
       for (int g = 0; g < SKT_SMAX / 16; ++g) {
         if (g * 16 < S) {  // warp-uniform
           uint32_t v[16];
-          tmem_ld_32x32b_x16(tsum(h, g), v);
+          tmem_ld_32x32b_x16(tsum(g), v);
           tmem_ld_wait();
 #pragma unroll
           for (int i = 0; i < 16; ++i)
@@ -195,8 +196,7 @@ __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, 
     return;
   }
   skt_epi_sync();  // the previous job's stores are done with os, cw, cs
-  cw[w0] = skt_box(a, j.b, w0, true);
-  cw[w0 + SKT_HALF] = skt_box(a, j.b, w0 + SKT_HALF, true);
+  cw[w] = skt_box(a, j.b, w, true);
   if (etid < S) cs[etid] = __ldg(a.c_s_off + etid);
   const bool py = a.p_walk == SK_P_Y;
   const int tx = a.tx, ty = a.ty;
@@ -222,9 +222,7 @@ __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, 
     if (hh < S && (hh == 0 || a.c_lin != SK_CLIN_SX)) {
       const int ns = a.c_lin == SK_CLIN_SX ? S : (S - hh < SK_SUB ? S - hh : SK_SUB);
       skt_epi_sync();  // the staging's last reader is done
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int w = w0 + h * SKT_HALF;
+      {
         int rstep;
         const int o = base(w, rstep);
         const bool in = a.c_lin == SK_CLIN_NONE || w < tx * ty;
@@ -232,7 +230,7 @@ __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, 
         for (int g = 0; g < SK_SUB / 16; ++g) {
           if (g * 16 < ns) {  // warp-uniform
             uint32_t v[16];
-            tmem_ld_32x32b_x16(tsum(h, hh / 16 + g), v);
+            tmem_ld_32x32b_x16(tsum(hh / 16 + g), v);
             tmem_ld_wait();
 #pragma unroll
             for (int i = 0; i < 16; ++i)
@@ -476,11 +474,12 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
     __syncwarp();
   } else {
     // ---------------- epilogue ----------------
-    const int etid = threadIdx.x - SKT_EPI_WARP0 * 32;  // 0..127
-    const int q = warp & 3;  // TMEM lanes [32 q, 32 q + 32) are this warp's
-    const int w0 = q * 32 + lane;  // positions w0 (half 0) and w0 + 128 (half 1)
+    const int etid = threadIdx.x - SKT_EPI_WARP0 * 32;  // 0..255
+    const int q = warp & 3;       // TMEM lanes [32 q, 32 q + 32) are this warp's
+    const int h = etid >> 7;      // its half box
+    const int w = h * SKT_HALF + q * 32 + lane;  // the thread's position
     const uint32_t tq = tbase + ((uint32_t)(q * 32) << 16);
-    auto tsum = [&](int h, int g) { return tq + (uint32_t)(SKT_SUMCOL + h * SKT_SMAX + g * 16); };
+    auto tsum = [&](int g) { return tq + (uint32_t)(SKT_SUMCOL + h * SKT_SMAX + g * 16); };
     int acc = 0;
     uint32_t acc_phase = 0;
     for (int jg = j0; jg < njobs; jg += js) {
@@ -499,24 +498,21 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         tc_fence_after();
         // running sums (TMEM) = round 0, then + each round (RN adds)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int g = 0; g < SKT_SMAX / 16; ++g) {
+          if (g * 16 < spad) {  // warp-uniform
+            uint32_t v[16];
+            tmem_ld_32x32b_x16(tq + (uint32_t)(acc * 2 * SKT_SMAX + h * SKT_SMAX + g * 16), v);
+            if (rd > 0) {
+              uint32_t u[16];
+              tmem_ld_32x32b_x16(tsum(g), u);
+              tmem_ld_wait();
 #pragma unroll
-          for (int g = 0; g < SKT_SMAX / 16; ++g) {
-            if (g * 16 < spad) {  // warp-uniform
-              uint32_t v[16];
-              tmem_ld_32x32b_x16(tq + (uint32_t)(acc * 2 * SKT_SMAX + h * SKT_SMAX + g * 16), v);
-              if (rd > 0) {
-                uint32_t u[16];
-                tmem_ld_32x32b_x16(tsum(h, g), u);
-                tmem_ld_wait();
-#pragma unroll
-                for (int i = 0; i < 16; ++i)
-                  v[i] = __float_as_uint(__fadd_rn(__uint_as_float(u[i]), __uint_as_float(v[i])));
-              } else {
-                tmem_ld_wait();
-              }
-              tmem_st_32x32b_x16(tsum(h, g), v);
+              for (int i = 0; i < 16; ++i)
+                v[i] = __float_as_uint(__fadd_rn(__uint_as_float(u[i]), __uint_as_float(v[i])));
+            } else {
+              tmem_ld_wait();
             }
+            tmem_st_32x32b_x16(tsum(g), v);
           }
         }
         tmem_st_wait();
@@ -529,7 +525,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         }
       }
       if (!skt_epi_and(ok)) break;  // every epilogue thread takes the same branch
-      skt_finish(a, jb, spad, tsum, os, cw, cs, w0, etid);
+      skt_finish(a, jb, spad, tsum, os, cw, cs, w, etid);
     }
     bulk_wait_all();  // bulk C copies complete before the CTA exits
   }
