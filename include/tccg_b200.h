@@ -132,7 +132,7 @@ typedef struct tccg_tuning {
                           the narrow operand in shared memory, the wide one streamed once in
                           place, C written once. 0 = chosen by the model, 1 = always (an
                           error where it does not apply), -1 = never; 2 = its tensor-core
-                          form (BF16X3, min(M, N) <= 64, K <= 2^29: the wide operand split
+                          form (BF16X3, K <= 2^29, passes of 64 rows: the wide operand split
                           into bf16 hi / lo on the fly, tcgen05 MMAs; 0 picks it for K > 32
                           and at least 48 blocks of positions) */
 } tccg_tuning;

@@ -223,9 +223,9 @@ def skinny_eligible(M: int, N: int, K: int, precision: str, dtype: str = "f32") 
 
 def skinny_tc_eligible(M: int, N: int, K: int, precision: str, dtype: str = "f32") -> bool:
     """Whether the tensor-core skinny kernel (tuning.skinny = 2) can run a GETT
-    of these extents: split-BF16x3 with FP32 operands, min(M, N) <= 64,
+    of these extents: split-BF16x3 with FP32 operands, min(M, N) <= 256,
     K <= 2^29 (the C ABI's rule)."""
-    return dtype == "f32" and precision == "bf16x3" and min(M, N) <= 64 and K <= (1 << 29)
+    return dtype == "f32" and precision == "bf16x3" and min(M, N) <= 256 and K <= (1 << 29)
 
 
 def _flush_l2(buf):

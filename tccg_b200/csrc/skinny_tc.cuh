@@ -55,7 +55,7 @@ constexpr int SKT_MMA_WARP = SKT_CONV_WARP0 + SKT_CONV_THREADS / 32;  // 16
 constexpr int SKT_EPI_WARP0 = SKT_MMA_WARP + 1;          // 17
 constexpr int SKT_EPI_THREADS = SK_BW;  // one position each: TMEM lane of its half
 constexpr int SKT_THREADS = SKT_COPY_THREADS + SKT_CONV_THREADS + 32 + SKT_EPI_THREADS;  // 800
-constexpr int SKT_SMAX = 64;   // largest narrow extent
+constexpr int SKT_SMAX = 64;   // rows per pass (a narrow side above 64 runs passes of 64)
 constexpr int SKT_HALF = 128;  // MMA rows: positions per half box
 constexpr int SKT_SLOTS = 3;   // FP32 staging ring
 constexpr int SKT_STAGES = 2;  // MMA operand stages
@@ -78,8 +78,8 @@ static_assert(SKT_SMEM_BYTES <= 227 * 1024, "one CTA per SM");
 static_assert(SKT_OFF_B % 1024 == 0 && SKT_B_STAGE % 1024 == 0, "swizzled stages 1024-byte aligned");
 
 struct SkinnyTcArgs {
-  SkinnyArgs sk;     // P, C, tables, boxes, jobs (rs = spad / 4, npass = 1); Q unused
-  int32_t spad;      // MMA N: S rounded up to 16
+  SkinnyArgs sk;     // P, C, tables, boxes, jobs (rs = spad / 4); Q unused
+  int32_t spad;      // MMA N = rows per pass: S rounded up to 16, or 64 (S > 64, passes)
   int32_t chunk_kb;  // chunks accumulated per TMEM round
 };
 
@@ -171,16 +171,18 @@ __device__ __forceinline__ void skt_convert(const float* slot, uint8_t* stA, int
 
 // The end of job j in the epilogue, its sums in TMEM (tsum(g): columns g *
 // 16 .. + 15 of the thread's half in its warp's lane quarter): raw sums to
-// its k slice, or the C block (staged in os, then the skinny kernel's store
-// walks or linear copies). Thread etid (0..255) holds position w.
+// its k slice, or the C block of its pass's rows (staged in os, then the
+// skinny kernel's store walks or linear copies). Thread etid (0..255) holds
+// position w.
 template <typename TSum>
 __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, int spad,
                                            TSum&& tsum, float* os, int32_t* cw, int32_t* cs,
                                            int w, int etid) {
-  const int S = a.S;
-  if (a.partial) {  // the skinny layout with one pass of spad (= 4 rs) rows
+  const int r0 = j.p * spad;  // the pass's first row
+  const int S = a.S - r0 < spad ? a.S - r0 : spad;  // rows of this pass
+  if (a.partial) {  // the skinny layout, passes of spad (= 4 rs) rows
     {
-      float* dst = a.partial + ((size_t)j.z * a.nblk + j.b) * (size_t)spad * SK_BW + w;
+      float* dst = a.partial + (((size_t)j.z * a.nblk + j.b) * a.npass + j.p) * (size_t)spad * SK_BW + w;
 #pragma unroll
       for (int g = 0; g < SKT_SMAX / 16; ++g) {
         if (g * 16 < S) {  // warp-uniform
@@ -197,7 +199,7 @@ __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, 
   }
   skt_epi_sync();  // the previous job's stores are done with os, cw, cs
   cw[w] = skt_box(a, j.b, w, true);
-  if (etid < S) cs[etid] = __ldg(a.c_s_off + etid);
+  if (etid < S) cs[etid] = __ldg(a.c_s_off + r0 + etid);
   const bool py = a.p_walk == SK_P_Y;
   const int tx = a.tx, ty = a.ty;
   const float sc = a.c_bulk ? a.alpha : 1.0f;
@@ -247,7 +249,7 @@ __device__ __forceinline__ void skt_finish(const SkinnyArgs& a, const SkJob& j, 
       } else if (a.c_lin == SK_CLIN_XS) {
         skinny_copy_rows<SKT_EPI_THREADS>(a, os, tx * SK_SUB, cw, cs[hh], tx * ns, etid);
       } else {
-        skinny_store<SKT_EPI_THREADS>(a, os, cw, cs + hh, hh, ns, etid);
+        skinny_store<SKT_EPI_THREADS>(a, os, cw, cs + hh, r0 + hh, ns, etid);
       }
     }
   }
@@ -358,7 +360,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
   } else if (warp < SKT_MMA_WARP) {
     // ---------------- converters ----------------
     const int w = threadIdx.x - SKT_COPY_THREADS;  // the thread's box position
-    int cg = j0, cc = 0, cc1 = 0;
+    int cg = j0, cc = 0, cc1 = 0, cq = 0;  // cq: the job's first Q row (its pass)
     bool inside = false;  // the position is inside the tensor (else the copies skip it)
     SktRef cr{};
     auto cseek = [&]() {
@@ -367,6 +369,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         const SkJob jb = skinny_job(cr.a->sk, cr.J);
         cc = jb.c0;
         cc1 = jb.c1;
+        cq = jb.p * cr.a->spad;
         inside = skt_inside(cr.a->sk, jb.b, w);
       }
     };
@@ -380,7 +383,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
       }
       if (w == 0) {  // Q's chunk, in flight while the copies are waited for
         mbar_arrive_expect_tx(&full[stage], (uint32_t)cr.a->spad * 128u);
-        tma_load_2d(sB + stage * SKT_B_STAGE, cr.tq, cc * 64, 0, &full[stage]);
+        tma_load_2d(sB + stage * SKT_B_STAGE, cr.tq, cc * 64, cq, &full[stage]);
       }
       if (!mbar_wait(&sfull[slot], sphase, wait_ns)) {
         record_error(status, 1);

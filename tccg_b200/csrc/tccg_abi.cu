@@ -436,12 +436,11 @@ static bool skinny_eligible(const tccg_plan* p) {
   return std::min(p->M, p->N) <= SK_SMAX && p->K <= INT32_MAX;
 }
 
-// The tensor-core skinny kernel: split-BF16x3, a narrow side of at most 64
-// (its MMA N and the epilogue's register sums), K whose packed Q columns
-// (2 x K rounded up to 32) stay TMA coordinates.
+// The tensor-core skinny kernel: split-BF16x3, the skinny kernel's narrow
+// sides (<= 256: passes of 64 rows above 64), K whose packed Q columns (2 x
+// K rounded up to 32) stay TMA coordinates.
 static bool skinny_tc_eligible(const tccg_plan* p) {
-  return skinny_eligible(p) && p->prec == TCCG_PREC_BF16X3 && std::min(p->M, p->N) <= SKT_SMAX &&
-         p->K <= (int64_t(1) << 29);
+  return skinny_eligible(p) && p->prec == TCCG_PREC_BF16X3 && p->K <= (int64_t(1) << 29);
 }
 
 static long long abs_ll(int64_t v) { return v < 0 ? -(long long)v : (long long)v; }
@@ -543,10 +542,10 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode, bool
   // more than the 128 registers two CTAs per SM leave a thread.
   const int64_t S = sn ? p->N : p->M;
   p->sk_tc = tc;
-  p->sk_spad = (int32_t)round_up(S, 16);
-  if (tc) {
+  p->sk_spad = (int32_t)std::min<int64_t>(round_up(S, 16), SKT_SMAX);
+  if (tc) {  // passes of spad rows (MMA N)
     a.rs = p->sk_spad / 4;
-    a.npass = 1;
+    a.npass = (int32_t)cdiv(S, p->sk_spad);
   } else if (S <= 48) {
     a.rs = (int32_t)std::max<int64_t>(4, round_up(cdiv(S, 4), 4));
     a.npass = 1;
@@ -576,7 +575,8 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode, bool
     double best = 1e300;
     for (int64_t s = 1; s <= std::max<int64_t>(1, std::min<int64_t>(2 * p->num_sms, a.nchunks / 4)); ++s) {
       const int64_t per = cdiv(a.nchunks, s), ns = cdiv(a.nchunks, per);
-      const double cost = (double)cdiv((int64_t)a.nblk * ns, p->num_sms) * (double)(per + (ns > 1 ? 2 : 0));
+      const double cost =
+          (double)cdiv((int64_t)a.nblk * a.npass * ns, p->num_sms) * (double)(per + (ns > 1 ? 2 : 0));
       if (cost < best) {
         best = cost;
         a.chunks_per_split = (int32_t)per;
@@ -667,7 +667,7 @@ static bool choose_skinny_tc(const tccg_plan* p) {
   if (t.variant != 0 || t.load != 0 || t.direct != 0 || t.shortk != 0 || t.simt_tile != 0 ||
       t.tile_n != 0 || t.ksplit != 0)
     return false;
-  return p->K > SK_KC && p->sk.nblk >= 48;
+  return p->K > SK_KC && p->sk.nblk >= 48 && p->sk.S <= SKT_SMAX;
 }
 
 static bool choose_skinny(const tccg_plan* p) {
@@ -938,7 +938,7 @@ extern "C" int tccg_plan_create(const tccg_desc* desc, int32_t dtype, int32_t pr
     if (p->tune.skinny == 2 && !skinny_tc_eligible(p)) {
       plan_free(p);
       return fail(TCCG_ERR_UNSUPPORTED,
-                  "the tensor-core skinny kernel needs split-BF16x3 precision, min(M, N) <= 64 "
+                  "the tensor-core skinny kernel needs split-BF16x3 precision, min(M, N) <= 256 "
                   "and K <= 2^29");
     }
     const bool use_tc = eligible && skinny_tc_eligible(p) && choose_skinny_tc(p);
@@ -1034,10 +1034,10 @@ static int plan_layout(tccg_plan* p) {
   const bool ttgt = p->tune.method == TCCG_METHOD_TTGT;
   if (p->skinny) {
     const SkinnyArgs& a = p->sk;
-    if (p->sk_tc) {  // packed Q: spad rows x Kc bf16 (K-major, [hi | lo] per 32 k)
+    if (p->sk_tc) {  // packed Q: passes x spad rows x Kc bf16 (K-major, [hi | lo] per 32 k)
       p->Kc = 2 * round_up(p->K, 32);
       p->off_q = 0;
-      ws = align_up((size_t)p->sk_spad * (size_t)p->Kc * 2, 256);
+      ws = align_up((size_t)a.npass * p->sk_spad * (size_t)p->Kc * 2, 256);
     }
     if (p->sk_ksplit > 1) {  // FP32 slices [split][block][pass][row][position]
       p->off_part = ws;
@@ -1048,10 +1048,10 @@ static int plan_layout(tccg_plan* p) {
     if (p->sk_tc) {
       snprintf(p->describe, sizeof(p->describe),
                "method=GETT prec=bf16x3 kernel=skinny_tc<BF16X3> M=%lld N=%lld K=%lld narrow=%s "
-               "S=%d n=%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
+               "S=%d n=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
                "grid=%lld load=%s%s store=%s%s%s pack=q",
                (long long)p->M, (long long)p->N, (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S,
-               p->sk_spad, a.tx, a.ty, (long long)a.ex, (long long)a.ey, (long long)a.nblk,
+               a.npass, p->sk_spad, a.tx, a.ty, (long long)a.ex, (long long)a.ey, (long long)a.nblk,
                a.nchunks, p->sk_ksplit, (long long)a.njobs,
                (long long)std::min<int64_t>(a.njobs, p->num_sms), pw[a.p_walk],
                p->sk_p_vec ? " x16B" : "", cw[a.c_walk],
@@ -1918,8 +1918,8 @@ static SkinnyArgs skinny_args(const tccg_plan* p, const void* GA, const void* GB
 static PackOperand skinny_tc_q(const tccg_plan* p, const void* GA, const void* GB, char* w) {
   const bool sn = p->sk_s_is_n;
   return pack_op(sn ? GB : GA, sn ? p->t_b_n : p->t_a_m, sn ? p->t_b_k : p->t_a_k,
-                 sn ? p->N : p->M, p->K, p->sk_spad, round_up(p->K, 32), w + p->off_q, p->Kc,
-                 sn ? p->read_k_fast_b : p->read_k_fast_a);
+                 sn ? p->N : p->M, p->K, (int64_t)p->sk.npass * p->sk_spad, round_up(p->K, 32),
+                 w + p->off_q, p->Kc, sn ? p->read_k_fast_b : p->read_k_fast_a);
 }
 
 static SkinnyTcArgs skinny_tc_args(const tccg_plan* p, const void* GA, const void* GB, float* C,
@@ -1941,7 +1941,7 @@ static int run_skinny_tc(const tccg_plan* p, const void* GA, const void* GB, flo
   int rc = launch_pack<float, __nv_bfloat16, PACK_K_BF16X3>(pa, s, &packed);
   if (rc) return rc;
   CUtensorMap tmQ;
-  rc = encode_kmajor(&tmQ, w + p->off_q, p->sk_spad, p->Kc, p->sk_spad);
+  rc = encode_kmajor(&tmQ, w + p->off_q, (int64_t)p->sk.npass * p->sk_spad, p->Kc, p->sk_spad);
   if (rc) return rc;
   const SkinnyTcArgs a = skinny_tc_args(p, GA, GB, C, alpha, beta, w);
   mark(1, 0, s);
@@ -1951,8 +1951,8 @@ static int run_skinny_tc(const tccg_plan* p, const void* GA, const void* GB, flo
   mark(1, 1, s);
   if (rc || p->sk_ksplit == 1) return rc;
   mark(2, 0, s);
-  launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)a.sk.nblk), dim3(SK_THREADS),
-               SK_SMEM_BYTES, s, a.sk);
+  launch_after(true, p, skinny_reduce_kernel, dim3((unsigned)(a.sk.nblk * a.sk.npass)),
+               dim3(SK_THREADS), SK_SMEM_BYTES, s, a.sk);
   rc = launch_check("skinny_reduce");
   mark(2, 1, s);
   return rc;
@@ -2698,7 +2698,8 @@ static int bind_sktc(tccg_group* g, tccg_group::Wave& wv, const void* const* A,
     const void* GB = p->d.swap_ab ? A[i] : B[i];
     SkinnyTcItem it;
     memset(&it, 0, sizeof(it));
-    int rc = encode_kmajor(&it.tmQ, w + p->off_q, p->sk_spad, p->Kc, p->sk_spad);
+    int rc = encode_kmajor(&it.tmQ, w + p->off_q, (int64_t)p->sk.npass * p->sk_spad, p->Kc,
+                           p->sk_spad);
     if (rc) return rc;
     it.args = skinny_tc_args(p, GA, GB, static_cast<float*>(C[i]), (float)alpha[i], (float)beta[i], w);
     it.begin = jobs_n;

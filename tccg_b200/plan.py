@@ -168,7 +168,7 @@ class Tuning:
     load: int = 0  # tcgen05 BF16x3, FP32 operands: 0 auto, 1 packing pass + TMA, 2 gather
     tile_n: int = 0  # tcgen05 tile width: 0 default, 128, 192 (BF16, BF16x3) or 256 (BF16)
     skinny: int = 0  # FP32 operands, min(M, N) small: 0 auto, 1 the skinny kernel, -1 never,
-    #                  2 its tensor-core form (BF16x3, min(M, N) <= 64)
+    #                  2 its tensor-core form (BF16x3)
     # mode orders of the GETT view (gett_view): 0 = heuristic
     n_order: int = 0  # 1 = C's order, 2 = GB's unit-stride N mode first
     k_order: int = 0  # 1 = GA's order, 2 = GB's order

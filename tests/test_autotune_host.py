@@ -96,15 +96,15 @@ def test_mode_order_candidates_change_the_view():
 
 def test_tensor_core_skinny_candidate():
     """The tensor-core skinny kernel (skinny = 2) is searched for split-BF16x3
-    with a narrow side of at most 64, right after the kernel families (grouped
-    items too); not for other precisions."""
+    with a narrow side of at most 256, right after the kernel families
+    (grouped items too); not for other precisions."""
     con = make_contraction("ab", "akl", "lkb", dict(a=900, b=24, k=40, l=30))
     cs = candidates(con, "bf16x3", methods=("gett",))
     i = [t.skinny for t in cs].index(2)
     assert [(t.load, t.variant) for t in cs[2:5]] == [(1, 0), (2, 0), (0, -1)] and i == 5
     assert any(t.skinny == 2 for t in candidates(con, "bf16x3", grouped=True))
     assert all(t.skinny != 2 for t in candidates(con, "fp32"))
-    wide = make_contraction("ab", "ak", "kb", dict(a=900, b=100, k=64))
+    wide = make_contraction("ab", "ak", "kb", dict(a=900, b=300, k=64))
     assert all(t.skinny != 2 for t in candidates(wide, "bf16x3"))
 
 

@@ -169,13 +169,15 @@ def test_skinny_grouped_equals_per_item(cuda):
         assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= 1e-6, str(con)
 
 
-# the tensor-core kernel (tuning.skinny = 2): every case with a narrow side <= 64
-TC_CASES = [n for n in sorted(CASES) if n != "passes"]
+# the tensor-core kernel (tuning.skinny = 2): every case ("passes": S = 150 in
+# passes of 64 rows)
+TC_CASES = sorted(CASES)
 # long K over several TMEM rounds (ksplit=1: 38 chunks = rounds of 16, 16, 6),
-# and a narrow side of exactly 64
+# a narrow side of exactly 64, and one of 200 (passes of 64, 64, 64, 8)
 TC_EXTRA = {
     "rounds": ("ab", "akl", "lkb", dict(a=900, b=24, k=40, l=30), 1.0, 0.5),
     "s64": ("sw", "sk", "kw", dict(s=64, w=1000, k=300), -1.0, 0.0),
+    "s200": ("ws", "kw", "sk", dict(s=200, w=700, k=100), 1.0, 0.25),
 }
 
 
@@ -205,7 +207,7 @@ def test_skinny_tc_matches_oracle(cuda, name, ksplit):
 
 def test_skinny_tc_is_deterministic_and_refuses(cuda):
     """Repeated runs (k slices added in order) are bitwise equal; the kernel
-    serves split-BF16x3 with a narrow side of at most 64 only."""
+    serves split-BF16x3 with a narrow side of at most 256 only."""
     from tccg_b200._native import TccgError
     lc, la, lb, sizes, alpha, beta = _tc_case("rounds")
     con = make_contraction(lc, la, lb, sizes, alpha, beta)
@@ -217,7 +219,7 @@ def test_skinny_tc_is_deterministic_and_refuses(cuda):
     assert "ksplit=1 " not in p.describe(), p.describe()
     with pytest.raises(TccgError):
         Plan(con, "fp32", tuning=Tuning(skinny=2))
-    wide = make_contraction(*CASES["passes"][:4])
+    wide = make_contraction("mn", "mk", "kn", dict(m=300, n=400, k=64))
     with pytest.raises(TccgError):
         Plan(wide, "bf16x3", tuning=Tuning(skinny=2))
 
@@ -228,9 +230,9 @@ def test_skinny_tc_grouped_equals_per_item(cuda):
     equals the per-item runs bit for bit, within the BF16x3 bound."""
     import torch
     from tccg_b200.grouped import Group
-    names = ["transpose", "matvec_split", "kfast", "xy", "passes_split"]
+    names = ["transpose", "matvec_split", "kfast", "xy", "passes_split", "passes"]
     items = [make_contraction(*_tc_case(n)[:4], 1.0, 0.0) for n in names + sorted(TC_EXTRA)]
-    items.append(make_contraction(*CASES["passes"][:4], 1.0, 0.0))  # CUDA-core skinny
+    items.append(make_contraction(*CASES["outer"][:4], 1.0, 0.0))  # CUDA-core skinny
     items.append(make_contraction("mn", "mk", "kn", dict(m=700, n=500, k=300), 1.0, 0.0))
     tc = len(items) - 2
     tunings = [Tuning(skinny=2)] * tc + [Tuning(skinny=1), Tuning(variant=16)]
