@@ -12,12 +12,14 @@
 //               the skinny kernel's copies, cp.async) as fast as slots free
 //               up; each thread's copies arrive on the slot's barrier as
 //               they land (cp.async.mbarrier.arrive);
-//   warps 8-15  (256 threads, thread = box position): per chunk, split the
-//               position's 32 staged values into bf16 hi / lo and write its
-//               row of the 128-byte-swizzled K-major MMA stage, [hi(32 k) |
-//               lo(32 k)] -- the layout TMA gives the tile kernel; thread 0
-//               first loads the matching chunk of the narrow operand Q,
-//               packed once per call into the same layout, by TMA;
+//   warps 8-15  (256 threads, thread = box position = TMEM lane of its
+//               half): per chunk, split the position's 32 staged values into
+//               bf16 hi / lo and write them to its TMEM lane of the chunk's A
+//               stage (tcgen05.st: 16 columns of hi, 16 of lo) -- the MMAs
+//               read the wide operand from TMEM, so it takes no shared-memory
+//               stage; thread 0 first loads the matching chunk of the narrow
+//               operand Q, packed once per call into the K-major layout, by
+//               TMA;
 //   warp 16     one thread issues per chunk and half box (128 positions)
 //               the three products hi*hi + hi*lo + lo*hi of both k16 steps
 //               (tcgen05.mma kind::f16, M = 128, N = S rounded up to 16)
@@ -36,10 +38,11 @@
 // took 1.7-2.8 us against the 0.7 us of its HBM bytes (the copy pattern
 // alone streams at 4.9-6.6 TB/s).
 //
-// One CTA per SM (214 KB of shared memory: three 33 KB staging slots, two
-// 40 KB MMA stages, the 33 KB epilogue staging and the offset tables; 25
-// warps); TMEM 512 columns. Every wait is bounded (TCCG_DEVICE_WAIT_NS): a wait that
-// runs out records a status code and the CTA winds down.
+// One CTA per SM (216 KB of shared memory: five 33 KB staging slots, two
+// 8 KB Q stages, the 33 KB epilogue staging and the offset tables; 25
+// warps); TMEM 512 columns (accumulators, running sums, A stages). Every
+// wait is bounded (TCCG_DEVICE_WAIT_NS): a wait that runs out records a
+// status code and the CTA winds down.
 #pragma once
 
 #include <cuda.h>
@@ -57,12 +60,11 @@ constexpr int SKT_EPI_THREADS = SK_BW;  // one position each: TMEM lane of its h
 constexpr int SKT_THREADS = SKT_COPY_THREADS + SKT_CONV_THREADS + 32 + SKT_EPI_THREADS;  // 800
 constexpr int SKT_SMAX = 64;   // rows per pass (a narrow side above 64 runs passes of 64)
 constexpr int SKT_HALF = 128;  // MMA rows: positions per half box
-constexpr int SKT_SLOTS = 3;   // FP32 staging ring
-constexpr int SKT_STAGES = 2;  // MMA operand stages
-constexpr size_t SKT_A_STAGE = (size_t)SK_BW * 128;     // two halves x 128 rows x 128 B
+constexpr int SKT_SLOTS = 5;   // FP32 staging ring
+constexpr int SKT_STAGES = 2;  // MMA operand stages (P in TMEM, Q in shared memory)
 constexpr size_t SKT_B_STAGE = (size_t)SKT_SMAX * 128;  // up to 64 Q rows x 128 B
 constexpr size_t SKT_SLOT = (size_t)SK_KC * SK_LDP * 4;
-constexpr size_t SKT_OFF_B = SKT_STAGES * SKT_A_STAGE;
+constexpr size_t SKT_OFF_B = 0;
 constexpr size_t SKT_OFF_SLOT = SKT_OFF_B + SKT_STAGES * SKT_B_STAGE;
 constexpr size_t SKT_OFF_OS = SKT_OFF_SLOT + SKT_SLOTS * SKT_SLOT;
 constexpr size_t SKT_OFF_TAB = SKT_OFF_OS + (size_t)SK_SUB * SK_LDP * 4;
@@ -70,9 +72,13 @@ constexpr size_t SKT_OFF_TAB = SKT_OFF_OS + (size_t)SK_SUB * SK_LDP * 4;
 constexpr size_t SKT_OFF_BAR = SKT_OFF_TAB + (size_t)(3 * SK_BW + SKT_SMAX) * 4;
 constexpr size_t SKT_SMEM_BYTES = 1024 + SKT_OFF_BAR + 24 * 8;
 // TMEM columns: accumulator b of half h at b * 2 SMAX + h SMAX, the job's
-// running sums of half h at SKT_SUMCOL + h SMAX
+// running sums of half h at SKT_SUMCOL + h SMAX, and the converted P (the
+// MMAs' A operand) of stage s, half h at SKT_ACOL + s * 64 + h * 32: 16
+// columns of hi then 16 of lo (two bf16 of k per column)
 constexpr int SKT_SUMCOL = 4 * SKT_SMAX;
-constexpr uint32_t SKT_TMEM_COLS = 8 * SKT_SMAX;
+constexpr int SKT_ACOL = SKT_SUMCOL + 2 * SKT_SMAX;
+constexpr uint32_t SKT_TMEM_COLS = 512;
+static_assert(SKT_ACOL + SKT_STAGES * 64 <= (int)SKT_TMEM_COLS, "TMEM columns");
 static_assert(SK_BW == 2 * SKT_HALF, "a box is two MMA halves");
 static_assert(SKT_SMEM_BYTES <= 227 * 1024, "one CTA per SM");
 static_assert(SKT_OFF_B % 1024 == 0 && SKT_B_STAGE % 1024 == 0, "swizzled stages 1024-byte aligned");
@@ -140,33 +146,25 @@ __device__ __forceinline__ bool skt_epi_and(bool v) {
 }
 
 // Converts position w's column of a staging slot ([k][position], k < kc
-// valid) into row w % 128 of half w / 128 of an MMA stage: hi = bf16(x), lo
-// = bf16(x - hi), K-major [hi(32 k) | lo(32 k)], 16-byte chunk j stored at
-// chunk j ^ (row & 7) (TMA's 128-byte swizzle); k past kc, and every k of a
-// position outside the tensor (kc = 0: the copies skip it), are zeros.
-__device__ __forceinline__ void skt_convert(const float* slot, uint8_t* stA, int w, int kc) {
-  // shared-window addresses: the accesses stay shared-memory loads / stores
+// valid) into its TMEM lane of an A stage (ta: the warp's lane quarter, the
+// stage and half's first column): hi = bf16(x) in 16 columns, then lo =
+// bf16(x - hi) in 16, two k per column (the lower k in the low half); k past
+// kc, and every k of a position outside the tensor (kc = 0: the copies skip
+// it), are zeros. Warp-collective (tcgen05.st).
+__device__ __forceinline__ void skt_convert(const float* slot, uint32_t ta, int w, int kc) {
+  // shared-window addresses: the reads stay shared-memory loads
   const uint32_t src = smem_u32(slot + w);
-  const int r = w & (SKT_HALF - 1);
-  const uint32_t row = smem_u32(stA + (size_t)(w / SKT_HALF) * (SKT_A_STAGE / 2) + r * 128);
-  const int sw = r & 7;
+  uint32_t hw[16], lw[16];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {  // 8 k at a time
-    float x[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      x[e] = 0.0f;
-      if (8 * j + e < kc)
-        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x[e]) : "r"(src + (8 * j + e) * SK_LDP * 4));
-    }
-    uint32_t hw[4], lw[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) split_bf16x2(x[2 * e], x[2 * e + 1], hw[e], lw[e]);
-    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(row + ((j ^ sw) << 4)), "r"(hw[0]),
-                 "r"(hw[1]), "r"(hw[2]), "r"(hw[3]) : "memory");
-    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(row + (((4 + j) ^ sw) << 4)),
-                 "r"(lw[0]), "r"(lw[1]), "r"(lw[2]), "r"(lw[3]) : "memory");
+  for (int e = 0; e < SK_KC; e += 2) {
+    float x0 = 0.0f, x1 = 0.0f;
+    if (e < kc) asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x0) : "r"(src + e * SK_LDP * 4));
+    if (e + 1 < kc)
+      asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x1) : "r"(src + (e + 1) * SK_LDP * 4));
+    split_bf16x2(x0, x1, hw[e / 2], lw[e / 2]);
   }
+  tmem_st_32x32b_x16(ta, hw);
+  tmem_st_32x32b_x16(ta + 16, lw);
 }
 
 // The end of job j in the epilogue, its sums in TMEM (tsum(g): columns g *
@@ -263,7 +261,6 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_addr = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + (((raw_addr + 1023u) & ~1023u) - raw_addr);
-  uint8_t* sA = smem;
   uint8_t* sB = smem + SKT_OFF_B;
   float* slots = reinterpret_cast<float*>(smem + SKT_OFF_SLOT);
   float* os = reinterpret_cast<float*>(smem + SKT_OFF_OS);
@@ -389,10 +386,14 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         record_error(status, 1);
         break;
       }
-      skt_convert(slots + slot * (SKT_SLOT / 4), sA + stage * SKT_A_STAGE, w,
-                  inside ? skinny_kc(cr.a->sk, cc) : 0);
+      tc_fence_after();  // the stage's MMAs (waited for above) are done with its TMEM columns
+      skt_convert(slots + slot * (SKT_SLOT / 4),
+                  tbase + ((uint32_t)((warp & 3) * 32) << 16) +
+                      (uint32_t)(SKT_ACOL + stage * 64 + (w / SKT_HALF) * 32),
+                  w, inside ? skinny_kc(cr.a->sk, cc) : 0);
       mbar_arrive(&sempty[slot]);
-      fence_proxy_async_smem();  // the stage is read by the tensor cores (async proxy)
+      tmem_st_wait();    // the stage's TMEM columns are written ...
+      tc_fence_before();  // ... before the MMA warp learns of it
       mbar_arrive(&full[stage]);
       if (++slot == SKT_SLOTS) {
         slot = 0;
@@ -442,14 +443,14 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
               if (c * SK_KC + ks * 16 < a.K) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                  const uint64_t ad = umma_desc_k128(
-                      smem_u32(sA + stage * SKT_A_STAGE + h * (SKT_A_STAGE / 2)));
+                  // A in TMEM: k step ks at column + 8 ks (16 bf16), lo 16 columns on
+                  const uint32_t ah = tbase + (uint32_t)(SKT_ACOL + stage * 64 + h * 32 + 8 * ks);
                   const uint32_t d = d0 + (uint32_t)(h * SKT_SMAX);
-                  // descriptor start addresses in 16-byte units: +2 = 32 B (16
+                  // B descriptor start addresses in 16-byte units: +2 = 32 B (16
                   // bf16), +4 = 64 B (the lo half of the 128-byte row)
-                  tc_mma_f16(d, ad + 2 * ks, bd + 2 * ks, idesc, accumulate);  // hi * hi
-                  tc_mma_f16(d, ad + 2 * ks, bd + 4 + 2 * ks, idesc, 1);       // hi * lo
-                  tc_mma_f16(d, ad + 4 + 2 * ks, bd + 2 * ks, idesc, 1);       // lo * hi
+                  tc_mma_f16_ts(d, ah, bd + 2 * ks, idesc, accumulate);       // hi * hi
+                  tc_mma_f16_ts(d, ah, bd + 4 + 2 * ks, idesc, 1);            // hi * lo
+                  tc_mma_f16_ts(d, ah + 16, bd + 2 * ks, idesc, 1);           // lo * hi
                 }
                 accumulate = 1;
               }
