@@ -338,31 +338,53 @@ __device__ __forceinline__ void skinny_plane(const SkinnyArgs& a, const float* o
 
 // Stores staged rows [0, ns) (C rows s0 .. s0 + ns - 1; cs[r] = C offset of
 // row s0 + r) in the walk's address order; the NT / 32 warps share the planes.
+// Parts of the x range per plane so that a walk of n planes gives every warp
+// work: at least 2 NW pieces where the box is flat (few y), at least 32
+// positions a piece.
+__device__ __forceinline__ int skinny_xparts(int n, int tx, int nw) {
+  if (n >= 2 * nw) return 1;
+  const int want = (2 * nw + n - 1) / n, most = (tx + 31) / 32;
+  return want < most ? want : most;
+}
+
 template <int NT = SK_THREADS>
 __device__ __forceinline__ void skinny_store(const SkinnyArgs& a, const float* os,
                                              const int32_t* cw, const int32_t* cs, int s0, int ns,
                                              int tid) {
+  constexpr int NW = NT / 32;
   const int warp = tid >> 5;
   const bool py = a.p_walk == SK_P_Y;
   const int tx = a.tx, ty = a.ty;
+  const int xs = py ? ty : 1;  // position step along x
   if (a.c_walk == SK_C_XS) {
-    for (int yl = warp; yl < ty; yl += NT / 32)
-      skinny_plane(a, os, cw, cs, tx, ns, py ? yl : tx * yl, py ? ty : 1, 0, 0, 0, 1);
+    // (x, s) planes per y, split along x when there are few y (a flat box
+    // would leave most warps without a plane)
+    const int parts = skinny_xparts(ty, tx, NW), xp = (tx + parts - 1) / parts;
+    for (int job = warp; job < ty * parts; job += NW) {
+      const int yl = job / parts, x0 = (job % parts) * xp;
+      const int xn = tx - x0 < xp ? tx - x0 : xp;
+      if (xn > 0)
+        skinny_plane(a, os, cw, cs, xn, ns, (py ? yl : tx * yl) + x0 * xs, xs, 0, 0, 0, 1);
+    }
   } else if (a.c_walk == SK_C_XY) {
-    for (int r = warp; r < ns; r += NT / 32)
-      skinny_plane(a, os, cw, cs, tx, ty, 0, py ? ty : 1, py ? 1 : tx, r, 0, 0);
+    for (int r = warp; r < ns; r += NW)
+      skinny_plane(a, os, cw, cs, tx, ty, 0, xs, py ? 1 : tx, r, 0, 0);
   } else {
-    // runs of e0 consecutive rows (C stride one), clipped to [s0, s0 + ns)
+    // runs of e0 consecutive rows (C stride one), clipped to [s0, s0 + ns),
+    // then x, per y; split along x like the (x, s) planes
     const int e0 = a.s_run;
     const int first = (s0 / e0) * e0;
     const int nruns = (s0 + ns - first + e0 - 1) / e0;
-    for (int job = warp; job < nruns * ty; job += NT / 32) {
-      const int run = job % nruns, yl = job / nruns;
+    const int parts = skinny_xparts(nruns * ty, tx, NW), xp = (tx + parts - 1) / parts;
+    for (int job = warp; job < nruns * ty * parts; job += NW) {
+      const int part = job % parts, rj = job / parts;
+      const int run = rj % nruns, yl = rj / nruns;
       const int rs = first + run * e0;
       const int ra = rs > s0 ? rs : s0;
       const int rb = rs + e0 < s0 + ns ? rs + e0 : s0 + ns;
-      if (rb <= ra) continue;
-      skinny_plane(a, os, cw, cs, rb - ra, tx, py ? yl : tx * yl, 0, py ? ty : 1, ra - s0, 1, 0);
+      const int x0 = part * xp, xn = tx - x0 < xp ? tx - x0 : xp;
+      if (rb <= ra || xn <= 0) continue;
+      skinny_plane(a, os, cw, cs, rb - ra, xn, (py ? yl : tx * yl) + x0 * xs, 0, xs, ra - s0, 1, 0);
     }
   }
 }

@@ -654,12 +654,12 @@ static void with_skinny_rs(int rs, F&& f) {
 // epilogue's short C runs (0.4-0.5 TB/s measured where it assumes 3).
 // Whether a plan runs the tensor-core skinny kernel (skinny_tc.cuh): asked
 // for with tuning.skinny = 2, or -- unless the tuning asks for something
-// else -- K > 32 (two chunks or more) and at least 48 blocks of positions
-// (enough CTAs without a deep k-split). Measured on the 169 items of the
-// 256-item batched workload it can take (standalone, L2 flushed): on the 26
-// such items it takes 10.96 ms in sum where the other kernels' choice took
-// 12.10 ms; it loses where K <= 32 (C stores dominate: 4 epilogue warps) and
-// on a few blocks with a very long K (few CTAs, deep k-splits).
+// else -- K > 32 (two chunks or more), at least 48 blocks of positions
+// (enough CTAs without a deep k-split) and 17-64 rows. Measured on the 169
+// items of the 256-item batched workload it can take (standalone, L2
+// flushed): on the 20 such items 0.52 ms less in sum than the kernels chosen
+// before; it loses where K <= 32 (C stores dominate) and on a few blocks
+// with a very long K (few CTAs, deep k-splits).
 static bool choose_skinny_tc(const tccg_plan* p) {
   if (p->tune.skinny == 2) return true;
   if (p->tune.skinny != 0) return false;
@@ -667,7 +667,9 @@ static bool choose_skinny_tc(const tccg_plan* p) {
   if (t.variant != 0 || t.load != 0 || t.direct != 0 || t.shortk != 0 || t.simt_tile != 0 ||
       t.tile_n != 0 || t.ksplit != 0)
     return false;
-  return p->K > SK_KC && p->sk.nblk >= 48 && p->sk.S <= SKT_SMAX;
+  // a narrow side of at most 16 takes the CUDA-core register path instead
+  // (choose_skinny): on the 8 such items 1.36 ms in sum against 1.50 ms here
+  return p->K > SK_KC && p->sk.nblk >= 48 && p->sk.S > 16 && p->sk.S <= SKT_SMAX;
 }
 
 static bool choose_skinny(const tccg_plan* p) {
@@ -684,6 +686,10 @@ static bool choose_skinny(const tccg_plan* p) {
   // of at most 48 and at least 4096 positions, any K -- on the 59 such items
   // 2.6 ms less in sum than the CUDA-core tiles (21 % of their time)
   if (p->prec == TCCG_PREC_FP32 && a.S <= 48 && W >= 4096) return true;
+  // split-BF16x3, a narrow side of at most 16 (the register path), K > 32
+  // and at least 48 blocks: on the 8 such items 1.36 ms in sum where the
+  // kernels chosen before took 2.13 ms (the tensor-core skinny kernel 1.50 ms)
+  if (p->sk_reg && p->K > SK_KC && a.nblk >= 48) return true;
   double other = simt_time(p);
   if (p->prec == TCCG_PREC_BF16X3) other = std::min(other, tc_time(p, false));
   return skinny_time(p) < other;

@@ -254,29 +254,46 @@ def plane(L0, L1, w0, wi, wj, r0, ri, rj, warp, out):
             step += 1
 
 
-def store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns):
+def xparts(n, tx, nw):
+    """skinny_xparts: pieces of the x range per plane."""
+    if n >= 2 * nw:
+        return 1
+    return min(-(-2 * nw // n), -(-tx // 32))
+
+
+def store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns, NW=THREADS // 32):
     """skinny_store: [(warp plane, (w, r), step, lane)] of one staged step."""
     out = []
     py = p_walk == P_Y
-    NW = THREADS // 32
+    xs = ty if py else 1
     for warp in range(NW):
         if c_walk == C_XS:
-            for yl in range(warp, ty, NW):
-                plane(tx, ns, yl if py else tx * yl, ty if py else 1, 0, 0, 0, 1, (warp, yl), out)
+            parts = xparts(ty, tx, NW)
+            xp = -(-tx // parts)
+            for job in range(warp, ty * parts, NW):
+                yl, x0 = job // parts, (job % parts) * xp
+                xn = min(xp, tx - x0)
+                if xn > 0:
+                    plane(xn, ns, (yl if py else tx * yl) + x0 * xs, xs, 0, 0, 0, 1, (warp, job), out)
         elif c_walk == C_XY:
             for r in range(warp, ns, NW):
-                plane(tx, ty, 0, ty if py else 1, 1 if py else tx, r, 0, 0, (warp, r), out)
+                plane(tx, ty, 0, xs, 1 if py else tx, r, 0, 0, (warp, r), out)
         else:
             e0 = s_run
             first = (s0 // e0) * e0
             nruns = (s0 + ns - first + e0 - 1) // e0
-            for job in range(warp, nruns * ty, NW):
-                run, yl = job % nruns, job // nruns
+            parts = xparts(nruns * ty, tx, NW)
+            xp = -(-tx // parts)
+            for job in range(warp, nruns * ty * parts, NW):
+                part, rj = job % parts, job // parts
+                run, yl = rj % nruns, rj // nruns
                 rs_ = first + run * e0
                 ra, rb = max(rs_, s0), min(rs_ + e0, s0 + ns)
-                if rb <= ra:
+                x0 = part * xp
+                xn = min(xp, tx - x0)
+                if rb <= ra or xn <= 0:
                     continue
-                plane(rb - ra, tx, yl if py else tx * yl, 0, ty if py else 1, ra - s0, 1, 0,
+                plane(rb - ra, xn, (yl if py else tx * yl) + x0 * xs, 0, xs, ra - s0, 1, 0,
                       (warp, job), out)
     return out
 
@@ -289,11 +306,25 @@ GEOMS = [(19, 13), (10, 25), (16, 16), (256, 1), (3, 5), (1, 1)]
 @pytest.mark.parametrize("tx,ty", GEOMS)
 @pytest.mark.parametrize("s0,ns,s_run", [(0, 32, 10), (32, 8, 10), (0, 20, 8), (64, 32, 19),
                                          (0, 1, 1), (96, 22, 64)])
-def test_store_walk_covers_each_element_once(c_walk, p_walk, tx, ty, s0, ns, s_run):
-    st = store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns)
+@pytest.mark.parametrize("nw", [8, 4])
+def test_store_walk_covers_each_element_once(c_walk, p_walk, tx, ty, s0, ns, s_run, nw):
+    st = store_walk(c_walk, p_walk, tx, ty, s_run, s0, ns, nw)
     got = sorted(e for _, e, _, _ in st)
     assert got == sorted((pos(p_walk, tx, ty, xl, yl), r)
                          for xl in range(tx) for yl in range(ty) for r in range(ns))
+
+
+def test_flat_boxes_give_every_warp_work():
+    """A box of 256 x 1 positions (one y): the (x, s) planes and the runs of
+    C's stride-one S mode are split along x so that all 8 warps store (before
+    the split 1 of 8, resp. 4 of 8 warps had work and the rest waited at the
+    barrier after the stores)."""
+    for c_walk, ns, s_run in ((C_XS, 32, 0), (C_SX, 32, 10)):
+        st = store_walk(c_walk, P_X, 256, 1, s_run, 0, ns)
+        per_warp = {}
+        for (warp, _), _, _, _ in st:
+            per_warp[warp] = per_warp.get(warp, 0) + 1
+        assert len(per_warp) == 8 and max(per_warp.values()) <= 2 * min(per_warp.values())
 
 
 def test_store_instructions_are_contiguous():
