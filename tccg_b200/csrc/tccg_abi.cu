@@ -2309,6 +2309,11 @@ struct tccg_group {
   };
   std::vector<Wave> waves;
   bool bound = false;
+  // concurrent lanes: two side streams (the CUDA-core skinny lanes; the
+  // CUDA-core tiles with their packing) forked from and joined back into the
+  // caller's stream around each wave's GETT launches, and their events
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
 };
 
 #ifndef TCCG_GROUP_WAVE_MB
@@ -2322,6 +2327,11 @@ static void group_free(tccg_group* g) {
                 g->d_sk, g->d_skr, g->d_sktc};
   for (void* q : ps)
     if (q) cudaFree(q);
+  for (cudaStream_t q : g->side)
+    if (q) cudaStreamDestroy(q);
+  if (g->ev_fork) cudaEventDestroy(g->ev_fork);
+  for (cudaEvent_t e : g->ev_join)
+    if (e) cudaEventDestroy(e);
   delete g;
 }
 
@@ -2746,6 +2756,11 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
   for (size_t i = 0; i < g->plans.size(); ++i)
     if (!A[i] || !B[i] || !C[i]) return fail(TCCG_ERR_INVALID, "null operand pointer for item %zu", i);
   g->bound = false;
+  if (!g->ev_fork) {  // the concurrent lanes' streams and events, once per group
+    for (cudaStream_t& q : g->side) CUDA_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
+    for (cudaEvent_t& e : g->ev_join) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
   char* w = static_cast<char*>(ws);
   int rc;
   // all waves' items, jobs and reductions in one array per kind, wave after
@@ -2822,28 +2837,70 @@ extern "C" int tccg_group_bind(tccg_group* g, const void* const* A, const void* 
   return TCCG_OK;
 }
 
-// Launches of a group run, wave by wave: packing (CUDA-core lane,
-// tensor-core lane), the two grouped GETT kernels and the k-split reduction
-// -- each only when the wave has work for it.
+// Launches of a group run, wave by wave. The lanes run concurrently: the
+// tensor-core lanes (their packing, the tcgen05 tiles, the tensor-core
+// skinny kernel) on the caller's stream, the CUDA-core skinny lanes on one
+// side stream and the CUDA-core tiles (with their packing) on another, forked
+// from the caller's stream and joined back before the k-split reductions --
+// so that a lane's last CTAs share the GPU with the next lane's first
+// instead of leaving SMs idle (in a CUDA graph the streams become parallel
+// branches). Each launch only when the wave has work for it.
 template <typename T>
 static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_t s) {
   int rc;
   const dim3 blk(32, 8);
   const int sj = 2 * wv.n_simt, tj = wv.ntcj;
+  bool skinny_side = false;
+  for (int cls = 0; cls < 3; ++cls) skinny_side |= wv.nsk[cls] > 0;
+  const bool simt_side = wv.n_simt > 0;
+  cudaStream_t s_sk = skinny_side ? g->side[0] : s, s_simt = simt_side ? g->side[1] : s;
+  if (skinny_side || simt_side) {
+    CUDA_TRY(cudaEventRecord(g->ev_fork, s));
+    if (skinny_side) CUDA_TRY(cudaStreamWaitEvent(s_sk, g->ev_fork, 0));
+    if (simt_side) CUDA_TRY(cudaStreamWaitEvent(s_simt, g->ev_fork, 0));
+  }
+  // CUDA-core tiles: packing and GETT on their stream
   const PackJob* sjobs = g->d_simt_jobs + 2 * wv.simt0;
   const int64_t* sb = g->b_simt_jobs + 2 * wv.simt0;
   if (wv.simt_pack_ctas > 0) {
     const dim3 pg((unsigned)wv.simt_pack_ctas);
     if (g->prec == TCCG_PREC_FP64)
-      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s>>>(sjobs, sb, sj);
+      pack_group_kernel<double, double, PACK_MN><<<pg, blk, 0, s_simt>>>(sjobs, sb, sj);
     else if (g->dtype == TCCG_BF16)
-      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s>>>(sjobs, sb, sj);
+      pack_group_kernel<__nv_bfloat16, float, PACK_MN><<<pg, blk, 0, s_simt>>>(sjobs, sb, sj);
     else if (g->prec == TCCG_PREC_BF16)
-      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s>>>(sjobs, sb, sj);
+      pack_group_kernel<float, float, PACK_MN_BF16><<<pg, blk, 0, s_simt>>>(sjobs, sb, sj);
     else
-      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s>>>(sjobs, sb, sj);
+      pack_group_kernel<float, float, PACK_MN><<<pg, blk, 0, s_simt>>>(sjobs, sb, sj);
     if ((rc = launch_check("pack_group"))) return rc;
   }
+  if (wv.n_simt > 0) {
+    simt_gett_group_kernel<T><<<(unsigned)wv.simt_tiles, 256, simt_group_smem_bytes<T>(), s_simt>>>(
+        static_cast<const SimtGroupItem<T>*>(g->d_simt) + wv.simt0, g->b_simt_items + wv.simt0,
+        wv.n_simt);
+    if ((rc = launch_check("simt_gett_group"))) return rc;
+  }
+  // CUDA-core skinny lanes on theirs
+  if constexpr (sizeof(T) == 4) {
+    for (int cls = 0; cls < 3; ++cls) {
+      if (wv.nsk[cls] == 0) continue;
+      if (wv.sk_reg[cls]) {  // the register path (its items all take it)
+        const unsigned grid =
+            (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SKR_CTAS_PER_SM * g->num_sms);
+        skinny_reg_group_kernel<<<grid, SKR_THREADS, SKR_SMEM_BYTES, s_sk>>>(
+            g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], (int)wv.sk_jobs[cls]);
+      } else {
+        const unsigned grid =
+            (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SK_CTAS_PER_SM * g->num_sms);
+        with_skinny_rs(4 * (cls + 1), [&](auto r) {
+          skinny_group_kernel<decltype(r)::value><<<grid, SK_THREADS, SK_SMEM_BYTES, s_sk>>>(
+              g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], wv.sk_jobs[cls]);
+        });
+      }
+      if ((rc = launch_check("skinny_group"))) return rc;
+    }
+  }
+  // tensor-core lanes on the caller's stream
   const bool x3 = g->prec == TCCG_PREC_BF16X3;
   const PackJob* tjobs = g->d_tc_jobs + wv.tcj0;
   const int64_t* tb = g->b_tc_jobs + wv.tcj0;
@@ -2856,12 +2913,6 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
     else
       pack_group_kernel<float, __nv_bfloat16, PACK_K_BF16><<<pg, blk, 0, s>>>(tjobs, tb, tj);
     if ((rc = launch_check("pack_group"))) return rc;
-  }
-  if (wv.n_simt > 0) {
-    simt_gett_group_kernel<T><<<(unsigned)wv.simt_tiles, 256, simt_group_smem_bytes<T>(), s>>>(
-        static_cast<const SimtGroupItem<T>*>(g->d_simt) + wv.simt0, g->b_simt_items + wv.simt0,
-        wv.n_simt);
-    if ((rc = launch_check("simt_gett_group"))) return rc;
   }
   for (int v = 0; v < TCV_COUNT; ++v) {
     if (wv.nlane[v] == 0) continue;
@@ -2878,29 +2929,23 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
     if ((rc = launch_check("gett_tc_group"))) return rc;
   }
   if constexpr (sizeof(T) == 4) {
-    for (int cls = 0; cls < 3; ++cls) {
-      if (wv.nsk[cls] == 0) continue;
-      if (wv.sk_reg[cls]) {  // the register path (its items all take it)
-        const unsigned grid =
-            (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SKR_CTAS_PER_SM * g->num_sms);
-        skinny_reg_group_kernel<<<grid, SKR_THREADS, SKR_SMEM_BYTES, s>>>(
-            g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], (int)wv.sk_jobs[cls]);
-      } else {
-        const unsigned grid =
-            (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SK_CTAS_PER_SM * g->num_sms);
-        with_skinny_rs(4 * (cls + 1), [&](auto r) {
-          skinny_group_kernel<decltype(r)::value><<<grid, SK_THREADS, SK_SMEM_BYTES, s>>>(
-              g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], wv.sk_jobs[cls]);
-        });
-      }
-      if ((rc = launch_check("skinny_group"))) return rc;
-    }
     if (wv.nsktc > 0) {
       const unsigned grid = (unsigned)std::min<int64_t>(wv.sktc_jobs, g->num_sms);
       skinny_tc_group_kernel<<<grid, SKT_THREADS, SKT_SMEM_BYTES, s>>>(
           g->d_sktc + wv.sktc0, g->b_sktc + wv.sktc0, wv.nsktc, (int)wv.sktc_jobs, g->sktc_status);
       if ((rc = launch_check("skinny_tc_group"))) return rc;
     }
+  }
+  // join, then the k-split reductions of every lane
+  if (skinny_side) {
+    CUDA_TRY(cudaEventRecord(g->ev_join[0], s_sk));
+    CUDA_TRY(cudaStreamWaitEvent(s, g->ev_join[0], 0));
+  }
+  if (simt_side) {
+    CUDA_TRY(cudaEventRecord(g->ev_join[1], s_simt));
+    CUDA_TRY(cudaStreamWaitEvent(s, g->ev_join[1], 0));
+  }
+  if constexpr (sizeof(T) == 4) {
     if (wv.nskr > 0) {
       skinny_reduce_group_kernel<<<(unsigned)wv.skr_ctas, SK_THREADS, SK_SMEM_BYTES, s>>>(
           g->d_skr + wv.skr0, g->b_skr + wv.skr0, wv.nskr);

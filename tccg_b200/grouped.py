@@ -8,9 +8,11 @@ multiplied before the next reuses the region, so the group's workspace is
 that of its largest wave rather than the sum over all items.
 ``bind(As, Bs, Cs)`` fixes the operand pointers and the workspace (uploading
 the device work lists once); after that ``run()`` issues, per wave, the
-grouped packing, the grouped GETT kernels (CUDA-core and tensor-core lanes)
-and the k-split reduction that have work, and ``capture()`` records them into
-a CUDA graph that ``replay()`` re-launches. ``run_per_item()`` is the
+grouped packing, the grouped GETT kernels (tensor-core lanes on the given
+stream, the CUDA-core skinny lanes and the CUDA-core tiles on two side
+streams forked from and joined back into it) and the k-split reductions that
+have work, and ``capture()`` records them into a CUDA graph (the side streams
+as parallel branches) that ``replay()`` re-launches. ``run_per_item()`` is the
 baseline: one tccg_plan_run per contraction.
 """
 from __future__ import annotations
