@@ -272,13 +272,16 @@ int tccg_transpose(int32_t dtype, int32_t dim, const int32_t* perm, const int64_
 /*
  * Grouped launch: many plans of the same precision run by a few launches per
  * wave (waves of at most 4 GiB of workspace): grouped packing, one grouped
- * GETT kernel per kernel family (CUDA cores, tcgen05 persistent) and the
- * grouped k-split reduction, each only when it has work. tccg_group_bind fixes
- * the operand pointers and workspace (it uploads the work lists,
- * synchronously), after which tccg_group_run only launches kernels and can be
- * captured in a CUDA graph. Groups run a plan's tcgen05 tiles without its tail
- * split (tuning.tail_split); plans made with tail_split = -1 give the same
- * sums in a group as alone.
+ * GETT kernel per kernel family (CUDA-core tiles, tcgen05 tiles, the skinny
+ * kernels) and the grouped k-split reductions, each only when it has work.
+ * The tensor-core lanes run on the given stream, the CUDA-core skinny lanes
+ * and the CUDA-core tiles on two side streams of the group forked from it and
+ * joined back before the reductions. tccg_group_bind fixes the operand
+ * pointers and workspace (it uploads the work lists, synchronously, and
+ * creates the side streams), after which tccg_group_run only launches kernels
+ * and can be captured in a CUDA graph. Groups run a plan's tcgen05 tiles
+ * without its tail split (tuning.tail_split); plans made with tail_split = -1
+ * give the same sums in a group as alone.
  */
 typedef struct tccg_group tccg_group; /* opaque */
 int tccg_group_create(const tccg_plan* const* plans, int32_t count, tccg_group** out);
