@@ -265,10 +265,19 @@ def test_skinny_choice_and_refusal(cuda):
     # item 69 of the 256-item batched workload (N = 40, K = 20, 5.0e6 positions, P
     # transposed against C): the library takes the skinny kernel
     from tccg_b200.workloads import batched_workload
-    con = batched_workload(256, seed=0)[69]
+    items = batched_workload(256, seed=0)
+    con = items[69]
     for precision in ("fp32", "bf16x3"):
         assert "skinny_gett" in Plan(con, precision).describe()
         assert "skinny_gett" not in Plan(con, precision, tuning=Tuning(skinny=-1)).describe()
+    # split-BF16x3 with K > 32 and >= 48 blocks: 17-64 rows take the
+    # tensor-core kernel (item 6: S = 18), up to 16 the register path (item
+    # 46: S = 11); FP32 keeps the CUDA cores
+    assert "skinny_tc" in Plan(items[6], "bf16x3").describe()
+    assert "skinny_gett" in Plan(items[6], "fp32").describe()
+    d = Plan(items[46], "bf16x3").describe()
+    assert "skinny_gett" in d and "path=registers" in d, d
+    assert "skinny_tc" not in Plan(items[6], "bf16x3", tuning=Tuning(skinny=1)).describe()
     # a square GEMM is not skinny; FP64 and BF16 are not served
     sq = make_contraction("mn", "mk", "kn", dict(m=512, n=512, k=512))
     assert "skinny_gett" not in Plan(sq, "fp32").describe()
