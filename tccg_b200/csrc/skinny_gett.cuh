@@ -92,7 +92,11 @@ enum SkinnyCWalk : int { SK_C_XS = 0, SK_C_XY = 1, SK_C_SX = 2 };
 // x + ex (s - s0) with the box covering all of X (SK_CLIN_XS), or C(x0 + x,
 // y, s) = C(x0, y, 0) + s + S x with all of S in one staged step
 // (SK_CLIN_SX).
-enum SkinnyCLin : int { SK_CLIN_NONE = 0, SK_CLIN_XS = 1, SK_CLIN_SX = 2 };
+// C's stride-one S mode of extent e0 (s_run) directly followed in C by X:
+// C(x, y, u e0 + o) = C(0, y, u e0) + x e0 + o, passes of whole runs, each
+// (run, box row) one range of e0 x floats (SK_CLIN_RUNS; staged like the
+// general case, copied range by range).
+enum SkinnyCLin : int { SK_CLIN_NONE = 0, SK_CLIN_XS = 1, SK_CLIN_SX = 2, SK_CLIN_RUNS = 3 };
 
 struct SkinnyArgs {
   const float* P;
@@ -112,6 +116,7 @@ struct SkinnyArgs {
   int32_t S, K;
   int32_t rs;              // rows of S per thread; a pass covers 4 * rs rows
   int32_t npass;           // passes over S (> 1 only with one chunk and no k-split)
+  int32_t spr;             // rows per pass: pass p covers S rows [p spr, p spr + spr), spr <= 4 rs
   int32_t ksplit;
   int32_t nchunks, chunks_per_split;
   int32_t kr_log2;         // SK_P_K: log2 of the lanes along k per position
@@ -178,8 +183,8 @@ __device__ __forceinline__ void skinny_begin(const SkinnyArgs& a, int b, int p, 
   const bool ok = w < a.tx * a.ty && x < a.ex && y < a.ey;
   pw[w] = ok ? x * a.px + __ldg(a.p_y_off + y) : SK_NONE;
   cw[w] = ok ? x * a.cx + __ldg(a.c_y_off + y) : SK_NONE;
-  if (!a.partial && w < sp) {
-    const int s = p * sp + w;
+  if (!a.partial && w < a.spr) {
+    const int s = p * a.spr + w;
     cs[w] = s < a.S ? __ldg(a.c_s_off + s) : 0;
   }
 }
@@ -272,14 +277,15 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
   const int tid = threadIdx.x, lane = tid & 31;
   const int k0 = c * SK_KC;
   const int kc = skinny_kc(a, c);
-  // Q rows p sp .. p sp + sp - 1 of k [0, kc); rows >= S are zeros
-  const int s0 = j.p * sp;
+  // Q rows p spr .. p spr + spr - 1 of k [0, kc) in the pass's sp slots;
+  // slots >= spr and rows >= S are zeros
+  const int s0 = j.p * a.spr;
   if (a.q_kfast) {
     if (lane < kc) {
       const int32_t ko = __ldg(a.q_k_off + k0 + lane);
       for (int r = tid >> 5; r < sp; r += SK_THREADS / 32) {
         float* d = qs + lane * SK_QLD + r;
-        if (s0 + r < a.S)
+        if (r < a.spr && s0 + r < a.S)
           cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s0 + r) + ko);
         else
           *d = 0.0f;
@@ -288,7 +294,7 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
   } else {
     for (int r = tid % sp, k = tid / sp; k < kc;) {
       float* d = qs + k * SK_QLD + r;
-      if (s0 + r < a.S)
+      if (r < a.spr && s0 + r < a.S)
         cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s0 + r) + __ldg(a.q_k_off + k0 + k));
       else
         *d = 0.0f;
@@ -425,6 +431,54 @@ __device__ __forceinline__ void skinny_fma(SkAcc<RS>& acc, const float* ps, cons
   }
 }
 
+// x extent of block b's box inside the tensor.
+__device__ __forceinline__ int skinny_box_xn(const SkinnyArgs& a, int b) {
+  const int ix = a.bxn == 1 ? 0 : b % a.bxn;
+  return a.ex - ix * a.tx < a.tx ? a.ex - ix * a.tx : a.tx;
+}
+
+// SK_CLIN_RUNS: stores staged rows [0, ns) (whole runs u = 0 .. ns / e0 - 1
+// of C's stride-one S mode, row u e0 + o of position w at os[(u e0 + o)
+// SK_LDP + w]) as ranges: run u of box row yl is the xn e0 consecutive floats
+// from C + cw(0, yl) + cs[u e0], element f = x e0 + o. A warp per range when
+// there are at least NT / 32 ranges, else the whole CTA per range; (x, o)
+// and the staging index advance by fixed steps (one carry at most per step).
+template <int NT = SK_THREADS>
+__device__ __forceinline__ void skinny_copy_runs(const SkinnyArgs& a, const float* os,
+                                                 const int32_t* cw, const int32_t* cs, int ns,
+                                                 int xn, int tid) {
+  constexpr int NW = NT / 32;
+  const int e0 = a.s_run, ty = a.ty;
+  const bool py = a.p_walk == SK_P_Y;
+  const int wx = py ? ty : 1;  // position step along x
+  const int n = xn * e0, nr = (ns / e0) * ty;
+  const bool per_warp = nr >= NW;
+  const int g0 = per_warp ? tid >> 5 : 0, gs = per_warp ? NW : 1;
+  const int f0 = per_warp ? tid & 31 : tid, fs = per_warp ? 32 : NT;
+  const int dx = fs / e0, dox = fs - dx * e0;
+  const int x0 = f0 / e0, o0 = f0 - x0 * e0;
+  const int dsi = dox * SK_LDP + dx * wx, csi = wx - e0 * SK_LDP;
+  const float alpha = a.alpha, beta = a.beta;
+  for (int g = g0; g < nr; g += gs) {
+    const int u = g / ty, yl = g - u * ty;
+    const int wy = py ? yl : a.tx * yl;  // position (0, yl)
+    const int32_t cy = cw[wy];
+    if (cy == SK_NONE) continue;  // y past the tensor (uniform per range)
+    float* c = a.C + cy + cs[u * e0];
+    int o = o0, si = (u * e0 + o0) * SK_LDP + wy + x0 * wx;
+    for (int f = f0; f < n; f += fs) {
+      const float v = alpha * os[si];
+      c[f] = beta != 0.0f ? fmaf(beta, c[f], v) : v;
+      o += dox;
+      si += dsi;
+      if (o >= e0) {
+        o -= e0;
+        si += csi;
+      }
+    }
+  }
+}
+
 // Stores the staged range [0, n) of box row yl (os[f]) at C + base + f; one
 // warp per row when there are at least 8 rows, else the whole CTA per row.
 // With c_bulk (staged values already scaled by alpha, beta = 0) a row whose
@@ -550,15 +604,15 @@ __device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& 
           make_float4(acc.v[i][0], acc.v[i][1], acc.v[i][2], acc.v[i][3]);
     return;
   }
-  if (a.c_lin != SK_CLIN_NONE) {
+  if (a.c_lin == SK_CLIN_XS || a.c_lin == SK_CLIN_SX) {
     skinny_finish_lin<RS>(a, j, acc, os, cw, cs);
     return;
   }
 #pragma unroll 1
-  for (int h = 0; h < SP; h += SK_SUB) {
-    const int s0 = j.p * SP + h;
+  for (int h = 0; h < a.spr; h += SK_SUB) {
+    const int s0 = j.p * a.spr + h;
     if (s0 >= a.S) break;
-    int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
+    int ns = a.spr - h < SK_SUB ? a.spr - h : SK_SUB;
     if (ns > a.S - s0) ns = a.S - s0;
     __syncthreads();  // the stage's last reader (the FMAs, or the previous step's stores) is done
 #pragma unroll
@@ -569,7 +623,10 @@ __device__ __forceinline__ void skinny_finish(const SkinnyArgs& a, const SkJob& 
             make_float4(acc.v[i][0], acc.v[i][1], acc.v[i][2], acc.v[i][3]);
     }
     __syncthreads();
-    skinny_store(a, os, cw, cs + h, s0, ns, threadIdx.x);
+    if (a.c_lin == SK_CLIN_RUNS)
+      skinny_copy_runs(a, os, cw, cs, ns, skinny_box_xn(a, j.b), threadIdx.x);
+    else
+      skinny_store(a, os, cw, cs + h, s0, ns, threadIdx.x);
   }
 }
 
@@ -673,10 +730,10 @@ __device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int r, 
   const size_t slice = (size_t)a.nblk * a.npass * SP * SK_BW;
   const float* src = a.partial + (size_t)r * SP * SK_BW + tid;
 #pragma unroll 1
-  for (int h = 0; h < SP; h += SK_SUB) {
-    const int s0 = p * SP + h;
+  for (int h = 0; h < a.spr; h += SK_SUB) {
+    const int s0 = p * a.spr + h;
     if (s0 >= a.S) break;
-    int ns = SP - h < SK_SUB ? SP - h : SK_SUB;
+    int ns = a.spr - h < SK_SUB ? a.spr - h : SK_SUB;
     if (ns > a.S - s0) ns = a.S - s0;
     __syncthreads();
     for (int rr = 0; rr < ns; ++rr) {
@@ -686,7 +743,10 @@ __device__ __forceinline__ void skinny_reduce_block(const SkinnyArgs& a, int r, 
       os[rr * SK_LDP + tid] = v;
     }
     __syncthreads();
-    skinny_store(a, os, cw, cs + h, s0, ns, threadIdx.x);
+    if (a.c_lin == SK_CLIN_RUNS)
+      skinny_copy_runs(a, os, cw, cs, ns, skinny_box_xn(a, b), threadIdx.x);
+    else
+      skinny_store(a, os, cw, cs + h, s0, ns, threadIdx.x);
   }
 }
 

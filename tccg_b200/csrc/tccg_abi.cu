@@ -563,6 +563,22 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode, bool
   // TCCG_B200_SKINNY_REG=0 keeps the shared-memory path
   const char* reg_env = std::getenv("TCCG_B200_SKINNY_REG");
   p->sk_reg = !tc && a.rs == 4 && a.npass == 1 && !(reg_env && std::strcmp(reg_env, "0") == 0);
+  a.spr = 4 * a.rs;
+  // C's stride-one S mode (extent e0 < S, unit stride) directly followed in C
+  // by X: passes of whole runs (spr = the most runs in one 32-row staging
+  // step), each (run, box row) stored as one range of e0 x floats
+  // (SK_CLIN_RUNS), when that takes no more passes
+  bool runs = false;
+  if (!tc && !p->sk_reg && a.c_walk == SK_C_SX && a.s_run < S && a.cx == a.s_run) {
+    const int32_t spr = (std::min<int32_t>(a.spr, SK_SUB) / a.s_run) * a.s_run;
+    int sfirst = -1;
+    for (int i = 0; i < nsm && sfirst < 0; ++i)
+      if (sext[i] > 1) sfirst = i;
+    if (spr > 0 && cdiv(S, spr) == a.npass && sc[sfirst] == 1) {
+      runs = true;
+      a.spr = spr;
+    }
+  }
   // k-split: (block, pass) jobs that cannot fill the persistent CTAs,
   // slices of >= 4 chunks
   const int64_t per_sm = tc ? 1 : p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM;
@@ -601,8 +617,10 @@ static bool skinny_geometry(tccg_plan* p, std::vector<int>& ym, int* xmode, bool
       if (t[i] != t[0] + (int64_t)i * st) return false;
     return true;
   };
-  a.c_lin = SK_CLIN_NONE;
-  if (a.c_walk == SK_C_XS && a.cx == 1 && a.tx == a.ex && a.bxn == 1 && affine(a.ex))
+  a.c_lin = runs ? SK_CLIN_RUNS : SK_CLIN_NONE;
+  if (runs)
+    ;
+  else if (a.c_walk == SK_C_XS && a.cx == 1 && a.tx == a.ex && a.bxn == 1 && affine(a.ex))
     a.c_lin = SK_CLIN_XS;
   else if (a.c_walk == SK_C_SX && a.npass == 1 && S <= SK_SUB && a.cx == S && affine(1))
     a.c_lin = SK_CLIN_SX;
@@ -1071,14 +1089,15 @@ static int plan_layout(tccg_plan* p) {
              "rows=%dx%d box=%dx%d ex=%lld ey=%lld blocks=%lld kchunks=%d ksplit=%d jobs=%lld "
              "grid=%lld load=%s%s%s store=%s%s%s%s pack=none",
              p->prec == TCCG_PREC_BF16X3 ? "bf16x3" : "fp32", (long long)p->M, (long long)p->N,
-             (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S, a.npass, 4 * a.rs, a.tx, a.ty,
+             (long long)p->K, p->sk_s_is_n ? "N" : "M", a.S, a.npass, a.spr, a.tx, a.ty,
              (long long)a.ex, (long long)a.ey, (long long)a.nblk, a.nchunks, p->sk_ksplit,
              (long long)a.njobs,
              (long long)std::min<int64_t>(
                  a.njobs, (int64_t)(p->sk_reg ? SKR_CTAS_PER_SM : SK_CTAS_PER_SM) * p->num_sms),
              pw[a.p_walk], p->sk_p_vec ? " x16B" : "", a.q_kfast ? " q=k" : " q=s", cw[a.c_walk],
              a.c_walk == SK_C_SX ? (std::string(" run=") + std::to_string(a.s_run)).c_str() : "",
-             a.c_lin ? " linear" : "", p->sk_reg ? " path=registers" : "");
+             a.c_lin == SK_CLIN_RUNS ? " ranges" : a.c_lin ? " linear" : "",
+             p->sk_reg ? " path=registers" : "");
     p->ws_bytes = ws;
     return TCCG_OK;
   }

@@ -33,9 +33,18 @@ CASES = {
     # P's stride-one index is contracted (u): loads along k
     "kfast": ("fjr", "ufr", "ju", dict(f=10, j=28, r=46, u=8), 1.0, 0.25,
               ["narrow=N", "load=k", "store=xs"]),
-    # S = 150 rows in five passes of 32
+    # S = 150 rows in five passes of three runs of o (C's stride-one mode,
+    # directly followed by r): each run of a box row one range of 10 x 37
     "passes": ("orak", "cok", "rac", dict(o=10, r=37, a=9, k=15, c=18), -0.75, 0.0,
-               ["narrow=M", "rows=5x32", "store=sx run=10"]),
+               ["narrow=M", "rows=5x30", "store=sx run=10 ranges"]),
+    # the same with a flat box (256 x 1; the whole CTA copies each range) and
+    # a ragged last box along x
+    "ranges_flat": ("orak", "cok", "rac", dict(o=10, r=300, a=2, k=15, c=18), 1.0, 0.0,
+                    ["rows=5x30", "box=256x1", "ranges"]),
+    # runs of 8 with passes of 32 rows, K split over slices (the reduction
+    # copies the ranges), beta != 0
+    "ranges_split": ("orkb", "lok", "rlb", dict(o=8, r=40, k=9, b=3, l=400), 0.5, 0.5,
+                     ["rows=3x32", "ranges"]),
     # C's next stride after X is a W mode: (x, y) planes; K over three chunks
     "xy": ("mpn", "pmk", "kn", dict(m=33, p=9, n=5, k=70), 1.0, 1.0,
            ["narrow=N", "load=y", "store=xy"]),

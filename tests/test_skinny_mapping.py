@@ -348,6 +348,45 @@ def test_store_instructions_are_contiguous():
     assert full and all(a == list(range(a[0], a[0] + 32)) for a in full)
 
 
+@pytest.mark.parametrize("p_walk", [P_X, P_Y])
+@pytest.mark.parametrize("tx,ty,xn", [(37, 6, 37), (256, 1, 256), (256, 1, 44), (19, 13, 7), (4, 64, 4)])
+@pytest.mark.parametrize("e0,ns", [(10, 30), (8, 32), (10, 20), (3, 30), (32, 32)])
+@pytest.mark.parametrize("nt", [256, 128])
+def test_run_ranges_copy_each_element_once(p_walk, tx, ty, xn, e0, ns, nt):
+    """skinny_copy_runs: range (u, yl) element f = x e0 + o reads staged row
+    u e0 + o of position (x, yl) at (u e0 + o) LDP + pos and writes C range
+    offset f; (x, o) and the staging index step by fs with one carry --
+    every (row, position) with x < xn copied once, to its own address."""
+    nw = nt // 32
+    n, nr = xn * e0, (ns // e0) * ty
+    per_warp = nr >= nw
+    wx = ty if p_walk == P_Y else 1
+    seen = {}
+    for tid in range(nt):
+        g0, gs = (tid >> 5, nw) if per_warp else (0, 1)
+        f0, fs = (tid & 31, 32) if per_warp else (tid, nt)
+        dx, dox = fs // e0, fs % e0
+        x0, o0 = f0 // e0, f0 % e0
+        dsi, csi = dox * LDP + dx * wx, wx - e0 * LDP
+        for g in range(g0, nr, gs):
+            u, yl = g // ty, g % ty
+            wy = yl if p_walk == P_Y else tx * yl
+            o, si = o0, (u * e0 + o0) * LDP + wy + x0 * wx
+            for f in range(f0, n, fs):
+                x = f // e0
+                assert o == f % e0
+                assert si == (u * e0 + o) * LDP + pos(p_walk, tx, ty, x, yl)
+                assert (u, yl, f) not in seen
+                seen[(u, yl, f)] = si
+                o += dox
+                si += dsi
+                if o >= e0:
+                    o -= e0
+                    si += csi
+    assert len(seen) == nr * n
+    assert len(set(seen.values())) == len(seen)
+
+
 def test_partial_slices_round_trip():
     """k-split: the job of slice z, block b, pass p writes row r, position w
     at (((z nblk + b) npass + p) SP + r) BW + w; the reduction CTA of (b, p)
