@@ -842,6 +842,13 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       } else {
         // chunked accumulation: sum the chunk accumulators in registers (RN adds)
         const int nchunks = (t.kb_end - t.kb_begin + a.chunk_kb - 1) / a.chunk_kb;
+        // C's offsets of this warp's columns, column 32 i + lane in lane's
+        // cn[i] (loaded while the MMAs run; passed around by shuffles when
+        // storing, so no store waits on a table load)
+        int64_t cn[HC / 32];
+#pragma unroll
+        for (int i = 0; i < HC / 32; ++i)
+          cn[i] = 32 * i + lane < nlim ? __ldg(a.c_n_off + n0 + 32 * i + lane) : 0;
         float sum[HC];
         for (int ch = 0; ch < nchunks; ++ch) {
           if (!mbar_wait(&accf[acc], acc_phase, wait_ns)) {
@@ -872,11 +879,13 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
           }
         }
         if (!ok) break;
-        if (m_ok && part) {
+        if (part) {  // warp-uniform, like the branches below
+          if (m_ok) {
 #pragma unroll
-          for (int j = 0; j < HC; ++j)
-            if (j < nlim) part[(size_t)(pc0 + j) * pld] = sum[j];
-        } else if (a.crun > 0 && !part) {
+            for (int j = 0; j < HC; ++j)
+              if (j < nlim) part[(size_t)(pc0 + j) * pld] = sum[j];
+          }
+        } else if (a.crun > 0) {
 #pragma unroll
           for (int cc = 0; cc < HC; cc += 16) {
             if (cc < nlim) {  // warp-uniform
@@ -891,23 +900,28 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
                          a.crun, alpha, beta, lane, cmo, cn_lane);
             }
           }
-        } else if (m_ok) {
+        } else {
+          // every lane takes part in the shuffles; rows past M store nothing
           if (beta != 0.0f) {
 #pragma unroll
             for (int cc = 0; cc < HC; cc += 8) {
+              int64_t o[8];
               float old[8];
 #pragma unroll
-              for (int j = 0; j < 8; ++j)
-                old[j] = (cc + j < nlim) ? a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] : 0.0f;
+              for (int j = 0; j < 8; ++j) {
+                o[j] = cmo + __shfl_sync(0xffffffffu, cn[(cc + j) / 32], (cc + j) % 32);
+                old[j] = m_ok && cc + j < nlim ? a.C[o[j]] : 0.0f;
+              }
 #pragma unroll
               for (int j = 0; j < 8; ++j)
-                if (cc + j < nlim)
-                  a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] = fmaf(beta, old[j], alpha * sum[cc + j]);
+                if (m_ok && cc + j < nlim) a.C[o[j]] = fmaf(beta, old[j], alpha * sum[cc + j]);
             }
           } else {
 #pragma unroll
-            for (int j = 0; j < HC; ++j)
-              if (j < nlim) a.C[cmo + __ldg(a.c_n_off + n0 + j)] = alpha * sum[j];
+            for (int j = 0; j < HC; ++j) {
+              const int64_t o = cmo + __shfl_sync(0xffffffffu, cn[j / 32], j % 32);
+              if (m_ok && j < nlim) a.C[o] = alpha * sum[j];
+            }
           }
         }
       }
