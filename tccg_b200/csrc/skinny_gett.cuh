@@ -324,10 +324,11 @@ __device__ __forceinline__ void skinny_plane(const SkinnyArgs& a, const float* o
   const int dw = wi * di + wj * dj, dr = ri * di + rj * dj;
   const int cw_carry = wj - wi * L0, cr_carry = rj - ri * L0;
   const float alpha = a.alpha, beta = a.beta;
+  float* const Cb = a.C;  // read once (a grouped launch's item is in global memory)
   for (int f = lane; f < total; f += 32) {
     const int32_t o = cw[w];
     if (o != SK_NONE) {
-      float* d = a.C + o + cs[r];
+      float* d = Cb + o + cs[r];
       const float v = alpha * os[r * SK_LDP + w];
       *d = beta != 0.0f ? fmaf(beta, *d, v) : v;
     }

@@ -274,6 +274,9 @@ __device__ __forceinline__ TileRef resolve_tile(int tile, const CUtensorMap* tmA
 __device__ __forceinline__ void store_runs(const float* stg, const TcArgs& a, int64_t m0,
                                            int ncols, int e0, float alpha, float beta, int lane,
                                            int64_t cm_lane, int64_t cn_lane) {
+  // fields read once: in a grouped launch a is the item in global memory,
+  // which the compiler must otherwise read again after every store
+  float* const Cb = a.C;
   int64_t mlim = a.M - m0;  // rows of this warp inside M
   if (mlim > 32) mlim = 32;
 #pragma unroll 1
@@ -290,7 +293,7 @@ __device__ __forceinline__ void store_runs(const float* stg, const TcArgs& a, in
       const int64_t cm = __shfl_sync(0xffffffffu, cm_lane, (ma + i) & 31);
       const int64_t cn = __shfl_sync(0xffffffffu, cn_lane, j & 31);
       if (f0 + lane < total) {
-        float* dst = a.C + cm + cn;
+        float* dst = Cb + cm + cn;
         const float v = alpha * stg[j * 33 + ma + i];
         *dst = beta != 0.0f ? fmaf(beta, *dst, v) : v;
       }
@@ -756,6 +759,10 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
       const int64_t n0 = (int64_t)t.tn * Cfg::BN + h * HC;
       const int64_t nlim = a.N - n0;
       const float alpha = a.alpha, beta = a.beta;
+      // C read once: in a grouped launch a is the item in global memory,
+      // which the compiler must otherwise read again after every store
+      float* const Cb = a.C;
+      const int64_t* const cno = a.c_n_off + n0;
       // k-split slice: raw sums to partial[z][n][M], a tail slice to its
       // tile's block of tail_partial (both coalesced along m): element
       // (m, column c of this warp's half) at part[(pc0 + c) * pld]
@@ -811,7 +818,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
                 __syncwarp();
                 const int64_t left = nlim - cc - hh;
                 const int64_t cn_lane =
-                    lane < 16 && cc + hh + lane < nlim ? __ldg(a.c_n_off + n0 + cc + hh + lane) : 0;
+                    lane < 16 && cc + hh + lane < nlim ? __ldg(cno + cc + hh + lane) : 0;
                 store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, left < 16 ? (int)left : 16,
                            a.crun, alpha, beta, lane, cmo, cn_lane);
               }
@@ -821,17 +828,17 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
               float old[32];
 #pragma unroll
               for (int j = 0; j < 32; ++j)
-                old[j] = (cc + j < nlim) ? a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] : 0.0f;
+                old[j] = (cc + j < nlim) ? Cb[cmo + __ldg(cno + cc + j)] : 0.0f;
 #pragma unroll
               for (int j = 0; j < 32; ++j)
                 if (cc + j < nlim)
-                  a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] =
+                  Cb[cmo + __ldg(cno + cc + j)] =
                       fmaf(beta, old[j], alpha * __uint_as_float(r[j]));
             } else {
 #pragma unroll
               for (int j = 0; j < 32; ++j)
                 if (cc + j < nlim)
-                  a.C[cmo + __ldg(a.c_n_off + n0 + cc + j)] = alpha * __uint_as_float(r[j]);
+                  Cb[cmo + __ldg(cno + cc + j)] = alpha * __uint_as_float(r[j]);
             }
           }
         }
@@ -848,7 +855,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
         int64_t cn[HC / 32];
 #pragma unroll
         for (int i = 0; i < HC / 32; ++i)
-          cn[i] = 32 * i + lane < nlim ? __ldg(a.c_n_off + n0 + 32 * i + lane) : 0;
+          cn[i] = 32 * i + lane < nlim ? __ldg(cno + 32 * i + lane) : 0;
         float sum[HC];
         for (int ch = 0; ch < nchunks; ++ch) {
           if (!mbar_wait(&accf[acc], acc_phase, wait_ns)) {
@@ -895,7 +902,7 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
               __syncwarp();
               const int64_t left = nlim - cc;
               const int64_t cn_lane =
-                  lane < 16 && cc + lane < nlim ? __ldg(a.c_n_off + n0 + cc + lane) : 0;
+                  lane < 16 && cc + lane < nlim ? __ldg(cno + cc + lane) : 0;
               store_runs(wstg, a, (int64_t)t.tm * Cfg::BM + q * 32, left < 16 ? (int)left : 16,
                          a.crun, alpha, beta, lane, cmo, cn_lane);
             }
@@ -910,17 +917,17 @@ __device__ __forceinline__ void gett_tc_body(const CUtensorMap* tmA, const CUten
 #pragma unroll
               for (int j = 0; j < 8; ++j) {
                 o[j] = cmo + __shfl_sync(0xffffffffu, cn[(cc + j) / 32], (cc + j) % 32);
-                old[j] = m_ok && cc + j < nlim ? a.C[o[j]] : 0.0f;
+                old[j] = m_ok && cc + j < nlim ? Cb[o[j]] : 0.0f;
               }
 #pragma unroll
               for (int j = 0; j < 8; ++j)
-                if (m_ok && cc + j < nlim) a.C[o[j]] = fmaf(beta, old[j], alpha * sum[cc + j]);
+                if (m_ok && cc + j < nlim) Cb[o[j]] = fmaf(beta, old[j], alpha * sum[cc + j]);
             }
           } else {
 #pragma unroll
             for (int j = 0; j < HC; ++j) {
               const int64_t o = cmo + __shfl_sync(0xffffffffu, cn[j / 32], j % 32);
-              if (m_ok && j < nlim) a.C[o] = alpha * sum[j];
+              if (m_ok && j < nlim) Cb[o] = alpha * sum[j];
             }
           }
         }
