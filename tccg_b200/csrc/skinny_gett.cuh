@@ -212,6 +212,9 @@ __device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float
   };
   const int tid = threadIdx.x;
   const int kc = skinny_kc(a, c);
+  // read once: each cp.async clobbers memory, and a grouped launch's item is
+  // in global memory, which the compiler would otherwise read again
+  const float* const P = a.P;
   if (a.p_walk == SK_P_K) {
     // lanes along k: thread tid takes k = tid % kr of positions tid / kr + i * 256 / kr
     const int lg = a.kr_log2, kl = tid & ((1 << lg) - 1);
@@ -221,7 +224,7 @@ __device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float
       for (int w = tid >> lg; w < SK_BW; w += SK_THREADS >> lg) {
         const int32_t po = pw[w];
         if (po != SK_NONE)
-          cp_async_elem<4>(d + w, a.P + po + ko);
+          cp_async_elem<4>(d + w, P + po + ko);
         else
           zero(d + w);
       }
@@ -237,13 +240,13 @@ __device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float
       const int32_t kok = __shfl_sync(0xffffffffu, ko, k);
       float* d = ps + k * SK_LDP + g;
       if (vec) {
-        cp_async_16(d, a.P + o0 + kok);
+        cp_async_16(d, P + o0 + kok);
       } else {
         const int32_t o[4] = {o0, o1, o2, o3};
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           if (o[e] != SK_NONE)
-            cp_async_elem<4>(d + e, a.P + o[e] + kok);
+            cp_async_elem<4>(d + e, P + o[e] + kok);
           else
             zero(d + e);
         }
@@ -255,7 +258,7 @@ __device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float
     // around by shuffles, so no copy waits on a table load
     const int32_t po = pw[tid];
     float* d = ps + tid;
-    const float* src = a.P + (po != SK_NONE ? po : 0);
+    const float* src = P + (po != SK_NONE ? po : 0);
 #pragma unroll 4
     for (int k = 0; k < kc; ++k) {
       const int32_t kok = __shfl_sync(0xffffffffu, ko, k);
@@ -280,13 +283,18 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
   // Q rows p spr .. p spr + spr - 1 of k [0, kc) in the pass's sp slots;
   // slots >= spr and rows >= S are zeros
   const int s0 = j.p * a.spr;
+  // fields read once (see skinny_issue_p); rows valid below nr
+  const float* const Q = a.Q;
+  const int32_t* const qso = a.q_s_off + s0;
+  const int32_t* const qko = a.q_k_off + k0;
+  const int nr = a.S - s0 < a.spr ? a.S - s0 : a.spr;
   if (a.q_kfast) {
     if (lane < kc) {
-      const int32_t ko = __ldg(a.q_k_off + k0 + lane);
+      const int32_t ko = __ldg(qko + lane);
       for (int r = tid >> 5; r < sp; r += SK_THREADS / 32) {
         float* d = qs + lane * SK_QLD + r;
-        if (r < a.spr && s0 + r < a.S)
-          cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s0 + r) + ko);
+        if (r < nr)
+          cp_async_elem<4>(d, Q + __ldg(qso + r) + ko);
         else
           *d = 0.0f;
       }
@@ -294,8 +302,8 @@ __device__ __forceinline__ void skinny_issue(const SkinnyArgs& a, const SkJob& j
   } else {
     for (int r = tid % sp, k = tid / sp; k < kc;) {
       float* d = qs + k * SK_QLD + r;
-      if (r < a.spr && s0 + r < a.S)
-        cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + s0 + r) + __ldg(a.q_k_off + k0 + k));
+      if (r < nr)
+        cp_async_elem<4>(d, Q + __ldg(qso + r) + __ldg(qko + k));
       else
         *d = 0.0f;
       r += SK_THREADS % sp;
@@ -828,13 +836,19 @@ __device__ __forceinline__ void skinny_reg_begin(const SkinnyArgs& a, int b, int
 
 // Q rows 0..15 of k [kb, kb + 16) into qs[k][row] (zeros past S or ke).
 __device__ __forceinline__ void skinny_reg_q(const SkinnyArgs& a, int kb, int ke, float* qs) {
+  // fields read once (each cp.async clobbers memory; a grouped item is in
+  // global memory)
+  const float* const Q = a.Q;
+  const int32_t* const qso = a.q_s_off;
+  const int32_t* const qko = a.q_k_off + kb;
+  const int S = a.S;
 #pragma unroll
   for (int i = 0; i < SKR_KR * SKR_ROWS / SKR_THREADS; ++i) {
     const int e = threadIdx.x + i * SKR_THREADS;
     const int kk = e / SKR_ROWS, r = e % SKR_ROWS;
     float* d = qs + e;
-    if (r < a.S && kb + kk < ke)
-      cp_async_elem<4>(d, a.Q + __ldg(a.q_s_off + r) + __ldg(a.q_k_off + kb + kk));
+    if (r < S && kb + kk < ke)
+      cp_async_elem<4>(d, Q + __ldg(qso + r) + __ldg(qko + kk));
     else
       *d = 0.0f;
   }
