@@ -160,7 +160,22 @@ __device__ __forceinline__ SkJob skinny_job(const SkinnyArgs& a, int J) {
   return j;
 }
 
-__device__ __forceinline__ int skinny_kc(const SkinnyArgs& a, int c) {
+// The fields the P copies of a chunk read (skinny_kc, skinny_p_ko,
+// skinny_issue_p): a caller that issues many chunks of one item keeps them in
+// registers (a grouped launch's item is in global memory, and every cp.async
+// clobbers memory: read through the item, each chunk would load them again).
+struct SkPFields {
+  const float* P;
+  const int32_t* p_k_off;
+  int32_t K, p_walk, p_vec, kr_log2;
+};
+
+__device__ __forceinline__ SkPFields skinny_p_fields(const SkinnyArgs& a) {
+  return SkPFields{a.P, a.p_k_off, a.K, a.p_walk, a.p_vec, a.kr_log2};
+}
+
+template <typename A>
+__device__ __forceinline__ int skinny_kc(const A& a, int c) {
   const int64_t k0 = (int64_t)c * SK_KC;
   return a.K - k0 < SK_KC ? (int)(a.K - k0) : SK_KC;
 }
@@ -193,7 +208,8 @@ __device__ __forceinline__ void skinny_begin(const SkinnyArgs& a, int b, int p, 
 // of the chunk for the walk along k, else k = lane (passed around the warp
 // by shuffles); 0 past the chunk's extent. A table load whose result the
 // copies wait for: callers load it a chunk ahead.
-__device__ __forceinline__ int32_t skinny_p_ko(const SkinnyArgs& a, int c) {
+template <typename A>
+__device__ __forceinline__ int32_t skinny_p_ko(const A& a, int c) {
   const int tid = threadIdx.x;
   const int kl = a.p_walk == SK_P_K ? tid & ((1 << a.kr_log2) - 1) : tid & 31;
   return kl < skinny_kc(a, c) ? __ldg(a.p_k_off + c * SK_KC + kl) : 0;
@@ -204,8 +220,8 @@ __device__ __forceinline__ int32_t skinny_p_ko(const SkinnyArgs& a, int c) {
 // the tensor are zeros); ko = skinny_p_ko(a, c). Threads 0 .. SK_THREADS - 1
 // take part; no commit. SKIP: positions outside the tensor are left
 // unwritten (the consumer substitutes zeros for them).
-template <bool SKIP = false>
-__device__ __forceinline__ void skinny_issue_p(const SkinnyArgs& a, int c, float* ps,
+template <bool SKIP = false, typename A = SkinnyArgs>
+__device__ __forceinline__ void skinny_issue_p(const A& a, int c, float* ps,
                                                const int32_t* pw, int32_t ko) {
   auto zero = [&](float* d) {
     if (!SKIP) *d = 0.0f;

@@ -315,10 +315,12 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
     int32_t iko = 0;
     bool inew = false;
     const SkinnyArgs* ia = nullptr;
+    SkPFields ipf{};  // ia's fields the copies of each chunk read
     auto iseek = [&]() {
       if (ig < njobs) {
         const SktRef r = resolve(ig);
         ia = &r.a->sk;
+        ipf = skinny_p_fields(*ia);
         const SkJob jb = skinny_job(*ia, r.J);
         ic = jb.c0;
         ic1 = jb.c1;
@@ -327,7 +329,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
       }
     };
     iseek();
-    if (ig < njobs) iko = skinny_p_ko(*ia, ic);
+    if (ig < njobs) iko = skinny_p_ko(ipf, ic);
     int slot = 0;
     uint32_t sphase = 0;
     while (ig < njobs) {
@@ -341,7 +343,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         named_barrier_sync(1, SKT_COPY_THREADS);  // walks read other threads' offsets
         inew = false;
       }
-      skinny_issue_p<true>(*ia, ic, slots + slot * (SKT_SLOT / 4), pw + ipw * SK_BW, iko);
+      skinny_issue_p<true>(ipf, ic, slots + slot * (SKT_SLOT / 4), pw + ipw * SK_BW, iko);
       cp_async_mbar_arrive(&sfull[slot]);
       if (++slot == SKT_SLOTS) {
         slot = 0;
@@ -351,13 +353,14 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         ig += js;
         iseek();
       }
-      if (ig < njobs) iko = skinny_p_ko(*ia, ic);
+      if (ig < njobs) iko = skinny_p_ko(ipf, ic);
     }
     cp_async_wait<0>();  // no copy in flight when the copy warps leave
   } else if (warp < SKT_MMA_WARP) {
     // ---------------- converters ----------------
     const int w = threadIdx.x - SKT_COPY_THREADS;  // the thread's box position
     int cg = j0, cc = 0, cc1 = 0, cq = 0;  // cq: the job's first Q row (its pass)
+    int cK = 0, cspad = 0;  // the item's K and rows per pass, read once per job
     bool inside = false;  // the position is inside the tensor (else the copies skip it)
     SktRef cr{};
     auto cseek = [&]() {
@@ -366,7 +369,9 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         const SkJob jb = skinny_job(cr.a->sk, cr.J);
         cc = jb.c0;
         cc1 = jb.c1;
-        cq = jb.p * cr.a->spad;
+        cK = cr.a->sk.K;
+        cspad = cr.a->spad;
+        cq = jb.p * cspad;
         inside = skt_inside(cr.a->sk, jb.b, w);
       }
     };
@@ -379,7 +384,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         break;
       }
       if (w == 0) {  // Q's chunk, in flight while the copies are waited for
-        mbar_arrive_expect_tx(&full[stage], (uint32_t)cr.a->spad * 128u);
+        mbar_arrive_expect_tx(&full[stage], (uint32_t)cspad * 128u);
         tma_load_2d(sB + stage * SKT_B_STAGE, cr.tq, cc * 64, cq, &full[stage]);
       }
       if (!mbar_wait(&sfull[slot], sphase, wait_ns)) {
@@ -390,7 +395,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
       skt_convert(slots + slot * (SKT_SLOT / 4),
                   tbase + ((uint32_t)((warp & 3) * 32) << 16) +
                       (uint32_t)(SKT_ACOL + stage * 64 + (w / SKT_HALF) * 32),
-                  w, inside ? skinny_kc(cr.a->sk, cc) : 0);
+                  w, inside ? (cK - cc * SK_KC < SK_KC ? cK - cc * SK_KC : SK_KC) : 0);
       mbar_arrive(&sempty[slot]);
       tmem_st_wait();    // the stage's TMEM columns are written ...
       tc_fence_before();  // ... before the MMA warp learns of it
@@ -420,6 +425,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
         const SkJob jb = skinny_job(a, r.J);
         const uint32_t idesc = idesc_bf16_f32(SKT_HALF, r.a->spad);
         const int ckb = r.a->chunk_kb;
+        const int K = a.K;  // read once (the waits below clobber memory)
         for (int c0 = jb.c0; c0 < jb.c1 && ok; c0 += ckb) {
           if (!mbar_wait(&acce[acc], acc_phase ^ 1, wait_ns)) {
             record_error(status, 2);
@@ -440,7 +446,7 @@ __device__ __forceinline__ void skinny_tc_body(int njobs, Resolve&& resolve, int
             const uint64_t bd = umma_desc_k128(smem_u32(sB + stage * SKT_B_STAGE));
 #pragma unroll
             for (int ks = 0; ks < 2; ++ks) {
-              if (c * SK_KC + ks * 16 < a.K) {
+              if (c * SK_KC + ks * 16 < K) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                   // A in TMEM: k step ks at column + 8 ks (16 bf16), lo 16 columns on
