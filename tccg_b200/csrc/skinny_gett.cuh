@@ -850,7 +850,8 @@ __device__ __forceinline__ void skinny_reg_begin(const SkinnyArgs& a, int b, int
   }
 }
 
-// Q rows 0..15 of k [kb, kb + 16) into qs[k][row] (zeros past S or ke).
+// Q rows 0..ROWS-1 of k [kb, kb + 16) into qs[k][row] (zeros past S or ke).
+template <int ROWS>
 __device__ __forceinline__ void skinny_reg_q(const SkinnyArgs& a, int kb, int ke, float* qs) {
   // fields read once (each cp.async clobbers memory; a grouped item is in
   // global memory)
@@ -859,9 +860,9 @@ __device__ __forceinline__ void skinny_reg_q(const SkinnyArgs& a, int kb, int ke
   const int32_t* const qko = a.q_k_off + kb;
   const int S = a.S;
 #pragma unroll
-  for (int i = 0; i < SKR_KR * SKR_ROWS / SKR_THREADS; ++i) {
+  for (int i = 0; i < SKR_KR * ROWS / SKR_THREADS; ++i) {
     const int e = threadIdx.x + i * SKR_THREADS;
-    const int kk = e / SKR_ROWS, r = e % SKR_ROWS;
+    const int kk = e / ROWS, r = e % ROWS;
     float* d = qs + e;
     if (r < S && kb + kk < ke)
       cp_async_elem<4>(d, Q + __ldg(qso + r) + __ldg(qko + kk));
@@ -893,14 +894,15 @@ __device__ __forceinline__ void skinny_reg_p(const SkinnyArgs& a, int kb, int ke
 }
 
 // The end of a job: raw sums to its k slice, or the rows to C (staged in os).
+template <int ROWS>
 __device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJob& j,
-                                                  const float (&acc)[2][SKR_ROWS], float* os,
+                                                  const float (&acc)[2][ROWS], float* os,
                                                   const int32_t* cw, const int32_t* cs) {
   const int tid = threadIdx.x;
-  if (a.partial) {  // layout of the 16-row (RS = 4) tile path
+  if (a.partial) {  // layout of the 16-row (RS = 4) tile path; rows >= ROWS not written
     float* dst = a.partial + (((size_t)j.z * a.nblk + j.b) * a.npass + j.p) * SKR_ROWS * SK_BW + tid;
 #pragma unroll
-    for (int r = 0; r < SKR_ROWS; ++r) {
+    for (int r = 0; r < ROWS; ++r) {
       dst[(size_t)r * SK_BW] = acc[0][r];
       dst[(size_t)r * SK_BW + SKR_THREADS] = acc[1][r];
     }
@@ -919,7 +921,7 @@ __device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJ
       const int xl = py ? w / ty : w % tx, yl = py ? w % ty : w / tx;
       float* o = os + yl * plane + (xs ? xl : xl * S);
 #pragma unroll
-      for (int r = 0; r < SKR_ROWS; ++r)
+      for (int r = 0; r < ROWS; ++r)
         if (r < S) o[xs ? r * tx : r] = sc * acc[h][r];
     }
     if (a.c_bulk) fence_proxy_async_smem();
@@ -934,7 +936,7 @@ __device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJ
     return;
   }
 #pragma unroll
-  for (int r = 0; r < SKR_ROWS; ++r) {
+  for (int r = 0; r < ROWS; ++r) {
     os[r * SK_LDP + tid] = acc[0][r];
     os[r * SK_LDP + tid + SKR_THREADS] = acc[1][r];
   }
@@ -942,15 +944,73 @@ __device__ __forceinline__ void skinny_reg_finish(const SkinnyArgs& a, const SkJ
   skinny_store<SKR_THREADS>(a, os, cw, cs, 0, S, tid);
 }
 
-template <typename Resolve>
+// One job of the register path with ROWS computed rows (16, or 8 for a
+// narrow side of at most 8: half the FMAs and Q copies).
+template <int ROWS>
+__device__ __forceinline__ void skinny_reg_job(const SkinnyArgs& a, const SkJob& job, float* Qs,
+                                               float* os, const int32_t* pw, const int32_t* cw,
+                                               const int32_t* cs) {
+  const int tid = threadIdx.x;
+  const int32_t po0 = pw[tid], po1 = pw[tid + SKR_THREADS];
+  const int kbeg = job.c0 * SK_KC;
+  const int kend = job.c1 * SK_KC < a.K ? job.c1 * SK_KC : a.K;
+  float acc[2][ROWS];
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) acc[0][r] = acc[1][r] = 0.0f;
+  float pc0[SKR_KR], pc1[SKR_KR];
+  skinny_reg_q<ROWS>(a, kbeg, kend, Qs);
+  skinny_reg_p(a, kbeg, kend, po0, po1, pc0, pc1, skinny_reg_ko(a, kbeg, kend));
+  int32_t ko_next = skinny_reg_ko(a, kbeg + SKR_KR, kend);  // the next step's
+  int st = 0;
+#pragma unroll 1
+  for (int kb = kbeg; kb < kend; kb += SKR_KR) {
+    const int nb = kb + SKR_KR;
+    float pn0[SKR_KR], pn1[SKR_KR];
+    if (nb < kend) {
+      __syncthreads();  // stage st ^ 1 was read by the previous step
+      skinny_reg_q<ROWS>(a, nb, kend, Qs + (st ^ 1) * SKR_KR * SKR_ROWS);
+      skinny_reg_p(a, nb, kend, po0, po1, pn0, pn1, ko_next);
+      ko_next = skinny_reg_ko(a, nb + SKR_KR, kend);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();  // Q of this step landed
+    const float* q = Qs + st * SKR_KR * SKR_ROWS;
+#pragma unroll
+    for (int kk = 0; kk < SKR_KR; ++kk) {
+      float qv[ROWS];
+#pragma unroll
+      for (int r = 0; r < ROWS; r += 4) {
+        const float4 t = *reinterpret_cast<const float4*>(q + kk * ROWS + r);
+        qv[r] = t.x; qv[r + 1] = t.y; qv[r + 2] = t.z; qv[r + 3] = t.w;
+      }
+#pragma unroll
+      for (int r = 0; r < ROWS; ++r) {
+        acc[0][r] = fmaf(qv[r], pc0[kk], acc[0][r]);
+        acc[1][r] = fmaf(qv[r], pc1[kk], acc[1][r]);
+      }
+    }
+    if (nb < kend) {
+#pragma unroll
+      for (int kk = 0; kk < SKR_KR; ++kk) {
+        pc0[kk] = pn0[kk];
+        pc1[kk] = pn1[kk];
+      }
+    }
+    st ^= 1;
+  }
+  skinny_reg_finish<ROWS>(a, job, acc, os, cw, cs);
+}
+
+template <int ROWS, typename Resolve>
 __device__ __forceinline__ void skinny_reg_loop(int j0, int jstep, int njobs, Resolve&& resolve,
                                                 uint8_t* smem) {
-  float* Qs = reinterpret_cast<float*>(smem);  // [2][KR][ROWS]
+  float* Qs = reinterpret_cast<float*>(smem);  // [2][KR][ROWS], stages SKR_ROWS rows apart
   float* os = reinterpret_cast<float*>(smem + SKR_OFF_OS);
   int32_t* pw = reinterpret_cast<int32_t*>(smem + SKR_OFF_TAB);
   int32_t* cw = pw + SK_BW;
   int32_t* cs = cw + SK_BW;
-  const int tid = threadIdx.x;
 #pragma unroll 1
   for (int jg = j0; jg < njobs; jg += jstep) {
     const SkRef ref = resolve(jg);
@@ -959,68 +1019,23 @@ __device__ __forceinline__ void skinny_reg_loop(int j0, int jstep, int njobs, Re
     __syncthreads();  // the previous job's stores are done with os, pw, cw, cs
     skinny_reg_begin(a, job.b, pw, cw, cs);
     __syncthreads();
-    const int32_t po0 = pw[tid], po1 = pw[tid + SKR_THREADS];
-    const int kbeg = job.c0 * SK_KC;
-    const int kend = job.c1 * SK_KC < a.K ? job.c1 * SK_KC : a.K;
-    float acc[2][SKR_ROWS];
-#pragma unroll
-    for (int r = 0; r < SKR_ROWS; ++r) acc[0][r] = acc[1][r] = 0.0f;
-    float pc0[SKR_KR], pc1[SKR_KR];
-    skinny_reg_q(a, kbeg, kend, Qs);
-    skinny_reg_p(a, kbeg, kend, po0, po1, pc0, pc1, skinny_reg_ko(a, kbeg, kend));
-    int32_t ko_next = skinny_reg_ko(a, kbeg + SKR_KR, kend);  // the next step's
-    int st = 0;
-#pragma unroll 1
-    for (int kb = kbeg; kb < kend; kb += SKR_KR) {
-      const int nb = kb + SKR_KR;
-      float pn0[SKR_KR], pn1[SKR_KR];
-      if (nb < kend) {
-        __syncthreads();  // stage st ^ 1 was read by the previous step
-        skinny_reg_q(a, nb, kend, Qs + (st ^ 1) * SKR_KR * SKR_ROWS);
-        skinny_reg_p(a, nb, kend, po0, po1, pn0, pn1, ko_next);
-        ko_next = skinny_reg_ko(a, nb + SKR_KR, kend);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncthreads();  // Q of this step landed
-      const float* q = Qs + st * SKR_KR * SKR_ROWS;
-#pragma unroll
-      for (int kk = 0; kk < SKR_KR; ++kk) {
-        float qv[SKR_ROWS];
-#pragma unroll
-        for (int r = 0; r < SKR_ROWS; r += 4) {
-          const float4 t = *reinterpret_cast<const float4*>(q + kk * SKR_ROWS + r);
-          qv[r] = t.x; qv[r + 1] = t.y; qv[r + 2] = t.z; qv[r + 3] = t.w;
-        }
-#pragma unroll
-        for (int r = 0; r < SKR_ROWS; ++r) {
-          acc[0][r] = fmaf(qv[r], pc0[kk], acc[0][r]);
-          acc[1][r] = fmaf(qv[r], pc1[kk], acc[1][r]);
-        }
-      }
-      if (nb < kend) {
-#pragma unroll
-        for (int kk = 0; kk < SKR_KR; ++kk) {
-          pc0[kk] = pn0[kk];
-          pc1[kk] = pn1[kk];
-        }
-      }
-      st ^= 1;
-    }
-    skinny_reg_finish(a, job, acc, os, cw, cs);
+    skinny_reg_job<ROWS>(a, job, Qs, os, pw, cw, cs);
   }
 }
 
+// ROWS = 16, or 8 for a narrow side of at most 8 (one kernel per row count:
+// both in one kernel would need more registers than four CTAs per SM leave)
+template <int ROWS>
 __global__ void __launch_bounds__(SKR_THREADS, SKR_CTAS_PER_SM)
     skinny_reg_kernel(const __grid_constant__ SkinnyArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   grid_dep_wait();
   auto resolve = [&](int J) { return SkRef{&a, J}; };
-  skinny_reg_loop(blockIdx.x, gridDim.x, a.njobs, resolve, smem);
+  skinny_reg_loop<ROWS>(blockIdx.x, gridDim.x, a.njobs, resolve, smem);
   bulk_wait_all();  // bulk C copies complete before the CTA exits
 }
 
+template <int ROWS>
 __global__ void __launch_bounds__(SKR_THREADS, SKR_CTAS_PER_SM)
     skinny_reg_group_kernel(const SkinnyItem* items, const int64_t* begin, int n, int njobs) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -1028,7 +1043,7 @@ __global__ void __launch_bounds__(SKR_THREADS, SKR_CTAS_PER_SM)
     const SkinnyItem& it = items[find_segment(begin, n, J)];
     return SkRef{&it.args, (int)(J - it.begin)};
   };
-  skinny_reg_loop(blockIdx.x, gridDim.x, njobs, resolve, smem);
+  skinny_reg_loop<ROWS>(blockIdx.x, gridDim.x, njobs, resolve, smem);
   bulk_wait_all();
 }
 

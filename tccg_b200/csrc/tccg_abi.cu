@@ -1402,9 +1402,11 @@ static cudaError_t set_attrs() {
                            (int)SKT_SMEM_BYTES));
   chk(cudaFuncSetAttribute(skinny_tc_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SKT_SMEM_BYTES));
-  chk(cudaFuncSetAttribute(skinny_reg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  chk(cudaFuncSetAttribute(skinny_reg_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SKR_SMEM_BYTES));
-  chk(cudaFuncSetAttribute(skinny_reg_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  chk(cudaFuncSetAttribute(skinny_reg_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SKR_SMEM_BYTES));
+  chk(cudaFuncSetAttribute(skinny_reg_group_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SKR_SMEM_BYTES));
   chk(cudaFuncSetAttribute(skinny_reduce_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SK_SMEM_BYTES));
@@ -1990,8 +1992,9 @@ static int run_skinny(const tccg_plan* p, const void* GA, const void* GB, float*
   mark(1, 0, s);
   if (p->sk_reg) {
     const int64_t grid = std::min<int64_t>(a.njobs, (int64_t)SKR_CTAS_PER_SM * p->num_sms);
-    launch_after(false, p, skinny_reg_kernel, dim3((unsigned)grid), dim3(SKR_THREADS),
-                 SKR_SMEM_BYTES, s, a);
+    // 8 computed rows for a narrow side of at most 8, else 16
+    launch_after(false, p, a.S <= 8 ? skinny_reg_kernel<8> : skinny_reg_kernel<16>,
+                 dim3((unsigned)grid), dim3(SKR_THREADS), SKR_SMEM_BYTES, s, a);
   } else {
     const int64_t grid = std::min<int64_t>(a.njobs, (int64_t)SK_CTAS_PER_SM * p->num_sms);
     with_skinny_rs(a.rs, [&](auto r) {
@@ -2904,9 +2907,13 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
     for (int cls = 0; cls < 3; ++cls) {
       if (wv.nsk[cls] == 0) continue;
       if (wv.sk_reg[cls]) {  // the register path (its items all take it)
+        // one launch of 16 computed rows for all of them: splitting the lane
+        // into an 8-row launch (narrow sides <= 8) and a 16-row one measured
+        // slower in configuration 5 (10.95 against 10.78 ms: two launch
+        // tails), though the 8-row kernel is faster for such an item alone
         const unsigned grid =
             (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SKR_CTAS_PER_SM * g->num_sms);
-        skinny_reg_group_kernel<<<grid, SKR_THREADS, SKR_SMEM_BYTES, s_sk>>>(
+        skinny_reg_group_kernel<16><<<grid, SKR_THREADS, SKR_SMEM_BYTES, s_sk>>>(
             g->d_sk + wv.sk0[cls], g->b_sk + wv.sk0[cls], wv.nsk[cls], (int)wv.sk_jobs[cls]);
       } else {
         const unsigned grid =

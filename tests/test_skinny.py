@@ -269,6 +269,47 @@ def test_skinny_tc_grouped_equals_per_item(cuda):
         assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= 1e-5, str(con)
 
 
+@pytest.mark.parametrize("mix", ["both", "rows8_only", "rows16_only"])
+def test_register_path_grouped_rows8_and_rows16(cuda, mix):
+    """Register-path items (narrow side <= 16), k-split ones among them: a
+    plan run of a narrow side of at most 8 takes the 8-row kernel, the
+    grouped lane computes 16 rows for every item. Each row's sums are formed
+    in the same order either way, so grouped equals the per-item runs bit for
+    bit, and both match the FP64 oracle."""
+    import torch
+    from tccg_b200.grouped import Group
+    rows8 = [("cdn", "dnxy", "yxc", dict(c=8, d=23, n=20, x=60, y=41)),       # S 8, K split
+             ("ab", "ak", "kb", dict(a=5, b=700, k=90)),                      # S 5
+             ("a", "ak", "k", dict(a=300, k=77))]                             # S 1
+    rows16 = [("ab", "ak", "kb", dict(a=13, b=900, k=70)),                    # S 13
+              ("pqn", "pqk", "kn", dict(p=40, q=30, n=16, k=45))]             # S 16
+    shapes = {"both": rows8 + rows16, "rows8_only": rows8, "rows16_only": rows16}[mix]
+    items = [make_contraction(lc, la, lb, sz, 0.5, 0.0) for lc, la, lb, sz in shapes]
+    grp = Group(items, "fp32", tunings=[Tuning(skinny=1)] * len(items))
+    for p in grp.plans:
+        assert "path=registers" in p.describe(), p.describe()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    As = [torch.randn(c.A0.num_elements(), generator=g, device="cuda") for c in items]
+    Bs = [torch.randn(c.B0.num_elements(), generator=g, device="cuda") for c in items]
+    Cs = [torch.zeros(c.C0.num_elements(), device="cuda") for c in items]
+    grp.bind(As, Bs, Cs)
+    grp.capture()
+    grp.replay()
+    torch.cuda.synchronize()
+    grouped = [c.clone() for c in Cs]
+    for c in Cs:
+        c.zero_()
+    grp.run_per_item()
+    torch.cuda.synchronize()
+    for a, b in zip(grouped, Cs):
+        assert torch.equal(a, b)
+    for con, A, B, C in zip(items, As, Bs, grouped):
+        ln = LoopNest(con.C0.labels, con.A0.labels, con.B0.labels,
+                      {i.label: i.size for t in (con.A0, con.B0, con.C0) for i in t.indices})
+        ref = ln.run(A.double().cpu().numpy(), B.double().cpu().numpy(), np.zeros(ln.size_c), 0.5, 0.0)
+        assert error_metrics(C.double().cpu().numpy(), ref)["normwise"] <= 1e-6, str(con)
+
+
 def test_skinny_choice_and_refusal(cuda):
     from tccg_b200._native import TccgError
     # item 69 of the 256-item batched workload (N = 40, K = 20, 5.0e6 positions, P
