@@ -687,6 +687,13 @@ static bool choose_skinny_tc(const tccg_plan* p) {
     return false;
   // a narrow side of at most 16 takes the CUDA-core register path instead
   // (choose_skinny): on the 8 such items 1.36 ms in sum against 1.50 ms here
+  // -- except where P's stride-one index is contracted and K spans at least
+  // 8 chunks: the register path's loads (16 consecutive k per lane) then
+  // touch 32 rows per warp load (items 40 / 48 of the 256-item batched
+  // workload: 0.21 / 0.31 ms there, 0.20 / 0.25 ms here)
+  if (p->K > SK_KC && p->sk.nblk >= 48 && p->sk.S <= 16 && p->sk.p_walk == SK_P_K &&
+      p->sk.nchunks >= 8)
+    return true;
   return p->K > SK_KC && p->sk.nblk >= 48 && p->sk.S > 16 && p->sk.S <= SKT_SMAX;
 }
 

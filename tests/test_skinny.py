@@ -328,6 +328,12 @@ def test_skinny_choice_and_refusal(cuda):
     d = Plan(items[46], "bf16x3").describe()
     assert "skinny_gett" in d and "path=registers" in d, d
     assert "skinny_tc" not in Plan(items[6], "bf16x3", tuning=Tuning(skinny=1)).describe()
+    # ... except where the wide operand's stride-one index is contracted and
+    # K spans >= 8 chunks (item 48: S = 8, 32 chunks): the tensor-core kernel;
+    # FP32 keeps the register path
+    assert "skinny_tc" in Plan(items[48], "bf16x3").describe()
+    d = Plan(items[48], "fp32").describe()
+    assert "path=registers" in d and "load=k" in d, d
     # a square GEMM is not skinny; FP64 and BF16 are not served
     sq = make_contraction("mn", "mk", "kn", dict(m=512, n=512, k=512))
     assert "skinny_gett" not in Plan(sq, "fp32").describe()
