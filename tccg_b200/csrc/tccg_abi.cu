@@ -2916,8 +2916,9 @@ static int run_wave(const tccg_group* g, const tccg_group::Wave& wv, cudaStream_
       if (wv.sk_reg[cls]) {  // the register path (its items all take it)
         // one launch of 16 computed rows for all of them: splitting the lane
         // into an 8-row launch (narrow sides <= 8) and a 16-row one measured
-        // slower in configuration 5 (10.95 against 10.78 ms: two launch
-        // tails), though the 8-row kernel is faster for such an item alone
+        // slower on the 256-item batched workload (10.95 against 10.78 ms:
+        // two launch tails), though the 8-row kernel is faster for such an
+        // item alone
         const unsigned grid =
             (unsigned)std::min<int64_t>(wv.sk_jobs[cls], (int64_t)SKR_CTAS_PER_SM * g->num_sms);
         skinny_reg_group_kernel<16><<<grid, SKR_THREADS, SKR_SMEM_BYTES, s_sk>>>(
